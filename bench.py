@@ -1,0 +1,348 @@
+"""Benchmark of the time-step hot path on B200.
+
+Workload (BASELINE configuration 3 grid and step structure): 1024 x 1024 x 64
+cells, dx = dy = 3 km, 16 km model top, moist sounding (theta 300 K, +4 K/km
+above 1 km, 90 % RH below 2 km decaying with a 1.5 km scale height to 1e-5,
+0.5 K rms seeded theta noise below 1 km), one step = dry SSPRK3 with 6 acoustic
+substeps + three-tracer SSPRK3 transport + warm rain with metric fallout
+(terminal velocity 12 m/s).  The step is run at dt = 1 s: the reference's
+discretisation is unstable at the configuration's 12 s on this grid.
+
+One JSON line is printed by rank 0.  ``value`` is whole-job cell updates per
+second (cells x steps / device time, max over ranks), with the state resident
+in HBM; ``e2e`` is the same metric through the public C-ABI with the state in
+pinned host memory, copied in and out every step.  ``--impl reference`` times
+the CPU restatement of the reference algorithm on the host cores instead.
+Under torchrun every rank advances an independent replica (the path is
+single-device; replicas scale weakly with no collective).
+"""
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 1024, 1024, 64
+DX = 3000.0
+ZTOP = 16000.0
+DT = 1.0
+NS = 6
+VT = 12.0
+
+
+def grid_spec(gwm, nx=NX, ny=NY, nz=NZ):
+    return gwm.GridSpec(nx, ny, nz, dx=DX, dy=DX, z_top=ZTOP)
+
+
+def case_params(gwm, seed=1):
+    return gwm.CaseParams(theta_ref=300.0, theta_lapse_k_per_m=0.004, relative_humidity=0.9,
+                          rh_top_m=2000.0, qv_scale_height_m=1500.0, qv_floor=1e-5,
+                          noise_rms_k=0.5, noise_depth_m=1000.0, seed=seed)
+
+
+def member_spec(gwm):
+    return gwm.MemberSpec(step=gwm.StepConfig(dt=DT, fast_substeps=NS),
+                          rain=gwm.WarmRainConfig(dt=DT, rain_terminal_velocity=VT), moist=True)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self._proc = None
+            return
+        threading.Thread(target=self._read, daemon=True).start()
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[3 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# Algorithmic bytes of one acoustic substep per cell (the dominant kernel): the
+# hot-path byte model counts 12 FP32 field accesses per cell per substep
+# (rho, theta, three momenta and three base momenta read; rho and three momenta
+# written).
+SUBSTEP_ALGO_BYTES_PER_CELL = 12 * 4
+
+
+def cpu_baseline(steps_sample=2, nx=128, ny=128):
+    import oracle
+    oracle.build()
+    threads = oracle.max_threads()
+    oracle.set_threads(threads)
+    gwm = importlib.import_module("gpu-wm-next_b200")
+    g = grid_spec(gwm, nx, ny, NZ)
+    s = gwm.build_case("moist_sounding", g, case_params(gwm), moist=True)
+    og = oracle.GridSpec(nx, ny, NZ, dx=DX, dy=DX, z_top=ZTOP)
+    st = {k: v.astype(np.float64) for k, v in s.items()}
+    t0 = time.perf_counter()
+    oracle.run(og, oracle.StepSpec(dt=DT, fast_substeps=NS), st, steps_sample,
+               phases=oracle.PHASE_DRY | oracle.PHASE_TRACERS | oracle.PHASE_RAIN,
+               rain=oracle.RainSpec(dt=DT, terminal_velocity=VT), precision=32)
+    dt = time.perf_counter() - t0
+    cells = nx * ny * NZ * steps_sample
+    return {"value": cells / dt, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+            "sample": f"{nx}x{ny}x{NZ} subdomain of the workload, {steps_sample} full moist steps, "
+                      f"FP32 oracle restatement, OpenMP {threads} threads, {dt:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    """CPU restatement of the reference algorithm (the reference has no CPU step)."""
+    if rank != 0:
+        return
+    import oracle
+    oracle.build()
+    threads = oracle.max_threads()
+    oracle.set_threads(threads)
+    gwm = importlib.import_module("gpu-wm-next_b200")
+    nx = ny = 128
+    g = grid_spec(gwm, nx, ny, NZ)
+    s = gwm.build_case("moist_sounding", g, case_params(gwm), moist=True)
+    og = oracle.GridSpec(nx, ny, NZ, dx=DX, dy=DX, z_top=ZTOP)
+    st = {k: v.astype(np.float64) for k, v in s.items()}
+    kw = dict(phases=oracle.PHASE_DRY | oracle.PHASE_TRACERS | oracle.PHASE_RAIN,
+              rain=oracle.RainSpec(dt=DT, terminal_velocity=VT), precision=32)
+    step = oracle.StepSpec(dt=DT, fast_substeps=NS)
+    for _ in range(args.warmup):
+        st = oracle.run(og, step, st, 1, **kw)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st = oracle.run(og, step, st, 1, **kw)
+    el = time.perf_counter() - t0
+    cells = nx * ny * NZ
+    val = cells * args.steps / el
+    sample = (f"{nx}x{ny}x{NZ} subdomain of the workload per step, FP32 oracle restatement "
+              f"(OpenMP {threads} threads)")
+    print(json.dumps({
+        "impl": "reference", "metric": "cell-updates/s", "value": val, "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "moist warm-rain step, BASELINE config 3 grid (sampled)",
+                   "nx": nx, "ny": ny, "nz": NZ, "dt": DT, "fast_substeps": NS},
+        "cpu_baseline": {"value": val, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": val, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--ny", type=int, default=NY)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    gwm = importlib.import_module("gpu-wm-next_b200")
+    g = grid_spec(gwm, args.nx, args.ny, NZ)
+    state = gwm.build_case("moist_sounding", g, case_params(gwm, seed=1 + rank), moist=True)
+    model = gwm.Model(g, member_spec(gwm))
+    stream = torch.cuda.Stream()
+    model.set_stream(stream.cuda_stream)
+    model.upload(state)
+    model.use_graph(True)
+    cells = args.nx * args.ny * NZ
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    # warm-up (also captures the step graph)
+    with torch.cuda.stream(stream):
+        model.step(max(args.warmup, 1))
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    t0.record(stream)
+    model.step(args.steps)
+    t1.record(stream)
+    barrier()
+    clocks.stop()
+    ms = t0.elapsed_time(t1)
+    launches = model.launch_count
+    ms_t = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = cells * args.steps * world / (ms_max * 1e-3)
+    budget = model.budgets()
+    finite = all(np.isfinite(v) for v in budget.values())
+
+    # dominant-kernel timing: one acoustic substep per launch; measured through a
+    # fast-mode-only step sequence on the same state (device events, same stream)
+    roof = substep_roofline(model, g, stream, torch)
+
+    # end-to-end through the C-ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = end_to_end(gwm, model, g, stream, torch, max(2, min(args.steps, 5)), world, dist)
+    model.close()
+
+    if rank == 0:
+        peak, which = load_peaks()
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "sim_s_per_wall_s": DT * args.steps / (ms_max * 1e-3),
+            "config": {"workload": "moist warm-rain step on the BASELINE config 3 grid",
+                       "nx": args.nx, "ny": args.ny, "nz": NZ, "dx_m": DX, "z_top_m": ZTOP,
+                       "dt_s": DT, "fast_substeps": NS, "rain_terminal_velocity": VT,
+                       "phases": "dry SSPRK3 + 3-tracer SSPRK3 + warm rain/fallout",
+                       "l2": "inputs larger than L2 (each field 282 MB)",
+                       "graph": True, "parallelism": f"replicas{world}"},
+            "gpu_launches": launches,
+            "state_finite": finite,
+            "roofline": roof,
+            "clocks": clocks.summary(),
+        }
+        line["roofline"]["peak"] = peak
+        line["roofline"]["peak_source"] = which
+        line["roofline"]["frac"] = roof["achieved"] / peak
+        if e2e:
+            line["e2e"] = e2e
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def substep_roofline(model, g, stream, torch, steps=2):
+    """Per-kernel device time from CUDA events recorded around each launch on the
+    launching stream (direct launches), for steps full steps after the timed region."""
+    with torch.cuda.stream(stream):
+        model.profile(True)
+        model.step(steps)
+        rep = model.profile_report()
+        model.profile(False)
+    cells = g.nx * g.ny * g.nz
+    fast = rep["k_fast_substep"]
+    achieved = SUBSTEP_ALGO_BYTES_PER_CELL * cells / (fast["avg_ms"] * 1e-3) / 1e9
+    total = sum(v["total_ms"] for v in rep.values())
+    shares = {k: round(v["total_ms"] / total, 4) for k, v in rep.items()}
+    return {"bound": "hbm", "achieved": achieved, "unit": "GB/s", "traffic": read_traffic(g),
+            "kernel": "k_fast_substep (one acoustic substep)",
+            "algorithmic_bytes_per_launch": SUBSTEP_ALGO_BYTES_PER_CELL * cells,
+            "avg_launch_ms": fast["avg_ms"], "kernel_shares": shares,
+            "kernel_avg_ms": {k: round(v["avg_ms"], 4) for k, v in rep.items()}}
+
+
+def read_traffic(g):
+    """DRAM bytes per substep launch from the committed ncu summary, scaled by cells."""
+    p = os.path.join(ROOT, "profiles", "k_fast_substep_dram.txt")
+    if not os.path.exists(p):
+        return None
+    vals = {}
+    for line in open(p):
+        if ":" in line:
+            k, v = line.split(":", 1)
+            vals[k.strip()] = v.strip()
+    try:
+        per_cell = float(vals["dram_bytes_per_cell"])
+    except (KeyError, ValueError):
+        return None
+    return per_cell * g.nx * g.ny * g.nz
+
+
+def end_to_end(gwm, model, g, stream, torch, steps, world, dist):
+    sh = g.shapes()
+    keys = ("rho", "rho_theta", "u", "v", "w", "qv", "qc", "qr")
+    host = {k: torch.empty(sh[k], dtype=torch.float32, pin_memory=True).numpy() for k in keys}
+    host["precip"] = torch.empty(sh["precip"], dtype=torch.float64, pin_memory=True).numpy()
+    model.download(out=host)
+    h2d = sum(host[k].nbytes for k in host)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        model.upload(host)
+        model.step(1)
+        model.download(out=host)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    el_t = torch.tensor([el], device="cuda")
+    if dist:
+        dist.all_reduce(el_t, op=dist.ReduceOp.MAX)
+    el = float(el_t.item())
+    return {"value": g.nx * g.ny * g.nz * steps * world / el, "unit": "cell-updates/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
+            "note": "full prognostic state copied host->device and back every step through the C-ABI"}
+
+
+if __name__ == "__main__":
+    main()

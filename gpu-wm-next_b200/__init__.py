@@ -1,0 +1,556 @@
+"""gwm-b200: B200-native time-step hot path of the gpu-wm-next weather model.
+
+Python front-end of ``libgwm_b200.so`` (CUDA kernels for sm_100a behind the C-ABI
+declared in ``include/gwm_b200.h``).  The object model mirrors the reference's
+operator API: a :class:`Model` owns the device state of one or more members and
+exposes ``advance_dry_state_ssprk3``, ``advance_passive_tracers_ssprk3``,
+``apply_warm_rain_microphysics``, ``compute_slow_tendencies``, the fast-mode
+integrator and the budget summaries; module functions expose the halo operators
+on the reference's per-rank layout.  Errors raise ``RuntimeError`` with the
+library's message, as the reference throws ``std::runtime_error``
+(include/gwm/core/types.hpp:24-28).
+
+There is no CPU fallback: every call runs the CUDA library, and importing the
+bindings fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_ROOT = os.path.dirname(_HERE)
+_LIB_PATH = os.path.join(_HERE, "_build", "libgwm_b200.so")
+_SOURCES = ["capi.cu", "dycore.cu", "physics.cu", "halo.cu", "cases.cpp"]
+_HEADERS = ["common.cuh", "dycore.cuh", "physics.cuh", "halo.cuh"]
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+              "-Xcompiler", "-fPIC", "-shared"]
+
+OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NO_DEVICE = 0, -1, -2, -3, -4
+CELL, FACE_X, FACE_Y, FACE_Z = 0, 1, 2, 3
+
+
+def _stale() -> bool:
+    if not os.path.exists(_LIB_PATH):
+        return True
+    t = os.path.getmtime(_LIB_PATH)
+    deps = [os.path.join(_HERE, "csrc", f) for f in _SOURCES + _HEADERS]
+    deps += [os.path.join(_ROOT, "include", f) for f in ("gwm_b200.h", "gwm_b200_cases.h")]
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile the CUDA library in-tree for sm_100a (nvcc cross-compiles without a GPU)."""
+    if not force and not _stale():
+        return _LIB_PATH
+    os.makedirs(os.path.dirname(_LIB_PATH), exist_ok=True)
+    srcs = [os.path.join(_HERE, "csrc", f) for f in _SOURCES]
+    cmd = ["nvcc", *NVCC_FLAGS, "-o", _LIB_PATH + ".tmp", *srcs]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    subprocess.run(cmd, check=True)
+    os.replace(_LIB_PATH + ".tmp", _LIB_PATH)
+    return _LIB_PATH
+
+
+# ---------------------------------------------------------------------------
+# C structures (include/gwm_b200.h, include/gwm_b200_cases.h)
+class _Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("halo", C.c_int),
+                ("ranks_x", C.c_int), ("ranks_y", C.c_int), ("periodic_x", C.c_int),
+                ("periodic_y", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
+                ("z_top", C.c_double), ("terrain_taper_eta", C.c_double),
+                ("terrain", C.POINTER(C.c_float)), ("eta_interfaces", C.POINTER(C.c_double))]
+
+
+class _Step(C.Structure):
+    _fields_ = [("dt", C.c_float), ("fast_substeps", C.c_int), ("gravity", C.c_float),
+                ("fast_update_horizontal_momentum", C.c_int), ("fast_update_density", C.c_int),
+                ("enable_fast_modes", C.c_int)]
+
+
+class _Rain(C.Structure):
+    _fields_ = [("dt", C.c_float), ("condensation_relaxation", C.c_float),
+                ("cloud_autoconversion_threshold", C.c_float),
+                ("cloud_autoconversion_rate", C.c_float), ("rain_evaporation_rate", C.c_float),
+                ("rain_terminal_velocity", C.c_float), ("sedimentation_layer_depth_m", C.c_float),
+                ("enable_latent_heating", C.c_int)]
+
+
+class _Member(C.Structure):
+    _fields_ = [("moist", C.c_int), ("enable_tracer_transport", C.c_int),
+                ("enable_warm_rain", C.c_int), ("step", _Step), ("rain", _Rain)]
+
+
+class _Fields(C.Structure):
+    _fields_ = [("rho_d", C.POINTER(C.c_float)), ("rho_theta_m", C.POINTER(C.c_float)),
+                ("mom_u", C.POINTER(C.c_float)), ("mom_v", C.POINTER(C.c_float)),
+                ("mom_w", C.POINTER(C.c_float)), ("qv", C.POINTER(C.c_float)),
+                ("qc", C.POINTER(C.c_float)), ("qr", C.POINTER(C.c_float)),
+                ("precip", C.POINTER(C.c_double))]
+
+
+_BUDGET_KEYS = ("total_dry_mass", "total_rho_theta_m", "total_horizontal_momentum_x",
+                "total_horizontal_momentum_y", "total_vertical_momentum", "rho_min", "rho_max",
+                "theta_min", "theta_max", "u_min", "u_max", "v_min", "v_max", "w_min", "w_max",
+                "vapor_water_path_sum_kg_m2", "cloud_water_path_sum_kg_m2",
+                "rain_water_path_sum_kg_m2", "accumulated_surface_precipitation_sum_mm",
+                "mean_surface_precipitation_mm", "max_surface_precipitation_mm")
+
+
+class _Budget(C.Structure):
+    _fields_ = [(k, C.c_double) for k in _BUDGET_KEYS]
+
+
+class _LayoutDesc(C.Structure):
+    _fields_ = [(k, C.c_int) for k in ("global_nx", "global_ny", "nz", "halo", "ranks_x",
+                                       "ranks_y", "periodic_x", "periodic_y")]
+
+
+class _CaseParams(C.Structure):
+    _fields_ = [(k, C.c_float) for k in (
+        "rho_background", "theta_background", "u_background", "v_background", "w_background",
+        "center_x_fraction", "center_y_fraction", "center_z_fraction", "radius_x_fraction",
+        "radius_y_fraction", "radius_z_fraction", "theta_perturbation", "rho_surface",
+        "theta_ref", "p_surface", "theta_lapse_k_per_m", "relative_humidity", "rh_top_m",
+        "qv_scale_height_m", "qv_floor", "noise_rms_k", "noise_depth_m")] + [("seed", C.c_uint64)]
+
+
+class _TerrainParams(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("height", "center_x_fraction", "center_y_fraction",
+                                          "half_width_x", "half_width_y")]
+
+
+_lib = None
+
+
+def lib():
+    """Load libgwm_b200.so (building it first when sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if _stale():
+        build()
+    if not os.path.exists(_LIB_PATH):
+        raise RuntimeError(f"gwm-b200: CUDA library missing at {_LIB_PATH}; run build()")
+    L = C.CDLL(_LIB_PATH)
+    vp = C.c_void_p
+    L.gwm_b200_create.argtypes = [C.POINTER(_Grid), C.POINTER(_Member), C.c_int, C.POINTER(vp)]
+    L.gwm_b200_destroy.argtypes = [vp]
+    L.gwm_b200_destroy.restype = None
+    L.gwm_b200_last_error.argtypes = [vp]
+    L.gwm_b200_last_error.restype = C.c_char_p
+    for name in ("gwm_b200_step", "gwm_b200_advance_dry"):
+        getattr(L, name).argtypes = [vp, C.c_int]
+    L.gwm_b200_warm_rain.argtypes = [vp, C.c_int]
+    L.gwm_b200_advance_tracers.argtypes = [vp]
+    L.gwm_b200_fast_modes.argtypes = [vp]
+    L.gwm_b200_synchronize.argtypes = [vp]
+    L.gwm_b200_use_graph.argtypes = [vp, C.c_int]
+    L.gwm_b200_set_stream.argtypes = [vp, vp]
+    L.gwm_b200_upload.argtypes = [vp, C.c_int, C.POINTER(_Fields)]
+    L.gwm_b200_download.argtypes = [vp, C.c_int, C.POINTER(_Fields)]
+    L.gwm_b200_slow_tendencies.argtypes = [vp, C.c_int, C.POINTER(_Fields)]
+    L.gwm_b200_budgets.argtypes = [vp, C.c_int, C.POINTER(_Budget)]
+    L.gwm_b200_profile.argtypes = [vp, C.c_int]
+    L.gwm_b200_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_longlong), C.POINTER(C.c_char_p)]
+    L.gwm_b200_launch_count.argtypes = [vp]
+    L.gwm_b200_launch_count.restype = C.c_longlong
+    L.gwm_b200_layout.argtypes = [C.POINTER(_LayoutDesc), C.POINTER(C.c_int), C.c_int]
+    L.gwm_b200_halo_exchange.argtypes = [C.POINTER(_LayoutDesc), C.c_int, C.c_int,
+                                         C.POINTER(C.c_void_p), vp]
+    L.gwm_b200_dry_pressure.argtypes = [vp, vp, vp, C.c_longlong, vp]
+    L.gwm_b200_ranks_to_global.argtypes = [C.POINTER(_LayoutDesc), C.c_int,
+                                           C.POINTER(C.c_void_p), vp]
+    L.gwm_b200_global_to_ranks.argtypes = [C.POINTER(_LayoutDesc), C.c_int, vp,
+                                           C.POINTER(C.c_void_p)]
+    L.gwm_b200_build_case.argtypes = [C.c_char_p, C.POINTER(_Grid), C.POINTER(_CaseParams),
+                                      C.POINTER(_Fields)]
+    L.gwm_b200_build_terrain.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_double,
+                                         C.POINTER(_TerrainParams), C.POINTER(C.c_float)]
+    _lib = L
+    return L
+
+
+# C-ABI symbols the header declares (checked by the CPU test-suite).
+EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b200_set_stream",
+            "gwm_b200_synchronize", "gwm_b200_use_graph", "gwm_b200_upload", "gwm_b200_download",
+            "gwm_b200_step", "gwm_b200_advance_dry", "gwm_b200_advance_tracers",
+            "gwm_b200_warm_rain", "gwm_b200_fast_modes", "gwm_b200_slow_tendencies",
+            "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_layout",
+            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_ranks_to_global",
+            "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
+
+
+# ---------------------------------------------------------------------------
+@dataclass
+class GridSpec:
+    """RectilinearDomainConfig / GridMetrics inputs (idealized_domain_builder.hpp:12-31)."""
+    nx: int
+    ny: int
+    nz: int
+    dx: float = 1000.0
+    dy: float = 1000.0
+    z_top: float = 16000.0
+    periodic_x: bool = True
+    periodic_y: bool = True
+    ranks_x: int = 1
+    ranks_y: int = 1
+    halo: int = 1
+    terrain_taper_eta: float = 0.25
+    terrain: Optional[np.ndarray] = None
+    eta_interfaces: Optional[np.ndarray] = None
+
+    def c(self) -> _Grid:
+        g = _Grid(self.nx, self.ny, self.nz, self.halo, self.ranks_x, self.ranks_y,
+                  int(self.periodic_x), int(self.periodic_y), self.dx, self.dy, self.z_top,
+                  self.terrain_taper_eta, None, None)
+        if self.terrain is not None:
+            self._t = np.ascontiguousarray(self.terrain, dtype=np.float32)
+            assert self._t.shape == (self.ny, self.nx)
+            g.terrain = self._t.ctypes.data_as(C.POINTER(C.c_float))
+        if self.eta_interfaces is not None:
+            self._e = np.ascontiguousarray(self.eta_interfaces, dtype=np.float64)
+            assert self._e.shape == (self.nz + 1,)
+            g.eta_interfaces = self._e.ctypes.data_as(C.POINTER(C.c_double))
+        return g
+
+    def shapes(self) -> Dict[str, tuple]:
+        nx, ny, nz = self.nx, self.ny, self.nz
+        return {"rho": (nz, ny, nx), "rho_theta": (nz, ny, nx), "u": (nz, ny, nx + 1),
+                "v": (nz, ny + 1, nx), "w": (nz + 1, ny, nx), "qv": (nz, ny, nx),
+                "qc": (nz, ny, nx), "qr": (nz, ny, nx), "precip": (ny, nx)}
+
+
+@dataclass
+class StepConfig:
+    """DryStepperConfig (include/gwm/dycore/dry_core.hpp:50-56)."""
+    dt: float = 2.0
+    fast_substeps: int = 1
+    gravity: float = 9.81
+    fast_update_horizontal_momentum: bool = True
+    fast_update_density: bool = True
+    enable_fast_modes: bool = True
+
+    def c(self) -> _Step:
+        return _Step(self.dt, self.fast_substeps, self.gravity,
+                     int(self.fast_update_horizontal_momentum), int(self.fast_update_density),
+                     int(self.enable_fast_modes))
+
+
+@dataclass
+class WarmRainConfig:
+    """WarmRainConfig (include/gwm/physics/warm_rain.hpp:14-23)."""
+    dt: float = 2.0
+    condensation_relaxation: float = 1.0
+    cloud_autoconversion_threshold: float = 1.0e-4
+    cloud_autoconversion_rate: float = 1.0e-3
+    rain_evaporation_rate: float = 5.0e-3
+    rain_terminal_velocity: float = 0.0
+    sedimentation_layer_depth_m: float = 0.0
+    enable_latent_heating: bool = True
+
+    def c(self) -> _Rain:
+        return _Rain(self.dt, self.condensation_relaxation, self.cloud_autoconversion_threshold,
+                     self.cloud_autoconversion_rate, self.rain_evaporation_rate,
+                     self.rain_terminal_velocity, self.sedimentation_layer_depth_m,
+                     int(self.enable_latent_heating))
+
+
+@dataclass
+class MemberSpec:
+    step: StepConfig = field(default_factory=StepConfig)
+    rain: WarmRainConfig = field(default_factory=WarmRainConfig)
+    moist: bool = False
+    enable_tracer_transport: bool = True
+    enable_warm_rain: bool = True
+
+    def c(self) -> _Member:
+        return _Member(int(self.moist), int(self.enable_tracer_transport),
+                       int(self.enable_warm_rain), self.step.c(), self.rain.c())
+
+
+STATE_KEYS = ("rho", "rho_theta", "u", "v", "w")
+TRACER_KEYS = ("qv", "qc", "qr")
+_C_NAMES = {"rho": "rho_d", "rho_theta": "rho_theta_m", "u": "mom_u", "v": "mom_v",
+            "w": "mom_w", "qv": "qv", "qc": "qc", "qr": "qr"}
+
+
+def _fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Model:
+    """Device state of one or more independent members behind ``gwm_b200_ctx``."""
+
+    def __init__(self, grids, members):
+        if isinstance(grids, GridSpec):
+            grids = [grids]
+        if isinstance(members, MemberSpec):
+            members = [members]
+        if len(grids) != len(members):
+            raise ValueError("one MemberSpec per GridSpec")
+        self.grids = list(grids)
+        self.members = list(members)
+        L = lib()
+        gs = (_Grid * len(grids))(*[g.c() for g in grids])
+        ms = (_Member * len(members))(*[m.c() for m in members])
+        h = C.c_void_p()
+        rc = L.gwm_b200_create(gs, ms, len(grids), C.byref(h))
+        if rc == ERR_NO_DEVICE:
+            raise RuntimeError("gwm-b200: no CUDA device visible (the library has no CPU path)")
+        if rc != OK:
+            raise RuntimeError(f"gwm-b200: create failed with status {rc}")
+        self._h = h
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gwm_b200_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            msg = lib().gwm_b200_last_error(self._h).decode()
+            raise RuntimeError(f"gwm-b200 {what}: status {rc}: {msg}")
+
+    # -- I/O
+    def upload(self, state: Dict[str, np.ndarray], member: int = 0):
+        g = self.grids[member]
+        sh = g.shapes()
+        f = _Fields()
+        keep = []
+        for k, cname in _C_NAMES.items():
+            if state.get(k) is not None:
+                a = np.ascontiguousarray(state[k], dtype=np.float32)
+                if a.shape != sh[k]:
+                    raise ValueError(f"{k}: shape {a.shape} != {sh[k]}")
+                keep.append(a)
+                setattr(f, cname, _fptr(a))
+        if state.get("precip") is not None:
+            p = np.ascontiguousarray(state["precip"], dtype=np.float64)
+            keep.append(p)
+            f.precip = p.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(lib().gwm_b200_upload(self._h, member, C.byref(f)), "upload")
+
+    def download(self, member: int = 0, keys: Optional[Sequence[str]] = None,
+                 out: Optional[Dict[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:
+        """Copy the state to host arrays (new ones, or the given ``out`` arrays)."""
+        g = self.grids[member]
+        sh = g.shapes()
+        moist = self.members[member].moist
+        if keys is None:
+            keys = list(out) if out else STATE_KEYS + ((TRACER_KEYS + ("precip",)) if moist else ())
+        out = {} if out is None else out
+        f = _Fields()
+        for k in keys:
+            dtype = np.float64 if k == "precip" else np.float32
+            if k not in out:
+                out[k] = np.zeros(sh[k], dtype=dtype)
+            a = out[k]
+            if a.shape != sh[k] or a.dtype != dtype or not a.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"download target {k} must be a C-contiguous {dtype} array of {sh[k]}")
+            if k == "precip":
+                f.precip = a.ctypes.data_as(C.POINTER(C.c_double))
+            else:
+                setattr(f, _C_NAMES[k], _fptr(a))
+        self._check(lib().gwm_b200_download(self._h, member, C.byref(f)), "download")
+        return out
+
+    # -- operators
+    def step(self, nsteps: int = 1):
+        """The prepared-case driver loop (gwm_prepared_case_driver.cpp:427-463)."""
+        self._check(lib().gwm_b200_step(self._h, nsteps), "step")
+
+    def advance_dry_state_ssprk3(self, nsteps: int = 1):
+        self._check(lib().gwm_b200_advance_dry(self._h, nsteps), "advance_dry_state_ssprk3")
+
+    def advance_passive_tracers_ssprk3(self):
+        self._check(lib().gwm_b200_advance_tracers(self._h), "advance_passive_tracers_ssprk3")
+
+    def apply_warm_rain_microphysics(self, fallout: Optional[str] = "metric"):
+        mode = {None: 0, "none": 0, "metric": 1, "nominal": 2}[fallout]
+        self._check(lib().gwm_b200_warm_rain(self._h, mode), "apply_warm_rain_microphysics")
+
+    def fast_modes(self):
+        """LocalSplitExplicitFastMode::apply on the current state."""
+        self._check(lib().gwm_b200_fast_modes(self._h), "fast_modes")
+
+    def compute_slow_tendencies(self, member: int = 0) -> Dict[str, np.ndarray]:
+        sh = self.grids[member].shapes()
+        out = {k: np.zeros(sh[k], dtype=np.float32) for k in STATE_KEYS}
+        f = _Fields()
+        for k in STATE_KEYS:
+            setattr(f, _C_NAMES[k], _fptr(out[k]))
+        self._check(lib().gwm_b200_slow_tendencies(self._h, member, C.byref(f)),
+                    "compute_slow_tendencies")
+        return out
+
+    def budgets(self, member: int = 0) -> Dict[str, float]:
+        b = _Budget()
+        self._check(lib().gwm_b200_budgets(self._h, member, C.byref(b)), "budgets")
+        return {k: getattr(b, k) for k in _BUDGET_KEYS}
+
+    def use_graph(self, enable: bool = True):
+        self._check(lib().gwm_b200_use_graph(self._h, int(enable)), "use_graph")
+
+    def set_stream(self, stream_handle: Optional[int]):
+        self._check(lib().gwm_b200_set_stream(self._h, stream_handle), "set_stream")
+
+    def synchronize(self):
+        self._check(lib().gwm_b200_synchronize(self._h), "synchronize")
+
+    @property
+    def launch_count(self) -> int:
+        return int(lib().gwm_b200_launch_count(self._h))
+
+    def profile(self, enable: bool = True):
+        """Per-kernel CUDA-event timing of subsequent direct (non-graph) launches."""
+        self._check(lib().gwm_b200_profile(self._h, int(enable)), "profile")
+
+    def profile_report(self) -> Dict[str, Dict[str, float]]:
+        rep = {}
+        n = lib().gwm_b200_profile_read(self._h, 0, None, None, None)
+        for kind in range(n):
+            ms, cnt, name = C.c_double(), C.c_longlong(), C.c_char_p()
+            lib().gwm_b200_profile_read(self._h, kind, C.byref(ms), C.byref(cnt), C.byref(name))
+            if cnt.value:
+                rep[name.value.decode()] = {"total_ms": ms.value, "launches": cnt.value,
+                                            "avg_ms": ms.value / cnt.value}
+        return rep
+
+
+# ---------------------------------------------------------------------------
+def _layout_desc(nx, ny, nz, halo, rx, ry, px, py) -> _LayoutDesc:
+    return _LayoutDesc(nx, ny, nz, halo, rx, ry, int(px), int(py))
+
+
+def layout(nx, ny, nz, halo=1, ranks_x=1, ranks_y=1, periodic_x=True, periodic_y=True) -> np.ndarray:
+    """VirtualRankLayout::build + neighbours: rows of 12 ints per rank."""
+    d = _layout_desc(nx, ny, nz, halo, ranks_x, ranks_y, periodic_x, periodic_y)
+    out = np.zeros(12 * ranks_x * ranks_y, dtype=np.int32)
+    n = lib().gwm_b200_layout(C.byref(d), out.ctypes.data_as(C.POINTER(C.c_int)), ranks_x * ranks_y)
+    if n < 0:
+        raise RuntimeError(f"layout: status {n}")
+    return out.reshape(n, 12)
+
+
+def halo_exchange(rank_ptrs: Sequence[int], nx, ny, nz, halo, ranks_x, ranks_y, periodic_x,
+                  periodic_y, orientation: int, op: str = "exchange", stream: Optional[int] = None):
+    """HaloExchange::exchange_* / synchronize_owned_face_interfaces on device buffers."""
+    d = _layout_desc(nx, ny, nz, halo, ranks_x, ranks_y, periodic_x, periodic_y)
+    arr = (C.c_void_p * len(rank_ptrs))(*rank_ptrs)
+    rc = lib().gwm_b200_halo_exchange(C.byref(d), orientation, 0 if op == "exchange" else 1, arr,
+                                      stream)
+    if rc != OK:
+        raise RuntimeError(f"halo_exchange: status {rc}")
+
+
+def dry_pressure(rho_ptr: int, rho_theta_ptr: int, p_ptr: int, n: int, stream: Optional[int] = None):
+    rc = lib().gwm_b200_dry_pressure(rho_ptr, rho_theta_ptr, p_ptr, n, stream)
+    if rc != OK:
+        raise RuntimeError(f"dry_pressure: status {rc}")
+
+
+def ranks_to_global(rank_arrays: Sequence[np.ndarray], nx, ny, nz, halo, ranks_x, ranks_y,
+                    periodic_x, periodic_y, orientation: int) -> np.ndarray:
+    d = _layout_desc(nx, ny, nz, halo, ranks_x, ranks_y, periodic_x, periodic_y)
+    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in rank_arrays]
+    shp = (nz + (orientation == 3), ny + (orientation == 2), nx + (orientation == 1))
+    out = np.zeros(shp, dtype=np.float32)
+    ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    rc = lib().gwm_b200_ranks_to_global(C.byref(d), orientation, ptrs, out.ctypes.data)
+    if rc != OK:
+        raise RuntimeError(f"ranks_to_global: status {rc}")
+    return out
+
+
+def global_to_ranks(glob: np.ndarray, rank_arrays: Sequence[np.ndarray], nx, ny, nz, halo,
+                    ranks_x, ranks_y, periodic_x, periodic_y, orientation: int):
+    d = _layout_desc(nx, ny, nz, halo, ranks_x, ranks_y, periodic_x, periodic_y)
+    g = np.ascontiguousarray(glob, dtype=np.float32)
+    for a in rank_arrays:
+        assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    ptrs = (C.c_void_p * len(rank_arrays))(*[a.ctypes.data for a in rank_arrays])
+    rc = lib().gwm_b200_global_to_ranks(C.byref(d), orientation, g.ctypes.data, ptrs)
+    if rc != OK:
+        raise RuntimeError(f"global_to_ranks: status {rc}")
+
+
+@dataclass
+class CaseParams:
+    """ThermoBubbleConfig + MountainWaveBackgroundConfig + moist sounding parameters."""
+    rho_background: float = 1.0
+    theta_background: float = 300.0
+    u_background: float = 0.0
+    v_background: float = 0.0
+    w_background: float = 0.0
+    center_x_fraction: float = 0.5
+    center_y_fraction: float = 0.5
+    center_z_fraction: float = 0.5
+    radius_x_fraction: float = 0.1
+    radius_y_fraction: float = 0.1
+    radius_z_fraction: float = 0.1
+    theta_perturbation: float = 2.0
+    rho_surface: float = 1.18
+    theta_ref: float = 300.0
+    p_surface: float = 100000.0
+    theta_lapse_k_per_m: float = 0.004
+    relative_humidity: float = 0.9
+    rh_top_m: float = 2000.0
+    qv_scale_height_m: float = 1500.0
+    qv_floor: float = 1.0e-5
+    noise_rms_k: float = 0.0
+    noise_depth_m: float = 1000.0
+    seed: int = 0
+
+    def c(self) -> _CaseParams:
+        vals = [getattr(self, n) for n, _ in _CaseParams._fields_]
+        return _CaseParams(*vals)
+
+
+def build_case(kind: str, grid: GridSpec, params: CaseParams, moist: bool = False) -> Dict[str, np.ndarray]:
+    """Initial state in the field I/O layout (C++ case builders of the library)."""
+    sh = grid.shapes()
+    keys = STATE_KEYS + ((TRACER_KEYS + ("precip",)) if moist else ())
+    out = {k: np.zeros(sh[k], dtype=np.float64 if k == "precip" else np.float32) for k in keys}
+    f = _Fields()
+    for k in keys:
+        if k == "precip":
+            f.precip = out[k].ctypes.data_as(C.POINTER(C.c_double))
+        else:
+            setattr(f, _C_NAMES[k], _fptr(out[k]))
+    gc, pc = grid.c(), params.c()
+    rc = lib().gwm_b200_build_case(kind.encode(), C.byref(gc), C.byref(pc), C.byref(f))
+    if rc != OK:
+        raise RuntimeError(f"build_case({kind}): status {rc}")
+    return out
+
+
+def build_terrain(kind: str, nx: int, ny: int, dx: float, dy: float, height: float = 0.0,
+                  center_x_fraction: float = 0.5, center_y_fraction: float = 0.5,
+                  half_width_x: float = 0.15, half_width_y: float = 0.15) -> np.ndarray:
+    out = np.zeros((ny, nx), dtype=np.float32)
+    p = _TerrainParams(height, center_x_fraction, center_y_fraction, half_width_x, half_width_y)
+    rc = lib().gwm_b200_build_terrain(kind.encode(), nx, ny, dx, dy, C.byref(p), _fptr(out))
+    if rc != OK:
+        raise RuntimeError(f"build_terrain({kind}): status {rc}")
+    return out

@@ -1,0 +1,979 @@
+// capi.cu — the C-ABI of libgwm_b200.so: context, device buffer plan, step
+// sequencing, state I/O, budgets and the halo operators.
+//
+// Buffer plan of one member (all fields share one padded geometry, see common.cuh):
+//   Q[5]        step state: rho_d, rho_theta_m, mom_u, mom_v, mom_w
+//   R[2]        density during a step (ping-pong between kernels)
+//   TH[2]       theta frozen for an RK stage (ping-pong between stages)
+//   B[2][3]     stage base momenta written by the slow kernel
+//   D[2][3]     acoustic momentum increments m - m_base (ping-pong between substeps)
+//   T0/T1/T2    tracer masses (state and two stage buffers), moist members
+//   precip      FP64 surface accumulation + Neumaier compensation
+//   acc         ring of three fixed-point level-sum slots (theta, or rho and p)
+// A kernel at ring position n reads slot n%3, accumulates into (n+1)%3 and clears
+// (n+2)%3; a dry step launches 3*(1+ns) ring kernels, a multiple of three, so the
+// slot pattern of every step is the same and one captured graph replays any step.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gwm_b200.h"
+#include "common.cuh"
+#include "dycore.cuh"
+#include "halo.cuh"
+#include "physics.cuh"
+
+using namespace gwmb;
+
+namespace {
+
+constexpr int kSlot = 2 * kMaxNz;  // ulls per ring slot (a, b)
+
+struct Member {
+  gwm_b200_grid_desc gd{};
+  gwm_b200_member_desc md{};
+  std::vector<float> terrain;
+  std::vector<double> eta;
+  Geom g{};
+  bool terrain_active = false;
+  size_t field_elems = 0;
+  char* block = nullptr;
+  float* Q[5]{};
+  float* R[2]{};
+  float* TH[2]{};
+  float* B[2][3]{};
+  float* D[2][3]{};
+  float* T0[3]{};
+  float* T1[3]{};
+  float* T2[3]{};
+  float *zc = nullptr, *idc = nullptr, *idf = nullptr;
+  double *precip = nullptr, *pcomp = nullptr;
+  unsigned long long* acc = nullptr;
+  float* staging = nullptr;
+  double* red_part = nullptr;
+  ReduceOut* red_out = nullptr;
+  int ring = 0;
+  bool theta_valid = false;
+
+  unsigned long long* slot(int s) { return acc + (size_t)(((s % 3) + 3) % 3) * kSlot; }
+};
+
+}  // namespace
+
+// Per-kernel CUDA-event timing (profiling mode, direct launches only).
+enum KernelKind { kKSlow = 0, kKFast, kKTracer, kKRain, kKOther, kKinds };
+const char* const kKindNames[kKinds] = {"k_slow_stage", "k_fast_substep", "k_tracer_stage",
+                                        "k_warm_rain", "other"};
+
+struct gwm_b200_ctx {
+  std::vector<Member> m;
+  bool profile = false;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_events;
+  double prof_ms[kKinds] = {0, 0, 0, 0, 0};
+  long long prof_n[kKinds] = {0, 0, 0, 0, 0};
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  bool use_graph = false;
+  cudaGraphExec_t graph = nullptr;
+  long long graph_launches = 0;
+  long long launches = 0;
+  long long cur_launches = 0;
+};
+
+namespace {
+
+int fail(gwm_b200_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                           \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(c, GWM_B200_ERR_CUDA,                                                    \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Hybrid-height metrics, FP64 compute and FP32 store: grid_metrics.hpp:87-239.
+struct HostMetrics {
+  std::vector<float> zc, idc, idf;  // unpadded (k, j, i)
+};
+
+double terrain_weight(double eta, double taper) {  // grid_metrics.hpp:126-144
+  if (eta <= 0.0) return 1.0;
+  if (eta >= 1.0) return 0.0;
+  if (taper <= 0.0) {
+    const double s = std::clamp(eta, 0.0, 1.0);
+    return 1.0 - s * s * (3.0 - 2.0 * s);
+  }
+  if (eta <= taper) return 1.0;
+  const double s = std::clamp((eta - taper) / std::max(1.0e-9, 1.0 - taper), 0.0, 1.0);
+  return 1.0 - s * s * (3.0 - 2.0 * s);
+}
+
+HostMetrics build_metrics(const Member& M) {
+  const int nx = M.gd.nx, ny = M.gd.ny, nz = M.gd.nz;
+  const double zt = M.gd.z_top, taper = M.gd.terrain_taper_eta;
+  std::vector<double> ei(nz + 1), ec(nz), bi(nz + 1), bc(nz), zi(nz + 1), zcc(nz);
+  for (int k = 0; k <= nz; ++k) {
+    ei[k] = M.eta.empty() ? (double)k / (double)nz : M.eta[k];
+    bi[k] = terrain_weight(ei[k], taper);
+    zi[k] = ei[k] * zt;
+  }
+  for (int k = 0; k < nz; ++k) {
+    ec[k] = M.eta.empty() ? ((double)k + 0.5) / (double)nz : 0.5 * (M.eta[k] + M.eta[k + 1]);
+    bc[k] = terrain_weight(ec[k], taper);
+    zcc[k] = ec[k] * zt;
+  }
+  HostMetrics H;
+  const size_t plane = (size_t)nx * ny;
+  H.zc.resize(plane * nz);
+  H.idc.resize(plane * nz);
+  H.idf.resize(plane * (nz + 1));
+  std::vector<float> zim(nz + 1);
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const double th = M.terrain.empty() ? 0.0 : (double)M.terrain[(size_t)j * nx + i];
+      for (int k = 0; k <= nz; ++k) {
+        zim[k] = (float)(zi[k] + bi[k] * th);
+        float f = 0.0f;
+        if (k > 0 && k < nz) {
+          const double dzf = (zcc[k] + bc[k] * th) - (zcc[k - 1] + bc[k - 1] * th);
+          f = (float)(1.0 / std::max(dzf, 1.0e-6));
+        }
+        H.idf[((size_t)k * ny + j) * nx + i] = f;
+      }
+      for (int k = 0; k < nz; ++k) {
+        H.zc[((size_t)k * ny + j) * nx + i] = (float)(zcc[k] + bc[k] * th);
+        const double dzc = (double)zim[k + 1] - (double)zim[k];
+        H.idc[((size_t)k * ny + j) * nx + i] = (float)(1.0 / std::max(dzc, 1.0e-6));
+      }
+    }
+  return H;
+}
+
+// Pad an unpadded metric field into the field geometry; halo columns take the
+// periodically wrapped values (the reference indexes metrics with
+// wrap_metric_index, dry_fast_modes.cu:24-30) or the clamped edge on open axes.
+std::vector<float> pad_metric(const Member& M, const std::vector<float>& src, int levels) {
+  const Geom& g = M.g;
+  std::vector<float> out((size_t)g.plane * (g.nz + 1), 0.0f);
+  auto wrap = [](int v, int n, bool per) {
+    if (per) { int m = v % n; return m < 0 ? m + n : m; }
+    return std::clamp(v, 0, n - 1);
+  };
+  for (int k = 0; k < levels; ++k)
+    for (int j = -1; j <= g.ny + 1; ++j)
+      for (int i = -1; i <= g.nx + 1; ++i) {
+        const int si = wrap(i, g.nx, g.per_x), sj = wrap(j, g.ny, g.per_y);
+        out[gidx(g, i, j, k)] = src[((size_t)k * g.ny + sj) * g.nx + si];
+      }
+  return out;
+}
+
+int alloc_member(gwm_b200_ctx* c, Member& M) {
+  const gwm_b200_grid_desc& d = M.gd;
+  Geom& g = M.g;
+  g.nx = d.nx; g.ny = d.ny; g.nz = d.nz;
+  g.pitch = ((kXOff + d.nx + 2 + 31) / 32) * 32;
+  g.rows = d.ny + 3;
+  g.plane = g.pitch * g.rows;
+  g.per_x = d.periodic_x ? 1 : 0;
+  g.per_y = d.periodic_y ? 1 : 0;
+  g.dx = (float)d.dx;
+  g.dy = (float)d.dy;
+  M.field_elems = (size_t)g.plane * (g.nz + 1);
+  const size_t fbytes = ((M.field_elems * sizeof(float) + 255) / 256) * 256;
+  const bool moist = M.md.moist != 0;
+  const int nfields = 5 + 2 + 2 + 6 + 6 + (moist ? 9 : 0) + (M.terrain_active ? 3 : 0);
+  const size_t owned_max = (size_t)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
+  const size_t plane2 = (size_t)d.nx * d.ny;
+  const size_t extra = ((2 * plane2 * sizeof(double) + 255) / 256) * 256 +
+                       3 * kSlot * sizeof(unsigned long long) + owned_max * sizeof(float) +
+                       3 * kReduceBlocks * sizeof(double) + 32 * sizeof(ReduceOut) + 4096 +
+                       3 * 4 * (kMaxNz + 1) * sizeof(float);
+  const size_t total = nfields * fbytes + extra;
+  CK(cudaMalloc(&M.block, total));
+  CK(cudaMemsetAsync(M.block, 0, total, c->stream));
+  char* p = M.block;
+  auto take = [&](size_t bytes) { char* r = p; p += ((bytes + 255) / 256) * 256; return r; };
+  for (auto& q : M.Q) q = (float*)take(fbytes);
+  for (auto& q : M.R) q = (float*)take(fbytes);
+  for (auto& q : M.TH) q = (float*)take(fbytes);
+  for (auto& b : M.B) for (auto& q : b) q = (float*)take(fbytes);
+  for (auto& b : M.D) for (auto& q : b) q = (float*)take(fbytes);
+  if (moist) {
+    for (auto& q : M.T0) q = (float*)take(fbytes);
+    for (auto& q : M.T1) q = (float*)take(fbytes);
+    for (auto& q : M.T2) q = (float*)take(fbytes);
+  }
+  M.precip = (double*)take(plane2 * sizeof(double));
+  M.pcomp = (double*)take(plane2 * sizeof(double));
+  M.acc = (unsigned long long*)take(3 * kSlot * sizeof(unsigned long long));
+  M.staging = (float*)take(owned_max * sizeof(float));
+  M.red_part = (double*)take(3 * kReduceBlocks * sizeof(double));
+  M.red_out = (ReduceOut*)take(32 * sizeof(ReduceOut));
+  // metrics
+  const HostMetrics H = build_metrics(M);
+  if (M.terrain_active) {
+    M.zc = (float*)take(fbytes);
+    M.idc = (float*)take(fbytes);
+    M.idf = (float*)take(fbytes);
+    const auto zc = pad_metric(M, H.zc, d.nz), idc = pad_metric(M, H.idc, d.nz),
+               idf = pad_metric(M, H.idf, d.nz + 1);
+    CK(cudaMemcpy(M.zc, zc.data(), zc.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(M.idc, idc.data(), idc.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(M.idf, idf.data(), idf.size() * sizeof(float), cudaMemcpyHostToDevice));
+  } else {  // horizontally uniform: one value per level
+    M.zc = (float*)take((kMaxNz + 1) * sizeof(float));
+    M.idc = (float*)take((kMaxNz + 1) * sizeof(float));
+    M.idf = (float*)take((kMaxNz + 1) * sizeof(float));
+    std::vector<float> zc(d.nz), idc(d.nz), idf(d.nz + 1);
+    const size_t plane = (size_t)d.nx * d.ny;
+    for (int k = 0; k < d.nz; ++k) { zc[k] = H.zc[k * plane]; idc[k] = H.idc[k * plane]; }
+    for (int k = 0; k <= d.nz; ++k) idf[k] = H.idf[k * plane];
+    CK(cudaMemcpy(M.zc, zc.data(), zc.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(M.idc, idc.data(), idc.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(M.idf, idf.data(), idf.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if ((size_t)(p - M.block) > total) return fail(c, GWM_B200_ERR_ARG, "internal: buffer plan overflow");
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+int count_launch(gwm_b200_ctx* c, cudaError_t e, const char* what) {
+  ++c->cur_launches;
+  if (e != cudaSuccess) return fail(c, GWM_B200_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return GWM_B200_OK;
+}
+
+int kind_of(const char* name) {
+  const std::string n(name);
+  if (n == "slow stage") return kKSlow;
+  if (n == "fast substep") return kKFast;
+  if (n == "tracer stage") return kKTracer;
+  if (n == "warm rain") return kKRain;
+  return kKOther;
+}
+
+void prof_begin(gwm_b200_ctx* c, cudaEvent_t* e0) {
+  *e0 = nullptr;
+  if (!c->profile) return;
+  cudaEventCreate(e0);
+  cudaEventRecord(*e0, c->stream);
+}
+void prof_end(gwm_b200_ctx* c, cudaEvent_t e0, const char* name) {
+  if (!c->profile || !e0) return;
+  cudaEvent_t e1;
+  cudaEventCreate(&e1);
+  cudaEventRecord(e1, c->stream);
+  c->prof_events.push_back({kind_of(name), {e0, e1}});
+}
+
+#define LAUNCH(expr, name)                          \
+  do {                                              \
+    cudaEvent_t e0_;                                \
+    prof_begin(c, &e0_);                            \
+    int rc_ = count_launch(c, (expr), name);        \
+    prof_end(c, e0_, name);                         \
+    if (rc_ != GWM_B200_OK) return rc_;             \
+  } while (0)
+
+double inv_count(const Member& M) { return 1.0 / ((double)M.g.nx * (double)M.g.ny); }
+
+// theta level sums of the step state into slot(ring) (dry_core.cu:462-490)
+int enqueue_theta(gwm_b200_ctx* c, Member& M) {
+  CK(cudaMemsetAsync(M.slot(M.ring), 0, kSlot * sizeof(unsigned long long), c->stream));
+  LevelSumArgs a{};
+  a.g = M.g; a.rho = M.Q[0]; a.rt = M.Q[1]; a.mode = 0;
+  a.acc_a = M.slot(M.ring); a.acc_b = M.slot(M.ring) + kMaxNz;
+  a.clr_a = M.slot(M.ring + 1); a.clr_b = M.slot(M.ring + 1) + kMaxNz;
+  LAUNCH(launch_level_sums(a, c->stream), "level sums");
+  M.theta_valid = true;
+  return GWM_B200_OK;
+}
+
+bool rain_feeds_theta(const Member& M) { return M.md.moist && M.md.enable_warm_rain; }
+
+// One advance_dry_state_ssprk3 (dry_core.cu:541-651).
+int enqueue_dry(gwm_b200_ctx* c, Member& M) {
+  const gwm_b200_step_config& sc = M.md.step;
+  const bool fast = sc.enable_fast_modes != 0;
+  const int ns = std::max(1, sc.fast_substeps);
+  const float dt = sc.dt;
+  const float dtf = dt / (float)ns;
+  const bool terr = M.terrain_active;
+  const bool rain_theta = rain_feeds_theta(M);
+  int rcur = 0, dcur = -1;
+  const float wa[3] = {0.0f, 0.75f, 1.0f / 3.0f}, wb[3] = {1.0f, 0.25f, 2.0f / 3.0f};
+  for (int s = 0; s < 3; ++s) {
+    SlowArgs a{};
+    a.g = M.g;
+    if (s == 0) {
+      a.rho = M.Q[0]; a.th = M.Q[1]; a.th_is_rt = 1;
+      a.u = M.Q[2]; a.v = M.Q[3]; a.w = M.Q[4];
+    } else {
+      a.rho = M.R[rcur]; a.th = M.TH[(s - 1) & 1]; a.th_is_rt = 0;
+      a.u = M.B[(s - 1) & 1][0]; a.v = M.B[(s - 1) & 1][1]; a.w = M.B[(s - 1) & 1][2];
+      if (fast && dcur >= 0) { a.du = M.D[dcur][0]; a.dv = M.D[dcur][1]; a.dw = M.D[dcur][2]; }
+      a.rho0 = M.Q[0]; a.rt0 = M.Q[1]; a.u0 = M.Q[2]; a.v0 = M.Q[3]; a.w0 = M.Q[4];
+    }
+    a.wa = wa[s]; a.wb = wb[s];
+    a.dt = dt; a.gravity = sc.gravity;
+    const int rnext = (s == 0) ? 0 : (rcur ^ 1);
+    if (fast || s < 2) {
+      a.o_rho = M.R[rnext]; a.o_th = M.TH[s & 1]; a.out_rt = 0;
+      a.o_u = M.B[s & 1][0]; a.o_v = M.B[s & 1][1]; a.o_w = M.B[s & 1][2];
+    } else {
+      a.o_rho = M.Q[0]; a.o_th = M.Q[1]; a.out_rt = 1;
+      a.o_u = M.Q[2]; a.o_v = M.Q[3]; a.o_w = M.Q[4];
+    }
+    a.th_acc = M.slot(M.ring);
+    a.acc_a = M.slot(M.ring + 1); a.acc_b = M.slot(M.ring + 1) + kMaxNz;
+    a.clr_a = M.slot(M.ring + 2); a.clr_b = M.slot(M.ring + 2) + kMaxNz;
+    a.acc_mode = fast ? (terr ? 0 : 1) : ((s == 2 && rain_theta) ? 0 : 2);
+    a.inv_count = inv_count(M);
+    a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf;
+    LAUNCH(launch_slow(a, terr, c->stream), "slow stage");
+    M.ring = (M.ring + 1) % 3;
+    rcur = rnext;
+    if (!fast) continue;
+    dcur = -1;
+    for (int n = 0; n < ns; ++n) {
+      FastArgs f{};
+      f.g = M.g;
+      f.rho_in = M.R[rcur]; f.rho_out = M.R[rcur ^ 1];
+      f.th = M.TH[s & 1];
+      const int dout = (n == 0) ? 0 : (dcur ^ 1);
+      if (n > 0) { f.du_in = M.D[dcur][0]; f.dv_in = M.D[dcur][1]; f.dw_in = M.D[dcur][2]; }
+      f.du_out = M.D[dout][0]; f.dv_out = M.D[dout][1]; f.dw_out = M.D[dout][2];
+      f.final_kind = (n == ns - 1) ? (s == 2 ? 2 : 1) : 0;
+      f.acc_off = (f.final_kind == 2 && rain_theta) ? 1 : 0;
+      f.bu = M.B[s & 1][0]; f.bv = M.B[s & 1][1]; f.bw = M.B[s & 1][2];
+      f.f_rho = M.Q[0]; f.f_rt = M.Q[1]; f.f_u = M.Q[2]; f.f_v = M.Q[3]; f.f_w = M.Q[4];
+      f.dtf = dtf; f.gravity = sc.gravity;
+      f.hmom = sc.fast_update_horizontal_momentum; f.dens = sc.fast_update_density;
+      f.ref_a = M.slot(M.ring); f.ref_b = M.slot(M.ring) + kMaxNz;
+      f.inv_count = inv_count(M);
+      f.acc_a = M.slot(M.ring + 1); f.acc_b = M.slot(M.ring + 1) + kMaxNz;
+      f.clr_a = M.slot(M.ring + 2); f.clr_b = M.slot(M.ring + 2) + kMaxNz;
+      f.zc = M.zc; f.idz_c = M.idc; f.idz_f = M.idf;
+      LAUNCH(launch_fast(f, n == 0, terr, c->stream), "fast substep");
+      M.ring = (M.ring + 1) % 3;
+      rcur ^= 1;
+      dcur = dout;
+    }
+  }
+  return GWM_B200_OK;
+}
+
+// advance_passive_tracers_ssprk3 (dry_transport.cu:440-518), three tracers per pass.
+int enqueue_tracers(gwm_b200_ctx* c, Member& M) {
+  float* const* ins[3] = {M.T0, M.T1, M.T2};
+  float* const* outs[3] = {M.T1, M.T2, M.T0};
+  const float wa[3] = {0.0f, 0.75f, 1.0f / 3.0f}, wb[3] = {1.0f, 0.25f, 2.0f / 3.0f};
+  for (int s = 0; s < 3; ++s) {
+    TracerArgs a{};
+    a.g = M.g;
+    a.rho = M.Q[0]; a.u = M.Q[2]; a.v = M.Q[3]; a.w = M.Q[4];
+    for (int t = 0; t < 3; ++t) {
+      a.q_in[t] = ins[s][t];
+      a.q0[t] = s == 0 ? nullptr : M.T0[t];
+      a.q_out[t] = outs[s][t];
+    }
+    a.wa = wa[s]; a.wb = wb[s]; a.dt = M.md.step.dt;
+    a.ntracers = 3;
+    a.idz_c = M.idc; a.terrain = M.terrain_active;
+    LAUNCH(launch_tracer_stage(a, c->stream), "tracer stage");
+  }
+  return GWM_B200_OK;
+}
+
+// apply_warm_rain_microphysics (warm_rain.cu:214-353)
+int enqueue_rain(gwm_b200_ctx* c, Member& M, int fallout) {
+  const gwm_b200_warm_rain_config& r = M.md.rain;
+  RainArgs a{};
+  a.g = M.g;
+  a.rho = M.Q[0]; a.rt = M.Q[1];
+  a.qv = M.T0[0]; a.qc = M.T0[1]; a.qr = M.T0[2];
+  a.precip = M.precip; a.precip_comp = M.pcomp;
+  a.dt = r.dt; a.relax = r.condensation_relaxation; a.thr = r.cloud_autoconversion_threshold;
+  a.rate = r.cloud_autoconversion_rate; a.evap = r.rain_evaporation_rate;
+  a.vt = r.rain_terminal_velocity; a.layer_depth = r.sedimentation_layer_depth_m;
+  a.latent = r.enable_latent_heating;
+  int mode = 0;
+  if (fallout == 1 && r.rain_terminal_velocity > 0.0f) mode = 1;
+  if (fallout == 2 && r.rain_terminal_velocity > 0.0f && r.sedimentation_layer_depth_m > 0.0f) mode = 2;
+  a.fallout_mode = mode;
+  a.idz_c = M.idc; a.terrain = M.terrain_active;
+  a.th_acc = M.slot(M.ring);
+  a.inv_count = inv_count(M);
+  LAUNCH(launch_warm_rain(a, c->stream), "warm rain");
+  return GWM_B200_OK;
+}
+
+int enqueue_full_step(gwm_b200_ctx* c, Member& M) {
+  int rc = enqueue_dry(c, M);
+  if (rc) return rc;
+  if (M.md.moist && M.md.enable_tracer_transport) {
+    rc = enqueue_tracers(c, M);
+    if (rc) return rc;
+  }
+  if (M.md.moist && M.md.enable_warm_rain) {
+    // the rain kernel accumulates the theta sums the next step's first stage reads
+    rc = enqueue_rain(c, M, 1);
+    if (rc) return rc;
+  }
+  return GWM_B200_OK;
+}
+
+int check_member(gwm_b200_ctx* c, int member) {
+  if (!c) return GWM_B200_ERR_ARG;
+  if (member < 0 || member >= (int)c->m.size()) return fail(c, GWM_B200_ERR_ARG, "member index out of range");
+  return GWM_B200_OK;
+}
+
+void drop_graph(gwm_b200_ctx* c) {
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int gwm_b200_create(const gwm_b200_grid_desc* grids, const gwm_b200_member_desc* members,
+                    int n_members, gwm_b200_ctx** out) {
+  if (!out || !grids || !members || n_members <= 0) return GWM_B200_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GWM_B200_ERR_NO_DEVICE;
+  auto* c = new gwm_b200_ctx();
+  cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete c; return GWM_B200_ERR_CUDA; }
+  c->stream = c->own_stream;
+  c->m.resize(n_members);
+  for (int i = 0; i < n_members; ++i) {
+    Member& M = c->m[i];
+    M.gd = grids[i];
+    M.md = members[i];
+    const gwm_b200_grid_desc& d = M.gd;
+    std::string why;
+    if (d.nx <= 0 || d.ny <= 0 || d.nz <= 0) why = "grid dimensions must be positive";
+    else if (d.halo != 1) why = "halo must be 1 (every stencil of the step reaches one cell)";
+    else if (d.nz > kMaxNz) why = "nz exceeds the supported maximum (256)";
+    else if (!(d.dx > 0 && d.dy > 0 && d.z_top > 0)) why = "dx, dy and z_top must be positive";
+    else if ((double)(((kXOff + d.nx + 2 + 31) / 32) * 32) * (d.ny + 3) * (d.nz + 1) >= 2147483647.0)
+      why = "grid too large for 32-bit field indexing";
+    else if (M.md.step.fast_substeps < 1 && M.md.step.enable_fast_modes) why = "fast_substeps must be >= 1";
+    if (!why.empty()) {
+      gwm_b200_destroy(c);
+      static thread_local std::string last;
+      last = why;
+      return GWM_B200_ERR_ARG;
+    }
+    if (d.terrain) {
+      M.terrain.assign(d.terrain, d.terrain + (size_t)d.nx * d.ny);
+      for (float h : M.terrain)  // terrain_active: dry_fast_modes.cu:484-492
+        if (std::abs((double)h) > 1.0e-6) { M.terrain_active = true; break; }
+    }
+    if (d.eta_interfaces) M.eta.assign(d.eta_interfaces, d.eta_interfaces + d.nz + 1);
+    M.gd.terrain = nullptr;
+    M.gd.eta_interfaces = nullptr;
+    int rc = alloc_member(c, M);
+    if (rc != GWM_B200_OK) {
+      std::fprintf(stderr, "gwm_b200_create: %s\n", c->err.c_str());
+      gwm_b200_destroy(c);
+      return rc;
+    }
+  }
+  *out = c;
+  return GWM_B200_OK;
+}
+
+void gwm_b200_destroy(gwm_b200_ctx* c) {
+  if (!c) return;
+  drop_graph(c);
+  for (auto& M : c->m)
+    if (M.block) cudaFree(M.block);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+}
+
+const char* gwm_b200_last_error(const gwm_b200_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int gwm_b200_set_stream(gwm_b200_ctx* c, void* stream) {
+  if (!c) return GWM_B200_ERR_ARG;
+  drop_graph(c);
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return GWM_B200_OK;
+}
+
+int gwm_b200_synchronize(gwm_b200_ctx* c) {
+  if (!c) return GWM_B200_ERR_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+int gwm_b200_use_graph(gwm_b200_ctx* c, int enable) {
+  if (!c) return GWM_B200_ERR_ARG;
+  c->use_graph = enable != 0;
+  if (!c->use_graph) drop_graph(c);
+  return GWM_B200_OK;
+}
+
+long long gwm_b200_launch_count(const gwm_b200_ctx* c) { return c ? c->launches : -1; }
+
+int gwm_b200_upload(gwm_b200_ctx* c, int member, const gwm_b200_fields* h) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  if (!h) return fail(c, GWM_B200_ERR_ARG, "null field set");
+  Member& M = c->m[member];
+  const Geom& g = M.g;
+  struct F { const float* src; float* dst; int o; };
+  std::vector<F> list = {{h->rho_d, M.Q[0], kCell}, {h->rho_theta_m, M.Q[1], kCell},
+                         {h->mom_u, M.Q[2], kFaceX}, {h->mom_v, M.Q[3], kFaceY},
+                         {h->mom_w, M.Q[4], kFaceZ}};
+  if (M.md.moist) {
+    list.push_back({h->qv, M.T0[0], kCell});
+    list.push_back({h->qc, M.T0[1], kCell});
+    list.push_back({h->qr, M.T0[2], kCell});
+  } else if (h->qv || h->qc || h->qr || h->precip) {
+    return fail(c, GWM_B200_ERR_ARG, "tracer fields given to a dry member");
+  }
+  for (const auto& f : list) {
+    if (!f.src) continue;
+    const size_t n = (size_t)(g.nx + (f.o == kFaceX)) * (g.ny + (f.o == kFaceY)) * (g.nz + (f.o == kFaceZ));
+    CK(cudaMemcpyAsync(M.staging, f.src, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    CK(launch_pack(g, f.o, M.staging, f.dst, c->stream));
+  }
+  if (M.md.moist && h->precip) {
+    const size_t n = (size_t)g.nx * g.ny;
+    CK(cudaMemcpyAsync(M.precip, h->precip, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(M.pcomp, 0, n * sizeof(double), c->stream));
+  }
+  if (h->rho_d || h->rho_theta_m) M.theta_valid = false;
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+int gwm_b200_download(gwm_b200_ctx* c, int member, gwm_b200_fields* h) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  if (!h) return fail(c, GWM_B200_ERR_ARG, "null field set");
+  Member& M = c->m[member];
+  const Geom& g = M.g;
+  struct F { float* dst; const float* src; int o; };
+  std::vector<F> list = {{h->rho_d, M.Q[0], kCell}, {h->rho_theta_m, M.Q[1], kCell},
+                         {h->mom_u, M.Q[2], kFaceX}, {h->mom_v, M.Q[3], kFaceY},
+                         {h->mom_w, M.Q[4], kFaceZ}};
+  if (M.md.moist) {
+    list.push_back({h->qv, M.T0[0], kCell});
+    list.push_back({h->qc, M.T0[1], kCell});
+    list.push_back({h->qr, M.T0[2], kCell});
+  }
+  for (const auto& f : list) {
+    if (!f.dst) continue;
+    const size_t n = (size_t)(g.nx + (f.o == kFaceX)) * (g.ny + (f.o == kFaceY)) * (g.nz + (f.o == kFaceZ));
+    CK(launch_unpack(g, f.o, f.src, M.staging, c->stream));
+    CK(cudaMemcpyAsync(f.dst, M.staging, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (M.md.moist && h->precip) {
+    const size_t n = (size_t)g.nx * g.ny;
+    std::vector<double> comp(n);
+    CK(cudaMemcpyAsync(h->precip, M.precip, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(comp.data(), M.pcomp, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (size_t q = 0; q < n; ++q) h->precip[q] += comp[q];
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+static int run_steps(gwm_b200_ctx* c, int nsteps, int (*one)(gwm_b200_ctx*, Member&)) {
+  c->cur_launches = 0;
+  for (auto& M : c->m)
+    if (!M.theta_valid) {
+      int rc = enqueue_theta(c, M);
+      if (rc) return rc;
+    }
+  if (c->use_graph && !c->profile && nsteps > 0 && one == enqueue_full_step) {
+    if (!c->graph) {
+      const long long before = c->cur_launches;
+      std::vector<int> rings;
+      for (auto& M : c->m) rings.push_back(M.ring);
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = GWM_B200_OK;
+      for (auto& M : c->m) {
+        rc = one(c, M);
+        if (rc) break;
+      }
+      cudaGraph_t graph = nullptr;
+      cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+      if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+      if (e != cudaSuccess) return fail(c, GWM_B200_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&c->graph, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return fail(c, GWM_B200_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+      c->graph_launches = c->cur_launches - before;
+      // a step advances every ring by a multiple of three: restore the positions
+      for (size_t i = 0; i < c->m.size(); ++i) c->m[i].ring = rings[i];
+      c->cur_launches = before;
+    }
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->graph, c->stream));
+    c->cur_launches += c->graph_launches * nsteps;
+  } else {
+    for (int s = 0; s < nsteps; ++s)
+      for (auto& M : c->m) {
+        int rc = one(c, M);
+        if (rc) return rc;
+      }
+  }
+  c->launches = c->cur_launches;
+  if (c->stream == c->own_stream || c->profile) CK(cudaStreamSynchronize(c->stream));
+  if (c->profile) {
+    for (auto& pe : c->prof_events) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, pe.second.first, pe.second.second);
+      c->prof_ms[pe.first] += ms;
+      c->prof_n[pe.first] += 1;
+      cudaEventDestroy(pe.second.first);
+      cudaEventDestroy(pe.second.second);
+    }
+    c->prof_events.clear();
+  }
+  return GWM_B200_OK;
+}
+
+int gwm_b200_profile(gwm_b200_ctx* c, int enable) {
+  if (!c) return GWM_B200_ERR_ARG;
+  c->profile = enable != 0;
+  if (c->profile) drop_graph(c);
+  for (int k = 0; k < kKinds; ++k) { c->prof_ms[k] = 0; c->prof_n[k] = 0; }
+  return GWM_B200_OK;
+}
+
+int gwm_b200_profile_read(const gwm_b200_ctx* c, int kind, double* total_ms, long long* launches,
+                          const char** name) {
+  if (!c || kind < 0 || kind >= kKinds) return GWM_B200_ERR_ARG;
+  if (total_ms) *total_ms = c->prof_ms[kind];
+  if (launches) *launches = c->prof_n[kind];
+  if (name) *name = kKindNames[kind];
+  return kKinds;
+}
+
+int gwm_b200_step(gwm_b200_ctx* c, int nsteps) {
+  if (!c || nsteps < 0) return GWM_B200_ERR_ARG;
+  return run_steps(c, nsteps, enqueue_full_step);
+}
+
+int gwm_b200_advance_dry(gwm_b200_ctx* c, int nsteps) {
+  if (!c || nsteps < 0) return GWM_B200_ERR_ARG;
+  // a dry-only call must leave theta sums of the dry result: treat rain as absent
+  std::vector<int> saved;
+  for (auto& M : c->m) { saved.push_back(M.md.enable_warm_rain); M.md.enable_warm_rain = 0; }
+  const int rc = run_steps(c, nsteps, enqueue_dry);
+  for (size_t i = 0; i < c->m.size(); ++i) c->m[i].md.enable_warm_rain = saved[i];
+  return rc;
+}
+
+int gwm_b200_advance_tracers(gwm_b200_ctx* c) {
+  if (!c) return GWM_B200_ERR_ARG;
+  c->cur_launches = 0;
+  for (auto& M : c->m) {
+    if (!M.md.moist) continue;
+    int rc = enqueue_tracers(c, M);
+    if (rc) return rc;
+  }
+  c->launches = c->cur_launches;
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+int gwm_b200_warm_rain(gwm_b200_ctx* c, int fallout) {
+  if (!c || fallout < 0 || fallout > 2) return GWM_B200_ERR_ARG;
+  c->cur_launches = 0;
+  for (auto& M : c->m) {
+    if (!M.md.moist) continue;
+    // fresh theta sums of the post-microphysics state
+    CK(cudaMemsetAsync(M.slot(M.ring), 0, kSlot * sizeof(unsigned long long), c->stream));
+    int rc = enqueue_rain(c, M, fallout);
+    if (rc) return rc;
+    M.theta_valid = true;
+  }
+  c->launches = c->cur_launches;
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+int gwm_b200_fast_modes(gwm_b200_ctx* c) {
+  if (!c) return GWM_B200_ERR_ARG;
+  c->cur_launches = 0;
+  for (auto& M : c->m) {
+    const gwm_b200_step_config& sc = M.md.step;
+    const int ns = std::max(1, sc.fast_substeps);
+    const bool terr = M.terrain_active;
+    // theta frozen from the state, base momenta = the state's momenta,
+    // density copied so the first substep never reads what it writes
+    LAUNCH(launch_theta_field(M.g, M.Q[0], M.Q[1], M.TH[0], c->stream), "theta field");
+    CK(cudaMemcpyAsync(M.R[0], M.Q[0], M.field_elems * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+    // rho and p level sums of the state (flat-terrain reference) into slot(ring)
+    CK(cudaMemsetAsync(M.slot(M.ring), 0, kSlot * sizeof(unsigned long long), c->stream));
+    LevelSumArgs ls{};
+    ls.g = M.g; ls.rho = M.Q[0]; ls.rt = M.Q[1]; ls.mode = 1;
+    ls.acc_a = M.slot(M.ring); ls.acc_b = M.slot(M.ring) + kMaxNz;
+    ls.clr_a = M.slot(M.ring + 1); ls.clr_b = M.slot(M.ring + 1) + kMaxNz;
+    LAUNCH(launch_level_sums(ls, c->stream), "level sums");
+    int rcur = 0, dcur = -1;
+    for (int n = 0; n < ns; ++n) {
+      FastArgs f{};
+      f.g = M.g;
+      f.rho_in = M.R[rcur]; f.rho_out = M.R[rcur ^ 1];
+      f.th = M.TH[0];
+      const int dout = (n == 0) ? 0 : (dcur ^ 1);
+      if (n > 0) { f.du_in = M.D[dcur][0]; f.dv_in = M.D[dcur][1]; f.dw_in = M.D[dcur][2]; }
+      f.du_out = M.D[dout][0]; f.dv_out = M.D[dout][1]; f.dw_out = M.D[dout][2];
+      f.final_kind = (n == ns - 1) ? 2 : 0;
+      f.bu = M.Q[2]; f.bv = M.Q[3]; f.bw = M.Q[4];
+      f.f_rho = M.Q[0]; f.f_rt = M.Q[1]; f.f_u = M.Q[2]; f.f_v = M.Q[3]; f.f_w = M.Q[4];
+      f.dtf = sc.dt / (float)ns; f.gravity = sc.gravity;
+      f.hmom = sc.fast_update_horizontal_momentum; f.dens = sc.fast_update_density;
+      f.ref_a = M.slot(M.ring); f.ref_b = M.slot(M.ring) + kMaxNz;
+      f.inv_count = inv_count(M);
+      f.acc_a = M.slot(M.ring + 1); f.acc_b = M.slot(M.ring + 1) + kMaxNz;
+      f.clr_a = M.slot(M.ring + 2); f.clr_b = M.slot(M.ring + 2) + kMaxNz;
+      f.zc = M.zc; f.idz_c = M.idc; f.idz_f = M.idf;
+      LAUNCH(launch_fast(f, n == 0, terr, c->stream), "fast substep");
+      M.ring = (M.ring + 1) % 3;
+      rcur ^= 1;
+      dcur = dout;
+    }
+    M.theta_valid = true;  // the final substep left theta sums of the result in slot(ring)
+  }
+  c->launches = c->cur_launches;
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+int gwm_b200_slow_tendencies(gwm_b200_ctx* c, int member, gwm_b200_fields* h) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  if (!M.theta_valid) {
+    rc = enqueue_theta(c, M);
+    if (rc) return rc;
+  }
+  SlowArgs a{};
+  a.g = M.g;
+  a.rho = M.Q[0]; a.th = M.Q[1]; a.th_is_rt = 1;
+  a.u = M.Q[2]; a.v = M.Q[3]; a.w = M.Q[4];
+  a.dt = M.md.step.dt; a.gravity = M.md.step.gravity;
+  a.o_rho = M.R[0]; a.o_th = M.TH[0]; a.o_u = M.B[0][0]; a.o_v = M.B[0][1]; a.o_w = M.B[0][2];
+  a.tend_only = 1;
+  a.th_acc = M.slot(M.ring);
+  a.acc_mode = 0;
+  a.inv_count = inv_count(M);
+  a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf;
+  CK(launch_slow(a, M.terrain_active, c->stream));
+  gwm_b200_fields tmp{};
+  tmp.rho_d = h->rho_d; tmp.rho_theta_m = h->rho_theta_m;
+  tmp.mom_u = h->mom_u; tmp.mom_v = h->mom_v; tmp.mom_w = h->mom_w;
+  const Geom& g = M.g;
+  struct F { float* dst; const float* src; int o; };
+  const F list[5] = {{tmp.rho_d, M.R[0], kCell}, {tmp.rho_theta_m, M.TH[0], kCell},
+                     {tmp.mom_u, M.B[0][0], kFaceX}, {tmp.mom_v, M.B[0][1], kFaceY},
+                     {tmp.mom_w, M.B[0][2], kFaceZ}};
+  for (const auto& f : list) {
+    if (!f.dst) continue;
+    const size_t n = (size_t)(g.nx + (f.o == kFaceX)) * (g.ny + (f.o == kFaceY)) * (g.nz + (f.o == kFaceZ));
+    CK(launch_unpack(g, f.o, f.src, M.staging, c->stream));
+    CK(cudaMemcpyAsync(f.dst, M.staging, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+int gwm_b200_budgets(gwm_b200_ctx* c, int member, gwm_b200_budget* out) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  if (!out) return fail(c, GWM_B200_ERR_ARG, "null budget");
+  Member& M = c->m[member];
+  const Geom& g = M.g;
+  cudaStream_t s = c->stream;
+  CK(launch_reduce(g, kCell, 0, M.Q[0], nullptr, nullptr, 0, M.red_part, M.red_out + 0, s));
+  CK(launch_reduce(g, kCell, 0, M.Q[1], nullptr, nullptr, 0, M.red_part, M.red_out + 1, s));
+  CK(launch_reduce(g, kFaceX, 0, M.Q[2], nullptr, nullptr, 0, M.red_part, M.red_out + 2, s));
+  CK(launch_reduce(g, kFaceY, 0, M.Q[3], nullptr, nullptr, 0, M.red_part, M.red_out + 3, s));
+  CK(launch_reduce(g, kFaceZ, 0, M.Q[4], nullptr, nullptr, 0, M.red_part, M.red_out + 4, s));
+  CK(launch_reduce(g, kCell, 1, M.Q[1], M.Q[0], nullptr, 0, M.red_part, M.red_out + 5, s));
+  int nout = 6;
+  if (M.md.moist) {
+    for (int t = 0; t < 3; ++t)
+      CK(launch_reduce(g, kCell, 2, M.T0[t], nullptr, M.idc, M.terrain_active, M.red_part, M.red_out + 6 + t, s));
+    CK(launch_reduce_2d(M.precip, M.pcomp, (long long)g.nx * g.ny, M.red_part, M.red_out + 9, s));
+    nout = 10;
+  }
+  ReduceOut r[10];
+  CK(cudaMemcpyAsync(r, M.red_out, nout * sizeof(ReduceOut), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  gwm_b200_budget& b = *out;
+  std::memset(&b, 0, sizeof(b));
+  b.total_dry_mass = r[0].sum; b.rho_min = r[0].mn; b.rho_max = r[0].mx;
+  b.total_rho_theta_m = r[1].sum;
+  b.total_horizontal_momentum_x = r[2].sum; b.u_min = r[2].mn; b.u_max = r[2].mx;
+  b.total_horizontal_momentum_y = r[3].sum; b.v_min = r[3].mn; b.v_max = r[3].mx;
+  b.total_vertical_momentum = r[4].sum; b.w_min = r[4].mn; b.w_max = r[4].mx;
+  b.theta_min = r[5].mn; b.theta_max = r[5].mx;
+  if (M.md.moist) {
+    b.vapor_water_path_sum_kg_m2 = r[6].sum;
+    b.cloud_water_path_sum_kg_m2 = r[7].sum;
+    b.rain_water_path_sum_kg_m2 = r[8].sum;
+    b.accumulated_surface_precipitation_sum_mm = r[9].sum;
+    b.mean_surface_precipitation_mm = r[9].sum / ((double)g.nx * g.ny);
+    b.max_surface_precipitation_mm = r[9].mx;
+  }
+  if (!std::isfinite(b.total_dry_mass) || !std::isfinite(b.total_rho_theta_m) || !(b.rho_min > 0.0))
+    return fail(c, GWM_B200_ERR_STATE, "non-finite or non-positive density in the state");
+  return GWM_B200_OK;
+}
+
+// ---------------------------------------------------------------------------
+static int layout_rows(const gwm_b200_layout_desc* d, std::vector<int>& rows) {
+  if (!d || d->global_nx <= 0 || d->global_ny <= 0 || d->nz <= 0 || d->ranks_x <= 0 ||
+      d->ranks_y <= 0 || d->halo < 0)
+    return GWM_B200_ERR_ARG;
+  const int rx = d->ranks_x, ry = d->ranks_y;
+  const int bnx = d->global_nx / rx, rnx = d->global_nx % rx;
+  const int bny = d->global_ny / ry, rny = d->global_ny % ry;
+  rows.assign((size_t)12 * rx * ry, 0);
+  int jb = 0, r = 0;
+  for (int y = 0; y < ry; ++y) {  // virtual_rank_layout.cpp:7-47
+    const int nyl = bny + (y < rny ? 1 : 0);
+    int ib = 0;
+    for (int x = 0; x < rx; ++x, ++r) {
+      const int nxl = bnx + (x < rnx ? 1 : 0);
+      int* o = &rows[(size_t)12 * r];
+      o[0] = r; o[1] = x; o[2] = y; o[3] = ib; o[4] = ib + nxl; o[5] = jb; o[6] = jb + nyl; o[11] = d->nz;
+      ib += nxl;
+    }
+    jb += nyl;
+  }
+  auto rank_at = [&](int cx, int cy) {  // cartesian_topology.cpp:29-53
+    if (d->periodic_x) cx = ((cx % rx) + rx) % rx; else if (cx < 0 || cx >= rx) return -1;
+    if (d->periodic_y) cy = ((cy % ry) + ry) % ry; else if (cy < 0 || cy >= ry) return -1;
+    return cy * rx + cx;
+  };
+  for (int q = 0; q < rx * ry; ++q) {
+    int* o = &rows[(size_t)12 * q];
+    o[7] = rank_at(o[1] - 1, o[2]); o[8] = rank_at(o[1] + 1, o[2]);
+    o[9] = rank_at(o[1], o[2] - 1); o[10] = rank_at(o[1], o[2] + 1);
+  }
+  return GWM_B200_OK;
+}
+
+int gwm_b200_layout(const gwm_b200_layout_desc* d, int* out, int capacity) {
+  std::vector<int> rows;
+  int rc = layout_rows(d, rows);
+  if (rc) return rc;
+  const int n = (int)(rows.size() / 12);
+  if (out) {
+    if (capacity < n) return GWM_B200_ERR_ARG;
+    std::memcpy(out, rows.data(), rows.size() * sizeof(int));
+  }
+  return n;
+}
+
+int gwm_b200_halo_exchange(const gwm_b200_layout_desc* d, int orientation, int op,
+                           float* const* rank_fields, void* stream) {
+  std::vector<int> rows;
+  int rc = layout_rows(d, rows);
+  if (rc) return rc;
+  const int n = (int)(rows.size() / 12);
+  if (n > kMaxRanks || orientation < 0 || orientation > 3 || op < 0 || op > 1 || !rank_fields)
+    return GWM_B200_ERR_ARG;
+  if (op == 1 && orientation == 0) return GWM_B200_ERR_ARG;
+  RankTable t{};
+  t.n = n; t.nz = d->nz; t.halo = d->halo; t.orient = orientation;
+  for (int r = 0; r < n; ++r) {
+    const int* o = &rows[(size_t)12 * r];
+    t.r[r].nxl = o[4] - o[3]; t.r[r].nyl = o[6] - o[5];
+    t.r[r].west = o[7]; t.r[r].east = o[8]; t.r[r].south = o[9]; t.r[r].north = o[10];
+    t.r[r].data = rank_fields[r];
+    if (!t.r[r].data) return GWM_B200_ERR_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  if (launch_rank_halo(t, op, s) != cudaSuccess) return GWM_B200_ERR_CUDA;
+  if (!stream && cudaStreamSynchronize(s) != cudaSuccess) return GWM_B200_ERR_CUDA;
+  return GWM_B200_OK;
+}
+
+int gwm_b200_dry_pressure(const float* rho, const float* rt, float* p, long long n, void* stream) {
+  if (!rho || !rt || !p || n < 0) return GWM_B200_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (launch_pressure(rho, rt, p, n, s) != cudaSuccess) return GWM_B200_ERR_CUDA;
+  if (!stream && cudaStreamSynchronize(s) != cudaSuccess) return GWM_B200_ERR_CUDA;
+  return GWM_B200_OK;
+}
+
+static void rank_shape(const int* row, int nz, int halo, int o, int& ox, int& oy, int& oz, int& px,
+                       int& py) {
+  ox = row[4] - row[3] + (o == 1);
+  oy = row[6] - row[5] + (o == 2);
+  oz = nz + (o == 3);
+  px = ox + 2 * halo;
+  py = oy + 2 * halo;
+}
+
+int gwm_b200_ranks_to_global(const gwm_b200_layout_desc* d, int o, const float* const* rf, float* glob) {
+  std::vector<int> rows;
+  int rc = layout_rows(d, rows);
+  if (rc) return rc;
+  if (o < 0 || o > 3 || !rf || !glob) return GWM_B200_ERR_ARG;
+  const int gx = d->global_nx + (o == 1), gy = d->global_ny + (o == 2), gz = d->nz + (o == 3);
+  const size_t n = (size_t)gx * gy * gz;
+  std::vector<float> sum(n, 0.0f);
+  std::vector<unsigned char> cnt(n, 0);
+  std::vector<float> first(n, 0.0f);
+  for (size_t r = 0; r < rows.size() / 12; ++r) {
+    const int* row = &rows[12 * r];
+    int ox, oy, oz, px, py;
+    rank_shape(row, d->nz, d->halo, o, ox, oy, oz, px, py);
+    for (int k = 0; k < oz; ++k)
+      for (int j = 0; j < oy; ++j)
+        for (int i = 0; i < ox; ++i) {
+          const float v = rf[r][((size_t)k * py + (j + d->halo)) * px + (i + d->halo)];
+          const size_t q = ((size_t)k * gy + (row[5] + j)) * gx + (row[3] + i);
+          if (cnt[q] == 0) first[q] = v; else sum[q] = v;
+          cnt[q]++;
+        }
+  }
+  for (size_t q = 0; q < n; ++q) glob[q] = cnt[q] >= 2 ? 0.5f * (first[q] + sum[q]) : first[q];
+  return GWM_B200_OK;
+}
+
+int gwm_b200_global_to_ranks(const gwm_b200_layout_desc* d, int o, const float* glob, float* const* rf) {
+  std::vector<int> rows;
+  int rc = layout_rows(d, rows);
+  if (rc) return rc;
+  if (o < 0 || o > 3 || !rf || !glob) return GWM_B200_ERR_ARG;
+  const int gx = d->global_nx + (o == 1), gy = d->global_ny + (o == 2);
+  for (size_t r = 0; r < rows.size() / 12; ++r) {
+    const int* row = &rows[12 * r];
+    int ox, oy, oz, px, py;
+    rank_shape(row, d->nz, d->halo, o, ox, oy, oz, px, py);
+    for (int k = 0; k < oz; ++k)
+      for (int j = 0; j < oy; ++j)
+        for (int i = 0; i < ox; ++i)
+          rf[r][((size_t)k * py + (j + d->halo)) * px + (i + d->halo)] =
+              glob[((size_t)k * gy + (row[5] + j)) * gx + (row[3] + i)];
+  }
+  return GWM_B200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,610 @@
+// dycore.cu — sm_100a kernels of the dry dynamics: one fused slow RK stage and
+// one fused acoustic substep.
+//
+// Both kernels use the same tiling.  A CTA of BX x BY threads owns an
+// (BX-2) x (BY-2) block of columns plus a one-column ring of halo columns; each
+// thread owns one column and marches k = 0..nz-1 keeping k-1, k, k+1 values
+// in registers, while the current plane is shared through shared memory for
+// the horizontal neighbours.  Halo threads load and derive the same per-column
+// quantities (pressure, cell velocities, dp/dz) so interior threads never wait
+// on another CTA.  Every owned output is written once, by its owner; values
+// that the reference's halo exchange would copy into halo slots are written
+// there by the same store (store_mirrored), so no separate halo pass runs.
+#include "dycore.cuh"
+
+namespace gwmb {
+namespace {
+
+constexpr int BX = 32;
+constexpr int BY = 8;
+constexpr int NT = BX * BY;
+constexpr int NW = NT / 32;
+
+__device__ __forceinline__ float met3(const float* m, const Geom& g, int i, int j, int k) {
+  return __ldg(m + gidx(g, i, j, k));
+}
+
+// Column values of one plane for the slow stage.
+struct SlowCol {
+  float rho, rt, th, p, uf, vf, wf;
+};
+
+__device__ __forceinline__ SlowCol slow_load(const SlowArgs& a, bool valid, int base, int kk) {
+  SlowCol c{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (!valid) return c;
+  const int o = base + kk * a.g.plane;
+  if (kk < a.g.nz) {
+    c.rho = __ldg(a.rho + o);
+    const float t = __ldg(a.th + o);
+    c.rt = a.th_is_rt ? t : c.rho * t;
+    c.th = theta_of(c.rho, c.rt);
+    c.p = eos_pressure(c.rho, c.rt);
+    c.uf = __ldg(a.u + o);
+    c.vf = __ldg(a.v + o);
+    if (a.du) { c.uf += __ldg(a.du + o); c.vf += __ldg(a.dv + o); }
+  }
+  if (kk <= a.g.nz) {
+    c.wf = __ldg(a.w + o);
+    if (a.dw) c.wf += __ldg(a.dw + o);
+  }
+  return c;
+}
+
+// One-sided / centred dp/dz of a column: dry_pressure_gradient.cu:37-73.
+__device__ __forceinline__ float column_dpdz(int k, int nz, float pm, float pc, float pn, float zm,
+                                             float zcc, float zn) {
+  if (nz == 1) return 0.0f;
+  if (k == 0) return (pn - pc) / fmaxf(zn - zcc, 1.0e-6f);
+  if (k + 1 == nz) return (pc - pm) / fmaxf(zcc - zm, 1.0e-6f);
+  return (pn - pm) / fmaxf(zn - zm, 1.0e-6f);
+}
+
+template <bool TERRAIN>
+__global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
+  const Geom& g = a.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
+  const int gi = blockIdx.x * (BX - 2) - 1 + tx;
+  const int gj = blockIdx.y * (BY - 2) - 1 + ty;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const bool valid = gi >= -1 && gi <= nx + 1 && gj >= -1 && gj <= ny + 1;
+  const bool inner = tx >= 1 && tx <= BX - 2 && ty >= 1 && ty <= BY - 2;
+  const bool own_c = inner && gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+  const bool own_u = inner && gi >= 0 && gi <= nx && gj >= 0 && gj < ny;
+  const bool own_v = inner && gi >= 0 && gi < nx && gj >= 0 && gj <= ny;
+  const bool open_x = !g.per_x, open_y = !g.per_y;
+  const int base = valid ? gidx(g, gi, gj, 0) : 0;
+  const float dx = g.dx, dy = g.dy;
+
+  __shared__ float s_th[2][BY][BX], s_p[2][BY][BX], s_u[2][BY][BX], s_v[2][BY][BX], s_w[2][BY][BX];
+  __shared__ float s_uc[2][BY][BX], s_vc[2][BY][BX], s_wc[2][BY][BX];
+  __shared__ float s_zc[TERRAIN ? 2 : 1][BY][BX], s_dz[TERRAIN ? 2 : 1][BY][BX];
+  __shared__ float s_thref[kMaxNz];
+  __shared__ double s_red[2][NW][2];
+
+  if (blockIdx.x == 0 && blockIdx.y == 0 && a.clr_a) {
+    for (int q = tid; q < nz; q += NT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
+  }
+  for (int q = tid; q < nz; q += NT)
+    s_thref[q] = (float)(acc_read(a.th_acc + q, kScaleTheta) * a.inv_count);
+
+  SlowCol cm{}, cc = slow_load(a, valid, base, 0), cn = slow_load(a, valid, base, 1);
+  float zm = 0.f, zcc = 0.f, zn = 0.f;
+  if (TERRAIN && valid) {
+    zcc = met3(a.zc, g, gi, gj, 0);
+    zn = nz > 1 ? met3(a.zc, g, gi, gj, 1) : 0.f;
+  }
+  const bool blend = a.rho0 != nullptr;
+
+  for (int k = 0; k < nz; ++k) {
+    const int pb = k & 1;
+    s_th[pb][ty][tx] = cc.th;
+    s_p[pb][ty][tx] = cc.p;
+    s_u[pb][ty][tx] = cc.uf;
+    s_v[pb][ty][tx] = cc.vf;
+    s_w[pb][ty][tx] = cc.wf;
+    if (TERRAIN) {
+      s_zc[pb][ty][tx] = zcc;
+      s_dz[pb][ty][tx] = column_dpdz(k, nz, cm.p, cc.p, cn.p, zm, zcc, zn);
+    }
+    __syncthreads();
+    // level sums of the previous plane (one thread, fixed order)
+    if (a.acc_mode && k > 0 && tid == 0) {
+      double sa = 0.0, sb = 0.0;
+      for (int w = 0; w < NW; ++w) { sa += s_red[pb ^ 1][w][0]; sb += s_red[pb ^ 1][w][1]; }
+      if (a.acc_mode == 1) { acc_add(a.acc_a + k - 1, sa, kScaleRho); acc_add(a.acc_b + k - 1, sb, kScaleP); }
+      else acc_add(a.acc_a + k - 1, sa, kScaleTheta);
+    }
+    // cell-centred velocities of plane k, halo included: dry_momentum_flux.cu:36-73
+    {
+      const float rr = fmaxf(cc.rho, 1.0e-6f);
+      s_uc[pb][ty][tx] = (tx + 1 < BX) ? 0.5f * (cc.uf + s_u[pb][ty][tx + 1]) / rr : 0.0f;
+      s_vc[pb][ty][tx] = (ty + 1 < BY) ? 0.5f * (cc.vf + s_v[pb][ty + 1][tx]) / rr : 0.0f;
+      s_wc[pb][ty][tx] = 0.5f * (cc.wf + cn.wf) / rr;
+    }
+    __syncthreads();
+
+    double red_a = 0.0, red_b = 0.0;
+    if (inner && valid) {
+      const int o = base + k * g.plane;
+      // ---- cell: K2 compute_cell_tendencies_kernel (dry_core.cu:62-144)
+      if (own_c) {
+        const float fw = cc.uf, fe = s_u[pb][ty][tx + 1], fs = cc.vf, fn = s_v[pb][ty + 1][tx];
+        const float fb = cc.wf, ft = cn.wf;
+        const float idz = TERRAIN ? met3(a.idz_c, g, gi, gj, k) : __ldg(a.idz_c + k);
+        const float div = (fe - fw) / dx + (fn - fs) / dy + (ft - fb) * idz;
+        const float t_rho = -div;
+        const float tc = cc.th;
+        const float tw = s_th[pb][ty][tx - 1], te = s_th[pb][ty][tx + 1];
+        const float ts = s_th[pb][ty - 1][tx], tn = s_th[pb][ty + 1][tx];
+        const float tb = (k > 0) ? cm.th : tc;
+        const float tt = (k + 1 < nz) ? cn.th : tc;
+        const float gw = fw * (fw >= 0.0f ? tw : tc);
+        const float ge = fe * (fe >= 0.0f ? tc : te);
+        const float gs = fs * (fs >= 0.0f ? ts : tc);
+        const float gn = fn * (fn >= 0.0f ? tc : tn);
+        const float gb = fb * (fb >= 0.0f ? tb : tc);
+        const float gt = ft * (ft >= 0.0f ? tc : tt);
+        const float t_rt = -((ge - gw) / dx + (gn - gs) / dy + (gt - gb) * idz);
+        if (a.tend_only) {
+          a.o_rho[o] = t_rho;
+          a.o_th[o] = t_rt;
+        } else {
+          // K4 update (floor 1e-6) and K5 blend
+          float r1 = fmaxf(1.0e-6f, cc.rho + a.dt * t_rho);
+          float q1 = fmaxf(1.0e-6f, cc.rt + a.dt * t_rt);
+          if (blend) {
+            r1 = a.wa * __ldg(a.rho0 + o) + a.wb * r1;
+            q1 = a.wa * __ldg(a.rt0 + o) + a.wb * q1;
+          }
+          const float th1 = q1 / fmaxf(r1, 1.0e-6f);
+          store_mirrored(a.o_rho, g, kCell, gi, gj, k, r1);
+          store_mirrored(a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1);
+          if (a.acc_mode == 1) {
+            red_a = r1;
+            red_b = eos_pressure(r1, r1 * th1);
+          } else if (a.acc_mode == 2) {
+            red_a = th1;
+          }
+        }
+      }
+      // ---- X face: K17 (dry_momentum_flux.cu:79-156) + K21 (dry_pressure_gradient.cu:75-123)
+      if (own_u) {
+        float t_u = 0.0f;
+        if (!((gi == 0 && open_x) || (gi == nx && open_x))) {
+          const float qw = s_u[pb][ty][tx - 1], qc = cc.uf, qe = s_u[pb][ty][tx + 1];
+          const float qs = s_u[pb][ty - 1][tx], qn = s_u[pb][ty + 1][tx];
+          const float qb = (k > 0) ? cm.uf : qc;
+          const float qt = (k + 1 < nz) ? cn.uf : qc;
+          const float flw = upwind(s_uc[pb][ty][tx - 1], qw, qc);
+          const float fle = upwind(s_uc[pb][ty][tx], qc, qe);
+          float fls = 0.0f, fln = 0.0f, flb = 0.0f, flt = 0.0f;
+          if (!(gj == 0 && open_y)) fls = upwind(0.5f * (s_vc[pb][ty - 1][tx - 1] + s_vc[pb][ty - 1][tx]), qs, qc);
+          if (!(gj + 1 == ny && open_y)) fln = upwind(0.5f * (s_vc[pb][ty][tx - 1] + s_vc[pb][ty][tx]), qc, qn);
+          if (k > 0) flb = upwind(0.5f * (s_wc[pb ^ 1][ty][tx - 1] + s_wc[pb ^ 1][ty][tx]), qb, qc);
+          if (k + 1 < nz) flt = upwind(0.5f * (s_wc[pb][ty][tx - 1] + s_wc[pb][ty][tx]), qc, qt);
+          const float idz = TERRAIN ? 0.5f * (met3(a.idz_c, g, gi - 1, gj, k) + met3(a.idz_c, g, gi, gj, k))
+                                    : __ldg(a.idz_c + k);
+          t_u = -((fle - flw) / dx + (fln - fls) / dy + (flt - flb) * idz);
+          const float pl = s_p[pb][ty][tx - 1], pr = cc.p;
+          if (TERRAIN) {
+            const float dzdx = (s_zc[pb][ty][tx] - s_zc[pb][ty][tx - 1]) / dx;
+            const float dpdz = 0.5f * (s_dz[pb][ty][tx - 1] + s_dz[pb][ty][tx]);
+            t_u += -((pr - pl) / dx - dzdx * dpdz);
+          } else {
+            t_u += -((pr - pl) / dx);
+          }
+        }
+        if (a.tend_only) {
+          a.o_u[o] = t_u;
+        } else {
+          float u1 = fmaxf(-1.0e30f, cc.uf + a.dt * t_u);
+          if (blend) u1 = a.wa * __ldg(a.u0 + o) + a.wb * u1;
+          store_mirrored(a.o_u, g, kFaceX, gi, gj, k, u1);
+        }
+      }
+      // ---- Y face: K18 (dry_momentum_flux.cu:158-235) + K22 (dry_pressure_gradient.cu:125-173)
+      if (own_v) {
+        float t_v = 0.0f;
+        if (!((gj == 0 && open_y) || (gj == ny && open_y))) {
+          const float qw = s_v[pb][ty][tx - 1], qc = cc.vf, qe = s_v[pb][ty][tx + 1];
+          const float qs = s_v[pb][ty - 1][tx], qn = s_v[pb][ty + 1][tx];
+          const float qb = (k > 0) ? cm.vf : qc;
+          const float qt = (k + 1 < nz) ? cn.vf : qc;
+          float flw = 0.0f, fle = 0.0f, flb = 0.0f, flt = 0.0f;
+          if (!(gi == 0 && open_x)) flw = upwind(0.5f * (s_uc[pb][ty - 1][tx - 1] + s_uc[pb][ty][tx - 1]), qw, qc);
+          if (!(gi + 1 == nx && open_x)) fle = upwind(0.5f * (s_uc[pb][ty - 1][tx] + s_uc[pb][ty][tx]), qc, qe);
+          const float fls = upwind(s_vc[pb][ty - 1][tx], qs, qc);
+          const float fln = upwind(s_vc[pb][ty][tx], qc, qn);
+          if (k > 0) flb = upwind(0.5f * (s_wc[pb ^ 1][ty - 1][tx] + s_wc[pb ^ 1][ty][tx]), qb, qc);
+          if (k + 1 < nz) flt = upwind(0.5f * (s_wc[pb][ty - 1][tx] + s_wc[pb][ty][tx]), qc, qt);
+          const float idz = TERRAIN ? 0.5f * (met3(a.idz_c, g, gi, gj - 1, k) + met3(a.idz_c, g, gi, gj, k))
+                                    : __ldg(a.idz_c + k);
+          t_v = -((fle - flw) / dx + (fln - fls) / dy + (flt - flb) * idz);
+          const float ps = s_p[pb][ty - 1][tx], pn = cc.p;
+          if (TERRAIN) {
+            const float dzdy = (s_zc[pb][ty][tx] - s_zc[pb][ty - 1][tx]) / dy;
+            const float dpdz = 0.5f * (s_dz[pb][ty - 1][tx] + s_dz[pb][ty][tx]);
+            t_v += -((pn - ps) / dy - dzdy * dpdz);
+          } else {
+            t_v += -((pn - ps) / dy);
+          }
+        }
+        if (a.tend_only) {
+          a.o_v[o] = t_v;
+        } else {
+          float v1 = fmaxf(-1.0e30f, cc.vf + a.dt * t_v);
+          if (blend) v1 = a.wa * __ldg(a.v0 + o) + a.wb * v1;
+          store_mirrored(a.o_v, g, kFaceY, gi, gj, k, v1);
+        }
+      }
+      // ---- Z face k: K19 (dry_momentum_flux.cu:237-312) + K3 buoyancy (dry_core.cu:146-187)
+      if (own_c) {
+        float t_w = 0.0f;
+        if (k > 0) {
+          const float qw = s_w[pb][ty][tx - 1], qc = cc.wf, qe = s_w[pb][ty][tx + 1];
+          const float qs = s_w[pb][ty - 1][tx], qn = s_w[pb][ty + 1][tx];
+          const float qb = cm.wf, qt = cn.wf;
+          float flw = 0.0f, fle = 0.0f, fls = 0.0f, fln = 0.0f;
+          if (!(gi == 0 && open_x)) flw = upwind(0.5f * (s_uc[pb ^ 1][ty][tx - 1] + s_uc[pb][ty][tx - 1]), qw, qc);
+          if (!(gi + 1 == nx && open_x)) fle = upwind(0.5f * (s_uc[pb ^ 1][ty][tx] + s_uc[pb][ty][tx]), qc, qe);
+          if (!(gj == 0 && open_y)) fls = upwind(0.5f * (s_vc[pb ^ 1][ty - 1][tx] + s_vc[pb][ty - 1][tx]), qs, qc);
+          if (!(gj + 1 == ny && open_y)) fln = upwind(0.5f * (s_vc[pb ^ 1][ty][tx] + s_vc[pb][ty][tx]), qc, qn);
+          const float flb = upwind(s_wc[pb ^ 1][ty][tx], qb, qc);
+          const float flt = upwind(s_wc[pb][ty][tx], qc, qt);
+          const float idz = TERRAIN ? met3(a.idz_f, g, gi, gj, k) : __ldg(a.idz_f + k);
+          t_w = -((fle - flw) / dx + (fln - fls) / dy + (flt - flb) * idz);
+          const float tl = cm.th, tu = cc.th;
+          const float tf = 0.5f * (tl + tu);
+          const float trf = 0.5f * (s_thref[k - 1] + s_thref[k]);
+          const float rf = 0.5f * (cm.rho + cc.rho);
+          const float b = a.gravity * (tf - trf) / fmaxf(trf, 1.0e-6f);
+          t_w += rf * b;
+        }
+        if (a.tend_only) {
+          a.o_w[o] = t_w;
+          if (k + 1 == nz) a.o_w[o + g.plane] = 0.0f;
+        } else {
+          float w1 = fmaxf(-1.0e30f, cc.wf + a.dt * t_w);
+          if (blend) w1 = a.wa * __ldg(a.w0 + o) + a.wb * w1;
+          store_mirrored(a.o_w, g, kFaceZ, gi, gj, k, w1);
+          if (k + 1 == nz) {  // top face: zero tendency
+            float wt = fmaxf(-1.0e30f, cn.wf);
+            if (blend) wt = a.wa * __ldg(a.w0 + o + g.plane) + a.wb * wt;
+            store_mirrored(a.o_w, g, kFaceZ, gi, gj, k + 1, wt);
+          }
+        }
+      }
+    }
+    if (a.acc_mode) {
+      red_a = warp_sum(red_a);
+      red_b = warp_sum(red_b);
+      if ((tid & 31) == 0) { s_red[pb][tid >> 5][0] = red_a; s_red[pb][tid >> 5][1] = red_b; }
+    }
+    // advance the column window
+    cm = cc;
+    cc = cn;
+    cn = slow_load(a, valid, base, k + 2);
+    if (TERRAIN && valid) {
+      zm = zcc;
+      zcc = zn;
+      zn = (k + 2 < nz) ? met3(a.zc, g, gi, gj, k + 2) : 0.f;
+    }
+  }
+  if (a.acc_mode) {
+    __syncthreads();
+    if (tid == 0) {
+      const int pb = (nz - 1) & 1;
+      double sa = 0.0, sb = 0.0;
+      for (int w = 0; w < NW; ++w) { sa += s_red[pb][w][0]; sb += s_red[pb][w][1]; }
+      if (a.acc_mode == 1) { acc_add(a.acc_a + nz - 1, sa, kScaleRho); acc_add(a.acc_b + nz - 1, sb, kScaleP); }
+      else acc_add(a.acc_a + nz - 1, sa, kScaleTheta);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Acoustic substep.
+struct FastCol {
+  float rho, th, thp, p;   // thp: theta recovered from (rho, rho*theta) as the reference does
+  float pref, rref;        // column hydrostatic reference (terrain)
+};
+
+template <bool TERRAIN>
+__device__ __forceinline__ FastCol fast_load(const FastArgs& a, bool valid, int base, int kk,
+                                             const FastCol& below, float dzk) {
+  FastCol c{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (!valid || kk >= a.g.nz) return c;
+  const int o = base + kk * a.g.plane;
+  c.rho = __ldg(a.rho_in + o);
+  c.th = __ldg(a.th + o);
+  const float rt = c.rho * c.th;  // K10 rebuild_rho_theta_from_theta_kernel
+  c.thp = theta_of(c.rho, rt);
+  c.p = eos_pressure(c.rho, rt);  // K20
+  if (TERRAIN) {  // K11 build_column_hydrostatic_reference_kernel (dry_fast_modes.cu:108-158)
+    if (kk == 0) {
+      c.pref = c.p;
+      c.rref = eos_rho(c.pref, c.thp);
+    } else {
+      float pn = fmaxf(1.0f, below.pref - a.gravity * below.rref * dzk);
+      for (int it = 0; it < 4; ++it) {
+        const float rn = eos_rho(pn, c.thp);
+        pn = below.pref - a.gravity * 0.5f * (below.rref + rn) * dzk;
+        pn = fmaxf(pn, 1.0f);
+      }
+      c.pref = pn;
+      c.rref = eos_rho(pn, c.thp);
+    }
+  }
+  return c;
+}
+
+template <bool TERRAIN, bool FIRST>
+__global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
+  const Geom& g = a.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
+  const int gi = blockIdx.x * (BX - 2) - 1 + tx;
+  const int gj = blockIdx.y * (BY - 2) - 1 + ty;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const bool valid = gi >= -1 && gi <= nx + 1 && gj >= -1 && gj <= ny + 1;
+  const bool inner = tx >= 1 && tx <= BX - 2 && ty >= 1 && ty <= BY - 2;
+  const bool own_c = inner && gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+  // faces computed by this thread (owned or the tile's far-edge duplicate)
+  const bool do_u = tx >= 1 && ty >= 1 && ty <= BY - 2 && gi >= 0 && gi <= nx && gj >= 0 && gj < ny;
+  const bool do_v = ty >= 1 && tx >= 1 && tx <= BX - 2 && gi >= 0 && gi < nx && gj >= 0 && gj <= ny;
+  const bool own_u = do_u && tx <= BX - 2;
+  const bool own_v = do_v && ty <= BY - 2;
+  const bool skip_u = (gi == 0 || gi == nx) && !g.per_x;
+  const bool skip_v = (gj == 0 || gj == ny) && !g.per_y;
+  const int base = valid ? gidx(g, gi, gj, 0) : 0;
+  const float dx = g.dx, dy = g.dy, dtf = a.dtf;
+  const bool final_step = a.final_kind == 2;
+
+  __shared__ float s_p[2][BY][BX], s_du[2][BY][BX], s_dv[2][BY][BX];
+  __shared__ float s_zc[TERRAIN ? 2 : 1][BY][BX], s_dz[TERRAIN ? 2 : 1][BY][BX];
+  __shared__ float s_pref[TERRAIN ? 1 : kMaxNz], s_rref[TERRAIN ? 1 : kMaxNz];
+  __shared__ double s_red[2][NW][2];
+
+  if (blockIdx.x == 0 && blockIdx.y == 0 && a.clr_a) {
+    for (int q = tid; q < nz; q += NT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
+  }
+  if (!TERRAIN) {  // K6/K7 level means (deterministic sums instead of float atomics)
+    for (int q = tid; q < nz; q += NT) {
+      s_rref[q] = (float)(acc_read(a.ref_a + q, kScaleRho) * a.inv_count);
+      s_pref[q] = (float)(acc_read(a.ref_b + q, kScaleP) * a.inv_count);
+    }
+    __syncthreads();
+  }
+  const int acc_mode = a.acc_off ? 0 : (a.final_kind == 0 ? (TERRAIN ? 0 : 1) : 2);
+
+  float zm = 0.f, zcc = 0.f, zn = 0.f;
+  if (TERRAIN && valid) {
+    zcc = met3(a.zc, g, gi, gj, 0);
+    zn = nz > 1 ? met3(a.zc, g, gi, gj, 1) : 0.f;
+  }
+  FastCol none{};
+  FastCol cm{}, cc = fast_load<TERRAIN>(a, valid, base, 0, none, 0.f);
+  FastCol cn = fast_load<TERRAIN>(a, valid, base, 1, cc, zn - zcc);
+  float dw_c = 0.0f;  // increment at face k (face 0 never changes)
+
+  for (int k = 0; k < nz; ++k) {
+    const int pb = k & 1;
+    const int o = base + k * g.plane;
+    s_p[pb][ty][tx] = cc.p;
+    if (TERRAIN) {
+      s_zc[pb][ty][tx] = zcc;
+      s_dz[pb][ty][tx] = column_dpdz(k, nz, cm.p, cc.p, cn.p, zm, zcc, zn);
+    }
+    __syncthreads();
+    if (acc_mode && k > 0 && tid == 0) {
+      double sa = 0.0, sb = 0.0;
+      for (int w = 0; w < NW; ++w) { sa += s_red[pb ^ 1][w][0]; sb += s_red[pb ^ 1][w][1]; }
+      if (acc_mode == 1) { acc_add(a.acc_a + k - 1, sa, kScaleRho); acc_add(a.acc_b + k - 1, sb, kScaleP); }
+      else acc_add(a.acc_a + k - 1, sa, kScaleTheta);
+    }
+    // K12: X-face momentum (dry_fast_modes.cu:160-229)
+    float du_new = 0.0f;
+    if (do_u) {
+      const float du_old = FIRST ? 0.0f : __ldg(a.du_in + o);
+      du_new = du_old;
+      if (a.hmom && !skip_u) {
+        const float pl = s_p[pb][ty][tx - 1], pr = cc.p;
+        float x;
+        if (TERRAIN) {
+          const float dzdx = (s_zc[pb][ty][tx] - s_zc[pb][ty][tx - 1]) / dx;
+          const float dpdz = 0.5f * (s_dz[pb][ty][tx - 1] + s_dz[pb][ty][tx]);
+          x = (pr - pl) / dx - dzdx * dpdz;
+        } else {
+          x = (pr - pl) / dx;
+        }
+        du_new = du_old + (-dtf * x);
+      }
+    }
+    s_du[pb][ty][tx] = du_new;
+    // K13: Y-face momentum (dry_fast_modes.cu:231-301)
+    float dv_new = 0.0f;
+    if (do_v) {
+      const float dv_old = FIRST ? 0.0f : __ldg(a.dv_in + o);
+      dv_new = dv_old;
+      if (a.hmom && !skip_v) {
+        const float ps = s_p[pb][ty - 1][tx], pn = cc.p;
+        float x;
+        if (TERRAIN) {
+          const float dzdy = (s_zc[pb][ty][tx] - s_zc[pb][ty - 1][tx]) / dy;
+          const float dpdz = 0.5f * (s_dz[pb][ty - 1][tx] + s_dz[pb][ty][tx]);
+          x = (pn - ps) / dy - dzdy * dpdz;
+        } else {
+          x = (pn - ps) / dy;
+        }
+        dv_new = dv_old + (-dtf * x);
+      }
+    }
+    s_dv[pb][ty][tx] = dv_new;
+    // K14: Z face k+1 (dry_fast_modes.cu:303-348), perturbations about the reference
+    float dw_n = 0.0f;
+    if (own_c && k + 1 <= nz) {
+      const float dw_old = (FIRST || k + 1 == nz) ? 0.0f : __ldg(a.dw_in + o + g.plane);
+      dw_n = dw_old;
+      if (k + 1 < nz) {
+        const float prl = TERRAIN ? cc.pref : s_pref[k], pru = TERRAIN ? cn.pref : s_pref[k + 1];
+        const float rrl = TERRAIN ? cc.rref : s_rref[k], rru = TERRAIN ? cn.rref : s_rref[k + 1];
+        const float ppl = cc.p - prl, ppu = cn.p - pru;
+        const float rpf = 0.5f * ((cc.rho - rrl) + (cn.rho - rru));
+        const float idz = TERRAIN ? met3(a.idz_f, g, gi, gj, k + 1) : __ldg(a.idz_f + k + 1);
+        const float tend = -(ppu - ppl) * idz - a.gravity * rpf;
+        dw_n = dw_old + dtf * tend;
+      }
+    }
+    __syncthreads();
+
+    double red_a = 0.0, red_b = 0.0;
+    if (own_c) {
+      // K15: density from the perturbation mass-flux divergence (dry_fast_modes.cu:350-394)
+      float rho_new = cc.rho;
+      if (a.dens) {
+        const float idz = TERRAIN ? met3(a.idz_c, g, gi, gj, k) : __ldg(a.idz_c + k);
+        const float div = (s_du[pb][ty][tx + 1] - s_du[pb][ty][tx]) / dx +
+                          (s_dv[pb][ty + 1][tx] - s_dv[pb][ty][tx]) / dy + (dw_n - dw_c) * idz;
+        rho_new = fmaxf(1.0e-6f, cc.rho - dtf * div);
+      }
+      const float rt_new = rho_new * cc.th;  // K10 on the state
+      if (final_step) {
+        store_mirrored(a.f_rho, g, kCell, gi, gj, k, rho_new);
+        store_mirrored(a.f_rt, g, kCell, gi, gj, k, rt_new);
+        if (k == 0) store_mirrored(a.f_w, g, kFaceZ, gi, gj, 0, __ldg(a.bw + o));
+        store_mirrored(a.f_w, g, kFaceZ, gi, gj, k + 1, __ldg(a.bw + o + g.plane) + dw_n);
+      } else {
+        store_mirrored(a.rho_out, g, kCell, gi, gj, k, rho_new);
+        if (k + 1 < nz) store_mirrored(a.dw_out, g, kFaceZ, gi, gj, k + 1, dw_n);
+      }
+      if (acc_mode == 1) {
+        red_a = rho_new;
+        red_b = eos_pressure(rho_new, rt_new);
+      } else if (acc_mode == 2) {
+        red_a = theta_of(rho_new, rt_new);
+      }
+    }
+    if (own_u) {
+      if (final_step) store_mirrored(a.f_u, g, kFaceX, gi, gj, k, __ldg(a.bu + o) + du_new);
+      else store_mirrored(a.du_out, g, kFaceX, gi, gj, k, du_new);
+    }
+    if (own_v) {
+      if (final_step) store_mirrored(a.f_v, g, kFaceY, gi, gj, k, __ldg(a.bv + o) + dv_new);
+      else store_mirrored(a.dv_out, g, kFaceY, gi, gj, k, dv_new);
+    }
+    if (acc_mode) {
+      red_a = warp_sum(red_a);
+      red_b = warp_sum(red_b);
+      if ((tid & 31) == 0) { s_red[pb][tid >> 5][0] = red_a; s_red[pb][tid >> 5][1] = red_b; }
+    }
+    dw_c = dw_n;
+    // advance the column window
+    cm = cc;
+    cc = cn;
+    float dzk = 0.f;
+    if (TERRAIN && valid) {
+      zm = zcc;
+      zcc = zn;
+      zn = (k + 2 < nz) ? met3(a.zc, g, gi, gj, k + 2) : 0.f;
+      dzk = zn - zcc;
+    }
+    cn = fast_load<TERRAIN>(a, valid, base, k + 2, cc, dzk);
+  }
+  if (acc_mode) {
+    __syncthreads();
+    if (tid == 0) {
+      const int pb = (nz - 1) & 1;
+      double sa = 0.0, sb = 0.0;
+      for (int w = 0; w < NW; ++w) { sa += s_red[pb][w][0]; sb += s_red[pb][w][1]; }
+      if (acc_mode == 1) { acc_add(a.acc_a + nz - 1, sa, kScaleRho); acc_add(a.acc_b + nz - 1, sb, kScaleP); }
+      else acc_add(a.acc_a + nz - 1, sa, kScaleTheta);
+    }
+  }
+}
+
+// Level sums of a stored (rho, rho*theta) state, one CTA row per level.
+__global__ void __launch_bounds__(256) k_level_sums(const LevelSumArgs a) {
+  const Geom& g = a.g;
+  const int k = blockIdx.y;
+  if (blockIdx.x == 0 && k == 0 && a.clr_a)
+    for (int q = threadIdx.x; q < g.nz; q += blockDim.x) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
+  __shared__ double s[8][2];
+  double va = 0.0, vb = 0.0;
+  const int n = g.nx * g.ny;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int i = q % g.nx, j = q / g.nx;
+    const int o = gidx(g, i, j, k);
+    const float rho = a.rho[o], rt = a.rt[o];
+    if (a.mode == 0) {
+      va += (double)theta_of(rho, rt);
+    } else {
+      const float rtf = rho * theta_of(rho, rt);
+      va += (double)rho;
+      vb += (double)eos_pressure(rho, rtf);
+    }
+  }
+  va = warp_sum(va);
+  vb = warp_sum(vb);
+  if ((threadIdx.x & 31) == 0) { s[threadIdx.x >> 5][0] = va; s[threadIdx.x >> 5][1] = vb; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0.0, tb = 0.0;
+    for (int w = 0; w < 8; ++w) { ta += s[w][0]; tb += s[w][1]; }
+    if (a.mode == 0) acc_add(a.acc_a + k, ta, kScaleTheta);
+    else { acc_add(a.acc_a + k, ta, kScaleRho); acc_add(a.acc_b + k, tb, kScaleP); }
+  }
+}
+
+__global__ void k_theta_field(const Geom g, const float* rho, const float* rt, float* th) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % g.nx);
+    const long long r = q / g.nx;
+    const int j = (int)(r % g.ny), k = (int)(r / g.ny);
+    const int o = gidx(g, i, j, k);
+    store_mirrored(th, g, kCell, i, j, k, theta_of(rho[o], rt[o]));
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_slow(const SlowArgs& a, bool terrain, cudaStream_t s) {
+  if (a.g.nz > kMaxNz) return cudaErrorInvalidValue;
+  const dim3 block(BX, BY);
+  const dim3 grid((a.g.nx + 1 + BX - 3) / (BX - 2), (a.g.ny + 1 + BY - 3) / (BY - 2));
+  if (terrain) k_slow_stage<true><<<grid, block, 0, s>>>(a);
+  else k_slow_stage<false><<<grid, block, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_t s) {
+  if (a.g.nz > kMaxNz) return cudaErrorInvalidValue;
+  const dim3 block(BX, BY);
+  const dim3 grid((a.g.nx + 1 + BX - 3) / (BX - 2), (a.g.ny + 1 + BY - 3) / (BY - 2));
+  if (terrain) {
+    if (first) k_fast_substep<true, true><<<grid, block, 0, s>>>(a);
+    else k_fast_substep<true, false><<<grid, block, 0, s>>>(a);
+  } else {
+    if (first) k_fast_substep<false, true><<<grid, block, 0, s>>>(a);
+    else k_fast_substep<false, false><<<grid, block, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_level_sums(const LevelSumArgs& a, cudaStream_t s) {
+  const int n = a.g.nx * a.g.ny;
+  const int bx = (n + 255) / 256 < 64 ? (n + 255) / 256 : 64;
+  k_level_sums<<<dim3(bx, a.g.nz), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_theta_field(const Geom& g, const float* rho, const float* rt, float* th,
+                               cudaStream_t s) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  long long b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  k_theta_field<<<(int)b, 256, 0, s>>>(g, rho, rt, th);
+  return cudaGetLastError();
+}
+
+}  // namespace gwmb

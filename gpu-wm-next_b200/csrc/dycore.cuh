@@ -1,0 +1,74 @@
+// dycore.cuh — launch interface of the dry-dynamics kernels (slow RK stage and
+// acoustic substep) of the time-step hot path.
+#pragma once
+
+#include "common.cuh"
+
+namespace gwmb {
+
+constexpr int kMaxNz = 256;   // level-mean tables live in shared memory
+
+// Arguments of one fused slow RK stage: tendencies of
+// src/dycore/dry_core.cu:400-539 (K2, K3, K16-K19, K21, K22) plus the stage
+// update (K4, :189-197) and SSPRK3 blend (K5, :199-205), for every owned cell and
+// face, in one pass up the columns.
+struct SlowArgs {
+  Geom g;
+  const float* rho;                 // stage input density
+  const float* th;                  // rho*theta (th_is_rt=1) or theta (0)
+  int th_is_rt;
+  const float *u, *v, *w;           // stage input momenta (base part)
+  const float *du, *dv, *dw;        // acoustic increments added to u,v,w (may be null)
+  const float *rho0, *rt0, *u0, *v0, *w0;  // SSPRK3 blend partner q0 (null: no blend)
+  float wa, wb;                     // out = wa*q0 + wb*max(floor, q + dt*L(q))
+  float dt, gravity;
+  float *o_rho, *o_th, *o_u, *o_v, *o_w;
+  int out_rt;                       // o_th receives rho*theta (1) or theta (0)
+  int tend_only;                    // write raw tendencies L(q), no update/blend/mirror
+  const unsigned long long* th_acc; // theta level sums of the input state
+  unsigned long long *acc_a, *acc_b; // level sums of the output (see acc_mode)
+  unsigned long long *clr_a, *clr_b; // ring slot cleared by block (0,0)
+  int acc_mode;                     // 0 none, 1 rho & p of output, 2 theta of output
+  double inv_count;                 // 1 / (nx*ny)
+  const float *zc, *idz_c, *idz_f;  // metrics: padded 3-D (terrain) or per level (flat)
+};
+
+// Arguments of one acoustic substep: src/dycore/dry_fast_modes.cu:495-652
+// (K9-K15) with momenta carried as increments D = m - m_base.
+struct FastArgs {
+  Geom g;
+  const float* rho_in;
+  float* rho_out;
+  const float* th;                  // theta frozen for the RK stage
+  const float *du_in, *dv_in, *dw_in;   // increments before the substep (null: zero)
+  float *du_out, *dv_out, *dw_out;
+  const float *bu, *bv, *bw;        // stage base momenta (final_kind == 2)
+  float *f_rho, *f_rt, *f_u, *f_v, *f_w;  // step result (final_kind == 2)
+  int final_kind;                   // 0 inner substep, 1 last of a stage, 2 last of the step
+  int acc_off;                      // skip the output level sums
+  float dtf, gravity;
+  int hmom, dens;
+  const unsigned long long *ref_a, *ref_b;  // level sums of rho_in, p(rho_in) (flat terrain)
+  double inv_count;
+  unsigned long long *acc_a, *acc_b, *clr_a, *clr_b;
+  const float *zc, *idz_c, *idz_f;
+};
+
+// Level sums of a stored state.  mode 0: theta = rt/max(rho,1e-6) (the host loop of
+// dry_core.cu:462-476); mode 1: rho and p(rho, rho*theta) (K6 of dry_fast_modes.cu:42-57).
+struct LevelSumArgs {
+  Geom g;
+  const float *rho, *rt;
+  int mode;
+  unsigned long long *acc_a, *acc_b, *clr_a, *clr_b;
+};
+
+cudaError_t launch_slow(const SlowArgs& a, bool terrain, cudaStream_t s);
+cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_t s);
+cudaError_t launch_level_sums(const LevelSumArgs& a, cudaStream_t s);
+// theta = rt/max(rho,1e-6) on owned cells with periodic halo mirroring
+// (compute_theta_field_kernel + exchange_scalar, dry_fast_modes.cu:86-95, 453-462).
+cudaError_t launch_theta_field(const Geom& g, const float* rho, const float* rt, float* th,
+                               cudaStream_t s);
+
+}  // namespace gwmb

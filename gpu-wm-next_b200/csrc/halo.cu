@@ -1,0 +1,320 @@
+// halo.cu — owned<->padded packing, the reference's virtual-rank halo exchange
+// as device kernels, EOS pressure and deterministic FP64 reductions.
+#include <cfloat>
+
+#include "halo.cuh"
+
+namespace gwmb {
+namespace {
+
+__device__ __forceinline__ void owned_shape(const Geom& g, int o, int& fx, int& fy, int& fz) {
+  fx = g.nx + (o == kFaceX);
+  fy = g.ny + (o == kFaceY);
+  fz = g.nz + (o == kFaceZ);
+}
+
+__global__ void k_pack(const Geom g, int o, const float* __restrict__ src, float* __restrict__ dst) {
+  int fx, fy, fz;
+  owned_shape(g, o, fx, fy, fz);
+  const long long n = (long long)fx * fy * fz;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % fx);
+    const long long r = q / fx;
+    const int j = (int)(r % fy);
+    const int k = (int)(r / fy);
+    float v = src[q];
+    if (o == kFaceX && g.per_x && (i == 0 || i == g.nx)) {
+      const long long row = q - i;
+      v = 0.5f * (src[row] + src[row + g.nx]);
+    }
+    if (o == kFaceY && g.per_y && (j == 0 || j == g.ny)) {
+      const long long col = q - (long long)j * fx;
+      v = 0.5f * (src[col] + src[col + (long long)g.ny * fx]);
+    }
+    store_mirrored(dst, g, o, i, j, k, v);
+  }
+}
+
+__global__ void k_unpack(const Geom g, int o, const float* __restrict__ src, float* __restrict__ dst) {
+  int fx, fy, fz;
+  owned_shape(g, o, fx, fy, fz);
+  const long long n = (long long)fx * fy * fz;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % fx);
+    const long long r = q / fx;
+    const int j = (int)(r % fy);
+    const int k = (int)(r / fy);
+    dst[q] = src[gidx(g, i, j, k)];
+  }
+}
+
+// Reference per-rank storage index: field3d.hpp:49-54
+struct RankView {
+  int ox, oy, oz, h;  // owned extents of this orientation, halo
+  float* d;
+  __device__ __forceinline__ float& at(int i, int j, int k) const {
+    return d[((long long)k * (oy + 2 * h) + (j + h)) * (ox + 2 * h) + (i + h)];
+  }
+};
+
+__device__ __forceinline__ RankView view(const RankTable& t, int r) {
+  RankView v;
+  v.ox = t.r[r].nxl + (t.orient == kFaceX);
+  v.oy = t.r[r].nyl + (t.orient == kFaceY);
+  v.oz = t.nz + (t.orient == kFaceZ);
+  v.h = t.halo;
+  v.d = t.r[r].data;
+  return v;
+}
+
+// x phase: pack_face_x_faces_impl / pack_scalar_x_faces + unpack (halo_exchange.cpp:32-73, 313-342)
+__global__ void k_rank_x(const RankTable t) {
+  const int r = blockIdx.y;
+  const RankView me = view(t, r);
+  const int h = t.halo;
+  const long long n = (long long)me.oz * me.oy * h * 2;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int side = (int)(q & 1);
+    long long rr = q >> 1;
+    const int hh = (int)(rr % h);
+    rr /= h;
+    const int j = (int)(rr % me.oy);
+    const int k = (int)(rr / me.oy);
+    if (side == 0) {  // west halo <- west neighbour's east send
+      const int w = t.r[r].west;
+      float v = 0.0f;
+      if (w >= 0) {
+        const RankView nb = view(t, w);
+        const int ei = (t.orient == kFaceX) ? t.r[w].nxl - h + hh : nb.ox - h + hh;
+        v = nb.at(ei, j, k);
+      }
+      me.at(-h + hh, j, k) = v;
+    } else {  // east halo <- east neighbour's west send
+      const int e = t.r[r].east;
+      float v = 0.0f;
+      if (e >= 0) {
+        const RankView nb = view(t, e);
+        const int wi = (t.orient == kFaceX) ? 1 + hh : hh;
+        v = nb.at(wi, j, k);
+      }
+      me.at(me.ox + hh, j, k) = v;
+    }
+  }
+}
+
+// y phase over i in [-h, ox+h): pack_face_y_faces_impl / pack_scalar_y_faces + unpack
+// (halo_exchange.cpp:75-116, 344-373)
+__global__ void k_rank_y(const RankTable t) {
+  const int r = blockIdx.y;
+  const RankView me = view(t, r);
+  const int h = t.halo;
+  const int wx = me.ox + 2 * h;
+  const long long n = (long long)me.oz * h * wx * 2;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int side = (int)(q & 1);
+    long long rr = q >> 1;
+    const int i = (int)(rr % wx) - h;
+    rr /= wx;
+    const int hh = (int)(rr % h);
+    const int k = (int)(rr / h);
+    if (side == 0) {
+      const int s = t.r[r].south;
+      float v = 0.0f;
+      if (s >= 0) {
+        const RankView nb = view(t, s);
+        const int nj = (t.orient == kFaceY) ? t.r[s].nyl - h + hh : nb.oy - h + hh;
+        v = nb.at(i, nj, k);
+      }
+      me.at(i, -h + hh, k) = v;
+    } else {
+      const int nn = t.r[r].north;
+      float v = 0.0f;
+      if (nn >= 0) {
+        const RankView nb = view(t, nn);
+        const int sj = (t.orient == kFaceY) ? 1 + hh : hh;
+        v = nb.at(i, sj, k);
+      }
+      me.at(i, me.oy + hh, k) = v;
+    }
+  }
+}
+
+// synchronize_face_owned_interfaces_impl (halo_exchange.cpp:249-284)
+__global__ void k_rank_sync(const RankTable t) {
+  const int r = blockIdx.y;
+  const RankView me = view(t, r);
+  if (t.orient == kFaceX) {
+    const int e = t.r[r].east;
+    if (!(e >= 0 && (r < e || e == r))) return;
+    const RankView nb = view(t, e);
+    const int nyl = t.r[r].nyl, nxl = t.r[r].nxl;
+    const long long n = (long long)me.oz * nyl;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x) {
+      const int j = (int)(q % nyl), k = (int)(q / nyl);
+      const float avg = 0.5f * (me.at(nxl, j, k) + nb.at(0, j, k));
+      me.at(nxl, j, k) = avg;
+      nb.at(0, j, k) = avg;
+    }
+  } else if (t.orient == kFaceY) {
+    const int nn = t.r[r].north;
+    if (!(nn >= 0 && (r < nn || nn == r))) return;
+    const RankView nb = view(t, nn);
+    const int nyl = t.r[r].nyl, nxl = t.r[r].nxl;
+    const long long n = (long long)me.oz * nxl;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x) {
+      const int i = (int)(q % nxl), k = (int)(q / nxl);
+      const float avg = 0.5f * (me.at(i, nyl, k) + nb.at(i, 0, k));
+      me.at(i, nyl, k) = avg;
+      nb.at(i, 0, k) = avg;
+    }
+  }
+}
+
+__global__ void k_pressure(const float* rho, const float* rt, float* p, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x)
+    p[q] = eos_pressure(rho[q], rt[q]);
+}
+
+__device__ __forceinline__ void block_reduce3(double& s, double& mn, double& mx) {
+  __shared__ double sh[3][32];
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  if (l == 0) { sh[0][w] = s; sh[1][w] = mn; sh[2][w] = mx; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s = 0.0; mn = DBL_MAX; mx = -DBL_MAX;
+    for (int q = 0; q < nw; ++q) { s += sh[0][q]; mn = fmin(mn, sh[1][q]); mx = fmax(mx, sh[2][q]); }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_reduce_pass1(const Geom g, int o, int mode, const float* f,
+                                                      const float* rho, const float* idz,
+                                                      int idz_terrain, double* part) {
+  int fx, fy, fz;
+  owned_shape(g, o, fx, fy, fz);
+  const long long n = (long long)fx * fy * fz;
+  double s = 0.0, mn = DBL_MAX, mx = -DBL_MAX;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % fx);
+    const long long r = q / fx;
+    const int j = (int)(r % fy);
+    const int k = (int)(r / fy);
+    const int a = gidx(g, i, j, k);
+    double v = (double)f[a];
+    if (mode == 1) v = v / fmax((double)rho[a], 1.0e-12);
+    if (mode == 2) v = v * (1.0 / (double)(idz_terrain ? idz[a] : idz[k]));
+    s += v;
+    mn = fmin(mn, v);
+    mx = fmax(mx, v);
+  }
+  block_reduce3(s, mn, mx);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s;
+    part[gridDim.x + blockIdx.x] = mn;
+    part[2 * gridDim.x + blockIdx.x] = mx;
+  }
+}
+
+__global__ void k_reduce_2d_pass1(const double* a, const double* b, long long n, double* part) {
+  double s = 0.0, mn = DBL_MAX, mx = -DBL_MAX;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const double v = a[q] + (b ? b[q] : 0.0);
+    s += v;
+    mn = fmin(mn, v);
+    mx = fmax(mx, v);
+  }
+  block_reduce3(s, mn, mx);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s;
+    part[gridDim.x + blockIdx.x] = mn;
+    part[2 * gridDim.x + blockIdx.x] = mx;
+  }
+}
+
+__global__ void k_reduce_pass2(const double* part, int nb, ReduceOut* out) {
+  double s = 0.0, mn = DBL_MAX, mx = -DBL_MAX;
+  for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+    s += part[q];
+    mn = fmin(mn, part[nb + q]);
+    mx = fmax(mx, part[2 * nb + q]);
+  }
+  block_reduce3(s, mn, mx);
+  if (threadIdx.x == 0) { out->sum = s; out->mn = mn; out->mx = mx; }
+}
+
+inline int blocks_for(long long n, int per) {
+  long long b = (n + per - 1) / per;
+  if (b < 1) b = 1;
+  if (b > 148 * 16) b = 148 * 16;
+  return (int)b;
+}
+
+}  // namespace
+
+cudaError_t launch_pack(const Geom& g, int orient, const float* src, float* dst, cudaStream_t s) {
+  const long long n = (long long)(g.nx + (orient == kFaceX)) * (g.ny + (orient == kFaceY)) *
+                      (g.nz + (orient == kFaceZ));
+  k_pack<<<blocks_for(n, 256), 256, 0, s>>>(g, orient, src, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(const Geom& g, int orient, const float* src, float* dst, cudaStream_t s) {
+  const long long n = (long long)(g.nx + (orient == kFaceX)) * (g.ny + (orient == kFaceY)) *
+                      (g.nz + (orient == kFaceZ));
+  k_unpack<<<blocks_for(n, 256), 256, 0, s>>>(g, orient, src, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rank_halo(const RankTable& t, int op, cudaStream_t s) {
+  if (t.n <= 0 || t.n > kMaxRanks) return cudaErrorInvalidValue;
+  if (op == 0) {
+    if (t.halo <= 0) return cudaSuccess;
+    k_rank_x<<<dim3(64, t.n), 256, 0, s>>>(t);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_rank_y<<<dim3(64, t.n), 256, 0, s>>>(t);
+    return cudaGetLastError();
+  }
+  if (t.orient != kFaceX && t.orient != kFaceY) return cudaSuccess;
+  k_rank_sync<<<dim3(64, t.n), 256, 0, s>>>(t);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pressure(const float* rho, const float* rt, float* p, long long n, cudaStream_t s) {
+  k_pressure<<<blocks_for(n, 256), 256, 0, s>>>(rho, rt, p, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce(const Geom& g, int orient, int mode, const float* f, const float* rho,
+                          const float* idz, int idz_terrain, double* partials, ReduceOut* out,
+                          cudaStream_t s) {
+  k_reduce_pass1<<<kReduceBlocks, 256, 0, s>>>(g, orient, mode, f, rho, idz, idz_terrain, partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_reduce_pass2<<<1, 256, 0, s>>>(partials, kReduceBlocks, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_2d(const double* a, const double* b, long long n, double* partials,
+                             ReduceOut* out, cudaStream_t s) {
+  k_reduce_2d_pass1<<<kReduceBlocks, 256, 0, s>>>(a, b, n, partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_reduce_pass2<<<1, 256, 0, s>>>(partials, kReduceBlocks, out);
+  return cudaGetLastError();
+}
+
+}  // namespace gwmb

@@ -1,0 +1,48 @@
+// halo.cuh — layout kernels: owned<->padded packing, virtual-rank halo exchange
+// on the reference's per-rank Field3D layout, and FP64 budget reductions.
+#pragma once
+
+#include "common.cuh"
+
+namespace gwmb {
+
+constexpr int kMaxRanks = 64;
+
+// Owned global array (fz, fy, fx) -> padded field; aliased periodic faces
+// (X face 0 / nx, Y face 0 / ny) receive their average, which is what the
+// reference's first interface sync makes of them (halo_exchange.cpp:217-285).
+cudaError_t launch_pack(const Geom& g, int orient, const float* src, float* dst, cudaStream_t s);
+cudaError_t launch_unpack(const Geom& g, int orient, const float* src, float* dst, cudaStream_t s);
+
+// Per-rank descriptor in the reference layout: include/gwm/domain/subdomain_descriptor.hpp:7-26
+struct RankDesc {
+  int nxl, nyl;
+  int west, east, south, north;
+  float* data;   // device pointer, Field3D storage of this rank
+};
+struct RankTable {
+  int n, nz, halo, orient;
+  RankDesc r[kMaxRanks];
+};
+// op 0: HaloExchange::exchange_* (halo_exchange.cpp:148-215, 563-620);
+// op 1: synchronize_owned_face_interfaces (:217-285).
+cudaError_t launch_rank_halo(const RankTable& t, int op, cudaStream_t s);
+
+// EOS over n values (K20 compute_pressure_kernel, dry_pressure_gradient.cu:27-35).
+cudaError_t launch_pressure(const float* rho, const float* rt, float* p, long long n, cudaStream_t s);
+
+// Reductions over owned positions.  mode 0: value; 1: theta = rt/max(rho,1e-12)
+// in FP64 (dry_diagnostics.cpp:33-45); 2: column water rho_q*dz with
+// dz = 1/inv_dz_cell in FP64 (runtime_summary.cpp:72-81).
+struct ReduceOut {
+  double sum, mn, mx;
+};
+// partials: scratch of >= 3*kReduceBlocks doubles; out: device ReduceOut.
+constexpr int kReduceBlocks = 296;
+cudaError_t launch_reduce(const Geom& g, int orient, int mode, const float* f, const float* rho,
+                          const float* idz, int idz_terrain, double* partials, ReduceOut* out,
+                          cudaStream_t s);
+cudaError_t launch_reduce_2d(const double* a, const double* b, long long n, double* partials,
+                             ReduceOut* out, cudaStream_t s);
+
+}  // namespace gwmb

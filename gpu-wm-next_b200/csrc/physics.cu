@@ -1,0 +1,231 @@
+// physics.cu — sm_100a kernels for the moist part of the step: the fused
+// three-tracer SSPRK3 stage and the warm-rain column kernel.
+#include "dycore.cuh"
+#include "physics.cuh"
+
+namespace gwmb {
+namespace {
+
+constexpr int BX = 32;
+constexpr int BY = 8;
+constexpr int NT = BX * BY;
+constexpr int NTR = 3;
+
+struct TrCol {
+  float rho, uf, vf, wf;
+  float rq[NTR], q[NTR];
+};
+
+__device__ __forceinline__ TrCol tr_load(const TracerArgs& a, bool valid, int base, int kk) {
+  TrCol c{};
+  if (!valid) return c;
+  const int o = base + kk * a.g.plane;
+  if (kk < a.g.nz) {
+    c.rho = __ldg(a.rho + o);
+    c.uf = __ldg(a.u + o);
+    c.vf = __ldg(a.v + o);
+    const float rr = fmaxf(c.rho, 1.0e-6f);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+      if (t < a.ntracers) {
+        c.rq[t] = __ldg(a.q_in[t] + o);
+        c.q[t] = c.rq[t] / rr;  // mixing ratio: dry_transport.cu:91-94
+      }
+    }
+  }
+  if (kk <= a.g.nz) c.wf = __ldg(a.w + o);
+  return c;
+}
+
+__global__ void __launch_bounds__(NT) k_tracer_stage(const TracerArgs a) {
+  const Geom& g = a.g;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int gi = blockIdx.x * (BX - 2) - 1 + tx;
+  const int gj = blockIdx.y * (BY - 2) - 1 + ty;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const bool valid = gi >= -1 && gi <= nx + 1 && gj >= -1 && gj <= ny + 1;
+  const bool inner = tx >= 1 && tx <= BX - 2 && ty >= 1 && ty <= BY - 2;
+  const bool own_c = inner && gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+  const int base = valid ? gidx(g, gi, gj, 0) : 0;
+  const float dx = g.dx, dy = g.dy;
+  const bool blend = a.q0[0] != nullptr;
+
+  __shared__ float s_q[NTR][2][BY][BX];
+  __shared__ float s_u[2][BY][BX], s_v[2][BY][BX];
+
+  TrCol cm{}, cc = tr_load(a, valid, base, 0), cn = tr_load(a, valid, base, 1);
+  for (int k = 0; k < nz; ++k) {
+    const int pb = k & 1;
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) s_q[t][pb][ty][tx] = cc.q[t];
+    s_u[pb][ty][tx] = cc.uf;
+    s_v[pb][ty][tx] = cc.vf;
+    __syncthreads();
+    if (own_c) {
+      const int o = base + k * g.plane;
+      const float fw = cc.uf, fe = s_u[pb][ty][tx + 1], fs = cc.vf, fn = s_v[pb][ty + 1][tx];
+      const float fb = cc.wf, ft = cn.wf;
+      const float idz = a.terrain ? __ldg(a.idz_c + o) : __ldg(a.idz_c + k);
+#pragma unroll
+      for (int t = 0; t < NTR; ++t) {
+        if (t >= a.ntracers) break;
+        const float qc = cc.q[t];
+        const float qw = s_q[t][pb][ty][tx - 1], qe = s_q[t][pb][ty][tx + 1];
+        const float qs = s_q[t][pb][ty - 1][tx], qn = s_q[t][pb][ty + 1][tx];
+        const float qb = (k > 0) ? cm.q[t] : qc;
+        const float qt = (k + 1 < nz) ? cn.q[t] : qc;
+        const float gw = fw * (fw >= 0.0f ? qw : qc);
+        const float ge = fe * (fe >= 0.0f ? qc : qe);
+        const float gs = fs * (fs >= 0.0f ? qs : qc);
+        const float gn = fn * (fn >= 0.0f ? qc : qn);
+        const float gb = fb * (fb >= 0.0f ? qb : qc);
+        const float gt = ft * (ft >= 0.0f ? qc : qt);
+        const float div = (ge - gw) / dx + (gn - gs) / dy + (gt - gb) * idz;
+        float out = fmaxf(0.0f, cc.rq[t] - a.dt * div);
+        if (blend) out = a.wa * __ldg(a.q0[t] + o) + a.wb * out;
+        store_mirrored(a.q_out[t], g, kCell, gi, gj, k, out);
+      }
+    }
+    cm = cc;
+    cc = cn;
+    cn = tr_load(a, valid, base, k + 2);
+  }
+}
+
+__device__ __forceinline__ float sat_vapor_pressure(float tk) {  // moist_thermo.hpp:23-29
+  const float tc = tk - 273.15f;
+  const float es_hpa = 6.112f * expf((17.67f * tc) / fmaxf(tc + 243.5f, 1.0e-6f));
+  return es_hpa * 100.0f;
+}
+__device__ __forceinline__ float qsat(float tk, float p) {  // moist_thermo.hpp:31-36
+  const float eps = kRd / kRv;
+  const float es = sat_vapor_pressure(tk);
+  const float denom = fmaxf(p - (1.0f - eps) * es, 1000.0f);
+  return fminf(fmaxf(eps * es / denom, 0.0f), 0.05f);
+}
+
+constexpr int RB = 128;  // columns per warm-rain block (one row segment)
+
+__global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
+  const Geom& g = a.g;
+  const int gi = blockIdx.x * RB + threadIdx.x;
+  const int gj = blockIdx.y;
+  const bool active = gi < g.nx && gj < g.ny;
+  __shared__ double s_th[kMaxNz][RB / 32];
+  float incoming = 0.0f;
+  for (int k = g.nz - 1; k >= 0; --k) {
+    double th_sum = 0.0;
+    if (active) {
+      const int o = gidx(g, gi, gj, k);
+      // warm_rain_kernel: warm_rain.cu:36-120
+      const float rho_d = __ldg(a.rho + o);
+      const float rho = fmaxf(rho_d, 1.0e-6f);
+      const float rt = a.rt[o];
+      float th = rt / rho;
+      float p = eos_pressure(rho, rt);
+      float temp;
+      {  // dry_temperature_from_conserved: moist_thermo.hpp:55-62
+        const float thc = theta_of(rho, rt);
+        const float pc = eos_pressure(rho, rt);
+        temp = thc * powf(fmaxf(pc / kP0, 1.0e-6f), kKappa);
+      }
+      const float exner = fmaxf(temp / fmaxf(th, 1.0e-6f), 1.0e-6f);
+      float qv = fmaxf(a.qv[o] / rho, 0.0f);
+      float qc = fmaxf(a.qc[o] / rho, 0.0f);
+      float qr = fmaxf(a.qr[o] / rho, 0.0f);
+      const float lh = kLv / (dry_cp() * fmaxf(exner, 1.0e-6f));
+      float qs = qsat(temp, p);
+      if (qv > qs) {
+        const float cond = fminf((qv - qs) * fmaxf(a.relax, 0.0f), qv);
+        qv -= cond;
+        qc += cond;
+        if (a.latent && cond > 0.0f) th += lh * cond;
+      } else if (qv < qs && qc > 0.0f) {
+        const float ev = fminf((qs - qv) * fmaxf(a.relax, 0.0f), qc);
+        qv += ev;
+        qc -= ev;
+        if (a.latent && ev > 0.0f) th -= lh * ev;
+      }
+      const float excess = fmaxf(qc - a.thr, 0.0f);
+      if (excess > 0.0f && a.rate > 0.0f) {
+        const float conv = fminf(excess, a.dt * a.rate * excess);
+        qc -= conv;
+        qr += conv;
+      }
+      p = eos_pressure(rho, rho * th);
+      temp = th * powf(fmaxf(p / kP0, 1.0e-6f), kKappa);
+      qs = qsat(temp, p);
+      if (qr > 0.0f && qv < qs && a.evap > 0.0f) {
+        const float ev = fminf(qr, a.dt * a.evap * fminf(qs - qv, qr));
+        qr -= ev;
+        qv += ev;
+        if (a.latent && ev > 0.0f) th -= lh * ev;
+      }
+      qv = fmaxf(qv, 0.0f);
+      qc = fmaxf(qc, 0.0f);
+      qr = fmaxf(qr, 0.0f);
+      float rqr = rho * qr;
+      // fallout of this cell, fed by the cell above
+      if (a.fallout_mode == 1) {  // rain_fallout_metric_kernel: warm_rain.cu:156-191
+        const float idz = fmaxf(a.terrain ? __ldg(a.idz_c + o) : __ldg(a.idz_c + k), 1.0e-6f);
+        const float dz = 1.0f / idz;
+        const float frac = fminf(fmaxf(a.vt * a.dt * idz, 0.0f), 1.0f);
+        const float old_a = fmaxf(rqr, 0.0f) * dz;
+        const float out = frac * old_a;
+        rqr = ((old_a - out) + incoming) * idz;
+        incoming = out;
+      } else if (a.fallout_mode == 2) {  // rain_fallout_nominal_kernel: warm_rain.cu:122-154
+        const float dz = fmaxf(a.layer_depth, 1.0e-3f);
+        const float frac = fminf(fmaxf(a.vt * a.dt / dz, 0.0f), 1.0f);
+        if (frac > 0.0f) {
+          const float old_a = fmaxf(rqr, 0.0f) * dz;
+          const float out = frac * old_a;
+          rqr = ((old_a - out) + incoming) / dz;
+          incoming = out;
+        }
+      }
+      const float rt_new = rho * th;
+      store_mirrored(a.qv, g, kCell, gi, gj, k, rho * qv);
+      store_mirrored(a.qc, g, kCell, gi, gj, k, rho * qc);
+      store_mirrored(a.qr, g, kCell, gi, gj, k, rqr);
+      store_mirrored(a.rt, g, kCell, gi, gj, k, rt_new);
+      th_sum = (double)theta_of(rho_d, rt_new);
+    }
+    if (a.th_acc) {
+      th_sum = warp_sum(th_sum);
+      if ((threadIdx.x & 31) == 0) s_th[k][threadIdx.x >> 5] = th_sum;
+    }
+  }
+  if (active && a.fallout_mode && a.precip) {  // compensated FP64 surface accumulation
+    const int q = gj * g.nx + gi;
+    const double s = a.precip[q], x = (double)incoming, t = s + x;
+    a.precip_comp[q] += (fabs(s) >= fabs(x)) ? (s - t) + x : (x - t) + s;
+    a.precip[q] = t;
+  }
+  if (a.th_acc) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < g.nz; k += RB) {
+      double t = 0.0;
+      for (int w = 0; w < RB / 32; ++w) t += s_th[k][w];
+      acc_add(a.th_acc + k, t, kScaleTheta);
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_tracer_stage(const TracerArgs& a, cudaStream_t s) {
+  const dim3 block(BX, BY);
+  const dim3 grid((a.g.nx + BX - 3) / (BX - 2), (a.g.ny + BY - 3) / (BY - 2));
+  k_tracer_stage<<<grid, block, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_warm_rain(const RainArgs& a, cudaStream_t s) {
+  if (a.g.nz > kMaxNz) return cudaErrorInvalidValue;
+  const dim3 grid((a.g.nx + RB - 1) / RB, a.g.ny);
+  k_warm_rain<<<grid, RB, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace gwmb

@@ -1,0 +1,43 @@
+// physics.cuh — launch interface of the moist kernels: passive-tracer SSPRK3
+// stages and warm-rain microphysics with bounded column fallout.
+#pragma once
+
+#include "common.cuh"
+
+namespace gwmb {
+
+// One SSPRK3 stage of the three warm-rain tracers with frozen dry mass fluxes:
+// passive_tracer_stage_kernel (src/dycore/dry_transport.cu:49-125) for all
+// tracers in one pass, fused with the blend (:40-47).
+struct TracerArgs {
+  Geom g;
+  const float* rho;                 // frozen dry density (end of the dry step)
+  const float *u, *v, *w;           // frozen mass fluxes
+  const float* q_in[3];             // stage input rho*q
+  const float* q0[3];               // blend partner (null: stage 1)
+  float* q_out[3];
+  float wa, wb, dt;
+  int ntracers;
+  const float* idz_c;               // per level (flat) or padded 3-D (terrain)
+  int terrain;
+};
+
+// Warm-rain microphysics (warm_rain.cu:36-120) followed, in the same column
+// sweep, by rain fallout (metric :156-191 or nominal :122-154).
+struct RainArgs {
+  Geom g;
+  const float* rho;
+  float *rt, *qv, *qc, *qr;
+  double *precip, *precip_comp;     // FP64 surface accumulation + Neumaier term, (ny, nx); null: none
+  float dt, relax, thr, rate, evap, vt, layer_depth;
+  int latent, fallout_mode;         // fallout_mode: 0 none, 1 metric, 2 nominal
+  const float* idz_c;
+  int terrain;
+  unsigned long long* th_acc;       // theta level sums of the result (null: none)
+  double inv_count;
+};
+
+cudaError_t launch_tracer_stage(const TracerArgs& a, cudaStream_t s);
+cudaError_t launch_warm_rain(const RainArgs& a, cudaStream_t s);
+
+}  // namespace gwmb

@@ -1,0 +1,193 @@
+/* gwm_b200.h — C-ABI of the B200 time-step hot path (libgwm_b200.so).
+ *
+ * Drop-in boundary for the dry SSPRK3 + split-explicit step, passive-tracer
+ * transport, warm-rain microphysics with fallout, C-grid halo fill and the
+ * budget reductions of FahrenheitResearch/gpu-wm-next.  Plain C types only:
+ * host pointers for field I/O, device pointers where stated, and an opaque
+ * context that owns all device buffers of one or more independent members.
+ *
+ * Field I/O layout ("global owned arrays", x fastest, float32):
+ *   cells       (nz,   ny,   nx)      rho_d, rho_theta_m, tracer masses rho*q
+ *   X faces     (nz,   ny,   nx+1)    mom_u
+ *   Y faces     (nz,   ny+1, nx)      mom_v
+ *   Z faces     (nz+1, ny,   nx)      mom_w
+ *   surface     (ny,   nx)            accumulated precipitation, float64
+ * These are the owned parts of the reference's Field3D / FaceField storage
+ * (include/gwm/state/field3d.hpp:49-54, face_field.hpp:16-23) gathered onto
+ * the global grid as VirtualRankLayout::gather_scalar / gather_face do
+ * (src/comm/virtual_rank_layout.cpp:73-137).  gwm_b200_ranks_to_global and
+ * gwm_b200_global_to_ranks convert per-rank halo-padded buffers.
+ *
+ * Every call returns GWM_B200_OK (0) or a negative status; no C++ exception
+ * crosses the boundary (the reference throws std::runtime_error from
+ * gwm::require, include/gwm/core/types.hpp:24-28).  Calls are synchronous
+ * unless a stream was set with gwm_b200_set_stream.
+ */
+#ifndef GWM_B200_H
+#define GWM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GWM_B200_OK 0
+#define GWM_B200_ERR_ARG (-1)          /* invalid argument / unsupported shape */
+#define GWM_B200_ERR_CUDA (-2)         /* CUDA runtime error; see gwm_b200_last_error */
+#define GWM_B200_ERR_STATE (-3)        /* non-finite or non-positive density detected */
+#define GWM_B200_ERR_NO_DEVICE (-4)    /* no CUDA device visible */
+
+typedef struct gwm_b200_ctx gwm_b200_ctx;
+
+/* Grid of one member.  Mirrors RectilinearDomainConfig + GridMetrics::make_hybrid_height
+ * (include/gwm/domain/idealized_domain_builder.hpp:12-31, grid_metrics.hpp:87-92). */
+typedef struct {
+  int nx, ny, nz;              /* global owned cells */
+  int halo;                    /* must be 1 (every reference stencil reaches one cell) */
+  int ranks_x, ranks_y;        /* virtual-rank layout of per-rank host buffers */
+  int periodic_x, periodic_y;  /* else open boundaries: halos read zero */
+  double dx, dy, z_top;
+  double terrain_taper_eta;    /* reference default 0.25 */
+  const float* terrain;        /* (ny, nx) terrain height in m, NULL = flat */
+  const double* eta_interfaces;/* (nz+1) eta levels, NULL = uniform k/nz (extension) */
+} gwm_b200_grid_desc;
+
+/* DryStepperConfig (include/gwm/dycore/dry_core.hpp:50-56) plus the fast-mode switch
+ * of the prepared-case driver (src/core/gwm_prepared_case_driver.cpp:37-41). */
+typedef struct {
+  float dt;
+  int fast_substeps;
+  float gravity;
+  int fast_update_horizontal_momentum;
+  int fast_update_density;
+  int enable_fast_modes;
+} gwm_b200_step_config;
+
+/* WarmRainConfig (include/gwm/physics/warm_rain.hpp:14-23). */
+typedef struct {
+  float dt;
+  float condensation_relaxation;
+  float cloud_autoconversion_threshold;
+  float cloud_autoconversion_rate;
+  float rain_evaporation_rate;
+  float rain_terminal_velocity;
+  float sedimentation_layer_depth_m;
+  int enable_latent_heating;
+} gwm_b200_warm_rain_config;
+
+/* One member: the dry state, and for moist members the warm-rain registry
+ * (specific_humidity, cloud_water_mixing_ratio, rain_water_mixing_ratio;
+ * include/gwm/state/tracer_registry.hpp:18-23,56-62) and surface precipitation. */
+typedef struct {
+  int moist;
+  int enable_tracer_transport;
+  int enable_warm_rain;
+  gwm_b200_step_config step;
+  gwm_b200_warm_rain_config rain;
+} gwm_b200_member_desc;
+
+/* Host field set for upload / download; NULL members are skipped. */
+typedef struct {
+  float* rho_d;
+  float* rho_theta_m;
+  float* mom_u;
+  float* mom_v;
+  float* mom_w;
+  float* qv;     /* rho_d * specific_humidity */
+  float* qc;     /* rho_d * cloud water */
+  float* qr;     /* rho_d * rain water */
+  double* precip;/* accumulated surface precipitation, kg m-2 */
+} gwm_b200_fields;
+
+/* summarize_dry_states (src/dycore/dry_diagnostics.cpp:11-96) and the moisture part
+ * of summarize_runtime_state / summarize_warm_rain (src/core/runtime_summary.cpp:27-178,
+ * src/physics/warm_rain.cpp:355-403), reduced on the device in FP64. */
+typedef struct {
+  double total_dry_mass, total_rho_theta_m;
+  double total_horizontal_momentum_x, total_horizontal_momentum_y, total_vertical_momentum;
+  double rho_min, rho_max, theta_min, theta_max;
+  double u_min, u_max, v_min, v_max, w_min, w_max;
+  double vapor_water_path_sum_kg_m2, cloud_water_path_sum_kg_m2, rain_water_path_sum_kg_m2;
+  double accumulated_surface_precipitation_sum_mm, mean_surface_precipitation_mm,
+      max_surface_precipitation_mm;
+} gwm_b200_budget;
+
+/* ---- context ------------------------------------------------------------ */
+/* Allocates device buffers for n_members independent members (grids[i], members[i]),
+ * builds the hybrid-height metrics (FP64 compute, FP32 store: grid_metrics.hpp:87-239). */
+int gwm_b200_create(const gwm_b200_grid_desc* grids, const gwm_b200_member_desc* members,
+                    int n_members, gwm_b200_ctx** out);
+void gwm_b200_destroy(gwm_b200_ctx* ctx);
+const char* gwm_b200_last_error(const gwm_b200_ctx* ctx);
+/* cudaStream_t passed as void*; NULL restores the context's own stream. */
+int gwm_b200_set_stream(gwm_b200_ctx* ctx, void* stream);
+int gwm_b200_synchronize(gwm_b200_ctx* ctx);
+/* Replay multi-step calls from a captured CUDA graph (1) or launch directly (0). */
+int gwm_b200_use_graph(gwm_b200_ctx* ctx, int enable);
+
+/* ---- state I/O ------------------------------------------------------------ */
+int gwm_b200_upload(gwm_b200_ctx* ctx, int member, const gwm_b200_fields* host);
+int gwm_b200_download(gwm_b200_ctx* ctx, int member, gwm_b200_fields* host);
+
+/* ---- time step -------------------------------------------------------------- */
+/* nsteps of the prepared-case driver loop (gwm_prepared_case_driver.cpp:427-463):
+ * dry SSPRK3 step, then (moist members) tracer transport and warm rain. */
+int gwm_b200_step(gwm_b200_ctx* ctx, int nsteps);
+/* advance_dry_state_ssprk3 with NullBoundaryUpdater and LocalSplitExplicitFastMode
+ * (include/gwm/dycore/dry_core.hpp:106-110, src/dycore/dry_core.cu:541-651). */
+int gwm_b200_advance_dry(gwm_b200_ctx* ctx, int nsteps);
+/* advance_passive_tracers_ssprk3 with NullTracerBoundaryUpdater
+ * (include/gwm/dycore/passive_tracer.hpp:44-49, src/dycore/dry_transport.cu:440-518). */
+int gwm_b200_advance_tracers(gwm_b200_ctx* ctx);
+/* apply_warm_rain_microphysics: fallout 1 = metric overload (warm_rain.hpp:63-68,
+ * warm_rain.cu:273-353), 2 = nominal-depth overload (:57-61, :214-271), 0 = none. */
+int gwm_b200_warm_rain(gwm_b200_ctx* ctx, int fallout);
+/* FastModeIntegrator::apply of LocalSplitExplicitFastMode on the current state
+ * (dry_core.hpp:73-88, dry_core.cu:341-346, dry_fast_modes.cu:400-656). */
+int gwm_b200_fast_modes(gwm_b200_ctx* ctx);
+/* compute_slow_tendencies of the current state (dry_core.hpp:100-104, dry_core.cu:400-539);
+ * the five tendency fields are written to host arrays in the field I/O layout
+ * (rho_theta_m receives the rho*theta tendency). */
+int gwm_b200_slow_tendencies(gwm_b200_ctx* ctx, int member, gwm_b200_fields* host_out);
+/* FP64 budgets of the current state. */
+int gwm_b200_budgets(gwm_b200_ctx* ctx, int member, gwm_b200_budget* out);
+/* Kernel launches issued by the last step call (for accounting). */
+long long gwm_b200_launch_count(const gwm_b200_ctx* ctx);
+/* Per-kernel CUDA-event timing on the context's stream (no graph while enabled).
+ * Enabling resets the accumulators; gwm_b200_profile_read returns the number of
+ * kernel kinds and, for kind, the accumulated device time, launch count and name. */
+int gwm_b200_profile(gwm_b200_ctx* ctx, int enable);
+int gwm_b200_profile_read(const gwm_b200_ctx* ctx, int kind, double* total_ms,
+                          long long* launches, const char** name);
+
+/* ---- halo operators on the reference per-rank layout (device pointers) ---- */
+/* Field orientation: 0 cell, 1 X face, 2 Y face, 3 Z face. */
+typedef struct {
+  int global_nx, global_ny, nz, halo, ranks_x, ranks_y, periodic_x, periodic_y;
+} gwm_b200_layout_desc;
+/* VirtualRankLayout::build + find_cartesian_neighbors (virtual_rank_layout.cpp:7-47,
+ * cartesian_topology.cpp:57-74): 12 ints per rank {rank, coord_x, coord_y, i_begin,
+ * i_end, j_begin, j_end, west, east, south, north, nz}.  Returns the rank count. */
+int gwm_b200_layout(const gwm_b200_layout_desc* d, int* out, int capacity);
+/* op 0: HaloExchange::exchange_scalar / exchange_face (halo_exchange.cpp:563-637);
+ * op 1: synchronize_owned_face_interfaces (:639-654).  rank_fields[r] is rank r's
+ * Field3D storage on the device (halo-padded, reference layout). */
+int gwm_b200_halo_exchange(const gwm_b200_layout_desc* d, int orientation, int op,
+                           float* const* rank_fields, void* stream);
+/* compute_dry_pressure_fields on n device values (dry_pressure_gradient.cu:177-202). */
+int gwm_b200_dry_pressure(const float* rho_d, const float* rho_theta_m, float* pressure,
+                          long long n, void* stream);
+
+/* ---- host layout helpers (no device work) --------------------------------- */
+/* Per-rank halo-padded host buffers <-> global owned arrays.  Faces shared by two
+ * ranks (and periodic aliases) take the average of both copies on the way in, as the
+ * reference's first interface sync does. */
+int gwm_b200_ranks_to_global(const gwm_b200_layout_desc* d, int orientation,
+                             const float* const* rank_fields, float* global);
+int gwm_b200_global_to_ranks(const gwm_b200_layout_desc* d, int orientation,
+                             const float* global, float* const* rank_fields);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GWM_B200_H */

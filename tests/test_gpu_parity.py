@@ -1,0 +1,395 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the CPU oracle.
+
+Integer/index work (halo maps) must match bit-exactly.  Floating-point fields
+are compared with the FP64 oracle of the same discretisation; the tolerance is
+stated per test as a maximum error relative to the field's largest magnitude
+(the dynamic fields carry FP32 rounding, the oracle none).
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("rho", "rho_theta", "u", "v", "w")
+
+
+def rel_err(a, b, floor=1e-12):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), floor))
+
+
+def perturbation_err(a, b, base):
+    """max |a-b| relative to the largest departure of b from a base field."""
+    a, b, base = (np.asarray(x, dtype=np.float64) for x in (a, b, base))
+    return float(np.abs(a - b).max() / max(np.abs(b - base).max(), 1e-12))
+
+
+def to64(d):
+    return {k: np.asarray(v, dtype=np.float64) for k, v in d.items()}
+
+
+def ogrid(orc, g):
+    return orc.GridSpec(g.nx, g.ny, g.nz, dx=g.dx, dy=g.dy, z_top=g.z_top, ranks_x=g.ranks_x,
+                        ranks_y=g.ranks_y, periodic_x=g.periodic_x, periodic_y=g.periodic_y,
+                        terrain=None if g.terrain is None else g.terrain.astype(np.float64),
+                        eta_interfaces=g.eta_interfaces)
+
+
+def ostep(orc, s):
+    return orc.StepSpec(dt=s.dt, fast_substeps=s.fast_substeps, gravity=s.gravity,
+                        fast_hmom=s.fast_update_horizontal_momentum,
+                        fast_density=s.fast_update_density, fast_modes=s.enable_fast_modes)
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch
+
+
+def test_native_library_loaded(gwm, torch_cuda):
+    gwm.lib()
+    maps = open("/proc/self/maps").read()
+    assert "libgwm_b200.so" in maps
+
+
+# ---------------------------------------------------------------------------
+LAYOUTS = [(8, 8, 2, 1, 2, 2, True, True), (13, 7, 3, 1, 3, 2, False, True),
+           (10, 9, 2, 1, 1, 3, True, False), (6, 5, 2, 1, 1, 1, False, False),
+           (9, 9, 2, 2, 2, 2, True, True), (7, 6, 2, 1, 1, 1, True, True)]
+
+
+@pytest.mark.parametrize("lay", LAYOUTS)
+@pytest.mark.parametrize("orient", [0, 1, 2, 3])
+@pytest.mark.parametrize("op", ["exchange", "sync"])
+def test_halo_ops_bit_exact(gwm, orc, torch_cuda, lay, orient, op):
+    if op == "sync" and orient in (0, 3):
+        pytest.skip("interface sync is defined for X and Y faces")
+    torch = torch_cuda
+    nx, ny, nz, h, rx, ry, px, py = lay
+    rows = orc.layout(nx, ny, nz, h, rx, ry, px, py)
+    name = {0: "cell", 1: "x", 2: "y", 3: "z"}[orient]
+    host, dev = [], []
+    rng = np.random.default_rng(orient * 7 + len(rows))
+    for row in rows:
+        shape = orc.rank_field_shape(row, nz, h, name)
+        a = np.full(shape, -999.0)
+        fz, fy, fx = shape
+        i0, j0 = int(row[3]), int(row[5])
+        for k in range(fz):
+            for j in range(fy - 2 * h):
+                for i in range(fx - 2 * h):
+                    a[k, j + h, i + h] = 1000 * k + 100 * (j0 + j) + (i0 + i) + rng.integers(0, 3) * 0.25
+        host.append(a)
+        dev.append(torch.tensor(a.astype(np.float32), device="cuda"))
+    ref = orc.halo([x.copy() for x in host], nx, ny, nz, h, rx, ry, px, py, name, op=op)
+    gwm.halo_exchange([t.data_ptr() for t in dev], nx, ny, nz, h, rx, ry, px, py, orient, op=op)
+    torch.cuda.synchronize()
+    for r, (t, b) in enumerate(zip(dev, ref)):
+        got = t.cpu().numpy().astype(np.float64)
+        assert np.array_equal(got, b), f"rank {r}: {np.argwhere(got != b)[:5]}"
+
+
+def test_dry_pressure_matches_reference_formula(gwm, orc, torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(1)
+    rho = rng.uniform(0.05, 1.3, 100000).astype(np.float32)
+    rt = (rho * rng.uniform(280.0, 500.0, rho.size)).astype(np.float32)
+    r, t = torch.tensor(rho, device="cuda"), torch.tensor(rt, device="cuda")
+    p = torch.empty_like(r)
+    gwm.dry_pressure(r.data_ptr(), t.data_ptr(), p.data_ptr(), rho.size)
+    torch.cuda.synchronize()
+    ref = orc.pressure(rho, rt, precision=64)
+    # FP32 powf against the FP64 formula: a few ulp
+    assert rel_err(p.cpu().numpy(), ref) < 1e-6
+    assert np.max(np.abs(p.cpu().numpy() / ref - 1.0)) < 2e-6
+
+
+# ---------------------------------------------------------------------------
+def bubble_grid(gwm, nx=32, ny=32, nz=40, **kw):
+    return gwm.GridSpec(nx, ny, nz, dx=500.0, dy=500.0, z_top=10000.0, **kw)
+
+
+def c1_state(gwm, g, u=0.0, v=0.0):
+    # +2 K cos^2 bubble (2 km radius, z = 2 km) on a 300 K hydrostatic base
+    p = gwm.CaseParams(rho_surface=np.float32(1e5 / (287.05 * 300.0)), theta_ref=300.0,
+                       theta_perturbation=2.0, center_x_fraction=0.5, center_y_fraction=0.5,
+                       center_z_fraction=0.2, radius_x_fraction=2000.0 / (g.nx * g.dx),
+                       radius_y_fraction=2000.0 / (g.ny * g.dy), radius_z_fraction=0.2,
+                       u_background=u, v_background=v)
+    s = gwm.build_case("hydrostatic_warm_bubble", g, p)
+    if u or v:
+        s["u"] = (np.full_like(s["u"], u) * 1.1).astype(np.float32)
+        s["v"] = (np.full_like(s["v"], v) * 1.1).astype(np.float32)
+    return s
+
+
+@pytest.mark.parametrize("variant", ["flat", "terrain", "open"])
+def test_slow_tendencies_vs_oracle(gwm, orc, variant):
+    kw = {}
+    if variant == "terrain":
+        kw["terrain"] = gwm.build_terrain("cosine_mountain", 24, 20, 500.0, 500.0, height=500.0,
+                                          half_width_x=0.3, half_width_y=0.3)
+    if variant == "open":
+        kw.update(periodic_x=False, periodic_y=False)
+    g = bubble_grid(gwm, 24, 20, 16, **kw)
+    s = c1_state(gwm, g, u=3.0, v=-2.0)
+    rng = np.random.default_rng(5)
+    s["w"] = (rng.standard_normal(s["w"].shape) * 0.2).astype(np.float32)
+    s["w"][0] = 0.0
+    s["w"][-1] = 0.0
+    step = gwm.StepConfig(dt=2.0, fast_substeps=3)
+    with gwm.Model(g, gwm.MemberSpec(step=step)) as m:
+        m.upload(s)
+        t = m.compute_slow_tendencies()
+    ref = orc.slow_tendencies(ogrid(orc, g), ostep(orc, step), to64(s), precision=64)
+    tol = {"rho": 2e-5, "rho_theta": 2e-5, "u": 2e-5, "v": 2e-5, "w": 2e-5}
+    for k in STATE:
+        e = rel_err(t[k], ref[k], floor=1e-9)
+        assert e < tol[k], f"{variant} {k}: {e:.3e}"
+
+
+def test_fast_modes_reference_kats(gwm):
+    # tests/unit/test_dry_fast_modes.cpp:65-192 through the CUDA path
+    g = gwm.GridSpec(20, 20, 8)
+    const = gwm.build_case("constant", g, gwm.CaseParams(rho_background=1.1, theta_background=300.0,
+                                                         u_background=12.0, v_background=-6.0))
+    with gwm.Model(g, gwm.MemberSpec(step=gwm.StepConfig(dt=2.0, fast_substeps=4))) as m:
+        m.upload(const)
+        b0 = m.budgets()
+        m.fast_modes()
+        b1 = m.budgets()
+    assert abs(b1["total_dry_mass"] - b0["total_dry_mass"]) < 1e-4
+    assert abs(b1["u_max"] - b0["u_max"]) < 1e-5 and abs(b1["v_min"] - b0["v_min"]) < 1e-5
+
+    def pulse():
+        s = gwm.build_case("constant", g, gwm.CaseParams(rho_background=1.0, theta_background=300.0))
+        s["rho"][4, 10, 10] += np.float32(0.02)
+        s["rho_theta"][4, 10, 10] = s["rho"][4, 10, 10] * np.float32(300.0)
+        return s
+
+    def run(step, n=1):
+        with gwm.Model(g, gwm.MemberSpec(step=step)) as m:
+            m.upload(pulse())
+            b0 = m.budgets()
+            for _ in range(n):
+                m.fast_modes()
+            return b0, m.budgets(), m.download()
+
+    b0, b1, _ = run(gwm.StepConfig(dt=1.0, fast_substeps=4), 3)
+    assert abs(b1["total_dry_mass"] - b0["total_dry_mass"]) < 1e-3
+    for hmom in (True, False):
+        b0, b1, out = run(gwm.StepConfig(dt=1.0, fast_substeps=1, fast_update_horizontal_momentum=hmom,
+                                         fast_update_density=False))
+        assert abs(b1["total_dry_mass"] - b0["total_dry_mass"]) < 1e-5
+        mag = max(abs(b1["u_min"]), abs(b1["u_max"]))
+        assert (mag > 1e-5) if hmom else (mag < 1e-8)
+        assert abs(b1["rho_max"] - 1.02) < 1e-6 and abs(b1["rho_min"] - 1.0) < 1e-6
+    b0, b1, _ = run(gwm.StepConfig(dt=1.0, fast_substeps=1, fast_update_horizontal_momentum=False,
+                                   fast_update_density=True))
+    assert abs(b1["total_dry_mass"] - b0["total_dry_mass"]) < 1e-5
+    assert abs(b1["rho_max"] - 1.02) > 1e-5
+
+
+@pytest.mark.parametrize("terrain", [False, True])
+def test_fast_modes_vs_oracle(gwm, orc, terrain):
+    kw = {}
+    if terrain:
+        kw["terrain"] = gwm.build_terrain("cosine_mountain", 20, 18, 1000.0, 1000.0, height=800.0,
+                                          half_width_x=0.3, half_width_y=0.3)
+    g = gwm.GridSpec(20, 18, 12, dx=1000.0, dy=1000.0, z_top=12000.0, **kw)
+    s = gwm.build_case("mountain_wave_background", g, gwm.CaseParams(rho_surface=1.18, theta_ref=300.0,
+                                                                     u_background=10.0))
+    s["rho"][5, 9, 10] *= np.float32(1.01)
+    s["rho_theta"][5, 9, 10] = s["rho"][5, 9, 10] * np.float32(300.0)
+    step = gwm.StepConfig(dt=4.0, fast_substeps=4)
+    with gwm.Model(g, gwm.MemberSpec(step=step)) as m:
+        m.upload(s)
+        m.fast_modes()
+        out = m.download()
+    ref = orc.fast_modes(ogrid(orc, g), ostep(orc, step), to64(s), precision=64)
+    base = to64(s)
+    assert rel_err(out["rho"], ref["rho"]) < 1e-6
+    assert rel_err(out["rho_theta"], ref["rho_theta"]) < 1e-6
+    for k in ("u", "v", "w"):
+        e = perturbation_err(out[k], ref[k], base[k])
+        assert e < 1e-4, f"{k}: {e:.3e}"
+
+
+# ---------------------------------------------------------------------------
+def run_both(gwm, orc, g, step, state, nsteps, graph=False):
+    with gwm.Model(g, gwm.MemberSpec(step=step)) as m:
+        m.use_graph(graph)
+        m.upload(state)
+        m.advance_dry_state_ssprk3(nsteps)
+        out = m.download()
+    ref = orc.run(ogrid(orc, g), ostep(orc, step), to64(state), nsteps, precision=64)
+    return out, ref
+
+
+@pytest.mark.parametrize("dt,nsteps", [(2.0, 1), (0.5, 4)])
+def test_c1_warm_bubble_vs_fp64_oracle(gwm, orc, dt, nsteps):
+    # BASELINE config 1 grid and state: 32x32x40, 500 m, dz 250 m, 3 acoustic substeps.
+    # At the configured dt = 2 s the reference discretisation is unstable from the
+    # second step on (c*dt/dz = 2.8 in the slow stage; the FP64 oracle reaches
+    # |w| ~ 1e19 at step 2), so the exact configuration is compared over one step
+    # and the 4-step comparison runs at dt = 0.5 s.
+    g = bubble_grid(gwm)
+    step = gwm.StepConfig(dt=dt, fast_substeps=3)
+    s = c1_state(gwm, g)
+    out, ref = run_both(gwm, orc, g, step, s, nsteps)
+    base = to64(s)
+    errs = {k: rel_err(out[k], ref[k]) for k in STATE}
+    for k in ("u", "v", "w", "rho"):
+        errs[k + "_pert"] = perturbation_err(out[k], ref[k], base[k])
+    # tolerance: 1e-4 relative; FP32 rounding gives ~1e-6
+    assert errs["rho"] < 1e-6 and errs["rho_theta"] < 1e-6, errs
+    for k in ("u_pert", "v_pert", "w_pert", "rho_pert"):
+        assert errs[k] < 1e-4, errs
+
+
+@pytest.mark.parametrize("variant", ["terrain", "open", "ranks"])
+def test_dry_step_variants_vs_oracle(gwm, orc, variant):
+    kw = {}
+    if variant == "terrain":
+        kw["terrain"] = gwm.build_terrain("cosine_mountain", 24, 20, 1000.0, 1000.0, height=600.0,
+                                          half_width_x=0.3, half_width_y=0.3)
+    if variant == "open":
+        kw.update(periodic_x=False, periodic_y=True)
+    if variant == "ranks":
+        kw.update(ranks_x=2, ranks_y=2)
+    g = gwm.GridSpec(24, 20, 16, dx=1000.0, dy=1000.0, z_top=12000.0, **kw)
+    if variant == "terrain":
+        s = gwm.build_case("mountain_wave_background", g, gwm.CaseParams(rho_surface=1.18, theta_ref=300.0,
+                                                                         u_background=10.0))
+    else:
+        s = gwm.build_case("density_current", g, gwm.CaseParams(rho_background=1.0, theta_background=300.0,
+                                                                theta_perturbation=3.0, center_z_fraction=0.35,
+                                                                radius_x_fraction=0.15, radius_y_fraction=0.15,
+                                                                radius_z_fraction=0.2))
+    step = gwm.StepConfig(dt=2.0, fast_substeps=3)
+    out, ref = run_both(gwm, orc, g, step, s, 3)
+    base = to64(s)
+    assert rel_err(out["rho"], ref["rho"]) < 1e-5
+    assert rel_err(out["rho_theta"], ref["rho_theta"]) < 1e-5
+    for k in ("u", "v", "w"):
+        e = perturbation_err(out[k], ref[k], base[k])
+        assert e < 5e-4, f"{variant} {k}: {e:.3e}"
+
+
+def test_fast_modes_off_path(gwm, orc):
+    g = bubble_grid(gwm, 16, 16, 12)
+    step = gwm.StepConfig(dt=1.0, fast_substeps=2, enable_fast_modes=False)
+    s = c1_state(gwm, g)
+    out, ref = run_both(gwm, orc, g, step, s, 2)
+    base = to64(s)
+    for k in ("u", "v", "w"):
+        assert perturbation_err(out[k], ref[k], base[k]) < 1e-4
+
+
+def test_determinism_and_graph_replay(gwm):
+    g = bubble_grid(gwm, 32, 24, 20)
+    step = gwm.StepConfig(dt=2.0, fast_substeps=3)
+    s = c1_state(gwm, g, u=2.0)
+    outs = []
+    for graph in (False, False, True):
+        with gwm.Model(g, gwm.MemberSpec(step=step)) as m:
+            m.use_graph(graph)
+            m.upload(s)
+            m.advance_dry_state_ssprk3(1)
+            m.step(2)
+            outs.append(m.download())
+    for k in STATE:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+        assert np.array_equal(outs[0][k], outs[2][k]), k
+
+
+def test_budgets_match_host_sums(gwm):
+    g = bubble_grid(gwm, 20, 16, 10)
+    s = c1_state(gwm, g, u=1.0)
+    with gwm.Model(g, gwm.MemberSpec(step=gwm.StepConfig(dt=2.0, fast_substeps=2))) as m:
+        m.upload(s)
+        m.advance_dry_state_ssprk3(1)
+        b = m.budgets()
+        out = m.download()
+    d = to64(out)
+    assert b["total_dry_mass"] == pytest.approx(d["rho"].sum(), rel=1e-13)
+    assert b["total_rho_theta_m"] == pytest.approx(d["rho_theta"].sum(), rel=1e-13)
+    assert b["total_horizontal_momentum_x"] == pytest.approx(d["u"].sum(), rel=1e-12, abs=1e-9)
+    assert b["rho_min"] == d["rho"].min() and b["w_max"] == d["w"].max()
+    th = d["rho_theta"] / np.maximum(d["rho"], 1e-12)
+    assert b["theta_max"] == pytest.approx(th.max(), rel=1e-15)
+
+
+# ---------------------------------------------------------------------------
+def moist_setup(gwm, nx=16, ny=12, nz=24, seed=7):
+    g = gwm.GridSpec(nx, ny, nz, dx=3000.0, dy=3000.0, z_top=18000.0)
+    p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=seed, relative_humidity=1.02)
+    s = gwm.build_case("moist_sounding", g, p, moist=True)
+    return g, s
+
+
+def test_moist_step_vs_fp64_oracle(gwm, orc):
+    # supersaturated moist sounding (RH 1.02) so condensation, autoconversion and
+    # fallout all act within a few steps; dt keeps the scheme inside its stable range
+    g, s = moist_setup(gwm)
+    step = gwm.StepConfig(dt=2.0, fast_substeps=4)
+    rain = gwm.WarmRainConfig(dt=2.0, rain_terminal_velocity=12.0)
+    ms = gwm.MemberSpec(step=step, rain=rain, moist=True)
+    with gwm.Model(g, ms) as m:
+        m.upload(s)
+        m.step(3)
+        out = m.download()
+        bud = m.budgets()
+    orain = orc.RainSpec(dt=2.0, terminal_velocity=12.0)
+    ref = orc.run(ogrid(orc, g), ostep(orc, step), to64(s), 3,
+                  phases=orc.PHASE_DRY | orc.PHASE_TRACERS | orc.PHASE_RAIN, rain=orain, precision=64)
+    assert rel_err(out["rho"], ref["rho"]) < 1e-5
+    assert rel_err(out["rho_theta"], ref["rho_theta"]) < 1e-5
+    for k in ("qv", "qc", "qr"):
+        assert rel_err(out[k], ref[k], floor=1e-9) < 1e-3, k
+    assert rel_err(out["precip"], ref["precip"], floor=1e-12) < 1e-3
+    assert ref["qc"].max() > 0 and ref["qr"].max() > 0  # the case rains
+    assert bud["accumulated_surface_precipitation_sum_mm"] == pytest.approx(out["precip"].sum(), rel=1e-12)
+
+
+@pytest.mark.parametrize("fallout", ["nominal", "metric"])
+def test_warm_rain_kats_gpu(gwm, fallout):
+    # tests/unit/test_warm_rain_microphysics.cpp:41-161 through the CUDA path
+    def one(rho, theta, qv, qc, qr, nz=1, z_top=1000.0, rain=None):
+        g = gwm.GridSpec(1, 1, nz, dx=1000.0, dy=1000.0, z_top=z_top)
+        s = gwm.build_case("constant", g, gwm.CaseParams(rho_background=rho, theta_background=theta), moist=True)
+        s["qv"][:] = np.asarray(qv, dtype=np.float32).reshape(nz, 1, 1) * np.float32(rho)
+        s["qc"][:] = np.asarray(qc, dtype=np.float32).reshape(nz, 1, 1) * np.float32(rho)
+        s["qr"][:] = np.asarray(qr, dtype=np.float32).reshape(nz, 1, 1) * np.float32(rho)
+        with gwm.Model(g, gwm.MemberSpec(rain=rain, moist=True)) as m:
+            m.upload(s)
+            m.apply_warm_rain_microphysics(fallout)
+            return m.download()
+
+    if fallout == "nominal":
+        o = one(1.0, 300.0, 0.030, 0.0, 0.0, rain=gwm.WarmRainConfig(dt=2.0, cloud_autoconversion_rate=0.0))
+        assert o["qv"][0, 0, 0] < 0.030 and o["qc"][0, 0, 0] > 0 and abs(o["qr"][0, 0, 0]) < 1e-6
+        assert abs(o["qv"].sum() + o["qc"].sum() + o["qr"].sum() - 0.030) < 1e-5
+        assert o["rho_theta"][0, 0, 0] / o["rho"][0, 0, 0] > 300.0
+        o = one(1.0, 295.0, [0, 0], [0, 0], [0.004, 0.010], nz=2, z_top=2000.0,
+                rain=gwm.WarmRainConfig(dt=1.0, cloud_autoconversion_rate=0.0, rain_evaporation_rate=0.0,
+                                        rain_terminal_velocity=250.0, sedimentation_layer_depth_m=1000.0,
+                                        enable_latent_heating=False))
+        assert abs(o["qr"][1, 0, 0] - 0.0075) < 1e-6 and abs(o["qr"][0, 0, 0] - 0.0055) < 1e-6
+        assert abs(o["precip"][0, 0] - 1.0) < 1e-6
+        o = one(1.0, 295.0, 0.006, 0.002, 0.001,
+                rain=gwm.WarmRainConfig(dt=2.0, cloud_autoconversion_threshold=1e-4, cloud_autoconversion_rate=1.0,
+                                        rain_evaporation_rate=0.0, enable_latent_heating=False))
+        assert o["qc"][0, 0, 0] < 0.002 and o["qr"][0, 0, 0] > 0.001
+        assert abs(o["qv"].sum() + o["qc"].sum() + o["qr"].sum() - 0.009) < 1e-5
+    else:
+        o = one(1.0, 295.0, 0.0, 0.0, 0.010,
+                rain=gwm.WarmRainConfig(dt=1.0, cloud_autoconversion_rate=0.0, rain_evaporation_rate=0.0,
+                                        rain_terminal_velocity=1500.0, enable_latent_heating=False))
+        assert abs(o["qr"][0, 0, 0]) < 1e-6
+        assert abs(o["precip"][0, 0] - 10.0) < 1e-6

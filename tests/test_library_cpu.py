@@ -1,0 +1,118 @@
+"""CPU-side checks of the product library: it builds, loads without a GPU,
+exports every symbol its headers declare, and its host-side code (layout table,
+rank<->global conversion, case builders, terrain) agrees with the oracle."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in ("gwm_b200.h", "gwm_b200_cases.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        names |= set(re.findall(r"\b(gwm_b200_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol(gwm):
+    L = gwm.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(gwm.EXPORTED) <= set(syms)
+
+
+def test_create_fails_loudly_without_device(gwm):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    with pytest.raises(RuntimeError, match="no CUDA device"):
+        gwm.Model(gwm.GridSpec(8, 8, 4), gwm.MemberSpec())
+
+
+@pytest.mark.parametrize("args", [(8, 8, 2, 1, 2, 2, True, True), (13, 7, 3, 1, 3, 2, False, True),
+                                  (10, 9, 2, 1, 1, 3, True, False), (5, 5, 1, 2, 2, 2, False, False)])
+def test_layout_matches_oracle(gwm, orc, args):
+    nx, ny, nz, h, rx, ry, px, py = args
+    a = gwm.layout(nx, ny, nz, h, rx, ry, px, py)
+    b = orc.layout(nx, ny, nz, h, rx, ry, px, py)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("orient", [0, 1, 2, 3])
+def test_rank_global_round_trip(gwm, orient):
+    nx, ny, nz, h, rx, ry = 11, 9, 3, 1, 3, 2
+    lay = gwm.layout(nx, ny, nz, h, rx, ry)
+    rng = np.random.default_rng(orient)
+    shp = (nz + (orient == 3), ny + (orient == 2), nx + (orient == 1))
+    glob = rng.standard_normal(shp).astype(np.float32)
+    ranks = []
+    for row in lay:
+        nxl, nyl = row[4] - row[3], row[6] - row[5]
+        ranks.append(np.zeros((nz + (orient == 3), nyl + (orient == 2) + 2 * h, nxl + (orient == 1) + 2 * h),
+                              dtype=np.float32))
+    gwm.global_to_ranks(glob, ranks, nx, ny, nz, h, rx, ry, True, True, orient)
+    back = gwm.ranks_to_global(ranks, nx, ny, nz, h, rx, ry, True, True, orient)
+    assert np.array_equal(back, glob)
+
+
+CASES = [
+    ("constant", dict(rho_background=1.1, theta_background=301.0, u_background=10.0, v_background=-4.0)),
+    ("warm_bubble", dict(theta_perturbation=2.0, center_z_fraction=0.3)),
+    ("density_current", dict(theta_perturbation=15.0, center_z_fraction=0.35, radius_x_fraction=0.15)),
+    ("hydrostatic_rest", dict(rho_surface=1.16, theta_ref=300.0)),
+    ("mountain_wave_background", dict(rho_surface=1.18, theta_ref=300.0, u_background=15.0)),
+    ("hydrostatic_warm_bubble", dict(rho_surface=1.16, theta_ref=300.0, theta_perturbation=2.0,
+                                     center_z_fraction=0.2, radius_x_fraction=0.25, radius_z_fraction=0.2)),
+]
+
+
+@pytest.mark.parametrize("kind,kw", CASES)
+def test_case_builders_match_oracle(gwm, orc, kind, kw):
+    terr = gwm.build_terrain("cosine_mountain", 16, 12, 1000.0, 1000.0, height=600.0,
+                             half_width_x=0.3, half_width_y=0.3)
+    g = gwm.GridSpec(16, 12, 10, dx=1000.0, dy=1000.0, z_top=10000.0, terrain=terr)
+    og = orc.GridSpec(16, 12, 10, dx=1000.0, dy=1000.0, z_top=10000.0, terrain=terr.astype(np.float64))
+    mine = gwm.build_case(kind, g, gwm.CaseParams(**kw))
+    ref = orc.case(kind, og, orc.CaseSpec(**{k: v for k, v in kw.items()}), precision=32)
+    for k in ("rho", "rho_theta", "u", "v", "w"):
+        np.testing.assert_allclose(mine[k], ref[k], rtol=2e-6, atol=1e-6, err_msg=f"{kind}:{k}")
+
+
+def test_cosine_terrain_kat(gwm):
+    # tests/unit/test_hybrid_height_metrics.cpp:29-41: the cosine hill peaks at the centre
+    t = gwm.build_terrain("cosine_mountain", 21, 21, 1000.0, 1000.0, height=1200.0,
+                          half_width_x=0.25, half_width_y=0.25)
+    assert t[10, 10] == pytest.approx(1200.0)
+    assert t[0, 0] == 0.0 and t.max() == t[10, 10]
+    a = gwm.build_terrain("agnesi", 64, 64, 1000.0, 1000.0, height=400.0,
+                          half_width_x=10000.0, half_width_y=10000.0)
+    assert a.max() <= 400.0 and a.max() > 390.0
+
+
+def test_moist_sounding_properties(gwm):
+    g = gwm.GridSpec(8, 6, 32, dx=3000.0, dy=3000.0, z_top=24000.0)
+    p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=3)
+    s = gwm.build_case("moist_sounding", g, p, moist=True)
+    th = s["rho_theta"] / s["rho"]
+    zc = (np.arange(32) + 0.5) * 750.0
+    qv = s["qv"] / s["rho"]
+    # theta: noisy below 1 km, 300 K + 4 K/km above (within FP32 of the EOS inversion)
+    upper = zc > 1500.0
+    np.testing.assert_allclose(th[upper, 0, 0], 300.0 + 0.004 * (zc[upper] - 1000.0), rtol=2e-5)
+    low = zc < 1000.0
+    assert np.std(th[low]) > 0.1
+    # hydrostatic: pressure decreases with height, density positive
+    assert np.all(s["rho"] > 0) and np.all(np.diff(s["rho"][:, 0, 0]) < 0)
+    assert np.all(qv >= 1e-5 * 0.999) and qv[0].mean() > 0.005
+    # same seed -> same state; another seed -> different noise
+    s2 = gwm.build_case("moist_sounding", g, p, moist=True)
+    assert np.array_equal(s["rho_theta"], s2["rho_theta"])
+    s3 = gwm.build_case("moist_sounding", g, gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=4), moist=True)
+    assert not np.array_equal(s["rho_theta"], s3["rho_theta"])
