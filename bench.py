@@ -95,7 +95,7 @@ class ClockSampler:
         sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
         mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[3 + i]})
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 
@@ -186,6 +186,7 @@ def main():
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="launch kernels directly (profiling)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -210,7 +211,7 @@ def main():
     stream = torch.cuda.Stream()
     model.set_stream(stream.cuda_stream)
     model.upload(state)
-    model.use_graph(True)
+    model.use_graph(not args.no_graph)
     cells = args.nx * args.ny * NZ
 
     def barrier():
@@ -264,7 +265,7 @@ def main():
                        "dt_s": DT, "fast_substeps": NS, "rain_terminal_velocity": VT,
                        "phases": "dry SSPRK3 + 3-tracer SSPRK3 + warm rain/fallout",
                        "l2": "inputs larger than L2 (each field 282 MB)",
-                       "graph": True, "parallelism": f"replicas{world}"},
+                       "graph": not args.no_graph, "parallelism": f"replicas{world}"},
             "gpu_launches": launches,
             "state_finite": finite,
             "roofline": roof,

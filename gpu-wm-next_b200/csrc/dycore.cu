@@ -28,26 +28,64 @@ __device__ __forceinline__ float met3(const float* m, const Geom& g, int i, int 
 struct SlowCol {
   float rho, rt, th, p, uf, vf, wf;
 };
+// Raw loads of one plane, issued ahead of use.
+struct SlowRaw {
+  float rho, t, u, v, w, du, dv, dw, z;
+};
+// Blend partner (q0) at the thread's own positions.
+struct SlowQ0 {
+  float rho, rt, u, v, w, wtop;
+};
 
-__device__ __forceinline__ SlowCol slow_load(const SlowArgs& a, bool valid, int base, int kk) {
-  SlowCol c{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  if (!valid) return c;
+template <bool TERRAIN>
+__device__ __forceinline__ SlowRaw slow_raw(const SlowArgs& a, bool valid, int base, int kk) {
+  SlowRaw r{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (!valid) return r;
   const int o = base + kk * a.g.plane;
   if (kk < a.g.nz) {
-    c.rho = __ldg(a.rho + o);
-    const float t = __ldg(a.th + o);
-    c.rt = a.th_is_rt ? t : c.rho * t;
-    c.th = theta_of(c.rho, c.rt);
-    c.p = eos_pressure(c.rho, c.rt);
-    c.uf = __ldg(a.u + o);
-    c.vf = __ldg(a.v + o);
-    if (a.du) { c.uf += __ldg(a.du + o); c.vf += __ldg(a.dv + o); }
+    r.rho = __ldg(a.rho + o);
+    r.t = __ldg(a.th + o);
+    r.u = __ldg(a.u + o);
+    r.v = __ldg(a.v + o);
+    if (a.du) { r.du = __ldg(a.du + o); r.dv = __ldg(a.dv + o); }
+    if (TERRAIN) r.z = __ldg(a.zc + o);
   }
   if (kk <= a.g.nz) {
-    c.wf = __ldg(a.w + o);
-    if (a.dw) c.wf += __ldg(a.dw + o);
+    r.w = __ldg(a.w + o);
+    if (a.dw) r.dw = __ldg(a.dw + o);
   }
+  return r;
+}
+
+__device__ __forceinline__ SlowCol slow_derive(const SlowArgs& a, const SlowRaw& r, bool valid, int kk) {
+  SlowCol c{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (!valid) return c;
+  if (kk < a.g.nz) {
+    c.rho = r.rho;
+    c.rt = a.th_is_rt ? r.t : c.rho * r.t;
+    c.th = theta_of(c.rho, c.rt);
+    c.p = eos_pressure(c.rho, c.rt);
+    c.uf = r.u + r.du;
+    c.vf = r.v + r.dv;
+  }
+  c.wf = r.w + r.dw;
   return c;
+}
+
+__device__ __forceinline__ SlowQ0 slow_q0(const SlowArgs& a, int base, int kk, bool own_c, bool own_u,
+                                          bool own_v) {
+  SlowQ0 q{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (!a.rho0 || kk >= a.g.nz) return q;
+  const int o = base + kk * a.g.plane;
+  if (own_c) {
+    q.rho = __ldg(a.rho0 + o);
+    q.rt = __ldg(a.rt0 + o);
+    q.w = __ldg(a.w0 + o);
+    if (kk + 1 == a.g.nz) q.wtop = __ldg(a.w0 + o + a.g.plane);
+  }
+  if (own_u) q.u = __ldg(a.u0 + o);
+  if (own_v) q.v = __ldg(a.v0 + o);
+  return q;
 }
 
 // One-sided / centred dp/dz of a column: dry_pressure_gradient.cu:37-73.
@@ -87,16 +125,19 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
   for (int q = tid; q < nz; q += NT)
     s_thref[q] = (float)(acc_read(a.th_acc + q, kScaleTheta) * a.inv_count);
 
-  SlowCol cm{}, cc = slow_load(a, valid, base, 0), cn = slow_load(a, valid, base, 1);
-  float zm = 0.f, zcc = 0.f, zn = 0.f;
-  if (TERRAIN && valid) {
-    zcc = met3(a.zc, g, gi, gj, 0);
-    zn = nz > 1 ? met3(a.zc, g, gi, gj, 1) : 0.f;
-  }
+  // software pipeline: plane fields two planes ahead, blend partner one plane ahead
+  const SlowRaw r0 = slow_raw<TERRAIN>(a, valid, base, 0);
+  const SlowRaw r1 = slow_raw<TERRAIN>(a, valid, base, 1);
+  SlowRaw r2 = slow_raw<TERRAIN>(a, valid, base, 2);
+  SlowQ0 q0c = slow_q0(a, base, 0, own_c, own_u, own_v);
+  SlowCol cm{}, cc = slow_derive(a, r0, valid, 0), cn = slow_derive(a, r1, valid, 1);
+  float zm = 0.f, zcc = r0.z, zn = r1.z;
   const bool blend = a.rho0 != nullptr;
 
   for (int k = 0; k < nz; ++k) {
     const int pb = k & 1;
+    const SlowRaw r3 = slow_raw<TERRAIN>(a, valid, base, k + 3);
+    const SlowQ0 q0n = slow_q0(a, base, k + 1, own_c, own_u, own_v);
     s_th[pb][ty][tx] = cc.th;
     s_p[pb][ty][tx] = cc.p;
     s_u[pb][ty][tx] = cc.uf;
@@ -153,8 +194,8 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
           float r1 = fmaxf(1.0e-6f, cc.rho + a.dt * t_rho);
           float q1 = fmaxf(1.0e-6f, cc.rt + a.dt * t_rt);
           if (blend) {
-            r1 = a.wa * __ldg(a.rho0 + o) + a.wb * r1;
-            q1 = a.wa * __ldg(a.rt0 + o) + a.wb * q1;
+            r1 = a.wa * q0c.rho + a.wb * r1;
+            q1 = a.wa * q0c.rt + a.wb * q1;
           }
           const float th1 = q1 / fmaxf(r1, 1.0e-6f);
           store_mirrored(a.o_rho, g, kCell, gi, gj, k, r1);
@@ -198,7 +239,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
           a.o_u[o] = t_u;
         } else {
           float u1 = fmaxf(-1.0e30f, cc.uf + a.dt * t_u);
-          if (blend) u1 = a.wa * __ldg(a.u0 + o) + a.wb * u1;
+          if (blend) u1 = a.wa * q0c.u + a.wb * u1;
           store_mirrored(a.o_u, g, kFaceX, gi, gj, k, u1);
         }
       }
@@ -233,7 +274,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
           a.o_v[o] = t_v;
         } else {
           float v1 = fmaxf(-1.0e30f, cc.vf + a.dt * t_v);
-          if (blend) v1 = a.wa * __ldg(a.v0 + o) + a.wb * v1;
+          if (blend) v1 = a.wa * q0c.v + a.wb * v1;
           store_mirrored(a.o_v, g, kFaceY, gi, gj, k, v1);
         }
       }
@@ -265,11 +306,11 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
           if (k + 1 == nz) a.o_w[o + g.plane] = 0.0f;
         } else {
           float w1 = fmaxf(-1.0e30f, cc.wf + a.dt * t_w);
-          if (blend) w1 = a.wa * __ldg(a.w0 + o) + a.wb * w1;
+          if (blend) w1 = a.wa * q0c.w + a.wb * w1;
           store_mirrored(a.o_w, g, kFaceZ, gi, gj, k, w1);
           if (k + 1 == nz) {  // top face: zero tendency
             float wt = fmaxf(-1.0e30f, cn.wf);
-            if (blend) wt = a.wa * __ldg(a.w0 + o + g.plane) + a.wb * wt;
+            if (blend) wt = a.wa * q0c.wtop + a.wb * wt;
             store_mirrored(a.o_w, g, kFaceZ, gi, gj, k + 1, wt);
           }
         }
@@ -283,12 +324,12 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
     // advance the column window
     cm = cc;
     cc = cn;
-    cn = slow_load(a, valid, base, k + 2);
-    if (TERRAIN && valid) {
-      zm = zcc;
-      zcc = zn;
-      zn = (k + 2 < nz) ? met3(a.zc, g, gi, gj, k + 2) : 0.f;
-    }
+    cn = slow_derive(a, r2, valid, k + 2);
+    zm = zcc;
+    zcc = zn;
+    zn = r2.z;
+    r2 = r3;
+    q0c = q0n;
   }
   if (a.acc_mode) {
     __syncthreads();
@@ -308,15 +349,32 @@ struct FastCol {
   float rho, th, thp, p;   // thp: theta recovered from (rho, rho*theta) as the reference does
   float pref, rref;        // column hydrostatic reference (terrain)
 };
+struct FastRaw {
+  float rho, th, z;        // plane values loaded ahead of use
+};
+struct FastInc {
+  float du, dv, dw1;       // increments at the plane's own faces (dw1: face k+1)
+};
 
 template <bool TERRAIN>
-__device__ __forceinline__ FastCol fast_load(const FastArgs& a, bool valid, int base, int kk,
-                                             const FastCol& below, float dzk) {
+__device__ __forceinline__ FastRaw fast_raw(const FastArgs& a, bool valid, int base, int kk, int gi,
+                                            int gj) {
+  FastRaw r{0.f, 0.f, 0.f};
+  if (!valid || kk >= a.g.nz) return r;
+  const int o = base + kk * a.g.plane;
+  r.rho = __ldg(a.rho_in + o);
+  r.th = __ldg(a.th + o);
+  if (TERRAIN) r.z = __ldg(a.zc + o);
+  return r;
+}
+
+template <bool TERRAIN>
+__device__ __forceinline__ FastCol fast_derive(const FastArgs& a, const FastRaw& r, bool valid, int kk,
+                                               const FastCol& below, float dzk) {
   FastCol c{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (!valid || kk >= a.g.nz) return c;
-  const int o = base + kk * a.g.plane;
-  c.rho = __ldg(a.rho_in + o);
-  c.th = __ldg(a.th + o);
+  c.rho = r.rho;
+  c.th = r.th;
   const float rt = c.rho * c.th;  // K10 rebuild_rho_theta_from_theta_kernel
   c.thp = theta_of(c.rho, rt);
   c.p = eos_pressure(c.rho, rt);  // K20
@@ -336,6 +394,18 @@ __device__ __forceinline__ FastCol fast_load(const FastArgs& a, bool valid, int 
     }
   }
   return c;
+}
+
+template <bool FIRST>
+__device__ __forceinline__ FastInc fast_inc(const FastArgs& a, int base, int kk, bool do_u, bool do_v,
+                                            bool own_c) {
+  FastInc d{0.f, 0.f, 0.f};
+  if (FIRST || kk >= a.g.nz) return d;
+  const int o = base + kk * a.g.plane;
+  if (do_u) d.du = __ldg(a.du_in + o);
+  if (do_v) d.dv = __ldg(a.dv_in + o);
+  if (own_c && kk + 1 < a.g.nz) d.dw1 = __ldg(a.dw_in + o + a.g.plane);
+  return d;
 }
 
 template <bool TERRAIN, bool FIRST>
@@ -367,6 +437,11 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
   if (blockIdx.x == 0 && blockIdx.y == 0 && a.clr_a) {
     for (int q = tid; q < nz; q += NT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
   }
+  // software pipeline: plane fields two planes ahead, increments one plane ahead
+  FastRaw r0 = fast_raw<TERRAIN>(a, valid, base, 0, gi, gj);
+  FastRaw r1 = fast_raw<TERRAIN>(a, valid, base, 1, gi, gj);
+  FastRaw r2 = fast_raw<TERRAIN>(a, valid, base, 2, gi, gj);
+  FastInc d0 = fast_inc<FIRST>(a, base, 0, do_u, do_v, own_c);
   if (!TERRAIN) {  // K6/K7 level means (deterministic sums instead of float atomics)
     for (int q = tid; q < nz; q += NT) {
       s_rref[q] = (float)(acc_read(a.ref_a + q, kScaleRho) * a.inv_count);
@@ -376,19 +451,29 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
   }
   const int acc_mode = a.acc_off ? 0 : (a.final_kind == 0 ? (TERRAIN ? 0 : 1) : 2);
 
-  float zm = 0.f, zcc = 0.f, zn = 0.f;
-  if (TERRAIN && valid) {
-    zcc = met3(a.zc, g, gi, gj, 0);
-    zn = nz > 1 ? met3(a.zc, g, gi, gj, 1) : 0.f;
-  }
+  float zm = 0.f, zcc = r0.z, zn = r1.z;
   FastCol none{};
-  FastCol cm{}, cc = fast_load<TERRAIN>(a, valid, base, 0, none, 0.f);
-  FastCol cn = fast_load<TERRAIN>(a, valid, base, 1, cc, zn - zcc);
+  FastCol cm{}, cc = fast_derive<TERRAIN>(a, r0, valid, 0, none, 0.f);
+  FastCol cn = fast_derive<TERRAIN>(a, r1, valid, 1, cc, zn - zcc);
   float dw_c = 0.0f;  // increment at face k (face 0 never changes)
 
   for (int k = 0; k < nz; ++k) {
     const int pb = k & 1;
     const int o = base + k * g.plane;
+    // issue the loads of later planes before any use of this plane
+    const FastRaw r3 = fast_raw<TERRAIN>(a, valid, base, k + 3, gi, gj);
+    const FastInc d1 = fast_inc<FIRST>(a, base, k + 1, do_u, do_v, own_c);
+    float bu0 = 0.f, bv0 = 0.f, bw0 = 0.f, bw1 = 0.f;
+    if (final_step) {
+      if (own_u) bu0 = __ldg(a.bu + o);
+      if (own_v) bv0 = __ldg(a.bv + o);
+      if (own_c) { bw1 = __ldg(a.bw + o + g.plane); if (k == 0) bw0 = __ldg(a.bw + o); }
+    }
+    float idzf = 0.f, idzc = 0.f;
+    if (own_c) {
+      idzf = (k + 1 < nz) ? (TERRAIN ? __ldg(a.idz_f + o + g.plane) : __ldg(a.idz_f + k + 1)) : 0.f;
+      idzc = TERRAIN ? __ldg(a.idz_c + o) : __ldg(a.idz_c + k);
+    }
     s_p[pb][ty][tx] = cc.p;
     if (TERRAIN) {
       s_zc[pb][ty][tx] = zcc;
@@ -402,57 +487,44 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
       else acc_add(a.acc_a + k - 1, sa, kScaleTheta);
     }
     // K12: X-face momentum (dry_fast_modes.cu:160-229)
-    float du_new = 0.0f;
-    if (do_u) {
-      const float du_old = FIRST ? 0.0f : __ldg(a.du_in + o);
-      du_new = du_old;
-      if (a.hmom && !skip_u) {
-        const float pl = s_p[pb][ty][tx - 1], pr = cc.p;
-        float x;
-        if (TERRAIN) {
-          const float dzdx = (s_zc[pb][ty][tx] - s_zc[pb][ty][tx - 1]) / dx;
-          const float dpdz = 0.5f * (s_dz[pb][ty][tx - 1] + s_dz[pb][ty][tx]);
-          x = (pr - pl) / dx - dzdx * dpdz;
-        } else {
-          x = (pr - pl) / dx;
-        }
-        du_new = du_old + (-dtf * x);
+    float du_new = d0.du;
+    if (do_u && a.hmom && !skip_u) {
+      const float pl = s_p[pb][ty][tx - 1], pr = cc.p;
+      float x;
+      if (TERRAIN) {
+        const float dzdx = (s_zc[pb][ty][tx] - s_zc[pb][ty][tx - 1]) / dx;
+        const float dpdz = 0.5f * (s_dz[pb][ty][tx - 1] + s_dz[pb][ty][tx]);
+        x = (pr - pl) / dx - dzdx * dpdz;
+      } else {
+        x = (pr - pl) / dx;
       }
+      du_new = d0.du + (-dtf * x);
     }
     s_du[pb][ty][tx] = du_new;
     // K13: Y-face momentum (dry_fast_modes.cu:231-301)
-    float dv_new = 0.0f;
-    if (do_v) {
-      const float dv_old = FIRST ? 0.0f : __ldg(a.dv_in + o);
-      dv_new = dv_old;
-      if (a.hmom && !skip_v) {
-        const float ps = s_p[pb][ty - 1][tx], pn = cc.p;
-        float x;
-        if (TERRAIN) {
-          const float dzdy = (s_zc[pb][ty][tx] - s_zc[pb][ty - 1][tx]) / dy;
-          const float dpdz = 0.5f * (s_dz[pb][ty - 1][tx] + s_dz[pb][ty][tx]);
-          x = (pn - ps) / dy - dzdy * dpdz;
-        } else {
-          x = (pn - ps) / dy;
-        }
-        dv_new = dv_old + (-dtf * x);
+    float dv_new = d0.dv;
+    if (do_v && a.hmom && !skip_v) {
+      const float ps = s_p[pb][ty - 1][tx], pn = cc.p;
+      float x;
+      if (TERRAIN) {
+        const float dzdy = (s_zc[pb][ty][tx] - s_zc[pb][ty - 1][tx]) / dy;
+        const float dpdz = 0.5f * (s_dz[pb][ty - 1][tx] + s_dz[pb][ty][tx]);
+        x = (pn - ps) / dy - dzdy * dpdz;
+      } else {
+        x = (pn - ps) / dy;
       }
+      dv_new = d0.dv + (-dtf * x);
     }
     s_dv[pb][ty][tx] = dv_new;
     // K14: Z face k+1 (dry_fast_modes.cu:303-348), perturbations about the reference
-    float dw_n = 0.0f;
-    if (own_c && k + 1 <= nz) {
-      const float dw_old = (FIRST || k + 1 == nz) ? 0.0f : __ldg(a.dw_in + o + g.plane);
-      dw_n = dw_old;
-      if (k + 1 < nz) {
-        const float prl = TERRAIN ? cc.pref : s_pref[k], pru = TERRAIN ? cn.pref : s_pref[k + 1];
-        const float rrl = TERRAIN ? cc.rref : s_rref[k], rru = TERRAIN ? cn.rref : s_rref[k + 1];
-        const float ppl = cc.p - prl, ppu = cn.p - pru;
-        const float rpf = 0.5f * ((cc.rho - rrl) + (cn.rho - rru));
-        const float idz = TERRAIN ? met3(a.idz_f, g, gi, gj, k + 1) : __ldg(a.idz_f + k + 1);
-        const float tend = -(ppu - ppl) * idz - a.gravity * rpf;
-        dw_n = dw_old + dtf * tend;
-      }
+    float dw_n = d0.dw1;
+    if (own_c && k + 1 < nz) {
+      const float prl = TERRAIN ? cc.pref : s_pref[k], pru = TERRAIN ? cn.pref : s_pref[k + 1];
+      const float rrl = TERRAIN ? cc.rref : s_rref[k], rru = TERRAIN ? cn.rref : s_rref[k + 1];
+      const float ppl = cc.p - prl, ppu = cn.p - pru;
+      const float rpf = 0.5f * ((cc.rho - rrl) + (cn.rho - rru));
+      const float tend = -(ppu - ppl) * idzf - a.gravity * rpf;
+      dw_n = d0.dw1 + dtf * tend;
     }
     __syncthreads();
 
@@ -461,17 +533,16 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
       // K15: density from the perturbation mass-flux divergence (dry_fast_modes.cu:350-394)
       float rho_new = cc.rho;
       if (a.dens) {
-        const float idz = TERRAIN ? met3(a.idz_c, g, gi, gj, k) : __ldg(a.idz_c + k);
         const float div = (s_du[pb][ty][tx + 1] - s_du[pb][ty][tx]) / dx +
-                          (s_dv[pb][ty + 1][tx] - s_dv[pb][ty][tx]) / dy + (dw_n - dw_c) * idz;
+                          (s_dv[pb][ty + 1][tx] - s_dv[pb][ty][tx]) / dy + (dw_n - dw_c) * idzc;
         rho_new = fmaxf(1.0e-6f, cc.rho - dtf * div);
       }
       const float rt_new = rho_new * cc.th;  // K10 on the state
       if (final_step) {
         store_mirrored(a.f_rho, g, kCell, gi, gj, k, rho_new);
         store_mirrored(a.f_rt, g, kCell, gi, gj, k, rt_new);
-        if (k == 0) store_mirrored(a.f_w, g, kFaceZ, gi, gj, 0, __ldg(a.bw + o));
-        store_mirrored(a.f_w, g, kFaceZ, gi, gj, k + 1, __ldg(a.bw + o + g.plane) + dw_n);
+        if (k == 0) store_mirrored(a.f_w, g, kFaceZ, gi, gj, 0, bw0);
+        store_mirrored(a.f_w, g, kFaceZ, gi, gj, k + 1, bw1 + dw_n);
       } else {
         store_mirrored(a.rho_out, g, kCell, gi, gj, k, rho_new);
         if (k + 1 < nz) store_mirrored(a.dw_out, g, kFaceZ, gi, gj, k + 1, dw_n);
@@ -484,11 +555,11 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
       }
     }
     if (own_u) {
-      if (final_step) store_mirrored(a.f_u, g, kFaceX, gi, gj, k, __ldg(a.bu + o) + du_new);
+      if (final_step) store_mirrored(a.f_u, g, kFaceX, gi, gj, k, bu0 + du_new);
       else store_mirrored(a.du_out, g, kFaceX, gi, gj, k, du_new);
     }
     if (own_v) {
-      if (final_step) store_mirrored(a.f_v, g, kFaceY, gi, gj, k, __ldg(a.bv + o) + dv_new);
+      if (final_step) store_mirrored(a.f_v, g, kFaceY, gi, gj, k, bv0 + dv_new);
       else store_mirrored(a.dv_out, g, kFaceY, gi, gj, k, dv_new);
     }
     if (acc_mode) {
@@ -497,17 +568,15 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
       if ((tid & 31) == 0) { s_red[pb][tid >> 5][0] = red_a; s_red[pb][tid >> 5][1] = red_b; }
     }
     dw_c = dw_n;
+    d0 = d1;
     // advance the column window
     cm = cc;
     cc = cn;
-    float dzk = 0.f;
-    if (TERRAIN && valid) {
-      zm = zcc;
-      zcc = zn;
-      zn = (k + 2 < nz) ? met3(a.zc, g, gi, gj, k + 2) : 0.f;
-      dzk = zn - zcc;
-    }
-    cn = fast_load<TERRAIN>(a, valid, base, k + 2, cc, dzk);
+    zm = zcc;
+    zcc = zn;
+    zn = r2.z;
+    cn = fast_derive<TERRAIN>(a, r2, valid, k + 2, cc, zn - zcc);
+    r2 = r3;
   }
   if (acc_mode) {
     __syncthreads();

@@ -24,17 +24,18 @@ __device__ __forceinline__ TrCol tr_load(const TracerArgs& a, bool valid, int ba
     c.rho = __ldg(a.rho + o);
     c.uf = __ldg(a.u + o);
     c.vf = __ldg(a.v + o);
-    const float rr = fmaxf(c.rho, 1.0e-6f);
 #pragma unroll
-    for (int t = 0; t < NTR; ++t) {
-      if (t < a.ntracers) {
-        c.rq[t] = __ldg(a.q_in[t] + o);
-        c.q[t] = c.rq[t] / rr;  // mixing ratio: dry_transport.cu:91-94
-      }
-    }
+    for (int t = 0; t < NTR; ++t)
+      if (t < a.ntracers) c.rq[t] = __ldg(a.q_in[t] + o);
   }
   if (kk <= a.g.nz) c.wf = __ldg(a.w + o);
   return c;
+}
+
+__device__ __forceinline__ void tr_mix(TrCol& c) {
+  const float rr = fmaxf(c.rho, 1.0e-6f);
+#pragma unroll
+  for (int t = 0; t < NTR; ++t) c.q[t] = c.rq[t] / rr;  // mixing ratio: dry_transport.cu:91-94
 }
 
 __global__ void __launch_bounds__(NT) k_tracer_stage(const TracerArgs a) {
@@ -54,18 +55,28 @@ __global__ void __launch_bounds__(NT) k_tracer_stage(const TracerArgs a) {
   __shared__ float s_u[2][BY][BX], s_v[2][BY][BX];
 
   TrCol cm{}, cc = tr_load(a, valid, base, 0), cn = tr_load(a, valid, base, 1);
+  TrCol c2 = tr_load(a, valid, base, 2);
+  tr_mix(cc);
+  tr_mix(cn);
   for (int k = 0; k < nz; ++k) {
     const int pb = k & 1;
+    const TrCol c3 = tr_load(a, valid, base, k + 3);
+    float q0v[NTR] = {0.f, 0.f, 0.f};
+    const int o = base + k * g.plane;
+    if (own_c && blend) {
+#pragma unroll
+      for (int t = 0; t < NTR; ++t)
+        if (t < a.ntracers) q0v[t] = __ldg(a.q0[t] + o);
+    }
+    const float idz = own_c ? (a.terrain ? __ldg(a.idz_c + o) : __ldg(a.idz_c + k)) : 0.f;
 #pragma unroll
     for (int t = 0; t < NTR; ++t) s_q[t][pb][ty][tx] = cc.q[t];
     s_u[pb][ty][tx] = cc.uf;
     s_v[pb][ty][tx] = cc.vf;
     __syncthreads();
     if (own_c) {
-      const int o = base + k * g.plane;
       const float fw = cc.uf, fe = s_u[pb][ty][tx + 1], fs = cc.vf, fn = s_v[pb][ty + 1][tx];
       const float fb = cc.wf, ft = cn.wf;
-      const float idz = a.terrain ? __ldg(a.idz_c + o) : __ldg(a.idz_c + k);
 #pragma unroll
       for (int t = 0; t < NTR; ++t) {
         if (t >= a.ntracers) break;
@@ -82,13 +93,15 @@ __global__ void __launch_bounds__(NT) k_tracer_stage(const TracerArgs a) {
         const float gt = ft * (ft >= 0.0f ? qc : qt);
         const float div = (ge - gw) / dx + (gn - gs) / dy + (gt - gb) * idz;
         float out = fmaxf(0.0f, cc.rq[t] - a.dt * div);
-        if (blend) out = a.wa * __ldg(a.q0[t] + o) + a.wb * out;
+        if (blend) out = a.wa * q0v[t] + a.wb * out;
         store_mirrored(a.q_out[t], g, kCell, gi, gj, k, out);
       }
     }
     cm = cc;
     cc = cn;
-    cn = tr_load(a, valid, base, k + 2);
+    cn = c2;
+    tr_mix(cn);
+    c2 = c3;
   }
 }
 
@@ -113,14 +126,25 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
   const bool active = gi < g.nx && gj < g.ny;
   __shared__ double s_th[kMaxNz][RB / 32];
   float incoming = 0.0f;
+  // one-cell-ahead prefetch down the column
+  float n_rho = 0.f, n_rt = 0.f, n_qv = 0.f, n_qc = 0.f, n_qr = 0.f;
+  if (active) {
+    const int o = gidx(g, gi, gj, g.nz - 1);
+    n_rho = __ldg(a.rho + o); n_rt = a.rt[o]; n_qv = a.qv[o]; n_qc = a.qc[o]; n_qr = a.qr[o];
+  }
   for (int k = g.nz - 1; k >= 0; --k) {
     double th_sum = 0.0;
+    const float c_rho = n_rho, c_rt = n_rt, c_qv = n_qv, c_qc = n_qc, c_qr = n_qr;
+    if (active && k > 0) {
+      const int o1 = gidx(g, gi, gj, k - 1);
+      n_rho = __ldg(a.rho + o1); n_rt = a.rt[o1]; n_qv = a.qv[o1]; n_qc = a.qc[o1]; n_qr = a.qr[o1];
+    }
     if (active) {
       const int o = gidx(g, gi, gj, k);
       // warm_rain_kernel: warm_rain.cu:36-120
-      const float rho_d = __ldg(a.rho + o);
+      const float rho_d = c_rho;
       const float rho = fmaxf(rho_d, 1.0e-6f);
-      const float rt = a.rt[o];
+      const float rt = c_rt;
       float th = rt / rho;
       float p = eos_pressure(rho, rt);
       float temp;
@@ -130,9 +154,9 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
         temp = thc * powf(fmaxf(pc / kP0, 1.0e-6f), kKappa);
       }
       const float exner = fmaxf(temp / fmaxf(th, 1.0e-6f), 1.0e-6f);
-      float qv = fmaxf(a.qv[o] / rho, 0.0f);
-      float qc = fmaxf(a.qc[o] / rho, 0.0f);
-      float qr = fmaxf(a.qr[o] / rho, 0.0f);
+      float qv = fmaxf(c_qv / rho, 0.0f);
+      float qc = fmaxf(c_qc / rho, 0.0f);
+      float qr = fmaxf(c_qr / rho, 0.0f);
       const float lh = kLv / (dry_cp() * fmaxf(exner, 1.0e-6f));
       float qs = qsat(temp, p);
       if (qv > qs) {
