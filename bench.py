@@ -81,6 +81,15 @@ class ClockSampler:
             if len(parts) >= 7:
                 self.samples.append(parts)
 
+    def wait_first(self, timeout):
+        t = time.time()
+        while self._proc and not self.samples and time.time() - t < timeout:
+            time.sleep(0.05)
+
+    def mark(self):
+        """Only samples taken after this point describe the timed region."""
+        self._start = len(self.samples)
+
     def stop(self):
         if self._proc:
             self._proc.terminate()
@@ -90,6 +99,7 @@ class ClockSampler:
                 self._proc.kill()
 
     def summary(self):
+        self.samples = self.samples[getattr(self, "_start", 0):]
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
@@ -219,12 +229,14 @@ def main():
         if dist:
             dist.barrier()
 
+    clocks = ClockSampler(local)
+    clocks.start()
     # warm-up (also captures the step graph)
     with torch.cuda.stream(stream):
         model.step(max(args.warmup, 1))
     barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
+    clocks.wait_first(10.0)
+    clocks.mark()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     t0.record(stream)

@@ -158,6 +158,7 @@ def lib():
     L.gwm_b200_slow_tendencies.argtypes = [vp, C.c_int, C.POINTER(_Fields)]
     L.gwm_b200_budgets.argtypes = [vp, C.c_int, C.POINTER(_Budget)]
     L.gwm_b200_profile.argtypes = [vp, C.c_int]
+    L.gwm_b200_set_tile.argtypes = [vp, C.c_int, C.c_int]
     L.gwm_b200_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double),
                                         C.POINTER(C.c_longlong), C.POINTER(C.c_char_p)]
     L.gwm_b200_launch_count.argtypes = [vp]
@@ -183,7 +184,7 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_synchronize", "gwm_b200_use_graph", "gwm_b200_upload", "gwm_b200_download",
             "gwm_b200_step", "gwm_b200_advance_dry", "gwm_b200_advance_tracers",
             "gwm_b200_warm_rain", "gwm_b200_fast_modes", "gwm_b200_slow_tendencies",
-            "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_layout",
+            "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_layout",
             "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_ranks_to_global",
             "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
 
@@ -421,6 +422,10 @@ class Model:
     @property
     def launch_count(self) -> int:
         return int(lib().gwm_b200_launch_count(self._h))
+
+    def set_tile(self, kernel: str, rows: int):
+        """CTA tile rows of a kernel ("fast_substep": 8 or 16)."""
+        self._check(lib().gwm_b200_set_tile(self._h, {"fast_substep": 1}[kernel], rows), "set_tile")
 
     def profile(self, enable: bool = True):
         """Per-kernel CUDA-event timing of subsequent direct (non-graph) launches."""

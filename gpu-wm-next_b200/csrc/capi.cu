@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -52,6 +53,8 @@ struct Member {
   float *zc = nullptr, *idc = nullptr, *idf = nullptr;
   double *precip = nullptr, *pcomp = nullptr;
   unsigned long long* acc = nullptr;
+  double* base = nullptr;            // FP64 base state of the perturbation EOS
+  bool base_valid = false;
   float* staging = nullptr;
   double* red_part = nullptr;
   ReduceOut* red_out = nullptr;
@@ -80,6 +83,7 @@ struct gwm_b200_ctx {
   bool use_graph = false;
   cudaGraphExec_t graph = nullptr;
   long long graph_launches = 0;
+  int fast_tile_rows = 8;  // acoustic-substep tile rows (tuned by gwm_b200_set_tile)
   long long launches = 0;
   long long cur_launches = 0;
 };
@@ -188,6 +192,8 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   g.per_y = d.periodic_y ? 1 : 0;
   g.dx = (float)d.dx;
   g.dy = (float)d.dy;
+  g.inv_dx = 1.0f / g.dx;
+  g.inv_dy = 1.0f / g.dy;
   M.field_elems = (size_t)g.plane * (g.nz + 1);
   const size_t fbytes = ((M.field_elems * sizeof(float) + 255) / 256) * 256;
   const bool moist = M.md.moist != 0;
@@ -197,7 +203,7 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   const size_t extra = ((2 * plane2 * sizeof(double) + 255) / 256) * 256 +
                        3 * kSlot * sizeof(unsigned long long) + owned_max * sizeof(float) +
                        3 * kReduceBlocks * sizeof(double) + 32 * sizeof(ReduceOut) + 4096 +
-                       3 * 4 * (kMaxNz + 1) * sizeof(float);
+                       3 * 4 * (kMaxNz + 1) * sizeof(float) + 3 * kMaxNz * sizeof(double) + 256;
   const size_t total = nfields * fbytes + extra;
   CK(cudaMalloc(&M.block, total));
   CK(cudaMemsetAsync(M.block, 0, total, c->stream));
@@ -216,6 +222,7 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   M.precip = (double*)take(plane2 * sizeof(double));
   M.pcomp = (double*)take(plane2 * sizeof(double));
   M.acc = (unsigned long long*)take(3 * kSlot * sizeof(unsigned long long));
+  M.base = (double*)take(3 * kMaxNz * sizeof(double));
   M.staging = (float*)take(owned_max * sizeof(float));
   M.red_part = (double*)take(3 * kReduceBlocks * sizeof(double));
   M.red_out = (ReduceOut*)take(32 * sizeof(ReduceOut));
@@ -287,6 +294,14 @@ void prof_end(gwm_b200_ctx* c, cudaEvent_t e0, const char* name) {
 
 double inv_count(const Member& M) { return 1.0 / ((double)M.g.nx * (double)M.g.ny); }
 
+// FP64 base state of the pressure-perturbation EOS from the current rho_theta
+int ensure_base(gwm_b200_ctx* c, Member& M) {
+  if (M.base_valid) return GWM_B200_OK;
+  LAUNCH(launch_base_state(M.g, M.Q[1], M.base, c->stream), "base state");
+  M.base_valid = true;
+  return GWM_B200_OK;
+}
+
 // theta level sums of the step state into slot(ring) (dry_core.cu:462-490)
 int enqueue_theta(gwm_b200_ctx* c, Member& M) {
   CK(cudaMemsetAsync(M.slot(M.ring), 0, kSlot * sizeof(unsigned long long), c->stream));
@@ -339,7 +354,7 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
     a.clr_a = M.slot(M.ring + 2); a.clr_b = M.slot(M.ring + 2) + kMaxNz;
     a.acc_mode = fast ? (terr ? 0 : 1) : ((s == 2 && rain_theta) ? 0 : 2);
     a.inv_count = inv_count(M);
-    a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf;
+    a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf; a.base = M.base;
     LAUNCH(launch_slow(a, terr, c->stream), "slow stage");
     M.ring = (M.ring + 1) % 3;
     rcur = rnext;
@@ -363,8 +378,8 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
       f.inv_count = inv_count(M);
       f.acc_a = M.slot(M.ring + 1); f.acc_b = M.slot(M.ring + 1) + kMaxNz;
       f.clr_a = M.slot(M.ring + 2); f.clr_b = M.slot(M.ring + 2) + kMaxNz;
-      f.zc = M.zc; f.idz_c = M.idc; f.idz_f = M.idf;
-      LAUNCH(launch_fast(f, n == 0, terr, c->stream), "fast substep");
+      f.zc = M.zc; f.idz_c = M.idc; f.idz_f = M.idf; f.base = M.base;
+      LAUNCH(launch_fast(f, n == 0, terr, c->stream, c->fast_tile_rows), "fast substep");
       M.ring = (M.ring + 1) % 3;
       rcur ^= 1;
       dcur = dout;
@@ -455,6 +470,7 @@ int gwm_b200_create(const gwm_b200_grid_desc* grids, const gwm_b200_member_desc*
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GWM_B200_ERR_NO_DEVICE;
   auto* c = new gwm_b200_ctx();
+  if (const char* t = std::getenv("GWM_B200_FAST_TILE_ROWS")) c->fast_tile_rows = std::atoi(t) == 16 ? 16 : 8;
   cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete c; return GWM_B200_ERR_CUDA; }
   c->stream = c->own_stream;
@@ -530,6 +546,13 @@ int gwm_b200_use_graph(gwm_b200_ctx* c, int enable) {
 
 long long gwm_b200_launch_count(const gwm_b200_ctx* c) { return c ? c->launches : -1; }
 
+int gwm_b200_set_tile(gwm_b200_ctx* c, int kernel, int rows) {
+  if (!c || kernel != 1 || (rows != 8 && rows != 16)) return GWM_B200_ERR_ARG;
+  drop_graph(c);
+  c->fast_tile_rows = rows;
+  return GWM_B200_OK;
+}
+
 int gwm_b200_upload(gwm_b200_ctx* c, int member, const gwm_b200_fields* h) {
   int rc = check_member(c, member);
   if (rc) return rc;
@@ -559,6 +582,7 @@ int gwm_b200_upload(gwm_b200_ctx* c, int member, const gwm_b200_fields* h) {
     CK(cudaMemsetAsync(M.pcomp, 0, n * sizeof(double), c->stream));
   }
   if (h->rho_d || h->rho_theta_m) M.theta_valid = false;
+  if (h->rho_theta_m) M.base_valid = false;
   CK(cudaStreamSynchronize(c->stream));
   return GWM_B200_OK;
 }
@@ -598,11 +622,14 @@ int gwm_b200_download(gwm_b200_ctx* c, int member, gwm_b200_fields* h) {
 
 static int run_steps(gwm_b200_ctx* c, int nsteps, int (*one)(gwm_b200_ctx*, Member&)) {
   c->cur_launches = 0;
-  for (auto& M : c->m)
+  for (auto& M : c->m) {
+    int rc = ensure_base(c, M);
+    if (rc) return rc;
     if (!M.theta_valid) {
-      int rc = enqueue_theta(c, M);
+      rc = enqueue_theta(c, M);
       if (rc) return rc;
     }
+  }
   if (c->use_graph && !c->profile && nsteps > 0 && one == enqueue_full_step) {
     if (!c->graph) {
       const long long before = c->cur_launches;
@@ -725,8 +752,10 @@ int gwm_b200_fast_modes(gwm_b200_ctx* c) {
     CK(cudaMemcpyAsync(M.R[0], M.Q[0], M.field_elems * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
     // rho and p level sums of the state (flat-terrain reference) into slot(ring)
     CK(cudaMemsetAsync(M.slot(M.ring), 0, kSlot * sizeof(unsigned long long), c->stream));
+    int rcb = ensure_base(c, M);
+    if (rcb) return rcb;
     LevelSumArgs ls{};
-    ls.g = M.g; ls.rho = M.Q[0]; ls.rt = M.Q[1]; ls.mode = 1;
+    ls.g = M.g; ls.rho = M.Q[0]; ls.rt = M.Q[1]; ls.mode = 1; ls.base = M.base;
     ls.acc_a = M.slot(M.ring); ls.acc_b = M.slot(M.ring) + kMaxNz;
     ls.clr_a = M.slot(M.ring + 1); ls.clr_b = M.slot(M.ring + 1) + kMaxNz;
     LAUNCH(launch_level_sums(ls, c->stream), "level sums");
@@ -748,8 +777,8 @@ int gwm_b200_fast_modes(gwm_b200_ctx* c) {
       f.inv_count = inv_count(M);
       f.acc_a = M.slot(M.ring + 1); f.acc_b = M.slot(M.ring + 1) + kMaxNz;
       f.clr_a = M.slot(M.ring + 2); f.clr_b = M.slot(M.ring + 2) + kMaxNz;
-      f.zc = M.zc; f.idz_c = M.idc; f.idz_f = M.idf;
-      LAUNCH(launch_fast(f, n == 0, terr, c->stream), "fast substep");
+      f.zc = M.zc; f.idz_c = M.idc; f.idz_f = M.idf; f.base = M.base;
+      LAUNCH(launch_fast(f, n == 0, terr, c->stream, c->fast_tile_rows), "fast substep");
       M.ring = (M.ring + 1) % 3;
       rcur ^= 1;
       dcur = dout;
@@ -765,6 +794,8 @@ int gwm_b200_slow_tendencies(gwm_b200_ctx* c, int member, gwm_b200_fields* h) {
   int rc = check_member(c, member);
   if (rc) return rc;
   Member& M = c->m[member];
+  rc = ensure_base(c, M);
+  if (rc) return rc;
   if (!M.theta_valid) {
     rc = enqueue_theta(c, M);
     if (rc) return rc;
@@ -779,7 +810,7 @@ int gwm_b200_slow_tendencies(gwm_b200_ctx* c, int member, gwm_b200_fields* h) {
   a.th_acc = M.slot(M.ring);
   a.acc_mode = 0;
   a.inv_count = inv_count(M);
-  a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf;
+  a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf; a.base = M.base;
   CK(launch_slow(a, M.terrain_active, c->stream));
   gwm_b200_fields tmp{};
   tmp.rho_d = h->rho_d; tmp.rho_theta_m = h->rho_theta_m;

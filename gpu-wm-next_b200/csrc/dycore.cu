@@ -20,6 +20,7 @@ constexpr int BY = 8;
 constexpr int NT = BX * BY;
 constexpr int NW = NT / 32;
 
+
 __device__ __forceinline__ float met3(const float* m, const Geom& g, int i, int j, int k) {
   return __ldg(m + gidx(g, i, j, k));
 }
@@ -57,6 +58,7 @@ __device__ __forceinline__ SlowRaw slow_raw(const SlowArgs& a, bool valid, int b
   return r;
 }
 
+template <bool TERRAIN>
 __device__ __forceinline__ SlowCol slow_derive(const SlowArgs& a, const SlowRaw& r, bool valid, int kk) {
   SlowCol c{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (!valid) return c;
@@ -64,7 +66,7 @@ __device__ __forceinline__ SlowCol slow_derive(const SlowArgs& a, const SlowRaw&
     c.rho = r.rho;
     c.rt = a.th_is_rt ? r.t : c.rho * r.t;
     c.th = theta_of(c.rho, c.rt);
-    c.p = eos_pressure(c.rho, c.rt);
+    c.p = TERRAIN ? eos_pressure(c.rho, c.rt) : eos_pprime(c.rho, c.rt, a.base, kk, a.g.nz);
     c.uf = r.u + r.du;
     c.vf = r.v + r.dv;
   }
@@ -111,7 +113,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
   const bool own_v = inner && gi >= 0 && gi < nx && gj >= 0 && gj <= ny;
   const bool open_x = !g.per_x, open_y = !g.per_y;
   const int base = valid ? gidx(g, gi, gj, 0) : 0;
-  const float dx = g.dx, dy = g.dy;
+  const float idx = g.inv_dx, idy = g.inv_dy;
 
   __shared__ float s_th[2][BY][BX], s_p[2][BY][BX], s_u[2][BY][BX], s_v[2][BY][BX], s_w[2][BY][BX];
   __shared__ float s_uc[2][BY][BX], s_vc[2][BY][BX], s_wc[2][BY][BX];
@@ -130,7 +132,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
   const SlowRaw r1 = slow_raw<TERRAIN>(a, valid, base, 1);
   SlowRaw r2 = slow_raw<TERRAIN>(a, valid, base, 2);
   SlowQ0 q0c = slow_q0(a, base, 0, own_c, own_u, own_v);
-  SlowCol cm{}, cc = slow_derive(a, r0, valid, 0), cn = slow_derive(a, r1, valid, 1);
+  SlowCol cm{}, cc = slow_derive<TERRAIN>(a, r0, valid, 0), cn = slow_derive<TERRAIN>(a, r1, valid, 1);
   float zm = 0.f, zcc = r0.z, zn = r1.z;
   const bool blend = a.rho0 != nullptr;
 
@@ -172,7 +174,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
         const float fw = cc.uf, fe = s_u[pb][ty][tx + 1], fs = cc.vf, fn = s_v[pb][ty + 1][tx];
         const float fb = cc.wf, ft = cn.wf;
         const float idz = TERRAIN ? met3(a.idz_c, g, gi, gj, k) : __ldg(a.idz_c + k);
-        const float div = (fe - fw) / dx + (fn - fs) / dy + (ft - fb) * idz;
+        const float div = (fe - fw) * idx + (fn - fs) * idy + (ft - fb) * idz;
         const float t_rho = -div;
         const float tc = cc.th;
         const float tw = s_th[pb][ty][tx - 1], te = s_th[pb][ty][tx + 1];
@@ -185,7 +187,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
         const float gn = fn * (fn >= 0.0f ? tc : tn);
         const float gb = fb * (fb >= 0.0f ? tb : tc);
         const float gt = ft * (ft >= 0.0f ? tc : tt);
-        const float t_rt = -((ge - gw) / dx + (gn - gs) / dy + (gt - gb) * idz);
+        const float t_rt = -((ge - gw) * idx + (gn - gs) * idy + (gt - gb) * idz);
         if (a.tend_only) {
           a.o_rho[o] = t_rho;
           a.o_th[o] = t_rt;
@@ -202,7 +204,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
           store_mirrored(a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1);
           if (a.acc_mode == 1) {
             red_a = r1;
-            red_b = eos_pressure(r1, r1 * th1);
+            red_b = eos_pprime(r1, r1 * th1, a.base, k, nz);
           } else if (a.acc_mode == 2) {
             red_a = th1;
           }
@@ -225,14 +227,14 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
           if (k + 1 < nz) flt = upwind(0.5f * (s_wc[pb][ty][tx - 1] + s_wc[pb][ty][tx]), qc, qt);
           const float idz = TERRAIN ? 0.5f * (met3(a.idz_c, g, gi - 1, gj, k) + met3(a.idz_c, g, gi, gj, k))
                                     : __ldg(a.idz_c + k);
-          t_u = -((fle - flw) / dx + (fln - fls) / dy + (flt - flb) * idz);
+          t_u = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
           const float pl = s_p[pb][ty][tx - 1], pr = cc.p;
           if (TERRAIN) {
-            const float dzdx = (s_zc[pb][ty][tx] - s_zc[pb][ty][tx - 1]) / dx;
+            const float dzdx = (s_zc[pb][ty][tx] - s_zc[pb][ty][tx - 1]) * idx;
             const float dpdz = 0.5f * (s_dz[pb][ty][tx - 1] + s_dz[pb][ty][tx]);
-            t_u += -((pr - pl) / dx - dzdx * dpdz);
+            t_u += -((pr - pl) * idx - dzdx * dpdz);
           } else {
-            t_u += -((pr - pl) / dx);
+            t_u += -((pr - pl) * idx);
           }
         }
         if (a.tend_only) {
@@ -260,14 +262,14 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
           if (k + 1 < nz) flt = upwind(0.5f * (s_wc[pb][ty - 1][tx] + s_wc[pb][ty][tx]), qc, qt);
           const float idz = TERRAIN ? 0.5f * (met3(a.idz_c, g, gi, gj - 1, k) + met3(a.idz_c, g, gi, gj, k))
                                     : __ldg(a.idz_c + k);
-          t_v = -((fle - flw) / dx + (fln - fls) / dy + (flt - flb) * idz);
+          t_v = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
           const float ps = s_p[pb][ty - 1][tx], pn = cc.p;
           if (TERRAIN) {
-            const float dzdy = (s_zc[pb][ty][tx] - s_zc[pb][ty - 1][tx]) / dy;
+            const float dzdy = (s_zc[pb][ty][tx] - s_zc[pb][ty - 1][tx]) * idy;
             const float dpdz = 0.5f * (s_dz[pb][ty - 1][tx] + s_dz[pb][ty][tx]);
-            t_v += -((pn - ps) / dy - dzdy * dpdz);
+            t_v += -((pn - ps) * idy - dzdy * dpdz);
           } else {
-            t_v += -((pn - ps) / dy);
+            t_v += -((pn - ps) * idy);
           }
         }
         if (a.tend_only) {
@@ -293,7 +295,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
           const float flb = upwind(s_wc[pb ^ 1][ty][tx], qb, qc);
           const float flt = upwind(s_wc[pb][ty][tx], qc, qt);
           const float idz = TERRAIN ? met3(a.idz_f, g, gi, gj, k) : __ldg(a.idz_f + k);
-          t_w = -((fle - flw) / dx + (fln - fls) / dy + (flt - flb) * idz);
+          t_w = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
           const float tl = cm.th, tu = cc.th;
           const float tf = 0.5f * (tl + tu);
           const float trf = 0.5f * (s_thref[k - 1] + s_thref[k]);
@@ -324,7 +326,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
     // advance the column window
     cm = cc;
     cc = cn;
-    cn = slow_derive(a, r2, valid, k + 2);
+    cn = slow_derive<TERRAIN>(a, r2, valid, k + 2);
     zm = zcc;
     zcc = zn;
     zn = r2.z;
@@ -377,7 +379,8 @@ __device__ __forceinline__ FastCol fast_derive(const FastArgs& a, const FastRaw&
   c.th = r.th;
   const float rt = c.rho * c.th;  // K10 rebuild_rho_theta_from_theta_kernel
   c.thp = theta_of(c.rho, rt);
-  c.p = eos_pressure(c.rho, rt);  // K20
+  // K20: full pressure for the terrain column reference, perturbation otherwise
+  c.p = TERRAIN ? eos_pressure(c.rho, rt) : eos_pprime(c.rho, rt, a.base, kk, a.g.nz);
   if (TERRAIN) {  // K11 build_column_hydrostatic_reference_kernel (dry_fast_modes.cu:108-158)
     if (kk == 0) {
       c.pref = c.p;
@@ -408,34 +411,36 @@ __device__ __forceinline__ FastInc fast_inc(const FastArgs& a, int base, int kk,
   return d;
 }
 
-template <bool TERRAIN, bool FIRST>
-__global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
+template <bool TERRAIN, bool FIRST, int FBY>
+__global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
+  constexpr int FNT = BX * FBY;
+  constexpr int FNW = FNT / 32;
   const Geom& g = a.g;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
   const int gi = blockIdx.x * (BX - 2) - 1 + tx;
-  const int gj = blockIdx.y * (BY - 2) - 1 + ty;
+  const int gj = blockIdx.y * (FBY - 2) - 1 + ty;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const bool valid = gi >= -1 && gi <= nx + 1 && gj >= -1 && gj <= ny + 1;
-  const bool inner = tx >= 1 && tx <= BX - 2 && ty >= 1 && ty <= BY - 2;
+  const bool inner = tx >= 1 && tx <= BX - 2 && ty >= 1 && ty <= FBY - 2;
   const bool own_c = inner && gi >= 0 && gi < nx && gj >= 0 && gj < ny;
   // faces computed by this thread (owned or the tile's far-edge duplicate)
-  const bool do_u = tx >= 1 && ty >= 1 && ty <= BY - 2 && gi >= 0 && gi <= nx && gj >= 0 && gj < ny;
+  const bool do_u = tx >= 1 && ty >= 1 && ty <= FBY - 2 && gi >= 0 && gi <= nx && gj >= 0 && gj < ny;
   const bool do_v = ty >= 1 && tx >= 1 && tx <= BX - 2 && gi >= 0 && gi < nx && gj >= 0 && gj <= ny;
   const bool own_u = do_u && tx <= BX - 2;
-  const bool own_v = do_v && ty <= BY - 2;
+  const bool own_v = do_v && ty <= FBY - 2;
   const bool skip_u = (gi == 0 || gi == nx) && !g.per_x;
   const bool skip_v = (gj == 0 || gj == ny) && !g.per_y;
   const int base = valid ? gidx(g, gi, gj, 0) : 0;
-  const float dx = g.dx, dy = g.dy, dtf = a.dtf;
+  const float idx = g.inv_dx, idy = g.inv_dy, dtf = a.dtf;
   const bool final_step = a.final_kind == 2;
 
-  __shared__ float s_p[2][BY][BX], s_du[2][BY][BX], s_dv[2][BY][BX];
-  __shared__ float s_zc[TERRAIN ? 2 : 1][BY][BX], s_dz[TERRAIN ? 2 : 1][BY][BX];
+  __shared__ float s_p[2][FBY][BX], s_du[2][FBY][BX], s_dv[2][FBY][BX];
+  __shared__ float s_zc[TERRAIN ? 2 : 1][FBY][BX], s_dz[TERRAIN ? 2 : 1][FBY][BX];
   __shared__ float s_pref[TERRAIN ? 1 : kMaxNz], s_rref[TERRAIN ? 1 : kMaxNz];
-  __shared__ double s_red[2][NW][2];
+  __shared__ double s_red[2][FNW][2];
 
   if (blockIdx.x == 0 && blockIdx.y == 0 && a.clr_a) {
-    for (int q = tid; q < nz; q += NT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
+    for (int q = tid; q < nz; q += FNT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
   }
   // software pipeline: plane fields two planes ahead, increments one plane ahead
   FastRaw r0 = fast_raw<TERRAIN>(a, valid, base, 0, gi, gj);
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
   FastRaw r2 = fast_raw<TERRAIN>(a, valid, base, 2, gi, gj);
   FastInc d0 = fast_inc<FIRST>(a, base, 0, do_u, do_v, own_c);
   if (!TERRAIN) {  // K6/K7 level means (deterministic sums instead of float atomics)
-    for (int q = tid; q < nz; q += NT) {
+    for (int q = tid; q < nz; q += FNT) {
       s_rref[q] = (float)(acc_read(a.ref_a + q, kScaleRho) * a.inv_count);
       s_pref[q] = (float)(acc_read(a.ref_b + q, kScaleP) * a.inv_count);
     }
@@ -482,7 +487,7 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
     __syncthreads();
     if (acc_mode && k > 0 && tid == 0) {
       double sa = 0.0, sb = 0.0;
-      for (int w = 0; w < NW; ++w) { sa += s_red[pb ^ 1][w][0]; sb += s_red[pb ^ 1][w][1]; }
+      for (int w = 0; w < FNW; ++w) { sa += s_red[pb ^ 1][w][0]; sb += s_red[pb ^ 1][w][1]; }
       if (acc_mode == 1) { acc_add(a.acc_a + k - 1, sa, kScaleRho); acc_add(a.acc_b + k - 1, sb, kScaleP); }
       else acc_add(a.acc_a + k - 1, sa, kScaleTheta);
     }
@@ -492,11 +497,11 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
       const float pl = s_p[pb][ty][tx - 1], pr = cc.p;
       float x;
       if (TERRAIN) {
-        const float dzdx = (s_zc[pb][ty][tx] - s_zc[pb][ty][tx - 1]) / dx;
+        const float dzdx = (s_zc[pb][ty][tx] - s_zc[pb][ty][tx - 1]) * idx;
         const float dpdz = 0.5f * (s_dz[pb][ty][tx - 1] + s_dz[pb][ty][tx]);
-        x = (pr - pl) / dx - dzdx * dpdz;
+        x = (pr - pl) * idx - dzdx * dpdz;
       } else {
-        x = (pr - pl) / dx;
+        x = (pr - pl) * idx;
       }
       du_new = d0.du + (-dtf * x);
     }
@@ -507,11 +512,11 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
       const float ps = s_p[pb][ty - 1][tx], pn = cc.p;
       float x;
       if (TERRAIN) {
-        const float dzdy = (s_zc[pb][ty][tx] - s_zc[pb][ty - 1][tx]) / dy;
+        const float dzdy = (s_zc[pb][ty][tx] - s_zc[pb][ty - 1][tx]) * idy;
         const float dpdz = 0.5f * (s_dz[pb][ty - 1][tx] + s_dz[pb][ty][tx]);
-        x = (pn - ps) / dy - dzdy * dpdz;
+        x = (pn - ps) * idy - dzdy * dpdz;
       } else {
-        x = (pn - ps) / dy;
+        x = (pn - ps) * idy;
       }
       dv_new = d0.dv + (-dtf * x);
     }
@@ -533,8 +538,8 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
       // K15: density from the perturbation mass-flux divergence (dry_fast_modes.cu:350-394)
       float rho_new = cc.rho;
       if (a.dens) {
-        const float div = (s_du[pb][ty][tx + 1] - s_du[pb][ty][tx]) / dx +
-                          (s_dv[pb][ty + 1][tx] - s_dv[pb][ty][tx]) / dy + (dw_n - dw_c) * idzc;
+        const float div = (s_du[pb][ty][tx + 1] - s_du[pb][ty][tx]) * idx +
+                          (s_dv[pb][ty + 1][tx] - s_dv[pb][ty][tx]) * idy + (dw_n - dw_c) * idzc;
         rho_new = fmaxf(1.0e-6f, cc.rho - dtf * div);
       }
       const float rt_new = rho_new * cc.th;  // K10 on the state
@@ -549,7 +554,7 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
       }
       if (acc_mode == 1) {
         red_a = rho_new;
-        red_b = eos_pressure(rho_new, rt_new);
+        red_b = eos_pprime(rho_new, rt_new, a.base, k, nz);
       } else if (acc_mode == 2) {
         red_a = theta_of(rho_new, rt_new);
       }
@@ -583,7 +588,7 @@ __global__ void __launch_bounds__(NT) k_fast_substep(const FastArgs a) {
     if (tid == 0) {
       const int pb = (nz - 1) & 1;
       double sa = 0.0, sb = 0.0;
-      for (int w = 0; w < NW; ++w) { sa += s_red[pb][w][0]; sb += s_red[pb][w][1]; }
+      for (int w = 0; w < FNW; ++w) { sa += s_red[pb][w][0]; sb += s_red[pb][w][1]; }
       if (acc_mode == 1) { acc_add(a.acc_a + nz - 1, sa, kScaleRho); acc_add(a.acc_b + nz - 1, sb, kScaleP); }
       else acc_add(a.acc_a + nz - 1, sa, kScaleTheta);
     }
@@ -608,7 +613,7 @@ __global__ void __launch_bounds__(256) k_level_sums(const LevelSumArgs a) {
     } else {
       const float rtf = rho * theta_of(rho, rt);
       va += (double)rho;
-      vb += (double)eos_pressure(rho, rtf);
+      vb += (double)eos_pprime(rho, rtf, a.base, k, g.nz);
     }
   }
   va = warp_sum(va);
@@ -620,6 +625,30 @@ __global__ void __launch_bounds__(256) k_level_sums(const LevelSumArgs a) {
     for (int w = 0; w < 8; ++w) { ta += s[w][0]; tb += s[w][1]; }
     if (a.mode == 0) acc_add(a.acc_a + k, ta, kScaleTheta);
     else { acc_add(a.acc_a + k, ta, kScaleRho); acc_add(a.acc_b + k, tb, kScaleP); }
+  }
+}
+
+// Per-level mean of rho_theta (FP64, fixed order) and the EOS of that mean.
+__global__ void __launch_bounds__(256) k_base_state(const Geom g, const float* rt, double* base) {
+  const int k = blockIdx.x;
+  __shared__ double sh[8];
+  double v = 0.0;
+  const int n = g.nx * g.ny;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const int i = q % g.nx, j = q / g.nx;
+    v += (double)rt[gidx(g, i, j, k)];
+  }
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += sh[w];
+    const double rt_ref = t / (double)n;
+    const double gamma = (double)(1.0f / (1.0f - kKappa));
+    base[k] = rt_ref;
+    base[g.nz + k] = 1.0 / rt_ref;
+    base[2 * g.nz + k] = (double)kP0 * pow((double)kRd * rt_ref / (double)kP0, gamma);
   }
 }
 
@@ -646,24 +675,35 @@ cudaError_t launch_slow(const SlowArgs& a, bool terrain, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_t s) {
-  if (a.g.nz > kMaxNz) return cudaErrorInvalidValue;
-  const dim3 block(BX, BY);
-  const dim3 grid((a.g.nx + 1 + BX - 3) / (BX - 2), (a.g.ny + 1 + BY - 3) / (BY - 2));
+template <int FBY>
+cudaError_t launch_fast_tile(const FastArgs& a, bool first, bool terrain, cudaStream_t s) {
+  const dim3 block(BX, FBY);
+  const dim3 grid((a.g.nx + 1 + BX - 3) / (BX - 2), (a.g.ny + 1 + FBY - 3) / (FBY - 2));
   if (terrain) {
-    if (first) k_fast_substep<true, true><<<grid, block, 0, s>>>(a);
-    else k_fast_substep<true, false><<<grid, block, 0, s>>>(a);
+    if (first) k_fast_substep<true, true, FBY><<<grid, block, 0, s>>>(a);
+    else k_fast_substep<true, false, FBY><<<grid, block, 0, s>>>(a);
   } else {
-    if (first) k_fast_substep<false, true><<<grid, block, 0, s>>>(a);
-    else k_fast_substep<false, false><<<grid, block, 0, s>>>(a);
+    if (first) k_fast_substep<false, true, FBY><<<grid, block, 0, s>>>(a);
+    else k_fast_substep<false, false, FBY><<<grid, block, 0, s>>>(a);
   }
   return cudaGetLastError();
+}
+
+cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_t s, int tile_rows) {
+  if (a.g.nz > kMaxNz) return cudaErrorInvalidValue;
+  if (tile_rows == 16) return launch_fast_tile<16>(a, first, terrain, s);
+  return launch_fast_tile<8>(a, first, terrain, s);
 }
 
 cudaError_t launch_level_sums(const LevelSumArgs& a, cudaStream_t s) {
   const int n = a.g.nx * a.g.ny;
   const int bx = (n + 255) / 256 < 64 ? (n + 255) / 256 : 64;
   k_level_sums<<<dim3(bx, a.g.nz), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_base_state(const Geom& g, const float* rt, double* base, cudaStream_t s) {
+  k_base_state<<<g.nz, 256, 0, s>>>(g, rt, base);
   return cudaGetLastError();
 }
 

@@ -31,6 +31,7 @@ struct SlowArgs {
   int acc_mode;                     // 0 none, 1 rho & p of output, 2 theta of output
   double inv_count;                 // 1 / (nx*ny)
   const float *zc, *idz_c, *idz_f;  // metrics: padded 3-D (terrain) or per level (flat)
+  const double* base;               // FP64 base state [rt_ref | 1/rt_ref | p_ref] per level
 };
 
 // Arguments of one acoustic substep: src/dycore/dry_fast_modes.cu:495-652
@@ -52,6 +53,7 @@ struct FastArgs {
   double inv_count;
   unsigned long long *acc_a, *acc_b, *clr_a, *clr_b;
   const float *zc, *idz_c, *idz_f;
+  const double* base;
 };
 
 // Level sums of a stored state.  mode 0: theta = rt/max(rho,1e-6) (the host loop of
@@ -61,11 +63,16 @@ struct LevelSumArgs {
   const float *rho, *rt;
   int mode;
   unsigned long long *acc_a, *acc_b, *clr_a, *clr_b;
+  const double* base;
 };
 
 cudaError_t launch_slow(const SlowArgs& a, bool terrain, cudaStream_t s);
-cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_t s);
+// tile_rows: CTA rows of the acoustic-substep tile (8 or 16; 32 columns wide).
+cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_t s, int tile_rows);
 cudaError_t launch_level_sums(const LevelSumArgs& a, cudaStream_t s);
+// FP64 base state of the pressure-perturbation EOS: per level the mean rho_theta of
+// the state, its reciprocal and p_ref = EOS(mean rho_theta); one CTA per level.
+cudaError_t launch_base_state(const Geom& g, const float* rt, double* base, cudaStream_t s);
 // theta = rt/max(rho,1e-6) on owned cells with periodic halo mirroring
 // (compute_theta_field_kernel + exchange_scalar, dry_fast_modes.cu:86-95, 453-462).
 cudaError_t launch_theta_field(const Geom& g, const float* rho, const float* rt, float* th,

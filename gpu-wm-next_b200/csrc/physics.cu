@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(NT) k_tracer_stage(const TracerArgs a) {
   const bool inner = tx >= 1 && tx <= BX - 2 && ty >= 1 && ty <= BY - 2;
   const bool own_c = inner && gi >= 0 && gi < nx && gj >= 0 && gj < ny;
   const int base = valid ? gidx(g, gi, gj, 0) : 0;
-  const float dx = g.dx, dy = g.dy;
+  const float idx = g.inv_dx, idy = g.inv_dy;
   const bool blend = a.q0[0] != nullptr;
 
   __shared__ float s_q[NTR][2][BY][BX];
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(NT) k_tracer_stage(const TracerArgs a) {
         const float gn = fn * (fn >= 0.0f ? qc : qn);
         const float gb = fb * (fb >= 0.0f ? qb : qc);
         const float gt = ft * (ft >= 0.0f ? qc : qt);
-        const float div = (ge - gw) / dx + (gn - gs) / dy + (gt - gb) * idz;
+        const float div = (ge - gw) * idx + (gn - gs) * idy + (gt - gb) * idz;
         float out = fmaxf(0.0f, cc.rq[t] - a.dt * div);
         if (blend) out = a.wa * q0v[t] + a.wb * out;
         store_mirrored(a.q_out[t], g, kCell, gi, gj, k, out);
