@@ -83,7 +83,7 @@ struct gwm_b200_ctx {
   bool use_graph = false;
   cudaGraphExec_t graph = nullptr;
   long long graph_launches = 0;
-  int fast_tile_rows = 8;  // acoustic-substep tile rows (tuned by gwm_b200_set_tile)
+  int fast_tile_rows = 0;  // acoustic substep: 0 owned-tile flat kernel, 8/16 overlapped tiles
   long long launches = 0;
   long long cur_launches = 0;
 };
@@ -470,7 +470,7 @@ int gwm_b200_create(const gwm_b200_grid_desc* grids, const gwm_b200_member_desc*
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GWM_B200_ERR_NO_DEVICE;
   auto* c = new gwm_b200_ctx();
-  if (const char* t = std::getenv("GWM_B200_FAST_TILE_ROWS")) c->fast_tile_rows = std::atoi(t) == 16 ? 16 : 8;
+  if (const char* t = std::getenv("GWM_B200_FAST_TILE_ROWS")) { const int r = std::atoi(t); c->fast_tile_rows = (r == 8 || r == 16) ? r : 0; }
   cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete c; return GWM_B200_ERR_CUDA; }
   c->stream = c->own_stream;
@@ -547,7 +547,7 @@ int gwm_b200_use_graph(gwm_b200_ctx* c, int enable) {
 long long gwm_b200_launch_count(const gwm_b200_ctx* c) { return c ? c->launches : -1; }
 
 int gwm_b200_set_tile(gwm_b200_ctx* c, int kernel, int rows) {
-  if (!c || kernel != 1 || (rows != 8 && rows != 16)) return GWM_B200_ERR_ARG;
+  if (!c || kernel != 1 || (rows != 0 && rows != 8 && rows != 16)) return GWM_B200_ERR_ARG;
   drop_graph(c);
   c->fast_tile_rows = rows;
   return GWM_B200_OK;

@@ -103,15 +103,17 @@ __device__ __forceinline__ float upwind(float a, float ql, float qr) {
 // alias under periodic wrap and are computed identically); face 1 feeds halo
 // face nx+1 and face nx-1 feeds halo face -1.  Open axes leave halos at zero.
 // Mirrors are shifts by +-nx columns and +-ny rows: cell 0 -> nx, cell nx-1 -> -1,
-// X face 1 -> nx+1, X face nx-1 -> -1 (same in y).  Interior positions take one
-// store and a predicated exit; only the edge ring takes the extra stores.
+// X face 0 -> nx (its periodic alias), X face 1 -> nx+1, X face nx-1 -> -1 (same
+// in y).  Interior positions take one store and a predicated exit; only the edge
+// ring takes the extra stores.
 __device__ __forceinline__ void store_mirrored(float* __restrict__ f, const Geom& g, int o, int i,
                                                int j, int k, float v) {
   const int at = gidx(g, i, j, k);
   f[at] = v;
-  const int lox = (o == kFaceX) ? 1 : 0, loy = (o == kFaceY) ? 1 : 0;
-  const bool xh = g.per_x && i == lox, xl = g.per_x && i == g.nx - 1;
-  const bool yh = g.per_y && j == loy, yl = g.per_y && j == g.ny - 1;
+  const bool xh = g.per_x && (i == 0 || (o == kFaceX && i == 1));
+  const bool xl = g.per_x && i == g.nx - 1;
+  const bool yh = g.per_y && (j == 0 || (o == kFaceY && j == 1));
+  const bool yl = g.per_y && j == g.ny - 1;
   if (!(xh || xl || yh || yl)) return;
   const int sx = g.nx, sy = g.ny * g.pitch;
   if (xh) f[at + sx] = v;

@@ -628,6 +628,251 @@ __global__ void __launch_bounds__(256) k_level_sums(const LevelSumArgs a) {
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Acoustic substep, flat terrain.  Owned tile of 32 x 16 columns per CTA of
+// 32 x 8 threads, two columns per thread (rows ty and ty+8) for instruction-level
+// parallelism.  The pressure perturbation at the 96 halo cells the tile needs
+// (west/east columns, south/north rows; no corners) is derived by 96 threads,
+// which also compute the tile's east X faces and north Y faces.  No CTA covers
+// X face nx or Y face ny: under periodic wrap they are written as the mirror of
+// face 0, on open boundaries they never change.
+namespace flat {
+constexpr int TX = 32, TY = 16, RY = 8, NT = 256, NW = NT / 32;
+
+struct Cell {
+  float rho, th, p;  // density, frozen theta, pressure perturbation
+};
+
+__device__ __forceinline__ Cell derive(const FastArgs& a, float rho, float th, int k) {
+  Cell c;
+  c.rho = rho;
+  c.th = th;
+  c.p = eos_pprime(rho, rho * th, a.base, k, a.g.nz);  // K10 + K20
+  return c;
+}
+}  // namespace flat
+
+template <bool FIRST>
+__global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
+  using flat::TX; using flat::TY; using flat::RY; using flat::Cell; using flat::derive;
+  constexpr int FT = flat::NT, FW = flat::NW;
+  const Geom& g = a.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int w = min(TX, nx - i0), h = min(TY, ny - j0);
+  const bool own0 = tx < w && ty < h, own1 = tx < w && ty + RY < h;
+  const int gi = i0 + tx, gj0 = j0 + ty, gj1 = j0 + ty + RY;
+  const int b0 = own0 ? gidx(g, gi, gj0, 0) : 0, b1 = own1 ? gidx(g, gi, gj1, 0) : 0;
+  const bool skip_u = gi == 0 && !g.per_x;         // open west face (never changes)
+  const bool skip_v0 = gj0 == 0 && !g.per_y;
+  // halo role: 0 west column, 1 east column, 2 south row, 3 north row
+  int role = -1, hi = 0, hj = 0;
+  if (tid < TY) { if (tid < h) { role = 0; hi = i0 - 1; hj = j0 + tid; } }
+  else if (tid < 2 * TY) { if (tid - TY < h) { role = 1; hi = i0 + w; hj = j0 + tid - TY; } }
+  else if (tid < 2 * TY + TX) { if (tid - 2 * TY < w) { role = 2; hi = i0 + tid - 2 * TY; hj = j0 - 1; } }
+  else if (tid < 2 * TY + 2 * TX) { if (tid - 2 * TY - TX < w) { role = 3; hi = i0 + tid - 2 * TY - TX; hj = j0 + h; } }
+  const int hb = role >= 0 ? gidx(g, hi, hj, 0) : 0;
+  const int hr = hj - j0 + 1, hc = hi - i0 + 1;    // smem coordinates of the halo cell
+  const bool h_skip = (role == 1 && hi == nx && !g.per_x) || (role == 3 && hj == ny && !g.per_y);
+  const float idx = g.inv_dx, idy = g.inv_dy, dtf = a.dtf;
+  const bool final_step = a.final_kind == 2;
+  const int acc_mode = a.acc_off ? 0 : (a.final_kind == 0 ? 1 : 2);
+  const int P = g.plane;
+
+  __shared__ float s_p[2][TY + 2][TX + 2];
+  __shared__ float s_du[2][TY][TX + 1];
+  __shared__ float s_dv[2][TY + 1][TX];
+  __shared__ float s_pref[kMaxNz], s_rref[kMaxNz];
+  __shared__ double s_red[2][FW][2];
+
+  if (blockIdx.x == 0 && blockIdx.y == 0 && a.clr_a)
+    for (int q = tid; q < nz; q += FT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
+  // K6/K7: level means of rho and p' (deterministic sums instead of float atomics)
+  for (int q = tid; q < nz; q += FT) {
+    s_rref[q] = (float)(acc_read(a.ref_a + q, kScaleRho) * a.inv_count);
+    s_pref[q] = (float)(acc_read(a.ref_b + q, kScaleP) * a.inv_count);
+  }
+
+  // pipeline: own cells two planes ahead, increments and halo one plane ahead
+  auto ld2 = [&](int b, bool own, int kk, float& r, float& t) {
+    r = 0.f; t = 0.f;
+    if (own && kk < nz) { r = __ldg(a.rho_in + b + kk * P); t = __ldg(a.th + b + kk * P); }
+  };
+  float ra0, ta0, ra1, ta1;  // raw plane k+2
+  ld2(b0, own0, 0, ra0, ta0);
+  ld2(b1, own1, 0, ra1, ta1);
+  Cell c0 = derive(a, ra0, ta0, 0), c1 = derive(a, ra1, ta1, 0);
+  ld2(b0, own0, 1, ra0, ta0);
+  ld2(b1, own1, 1, ra1, ta1);
+  Cell n0 = derive(a, ra0, ta0, 1), n1 = derive(a, ra1, ta1, 1);
+  ld2(b0, own0, 2, ra0, ta0);
+  ld2(b1, own1, 2, ra1, ta1);
+  // increments of plane k: du, dv at own faces, dw at face k+1
+  float du0 = 0.f, dv0 = 0.f, dw0 = 0.f, du1 = 0.f, dv1 = 0.f, dw1 = 0.f;
+  if (!FIRST) {
+    if (own0) { du0 = __ldg(a.du_in + b0); dv0 = __ldg(a.dv_in + b0); if (nz > 1) dw0 = __ldg(a.dw_in + b0 + P); }
+    if (own1) { du1 = __ldg(a.du_in + b1); dv1 = __ldg(a.dv_in + b1); if (nz > 1) dw1 = __ldg(a.dw_in + b1 + P); }
+  }
+  // halo: p' of plane k and the edge-face increment of plane k
+  float hp = 0.f, hd = 0.f;
+  if (role >= 0) {
+    hp = eos_pprime(__ldg(a.rho_in + hb), __ldg(a.rho_in + hb) * __ldg(a.th + hb), a.base, 0, nz);
+    if (!FIRST && role == 1) hd = __ldg(a.du_in + hb);
+    if (!FIRST && role == 3) hd = __ldg(a.dv_in + hb);
+  }
+  float dwc0 = 0.f, dwc1 = 0.f;  // increment at face k (face 0 never changes)
+  __syncthreads();
+
+  for (int k = 0; k < nz; ++k) {
+    const int pb = k & 1;
+    // ---- issue the loads of later planes
+    float nr0, nt0, nr1, nt1;
+    ld2(b0, own0, k + 3, nr0, nt0);
+    ld2(b1, own1, k + 3, nr1, nt1);
+    float ndu0 = 0.f, ndv0 = 0.f, ndw0 = 0.f, ndu1 = 0.f, ndv1 = 0.f, ndw1 = 0.f;
+    if (!FIRST && k + 1 < nz) {
+      const int o = (k + 1) * P;
+      if (own0) { ndu0 = __ldg(a.du_in + b0 + o); ndv0 = __ldg(a.dv_in + b0 + o); if (k + 2 < nz) ndw0 = __ldg(a.dw_in + b0 + o + P); }
+      if (own1) { ndu1 = __ldg(a.du_in + b1 + o); ndv1 = __ldg(a.dv_in + b1 + o); if (k + 2 < nz) ndw1 = __ldg(a.dw_in + b1 + o + P); }
+    }
+    float hrho = 0.f, hth = 0.f, hdn = 0.f;
+    if (role >= 0 && k + 1 < nz) {
+      const int o = hb + (k + 1) * P;
+      hrho = __ldg(a.rho_in + o);
+      hth = __ldg(a.th + o);
+      if (!FIRST && role == 1) hdn = __ldg(a.du_in + o);
+      if (!FIRST && role == 3) hdn = __ldg(a.dv_in + o);
+    }
+    float bu0 = 0.f, bv0 = 0.f, bw0 = 0.f, bu1 = 0.f, bv1 = 0.f, bw1 = 0.f, bwz0 = 0.f, bwz1 = 0.f;
+    if (final_step) {
+      const int o = k * P;
+      if (own0) { bu0 = __ldg(a.bu + b0 + o); bv0 = __ldg(a.bv + b0 + o); bw0 = __ldg(a.bw + b0 + o + P); if (k == 0) bwz0 = __ldg(a.bw + b0); }
+      if (own1) { bu1 = __ldg(a.bu + b1 + o); bv1 = __ldg(a.bv + b1 + o); bw1 = __ldg(a.bw + b1 + o + P); if (k == 0) bwz1 = __ldg(a.bw + b1); }
+    }
+    const float idzc = __ldg(a.idz_c + k);
+    const float idzf = (k + 1 < nz) ? __ldg(a.idz_f + k + 1) : 0.f;
+    // ---- plane k pressure perturbation into shared memory
+    // only owners write tile slots: on partial edge tiles the slot next to the last
+    // owned column/row belongs to a halo thread
+    if (own0) s_p[pb][ty + 1][tx + 1] = c0.p;
+    if (own1) s_p[pb][ty + RY + 1][tx + 1] = c1.p;
+    if (role >= 0) s_p[pb][hr][hc] = hp;
+    __syncthreads();
+    if (acc_mode && k > 0 && tid == 0) {
+      double sa = 0.0, sb = 0.0;
+      for (int q = 0; q < FW; ++q) { sa += s_red[pb ^ 1][q][0]; sb += s_red[pb ^ 1][q][1]; }
+      if (acc_mode == 1) { acc_add(a.acc_a + k - 1, sa, kScaleRho); acc_add(a.acc_b + k - 1, sb, kScaleP); }
+      else acc_add(a.acc_a + k - 1, sa, kScaleTheta);
+    }
+    // ---- K12/K13 horizontal momenta, K14 vertical momentum at face k+1
+    const bool hm = a.hmom != 0;
+    float un0 = du0, vn0 = dv0, un1 = du1, vn1 = dv1;
+    if (hm) {
+      if (!skip_u) {
+        un0 = du0 + (-dtf * ((c0.p - s_p[pb][ty + 1][tx]) * idx));
+        un1 = du1 + (-dtf * ((c1.p - s_p[pb][ty + RY + 1][tx]) * idx));
+      }
+      if (!skip_v0) vn0 = dv0 + (-dtf * ((c0.p - s_p[pb][ty][tx + 1]) * idy));
+      vn1 = dv1 + (-dtf * ((c1.p - s_p[pb][ty + RY][tx + 1]) * idy));
+    }
+    if (own0) { s_du[pb][ty][tx] = un0; s_dv[pb][ty][tx] = vn0; }
+    if (own1) { s_du[pb][ty + RY][tx] = un1; s_dv[pb][ty + RY][tx] = vn1; }
+    if (role == 1) {  // tile's east X face
+      float d = hd;
+      if (hm && !h_skip) d = hd + (-dtf * ((hp - s_p[pb][hr][hc - 1]) * idx));
+      s_du[pb][hr - 1][hc - 1] = d;
+    } else if (role == 3) {  // tile's north Y face
+      float d = hd;
+      if (hm && !h_skip) d = hd + (-dtf * ((hp - s_p[pb][hr - 1][hc]) * idy));
+      s_dv[pb][hr - 1][hc - 1] = d;
+    }
+    float wn0 = dw0, wn1 = dw1;
+    if (k + 1 < nz) {
+      const float prl = s_pref[k], pru = s_pref[k + 1], rrl = s_rref[k], rru = s_rref[k + 1];
+      wn0 = dw0 + dtf * (-((n0.p - pru) - (c0.p - prl)) * idzf - a.gravity * (0.5f * ((c0.rho - rrl) + (n0.rho - rru))));
+      wn1 = dw1 + dtf * (-((n1.p - pru) - (c1.p - prl)) * idzf - a.gravity * (0.5f * ((c1.rho - rrl) + (n1.rho - rru))));
+    }
+    __syncthreads();
+    // ---- K15 density, K10 rho*theta, stores
+    float sa = 0.f, sb = 0.f;
+    if (own0) {
+      float rn = c0.rho;
+      if (a.dens) {
+        const float div = (s_du[pb][ty][tx + 1] - un0) * idx + (s_dv[pb][ty + 1][tx] - vn0) * idy + (wn0 - dwc0) * idzc;
+        rn = fmaxf(1.0e-6f, c0.rho - dtf * div);
+      }
+      const float rt = rn * c0.th;
+      const int o = b0 + k * P;
+      if (final_step) {
+        store_mirrored(a.f_rho, g, kCell, gi, gj0, k, rn);
+        store_mirrored(a.f_rt, g, kCell, gi, gj0, k, rt);
+        store_mirrored(a.f_u, g, kFaceX, gi, gj0, k, bu0 + un0);
+        store_mirrored(a.f_v, g, kFaceY, gi, gj0, k, bv0 + vn0);
+        if (k == 0) store_mirrored(a.f_w, g, kFaceZ, gi, gj0, 0, bwz0);
+        store_mirrored(a.f_w, g, kFaceZ, gi, gj0, k + 1, bw0 + wn0);
+      } else {
+        store_mirrored(a.rho_out, g, kCell, gi, gj0, k, rn);
+        store_mirrored(a.du_out, g, kFaceX, gi, gj0, k, un0);
+        store_mirrored(a.dv_out, g, kFaceY, gi, gj0, k, vn0);
+        if (k + 1 < nz) store_mirrored(a.dw_out, g, kFaceZ, gi, gj0, k + 1, wn0);
+      }
+      (void)o;
+      if (acc_mode == 1) { sa = rn; sb = eos_pprime(rn, rt, a.base, k, nz); }
+      else if (acc_mode == 2) { sa = theta_of(rn, rt); }
+    }
+    if (own1) {
+      float rn = c1.rho;
+      if (a.dens) {
+        const float div = (s_du[pb][ty + RY][tx + 1] - un1) * idx + (s_dv[pb][ty + RY + 1][tx] - vn1) * idy + (wn1 - dwc1) * idzc;
+        rn = fmaxf(1.0e-6f, c1.rho - dtf * div);
+      }
+      const float rt = rn * c1.th;
+      if (final_step) {
+        store_mirrored(a.f_rho, g, kCell, gi, gj1, k, rn);
+        store_mirrored(a.f_rt, g, kCell, gi, gj1, k, rt);
+        store_mirrored(a.f_u, g, kFaceX, gi, gj1, k, bu1 + un1);
+        store_mirrored(a.f_v, g, kFaceY, gi, gj1, k, bv1 + vn1);
+        if (k == 0) store_mirrored(a.f_w, g, kFaceZ, gi, gj1, 0, bwz1);
+        store_mirrored(a.f_w, g, kFaceZ, gi, gj1, k + 1, bw1 + wn1);
+      } else {
+        store_mirrored(a.rho_out, g, kCell, gi, gj1, k, rn);
+        store_mirrored(a.du_out, g, kFaceX, gi, gj1, k, un1);
+        store_mirrored(a.dv_out, g, kFaceY, gi, gj1, k, vn1);
+        if (k + 1 < nz) store_mirrored(a.dw_out, g, kFaceZ, gi, gj1, k + 1, wn1);
+      }
+      if (acc_mode == 1) { sa += rn; sb += eos_pprime(rn, rt, a.base, k, nz); }
+      else if (acc_mode == 2) { sa += theta_of(rn, rt); }
+    }
+    if (acc_mode) {
+      const float wa = warp_sum_f(sa), wb = warp_sum_f(sb);
+      if (tx == 0) { s_red[pb][ty][0] = (double)wa; s_red[pb][ty][1] = (double)wb; }
+    }
+    // ---- advance the pipeline
+    dwc0 = wn0; dwc1 = wn1;
+    c0 = n0; c1 = n1;
+    n0 = derive(a, ra0, ta0, k + 2 < nz ? k + 2 : 0);
+    n1 = derive(a, ra1, ta1, k + 2 < nz ? k + 2 : 0);
+    ra0 = nr0; ta0 = nt0; ra1 = nr1; ta1 = nt1;
+    du0 = ndu0; dv0 = ndv0; dw0 = ndw0; du1 = ndu1; dv1 = ndv1; dw1 = ndw1;
+    if (role >= 0 && k + 1 < nz) {
+      hp = eos_pprime(hrho, hrho * hth, a.base, k + 1, nz);
+      hd = hdn;
+    }
+  }
+  if (acc_mode) {
+    __syncthreads();
+    if (tid == 0) {
+      const int pb = (nz - 1) & 1;
+      double sa = 0.0, sb = 0.0;
+      for (int q = 0; q < FW; ++q) { sa += s_red[pb][q][0]; sb += s_red[pb][q][1]; }
+      if (acc_mode == 1) { acc_add(a.acc_a + nz - 1, sa, kScaleRho); acc_add(a.acc_b + nz - 1, sb, kScaleP); }
+      else acc_add(a.acc_a + nz - 1, sa, kScaleTheta);
+    }
+  }
+}
+
 // Per-level mean of rho_theta (FP64, fixed order) and the EOS of that mean.
 __global__ void __launch_bounds__(256) k_base_state(const Geom g, const float* rt, double* base) {
   const int k = blockIdx.x;
@@ -691,6 +936,13 @@ cudaError_t launch_fast_tile(const FastArgs& a, bool first, bool terrain, cudaSt
 
 cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_t s, int tile_rows) {
   if (a.g.nz > kMaxNz) return cudaErrorInvalidValue;
+  if (!terrain && tile_rows == 0) {  // flat-terrain kernel with owned 32 x 16 tiles
+    const dim3 block(flat::TX, flat::RY);
+    const dim3 grid((a.g.nx + flat::TX - 1) / flat::TX, (a.g.ny + flat::TY - 1) / flat::TY);
+    if (first) k_fast_flat<true><<<grid, block, 0, s>>>(a);
+    else k_fast_flat<false><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+  }
   if (tile_rows == 16) return launch_fast_tile<16>(a, first, terrain, s);
   return launch_fast_tile<8>(a, first, terrain, s);
 }

@@ -150,8 +150,9 @@ int gwm_b200_fast_modes(gwm_b200_ctx* ctx);
 int gwm_b200_slow_tendencies(gwm_b200_ctx* ctx, int member, gwm_b200_fields* host_out);
 /* FP64 budgets of the current state. */
 int gwm_b200_budgets(gwm_b200_ctx* ctx, int member, gwm_b200_budget* out);
-/* Tile shape of a kernel: kernel 1 = acoustic substep, rows = CTA tile rows (8 or 16,
- * tiles are 32 columns wide).  The environment variable GWM_B200_FAST_TILE_ROWS sets
+/* Tile shape of a kernel: kernel 1 = acoustic substep; rows 0 = owned 32x16 tiles
+ * (flat terrain; terrain falls back to 8), 8 or 16 = overlapped 32-wide tiles of that
+ * many rows.  The environment variable GWM_B200_FAST_TILE_ROWS sets
  * the default at context creation. */
 int gwm_b200_set_tile(gwm_b200_ctx* ctx, int kernel, int rows);
 /* Kernel launches issued by the last step call (for accounting). */
