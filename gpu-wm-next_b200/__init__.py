@@ -167,6 +167,7 @@ def lib():
     L.gwm_b200_halo_exchange.argtypes = [C.POINTER(_LayoutDesc), C.c_int, C.c_int,
                                          C.POINTER(C.c_void_p), vp]
     L.gwm_b200_dry_pressure.argtypes = [vp, vp, vp, C.c_longlong, vp]
+    L.gwm_b200_field_stats_noalloc.argtypes = [vp, C.c_longlong, vp, vp]
     L.gwm_b200_ranks_to_global.argtypes = [C.POINTER(_LayoutDesc), C.c_int,
                                            C.POINTER(C.c_void_p), vp]
     L.gwm_b200_global_to_ranks.argtypes = [C.POINTER(_LayoutDesc), C.c_int, vp,
@@ -185,7 +186,7 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_step", "gwm_b200_advance_dry", "gwm_b200_advance_tracers",
             "gwm_b200_warm_rain", "gwm_b200_fast_modes", "gwm_b200_slow_tendencies",
             "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_layout",
-            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_ranks_to_global",
+            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_ranks_to_global",
             "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
 
 
@@ -473,6 +474,19 @@ def dry_pressure(rho_ptr: int, rho_theta_ptr: int, p_ptr: int, n: int, stream: O
     rc = lib().gwm_b200_dry_pressure(rho_ptr, rho_theta_ptr, p_ptr, n, stream)
     if rc != OK:
         raise RuntimeError(f"dry_pressure: status {rc}")
+
+
+def field_stats_noalloc(x_ptr: int, n: int, out_ptr: int, stream: Optional[int] = None):
+    """FP64 {sum, min, max} of n device floats into 3 device doubles, allocating nothing.
+
+    For callers that cannot allocate device memory at the call site (their own memory
+    pool owns the device, or cudaMalloc's implicit synchronisation is not allowed
+    there).  The scratch is a fixed 24 KiB device array inside the library; concurrent
+    calls that can overlap on the GPU race.  Make the first call on a device before
+    any stream capture (it resolves the array's device address)."""
+    rc = lib().gwm_b200_field_stats_noalloc(x_ptr, n, out_ptr, stream)
+    if rc != OK:
+        raise RuntimeError(f"field_stats_noalloc: status {rc}")
 
 
 def ranks_to_global(rank_arrays: Sequence[np.ndarray], nx, ny, nz, halo, ranks_x, ranks_y,

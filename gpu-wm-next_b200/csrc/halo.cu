@@ -1,7 +1,10 @@
 // halo.cu — owned<->padded packing, the reference's virtual-rank halo exchange
 // as device kernels, EOS pressure and deterministic FP64 reductions.
 #include <cfloat>
+#include <climits>
+#include <mutex>
 
+#include "../../include/gwm_b200.h"
 #include "halo.cuh"
 
 namespace gwmb {
@@ -255,6 +258,29 @@ __global__ void k_reduce_pass2(const double* part, int nb, ReduceOut* out) {
   if (threadIdx.x == 0) { out->sum = s; out->mn = mn; out->mx = mx; }
 }
 
+// Allocation-free field statistics: the per-block partials live in a fixed
+// device array of this file instead of caller- or context-allocated memory.
+constexpr int kNoAllocBlocks = 1024;  // 3 x 1024 doubles = 24 KiB per device
+static __device__ __align__(256) double g_noalloc_partials[3 * kNoAllocBlocks];
+
+__global__ void __launch_bounds__(256) k_stats_pass1(const float* __restrict__ x, long long n,
+                                                     double* part) {
+  double s = 0.0, mn = DBL_MAX, mx = -DBL_MAX;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const double v = (double)x[q];
+    s += v;
+    mn = fmin(mn, v);
+    mx = fmax(mx, v);
+  }
+  block_reduce3(s, mn, mx);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s;
+    part[gridDim.x + blockIdx.x] = mn;
+    part[2 * gridDim.x + blockIdx.x] = mx;
+  }
+}
+
 inline int blocks_for(long long n, int per) {
   long long b = (n + per - 1) / per;
   if (b < 1) b = 1;
@@ -318,3 +344,42 @@ cudaError_t launch_reduce_2d(const double* a, const double* b, long long n, doub
 }
 
 }  // namespace gwmb
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point (see include/gwm_b200.h).  The device address of
+// g_noalloc_partials is resolved once per device, with that device current, and
+// cached; every later call on the device reuses it.
+using namespace gwmb;
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[kMaxDevices] = {};
+}  // namespace
+
+extern "C" int gwm_b200_field_stats_noalloc(const float* x, long long n, double* out, void* stream) {
+  if (!x || !out || n <= 0 || n > (long long)INT_MAX) return GWM_B200_ERR_ARG;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return GWM_B200_ERR_CUDA;
+  if (dev < 0 || dev >= kMaxDevices) return GWM_B200_ERR_ARG;
+  double* part = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return GWM_B200_ERR_CUDA;
+      g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    part = g_noalloc_addr[dev];
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  long long nb = (n + 256LL * 8 - 1) / (256LL * 8);
+  if (nb > kNoAllocBlocks) nb = kNoAllocBlocks;
+  // every partial the second pass reads is written by the first: nothing to clear
+  k_stats_pass1<<<(int)nb, 256, 0, s>>>(x, n, part);
+  if (cudaGetLastError() != cudaSuccess) return GWM_B200_ERR_CUDA;
+  k_reduce_pass2<<<1, 256, 0, s>>>(part, (int)nb, reinterpret_cast<ReduceOut*>(out));
+  if (cudaGetLastError() != cudaSuccess) return GWM_B200_ERR_CUDA;
+  if (!stream && cudaStreamSynchronize(s) != cudaSuccess) return GWM_B200_ERR_CUDA;
+  return GWM_B200_OK;
+}

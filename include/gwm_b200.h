@@ -182,6 +182,19 @@ int gwm_b200_halo_exchange(const gwm_b200_layout_desc* d, int orientation, int o
 int gwm_b200_dry_pressure(const float* rho_d, const float* rho_theta_m, float* pressure,
                           long long n, void* stream);
 
+/* Allocation-free FP64 statistics of n device floats: out (3 doubles, device memory)
+ * receives {sum, minimum, maximum}, reduced in a fixed order (bitwise reproducible).
+ * No counterpart in the reference.  For callers that must not allocate device memory
+ * at the point of the call: code that owns every device allocation through its own
+ * pool, code running where cudaMalloc would synchronise the device or is not allowed,
+ * and callers without a gwm_b200_ctx.  The scratch is a fixed 24 KiB array inside the
+ * library (1024 blocks of partials), held on every device that loads the library until
+ * process exit; n must lie in [1, 2^31-1].  The first call on a device resolves that
+ * array's device address, so make it before any stream capture on that device.  All
+ * calls share the array: calls that can overlap on the GPU (different streams, or
+ * threads without ordering) race and must be serialised by the caller. */
+int gwm_b200_field_stats_noalloc(const float* x, long long n, double* out, void* stream);
+
 /* ---- host layout helpers (no device work) --------------------------------- */
 /* Per-rank halo-padded host buffers <-> global owned arrays.  Faces shared by two
  * ranks (and periodic aliases) take the average of both copies on the way in, as the
