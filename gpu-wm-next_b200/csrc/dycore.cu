@@ -113,6 +113,9 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
   const bool own_v = inner && gi >= 0 && gi < nx && gj >= 0 && gj <= ny;
   const bool open_x = !g.per_x, open_y = !g.per_y;
   const int base = valid ? gidx(g, gi, gj, 0) : 0;
+  const int ilo = blockIdx.x * (BX - 2), jlo = blockIdx.y * (BY - 2);
+  const bool edge = (g.per_x && (ilo <= 1 || ilo + BX - 3 >= nx - 1)) ||
+                    (g.per_y && (jlo <= 1 || jlo + BY - 3 >= ny - 1));
   const float idx = g.inv_dx, idy = g.inv_dy;
 
   __shared__ float s_th[2][BY][BX], s_p[2][BY][BX], s_u[2][BY][BX], s_v[2][BY][BX], s_w[2][BY][BX];
@@ -200,8 +203,8 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
             q1 = a.wa * q0c.rt + a.wb * q1;
           }
           const float th1 = q1 / fmaxf(r1, 1.0e-6f);
-          store_mirrored(a.o_rho, g, kCell, gi, gj, k, r1);
-          store_mirrored(a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1);
+          store_tile(a.o_rho, g, kCell, gi, gj, k, r1, edge);
+          store_tile(a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1, edge);
           if (a.acc_mode == 1) {
             red_a = r1;
             red_b = eos_pprime(r1, r1 * th1, a.base, k, nz);
@@ -242,7 +245,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
         } else {
           float u1 = fmaxf(-1.0e30f, cc.uf + a.dt * t_u);
           if (blend) u1 = a.wa * q0c.u + a.wb * u1;
-          store_mirrored(a.o_u, g, kFaceX, gi, gj, k, u1);
+          store_tile(a.o_u, g, kFaceX, gi, gj, k, u1, edge);
         }
       }
       // ---- Y face: K18 (dry_momentum_flux.cu:158-235) + K22 (dry_pressure_gradient.cu:125-173)
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
         } else {
           float v1 = fmaxf(-1.0e30f, cc.vf + a.dt * t_v);
           if (blend) v1 = a.wa * q0c.v + a.wb * v1;
-          store_mirrored(a.o_v, g, kFaceY, gi, gj, k, v1);
+          store_tile(a.o_v, g, kFaceY, gi, gj, k, v1, edge);
         }
       }
       // ---- Z face k: K19 (dry_momentum_flux.cu:237-312) + K3 buoyancy (dry_core.cu:146-187)
@@ -309,11 +312,11 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
         } else {
           float w1 = fmaxf(-1.0e30f, cc.wf + a.dt * t_w);
           if (blend) w1 = a.wa * q0c.w + a.wb * w1;
-          store_mirrored(a.o_w, g, kFaceZ, gi, gj, k, w1);
+          store_tile(a.o_w, g, kFaceZ, gi, gj, k, w1, edge);
           if (k + 1 == nz) {  // top face: zero tendency
             float wt = fmaxf(-1.0e30f, cn.wf);
             if (blend) wt = a.wa * q0c.wtop + a.wb * wt;
-            store_mirrored(a.o_w, g, kFaceZ, gi, gj, k + 1, wt);
+            store_tile(a.o_w, g, kFaceZ, gi, gj, k + 1, wt, edge);
           }
         }
       }
@@ -667,6 +670,8 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
   const int b0 = own0 ? gidx(g, gi, gj0, 0) : 0, b1 = own1 ? gidx(g, gi, gj1, 0) : 0;
   const bool skip_u = gi == 0 && !g.per_x;         // open west face (never changes)
   const bool skip_v0 = gj0 == 0 && !g.per_y;
+  // tiles away from the periodic edge rings store without mirror checks
+  const bool edge = (g.per_x && (i0 <= 1 || i0 + w >= nx - 1)) || (g.per_y && (j0 <= 1 || j0 + h >= ny - 1));
   // halo role: 0 west column, 1 east column, 2 south row, 3 north row
   int role = -1, hi = 0, hj = 0;
   if (tid < TY) { if (tid < h) { role = 0; hi = i0 - 1; hj = j0 + tid; } }
@@ -680,6 +685,7 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
   const bool final_step = a.final_kind == 2;
   const int acc_mode = a.acc_off ? 0 : (a.final_kind == 0 ? 1 : 2);
   const int P = g.plane;
+  const bool hm = a.hmom != 0, dn = a.dens != 0;
 
   __shared__ float s_p[2][TY + 2][TX + 2];
   __shared__ float s_du[2][TY][TX + 1];
@@ -722,52 +728,123 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
     if (!FIRST && role == 1) hd = __ldg(a.du_in + hb);
     if (!FIRST && role == 3) hd = __ldg(a.dv_in + hb);
   }
+  // state carried from the faces of plane k to its density update one iteration later
+  float pun0 = 0.f, pvn0 = 0.f, pwn0 = 0.f, pwc0 = 0.f, prho0 = 0.f, pth0 = 0.f;
+  float pun1 = 0.f, pvn1 = 0.f, pwn1 = 0.f, pwc1 = 0.f, prho1 = 0.f, pth1 = 0.f;
+  float pbu0 = 0.f, pbv0 = 0.f, pbw0 = 0.f, pbwz0 = 0.f, pbu1 = 0.f, pbv1 = 0.f, pbw1 = 0.f, pbwz1 = 0.f;
+  float pidzc = 0.f;
   float dwc0 = 0.f, dwc1 = 0.f;  // increment at face k (face 0 never changes)
   __syncthreads();
 
-  for (int k = 0; k < nz; ++k) {
+  // K15 density, K10 rho*theta and the stores of plane kk, from the faces computed
+  // one iteration earlier (their tiles are published by this iteration's barrier)
+  auto finish_plane = [&](int kk, int pbk, float& sa, float& sb) {
+    if (own0) {
+      float rn = prho0;
+      if (dn) {
+        const float div = (s_du[pbk][ty][tx + 1] - pun0) * idx + (s_dv[pbk][ty + 1][tx] - pvn0) * idy +
+                          (pwn0 - pwc0) * pidzc;
+        rn = fmaxf(1.0e-6f, prho0 - dtf * div);
+      }
+      const float rt = rn * pth0;
+      if (final_step) {
+        store_tile(a.f_rho, g, kCell, gi, gj0, kk, rn, edge);
+        store_tile(a.f_rt, g, kCell, gi, gj0, kk, rt, edge);
+        store_tile(a.f_u, g, kFaceX, gi, gj0, kk, pbu0 + pun0, edge);
+        store_tile(a.f_v, g, kFaceY, gi, gj0, kk, pbv0 + pvn0, edge);
+        if (kk == 0) store_tile(a.f_w, g, kFaceZ, gi, gj0, 0, pbwz0, edge);
+        store_tile(a.f_w, g, kFaceZ, gi, gj0, kk + 1, pbw0 + pwn0, edge);
+      } else {
+        store_tile(a.rho_out, g, kCell, gi, gj0, kk, rn, edge);
+        store_tile(a.du_out, g, kFaceX, gi, gj0, kk, pun0, edge);
+        store_tile(a.dv_out, g, kFaceY, gi, gj0, kk, pvn0, edge);
+        if (kk + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj0, kk + 1, pwn0, edge);
+      }
+      if (acc_mode == 1) { sa = rn; sb = eos_pprime(rn, rt, a.base, kk, nz); }
+      else if (acc_mode == 2) { sa = theta_of(rn, rt); }
+    }
+    if (own1) {
+      float rn = prho1;
+      if (dn) {
+        const float div = (s_du[pbk][ty + RY][tx + 1] - pun1) * idx + (s_dv[pbk][ty + RY + 1][tx] - pvn1) * idy +
+                          (pwn1 - pwc1) * pidzc;
+        rn = fmaxf(1.0e-6f, prho1 - dtf * div);
+      }
+      const float rt = rn * pth1;
+      if (final_step) {
+        store_tile(a.f_rho, g, kCell, gi, gj1, kk, rn, edge);
+        store_tile(a.f_rt, g, kCell, gi, gj1, kk, rt, edge);
+        store_tile(a.f_u, g, kFaceX, gi, gj1, kk, pbu1 + pun1, edge);
+        store_tile(a.f_v, g, kFaceY, gi, gj1, kk, pbv1 + pvn1, edge);
+        if (kk == 0) store_tile(a.f_w, g, kFaceZ, gi, gj1, 0, pbwz1, edge);
+        store_tile(a.f_w, g, kFaceZ, gi, gj1, kk + 1, pbw1 + pwn1, edge);
+      } else {
+        store_tile(a.rho_out, g, kCell, gi, gj1, kk, rn, edge);
+        store_tile(a.du_out, g, kFaceX, gi, gj1, kk, pun1, edge);
+        store_tile(a.dv_out, g, kFaceY, gi, gj1, kk, pvn1, edge);
+        if (kk + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj1, kk + 1, pwn1, edge);
+      }
+      if (acc_mode == 1) { sa += rn; sb += eos_pprime(rn, rt, a.base, kk, nz); }
+      else if (acc_mode == 2) { sa += theta_of(rn, rt); }
+    }
+  };
+
+  for (int k = 0; k <= nz; ++k) {
     const int pb = k & 1;
+    const bool active = k < nz;
     // ---- issue the loads of later planes
-    float nr0, nt0, nr1, nt1;
-    ld2(b0, own0, k + 3, nr0, nt0);
-    ld2(b1, own1, k + 3, nr1, nt1);
+    float nr0 = 0.f, nt0 = 0.f, nr1 = 0.f, nt1 = 0.f;
     float ndu0 = 0.f, ndv0 = 0.f, ndw0 = 0.f, ndu1 = 0.f, ndv1 = 0.f, ndw1 = 0.f;
-    if (!FIRST && k + 1 < nz) {
-      const int o = (k + 1) * P;
-      if (own0) { ndu0 = __ldg(a.du_in + b0 + o); ndv0 = __ldg(a.dv_in + b0 + o); if (k + 2 < nz) ndw0 = __ldg(a.dw_in + b0 + o + P); }
-      if (own1) { ndu1 = __ldg(a.du_in + b1 + o); ndv1 = __ldg(a.dv_in + b1 + o); if (k + 2 < nz) ndw1 = __ldg(a.dw_in + b1 + o + P); }
-    }
     float hrho = 0.f, hth = 0.f, hdn = 0.f;
-    if (role >= 0 && k + 1 < nz) {
-      const int o = hb + (k + 1) * P;
-      hrho = __ldg(a.rho_in + o);
-      hth = __ldg(a.th + o);
-      if (!FIRST && role == 1) hdn = __ldg(a.du_in + o);
-      if (!FIRST && role == 3) hdn = __ldg(a.dv_in + o);
-    }
     float bu0 = 0.f, bv0 = 0.f, bw0 = 0.f, bu1 = 0.f, bv1 = 0.f, bw1 = 0.f, bwz0 = 0.f, bwz1 = 0.f;
-    if (final_step) {
-      const int o = k * P;
-      if (own0) { bu0 = __ldg(a.bu + b0 + o); bv0 = __ldg(a.bv + b0 + o); bw0 = __ldg(a.bw + b0 + o + P); if (k == 0) bwz0 = __ldg(a.bw + b0); }
-      if (own1) { bu1 = __ldg(a.bu + b1 + o); bv1 = __ldg(a.bv + b1 + o); bw1 = __ldg(a.bw + b1 + o + P); if (k == 0) bwz1 = __ldg(a.bw + b1); }
+    float idzc = 0.f, idzf = 0.f;
+    if (active) {
+      ld2(b0, own0, k + 3, nr0, nt0);
+      ld2(b1, own1, k + 3, nr1, nt1);
+      if (!FIRST && k + 1 < nz) {
+        const int o = (k + 1) * P;
+        if (own0) { ndu0 = __ldg(a.du_in + b0 + o); ndv0 = __ldg(a.dv_in + b0 + o); if (k + 2 < nz) ndw0 = __ldg(a.dw_in + b0 + o + P); }
+        if (own1) { ndu1 = __ldg(a.du_in + b1 + o); ndv1 = __ldg(a.dv_in + b1 + o); if (k + 2 < nz) ndw1 = __ldg(a.dw_in + b1 + o + P); }
+      }
+      if (role >= 0 && k + 1 < nz) {
+        const int o = hb + (k + 1) * P;
+        hrho = __ldg(a.rho_in + o);
+        hth = __ldg(a.th + o);
+        if (!FIRST && role == 1) hdn = __ldg(a.du_in + o);
+        if (!FIRST && role == 3) hdn = __ldg(a.dv_in + o);
+      }
+      if (final_step) {
+        const int o = k * P;
+        if (own0) { bu0 = __ldg(a.bu + b0 + o); bv0 = __ldg(a.bv + b0 + o); bw0 = __ldg(a.bw + b0 + o + P); if (k == 0) bwz0 = __ldg(a.bw + b0); }
+        if (own1) { bu1 = __ldg(a.bu + b1 + o); bv1 = __ldg(a.bv + b1 + o); bw1 = __ldg(a.bw + b1 + o + P); if (k == 0) bwz1 = __ldg(a.bw + b1); }
+      }
+      idzc = __ldg(a.idz_c + k);
+      idzf = (k + 1 < nz) ? __ldg(a.idz_f + k + 1) : 0.f;
+      // ---- plane k pressure perturbation into shared memory (owners and halo only:
+      // on partial edge tiles the slot next to the last owned column/row is a halo slot)
+      if (own0) s_p[pb][ty + 1][tx + 1] = c0.p;
+      if (own1) s_p[pb][ty + RY + 1][tx + 1] = c1.p;
+      if (role >= 0) s_p[pb][hr][hc] = hp;
     }
-    const float idzc = __ldg(a.idz_c + k);
-    const float idzf = (k + 1 < nz) ? __ldg(a.idz_f + k + 1) : 0.f;
-    // ---- plane k pressure perturbation into shared memory
-    // only owners write tile slots: on partial edge tiles the slot next to the last
-    // owned column/row belongs to a halo thread
-    if (own0) s_p[pb][ty + 1][tx + 1] = c0.p;
-    if (own1) s_p[pb][ty + RY + 1][tx + 1] = c1.p;
-    if (role >= 0) s_p[pb][hr][hc] = hp;
     __syncthreads();
-    if (acc_mode && k > 0 && tid == 0) {
-      double sa = 0.0, sb = 0.0;
-      for (int q = 0; q < FW; ++q) { sa += s_red[pb ^ 1][q][0]; sb += s_red[pb ^ 1][q][1]; }
-      if (acc_mode == 1) { acc_add(a.acc_a + k - 1, sa, kScaleRho); acc_add(a.acc_b + k - 1, sb, kScaleP); }
-      else acc_add(a.acc_a + k - 1, sa, kScaleTheta);
+    // ---- plane k-1: density update and stores (its face tiles are now published)
+    if (k > 0) {
+      float sa = 0.f, sb = 0.f;
+      finish_plane(k - 1, pb ^ 1, sa, sb);
+      if (acc_mode) {
+        const float wa = warp_sum_f(sa), wb = warp_sum_f(sb);
+        if (tx == 0) { s_red[pb ^ 1][ty][0] = (double)wa; s_red[pb ^ 1][ty][1] = (double)wb; }
+      }
     }
-    // ---- K12/K13 horizontal momenta, K14 vertical momentum at face k+1
-    const bool hm = a.hmom != 0;
+    // level sums of plane k-2, whose warp partials the previous barrier published
+    if (acc_mode && k > 1 && tid == 0) {
+      double sa = 0.0, sb = 0.0;
+      for (int q = 0; q < FW; ++q) { sa += s_red[pb][q][0]; sb += s_red[pb][q][1]; }
+      if (acc_mode == 1) { acc_add(a.acc_a + k - 2, sa, kScaleRho); acc_add(a.acc_b + k - 2, sb, kScaleP); }
+      else acc_add(a.acc_a + k - 2, sa, kScaleTheta);
+    }
+    if (!active) break;
+    // ---- plane k faces: K12/K13 horizontal momenta, K14 vertical momentum at face k+1
     float un0 = du0, vn0 = dv0, un1 = du1, vn1 = dv1;
     if (hm) {
       if (!skip_u) {
@@ -794,62 +871,11 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
       wn0 = dw0 + dtf * (-((n0.p - pru) - (c0.p - prl)) * idzf - a.gravity * (0.5f * ((c0.rho - rrl) + (n0.rho - rru))));
       wn1 = dw1 + dtf * (-((n1.p - pru) - (c1.p - prl)) * idzf - a.gravity * (0.5f * ((c1.rho - rrl) + (n1.rho - rru))));
     }
-    __syncthreads();
-    // ---- K15 density, K10 rho*theta, stores
-    float sa = 0.f, sb = 0.f;
-    if (own0) {
-      float rn = c0.rho;
-      if (a.dens) {
-        const float div = (s_du[pb][ty][tx + 1] - un0) * idx + (s_dv[pb][ty + 1][tx] - vn0) * idy + (wn0 - dwc0) * idzc;
-        rn = fmaxf(1.0e-6f, c0.rho - dtf * div);
-      }
-      const float rt = rn * c0.th;
-      const int o = b0 + k * P;
-      if (final_step) {
-        store_mirrored(a.f_rho, g, kCell, gi, gj0, k, rn);
-        store_mirrored(a.f_rt, g, kCell, gi, gj0, k, rt);
-        store_mirrored(a.f_u, g, kFaceX, gi, gj0, k, bu0 + un0);
-        store_mirrored(a.f_v, g, kFaceY, gi, gj0, k, bv0 + vn0);
-        if (k == 0) store_mirrored(a.f_w, g, kFaceZ, gi, gj0, 0, bwz0);
-        store_mirrored(a.f_w, g, kFaceZ, gi, gj0, k + 1, bw0 + wn0);
-      } else {
-        store_mirrored(a.rho_out, g, kCell, gi, gj0, k, rn);
-        store_mirrored(a.du_out, g, kFaceX, gi, gj0, k, un0);
-        store_mirrored(a.dv_out, g, kFaceY, gi, gj0, k, vn0);
-        if (k + 1 < nz) store_mirrored(a.dw_out, g, kFaceZ, gi, gj0, k + 1, wn0);
-      }
-      (void)o;
-      if (acc_mode == 1) { sa = rn; sb = eos_pprime(rn, rt, a.base, k, nz); }
-      else if (acc_mode == 2) { sa = theta_of(rn, rt); }
-    }
-    if (own1) {
-      float rn = c1.rho;
-      if (a.dens) {
-        const float div = (s_du[pb][ty + RY][tx + 1] - un1) * idx + (s_dv[pb][ty + RY + 1][tx] - vn1) * idy + (wn1 - dwc1) * idzc;
-        rn = fmaxf(1.0e-6f, c1.rho - dtf * div);
-      }
-      const float rt = rn * c1.th;
-      if (final_step) {
-        store_mirrored(a.f_rho, g, kCell, gi, gj1, k, rn);
-        store_mirrored(a.f_rt, g, kCell, gi, gj1, k, rt);
-        store_mirrored(a.f_u, g, kFaceX, gi, gj1, k, bu1 + un1);
-        store_mirrored(a.f_v, g, kFaceY, gi, gj1, k, bv1 + vn1);
-        if (k == 0) store_mirrored(a.f_w, g, kFaceZ, gi, gj1, 0, bwz1);
-        store_mirrored(a.f_w, g, kFaceZ, gi, gj1, k + 1, bw1 + wn1);
-      } else {
-        store_mirrored(a.rho_out, g, kCell, gi, gj1, k, rn);
-        store_mirrored(a.du_out, g, kFaceX, gi, gj1, k, un1);
-        store_mirrored(a.dv_out, g, kFaceY, gi, gj1, k, vn1);
-        if (k + 1 < nz) store_mirrored(a.dw_out, g, kFaceZ, gi, gj1, k + 1, wn1);
-      }
-      if (acc_mode == 1) { sa += rn; sb += eos_pprime(rn, rt, a.base, k, nz); }
-      else if (acc_mode == 2) { sa += theta_of(rn, rt); }
-    }
-    if (acc_mode) {
-      const float wa = warp_sum_f(sa), wb = warp_sum_f(sb);
-      if (tx == 0) { s_red[pb][ty][0] = (double)wa; s_red[pb][ty][1] = (double)wb; }
-    }
-    // ---- advance the pipeline
+    // ---- hand plane k to the next iteration's density update, advance the pipeline
+    pun0 = un0; pvn0 = vn0; pwn0 = wn0; pwc0 = dwc0; prho0 = c0.rho; pth0 = c0.th;
+    pun1 = un1; pvn1 = vn1; pwn1 = wn1; pwc1 = dwc1; prho1 = c1.rho; pth1 = c1.th;
+    pbu0 = bu0; pbv0 = bv0; pbw0 = bw0; pbwz0 = bwz0; pbu1 = bu1; pbv1 = bv1; pbw1 = bw1; pbwz1 = bwz1;
+    pidzc = idzc;
     dwc0 = wn0; dwc1 = wn1;
     c0 = n0; c1 = n1;
     n0 = derive(a, ra0, ta0, k + 2 < nz ? k + 2 : 0);
@@ -861,6 +887,7 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
       hd = hdn;
     }
   }
+  // level sums of the last plane
   if (acc_mode) {
     __syncthreads();
     if (tid == 0) {

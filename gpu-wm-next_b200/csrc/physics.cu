@@ -48,6 +48,9 @@ __global__ void __launch_bounds__(NT) k_tracer_stage(const TracerArgs a) {
   const bool inner = tx >= 1 && tx <= BX - 2 && ty >= 1 && ty <= BY - 2;
   const bool own_c = inner && gi >= 0 && gi < nx && gj >= 0 && gj < ny;
   const int base = valid ? gidx(g, gi, gj, 0) : 0;
+  const int ilo = blockIdx.x * (BX - 2), jlo = blockIdx.y * (BY - 2);
+  const bool edge = (g.per_x && (ilo <= 1 || ilo + BX - 3 >= nx - 1)) ||
+                    (g.per_y && (jlo <= 1 || jlo + BY - 3 >= ny - 1));
   const float idx = g.inv_dx, idy = g.inv_dy;
   const bool blend = a.q0[0] != nullptr;
 
@@ -94,7 +97,7 @@ __global__ void __launch_bounds__(NT) k_tracer_stage(const TracerArgs a) {
         const float div = (ge - gw) * idx + (gn - gs) * idy + (gt - gb) * idz;
         float out = fmaxf(0.0f, cc.rq[t] - a.dt * div);
         if (blend) out = a.wa * q0v[t] + a.wb * out;
-        store_mirrored(a.q_out[t], g, kCell, gi, gj, k, out);
+        store_tile(a.q_out[t], g, kCell, gi, gj, k, out, edge);
       }
     }
     cm = cc;
@@ -124,6 +127,9 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
   const int gi = blockIdx.x * RB + threadIdx.x;
   const int gj = blockIdx.y;
   const bool active = gi < g.nx && gj < g.ny;
+  const int ilo = blockIdx.x * RB;
+  const bool edge = (g.per_x && (ilo <= 1 || ilo + RB - 1 >= g.nx - 1)) ||
+                    (g.per_y && (gj <= 1 || gj >= g.ny - 1));
   __shared__ double s_th[kMaxNz][RB / 32];
   float incoming = 0.0f;
   // one-cell-ahead prefetch down the column
@@ -209,10 +215,10 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
         }
       }
       const float rt_new = rho * th;
-      store_mirrored(a.qv, g, kCell, gi, gj, k, rho * qv);
-      store_mirrored(a.qc, g, kCell, gi, gj, k, rho * qc);
-      store_mirrored(a.qr, g, kCell, gi, gj, k, rqr);
-      store_mirrored(a.rt, g, kCell, gi, gj, k, rt_new);
+      store_tile(a.qv, g, kCell, gi, gj, k, rho * qv, edge);
+      store_tile(a.qc, g, kCell, gi, gj, k, rho * qc, edge);
+      store_tile(a.qr, g, kCell, gi, gj, k, rqr, edge);
+      store_tile(a.rt, g, kCell, gi, gj, k, rt_new, edge);
       th_sum = (double)theta_of(rho_d, rt_new);
     }
     if (a.th_acc) {

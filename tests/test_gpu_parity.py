@@ -408,3 +408,44 @@ def test_warm_rain_kats_gpu(gwm, fallout):
                                         rain_terminal_velocity=1500.0, enable_latent_heating=False))
         assert abs(o["qr"][0, 0, 0]) < 1e-6
         assert abs(o["precip"][0, 0] - 10.0) < 1e-6
+
+
+def test_interior_tiles_vs_oracle(gwm, orc):
+    # a grid wide enough that every kernel has CTAs away from the periodic edge ring
+    # (those take plain stores; edge CTAs also write the mirrored halo slots)
+    g = gwm.GridSpec(160, 96, 10, dx=2000.0, dy=2000.0, z_top=12000.0)
+    p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=11, relative_humidity=1.02)
+    s = gwm.build_case("moist_sounding", g, p, moist=True)
+    step = gwm.StepConfig(dt=2.0, fast_substeps=3)
+    rain = gwm.WarmRainConfig(dt=2.0, rain_terminal_velocity=12.0)
+    with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=True)) as m:
+        m.upload(s)
+        m.step(2)
+        out = m.download()
+    kw = dict(phases=orc.PHASE_DRY | orc.PHASE_TRACERS | orc.PHASE_RAIN, rain=orc.RainSpec(dt=2.0, terminal_velocity=12.0))
+    ref = orc.run(ogrid(orc, g), ostep(orc, step), to64(s), 2, precision=64, **kw)
+    ref32 = orc.run(ogrid(orc, g), ostep(orc, step), to64(s), 2, precision=32, **kw)
+    base = to64(s)
+    assert_envelope(out, ref, ref32, ("rho", "rho_theta"), floor=1e-6, tag="interior")
+    assert_envelope(out, ref, ref32, ("u", "v", "w"), base=base, floor=1e-4, tag="interior")
+    for k in ("qv", "qc", "qr"):
+        assert rel_err(out[k], ref[k], floor=1e-9) < 1e-3, k
+
+
+@pytest.mark.parametrize("rows", [0, 8, 16])
+def test_substep_tilings_agree(gwm, rows):
+    g = gwm.GridSpec(100, 70, 12, dx=2000.0, dy=2000.0, z_top=12000.0)
+    s = c1_state(gwm, g, u=2.0, v=1.0)
+    step = gwm.StepConfig(dt=1.0, fast_substeps=4)
+    outs = {}
+    for r in (0, rows):
+        with gwm.Model(g, gwm.MemberSpec(step=step)) as m:
+            m.set_tile("fast_substep", r)
+            m.upload(s)
+            m.advance_dry_state_ssprk3(2)
+            outs[r] = m.download()
+    base = to64(s)
+    for k in ("rho", "rho_theta"):
+        assert rel_err(outs[rows][k], outs[0][k]) < 1e-6, k
+    for k in ("u", "v", "w"):
+        assert perturbation_err(outs[rows][k], outs[0][k], base[k]) < 1e-4, k
