@@ -197,6 +197,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels directly (profiling)")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default tiles (no autotune)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -221,6 +222,14 @@ def main():
     stream = torch.cuda.Stream()
     model.set_stream(stream.cuda_stream)
     model.upload(state)
+    tiles = None
+    if not args.no_tune:
+        # pick each stencil kernel's tile by timing it, then restart from the initial state
+        with torch.cuda.stream(stream):
+            tiles = model.autotune(1)
+        model.upload(state)
+    else:
+        tiles = {k: model.get_tile(k) for k in ("slow_stage", "fast_substep", "tracer_stage")}
     model.use_graph(not args.no_graph)
     cells = args.nx * args.ny * NZ
 
@@ -277,7 +286,8 @@ def main():
                        "dt_s": DT, "fast_substeps": NS, "rain_terminal_velocity": VT,
                        "phases": "dry SSPRK3 + 3-tracer SSPRK3 + warm rain/fallout",
                        "l2": "inputs larger than L2 (each field 282 MB)",
-                       "graph": not args.no_graph, "parallelism": f"replicas{world}"},
+                       "graph": not args.no_graph, "tile_rows": tiles,
+                       "parallelism": f"replicas{world}"},
             "gpu_launches": launches,
             "state_finite": finite,
             "roofline": roof,

@@ -159,6 +159,7 @@ def lib():
     L.gwm_b200_budgets.argtypes = [vp, C.c_int, C.POINTER(_Budget)]
     L.gwm_b200_profile.argtypes = [vp, C.c_int]
     L.gwm_b200_set_tile.argtypes = [vp, C.c_int, C.c_int]
+    L.gwm_b200_get_tile.argtypes = [vp, C.c_int]
     L.gwm_b200_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double),
                                         C.POINTER(C.c_longlong), C.POINTER(C.c_char_p)]
     L.gwm_b200_launch_count.argtypes = [vp]
@@ -185,7 +186,7 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_synchronize", "gwm_b200_use_graph", "gwm_b200_upload", "gwm_b200_download",
             "gwm_b200_step", "gwm_b200_advance_dry", "gwm_b200_advance_tracers",
             "gwm_b200_warm_rain", "gwm_b200_fast_modes", "gwm_b200_slow_tendencies",
-            "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_layout",
+            "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_get_tile", "gwm_b200_layout",
             "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_ranks_to_global",
             "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
 
@@ -424,9 +425,44 @@ class Model:
     def launch_count(self) -> int:
         return int(lib().gwm_b200_launch_count(self._h))
 
+    _TILE_KERNELS = {"slow_stage": 0, "fast_substep": 1, "tracer_stage": 2}
+
     def set_tile(self, kernel: str, rows: int):
-        """CTA tile rows of a kernel ("fast_substep": 8 or 16)."""
-        self._check(lib().gwm_b200_set_tile(self._h, {"fast_substep": 1}[kernel], rows), "set_tile")
+        """CTA tile rows of a kernel: "slow_stage"/"tracer_stage" 8 or 16,
+        "fast_substep" 0 (owned flat tiles), 8 or 16."""
+        self._check(lib().gwm_b200_set_tile(self._h, self._TILE_KERNELS[kernel], rows), "set_tile")
+
+    def get_tile(self, kernel: str) -> int:
+        r = lib().gwm_b200_get_tile(self._h, self._TILE_KERNELS[kernel])
+        if r < 0:
+            raise ValueError(kernel)
+        return r
+
+    def autotune(self, steps: int = 1) -> Dict[str, int]:
+        """Pick the fastest tile of each stencil kernel by timing real steps.
+
+        Every tiling computes the same values, so the tuning steps are ordinary
+        model steps: the state advances by ``steps`` per candidate (7 candidates
+        per pass).  Re-upload the initial state afterwards to start from it.
+        Returns the chosen rows per kernel."""
+        candidates = {"slow_stage": (8, 16), "fast_substep": (0, 8, 16), "tracer_stage": (8, 16)}
+        kinds = {"slow_stage": "k_slow_stage", "fast_substep": "k_fast_substep",
+                 "tracer_stage": "k_tracer_stage"}
+        best = {k: self.get_tile(k) for k in candidates}
+        for kernel, rows_list in candidates.items():
+            times = {}
+            for rows in rows_list:
+                self.set_tile(kernel, rows)
+                self.profile(True)
+                self.step(steps)
+                rep = self.profile_report().get(kinds[kernel])
+                self.profile(False)
+                if rep:
+                    times[rows] = rep["avg_ms"]
+            if times:
+                best[kernel] = min(times, key=times.get)
+            self.set_tile(kernel, best[kernel])
+        return best
 
     def profile(self, enable: bool = True):
         """Per-kernel CUDA-event timing of subsequent direct (non-graph) launches."""

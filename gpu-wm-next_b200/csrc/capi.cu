@@ -84,6 +84,8 @@ struct gwm_b200_ctx {
   cudaGraphExec_t graph = nullptr;
   long long graph_launches = 0;
   int fast_tile_rows = 0;  // acoustic substep: 0 owned-tile flat kernel, 8/16 overlapped tiles
+  int slow_tile_rows = 16;    // slow stage: overlapped tiles of 8 or 16 rows
+  int tracer_tile_rows = 16;  // tracer stage: overlapped tiles of 8 or 16 rows
   long long launches = 0;
   long long cur_launches = 0;
 };
@@ -355,7 +357,7 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
     a.acc_mode = fast ? (terr ? 0 : 1) : ((s == 2 && rain_theta) ? 0 : 2);
     a.inv_count = inv_count(M);
     a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf; a.base = M.base;
-    LAUNCH(launch_slow(a, terr, c->stream), "slow stage");
+    LAUNCH(launch_slow(a, terr, c->stream, c->slow_tile_rows), "slow stage");
     M.ring = (M.ring + 1) % 3;
     rcur = rnext;
     if (!fast) continue;
@@ -405,7 +407,7 @@ int enqueue_tracers(gwm_b200_ctx* c, Member& M) {
     a.wa = wa[s]; a.wb = wb[s]; a.dt = M.md.step.dt;
     a.ntracers = 3;
     a.idz_c = M.idc; a.terrain = M.terrain_active;
-    LAUNCH(launch_tracer_stage(a, c->stream), "tracer stage");
+    LAUNCH(launch_tracer_stage(a, c->stream, c->tracer_tile_rows), "tracer stage");
   }
   return GWM_B200_OK;
 }
@@ -547,10 +549,21 @@ int gwm_b200_use_graph(gwm_b200_ctx* c, int enable) {
 long long gwm_b200_launch_count(const gwm_b200_ctx* c) { return c ? c->launches : -1; }
 
 int gwm_b200_set_tile(gwm_b200_ctx* c, int kernel, int rows) {
-  if (!c || kernel != 1 || (rows != 0 && rows != 8 && rows != 16)) return GWM_B200_ERR_ARG;
+  if (!c) return GWM_B200_ERR_ARG;
+  const bool ok = kernel == 1 ? (rows == 0 || rows == 8 || rows == 16)
+                              : (kernel == 0 || kernel == 2) && (rows == 8 || rows == 16);
+  if (!ok) return GWM_B200_ERR_ARG;
   drop_graph(c);
-  c->fast_tile_rows = rows;
+  (kernel == 0 ? c->slow_tile_rows : kernel == 1 ? c->fast_tile_rows : c->tracer_tile_rows) = rows;
   return GWM_B200_OK;
+}
+
+int gwm_b200_get_tile(const gwm_b200_ctx* c, int kernel) {
+  if (!c) return GWM_B200_ERR_ARG;
+  if (kernel == 0) return c->slow_tile_rows;
+  if (kernel == 1) return c->fast_tile_rows;
+  if (kernel == 2) return c->tracer_tile_rows;
+  return GWM_B200_ERR_ARG;
 }
 
 int gwm_b200_upload(gwm_b200_ctx* c, int member, const gwm_b200_fields* h) {
@@ -811,7 +824,7 @@ int gwm_b200_slow_tendencies(gwm_b200_ctx* c, int member, gwm_b200_fields* h) {
   a.acc_mode = 0;
   a.inv_count = inv_count(M);
   a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf; a.base = M.base;
-  CK(launch_slow(a, M.terrain_active, c->stream));
+  CK(launch_slow(a, M.terrain_active, c->stream, c->slow_tile_rows));
   gwm_b200_fields tmp{};
   tmp.rho_d = h->rho_d; tmp.rho_theta_m = h->rho_theta_m;
   tmp.mom_u = h->mom_u; tmp.mom_v = h->mom_v; tmp.mom_w = h->mom_w;

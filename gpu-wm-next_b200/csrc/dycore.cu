@@ -99,35 +99,36 @@ __device__ __forceinline__ float column_dpdz(int k, int nz, float pm, float pc, 
   return (pn - pm) / fmaxf(zn - zm, 1.0e-6f);
 }
 
-template <bool TERRAIN>
-__global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
+template <bool TERRAIN, int SBY>
+__global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
+  constexpr int SNT = BX * SBY, SNW = SNT / 32;
   const Geom& g = a.g;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
   const int gi = blockIdx.x * (BX - 2) - 1 + tx;
-  const int gj = blockIdx.y * (BY - 2) - 1 + ty;
+  const int gj = blockIdx.y * (SBY - 2) - 1 + ty;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const bool valid = gi >= -1 && gi <= nx + 1 && gj >= -1 && gj <= ny + 1;
-  const bool inner = tx >= 1 && tx <= BX - 2 && ty >= 1 && ty <= BY - 2;
+  const bool inner = tx >= 1 && tx <= BX - 2 && ty >= 1 && ty <= SBY - 2;
   const bool own_c = inner && gi >= 0 && gi < nx && gj >= 0 && gj < ny;
   const bool own_u = inner && gi >= 0 && gi <= nx && gj >= 0 && gj < ny;
   const bool own_v = inner && gi >= 0 && gi < nx && gj >= 0 && gj <= ny;
   const bool open_x = !g.per_x, open_y = !g.per_y;
   const int base = valid ? gidx(g, gi, gj, 0) : 0;
-  const int ilo = blockIdx.x * (BX - 2), jlo = blockIdx.y * (BY - 2);
+  const int ilo = blockIdx.x * (BX - 2), jlo = blockIdx.y * (SBY - 2);
   const bool edge = (g.per_x && (ilo <= 1 || ilo + BX - 3 >= nx - 1)) ||
-                    (g.per_y && (jlo <= 1 || jlo + BY - 3 >= ny - 1));
+                    (g.per_y && (jlo <= 1 || jlo + SBY - 3 >= ny - 1));
   const float idx = g.inv_dx, idy = g.inv_dy;
 
-  __shared__ float s_th[2][BY][BX], s_p[2][BY][BX], s_u[2][BY][BX], s_v[2][BY][BX], s_w[2][BY][BX];
-  __shared__ float s_uc[2][BY][BX], s_vc[2][BY][BX], s_wc[2][BY][BX];
-  __shared__ float s_zc[TERRAIN ? 2 : 1][BY][BX], s_dz[TERRAIN ? 2 : 1][BY][BX];
+  __shared__ float s_th[2][SBY][BX], s_p[2][SBY][BX], s_u[2][SBY][BX], s_v[2][SBY][BX], s_w[2][SBY][BX];
+  __shared__ float s_uc[2][SBY][BX], s_vc[2][SBY][BX], s_wc[2][SBY][BX];
+  __shared__ float s_zc[TERRAIN ? 2 : 1][SBY][BX], s_dz[TERRAIN ? 2 : 1][SBY][BX];
   __shared__ float s_thref[kMaxNz];
-  __shared__ double s_red[2][NW][2];
+  __shared__ double s_red[2][SNW][2];
 
   if (blockIdx.x == 0 && blockIdx.y == 0 && a.clr_a) {
-    for (int q = tid; q < nz; q += NT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
+    for (int q = tid; q < nz; q += SNT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
   }
-  for (int q = tid; q < nz; q += NT)
+  for (int q = tid; q < nz; q += SNT)
     s_thref[q] = (float)(acc_read(a.th_acc + q, kScaleTheta) * a.inv_count);
 
   // software pipeline: plane fields two planes ahead, blend partner one plane ahead
@@ -156,7 +157,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
     // level sums of the previous plane (one thread, fixed order)
     if (a.acc_mode && k > 0 && tid == 0) {
       double sa = 0.0, sb = 0.0;
-      for (int w = 0; w < NW; ++w) { sa += s_red[pb ^ 1][w][0]; sb += s_red[pb ^ 1][w][1]; }
+      for (int w = 0; w < SNW; ++w) { sa += s_red[pb ^ 1][w][0]; sb += s_red[pb ^ 1][w][1]; }
       if (a.acc_mode == 1) { acc_add(a.acc_a + k - 1, sa, kScaleRho); acc_add(a.acc_b + k - 1, sb, kScaleP); }
       else acc_add(a.acc_a + k - 1, sa, kScaleTheta);
     }
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
     {
       const float rr = fmaxf(cc.rho, 1.0e-6f);
       s_uc[pb][ty][tx] = (tx + 1 < BX) ? 0.5f * (cc.uf + s_u[pb][ty][tx + 1]) / rr : 0.0f;
-      s_vc[pb][ty][tx] = (ty + 1 < BY) ? 0.5f * (cc.vf + s_v[pb][ty + 1][tx]) / rr : 0.0f;
+      s_vc[pb][ty][tx] = (ty + 1 < SBY) ? 0.5f * (cc.vf + s_v[pb][ty + 1][tx]) / rr : 0.0f;
       s_wc[pb][ty][tx] = 0.5f * (cc.wf + cn.wf) / rr;
     }
     __syncthreads();
@@ -341,7 +342,7 @@ __global__ void __launch_bounds__(NT) k_slow_stage(const SlowArgs a) {
     if (tid == 0) {
       const int pb = (nz - 1) & 1;
       double sa = 0.0, sb = 0.0;
-      for (int w = 0; w < NW; ++w) { sa += s_red[pb][w][0]; sb += s_red[pb][w][1]; }
+      for (int w = 0; w < SNW; ++w) { sa += s_red[pb][w][0]; sb += s_red[pb][w][1]; }
       if (a.acc_mode == 1) { acc_add(a.acc_a + nz - 1, sa, kScaleRho); acc_add(a.acc_b + nz - 1, sb, kScaleP); }
       else acc_add(a.acc_a + nz - 1, sa, kScaleTheta);
     }
@@ -672,12 +673,15 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
   const bool skip_v0 = gj0 == 0 && !g.per_y;
   // tiles away from the periodic edge rings store without mirror checks
   const bool edge = (g.per_x && (i0 <= 1 || i0 + w >= nx - 1)) || (g.per_y && (j0 <= 1 || j0 + h >= ny - 1));
-  // halo role: 0 west column, 1 east column, 2 south row, 3 north row
+  // halo role: 0 west column, 1 east column, 2 south row, 3 north row.  The 96 halo
+  // cells are spread 12 per warp (lanes 0-11) so every warp reaches the plane barrier
+  // with the same amount of work.
   int role = -1, hi = 0, hj = 0;
-  if (tid < TY) { if (tid < h) { role = 0; hi = i0 - 1; hj = j0 + tid; } }
-  else if (tid < 2 * TY) { if (tid - TY < h) { role = 1; hi = i0 + w; hj = j0 + tid - TY; } }
-  else if (tid < 2 * TY + TX) { if (tid - 2 * TY < w) { role = 2; hi = i0 + tid - 2 * TY; hj = j0 - 1; } }
-  else if (tid < 2 * TY + 2 * TX) { if (tid - 2 * TY - TX < w) { role = 3; hi = i0 + tid - 2 * TY - TX; hj = j0 + h; } }
+  const int hq = tx < 12 ? ty * 12 + tx : -1;
+  if (hq >= 0 && hq < TY) { if (hq < h) { role = 0; hi = i0 - 1; hj = j0 + hq; } }
+  else if (hq >= TY && hq < 2 * TY) { if (hq - TY < h) { role = 1; hi = i0 + w; hj = j0 + hq - TY; } }
+  else if (hq >= 2 * TY && hq < 2 * TY + TX) { if (hq - 2 * TY < w) { role = 2; hi = i0 + hq - 2 * TY; hj = j0 - 1; } }
+  else if (hq >= 2 * TY + TX && hq < 2 * TY + 2 * TX) { if (hq - 2 * TY - TX < w) { role = 3; hi = i0 + hq - 2 * TY - TX; hj = j0 + h; } }
   const int hb = role >= 0 ? gidx(g, hi, hj, 0) : 0;
   const int hr = hj - j0 + 1, hc = hi - i0 + 1;    // smem coordinates of the halo cell
   const bool h_skip = (role == 1 && hi == nx && !g.per_x) || (role == 3 && hj == ny && !g.per_y);
@@ -860,10 +864,13 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
       float d = hd;
       if (hm && !h_skip) d = hd + (-dtf * ((hp - s_p[pb][hr][hc - 1]) * idx));
       s_du[pb][hr - 1][hc - 1] = d;
+      // open east boundary: face nx belongs to no tile; its step value is base + 0
+      if (final_step && h_skip) a.f_u[hb + k * P] = __ldg(a.bu + hb + k * P) + d;
     } else if (role == 3) {  // tile's north Y face
       float d = hd;
       if (hm && !h_skip) d = hd + (-dtf * ((hp - s_p[pb][hr - 1][hc]) * idy));
       s_dv[pb][hr - 1][hc - 1] = d;
+      if (final_step && h_skip) a.f_v[hb + k * P] = __ldg(a.bv + hb + k * P) + d;
     }
     float wn0 = dw0, wn1 = dw1;
     if (k + 1 < nz) {
@@ -938,13 +945,19 @@ __global__ void k_theta_field(const Geom g, const float* rho, const float* rt, f
 
 }  // namespace
 
-cudaError_t launch_slow(const SlowArgs& a, bool terrain, cudaStream_t s) {
-  if (a.g.nz > kMaxNz) return cudaErrorInvalidValue;
-  const dim3 block(BX, BY);
-  const dim3 grid((a.g.nx + 1 + BX - 3) / (BX - 2), (a.g.ny + 1 + BY - 3) / (BY - 2));
-  if (terrain) k_slow_stage<true><<<grid, block, 0, s>>>(a);
-  else k_slow_stage<false><<<grid, block, 0, s>>>(a);
+template <int SBY>
+cudaError_t launch_slow_tile(const SlowArgs& a, bool terrain, cudaStream_t s) {
+  const dim3 block(BX, SBY);
+  const dim3 grid((a.g.nx + 1 + BX - 3) / (BX - 2), (a.g.ny + 1 + SBY - 3) / (SBY - 2));
+  if (terrain) k_slow_stage<true, SBY><<<grid, block, 0, s>>>(a);
+  else k_slow_stage<false, SBY><<<grid, block, 0, s>>>(a);
   return cudaGetLastError();
+}
+
+cudaError_t launch_slow(const SlowArgs& a, bool terrain, cudaStream_t s, int tile_rows) {
+  if (a.g.nz > kMaxNz) return cudaErrorInvalidValue;
+  if (tile_rows == 16) return launch_slow_tile<16>(a, terrain, s);
+  return launch_slow_tile<8>(a, terrain, s);
 }
 
 template <int FBY>

@@ -66,7 +66,8 @@ struct LevelSumArgs {
   const double* base;
 };
 
-cudaError_t launch_slow(const SlowArgs& a, bool terrain, cudaStream_t s);
+// tile_rows: CTA rows of the overlapped slow-stage tile (8 or 16; 32 columns wide).
+cudaError_t launch_slow(const SlowArgs& a, bool terrain, cudaStream_t s, int tile_rows);
 // tile_rows: CTA rows of the acoustic-substep tile (8 or 16; 32 columns wide).
 cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_t s, int tile_rows);
 cudaError_t launch_level_sums(const LevelSumArgs& a, cudaStream_t s);

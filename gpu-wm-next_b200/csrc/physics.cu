@@ -38,24 +38,25 @@ __device__ __forceinline__ void tr_mix(TrCol& c) {
   for (int t = 0; t < NTR; ++t) c.q[t] = c.rq[t] / rr;  // mixing ratio: dry_transport.cu:91-94
 }
 
-__global__ void __launch_bounds__(NT) k_tracer_stage(const TracerArgs a) {
+template <int TBY>
+__global__ void __launch_bounds__(BX * TBY) k_tracer_stage(const TracerArgs a) {
   const Geom& g = a.g;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int gi = blockIdx.x * (BX - 2) - 1 + tx;
-  const int gj = blockIdx.y * (BY - 2) - 1 + ty;
+  const int gj = blockIdx.y * (TBY - 2) - 1 + ty;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const bool valid = gi >= -1 && gi <= nx + 1 && gj >= -1 && gj <= ny + 1;
-  const bool inner = tx >= 1 && tx <= BX - 2 && ty >= 1 && ty <= BY - 2;
+  const bool inner = tx >= 1 && tx <= BX - 2 && ty >= 1 && ty <= TBY - 2;
   const bool own_c = inner && gi >= 0 && gi < nx && gj >= 0 && gj < ny;
   const int base = valid ? gidx(g, gi, gj, 0) : 0;
-  const int ilo = blockIdx.x * (BX - 2), jlo = blockIdx.y * (BY - 2);
+  const int ilo = blockIdx.x * (BX - 2), jlo = blockIdx.y * (TBY - 2);
   const bool edge = (g.per_x && (ilo <= 1 || ilo + BX - 3 >= nx - 1)) ||
-                    (g.per_y && (jlo <= 1 || jlo + BY - 3 >= ny - 1));
+                    (g.per_y && (jlo <= 1 || jlo + TBY - 3 >= ny - 1));
   const float idx = g.inv_dx, idy = g.inv_dy;
   const bool blend = a.q0[0] != nullptr;
 
-  __shared__ float s_q[NTR][2][BY][BX];
-  __shared__ float s_u[2][BY][BX], s_v[2][BY][BX];
+  __shared__ float s_q[NTR][2][TBY][BX];
+  __shared__ float s_u[2][TBY][BX], s_v[2][TBY][BX];
 
   TrCol cm{}, cc = tr_load(a, valid, base, 0), cn = tr_load(a, valid, base, 1);
   TrCol c2 = tr_load(a, valid, base, 2);
@@ -244,10 +245,14 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
 
 }  // namespace
 
-cudaError_t launch_tracer_stage(const TracerArgs& a, cudaStream_t s) {
-  const dim3 block(BX, BY);
-  const dim3 grid((a.g.nx + BX - 3) / (BX - 2), (a.g.ny + BY - 3) / (BY - 2));
-  k_tracer_stage<<<grid, block, 0, s>>>(a);
+cudaError_t launch_tracer_stage(const TracerArgs& a, cudaStream_t s, int tile_rows) {
+  if (tile_rows == 16) {
+    const dim3 grid((a.g.nx + BX - 3) / (BX - 2), (a.g.ny + 16 - 3) / (16 - 2));
+    k_tracer_stage<16><<<grid, dim3(BX, 16), 0, s>>>(a);
+  } else {
+    const dim3 grid((a.g.nx + BX - 3) / (BX - 2), (a.g.ny + 8 - 3) / (8 - 2));
+    k_tracer_stage<8><<<grid, dim3(BX, 8), 0, s>>>(a);
+  }
   return cudaGetLastError();
 }
 

@@ -37,7 +37,8 @@ struct RainArgs {
   double inv_count;
 };
 
-cudaError_t launch_tracer_stage(const TracerArgs& a, cudaStream_t s);
+// tile_rows: CTA rows of the overlapped tracer tile (8 or 16; 32 columns wide).
+cudaError_t launch_tracer_stage(const TracerArgs& a, cudaStream_t s, int tile_rows);
 cudaError_t launch_warm_rain(const RainArgs& a, cudaStream_t s);
 
 }  // namespace gwmb

@@ -150,11 +150,14 @@ int gwm_b200_fast_modes(gwm_b200_ctx* ctx);
 int gwm_b200_slow_tendencies(gwm_b200_ctx* ctx, int member, gwm_b200_fields* host_out);
 /* FP64 budgets of the current state. */
 int gwm_b200_budgets(gwm_b200_ctx* ctx, int member, gwm_b200_budget* out);
-/* Tile shape of a kernel: kernel 1 = acoustic substep; rows 0 = owned 32x16 tiles
- * (flat terrain; terrain falls back to 8), 8 or 16 = overlapped 32-wide tiles of that
- * many rows.  The environment variable GWM_B200_FAST_TILE_ROWS sets
- * the default at context creation. */
+/* Tile shape of a kernel.  kernel 0 = slow stage, 2 = tracer stage: rows 8 or 16
+ * (overlapped 32-wide tiles, default 16).  kernel 1 = acoustic substep: rows 0 = owned
+ * 32x16 tiles (flat terrain; terrain falls back to 8), 8 or 16 = overlapped 32-wide
+ * tiles of that many rows.  The environment variable GWM_B200_FAST_TILE_ROWS sets the
+ * acoustic default at context creation.  The choice changes speed only: every tiling
+ * computes the same values.  gwm_b200_get_tile returns the current rows (or < 0). */
 int gwm_b200_set_tile(gwm_b200_ctx* ctx, int kernel, int rows);
+int gwm_b200_get_tile(const gwm_b200_ctx* ctx, int kernel);
 /* Kernel launches issued by the last step call (for accounting). */
 long long gwm_b200_launch_count(const gwm_b200_ctx* ctx);
 /* Per-kernel CUDA-event timing on the context's stream (no graph while enabled).
