@@ -137,21 +137,32 @@ __device__ __forceinline__ void store_mirrored(float* __restrict__ f, const Geom
 }
 
 // ---------------------------------------------------------------------------
-// Deterministic level sums.  Each CTA reduces its cells in a fixed order (FP64),
-// converts the partial to 64-bit fixed point and adds it with an integer atomic.
-// Integer addition is associative, so the result does not depend on CTA
-// arrival order: reruns are bitwise identical.  Scales keep the largest sums
-// (1.6e7 cells per level) inside int64.
+// Deterministic level sums.  Every cell's value is converted to 64-bit fixed point
+// on its own (v * 2^s is exact in FP32 for a power-of-two scale; the conversion
+// rounds to nearest) and the integers are summed: warp shuffles, a CTA total and one
+// integer atomic per CTA and level.  Integer addition is exact and associative, so a
+// level sum depends only on the cell values: not on CTA arrival order, tile shape or
+// which kernel computed it.  Reruns, and runs with different tile choices, are
+// bitwise identical.  Scales keep the largest sums (1.6e7 cells per level) inside
+// int64.
 constexpr double kScaleRho = 4294967296.0;    // 2^32
 constexpr double kScaleP = 16777216.0;        // 2^24 (pressure perturbations)
 constexpr double kScaleTheta = 268435456.0;   // 2^28
+constexpr float kFxRho = 4294967296.0f;
+constexpr float kFxP = 16777216.0f;
+constexpr float kFxTheta = 268435456.0f;
 
-__device__ __forceinline__ void acc_add(unsigned long long* acc, double v, double scale) {
-  const long long q = __double2ll_rn(v * scale);
+__device__ __forceinline__ long long fx(float v, float scale) { return __float2ll_rn(v * scale); }
+__device__ __forceinline__ void acc_add(unsigned long long* acc, long long q) {
   atomicAdd(acc, (unsigned long long)q);
 }
 __device__ __forceinline__ double acc_read(const unsigned long long* acc, double scale) {
   return (double)(long long)(*acc) / scale;
+}
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
 
 __device__ __forceinline__ float warp_sum_f(float v) {

@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
   __shared__ float s_uc[2][SBY][BX], s_vc[2][SBY][BX], s_wc[2][SBY][BX];
   __shared__ float s_zc[TERRAIN ? 2 : 1][SBY][BX], s_dz[TERRAIN ? 2 : 1][SBY][BX];
   __shared__ float s_thref[kMaxNz];
-  __shared__ double s_red[2][SNW][2];
+  __shared__ long long s_red[2][SNW][2];
 
   if (blockIdx.x == 0 && blockIdx.y == 0 && a.clr_a) {
     for (int q = tid; q < nz; q += SNT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
@@ -156,10 +156,10 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
     __syncthreads();
     // level sums of the previous plane (one thread, fixed order)
     if (a.acc_mode && k > 0 && tid == 0) {
-      double sa = 0.0, sb = 0.0;
+      long long sa = 0, sb = 0;
       for (int w = 0; w < SNW; ++w) { sa += s_red[pb ^ 1][w][0]; sb += s_red[pb ^ 1][w][1]; }
-      if (a.acc_mode == 1) { acc_add(a.acc_a + k - 1, sa, kScaleRho); acc_add(a.acc_b + k - 1, sb, kScaleP); }
-      else acc_add(a.acc_a + k - 1, sa, kScaleTheta);
+      if (a.acc_mode == 1) { acc_add(a.acc_a + k - 1, sa); acc_add(a.acc_b + k - 1, sb); }
+      else acc_add(a.acc_a + k - 1, sa);
     }
     // cell-centred velocities of plane k, halo included: dry_momentum_flux.cu:36-73
     {
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
     }
     __syncthreads();
 
-    double red_a = 0.0, red_b = 0.0;
+    long long red_a = 0, red_b = 0;
     if (inner && valid) {
       const int o = base + k * g.plane;
       // ---- cell: K2 compute_cell_tendencies_kernel (dry_core.cu:62-144)
@@ -207,10 +207,10 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
           store_tile(a.o_rho, g, kCell, gi, gj, k, r1, edge);
           store_tile(a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1, edge);
           if (a.acc_mode == 1) {
-            red_a = r1;
-            red_b = eos_pprime(r1, r1 * th1, a.base, k, nz);
+            red_a = fx(r1, kFxRho);
+            red_b = fx(eos_pprime(r1, r1 * th1, a.base, k, nz), kFxP);
           } else if (a.acc_mode == 2) {
-            red_a = th1;
+            red_a = fx(th1, kFxTheta);
           }
         }
       }
@@ -323,8 +323,8 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
       }
     }
     if (a.acc_mode) {
-      red_a = warp_sum(red_a);
-      red_b = warp_sum(red_b);
+      red_a = warp_sum_ll(red_a);
+      red_b = warp_sum_ll(red_b);
       if ((tid & 31) == 0) { s_red[pb][tid >> 5][0] = red_a; s_red[pb][tid >> 5][1] = red_b; }
     }
     // advance the column window
@@ -341,10 +341,10 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
     __syncthreads();
     if (tid == 0) {
       const int pb = (nz - 1) & 1;
-      double sa = 0.0, sb = 0.0;
+      long long sa = 0, sb = 0;
       for (int w = 0; w < SNW; ++w) { sa += s_red[pb][w][0]; sb += s_red[pb][w][1]; }
-      if (a.acc_mode == 1) { acc_add(a.acc_a + nz - 1, sa, kScaleRho); acc_add(a.acc_b + nz - 1, sb, kScaleP); }
-      else acc_add(a.acc_a + nz - 1, sa, kScaleTheta);
+      if (a.acc_mode == 1) { acc_add(a.acc_a + nz - 1, sa); acc_add(a.acc_b + nz - 1, sb); }
+      else acc_add(a.acc_a + nz - 1, sa);
     }
   }
 }
@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
   __shared__ float s_p[2][FBY][BX], s_du[2][FBY][BX], s_dv[2][FBY][BX];
   __shared__ float s_zc[TERRAIN ? 2 : 1][FBY][BX], s_dz[TERRAIN ? 2 : 1][FBY][BX];
   __shared__ float s_pref[TERRAIN ? 1 : kMaxNz], s_rref[TERRAIN ? 1 : kMaxNz];
-  __shared__ double s_red[2][FNW][2];
+  __shared__ long long s_red[2][FNW][2];
 
   if (blockIdx.x == 0 && blockIdx.y == 0 && a.clr_a) {
     for (int q = tid; q < nz; q += FNT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
@@ -490,10 +490,10 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
     }
     __syncthreads();
     if (acc_mode && k > 0 && tid == 0) {
-      double sa = 0.0, sb = 0.0;
+      long long sa = 0, sb = 0;
       for (int w = 0; w < FNW; ++w) { sa += s_red[pb ^ 1][w][0]; sb += s_red[pb ^ 1][w][1]; }
-      if (acc_mode == 1) { acc_add(a.acc_a + k - 1, sa, kScaleRho); acc_add(a.acc_b + k - 1, sb, kScaleP); }
-      else acc_add(a.acc_a + k - 1, sa, kScaleTheta);
+      if (acc_mode == 1) { acc_add(a.acc_a + k - 1, sa); acc_add(a.acc_b + k - 1, sb); }
+      else acc_add(a.acc_a + k - 1, sa);
     }
     // K12: X-face momentum (dry_fast_modes.cu:160-229)
     float du_new = d0.du;
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
     }
     __syncthreads();
 
-    double red_a = 0.0, red_b = 0.0;
+    long long red_a = 0, red_b = 0;
     if (own_c) {
       // K15: density from the perturbation mass-flux divergence (dry_fast_modes.cu:350-394)
       float rho_new = cc.rho;
@@ -557,10 +557,10 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
         if (k + 1 < nz) store_mirrored(a.dw_out, g, kFaceZ, gi, gj, k + 1, dw_n);
       }
       if (acc_mode == 1) {
-        red_a = rho_new;
-        red_b = eos_pprime(rho_new, rt_new, a.base, k, nz);
+        red_a = fx(rho_new, kFxRho);
+        red_b = fx(eos_pprime(rho_new, rt_new, a.base, k, nz), kFxP);
       } else if (acc_mode == 2) {
-        red_a = theta_of(rho_new, rt_new);
+        red_a = fx(theta_of(rho_new, rt_new), kFxTheta);
       }
     }
     if (own_u) {
@@ -572,8 +572,8 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
       else store_mirrored(a.dv_out, g, kFaceY, gi, gj, k, dv_new);
     }
     if (acc_mode) {
-      red_a = warp_sum(red_a);
-      red_b = warp_sum(red_b);
+      red_a = warp_sum_ll(red_a);
+      red_b = warp_sum_ll(red_b);
       if ((tid & 31) == 0) { s_red[pb][tid >> 5][0] = red_a; s_red[pb][tid >> 5][1] = red_b; }
     }
     dw_c = dw_n;
@@ -591,10 +591,10 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
     __syncthreads();
     if (tid == 0) {
       const int pb = (nz - 1) & 1;
-      double sa = 0.0, sb = 0.0;
+      long long sa = 0, sb = 0;
       for (int w = 0; w < FNW; ++w) { sa += s_red[pb][w][0]; sb += s_red[pb][w][1]; }
-      if (acc_mode == 1) { acc_add(a.acc_a + nz - 1, sa, kScaleRho); acc_add(a.acc_b + nz - 1, sb, kScaleP); }
-      else acc_add(a.acc_a + nz - 1, sa, kScaleTheta);
+      if (acc_mode == 1) { acc_add(a.acc_a + nz - 1, sa); acc_add(a.acc_b + nz - 1, sb); }
+      else acc_add(a.acc_a + nz - 1, sa);
     }
   }
 }
@@ -605,30 +605,30 @@ __global__ void __launch_bounds__(256) k_level_sums(const LevelSumArgs a) {
   const int k = blockIdx.y;
   if (blockIdx.x == 0 && k == 0 && a.clr_a)
     for (int q = threadIdx.x; q < g.nz; q += blockDim.x) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
-  __shared__ double s[8][2];
-  double va = 0.0, vb = 0.0;
+  __shared__ long long s[8][2];
+  long long va = 0, vb = 0;
   const int n = g.nx * g.ny;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
     const int i = q % g.nx, j = q / g.nx;
     const int o = gidx(g, i, j, k);
     const float rho = a.rho[o], rt = a.rt[o];
     if (a.mode == 0) {
-      va += (double)theta_of(rho, rt);
+      va += fx(theta_of(rho, rt), kFxTheta);
     } else {
       const float rtf = rho * theta_of(rho, rt);
-      va += (double)rho;
-      vb += (double)eos_pprime(rho, rtf, a.base, k, g.nz);
+      va += fx(rho, kFxRho);
+      vb += fx(eos_pprime(rho, rtf, a.base, k, g.nz), kFxP);
     }
   }
-  va = warp_sum(va);
-  vb = warp_sum(vb);
+  va = warp_sum_ll(va);
+  vb = warp_sum_ll(vb);
   if ((threadIdx.x & 31) == 0) { s[threadIdx.x >> 5][0] = va; s[threadIdx.x >> 5][1] = vb; }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double ta = 0.0, tb = 0.0;
+    long long ta = 0, tb = 0;
     for (int w = 0; w < 8; ++w) { ta += s[w][0]; tb += s[w][1]; }
-    if (a.mode == 0) acc_add(a.acc_a + k, ta, kScaleTheta);
-    else { acc_add(a.acc_a + k, ta, kScaleRho); acc_add(a.acc_b + k, tb, kScaleP); }
+    acc_add(a.acc_a + k, ta);
+    if (a.mode != 0) acc_add(a.acc_b + k, tb);
   }
 }
 
@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
   __shared__ float s_du[2][TY][TX + 1];
   __shared__ float s_dv[2][TY + 1][TX];
   __shared__ float s_pref[kMaxNz], s_rref[kMaxNz];
-  __shared__ double s_red[2][FW][2];
+  __shared__ long long s_red[2][FW][2];
 
   if (blockIdx.x == 0 && blockIdx.y == 0 && a.clr_a)
     for (int q = tid; q < nz; q += FT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
@@ -742,7 +742,7 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
 
   // K15 density, K10 rho*theta and the stores of plane kk, from the faces computed
   // one iteration earlier (their tiles are published by this iteration's barrier)
-  auto finish_plane = [&](int kk, int pbk, float& sa, float& sb) {
+  auto finish_plane = [&](int kk, int pbk, long long& sa, long long& sb) {
     if (own0) {
       float rn = prho0;
       if (dn) {
@@ -764,8 +764,8 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
         store_tile(a.dv_out, g, kFaceY, gi, gj0, kk, pvn0, edge);
         if (kk + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj0, kk + 1, pwn0, edge);
       }
-      if (acc_mode == 1) { sa = rn; sb = eos_pprime(rn, rt, a.base, kk, nz); }
-      else if (acc_mode == 2) { sa = theta_of(rn, rt); }
+      if (acc_mode == 1) { sa = fx(rn, kFxRho); sb = fx(eos_pprime(rn, rt, a.base, kk, nz), kFxP); }
+      else if (acc_mode == 2) { sa = fx(theta_of(rn, rt), kFxTheta); }
     }
     if (own1) {
       float rn = prho1;
@@ -788,8 +788,8 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
         store_tile(a.dv_out, g, kFaceY, gi, gj1, kk, pvn1, edge);
         if (kk + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj1, kk + 1, pwn1, edge);
       }
-      if (acc_mode == 1) { sa += rn; sb += eos_pprime(rn, rt, a.base, kk, nz); }
-      else if (acc_mode == 2) { sa += theta_of(rn, rt); }
+      if (acc_mode == 1) { sa += fx(rn, kFxRho); sb += fx(eos_pprime(rn, rt, a.base, kk, nz), kFxP); }
+      else if (acc_mode == 2) { sa += fx(theta_of(rn, rt), kFxTheta); }
     }
   };
 
@@ -833,19 +833,19 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
     __syncthreads();
     // ---- plane k-1: density update and stores (its face tiles are now published)
     if (k > 0) {
-      float sa = 0.f, sb = 0.f;
+      long long sa = 0, sb = 0;
       finish_plane(k - 1, pb ^ 1, sa, sb);
       if (acc_mode) {
-        const float wa = warp_sum_f(sa), wb = warp_sum_f(sb);
-        if (tx == 0) { s_red[pb ^ 1][ty][0] = (double)wa; s_red[pb ^ 1][ty][1] = (double)wb; }
+        const long long wa = warp_sum_ll(sa), wb = warp_sum_ll(sb);
+        if (tx == 0) { s_red[pb ^ 1][ty][0] = wa; s_red[pb ^ 1][ty][1] = wb; }
       }
     }
     // level sums of plane k-2, whose warp partials the previous barrier published
     if (acc_mode && k > 1 && tid == 0) {
-      double sa = 0.0, sb = 0.0;
+      long long sa = 0, sb = 0;
       for (int q = 0; q < FW; ++q) { sa += s_red[pb][q][0]; sb += s_red[pb][q][1]; }
-      if (acc_mode == 1) { acc_add(a.acc_a + k - 2, sa, kScaleRho); acc_add(a.acc_b + k - 2, sb, kScaleP); }
-      else acc_add(a.acc_a + k - 2, sa, kScaleTheta);
+      if (acc_mode == 1) { acc_add(a.acc_a + k - 2, sa); acc_add(a.acc_b + k - 2, sb); }
+      else acc_add(a.acc_a + k - 2, sa);
     }
     if (!active) break;
     // ---- plane k faces: K12/K13 horizontal momenta, K14 vertical momentum at face k+1
@@ -899,10 +899,10 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
     __syncthreads();
     if (tid == 0) {
       const int pb = (nz - 1) & 1;
-      double sa = 0.0, sb = 0.0;
+      long long sa = 0, sb = 0;
       for (int q = 0; q < FW; ++q) { sa += s_red[pb][q][0]; sb += s_red[pb][q][1]; }
-      if (acc_mode == 1) { acc_add(a.acc_a + nz - 1, sa, kScaleRho); acc_add(a.acc_b + nz - 1, sb, kScaleP); }
-      else acc_add(a.acc_a + nz - 1, sa, kScaleTheta);
+      if (acc_mode == 1) { acc_add(a.acc_a + nz - 1, sa); acc_add(a.acc_b + nz - 1, sb); }
+      else acc_add(a.acc_a + nz - 1, sa);
     }
   }
 }

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
   const int ilo = blockIdx.x * RB;
   const bool edge = (g.per_x && (ilo <= 1 || ilo + RB - 1 >= g.nx - 1)) ||
                     (g.per_y && (gj <= 1 || gj >= g.ny - 1));
-  __shared__ double s_th[kMaxNz][RB / 32];
+  __shared__ long long s_th[kMaxNz][RB / 32];
   float incoming = 0.0f;
   // one-cell-ahead prefetch down the column
   float n_rho = 0.f, n_rt = 0.f, n_qv = 0.f, n_qc = 0.f, n_qr = 0.f;
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
     n_rho = __ldg(a.rho + o); n_rt = a.rt[o]; n_qv = a.qv[o]; n_qc = a.qc[o]; n_qr = a.qr[o];
   }
   for (int k = g.nz - 1; k >= 0; --k) {
-    double th_sum = 0.0;
+    long long th_sum = 0;
     const float c_rho = n_rho, c_rt = n_rt, c_qv = n_qv, c_qc = n_qc, c_qr = n_qr;
     if (active && k > 0) {
       const int o1 = gidx(g, gi, gj, k - 1);
@@ -220,10 +220,10 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
       store_tile(a.qc, g, kCell, gi, gj, k, rho * qc, edge);
       store_tile(a.qr, g, kCell, gi, gj, k, rqr, edge);
       store_tile(a.rt, g, kCell, gi, gj, k, rt_new, edge);
-      th_sum = (double)theta_of(rho_d, rt_new);
+      th_sum = fx(theta_of(rho_d, rt_new), kFxTheta);
     }
     if (a.th_acc) {
-      th_sum = warp_sum(th_sum);
+      th_sum = warp_sum_ll(th_sum);
       if ((threadIdx.x & 31) == 0) s_th[k][threadIdx.x >> 5] = th_sum;
     }
   }
@@ -236,9 +236,9 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
   if (a.th_acc) {
     __syncthreads();
     for (int k = threadIdx.x; k < g.nz; k += RB) {
-      double t = 0.0;
+      long long t = 0;
       for (int w = 0; w < RB / 32; ++w) t += s_th[k][w];
-      acc_add(a.th_acc + k, t, kScaleTheta);
+      acc_add(a.th_acc + k, t);
     }
   }
 }
