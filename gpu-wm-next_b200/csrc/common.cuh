@@ -74,14 +74,15 @@ __device__ __forceinline__ float eos_pprime(float rho, float rt, const double* _
   const double d = fma((double)rt, __ldg(base + nz + k), -1.0);
   const double pref = __ldg(base + 2 * nz + k);
   if (rho >= 1.0e-6f && fabs(d) < 0.0625) {
-    // C(g, n), n = 7 .. 1, for g = 1.0f / (1.0f - 0.2854f)
-    double s = -0.0045925100129794545;
-    s = fma(s, d, 0.0069876670302162856);
-    s = fma(s, d, -0.011644120505748048);
-    s = fma(s, d, 0.022387238647368683);
-    s = fma(s, d, -0.055946570454669185);
-    s = fma(s, d, 0.2794461309425813);
-    s = fma(s, d, 1.3993843793869019);
+    // C(g, n), n = 1 .. 7, for g = 1.0f / (1.0f - 0.2854f); Estrin's scheme keeps the
+    // dependent FP64 chain three operations deep instead of seven (Horner)
+    const double d2 = d * d, d4 = d2 * d2;
+    const double a = fma(0.2794461309425813, d, 1.3993843793869019);
+    const double b = fma(0.022387238647368683, d, -0.055946570454669185);
+    const double c = fma(0.0069876670302162856, d, -0.011644120505748048);
+    const double lo = fma(b, d2, a);
+    const double hi = fma(-0.0045925100129794545, d2, c);
+    const double s = fma(hi, d4, lo);
     return (float)(pref * (s * d));
   }
   return (float)((double)eos_pressure(rho, rt) - pref);
@@ -159,6 +160,31 @@ __device__ __forceinline__ void acc_add(unsigned long long* acc, long long q) {
 __device__ __forceinline__ double acc_read(const unsigned long long* acc, double scale) {
   return (double)(long long)(*acc) / scale;
 }
+// Per-thread fixed-point accumulator for at most 4 cells (the warp's sum of lo
+// parts must stay below 2^32), reduced across
+// the warp with two 32-bit integer reductions.  A cell's fixed-point value
+// x = rint(v * scale) (the integer fx() returns) is split as x = hi * 2^24 + lo
+// with 0 <= lo < 2^24; every step is exact in FP32 (x and hi * 2^24 are integers
+// representable in FP32, their difference is below 2^24).  The warp total
+// sum(hi) * 2^24 + sum(lo) therefore equals the int64 sum of fx() over the same
+// cells, bit for bit, at a fraction of the cost of 64-bit shuffles.
+struct FxAcc {
+  int hi = 0;
+  unsigned lo = 0;
+  __device__ __forceinline__ void add(float v, float scale) {
+    const float x = rintf(v * scale);
+    const float h = floorf(x * 5.9604644775390625e-08f);  // 2^-24
+    hi += (int)h;
+    lo += (unsigned)fmaf(-h, 16777216.0f, x);
+  }
+  // warp total (all lanes get it); every lane of the warp must call it
+  __device__ __forceinline__ long long warp_total() const {
+    const int sh = __reduce_add_sync(0xffffffffu, hi);
+    const unsigned sl = __reduce_add_sync(0xffffffffu, lo);
+    return (long long)sh * 16777216LL + (long long)sl;
+  }
+};
+
 __device__ __forceinline__ long long warp_sum_ll(long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
     }
     __syncthreads();
 
-    long long red_a = 0, red_b = 0;
+    FxAcc red_a, red_b;
     if (inner && valid) {
       const int o = base + k * g.plane;
       // ---- cell: K2 compute_cell_tendencies_kernel (dry_core.cu:62-144)
@@ -207,10 +207,10 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
           store_tile(a.o_rho, g, kCell, gi, gj, k, r1, edge);
           store_tile(a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1, edge);
           if (a.acc_mode == 1) {
-            red_a = fx(r1, kFxRho);
-            red_b = fx(eos_pprime(r1, r1 * th1, a.base, k, nz), kFxP);
+            red_a.add(r1, kFxRho);
+            red_b.add(eos_pprime(r1, r1 * th1, a.base, k, nz), kFxP);
           } else if (a.acc_mode == 2) {
-            red_a = fx(th1, kFxTheta);
+            red_a.add(th1, kFxTheta);
           }
         }
       }
@@ -323,9 +323,8 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
       }
     }
     if (a.acc_mode) {
-      red_a = warp_sum_ll(red_a);
-      red_b = warp_sum_ll(red_b);
-      if ((tid & 31) == 0) { s_red[pb][tid >> 5][0] = red_a; s_red[pb][tid >> 5][1] = red_b; }
+      const long long ta = red_a.warp_total(), tb = red_b.warp_total();
+      if ((tid & 31) == 0) { s_red[pb][tid >> 5][0] = ta; s_red[pb][tid >> 5][1] = tb; }
     }
     // advance the column window
     cm = cc;
@@ -537,7 +536,7 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
     }
     __syncthreads();
 
-    long long red_a = 0, red_b = 0;
+    FxAcc red_a, red_b;
     if (own_c) {
       // K15: density from the perturbation mass-flux divergence (dry_fast_modes.cu:350-394)
       float rho_new = cc.rho;
@@ -557,10 +556,10 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
         if (k + 1 < nz) store_mirrored(a.dw_out, g, kFaceZ, gi, gj, k + 1, dw_n);
       }
       if (acc_mode == 1) {
-        red_a = fx(rho_new, kFxRho);
-        red_b = fx(eos_pprime(rho_new, rt_new, a.base, k, nz), kFxP);
+        red_a.add(rho_new, kFxRho);
+        red_b.add(eos_pprime(rho_new, rt_new, a.base, k, nz), kFxP);
       } else if (acc_mode == 2) {
-        red_a = fx(theta_of(rho_new, rt_new), kFxTheta);
+        red_a.add(theta_of(rho_new, rt_new), kFxTheta);
       }
     }
     if (own_u) {
@@ -572,9 +571,8 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
       else store_mirrored(a.dv_out, g, kFaceY, gi, gj, k, dv_new);
     }
     if (acc_mode) {
-      red_a = warp_sum_ll(red_a);
-      red_b = warp_sum_ll(red_b);
-      if ((tid & 31) == 0) { s_red[pb][tid >> 5][0] = red_a; s_red[pb][tid >> 5][1] = red_b; }
+      const long long ta = red_a.warp_total(), tb = red_b.warp_total();
+      if ((tid & 31) == 0) { s_red[pb][tid >> 5][0] = ta; s_red[pb][tid >> 5][1] = tb; }
     }
     dw_c = dw_n;
     d0 = d1;
@@ -674,10 +672,11 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
   // tiles away from the periodic edge rings store without mirror checks
   const bool edge = (g.per_x && (i0 <= 1 || i0 + w >= nx - 1)) || (g.per_y && (j0 <= 1 || j0 + h >= ny - 1));
   // halo role: 0 west column, 1 east column, 2 south row, 3 north row.  The 96 halo
-  // cells are spread 12 per warp (lanes 0-11) so every warp reaches the plane barrier
-  // with the same amount of work.
+  // cells go to threads 0-95, i.e. whole warps 0-2: spreading them over all warps
+  // balances the barrier but makes every warp execute the divergent halo path, which
+  // costs more issue slots than the barrier wait it saves.
   int role = -1, hi = 0, hj = 0;
-  const int hq = tx < 12 ? ty * 12 + tx : -1;
+  const int hq = tid < 2 * TY + 2 * TX ? tid : -1;
   if (hq >= 0 && hq < TY) { if (hq < h) { role = 0; hi = i0 - 1; hj = j0 + hq; } }
   else if (hq >= TY && hq < 2 * TY) { if (hq - TY < h) { role = 1; hi = i0 + w; hj = j0 + hq - TY; } }
   else if (hq >= 2 * TY && hq < 2 * TY + TX) { if (hq - 2 * TY < w) { role = 2; hi = i0 + hq - 2 * TY; hj = j0 - 1; } }
@@ -742,7 +741,7 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
 
   // K15 density, K10 rho*theta and the stores of plane kk, from the faces computed
   // one iteration earlier (their tiles are published by this iteration's barrier)
-  auto finish_plane = [&](int kk, int pbk, long long& sa, long long& sb) {
+  auto finish_plane = [&](int kk, int pbk, FxAcc& sa, FxAcc& sb) {
     if (own0) {
       float rn = prho0;
       if (dn) {
@@ -764,8 +763,8 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
         store_tile(a.dv_out, g, kFaceY, gi, gj0, kk, pvn0, edge);
         if (kk + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj0, kk + 1, pwn0, edge);
       }
-      if (acc_mode == 1) { sa = fx(rn, kFxRho); sb = fx(eos_pprime(rn, rt, a.base, kk, nz), kFxP); }
-      else if (acc_mode == 2) { sa = fx(theta_of(rn, rt), kFxTheta); }
+      if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime(rn, rt, a.base, kk, nz), kFxP); }
+      else if (acc_mode == 2) { sa.add(theta_of(rn, rt), kFxTheta); }
     }
     if (own1) {
       float rn = prho1;
@@ -788,8 +787,8 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
         store_tile(a.dv_out, g, kFaceY, gi, gj1, kk, pvn1, edge);
         if (kk + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj1, kk + 1, pwn1, edge);
       }
-      if (acc_mode == 1) { sa += fx(rn, kFxRho); sb += fx(eos_pprime(rn, rt, a.base, kk, nz), kFxP); }
-      else if (acc_mode == 2) { sa += fx(theta_of(rn, rt), kFxTheta); }
+      if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime(rn, rt, a.base, kk, nz), kFxP); }
+      else if (acc_mode == 2) { sa.add(theta_of(rn, rt), kFxTheta); }
     }
   };
 
@@ -833,10 +832,10 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
     __syncthreads();
     // ---- plane k-1: density update and stores (its face tiles are now published)
     if (k > 0) {
-      long long sa = 0, sb = 0;
+      FxAcc sa, sb;
       finish_plane(k - 1, pb ^ 1, sa, sb);
       if (acc_mode) {
-        const long long wa = warp_sum_ll(sa), wb = warp_sum_ll(sb);
+        const long long wa = sa.warp_total(), wb = sb.warp_total();
         if (tx == 0) { s_red[pb ^ 1][ty][0] = wa; s_red[pb ^ 1][ty][1] = wb; }
       }
     }

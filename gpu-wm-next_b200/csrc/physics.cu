@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
     n_rho = __ldg(a.rho + o); n_rt = a.rt[o]; n_qv = a.qv[o]; n_qc = a.qc[o]; n_qr = a.qr[o];
   }
   for (int k = g.nz - 1; k >= 0; --k) {
-    long long th_sum = 0;
+    FxAcc th_sum;
     const float c_rho = n_rho, c_rt = n_rt, c_qv = n_qv, c_qc = n_qc, c_qr = n_qr;
     if (active && k > 0) {
       const int o1 = gidx(g, gi, gj, k - 1);
@@ -220,11 +220,11 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
       store_tile(a.qc, g, kCell, gi, gj, k, rho * qc, edge);
       store_tile(a.qr, g, kCell, gi, gj, k, rqr, edge);
       store_tile(a.rt, g, kCell, gi, gj, k, rt_new, edge);
-      th_sum = fx(theta_of(rho_d, rt_new), kFxTheta);
+      th_sum.add(theta_of(rho_d, rt_new), kFxTheta);
     }
     if (a.th_acc) {
-      th_sum = warp_sum_ll(th_sum);
-      if ((threadIdx.x & 31) == 0) s_th[k][threadIdx.x >> 5] = th_sum;
+      const long long t = th_sum.warp_total();
+      if ((threadIdx.x & 31) == 0) s_th[k][threadIdx.x >> 5] = t;
     }
   }
   if (active && a.fallout_mode && a.precip) {  // compensated FP64 surface accumulation

@@ -1,0 +1,162 @@
+"""Generate golden vectors from the reference implementation itself.
+
+Each case builds an initial state with the library's case builders (host code),
+writes it as a case file, runs ``oracle/_ref/gwm_ref_golden`` (the reference's own
+step operators compiled from its sources by ``make -C oracle ref``; it needs a
+GPU because the reference runs its kernels on managed memory) and stores inputs,
+parameters and outputs in ``ref_<case>.npz``.  The reference's level-mean
+reduction uses float atomics, so its output is reproducible only to rounding;
+the tests compare against it with tolerances, never bitwise.
+
+Usage (on a machine with a GPU and the built driver):
+    python tests/golden/make_golden.py --out tests/golden
+"""
+import argparse
+import importlib
+import json
+import os
+import struct
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "gwm_ref_golden")
+
+# name -> (grid, case kind, case params, terrain, step, moist/rain, steps)
+CASES = {
+    "bubble_periodic": dict(
+        grid=dict(nx=24, ny=20, nz=16, dx=500.0, dy=500.0, z_top=8000.0),
+        kind="hydrostatic_warm_bubble",
+        params=dict(rho_surface=1.16123, theta_ref=300.0, center_z_fraction=0.25,
+                    radius_x_fraction=0.2, radius_y_fraction=0.2, radius_z_fraction=0.2,
+                    theta_perturbation=2.0),
+        step=dict(dt=1.0, fast_substeps=3), steps=3),
+    "ranks_open_wind": dict(
+        grid=dict(nx=22, ny=18, nz=12, dx=1000.0, dy=1000.0, z_top=10000.0,
+                  periodic_x=False, periodic_y=False, ranks_x=2, ranks_y=2),
+        kind="hydrostatic_warm_bubble",
+        params=dict(rho_surface=1.16123, theta_ref=300.0, center_x_fraction=0.4, center_z_fraction=0.3, radius_x_fraction=0.2,
+                    radius_y_fraction=0.25, radius_z_fraction=0.25, theta_perturbation=1.5),
+        wind=(4.0, -2.0), step=dict(dt=1.0, fast_substeps=4), steps=3),
+    "terrain_cosine": dict(
+        grid=dict(nx=32, ny=12, nz=14, dx=1000.0, dy=1000.0, z_top=12000.0, periodic_y=True),
+        kind="mountain_wave_background",
+        params=dict(rho_surface=1.16123, theta_ref=300.0, u_background=8.0),
+        terrain=dict(kind="cosine_mountain", height=400.0, half_width_x=0.2, half_width_y=0.5),
+        step=dict(dt=1.0, fast_substeps=4), steps=2),
+    "fast_off": dict(
+        grid=dict(nx=16, ny=16, nz=12, dx=500.0, dy=500.0, z_top=6000.0),
+        kind="hydrostatic_warm_bubble",
+        params=dict(rho_surface=1.16123, theta_ref=300.0, radius_x_fraction=0.25,
+                    radius_y_fraction=0.25, radius_z_fraction=0.25, theta_perturbation=1.0),
+        step=dict(dt=0.5, fast_substeps=2, fast_modes=False), steps=2),
+    "moist_metric": dict(
+        grid=dict(nx=20, ny=16, nz=16, dx=2000.0, dy=2000.0, z_top=8000.0),
+        kind="moist_sounding",
+        params=dict(theta_ref=300.0, relative_humidity=1.03, noise_rms_k=0.5, seed=3),
+        step=dict(dt=2.0, fast_substeps=4), moist=True,
+        rain=dict(mode=1, terminal_velocity=12.0), steps=3),
+    "moist_nominal": dict(
+        grid=dict(nx=16, ny=12, nz=12, dx=2000.0, dy=2000.0, z_top=6000.0),
+        kind="moist_sounding",
+        params=dict(theta_ref=300.0, relative_humidity=1.05, noise_rms_k=0.3, seed=7),
+        step=dict(dt=2.0, fast_substeps=3), moist=True,
+        rain=dict(mode=2, terminal_velocity=5.0, layer_depth=500.0), steps=2),
+}
+
+RAIN_DEFAULTS = dict(mode=1, relax=1.0, autoconv_threshold=1.0e-4, autoconv_rate=1.0e-3,
+                     evap_rate=5.0e-3, terminal_velocity=0.0, layer_depth=0.0, latent=True)
+STEP_DEFAULTS = dict(dt=2.0, fast_substeps=1, gravity=9.81, fast_hmom=True, fast_density=True,
+                     fast_modes=True)
+
+
+def case_state(gwm, spec):
+    """Initial fields (float32, global C order) and terrain for a case spec."""
+    gkw = dict(spec["grid"])
+    terrain = np.zeros((gkw["ny"], gkw["nx"]), dtype=np.float32)
+    if "terrain" in spec:
+        t = dict(spec["terrain"])
+        kind = t.pop("kind")
+        terrain = gwm.build_terrain(kind, gkw["nx"], gkw["ny"], gkw["dx"], gkw["dy"], **t)
+        gkw["terrain"] = terrain
+    g = gwm.GridSpec(**gkw)
+    moist = spec.get("moist", False)
+    s = gwm.build_case(spec["kind"], g, gwm.CaseParams(**spec["params"]), moist=moist)
+    if "wind" in spec:  # uniform wind on the bubble: face momentum = face-mean density * wind
+        ub, vb = spec["wind"]
+        r = s["rho"]
+        ru = np.concatenate([r[:, :, :1], 0.5 * (r[:, :, 1:] + r[:, :, :-1]), r[:, :, -1:]], axis=2)
+        rv = np.concatenate([r[:, :1, :], 0.5 * (r[:, 1:, :] + r[:, :-1, :]), r[:, -1:, :]], axis=1)
+        s["u"] = (ru * ub).astype(np.float32)
+        s["v"] = (rv * vb).astype(np.float32)
+    return s, terrain
+
+
+def write_case(path, spec, state, terrain):
+    g = spec["grid"]
+    st = dict(STEP_DEFAULTS, **spec["step"])
+    rn = dict(RAIN_DEFAULTS, **spec.get("rain", {}))
+    moist = spec.get("moist", False)
+    hdr = struct.pack("<8s16i12d", b"GWMCASE1", g["nx"], g["ny"], g["nz"], g.get("ranks_x", 1),
+                      g.get("ranks_y", 1), int(g.get("periodic_x", True)), int(g.get("periodic_y", True)),
+                      st["fast_substeps"], int(st["fast_hmom"]), int(st["fast_density"]),
+                      int(st["fast_modes"]), spec["steps"], int(moist), rn["mode"] if moist else 0,
+                      int(rn["latent"]), 0,
+                      g["dx"], g["dy"], g["z_top"], g.get("terrain_taper_eta", 0.25), st["dt"],
+                      st["gravity"], rn["relax"], rn["autoconv_threshold"], rn["autoconv_rate"],
+                      rn["evap_rate"], rn["terminal_velocity"], rn["layer_depth"])
+    keys = ("rho", "rho_theta", "u", "v", "w") + (("qv", "qc", "qr") if moist else ())
+    with open(path, "wb") as f:
+        f.write(hdr)
+        f.write(np.ascontiguousarray(terrain, dtype=np.float32).tobytes())
+        for k in keys:
+            f.write(np.ascontiguousarray(state[k], dtype=np.float32).tobytes())
+
+
+def read_out(path, spec, shapes):
+    moist = spec.get("moist", False)
+    keys = ("rho", "rho_theta", "u", "v", "w") + (("qv", "qc", "qr", "precip") if moist else ())
+    raw = open(path, "rb").read()
+    assert raw[:8] == b"GWMOUT01", "bad output header"
+    off, out = 8, {}
+    for k in keys:
+        n = int(np.prod(shapes[k]))
+        out[k] = np.frombuffer(raw, dtype=np.float32, count=n, offset=off).reshape(shapes[k]).copy()
+        off += 4 * n
+    assert off == len(raw), "output size mismatch"
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
+    ap.add_argument("--cases", nargs="*", default=list(CASES))
+    args = ap.parse_args()
+    if not os.path.exists(DRIVER):
+        sys.exit(f"{DRIVER} missing: build it with `make -C oracle ref`")
+    sys.path.insert(0, ROOT)
+    gwm = importlib.import_module("gpu-wm-next_b200")
+    os.makedirs(args.out, exist_ok=True)
+    with tempfile.TemporaryDirectory() as tmp:
+        for name in args.cases:
+            spec = CASES[name]
+            state, terrain = case_state(gwm, spec)
+            cpath, opath = os.path.join(tmp, name + ".case"), os.path.join(tmp, name + ".out")
+            write_case(cpath, spec, state, terrain)
+            subprocess.run([DRIVER, cpath, opath], check=True, timeout=600)
+            shapes = gwm.GridSpec(**{k: v for k, v in spec["grid"].items()}).shapes()
+            out = read_out(opath, spec, shapes)
+            arrays = {"in_" + k: np.asarray(v, dtype=np.float32) for k, v in state.items() if k != "precip"}
+            arrays.update({"out_" + k: v for k, v in out.items()})
+            arrays["terrain"] = terrain
+            np.savez_compressed(os.path.join(args.out, f"ref_{name}.npz"),
+                                spec=np.frombuffer(json.dumps(spec).encode(), dtype=np.uint8), **arrays)
+            fin = all(np.isfinite(v).all() for v in out.values())
+            print(f"{name}: wrote ref_{name}.npz (finite={fin})", flush=True)
+
+
+if __name__ == "__main__":
+    main()
