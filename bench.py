@@ -198,6 +198,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels directly (profiling)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default tiles (no autotune)")
+    ap.add_argument("--fast-tile", type=int, default=None,
+                    help="acoustic-substep kernel (0 owned tile, 3 TMA-fed, 8/16 overlapped); implies --no-tune")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -223,6 +225,9 @@ def main():
     model.set_stream(stream.cuda_stream)
     model.upload(state)
     tiles = None
+    if args.fast_tile is not None:
+        args.no_tune = True
+        model.set_tile("fast_substep", args.fast_tile)
     if not args.no_tune:
         # pick each stencil kernel's tile by timing it, then restart from the initial state
         with torch.cuda.stream(stream):

@@ -18,8 +18,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
+
+#include <cuda.h>
 
 #include "../../include/gwm_b200.h"
 #include "common.cuh"
@@ -60,6 +64,14 @@ struct Member {
   ReduceOut* red_out = nullptr;
   int ring = 0;
   bool theta_valid = false;
+  int* err = nullptr;                // device error word (bounded waits that gave up)
+  // TMA descriptors of the substep's buffers: (buffer, box kind 0 cell / 1 face / 2 own, map)
+  std::vector<std::tuple<const float*, int, CUtensorMap>> tmaps;
+  const CUtensorMap* tmap(const float* buf, int kind) const {
+    for (const auto& t : tmaps)
+      if (std::get<0>(t) == buf && std::get<1>(t) == kind) return &std::get<2>(t);
+    return nullptr;
+  }
 
   unsigned long long* slot(int s) { return acc + (size_t)(((s % 3) + 3) % 3) * kSlot; }
 };
@@ -183,6 +195,58 @@ std::vector<float> pad_metric(const Member& M, const std::vector<float>& src, in
   return out;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn tensor_map_encoder() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// 3-D map over one padded field (pitch x rows x (nz+1) FP32) with an (bx, by, 1) box.
+bool encode_field_map(CUtensorMap* out, const float* base, const Geom& g, int bx, int by) {
+  const EncodeTiledFn fn = tensor_map_encoder();
+  if (!fn || (reinterpret_cast<uintptr_t>(base) & 15) || (g.pitch * 4) % 16) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)g.rows, (cuuint64_t)(g.nz + 1)};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.pitch * 4, (cuuint64_t)g.plane * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Maps of every buffer the flat-terrain TMA substep may read (false if unavailable).
+bool build_substep_maps(Member& M) {
+  M.tmaps.clear();
+  const int* boxes[3] = {kTmaCellBox, kTmaFaceBox, kTmaOwnBox};
+  auto add = [&](const float* buf, int kind) {
+    CUtensorMap m;
+    if (!encode_field_map(&m, buf, M.g, boxes[kind][0], boxes[kind][1])) return false;
+    M.tmaps.emplace_back(buf, kind, m);
+    return true;
+  };
+  bool ok = true;
+  for (int i = 0; i < 2; ++i) {
+    ok = ok && add(M.R[i], 0) && add(M.TH[i], 0);
+    ok = ok && add(M.D[i][0], 1) && add(M.D[i][1], 1) && add(M.D[i][2], 2);
+    for (int f = 0; f < 3; ++f) ok = ok && add(M.B[i][f], 2);
+  }
+  for (int f = 2; f < 5; ++f) ok = ok && add(M.Q[f], 2);  // bases of the stand-alone fast modes
+  if (!ok) M.tmaps.clear();
+  return ok;
+}
+
 int alloc_member(gwm_b200_ctx* c, Member& M) {
   const gwm_b200_grid_desc& d = M.gd;
   Geom& g = M.g;
@@ -205,7 +269,7 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   const size_t extra = ((2 * plane2 * sizeof(double) + 255) / 256) * 256 +
                        3 * kSlot * sizeof(unsigned long long) + owned_max * sizeof(float) +
                        3 * kReduceBlocks * sizeof(double) + 32 * sizeof(ReduceOut) + 4096 +
-                       3 * 4 * (kMaxNz + 1) * sizeof(float) + 3 * kMaxNz * sizeof(double) + 256;
+                       3 * 4 * (kMaxNz + 1) * sizeof(float) + 3 * kMaxNz * sizeof(double) + 512;
   const size_t total = nfields * fbytes + extra;
   CK(cudaMalloc(&M.block, total));
   CK(cudaMemsetAsync(M.block, 0, total, c->stream));
@@ -228,6 +292,7 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   M.staging = (float*)take(owned_max * sizeof(float));
   M.red_part = (double*)take(3 * kReduceBlocks * sizeof(double));
   M.red_out = (ReduceOut*)take(32 * sizeof(ReduceOut));
+  M.err = (int*)take(sizeof(int));
   // metrics
   const HostMetrics H = build_metrics(M);
   if (M.terrain_active) {
@@ -252,7 +317,48 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
     CK(cudaMemcpy(M.idf, idf.data(), idf.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
   if ((size_t)(p - M.block) > total) return fail(c, GWM_B200_ERR_ARG, "internal: buffer plan overflow");
+  if (!M.terrain_active) build_substep_maps(M);  // empty when TMA descriptors are unavailable
   CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+constexpr int kFastTma = 3;  // fast_tile_rows value selecting the TMA-fed substep
+
+// One acoustic substep: the TMA-fed kernel when selected on flat terrain, else the
+// owned-tile or overlapped-tile kernels.
+cudaError_t launch_substep(gwm_b200_ctx* c, const Member& M, const FastArgs& f, bool first, bool terr) {
+  if (!terr && c->fast_tile_rows == kFastTma) {
+    FastMaps m{};
+    const bool fin = f.final_kind == 2;
+    const CUtensorMap* rho = M.tmap(f.rho_in, 0);
+    const CUtensorMap* th = M.tmap(f.th, 0);
+    const CUtensorMap* du = first ? nullptr : M.tmap(f.du_in, 1);
+    const CUtensorMap* dv = first ? nullptr : M.tmap(f.dv_in, 1);
+    const CUtensorMap* dw = first ? nullptr : M.tmap(f.dw_in, 2);
+    const CUtensorMap* bu = fin ? M.tmap(f.bu, 2) : nullptr;
+    const CUtensorMap* bv = fin ? M.tmap(f.bv, 2) : nullptr;
+    const CUtensorMap* bw = fin ? M.tmap(f.bw, 2) : nullptr;
+    if (!rho || !th || (!first && (!du || !dv || !dw)) || (fin && (!bu || !bv || !bw)))
+      return cudaErrorInvalidValue;
+    m.rho = *rho; m.th = *th;
+    if (!first) { m.du = *du; m.dv = *dv; m.dw = *dw; }
+    if (fin) { m.bu = *bu; m.bv = *bv; m.bw = *bw; }
+    return launch_fast_tma(f, m, first, c->stream);
+  }
+  return launch_fast(f, first, terr, c->stream, c->fast_tile_rows);
+}
+
+// Reads and clears the device error words; call after the stream has drained.
+int check_device_errors(gwm_b200_ctx* c) {
+  for (auto& M : c->m) {
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, M.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (e) {
+      CK(cudaMemsetAsync(M.err, 0, sizeof(int), c->stream));
+      return fail(c, GWM_B200_ERR_TIMEOUT, "a bounded wait in the acoustic substep gave up (tile load did not complete)");
+    }
+  }
   return GWM_B200_OK;
 }
 
@@ -381,7 +487,8 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
       f.acc_a = M.slot(M.ring + 1); f.acc_b = M.slot(M.ring + 1) + kMaxNz;
       f.clr_a = M.slot(M.ring + 2); f.clr_b = M.slot(M.ring + 2) + kMaxNz;
       f.zc = M.zc; f.idz_c = M.idc; f.idz_f = M.idf; f.base = M.base;
-      LAUNCH(launch_fast(f, n == 0, terr, c->stream, c->fast_tile_rows), "fast substep");
+      f.err = M.err;
+      LAUNCH(launch_substep(c, M, f, n == 0, terr), "fast substep");
       M.ring = (M.ring + 1) % 3;
       rcur ^= 1;
       dcur = dout;
@@ -476,6 +583,7 @@ int gwm_b200_create(const gwm_b200_grid_desc* grids, const gwm_b200_member_desc*
   cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete c; return GWM_B200_ERR_CUDA; }
   c->stream = c->own_stream;
+  if (init_fast_tma() != cudaSuccess) { cudaStreamDestroy(c->own_stream); delete c; return GWM_B200_ERR_CUDA; }
   c->m.resize(n_members);
   for (int i = 0; i < n_members; ++i) {
     Member& M = c->m[i];
@@ -536,7 +644,7 @@ int gwm_b200_set_stream(gwm_b200_ctx* c, void* stream) {
 int gwm_b200_synchronize(gwm_b200_ctx* c) {
   if (!c) return GWM_B200_ERR_ARG;
   CK(cudaStreamSynchronize(c->stream));
-  return GWM_B200_OK;
+  return check_device_errors(c);
 }
 
 int gwm_b200_use_graph(gwm_b200_ctx* c, int enable) {
@@ -550,9 +658,13 @@ long long gwm_b200_launch_count(const gwm_b200_ctx* c) { return c ? c->launches 
 
 int gwm_b200_set_tile(gwm_b200_ctx* c, int kernel, int rows) {
   if (!c) return GWM_B200_ERR_ARG;
-  const bool ok = kernel == 1 ? (rows == 0 || rows == 8 || rows == 16)
+  const bool ok = kernel == 1 ? (rows == 0 || rows == kFastTma || rows == 8 || rows == 16)
                               : (kernel == 0 || kernel == 2) && (rows == 8 || rows == 16);
   if (!ok) return GWM_B200_ERR_ARG;
+  if (kernel == 1 && rows == kFastTma)
+    for (const auto& M : c->m)
+      if (!M.terrain_active && M.tmaps.empty())
+        return fail(c, GWM_B200_ERR_ARG, "TMA substep unavailable (tensor-map encoder not found)");
   drop_graph(c);
   (kernel == 0 ? c->slow_tile_rows : kernel == 1 ? c->fast_tile_rows : c->tracer_tile_rows) = rows;
   return GWM_B200_OK;
@@ -676,7 +788,11 @@ static int run_steps(gwm_b200_ctx* c, int nsteps, int (*one)(gwm_b200_ctx*, Memb
       }
   }
   c->launches = c->cur_launches;
-  if (c->stream == c->own_stream || c->profile) CK(cudaStreamSynchronize(c->stream));
+  if (c->stream == c->own_stream || c->profile) {
+    CK(cudaStreamSynchronize(c->stream));
+    const int rc = check_device_errors(c);
+    if (rc) return rc;
+  }
   if (c->profile) {
     for (auto& pe : c->prof_events) {
       float ms = 0.f;
@@ -791,7 +907,8 @@ int gwm_b200_fast_modes(gwm_b200_ctx* c) {
       f.acc_a = M.slot(M.ring + 1); f.acc_b = M.slot(M.ring + 1) + kMaxNz;
       f.clr_a = M.slot(M.ring + 2); f.clr_b = M.slot(M.ring + 2) + kMaxNz;
       f.zc = M.zc; f.idz_c = M.idc; f.idz_f = M.idf; f.base = M.base;
-      LAUNCH(launch_fast(f, n == 0, terr, c->stream, c->fast_tile_rows), "fast substep");
+      f.err = M.err;
+      LAUNCH(launch_substep(c, M, f, n == 0, terr), "fast substep");
       M.ring = (M.ring + 1) % 3;
       rcur ^= 1;
       dcur = dout;

@@ -1,8 +1,8 @@
 // dycore.cu — sm_100a kernels of the dry dynamics: one fused slow RK stage and
 // one fused acoustic substep.
 //
-// Both kernels use the same tiling.  A CTA of BX x BY threads owns an
-// (BX-2) x (BY-2) block of columns plus a one-column ring of halo columns; each
+// The overlapped-tile kernels share one tiling.  A CTA of BX x R threads owns an
+// (BX-2) x (R-2) block of columns plus a one-column ring of halo columns; each
 // thread owns one column and marches k = 0..nz-1 keeping k-1, k, k+1 values
 // in registers, while the current plane is shared through shared memory for
 // the horizontal neighbours.  Halo threads load and derive the same per-column
@@ -16,10 +16,6 @@ namespace gwmb {
 namespace {
 
 constexpr int BX = 32;
-constexpr int BY = 8;
-constexpr int NT = BX * BY;
-constexpr int NW = NT / 32;
-
 
 __device__ __forceinline__ float met3(const float* m, const Geom& g, int i, int j, int k) {
   return __ldg(m + gidx(g, i, j, k));

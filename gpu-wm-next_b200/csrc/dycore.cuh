@@ -2,6 +2,8 @@
 // acoustic substep) of the time-step hot path.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace gwmb {
@@ -54,7 +56,21 @@ struct FastArgs {
   unsigned long long *acc_a, *acc_b, *clr_a, *clr_b;
   const float *zc, *idz_c, *idz_f;
   const double* base;
+  int* err;                         // error word: set to 1 when a bounded wait gave up
 };
+
+// TMA descriptors of one acoustic substep (flat terrain, k_fast_tma): 3-D tiled maps
+// over the padded field layout (dims pitch x rows x (nz+1), FP32, no swizzle).
+struct FastMaps {
+  CUtensorMap rho, th;     // box 40 x 18: cells with the halo ring
+  CUtensorMap du, dv;      // box 36 x 17: owned faces + the tile's east/north face
+  CUtensorMap dw;          // box 32 x 16
+  CUtensorMap bu, bv, bw;  // box 32 x 16 (last substep of the step)
+};
+// Box extents (x, y) of the maps above.
+constexpr int kTmaCellBox[2] = {40, 18};
+constexpr int kTmaFaceBox[2] = {36, 17};
+constexpr int kTmaOwnBox[2] = {32, 16};
 
 // Level sums of a stored state.  mode 0: theta = rt/max(rho,1e-6) (the host loop of
 // dry_core.cu:462-476); mode 1: rho and p(rho, rho*theta) (K6 of dry_fast_modes.cu:42-57).
@@ -70,6 +86,10 @@ struct LevelSumArgs {
 cudaError_t launch_slow(const SlowArgs& a, bool terrain, cudaStream_t s, int tile_rows);
 // tile_rows: CTA rows of the acoustic-substep tile (8 or 16; 32 columns wide).
 cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_t s, int tile_rows);
+// Flat-terrain acoustic substep fed by TMA tile loads (owned 32 x 16 tiles).
+cudaError_t launch_fast_tma(const FastArgs& a, const FastMaps& m, bool first, cudaStream_t s);
+// One-time kernel attributes (dynamic shared memory) of the TMA substep.
+cudaError_t init_fast_tma();
 cudaError_t launch_level_sums(const LevelSumArgs& a, cudaStream_t s);
 // FP64 base state of the pressure-perturbation EOS: per level the mean rho_theta of
 // the state, its reciprocal and p_ref = EOS(mean rho_theta); one CTA per level.

@@ -1,0 +1,325 @@
+// fast_tma.cu — acoustic substep (flat terrain) fed by TMA tile loads.
+//
+// Same operator as k_fast_flat (LocalSplitExplicitFastMode::apply,
+// dry_fast_modes.cu:400-656, K9-K15 on one substep) and the same per-cell
+// arithmetic, with a different data path: one elected thread per CTA fetches every
+// plane's tiles with cp.async.bulk.tensor.3d into a three-slot shared-memory ring,
+// two planes ahead of the compute, and the 256 threads work from shared memory.
+// Per plane k the ring slot holds
+//   rho(k), theta(k)        40 x 18 box: columns i0-4 .. i0+35, rows j0-1 .. j0+16
+//                           (the owned 32 x 16 tile and its one-cell halo ring; the
+//                           box starts 4 columns left so x stays 16-byte aligned)
+//   du(k), dv(k)            36 x 17 box: owned faces plus the tile's east/north face
+//   dw(k+1)                 32 x 16 box: owned Z faces above the plane
+//   bu(k), bv(k), bw(k+1)   32 x 16 boxes, last substep of the step only (m = B + D)
+// so the kernel issues no per-thread global loads on the main path, holds no load
+// pipeline in registers and needs no halo threads reading global memory.
+#include "dycore.cuh"
+#include "tma.cuh"
+
+namespace gwmb {
+namespace {
+
+namespace ft {
+constexpr int TX = 32, TY = 16, RY = 8, NT = 256, NW = NT / 32;
+constexpr int CBW = 40, CBH = 18;  // cell box
+constexpr int FBW = 36, FBH = 17;  // face box (owned faces + east/north face)
+constexpr int OBW = 32, OBH = 16;  // owned box
+// slot layout in floats; every sub-buffer starts on a 128-byte boundary
+// (the base-momentum boxes are only present, and the slot only that long, in the last
+// substep of the step: other substeps use the shorter slot and fit three CTAs per SM)
+constexpr int O_RHO = 0, O_TH = 736, O_DU = 1472, O_DV = 2112, O_DW = 2752, O_BU = 3264,
+              O_BV = 3776, O_BW = 4288, SLOT = 4800, SLOT_SHORT = 3264, NSLOT = 3;
+constexpr unsigned B_CELL = CBW * CBH * 4, B_FACE = FBW * FBH * 4, B_OWN = OBW * OBH * 4;
+constexpr size_t kDynSmem = size_t(SLOT) * NSLOT * sizeof(float) + 128;
+constexpr size_t kDynSmemShort = size_t(SLOT_SHORT) * NSLOT * sizeof(float) + 128;
+static_assert(O_TH % 32 == 0 && O_DU % 32 == 0 && O_DV % 32 == 0 && O_DW % 32 == 0 && O_BU % 32 == 0 &&
+                  O_BV % 32 == 0 && O_BW % 32 == 0 && SLOT % 32 == 0 && SLOT_SHORT % 32 == 0 &&
+                  SLOT_SHORT == O_BU,
+              "128-byte aligned sub-buffers");
+static_assert(O_TH - O_RHO >= CBW * CBH && O_DU - O_TH >= CBW * CBH && O_DV - O_DU >= FBW * FBH &&
+                  O_DW - O_DV >= FBW * FBH && O_BU - O_DW >= OBW * OBH && O_BV - O_BU >= OBW * OBH &&
+                  O_BW - O_BV >= OBW * OBH && SLOT - O_BW >= OBW * OBH,
+              "boxes fit their sub-buffers");
+}  // namespace ft
+
+template <bool FIRST>
+__global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const __grid_constant__ FastMaps m) {
+  using namespace ft;
+  extern __shared__ unsigned char s_dyn[];
+  __shared__ float s_p[2][TY + 2][TX + 2];  // pressure perturbation, tile + halo ring
+  __shared__ float s_du[2][TY][TX + 1];     // new X-face increments (own + east face)
+  __shared__ float s_dv[2][TY + 1][TX];     // new Y-face increments (own + north face)
+  __shared__ float s_pref[kMaxNz], s_rref[kMaxNz], s_idzc[kMaxNz], s_idzf[kMaxNz];
+  __shared__ long long s_red[2][NW][2];
+  __shared__ __align__(8) uint64_t s_bar[NSLOT];
+  __shared__ int s_abort[2];  // per plane parity: set before barrier k, read after it
+  float* const ring = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
+
+  const Geom& g = a.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int w = min(TX, nx - i0), h = min(TY, ny - j0);
+  const bool own0 = tx < w && ty < h, own1 = tx < w && ty + RY < h;
+  const int gi = i0 + tx, gj0 = j0 + ty, gj1 = j0 + ty + RY;
+  const bool skip_u = gi == 0 && !g.per_x;  // open west face (never changes)
+  const bool skip_v0 = gj0 == 0 && !g.per_y;
+  const bool edge = (g.per_x && (i0 <= 1 || i0 + w >= nx - 1)) || (g.per_y && (j0 <= 1 || j0 + h >= ny - 1));
+  // halo roles (threads 0-95, whole warps): 0 west column, 1 east column, 2 south row,
+  // 3 north row; (hr, hc) are s_p coordinates (row 0 = j0-1, column 0 = i0-1)
+  int role = -1, hr = 0, hc = 0;
+  if (tid < TY) { if (tid < h) { role = 0; hr = tid + 1; hc = 0; } }
+  else if (tid < 2 * TY) { if (tid - TY < h) { role = 1; hr = tid - TY + 1; hc = w + 1; } }
+  else if (tid < 2 * TY + TX) { if (tid - 2 * TY < w) { role = 2; hr = 0; hc = tid - 2 * TY + 1; } }
+  else if (tid < 2 * TY + 2 * TX) { if (tid - 2 * TY - TX < w) { role = 3; hr = h + 1; hc = tid - 2 * TY - TX + 1; } }
+  const int hi = i0 + hc - 1, hj = j0 + hr - 1;  // global cell of the halo role
+  const bool h_skip = (role == 1 && hi == nx && !g.per_x) || (role == 3 && hj == ny && !g.per_y);
+  const float idx = g.inv_dx, idy = g.inv_dy, dtf = a.dtf;
+  const bool final_step = a.final_kind == 2;
+  const int acc_mode = a.acc_off ? 0 : (a.final_kind == 0 ? 1 : 2);
+  const bool hm = a.hmom != 0, dn = a.dens != 0;
+  const int slot = final_step ? SLOT : SLOT_SHORT;
+
+  if (tid == 0) {
+    for (int s = 0; s < NSLOT; ++s) mbar_init(&s_bar[s], 1);
+    mbar_fence_init();
+    s_abort[0] = 0;
+    s_abort[1] = 0;
+  }
+  if (blockIdx.x == 0 && blockIdx.y == 0 && a.clr_a)
+    for (int q = tid; q < nz; q += NT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
+  for (int q = tid; q < nz; q += NT) {  // K6/K7 level means; metric columns
+    s_rref[q] = (float)(acc_read(a.ref_a + q, kScaleRho) * a.inv_count);
+    s_pref[q] = (float)(acc_read(a.ref_b + q, kScaleP) * a.inv_count);
+    s_idzc[q] = __ldg(a.idz_c + q);
+    s_idzf[q] = __ldg(a.idz_f + q);
+  }
+  __syncthreads();
+
+  // producer: all tiles of plane kk into slot kk % NSLOT, completing on its barrier
+  auto issue = [&](int kk) {
+    float* st = ring + (kk % NSLOT) * slot;
+    uint64_t* bar = &s_bar[kk % NSLOT];
+    const bool wface = kk + 1 < nz;
+    unsigned bytes = 2 * B_CELL;
+    if (!FIRST) bytes += 2 * B_FACE + (wface ? B_OWN : 0u);
+    if (final_step) bytes += 3 * B_OWN;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, bytes);
+    tma_load_3d(st + O_RHO, &m.rho, i0 + kXOff - 4, j0, kk, bar);
+    tma_load_3d(st + O_TH, &m.th, i0 + kXOff - 4, j0, kk, bar);
+    if (!FIRST) {
+      tma_load_3d(st + O_DU, &m.du, i0 + kXOff, j0 + 1, kk, bar);
+      tma_load_3d(st + O_DV, &m.dv, i0 + kXOff, j0 + 1, kk, bar);
+      if (wface) tma_load_3d(st + O_DW, &m.dw, i0 + kXOff, j0 + 1, kk + 1, bar);
+    }
+    if (final_step) {
+      tma_load_3d(st + O_BU, &m.bu, i0 + kXOff, j0 + 1, kk, bar);
+      tma_load_3d(st + O_BV, &m.bv, i0 + kXOff, j0 + 1, kk, bar);
+      tma_load_3d(st + O_BW, &m.bw, i0 + kXOff, j0 + 1, kk + 1, bar);
+    }
+  };
+  int issued = -1, waited = -1;  // planes issued / waited for (producer bookkeeping)
+  auto wait_plane = [&](int kk, int epoch) {
+    if (!mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1)) {
+      s_abort[epoch & 1] = 1;
+      atomicExch(a.err, 1);
+    }
+    waited = kk;
+  };
+  // K10 + K20: pressure perturbation of plane kk at the owned cells and the halo ring
+  auto cell_p = [&](const float* st, int r, int c, int kk) {
+    const float rho = st[O_RHO + r * CBW + c + 3], th = st[O_TH + r * CBW + c + 3];
+    return eos_pprime(rho, rho * th, a.base, kk, nz);
+  };
+  auto plane_p = [&](int kk) {
+    const float* st = ring + (kk % NSLOT) * slot;
+    float(*sp)[TX + 2] = s_p[kk & 1];
+    if (own0) sp[ty + 1][tx + 1] = cell_p(st, ty + 1, tx + 1, kk);
+    if (own1) sp[ty + RY + 1][tx + 1] = cell_p(st, ty + RY + 1, tx + 1, kk);
+    if (role >= 0) sp[hr][hc] = cell_p(st, hr, hc, kk);
+  };
+
+  if (tid == 0) {
+    issue(0);
+    issued = 0;
+    if (nz > 1) { issue(1); issued = 1; }
+  }
+  wait_plane(0, 0);
+  plane_p(0);
+  float dwc0 = 0.f, dwc1 = 0.f;  // increment at face k (face 0 never changes)
+  float bwz0 = 0.f, bwz1 = 0.f;  // base momentum at face 0 (last substep of the step)
+  if (final_step) {
+    if (own0) bwz0 = __ldg(a.bw + gidx(g, gi, gj0, 0));
+    if (own1) bwz1 = __ldg(a.bw + gidx(g, gi, gj1, 0));
+  }
+  __syncthreads();
+
+  bool aborted = false;
+  for (int k = 0; k < nz; ++k) {
+    const int pb = k & 1;
+    const float* st = ring + (k % NSLOT) * slot;
+    const float* stn = ring + ((k + 1) % NSLOT) * slot;
+    // ---- pressure perturbation of plane k+1 (its tiles were issued a plane ago)
+    if (k + 1 < nz) {
+      wait_plane(k + 1, k);
+      plane_p(k + 1);
+    }
+    // ---- faces of plane k: K12/K13 horizontal momenta, K14 vertical momentum at face k+1
+    const float(*sp)[TX + 2] = s_p[pb];
+    float du0 = 0.f, dv0 = 0.f, du1 = 0.f, dv1 = 0.f, dw0 = 0.f, dw1 = 0.f;
+    if (!FIRST) {
+      du0 = st[O_DU + ty * FBW + tx];
+      dv0 = st[O_DV + ty * FBW + tx];
+      du1 = st[O_DU + (ty + RY) * FBW + tx];
+      dv1 = st[O_DV + (ty + RY) * FBW + tx];
+      if (k + 1 < nz) { dw0 = st[O_DW + ty * OBW + tx]; dw1 = st[O_DW + (ty + RY) * OBW + tx]; }
+    }
+    const float pc0 = sp[ty + 1][tx + 1], pc1 = sp[ty + RY + 1][tx + 1];
+    float un0 = du0, vn0 = dv0, un1 = du1, vn1 = dv1;
+    if (hm) {
+      if (!skip_u) {
+        un0 = du0 + (-dtf * ((pc0 - sp[ty + 1][tx]) * idx));
+        un1 = du1 + (-dtf * ((pc1 - sp[ty + RY + 1][tx]) * idx));
+      }
+      if (!skip_v0) vn0 = dv0 + (-dtf * ((pc0 - sp[ty][tx + 1]) * idy));
+      vn1 = dv1 + (-dtf * ((pc1 - sp[ty + RY][tx + 1]) * idy));
+    }
+    if (own0) { s_du[pb][ty][tx] = un0; s_dv[pb][ty][tx] = vn0; }
+    if (own1) { s_du[pb][ty + RY][tx] = un1; s_dv[pb][ty + RY][tx] = vn1; }
+    if (role == 1) {  // the tile's east X face
+      float d = FIRST ? 0.f : st[O_DU + (hr - 1) * FBW + w];
+      if (hm && !h_skip) d = d + (-dtf * ((sp[hr][hc] - sp[hr][hc - 1]) * idx));
+      s_du[pb][hr - 1][w] = d;
+      // open east boundary: face nx belongs to no tile; its step value is base + increment
+      if (final_step && h_skip) {
+        const int o = gidx(g, hi, hj, k);
+        a.f_u[o] = __ldg(a.bu + o) + d;
+      }
+    } else if (role == 3) {  // the tile's north Y face
+      float d = FIRST ? 0.f : st[O_DV + h * FBW + hc - 1];
+      if (hm && !h_skip) d = d + (-dtf * ((sp[hr][hc] - sp[hr - 1][hc]) * idy));
+      s_dv[pb][h][hc - 1] = d;
+      if (final_step && h_skip) {
+        const int o = gidx(g, hi, hj, k);
+        a.f_v[o] = __ldg(a.bv + o) + d;
+      }
+    }
+    const float rc0 = st[O_RHO + (ty + 1) * CBW + tx + 4], rc1 = st[O_RHO + (ty + RY + 1) * CBW + tx + 4];
+    float wn0 = dw0, wn1 = dw1;
+    if (k + 1 < nz) {
+      const float prl = s_pref[k], pru = s_pref[k + 1], rrl = s_rref[k], rru = s_rref[k + 1];
+      const float idzf = s_idzf[k + 1];
+      const float(*spn)[TX + 2] = s_p[pb ^ 1];
+      const float pn0 = spn[ty + 1][tx + 1], pn1 = spn[ty + RY + 1][tx + 1];
+      const float rn0 = stn[O_RHO + (ty + 1) * CBW + tx + 4], rn1 = stn[O_RHO + (ty + RY + 1) * CBW + tx + 4];
+      wn0 = dw0 + dtf * (-((pn0 - pru) - (pc0 - prl)) * idzf - a.gravity * (0.5f * ((rc0 - rrl) + (rn0 - rru))));
+      wn1 = dw1 + dtf * (-((pn1 - pru) - (pc1 - prl)) * idzf - a.gravity * (0.5f * ((rc1 - rrl) + (rn1 - rru))));
+    }
+    __syncthreads();  // publishes s_p(k+1), s_du(k), s_dv(k); slot (k-1) is free
+    if (s_abort[pb]) { aborted = true; break; }
+    if (tid == 0) {
+      if (acc_mode && k > 0) {  // level sums of plane k-1 (warp totals published above)
+        long long sa = 0, sb = 0;
+        for (int q = 0; q < NW; ++q) { sa += s_red[pb ^ 1][q][0]; sb += s_red[pb ^ 1][q][1]; }
+        acc_add(a.acc_a + k - 1, sa);
+        if (acc_mode == 1) acc_add(a.acc_b + k - 1, sb);
+      }
+      if (k + 2 < nz) { issue(k + 2); issued = k + 2; }
+    }
+    // ---- K15 density of plane k, K10 rho*theta, stores
+    const float idzc = s_idzc[k];
+    FxAcc sa, sb;
+    if (own0) {
+      float rn = rc0;
+      if (dn) {
+        const float div = (s_du[pb][ty][tx + 1] - un0) * idx + (s_dv[pb][ty + 1][tx] - vn0) * idy + (wn0 - dwc0) * idzc;
+        rn = fmaxf(1.0e-6f, rc0 - dtf * div);
+      }
+      const float rt = rn * st[O_TH + (ty + 1) * CBW + tx + 4];
+      if (final_step) {
+        store_tile(a.f_rho, g, kCell, gi, gj0, k, rn, edge);
+        store_tile(a.f_rt, g, kCell, gi, gj0, k, rt, edge);
+        store_tile(a.f_u, g, kFaceX, gi, gj0, k, st[O_BU + ty * OBW + tx] + un0, edge);
+        store_tile(a.f_v, g, kFaceY, gi, gj0, k, st[O_BV + ty * OBW + tx] + vn0, edge);
+        if (k == 0) store_tile(a.f_w, g, kFaceZ, gi, gj0, 0, bwz0, edge);
+        store_tile(a.f_w, g, kFaceZ, gi, gj0, k + 1, st[O_BW + ty * OBW + tx] + wn0, edge);
+      } else {
+        store_tile(a.rho_out, g, kCell, gi, gj0, k, rn, edge);
+        store_tile(a.du_out, g, kFaceX, gi, gj0, k, un0, edge);
+        store_tile(a.dv_out, g, kFaceY, gi, gj0, k, vn0, edge);
+        if (k + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj0, k + 1, wn0, edge);
+      }
+      if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime(rn, rt, a.base, k, nz), kFxP); }
+      else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
+    }
+    if (own1) {
+      float rn = rc1;
+      if (dn) {
+        const float div = (s_du[pb][ty + RY][tx + 1] - un1) * idx + (s_dv[pb][ty + RY + 1][tx] - vn1) * idy +
+                          (wn1 - dwc1) * idzc;
+        rn = fmaxf(1.0e-6f, rc1 - dtf * div);
+      }
+      const float rt = rn * st[O_TH + (ty + RY + 1) * CBW + tx + 4];
+      if (final_step) {
+        store_tile(a.f_rho, g, kCell, gi, gj1, k, rn, edge);
+        store_tile(a.f_rt, g, kCell, gi, gj1, k, rt, edge);
+        store_tile(a.f_u, g, kFaceX, gi, gj1, k, st[O_BU + (ty + RY) * OBW + tx] + un1, edge);
+        store_tile(a.f_v, g, kFaceY, gi, gj1, k, st[O_BV + (ty + RY) * OBW + tx] + vn1, edge);
+        if (k == 0) store_tile(a.f_w, g, kFaceZ, gi, gj1, 0, bwz1, edge);
+        store_tile(a.f_w, g, kFaceZ, gi, gj1, k + 1, st[O_BW + (ty + RY) * OBW + tx] + wn1, edge);
+      } else {
+        store_tile(a.rho_out, g, kCell, gi, gj1, k, rn, edge);
+        store_tile(a.du_out, g, kFaceX, gi, gj1, k, un1, edge);
+        store_tile(a.dv_out, g, kFaceY, gi, gj1, k, vn1, edge);
+        if (k + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj1, k + 1, wn1, edge);
+      }
+      if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime(rn, rt, a.base, k, nz), kFxP); }
+      else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
+    }
+    if (acc_mode) {
+      const long long ta = sa.warp_total(), tb = sb.warp_total();
+      if (tx == 0) { s_red[pb][ty][0] = ta; s_red[pb][ty][1] = tb; }
+    }
+    dwc0 = wn0;
+    dwc1 = wn1;
+  }
+  if (aborted) {
+    // drain the tiles still in flight (bounded) before the CTA's shared memory goes away
+    if (tid == 0)
+      for (int kk = waited + 1; kk <= issued; ++kk) mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1);
+    return;
+  }
+  if (acc_mode) {  // level sums of the last plane
+    __syncthreads();
+    if (tid == 0) {
+      const int pb = (nz - 1) & 1;
+      long long sa = 0, sb = 0;
+      for (int q = 0; q < NW; ++q) { sa += s_red[pb][q][0]; sb += s_red[pb][q][1]; }
+      acc_add(a.acc_a + nz - 1, sa);
+      if (acc_mode == 1) acc_add(a.acc_b + nz - 1, sb);
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t init_fast_tma() {
+  cudaError_t e = cudaFuncSetAttribute(k_fast_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ft::kDynSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_fast_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ft::kDynSmem);
+}
+
+cudaError_t launch_fast_tma(const FastArgs& a, const FastMaps& m, bool first, cudaStream_t s) {
+  if (a.g.nz > kMaxNz || !a.err) return cudaErrorInvalidValue;
+  const dim3 block(ft::TX, ft::RY);
+  const dim3 grid((a.g.nx + ft::TX - 1) / ft::TX, (a.g.ny + ft::TY - 1) / ft::TY);
+  const size_t smem = a.final_kind == 2 ? ft::kDynSmem : ft::kDynSmemShort;
+  if (first) k_fast_tma<true><<<grid, block, smem, s>>>(a, m);
+  else k_fast_tma<false><<<grid, block, smem, s>>>(a, m);
+  return cudaGetLastError();
+}
+
+}  // namespace gwmb

@@ -7,8 +7,6 @@ namespace gwmb {
 namespace {
 
 constexpr int BX = 32;
-constexpr int BY = 8;
-constexpr int NT = BX * BY;
 constexpr int NTR = 3;
 
 struct TrCol {

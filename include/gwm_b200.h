@@ -35,6 +35,7 @@ extern "C" {
 #define GWM_B200_ERR_CUDA (-2)         /* CUDA runtime error; see gwm_b200_last_error */
 #define GWM_B200_ERR_STATE (-3)        /* non-finite or non-positive density detected */
 #define GWM_B200_ERR_NO_DEVICE (-4)    /* no CUDA device visible */
+#define GWM_B200_ERR_TIMEOUT (-5)      /* a bounded device wait gave up; the step's result is invalid */
 
 typedef struct gwm_b200_ctx gwm_b200_ctx;
 
@@ -152,7 +153,8 @@ int gwm_b200_slow_tendencies(gwm_b200_ctx* ctx, int member, gwm_b200_fields* hos
 int gwm_b200_budgets(gwm_b200_ctx* ctx, int member, gwm_b200_budget* out);
 /* Tile shape of a kernel.  kernel 0 = slow stage, 2 = tracer stage: rows 8 or 16
  * (overlapped 32-wide tiles, default 16).  kernel 1 = acoustic substep: rows 0 = owned
- * 32x16 tiles (flat terrain; terrain falls back to 8), 8 or 16 = overlapped 32-wide
+ * 32x16 tiles (flat terrain; terrain falls back to 8), 3 = owned 32x16 tiles fed by TMA
+ * tile loads (flat terrain; terrain falls back to 8), 8 or 16 = overlapped 32-wide
  * tiles of that many rows.  The environment variable GWM_B200_FAST_TILE_ROWS sets the
  * acoustic default at context creation.  The choice changes speed only: every tiling
  * computes the same values.  gwm_b200_get_tile returns the current rows (or < 0). */

@@ -432,7 +432,7 @@ def test_interior_tiles_vs_oracle(gwm, orc):
         assert rel_err(out[k], ref[k], floor=1e-9) < 1e-3, k
 
 
-@pytest.mark.parametrize("rows", [0, 8, 16])
+@pytest.mark.parametrize("rows", [0, 3, 8, 16])
 def test_substep_tilings_agree(gwm, rows):
     g = gwm.GridSpec(100, 70, 12, dx=2000.0, dy=2000.0, z_top=12000.0)
     s = c1_state(gwm, g, u=2.0, v=1.0)
@@ -472,3 +472,25 @@ def test_stage_tilings_bit_exact(gwm, kernel, periodic):
             outs[r] = m.download()
     for k in outs[8]:
         assert np.array_equal(outs[8][k], outs[16][k]), k
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_tma_substep_bit_exact(gwm, periodic):
+    # the TMA-fed substep runs the owned-tile kernel's arithmetic on the same values:
+    # a full moist step (every substep kind: first, inner, stage end, step end) must
+    # agree bit for bit; 100 x 70 leaves partial tiles on both axes
+    g = gwm.GridSpec(100, 70, 12, dx=2000.0, dy=2000.0, z_top=12000.0,
+                     periodic_x=periodic, periodic_y=periodic)
+    p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=9, relative_humidity=1.02)
+    s = gwm.build_case("moist_sounding", g, p, moist=True)
+    step = gwm.StepConfig(dt=1.0, fast_substeps=4)
+    rain = gwm.WarmRainConfig(dt=1.0, rain_terminal_velocity=12.0)
+    outs = {}
+    for r in (0, 3):
+        with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=True)) as m:
+            m.set_tile("fast_substep", r)
+            m.upload(s)
+            m.step(3)
+            outs[r] = m.download()
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[3][k]), k
