@@ -229,7 +229,7 @@ bool encode_field_map(CUtensorMap* out, const float* base, const Geom& g, int bx
 // Maps of every buffer the flat-terrain TMA substep may read (false if unavailable).
 bool build_substep_maps(Member& M) {
   M.tmaps.clear();
-  const int* boxes[3] = {kTmaCellBox, kTmaFaceBox, kTmaOwnBox};
+  const int* boxes[4] = {kTmaCellBox, kTmaFaceBox, kTmaOwnBox, kTmaYFaceBox};
   auto add = [&](const float* buf, int kind) {
     CUtensorMap m;
     if (!encode_field_map(&m, buf, M.g, boxes[kind][0], boxes[kind][1])) return false;
@@ -243,6 +243,13 @@ bool build_substep_maps(Member& M) {
     for (int f = 0; f < 3; ++f) ok = ok && add(M.B[i][f], 2);
   }
   for (int f = 2; f < 5; ++f) ok = ok && add(M.Q[f], 2);  // bases of the stand-alone fast modes
+  // slow stage: inputs with 40 x 18 boxes (kind 0) and Y faces with 40 x 19 (kind 3)
+  for (int f : {0, 1, 2, 4}) ok = ok && add(M.Q[f], 0);
+  ok = ok && add(M.Q[3], 3);
+  for (int i = 0; i < 2; ++i) {
+    ok = ok && add(M.B[i][0], 0) && add(M.B[i][2], 0) && add(M.B[i][1], 3);
+    ok = ok && add(M.D[i][0], 0) && add(M.D[i][2], 0) && add(M.D[i][1], 3);
+  }
   if (!ok) M.tmaps.clear();
   return ok;
 }
@@ -323,6 +330,24 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
 }
 
 constexpr int kFastTma = 3;  // fast_tile_rows value selecting the TMA-fed substep
+constexpr int kSlowTma = 3;  // slow_tile_rows value selecting the TMA-fed slow stage
+
+// One slow stage: the TMA-fed kernel when selected on flat terrain, else overlapped tiles.
+cudaError_t launch_stage(gwm_b200_ctx* c, const Member& M, const SlowArgs& a, bool terr) {
+  if (!terr && !a.tend_only && c->slow_tile_rows == kSlowTma) {
+    SlowMaps m{};
+    const CUtensorMap* p[8] = {M.tmap(a.rho, 0), M.tmap(a.th, 0), M.tmap(a.u, 0), M.tmap(a.v, 3),
+                               M.tmap(a.w, 0), a.du ? M.tmap(a.du, 0) : nullptr,
+                               a.du ? M.tmap(a.dv, 3) : nullptr, a.du ? M.tmap(a.dw, 0) : nullptr};
+    for (int i = 0; i < 5; ++i)
+      if (!p[i]) return cudaErrorInvalidValue;
+    if (a.du && (!p[5] || !p[6] || !p[7] || !a.dv || !a.dw)) return cudaErrorInvalidValue;
+    m.rho = *p[0]; m.th = *p[1]; m.u = *p[2]; m.v = *p[3]; m.w = *p[4];
+    if (a.du) { m.du = *p[5]; m.dv = *p[6]; m.dw = *p[7]; }
+    return launch_slow_tma(a, m, c->stream);
+  }
+  return launch_slow(a, terr, c->stream, c->slow_tile_rows == kSlowTma ? 16 : c->slow_tile_rows);
+}
 
 // One acoustic substep: the TMA-fed kernel when selected on flat terrain, else the
 // owned-tile or overlapped-tile kernels.
@@ -463,7 +488,8 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
     a.acc_mode = fast ? (terr ? 0 : 1) : ((s == 2 && rain_theta) ? 0 : 2);
     a.inv_count = inv_count(M);
     a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf; a.base = M.base;
-    LAUNCH(launch_slow(a, terr, c->stream, c->slow_tile_rows), "slow stage");
+    a.err = M.err;
+    LAUNCH(launch_stage(c, M, a, terr), "slow stage");
     M.ring = (M.ring + 1) % 3;
     rcur = rnext;
     if (!fast) continue;
@@ -583,7 +609,11 @@ int gwm_b200_create(const gwm_b200_grid_desc* grids, const gwm_b200_member_desc*
   cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete c; return GWM_B200_ERR_CUDA; }
   c->stream = c->own_stream;
-  if (init_fast_tma() != cudaSuccess) { cudaStreamDestroy(c->own_stream); delete c; return GWM_B200_ERR_CUDA; }
+  if (init_fast_tma() != cudaSuccess || init_slow_tma() != cudaSuccess) {
+    cudaStreamDestroy(c->own_stream);
+    delete c;
+    return GWM_B200_ERR_CUDA;
+  }
   c->m.resize(n_members);
   for (int i = 0; i < n_members; ++i) {
     Member& M = c->m[i];
@@ -658,10 +688,11 @@ long long gwm_b200_launch_count(const gwm_b200_ctx* c) { return c ? c->launches 
 
 int gwm_b200_set_tile(gwm_b200_ctx* c, int kernel, int rows) {
   if (!c) return GWM_B200_ERR_ARG;
-  const bool ok = kernel == 1 ? (rows == 0 || rows == kFastTma || rows == 8 || rows == 16)
-                              : (kernel == 0 || kernel == 2) && (rows == 8 || rows == 16);
+  const bool ok = kernel == 1   ? (rows == 0 || rows == kFastTma || rows == 8 || rows == 16)
+                  : kernel == 0 ? (rows == kSlowTma || rows == 8 || rows == 16)
+                                : kernel == 2 && (rows == 8 || rows == 16);
   if (!ok) return GWM_B200_ERR_ARG;
-  if (kernel == 1 && rows == kFastTma)
+  if ((kernel == 1 && rows == kFastTma) || (kernel == 0 && rows == kSlowTma))
     for (const auto& M : c->m)
       if (!M.terrain_active && M.tmaps.empty())
         return fail(c, GWM_B200_ERR_ARG, "TMA substep unavailable (tensor-map encoder not found)");
@@ -941,7 +972,7 @@ int gwm_b200_slow_tendencies(gwm_b200_ctx* c, int member, gwm_b200_fields* h) {
   a.acc_mode = 0;
   a.inv_count = inv_count(M);
   a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf; a.base = M.base;
-  CK(launch_slow(a, M.terrain_active, c->stream, c->slow_tile_rows));
+  CK(launch_slow(a, M.terrain_active, c->stream, c->slow_tile_rows == kSlowTma ? 16 : c->slow_tile_rows));
   gwm_b200_fields tmp{};
   tmp.rho_d = h->rho_d; tmp.rho_theta_m = h->rho_theta_m;
   tmp.mom_u = h->mom_u; tmp.mom_v = h->mom_v; tmp.mom_w = h->mom_w;

@@ -69,10 +69,9 @@ __device__ __forceinline__ float dry_cp() { return kRd / kKappa; }
 // real arithmetic (the base is constant on a level) but keep ~1e-5 Pa resolution
 // instead of the ~1e-2 Pa of an FP32 pressure near 1e5 Pa.
 // base layout: [rt_ref(nz) | 1/rt_ref(nz) | p_ref(nz)], FP64.
-__device__ __forceinline__ float eos_pprime(float rho, float rt, const double* __restrict__ base, int k,
-                                            int nz) {
-  const double d = fma((double)rt, __ldg(base + nz + k), -1.0);
-  const double pref = __ldg(base + 2 * nz + k);
+// Core form with the level's 1/rt_ref and p_ref already at hand.
+__device__ __forceinline__ float eos_pprime_ref(float rho, float rt, double inv_rt_ref, double pref) {
+  const double d = fma((double)rt, inv_rt_ref, -1.0);
   if (rho >= 1.0e-6f && fabs(d) < 0.0625) {
     // C(g, n), n = 1 .. 7, for g = 1.0f / (1.0f - 0.2854f); Estrin's scheme keeps the
     // dependent FP64 chain three operations deep instead of seven (Horner)
@@ -86,6 +85,10 @@ __device__ __forceinline__ float eos_pprime(float rho, float rt, const double* _
     return (float)(pref * (s * d));
   }
   return (float)((double)eos_pressure(rho, rt) - pref);
+}
+__device__ __forceinline__ float eos_pprime(float rho, float rt, const double* __restrict__ base, int k,
+                                            int nz) {
+  return eos_pprime_ref(rho, rt, __ldg(base + nz + k), __ldg(base + 2 * nz + k));
 }
 
 __device__ __forceinline__ float upwind(float a, float ql, float qr) {

@@ -34,6 +34,13 @@ struct SlowArgs {
   double inv_count;                 // 1 / (nx*ny)
   const float *zc, *idz_c, *idz_f;  // metrics: padded 3-D (terrain) or per level (flat)
   const double* base;               // FP64 base state [rt_ref | 1/rt_ref | p_ref] per level
+  int* err;                         // error word: set to 1 when a bounded wait gave up
+};
+
+// TMA descriptors of one slow stage (flat terrain, k_slow_tma): 3-D tiled maps over the
+// padded layout with 40 x 18 boxes (cells, X and Z faces) and 40 x 19 (Y faces).
+struct SlowMaps {
+  CUtensorMap rho, th, u, v, w, du, dv, dw;
 };
 
 // Arguments of one acoustic substep: src/dycore/dry_fast_modes.cu:495-652
@@ -71,6 +78,7 @@ struct FastMaps {
 constexpr int kTmaCellBox[2] = {40, 18};
 constexpr int kTmaFaceBox[2] = {36, 17};
 constexpr int kTmaOwnBox[2] = {32, 16};
+constexpr int kTmaYFaceBox[2] = {40, 19};
 
 // Level sums of a stored state.  mode 0: theta = rt/max(rho,1e-6) (the host loop of
 // dry_core.cu:462-476); mode 1: rho and p(rho, rho*theta) (K6 of dry_fast_modes.cu:42-57).
@@ -86,6 +94,9 @@ struct LevelSumArgs {
 cudaError_t launch_slow(const SlowArgs& a, bool terrain, cudaStream_t s, int tile_rows);
 // tile_rows: CTA rows of the acoustic-substep tile (8 or 16; 32 columns wide).
 cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_t s, int tile_rows);
+// Flat-terrain slow stage on owned 32 x 16 tiles fed by TMA (not for tend_only).
+cudaError_t launch_slow_tma(const SlowArgs& a, const SlowMaps& m, cudaStream_t s);
+cudaError_t init_slow_tma();
 // Flat-terrain acoustic substep fed by TMA tile loads (owned 32 x 16 tiles).
 cudaError_t launch_fast_tma(const FastArgs& a, const FastMaps& m, bool first, cudaStream_t s);
 // One-time kernel attributes (dynamic shared memory) of the TMA substep.

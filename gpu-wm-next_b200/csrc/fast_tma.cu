@@ -51,6 +51,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
   __shared__ float s_du[2][TY][TX + 1];     // new X-face increments (own + east face)
   __shared__ float s_dv[2][TY + 1][TX];     // new Y-face increments (own + north face)
   __shared__ float s_pref[kMaxNz], s_rref[kMaxNz], s_idzc[kMaxNz], s_idzf[kMaxNz];
+  __shared__ double s_binv[kMaxNz], s_bpr[kMaxNz];  // EOS base state: 1/rt_ref, p_ref
   __shared__ long long s_red[2][NW][2];
   __shared__ __align__(8) uint64_t s_bar[NSLOT];
   __shared__ int s_abort[2];  // per plane parity: set before barrier k, read after it
@@ -94,6 +95,8 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     s_pref[q] = (float)(acc_read(a.ref_b + q, kScaleP) * a.inv_count);
     s_idzc[q] = __ldg(a.idz_c + q);
     s_idzf[q] = __ldg(a.idz_f + q);
+    s_binv[q] = __ldg(a.base + nz + q);
+    s_bpr[q] = __ldg(a.base + 2 * nz + q);
   }
   __syncthreads();
 
@@ -131,7 +134,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
   // K10 + K20: pressure perturbation of plane kk at the owned cells and the halo ring
   auto cell_p = [&](const float* st, int r, int c, int kk) {
     const float rho = st[O_RHO + r * CBW + c + 3], th = st[O_TH + r * CBW + c + 3];
-    return eos_pprime(rho, rho * th, a.base, kk, nz);
+    return eos_pprime_ref(rho, rho * th, s_binv[kk], s_bpr[kk]);
   };
   auto plane_p = [&](int kk) {
     const float* st = ring + (kk % NSLOT) * slot;
@@ -251,7 +254,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
         store_tile(a.dv_out, g, kFaceY, gi, gj0, k, vn0, edge);
         if (k + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj0, k + 1, wn0, edge);
       }
-      if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime(rn, rt, a.base, k, nz), kFxP); }
+      if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime_ref(rn, rt, s_binv[k], s_bpr[k]), kFxP); }
       else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
     }
     if (own1) {
@@ -275,7 +278,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
         store_tile(a.dv_out, g, kFaceY, gi, gj1, k, vn1, edge);
         if (k + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj1, k + 1, wn1, edge);
       }
-      if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime(rn, rt, a.base, k, nz), kFxP); }
+      if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime_ref(rn, rt, s_binv[k], s_bpr[k]), kFxP); }
       else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
     }
     if (acc_mode) {

@@ -1,0 +1,407 @@
+// slow_tma.cu — one fused slow RK stage (flat terrain) on owned tiles fed by TMA.
+//
+// Same operator and per-cell arithmetic as k_slow_stage<false, R>: the K2/K3/K16-K19/
+// K21/K22 tendencies of compute_slow_tendencies (src/dycore/dry_core.cu:400-539), the
+// stage update K4 (:189-197) and the SSPRK3 blend K5 (:199-205).  The data path is
+// different.  A CTA owns a 32 x 16 tile, two columns per thread, and one elected
+// thread fetches each plane's boxes with cp.async.bulk.tensor.3d into a three-slot
+// shared-memory ring two planes ahead:
+//   rho, theta (or rho*theta), u, w (+ du, dw)   40 x 18 boxes, columns i0-4..i0+35,
+//                                                rows j0-1..j0+16 (tile, halo ring,
+//                                                corners; x stays 16-byte aligned)
+//   v (+ dv)                                     40 x 19 (one more Y-face row)
+// Plane nz carries only w (+ dw), the top faces.  Per plane the CTA derives theta, the
+// pressure perturbation and the cell velocities uc, vc, wc at all 34 x 18 positions
+// of the tile and its ring (corners included: the Y-face fluxes need uc there), then
+// one barrier publishes them and every thread computes its cells and faces.  uc, vc,
+// wc are triple-buffered (a face at plane k reads planes k-1 and k while the next
+// plane is derived), theta and p double-buffered, so one barrier per plane suffices.
+// The blend partner q0 is read per thread (owned positions only, coalesced).
+#include "dycore.cuh"
+#include "tma.cuh"
+
+namespace gwmb {
+namespace {
+
+namespace sl {
+constexpr int TX = 32, TY = 16, RY = 8, NT = 256, NW = NT / 32;
+constexpr int BW = 40, BH = 18, BHV = 19;  // boxes: cells, X and Z faces / Y faces
+constexpr int DW = TX + 2, DH = TY + 2, DN = DW * DH;  // derived plane: 34 x 18
+// raw slot (floats; sub-buffers on 128-byte boundaries)
+constexpr int R_RHO = 0, R_TH = 736, R_U = 1472, R_W = 2208, R_V = 2944, R_DU = 3712, R_DW = 4448,
+              R_DV = 5184, SLOT = 5952, SLOT_SHORT = 3712, NSLOT = 3;
+constexpr unsigned B_BOX = BW * BH * 4, B_BOXV = BW * BHV * 4;
+// derived arrays (floats): uc, vc, wc [3][DN]; theta, p [2][DN]
+constexpr int D_UC = 0, D_VC = 3 * DN, D_WC = 6 * DN, D_TH = 9 * DN, D_P = 11 * DN, DERIVED = 13 * DN;
+static_assert(R_TH % 32 == 0 && R_U % 32 == 0 && R_W % 32 == 0 && R_V % 32 == 0 && R_DU % 32 == 0 &&
+                  R_DW % 32 == 0 && R_DV % 32 == 0 && SLOT % 32 == 0 && SLOT_SHORT == R_DU,
+              "128-byte aligned sub-buffers");
+static_assert(R_TH - R_RHO >= BW * BH && R_U - R_TH >= BW * BH && R_W - R_U >= BW * BH &&
+                  R_V - R_W >= BW * BH && R_DU - R_V >= BW * BHV && R_DW - R_DU >= BW * BH &&
+                  R_DV - R_DW >= BW * BH && SLOT - R_DV >= BW * BHV,
+              "boxes fit their sub-buffers");
+constexpr size_t smem_bytes(bool inc) {
+  return size_t((inc ? SLOT : SLOT_SHORT) * NSLOT + DERIVED) * sizeof(float) + 128;
+}
+}  // namespace sl
+
+// Values of one owned column carried from plane k-1 to plane k.
+struct SlowCarry {
+  float rho, th, uf, vf, wf;
+};
+// Blend partner q0 at a column's owned positions of one plane.
+struct SlowBlend {
+  float rho, rt, u, v, w;
+};
+
+template <bool INC>
+__global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const __grid_constant__ SlowMaps m) {
+  using namespace sl;
+  extern __shared__ unsigned char s_dyn[];
+  __shared__ float s_thref[kMaxNz];
+  __shared__ double s_binv[kMaxNz], s_bpr[kMaxNz];  // EOS base state: 1/rt_ref, p_ref
+  __shared__ long long s_red[2][NW][2];
+  __shared__ __align__(8) uint64_t s_bar[NSLOT];
+  __shared__ int s_abort[2];
+  constexpr int slot = INC ? SLOT : SLOT_SHORT;
+  float* const ring = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
+  float* const der = ring + NSLOT * slot;
+
+  const Geom& g = a.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int w = min(TX, nx - i0), h = min(TY, ny - j0);
+  const bool own0 = tx < w && ty < h, own1 = tx < w && ty + RY < h;
+  const int gi = i0 + tx, gj0 = j0 + ty, gj1 = j0 + ty + RY;
+  const bool open_x = !g.per_x, open_y = !g.per_y;
+  const bool edge = (g.per_x && (i0 <= 1 || i0 + w >= nx - 1)) || (g.per_y && (j0 <= 1 || j0 + h >= ny - 1));
+  const float idx = g.inv_dx, idy = g.inv_dy, dt = a.dt;
+  const bool blend = a.rho0 != nullptr;
+  // open boundaries: X face nx and Y face ny belong to the last tiles; their tendency
+  // is zero (dry_momentum_flux.cu:79-235 skips them), so they are blends of the stage
+  // value.  Under periodic wrap they are the mirrors of faces 0 written by store_tile.
+  const bool xf = open_x && i0 + w == nx && ty == 0 && tx < h;  // X face nx, row j0+tx
+  const bool yf = open_y && j0 + h == ny && ty == 1 && tx < w;  // Y face ny, column i0+tx
+
+  if (tid == 0) {
+    for (int s = 0; s < NSLOT; ++s) mbar_init(&s_bar[s], 1);
+    mbar_fence_init();
+    s_abort[0] = 0;
+    s_abort[1] = 0;
+  }
+  if (blockIdx.x == 0 && blockIdx.y == 0 && a.clr_a)
+    for (int q = tid; q < nz; q += NT) { a.clr_a[q] = 0ull; a.clr_b[q] = 0ull; }
+  for (int q = tid; q < nz; q += NT) {
+    s_thref[q] = (float)(acc_read(a.th_acc + q, kScaleTheta) * a.inv_count);
+    s_binv[q] = __ldg(a.base + nz + q);
+    s_bpr[q] = __ldg(a.base + 2 * nz + q);
+  }
+  __syncthreads();
+
+  auto issue = [&](int kk) {  // plane kk in [0, nz] into slot kk % NSLOT
+    float* sr = ring + (kk % NSLOT) * slot;
+    uint64_t* bar = &s_bar[kk % NSLOT];
+    const bool cells = kk < nz;
+    unsigned bytes = (INC ? 2u : 1u) * B_BOX;
+    if (cells) bytes += 3 * B_BOX + B_BOXV + (INC ? B_BOX + B_BOXV : 0u);
+    const int x = i0 + kXOff - 4, y = j0;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, bytes);
+    tma_load_3d(sr + R_W, &m.w, x, y, kk, bar);
+    if (INC) tma_load_3d(sr + R_DW, &m.dw, x, y, kk, bar);
+    if (cells) {
+      tma_load_3d(sr + R_RHO, &m.rho, x, y, kk, bar);
+      tma_load_3d(sr + R_TH, &m.th, x, y, kk, bar);
+      tma_load_3d(sr + R_U, &m.u, x, y, kk, bar);
+      tma_load_3d(sr + R_V, &m.v, x, y, kk, bar);
+      if (INC) {
+        tma_load_3d(sr + R_DU, &m.du, x, y, kk, bar);
+        tma_load_3d(sr + R_DV, &m.dv, x, y, kk, bar);
+      }
+    }
+  };
+  int issued = -1, waited = -1;
+  auto wait_plane = [&](int kk, int epoch) {
+    if (!mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1)) {
+      s_abort[epoch & 1] = 1;
+      atomicExch(a.err, 1);
+    }
+    waited = kk;
+  };
+  // raw accessors: box index of derived position (r, c) is r * BW + c + 3
+  auto U = [&](const float* sr, int b) { return INC ? sr[R_U + b] + sr[R_DU + b] : sr[R_U + b]; };
+  auto V = [&](const float* sr, int b) { return INC ? sr[R_V + b] + sr[R_DV + b] : sr[R_V + b]; };
+  auto W = [&](const float* sr, int b) { return INC ? sr[R_W + b] + sr[R_DW + b] : sr[R_W + b]; };
+  auto RT = [&](const float* sr, int b) {
+    const float t = sr[R_TH + b];
+    return a.th_is_rt ? t : sr[R_RHO + b] * t;
+  };
+
+  // blend partner of plane kk at the thread's owned positions
+  auto load_q0 = [&](int gj, bool own, int kk) {
+    SlowBlend q{0.f, 0.f, 0.f, 0.f, 0.f};
+    if (!blend || !own || kk >= nz) return q;
+    const int o = gidx(g, gi, gj, kk);
+    q.rho = __ldg(a.rho0 + o);
+    q.rt = __ldg(a.rt0 + o);
+    q.u = __ldg(a.u0 + o);
+    q.v = __ldg(a.v0 + o);
+    q.w = __ldg(a.w0 + o);
+    return q;
+  };
+
+  if (tid == 0) {
+    issue(0);
+    issue(1);
+    issued = 1;
+  }
+  SlowBlend q0a = load_q0(gj0, own0, 0), q0b = load_q0(gj1, own1, 0);
+  SlowCarry ca{0.f, 0.f, 0.f, 0.f, 0.f}, cb{0.f, 0.f, 0.f, 0.f, 0.f};
+  wait_plane(0, 0);
+
+  // one owned column: cell, X face, Y face and Z face of plane k (+ the top face)
+  auto column = [&](int k, int r, int gj, bool own, SlowCarry& cy, const SlowBlend& q0, FxAcc& ra, FxAcc& rb) {
+    const float* sr = ring + (k % NSLOT) * slot;
+    const float* sn = ring + ((k + 1) % NSLOT) * slot;
+    const float* uc = der + D_UC + (k % 3) * DN;
+    const float* vc = der + D_VC + (k % 3) * DN;
+    const float* wc = der + D_WC + (k % 3) * DN;
+    const float* ucm = der + D_UC + ((k + 2) % 3) * DN;  // plane k-1
+    const float* vcm = der + D_VC + ((k + 2) % 3) * DN;
+    const float* wcm = der + D_WC + ((k + 2) % 3) * DN;
+    const float* th = der + D_TH + (k & 1) * DN;
+    const float* pp = der + D_P + (k & 1) * DN;
+    const int c = tx + 1;
+    const int d = r * DW + c;   // derived index
+    const int b = r * BW + c + 3;  // raw box index
+    const bool top = k + 1 == nz;
+    // values of the column at planes k and k+1
+    const float rho = sr[R_RHO + b], rt = RT(sr, b);
+    const float tc = th[d], pc = pp[d];
+    const float uf = U(sr, b), vf = V(sr, b), wf = W(sr, b);
+    const float wft = W(sn, b);  // face k+1 (plane nz holds the top faces)
+    float uft = uf, vft = vf, tt = tc;
+    if (!top) {
+      uft = U(sn, b);
+      vft = V(sn, b);
+      tt = theta_of(sn[R_RHO + b], RT(sn, b));
+    }
+    const float tb = k > 0 ? cy.th : tc;
+    const float idz = __ldg(a.idz_c + k);
+    // ---- cell: K2 compute_cell_tendencies_kernel (dry_core.cu:62-144)
+    {
+      const float fw = uf, fe = U(sr, b + 1), fs = vf, fn = V(sr, b + BW);
+      const float fb = wf, ft = wft;
+      const float div = (fe - fw) * idx + (fn - fs) * idy + (ft - fb) * idz;
+      const float t_rho = -div;
+      const float tw = th[d - 1], te = th[d + 1], ts = th[d - DW], tn = th[d + DW];
+      const float gw = fw * (fw >= 0.0f ? tw : tc);
+      const float ge = fe * (fe >= 0.0f ? tc : te);
+      const float gs = fs * (fs >= 0.0f ? ts : tc);
+      const float gn = fn * (fn >= 0.0f ? tc : tn);
+      const float gb = fb * (fb >= 0.0f ? tb : tc);
+      const float gt = ft * (ft >= 0.0f ? tc : tt);
+      const float t_rt = -((ge - gw) * idx + (gn - gs) * idy + (gt - gb) * idz);
+      float r1 = fmaxf(1.0e-6f, rho + dt * t_rho);
+      float q1 = fmaxf(1.0e-6f, rt + dt * t_rt);
+      if (blend) {
+        r1 = a.wa * q0.rho + a.wb * r1;
+        q1 = a.wa * q0.rt + a.wb * q1;
+      }
+      const float th1 = q1 / fmaxf(r1, 1.0e-6f);
+      if (own) {
+        store_tile(a.o_rho, g, kCell, gi, gj, k, r1, edge);
+        store_tile(a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1, edge);
+        if (a.acc_mode == 1) {
+          ra.add(r1, kFxRho);
+          rb.add(eos_pprime_ref(r1, r1 * th1, s_binv[k], s_bpr[k]), kFxP);
+        } else if (a.acc_mode == 2) {
+          ra.add(th1, kFxTheta);
+        }
+      }
+    }
+    // ---- X face: K17 (dry_momentum_flux.cu:79-156) + K21 (dry_pressure_gradient.cu:75-123)
+    {
+      float t_u = 0.0f;
+      if (!(gi == 0 && open_x)) {
+        const float qw = U(sr, b - 1), qc = uf, qe = U(sr, b + 1);
+        const float qs = U(sr, b - BW), qn = U(sr, b + BW);
+        const float qb = k > 0 ? cy.uf : qc;
+        const float qt = top ? qc : uft;
+        const float flw = upwind(uc[d - 1], qw, qc);
+        const float fle = upwind(uc[d], qc, qe);
+        float fls = 0.0f, fln = 0.0f, flb = 0.0f, flt = 0.0f;
+        if (!(gj == 0 && open_y)) fls = upwind(0.5f * (vc[d - DW - 1] + vc[d - DW]), qs, qc);
+        if (!(gj + 1 == ny && open_y)) fln = upwind(0.5f * (vc[d - 1] + vc[d]), qc, qn);
+        if (k > 0) flb = upwind(0.5f * (wcm[d - 1] + wcm[d]), qb, qc);
+        if (!top) flt = upwind(0.5f * (wc[d - 1] + wc[d]), qc, qt);
+        t_u = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
+        t_u += -((pc - pp[d - 1]) * idx);
+      }
+      float u1 = fmaxf(-1.0e30f, uf + dt * t_u);
+      if (blend) u1 = a.wa * q0.u + a.wb * u1;
+      if (own) store_tile(a.o_u, g, kFaceX, gi, gj, k, u1, edge);
+    }
+    // ---- Y face: K18 (dry_momentum_flux.cu:158-235) + K22 (dry_pressure_gradient.cu:125-173)
+    {
+      float t_v = 0.0f;
+      if (!(gj == 0 && open_y)) {
+        const float qw = V(sr, b - 1), qc = vf, qe = V(sr, b + 1);
+        const float qs = V(sr, b - BW), qn = V(sr, b + BW);
+        const float qb = k > 0 ? cy.vf : qc;
+        const float qt = top ? qc : vft;
+        float flw = 0.0f, fle = 0.0f, flb = 0.0f, flt = 0.0f;
+        if (!(gi == 0 && open_x)) flw = upwind(0.5f * (uc[d - DW - 1] + uc[d - 1]), qw, qc);
+        if (!(gi + 1 == nx && open_x)) fle = upwind(0.5f * (uc[d - DW] + uc[d]), qc, qe);
+        const float fls = upwind(vc[d - DW], qs, qc);
+        const float fln = upwind(vc[d], qc, qn);
+        if (k > 0) flb = upwind(0.5f * (wcm[d - DW] + wcm[d]), qb, qc);
+        if (!top) flt = upwind(0.5f * (wc[d - DW] + wc[d]), qc, qt);
+        t_v = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
+        t_v += -((pc - pp[d - DW]) * idy);
+      }
+      float v1 = fmaxf(-1.0e30f, vf + dt * t_v);
+      if (blend) v1 = a.wa * q0.v + a.wb * v1;
+      if (own) store_tile(a.o_v, g, kFaceY, gi, gj, k, v1, edge);
+    }
+    // ---- Z face k: K19 (dry_momentum_flux.cu:237-312) + K3 buoyancy (dry_core.cu:146-187)
+    {
+      float t_w = 0.0f;
+      if (k > 0) {
+        const float qw = W(sr, b - 1), qc = wf, qe = W(sr, b + 1);
+        const float qs = W(sr, b - BW), qn = W(sr, b + BW);
+        const float qb = cy.wf, qt = wft;
+        float flw = 0.0f, fle = 0.0f, fls = 0.0f, fln = 0.0f;
+        if (!(gi == 0 && open_x)) flw = upwind(0.5f * (ucm[d - 1] + uc[d - 1]), qw, qc);
+        if (!(gi + 1 == nx && open_x)) fle = upwind(0.5f * (ucm[d] + uc[d]), qc, qe);
+        if (!(gj == 0 && open_y)) fls = upwind(0.5f * (vcm[d - DW] + vc[d - DW]), qs, qc);
+        if (!(gj + 1 == ny && open_y)) fln = upwind(0.5f * (vcm[d] + vc[d]), qc, qn);
+        const float flb = upwind(wcm[d], qb, qc);
+        const float flt = upwind(wc[d], qc, qt);
+        const float idzf = __ldg(a.idz_f + k);
+        t_w = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idzf);
+        const float tf = 0.5f * (cy.th + tc);
+        const float trf = 0.5f * (s_thref[k - 1] + s_thref[k]);
+        const float rf = 0.5f * (cy.rho + rho);
+        const float bu = a.gravity * (tf - trf) / fmaxf(trf, 1.0e-6f);
+        t_w += rf * bu;
+      }
+      float w1 = fmaxf(-1.0e30f, wf + dt * t_w);
+      if (blend) w1 = a.wa * q0.w + a.wb * w1;
+      if (own) {
+        store_tile(a.o_w, g, kFaceZ, gi, gj, k, w1, edge);
+        if (top) {  // top face: zero tendency
+          float wt = fmaxf(-1.0e30f, wft);
+          if (blend) wt = a.wa * __ldg(a.w0 + gidx(g, gi, gj, nz)) + a.wb * wt;
+          store_tile(a.o_w, g, kFaceZ, gi, gj, nz, wt, edge);
+        }
+      }
+    }
+    cy.rho = rho;
+    cy.th = tc;
+    cy.uf = uf;
+    cy.vf = vf;
+    cy.wf = wf;
+  };
+
+  bool aborted = false;
+  for (int k = 0; k < nz; ++k) {
+    const int pb = k & 1;
+    // ---- derive plane k: theta, p', uc, vc, wc at the 34 x 18 positions
+    wait_plane(k + 1, k);
+    {
+      const float* sr = ring + (k % NSLOT) * slot;
+      const float* sn = ring + ((k + 1) % NSLOT) * slot;
+      float* uc = der + D_UC + (k % 3) * DN;
+      float* vc = der + D_VC + (k % 3) * DN;
+      float* wc = der + D_WC + (k % 3) * DN;
+      float* th = der + D_TH + pb * DN;
+      float* pp = der + D_P + pb * DN;
+      for (int q = tid; q < DN; q += NT) {
+        const int r = q / DW, c = q - r * DW;
+        const int b = r * BW + c + 3;
+        const float rho = sr[R_RHO + b], rt = RT(sr, b);
+        th[q] = theta_of(rho, rt);
+        pp[q] = eos_pprime_ref(rho, rt, s_binv[k], s_bpr[k]);
+        // cell-centred velocities: dry_momentum_flux.cu:36-73
+        const float rr = fmaxf(rho, 1.0e-6f);
+        uc[q] = 0.5f * (U(sr, b) + U(sr, b + 1)) / rr;
+        vc[q] = 0.5f * (V(sr, b) + V(sr, b + BW)) / rr;
+        wc[q] = 0.5f * (W(sr, b) + W(sn, b)) / rr;
+      }
+    }
+    const SlowBlend n0a = load_q0(gj0, own0, k + 1), n0b = load_q0(gj1, own1, k + 1);
+    __syncthreads();  // publishes plane k's derived values; slot (k-1) is free
+    if (s_abort[pb]) { aborted = true; break; }
+    if (tid == 0) {
+      if (a.acc_mode && k > 0) {
+        long long sa = 0, sb = 0;
+        for (int q = 0; q < NW; ++q) { sa += s_red[pb ^ 1][q][0]; sb += s_red[pb ^ 1][q][1]; }
+        acc_add(a.acc_a + k - 1, sa);
+        if (a.acc_mode == 1) acc_add(a.acc_b + k - 1, sb);
+      }
+      if (k + 2 <= nz) { issue(k + 2); issued = k + 2; }
+    }
+    // ---- cells and faces of plane k
+    FxAcc ra, rb;
+    column(k, ty + 1, gj0, own0, ca, q0a, ra, rb);
+    column(k, ty + RY + 1, gj1, own1, cb, q0b, ra, rb);
+    if (xf) {  // open east boundary: X face nx of row j0+tx
+      const float* sr = ring + (k % NSLOT) * slot;
+      const float uf = U(sr, (tx + 1) * BW + w + 4);
+      float u1 = fmaxf(-1.0e30f, uf + dt * 0.0f);
+      if (blend) u1 = a.wa * __ldg(a.u0 + gidx(g, nx, j0 + tx, k)) + a.wb * u1;
+      store_tile(a.o_u, g, kFaceX, nx, j0 + tx, k, u1, edge);
+    }
+    if (yf) {  // open north boundary: Y face ny of column i0+tx
+      const float* sr = ring + (k % NSLOT) * slot;
+      const float vf = V(sr, (h + 1) * BW + tx + 4);
+      float v1 = fmaxf(-1.0e30f, vf + dt * 0.0f);
+      if (blend) v1 = a.wa * __ldg(a.v0 + gidx(g, i0 + tx, ny, k)) + a.wb * v1;
+      store_tile(a.o_v, g, kFaceY, i0 + tx, ny, k, v1, edge);
+    }
+    if (a.acc_mode) {
+      const long long ta = ra.warp_total(), tb = rb.warp_total();
+      if (tx == 0) { s_red[pb][ty][0] = ta; s_red[pb][ty][1] = tb; }
+    }
+    q0a = n0a;
+    q0b = n0b;
+  }
+  if (aborted) {
+    if (tid == 0)
+      for (int kk = waited + 1; kk <= issued; ++kk) mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1);
+    return;
+  }
+  if (a.acc_mode) {
+    __syncthreads();
+    if (tid == 0) {
+      const int pb = (nz - 1) & 1;
+      long long sa = 0, sb = 0;
+      for (int q = 0; q < NW; ++q) { sa += s_red[pb][q][0]; sb += s_red[pb][q][1]; }
+      acc_add(a.acc_a + nz - 1, sa);
+      if (a.acc_mode == 1) acc_add(a.acc_b + nz - 1, sb);
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t init_slow_tma() {
+  cudaError_t e = cudaFuncSetAttribute(k_slow_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sl::smem_bytes(true));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_slow_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sl::smem_bytes(false));
+}
+
+cudaError_t launch_slow_tma(const SlowArgs& a, const SlowMaps& m, cudaStream_t s) {
+  if (a.g.nz > kMaxNz || a.g.nz < 1 || !a.err || a.tend_only) return cudaErrorInvalidValue;
+  const dim3 block(sl::TX, sl::RY);
+  const dim3 grid((a.g.nx + sl::TX - 1) / sl::TX, (a.g.ny + sl::TY - 1) / sl::TY);
+  if (a.du) k_slow_tma<true><<<grid, block, sl::smem_bytes(true), s>>>(a, m);
+  else k_slow_tma<false><<<grid, block, sl::smem_bytes(false), s>>>(a, m);
+  return cudaGetLastError();
+}
+
+}  // namespace gwmb

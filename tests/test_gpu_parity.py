@@ -136,7 +136,7 @@ def bubble_grid(gwm, nx=32, ny=32, nz=40, **kw):
 
 
 def c1_state(gwm, g, u=0.0, v=0.0):
-    # +2 K cos^2 bubble (2 km radius, z = 2 km) on a 300 K hydrostatic base
+    # C1 warm bubble: +2 K cos^2 bubble (2 km radius, z = 2 km) on a 300 K hydrostatic base
     p = gwm.CaseParams(rho_surface=np.float32(1e5 / (287.05 * 300.0)), theta_ref=300.0,
                        theta_perturbation=2.0, center_x_fraction=0.5, center_y_fraction=0.5,
                        center_z_fraction=0.2, radius_x_fraction=2000.0 / (g.nx * g.dx),
@@ -255,7 +255,7 @@ def run_both(gwm, orc, g, step, state, nsteps, graph=False):
 
 @pytest.mark.parametrize("dt,nsteps", [(2.0, 1), (0.5, 4)])
 def test_c1_warm_bubble_vs_fp64_oracle(gwm, orc, dt, nsteps):
-    # BASELINE config 1 grid and state: 32x32x40, 500 m, dz 250 m, 3 acoustic substeps.
+    # C1 grid and state: 32x32x40, 500 m, dz 250 m, 3 acoustic substeps.
     # At the configured dt = 2 s the reference discretisation is unstable from the
     # second step on (c*dt/dz = 2.8 in the slow stage; the FP64 oracle reaches
     # |w| ~ 1e19 at step 2), so the exact configuration is compared over one step
@@ -463,15 +463,17 @@ def test_stage_tilings_bit_exact(gwm, kernel, periodic):
     step = gwm.StepConfig(dt=1.0, fast_substeps=4)
     rain = gwm.WarmRainConfig(dt=1.0, rain_terminal_velocity=12.0)
     outs = {}
-    for r in (8, 16):
+    choices = (3, 8, 16) if kernel == "slow_stage" else (8, 16)  # 3: owned tiles fed by TMA
+    for r in choices:
         with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=True)) as m:
             m.set_tile(kernel, r)
             assert m.get_tile(kernel) == r
             m.upload(s)
             m.step(2)
             outs[r] = m.download()
-    for k in outs[8]:
-        assert np.array_equal(outs[8][k], outs[16][k]), k
+    for r in choices[1:]:
+        for k in outs[16]:
+            assert np.array_equal(outs[choices[0]][k], outs[r][k]), (r, k)
 
 
 @pytest.mark.parametrize("periodic", [True, False])
@@ -494,3 +496,22 @@ def test_tma_substep_bit_exact(gwm, periodic):
             outs[r] = m.download()
     for k in outs[0]:
         assert np.array_equal(outs[0][k], outs[3][k]), k
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_tma_slow_stage_without_fast_modes(gwm, periodic):
+    # the TMA slow stage on stage inputs without acoustic increments (fast modes off)
+    # and with the last stage writing rho*theta straight into the state
+    g = gwm.GridSpec(72, 40, 10, dx=1000.0, dy=1000.0, z_top=10000.0,
+                     periodic_x=periodic, periodic_y=periodic)
+    s = c1_state(gwm, g, u=3.0, v=-1.0)
+    step = gwm.StepConfig(dt=0.5, fast_substeps=2, enable_fast_modes=False)
+    outs = {}
+    for r in (3, 16):
+        with gwm.Model(g, gwm.MemberSpec(step=step)) as m:
+            m.set_tile("slow_stage", r)
+            m.upload(s)
+            m.advance_dry_state_ssprk3(2)
+            outs[r] = m.download()
+    for k in outs[16]:
+        assert np.array_equal(outs[3][k], outs[16][k]), k
