@@ -26,7 +26,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _ROOT = os.path.dirname(_HERE)
 _LIB_PATH = os.path.join(_HERE, "_build", "libgwm_b200.so")
-_SOURCES = ["capi.cu", "dycore.cu", "fast_tma.cu", "slow_tma.cu", "physics.cu", "halo.cu", "cases.cpp"]
+_SOURCES = ["capi.cu", "dycore.cu", "fast_tma.cu", "slow_tma.cu", "tracer_tma.cu", "physics.cu", "halo.cu",
+            "cases.cpp"]
 _HEADERS = ["common.cuh", "dycore.cuh", "physics.cuh", "halo.cuh", "tma.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
@@ -429,8 +430,8 @@ class Model:
 
     def set_tile(self, kernel: str, rows: int):
         """CTA tile rows of a kernel: "slow_stage" 3 (owned flat tiles fed by TMA), 8 or 16;
-        "tracer_stage" 8 or 16; "fast_substep" 0 (owned flat tiles), 3 (owned flat
-        tiles fed by TMA), 8 or 16."""
+        "tracer_stage" 3 (owned flat tiles fed by TMA), 8 or 16; "fast_substep" 0 (owned
+        flat tiles), 3 (owned flat tiles fed by TMA), 8 or 16."""
         self._check(lib().gwm_b200_set_tile(self._h, self._TILE_KERNELS[kernel], rows), "set_tile")
 
     def get_tile(self, kernel: str) -> int:
@@ -443,10 +444,10 @@ class Model:
         """Pick the fastest tile of each stencil kernel by timing real steps.
 
         Every tiling computes the same values, so the tuning steps are ordinary
-        model steps: the state advances by ``steps`` per candidate (9 candidates
+        model steps: the state advances by ``steps`` per candidate (10 candidates
         per pass).  Re-upload the initial state afterwards to start from it.
         Returns the chosen rows per kernel."""
-        candidates = {"slow_stage": (3, 8, 16), "fast_substep": (0, 3, 8, 16), "tracer_stage": (8, 16)}
+        candidates = {"slow_stage": (3, 8, 16), "fast_substep": (0, 3, 8, 16), "tracer_stage": (3, 8, 16)}
         kinds = {"slow_stage": "k_slow_stage", "fast_substep": "k_fast_substep",
                  "tracer_stage": "k_tracer_stage"}
         best = {k: self.get_tile(k) for k in candidates}

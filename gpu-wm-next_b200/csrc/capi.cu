@@ -250,6 +250,10 @@ bool build_substep_maps(Member& M) {
     ok = ok && add(M.B[i][0], 0) && add(M.B[i][2], 0) && add(M.B[i][1], 3);
     ok = ok && add(M.D[i][0], 0) && add(M.D[i][2], 0) && add(M.D[i][1], 3);
   }
+  // tracer stage: the three tracer generations (cells) and the frozen X/Y fluxes
+  if (M.md.moist)
+    for (int t = 0; t < 3; ++t) ok = ok && add(M.T0[t], 0) && add(M.T1[t], 0) && add(M.T2[t], 0);
+  ok = ok && add(M.Q[2], 1) && add(M.Q[3], 1);
   if (!ok) M.tmaps.clear();
   return ok;
 }
@@ -331,6 +335,27 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
 
 constexpr int kFastTma = 3;  // fast_tile_rows value selecting the TMA-fed substep
 constexpr int kSlowTma = 3;  // slow_tile_rows value selecting the TMA-fed slow stage
+constexpr int kTracerTma = 3;  // tracer_tile_rows value selecting the TMA-fed tracer stage
+
+// One tracer stage: the TMA-fed kernel when selected on flat terrain, else overlapped tiles.
+cudaError_t launch_tracers(gwm_b200_ctx* c, const Member& M, const TracerArgs& a) {
+  if (!a.terrain && c->tracer_tile_rows == kTracerTma) {
+    TracerMaps m{};
+    const CUtensorMap* rho = M.tmap(a.rho, 0);
+    const CUtensorMap* u = M.tmap(a.u, 1);
+    const CUtensorMap* v = M.tmap(a.v, 1);
+    const CUtensorMap* w = M.tmap(a.w, 2);
+    if (!rho || !u || !v || !w) return cudaErrorInvalidValue;
+    for (int t = 0; t < a.ntracers; ++t) {
+      const CUtensorMap* q = M.tmap(a.q_in[t], 0);
+      if (!q) return cudaErrorInvalidValue;
+      m.q[t] = *q;
+    }
+    m.rho = *rho; m.u = *u; m.v = *v; m.w = *w;
+    return launch_tracer_tma(a, m, c->stream);
+  }
+  return launch_tracer_stage(a, c->stream, c->tracer_tile_rows == kTracerTma ? 16 : c->tracer_tile_rows);
+}
 
 // One slow stage: the TMA-fed kernel when selected on flat terrain, else overlapped tiles.
 cudaError_t launch_stage(gwm_b200_ctx* c, const Member& M, const SlowArgs& a, bool terr) {
@@ -540,7 +565,8 @@ int enqueue_tracers(gwm_b200_ctx* c, Member& M) {
     a.wa = wa[s]; a.wb = wb[s]; a.dt = M.md.step.dt;
     a.ntracers = 3;
     a.idz_c = M.idc; a.terrain = M.terrain_active;
-    LAUNCH(launch_tracer_stage(a, c->stream, c->tracer_tile_rows), "tracer stage");
+    a.err = M.err;
+    LAUNCH(launch_tracers(c, M, a), "tracer stage");
   }
   return GWM_B200_OK;
 }
@@ -609,7 +635,7 @@ int gwm_b200_create(const gwm_b200_grid_desc* grids, const gwm_b200_member_desc*
   cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete c; return GWM_B200_ERR_CUDA; }
   c->stream = c->own_stream;
-  if (init_fast_tma() != cudaSuccess || init_slow_tma() != cudaSuccess) {
+  if (init_fast_tma() != cudaSuccess || init_slow_tma() != cudaSuccess || init_tracer_tma() != cudaSuccess) {
     cudaStreamDestroy(c->own_stream);
     delete c;
     return GWM_B200_ERR_CUDA;
@@ -690,9 +716,9 @@ int gwm_b200_set_tile(gwm_b200_ctx* c, int kernel, int rows) {
   if (!c) return GWM_B200_ERR_ARG;
   const bool ok = kernel == 1   ? (rows == 0 || rows == kFastTma || rows == 8 || rows == 16)
                   : kernel == 0 ? (rows == kSlowTma || rows == 8 || rows == 16)
-                                : kernel == 2 && (rows == 8 || rows == 16);
+                                : kernel == 2 && (rows == kTracerTma || rows == 8 || rows == 16);
   if (!ok) return GWM_B200_ERR_ARG;
-  if ((kernel == 1 && rows == kFastTma) || (kernel == 0 && rows == kSlowTma))
+  if ((kernel == 1 && rows == kFastTma) || (kernel == 0 && rows == kSlowTma) || (kernel == 2 && rows == kTracerTma))
     for (const auto& M : c->m)
       if (!M.terrain_active && M.tmaps.empty())
         return fail(c, GWM_B200_ERR_ARG, "TMA substep unavailable (tensor-map encoder not found)");

@@ -2,6 +2,8 @@
 // stages and warm-rain microphysics with bounded column fallout.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace gwmb {
@@ -20,6 +22,14 @@ struct TracerArgs {
   int ntracers;
   const float* idz_c;               // per level (flat) or padded 3-D (terrain)
   int terrain;
+  int* err;                         // error word: set to 1 when a bounded wait gave up
+};
+
+// TMA descriptors of one tracer stage (flat terrain, k_tracer_tma).
+struct TracerMaps {
+  CUtensorMap rho, q[3];  // box 40 x 18: cells with the halo ring
+  CUtensorMap u, v;       // box 36 x 17: owned faces + the east/north face
+  CUtensorMap w;          // box 32 x 16
 };
 
 // Warm-rain microphysics (warm_rain.cu:36-120) followed, in the same column
@@ -39,6 +49,9 @@ struct RainArgs {
 
 // tile_rows: CTA rows of the overlapped tracer tile (8 or 16; 32 columns wide).
 cudaError_t launch_tracer_stage(const TracerArgs& a, cudaStream_t s, int tile_rows);
+// Flat-terrain tracer stage on owned 32 x 16 tiles fed by TMA.
+cudaError_t launch_tracer_tma(const TracerArgs& a, const TracerMaps& m, cudaStream_t s);
+cudaError_t init_tracer_tma();
 cudaError_t launch_warm_rain(const RainArgs& a, cudaStream_t s);
 
 }  // namespace gwmb

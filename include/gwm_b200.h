@@ -153,7 +153,8 @@ int gwm_b200_slow_tendencies(gwm_b200_ctx* ctx, int member, gwm_b200_fields* hos
 int gwm_b200_budgets(gwm_b200_ctx* ctx, int member, gwm_b200_budget* out);
 /* Tile shape of a kernel.  kernel 0 = slow stage: rows 3 = owned 32x16 tiles fed by
  * TMA tile loads (flat terrain; terrain falls back to 16), 8 or 16 = overlapped 32-wide
- * tiles (default 16).  kernel 2 = tracer stage: rows 8 or 16 (overlapped, default 16).  kernel 1 = acoustic substep: rows 0 = owned
+ * tiles (default 16).  kernel 2 = tracer stage: rows 3 = owned 32x16 tiles fed by TMA
+ * (flat terrain; terrain falls back to 16), 8 or 16 (overlapped, default 16).  kernel 1 = acoustic substep: rows 0 = owned
  * 32x16 tiles (flat terrain; terrain falls back to 8), 3 = owned 32x16 tiles fed by TMA
  * tile loads (flat terrain; terrain falls back to 8), 8 or 16 = overlapped 32-wide
  * tiles of that many rows.  The environment variable GWM_B200_FAST_TILE_ROWS sets the

@@ -463,7 +463,7 @@ def test_stage_tilings_bit_exact(gwm, kernel, periodic):
     step = gwm.StepConfig(dt=1.0, fast_substeps=4)
     rain = gwm.WarmRainConfig(dt=1.0, rain_terminal_velocity=12.0)
     outs = {}
-    choices = (3, 8, 16) if kernel == "slow_stage" else (8, 16)  # 3: owned tiles fed by TMA
+    choices = (3, 8, 16)  # 3: owned tiles fed by TMA
     for r in choices:
         with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=True)) as m:
             m.set_tile(kernel, r)
