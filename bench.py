@@ -265,11 +265,8 @@ def main():
     clocks.stop()
     ms = t0.elapsed_time(t1)
     launches = model.launch_count
-    ms_t = torch.tensor([ms], device="cuda")
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = cells * args.steps * world / (ms_max * 1e-3)
+    ms_max = max_over_ranks(ms, torch, dist, "cuda")
+    value = job_throughput(cells, args.steps, world, ms_max)
     budget = model.budgets()
     finite = all(np.isfinite(v) for v in budget.values())
 
@@ -353,6 +350,20 @@ def read_traffic(g):
     return per_cell * g.nx * g.ny * g.nz
 
 
+def max_over_ranks(x, torch, dist, device):
+    """The slowest rank's time: every rank contributes its own device-timed value."""
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(cells_per_rank, steps, world, ms_max):
+    """Whole-job cell updates per second: every rank advances its own replica of
+    cells_per_rank cells, and the job takes as long as its slowest rank."""
+    return cells_per_rank * steps * world / (ms_max * 1e-3)
+
+
 def end_to_end(gwm, model, g, stream, torch, steps, world, dist):
     sh = g.shapes()
     keys = ("rho", "rho_theta", "u", "v", "w", "qv", "qc", "qr")
@@ -361,18 +372,20 @@ def end_to_end(gwm, model, g, stream, torch, steps, world, dist):
     model.download(out=host)
     h2d = sum(host[k].nbytes for k in host)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    if dist:
+        dist.barrier()
+    # device-timed on the model's stream: the span from before the first upload to after
+    # the last download, host-side staging and the waits between calls included
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
     for _ in range(steps):
         model.upload(host)
         model.step(1)
         model.download(out=host)
+    t1.record(stream)
     torch.cuda.synchronize()
-    el = time.perf_counter() - t0
-    el_t = torch.tensor([el], device="cuda")
-    if dist:
-        dist.all_reduce(el_t, op=dist.ReduceOp.MAX)
-    el = float(el_t.item())
-    return {"value": g.nx * g.ny * g.nz * steps * world / el, "unit": "cell-updates/s",
+    el_ms = max_over_ranks(t0.elapsed_time(t1), torch, dist, "cuda")
+    return {"value": job_throughput(g.nx * g.ny * g.nz, steps, world, el_ms), "unit": "cell-updates/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
             "note": "full prognostic state copied host->device and back every step through the C-ABI"}
 

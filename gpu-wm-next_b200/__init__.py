@@ -160,6 +160,8 @@ def lib():
     L.gwm_b200_budgets.argtypes = [vp, C.c_int, C.POINTER(_Budget)]
     L.gwm_b200_profile.argtypes = [vp, C.c_int]
     L.gwm_b200_set_tile.argtypes = [vp, C.c_int, C.c_int]
+    L.gwm_b200_set_boundary_state.argtypes = [vp, C.c_int, C.POINTER(_Fields)]
+    L.gwm_b200_apply_reference_boundaries.argtypes = [vp, C.c_int]
     L.gwm_b200_get_tile.argtypes = [vp, C.c_int]
     L.gwm_b200_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double),
                                         C.POINTER(C.c_longlong), C.POINTER(C.c_char_p)]
@@ -187,7 +189,8 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_synchronize", "gwm_b200_use_graph", "gwm_b200_upload", "gwm_b200_download",
             "gwm_b200_step", "gwm_b200_advance_dry", "gwm_b200_advance_tracers",
             "gwm_b200_warm_rain", "gwm_b200_fast_modes", "gwm_b200_slow_tendencies",
-            "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_get_tile", "gwm_b200_layout",
+            "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_get_tile", "gwm_b200_set_boundary_state",
+            "gwm_b200_apply_reference_boundaries", "gwm_b200_layout",
             "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_ranks_to_global",
             "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
 
@@ -354,6 +357,28 @@ class Model:
             keep.append(p)
             f.precip = p.ctypes.data_as(C.POINTER(C.c_double))
         self._check(lib().gwm_b200_upload(self._h, member, C.byref(f)), "upload")
+
+    def set_boundary_state(self, boundary: Optional[Dict[str, np.ndarray]], member: int = 0):
+        """Reference boundary state applied on the open sides at every stage start
+        (apply_reference_boundaries); ``None`` removes it (the Null updaters)."""
+        if boundary is None:
+            self._check(lib().gwm_b200_set_boundary_state(self._h, member, None), "set_boundary_state")
+            return
+        sh = self.grids[member].shapes()
+        f = _Fields()
+        keep = []
+        for k, cname in _C_NAMES.items():
+            if boundary.get(k) is not None:
+                a = np.ascontiguousarray(boundary[k], dtype=np.float32)
+                if a.shape != sh[k]:
+                    raise ValueError(f"{k}: shape {a.shape} != {sh[k]}")
+                keep.append(a)
+                setattr(f, cname, _fptr(a))
+        self._check(lib().gwm_b200_set_boundary_state(self._h, member, C.byref(f)), "set_boundary_state")
+
+    def apply_reference_boundaries(self, member: int = 0):
+        """apply_reference_boundaries once on the current state."""
+        self._check(lib().gwm_b200_apply_reference_boundaries(self._h, member), "apply_reference_boundaries")
 
     def download(self, member: int = 0, keys: Optional[Sequence[str]] = None,
                  out: Optional[Dict[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:

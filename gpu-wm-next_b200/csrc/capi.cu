@@ -65,6 +65,13 @@ struct Member {
   int ring = 0;
   bool theta_valid = false;
   int* err = nullptr;                // device error word (bounded waits that gave up)
+  // reference boundary state (apply_reference_boundaries at every stage start): compact
+  // strips of rho, rho*theta, u, v, w and the three tracers; bsave holds the stage-1
+  // input's own strips, which the blends of stages 2 and 3 need unchanged
+  float* bstrip = nullptr;
+  float* bsave = nullptr;
+  long long boff[9]{};
+  bool has_boundary = false, has_tracer_boundary = false;
   // TMA descriptors of the substep's buffers: (buffer, box kind 0 cell / 1 face / 2 own, map)
   std::vector<std::tuple<const float*, int, CUtensorMap>> tmaps;
   const CUtensorMap* tmap(const float* buf, int kind) const {
@@ -398,6 +405,18 @@ cudaError_t launch_substep(gwm_b200_ctx* c, const Member& M, const FastArgs& f, 
   return launch_fast(f, first, terr, c->stream, c->fast_tile_rows);
 }
 
+constexpr int kStripOrient[8] = {kCell, kCell, kFaceX, kFaceY, kFaceZ, kCell, kCell, kCell};
+
+StripJob strip_job(float* padded, float* compact, const float* aux, int orient, int mode) {
+  StripJob j{};
+  j.padded = padded; j.compact = compact; j.aux = aux; j.orient = orient; j.mode = mode;
+  return j;
+}
+
+// theta level sums of a stage input into slot(ring), replacing those of the state
+// before the boundary strips were written (mode 0: rho*theta stored, 2: theta stored)
+int recompute_theta_sums(gwm_b200_ctx* c, Member& M, const float* rho, const float* th, int mode);
+
 // Reads and clears the device error words; call after the stream has drained.
 int check_device_errors(gwm_b200_ctx* c) {
   for (auto& M : c->m) {
@@ -474,6 +493,47 @@ int enqueue_theta(gwm_b200_ctx* c, Member& M) {
 
 bool rain_feeds_theta(const Member& M) { return M.md.moist && M.md.enable_warm_rain; }
 
+int recompute_theta_sums(gwm_b200_ctx* c, Member& M, const float* rho, const float* th, int mode) {
+  CK(cudaMemsetAsync(M.slot(M.ring), 0, kMaxNz * sizeof(unsigned long long), c->stream));
+  LevelSumArgs a{};
+  a.g = M.g; a.rho = rho; a.rt = th; a.mode = mode;
+  a.acc_a = M.slot(M.ring); a.acc_b = M.slot(M.ring) + kMaxNz;
+  LAUNCH(launch_level_sums(a, c->stream), "level sums");
+  return GWM_B200_OK;
+}
+
+// BoundaryUpdater::apply at a stage start (dry_core.cu:568, 591, 620) with the reference
+// boundary state: the stage input is (rho, rho*theta or theta, B + D).
+int enqueue_dry_boundary(gwm_b200_ctx* c, Member& M, int s, const float* rho, const float* th,
+                         float* const* base, float* const* inc) {
+  StripJobs J{};
+  auto push = [&](const StripJob& j) { J.j[J.n++] = j; };
+  if (s == 0) {  // keep q0 intact: save the input's strips, write the boundary's
+    StripJobs S{};
+    for (int f = 0; f < 5; ++f) S.j[S.n++] = strip_job(M.Q[f], M.bsave + M.boff[f], nullptr, kStripOrient[f], 1);
+    LAUNCH(launch_strips(M.g, S, c->stream), "boundary strips");
+    for (int f = 0; f < 5; ++f) push(strip_job(M.Q[f], M.bstrip + M.boff[f], nullptr, kStripOrient[f], 0));
+  } else {
+    push(strip_job(const_cast<float*>(rho), M.bstrip + M.boff[0], nullptr, kCell, 0));
+    push(strip_job(const_cast<float*>(th), M.bstrip + M.boff[1], M.bstrip + M.boff[0], kCell, 3));
+    for (int f = 0; f < 3; ++f) {
+      push(strip_job(base[f], M.bstrip + M.boff[2 + f], nullptr, kStripOrient[2 + f], 0));
+      if (inc) push(strip_job(inc[f], nullptr, nullptr, kStripOrient[2 + f], 4));
+    }
+  }
+  LAUNCH(launch_strips(M.g, J, c->stream), "boundary strips");
+  return recompute_theta_sums(c, M, rho, th, s == 0 ? 0 : 2);
+}
+
+// Put back the stage-1 input's own strips once the first slow stage has read them.
+int restore_stage1_strips(gwm_b200_ctx* c, Member& M, int first, int count, float* const* fields) {
+  StripJobs J{};
+  for (int f = 0; f < count; ++f)
+    J.j[J.n++] = strip_job(fields[f], M.bsave + M.boff[first + f], nullptr, kStripOrient[first + f], 0);
+  LAUNCH(launch_strips(M.g, J, c->stream), "boundary strips");
+  return GWM_B200_OK;
+}
+
 // One advance_dry_state_ssprk3 (dry_core.cu:541-651).
 int enqueue_dry(gwm_b200_ctx* c, Member& M) {
   const gwm_b200_step_config& sc = M.md.step;
@@ -514,7 +574,17 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
     a.inv_count = inv_count(M);
     a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf; a.base = M.base;
     a.err = M.err;
+    if (M.has_boundary) {
+      float* base[3] = {const_cast<float*>(a.u), const_cast<float*>(a.v), const_cast<float*>(a.w)};
+      float* inc[3] = {const_cast<float*>(a.du), const_cast<float*>(a.dv), const_cast<float*>(a.dw)};
+      const int rc = enqueue_dry_boundary(c, M, s, a.rho, a.th, base, a.du ? inc : nullptr);
+      if (rc) return rc;
+    }
     LAUNCH(launch_stage(c, M, a, terr), "slow stage");
+    if (M.has_boundary && s == 0) {
+      const int rc = restore_stage1_strips(c, M, 0, 5, M.Q);
+      if (rc) return rc;
+    }
     M.ring = (M.ring + 1) % 3;
     rcur = rnext;
     if (!fast) continue;
@@ -566,7 +636,21 @@ int enqueue_tracers(gwm_b200_ctx* c, Member& M) {
     a.ntracers = 3;
     a.idz_c = M.idc; a.terrain = M.terrain_active;
     a.err = M.err;
+    if (M.has_tracer_boundary) {  // TracerBoundaryUpdater::apply on the stage input
+      if (s == 0) {
+        StripJobs J{};
+        for (int t = 0; t < 3; ++t) J.j[J.n++] = strip_job(M.T0[t], M.bsave + M.boff[5 + t], nullptr, kCell, 1);
+        LAUNCH(launch_strips(M.g, J, c->stream), "boundary strips");
+      }
+      StripJobs A{};
+      for (int t = 0; t < 3; ++t) A.j[A.n++] = strip_job(ins[s][t], M.bstrip + M.boff[5 + t], nullptr, kCell, 0);
+      LAUNCH(launch_strips(M.g, A, c->stream), "boundary strips");
+    }
     LAUNCH(launch_tracers(c, M, a), "tracer stage");
+    if (M.has_tracer_boundary && s == 0) {
+      const int rc = restore_stage1_strips(c, M, 5, 3, M.T0);
+      if (rc) return rc;
+    }
   }
   return GWM_B200_OK;
 }
@@ -682,8 +766,10 @@ int gwm_b200_create(const gwm_b200_grid_desc* grids, const gwm_b200_member_desc*
 void gwm_b200_destroy(gwm_b200_ctx* c) {
   if (!c) return;
   drop_graph(c);
-  for (auto& M : c->m)
+  for (auto& M : c->m) {
     if (M.block) cudaFree(M.block);
+    if (M.bstrip) cudaFree(M.bstrip);
+  }
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
@@ -765,6 +851,57 @@ int gwm_b200_upload(gwm_b200_ctx* c, int member, const gwm_b200_fields* h) {
   }
   if (h->rho_d || h->rho_theta_m) M.theta_valid = false;
   if (h->rho_theta_m) M.base_valid = false;
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+int gwm_b200_set_boundary_state(gwm_b200_ctx* c, int member, const gwm_b200_fields* h) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  drop_graph(c);
+  if (!h) {
+    M.has_boundary = M.has_tracer_boundary = false;
+    return GWM_B200_OK;
+  }
+  if (!h->rho_d || !h->rho_theta_m || !h->mom_u || !h->mom_v || !h->mom_w)
+    return fail(c, GWM_B200_ERR_ARG, "boundary state needs rho_d, rho_theta_m and the three momenta");
+  const bool tracers = M.md.moist && h->qv && h->qc && h->qr;
+  if (!M.bstrip) {
+    long long off = 0;
+    for (int f = 0; f < 8; ++f) { M.boff[f] = off; off += strip_len(M.g, kStripOrient[f]); }
+    M.boff[8] = off;
+    CK(cudaMalloc(&M.bstrip, 2 * off * sizeof(float)));
+    CK(cudaMemsetAsync(M.bstrip, 0, 2 * off * sizeof(float), c->stream));
+    M.bsave = M.bstrip + off;
+  }
+  const float* src[8] = {h->rho_d, h->rho_theta_m, h->mom_u, h->mom_v, h->mom_w, h->qv, h->qc, h->qr};
+  const Geom& g = M.g;
+  for (int f = 0; f < (tracers ? 8 : 5); ++f) {
+    const int o = kStripOrient[f];
+    const size_t n = (size_t)(g.nx + (o == kFaceX)) * (g.ny + (o == kFaceY)) * (g.nz + (o == kFaceZ));
+    CK(cudaMemcpyAsync(M.staging, src[f], n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    StripJobs J{};
+    J.j[J.n++] = strip_job(nullptr, M.bstrip + M.boff[f], M.staging, o, 2);
+    CK(launch_strips(g, J, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  M.has_boundary = true;
+  M.has_tracer_boundary = tracers;
+  return GWM_B200_OK;
+}
+
+int gwm_b200_apply_reference_boundaries(gwm_b200_ctx* c, int member) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  if (!M.has_boundary) return fail(c, GWM_B200_ERR_ARG, "no boundary state set");
+  StripJobs J{};
+  for (int f = 0; f < 5; ++f) J.j[J.n++] = strip_job(M.Q[f], M.bstrip + M.boff[f], nullptr, kStripOrient[f], 0);
+  if (M.has_tracer_boundary)
+    for (int t = 0; t < 3; ++t) J.j[J.n++] = strip_job(M.T0[t], M.bstrip + M.boff[5 + t], nullptr, kCell, 0);
+  CK(launch_strips(M.g, J, c->stream));
+  M.theta_valid = false;
   CK(cudaStreamSynchronize(c->stream));
   return GWM_B200_OK;
 }

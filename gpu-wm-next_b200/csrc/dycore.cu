@@ -608,6 +608,8 @@ __global__ void __launch_bounds__(256) k_level_sums(const LevelSumArgs a) {
     const float rho = a.rho[o], rt = a.rt[o];
     if (a.mode == 0) {
       va += fx(theta_of(rho, rt), kFxTheta);
+    } else if (a.mode == 2) {  // the field holds theta: the slow stage's theta_of(rho, rho*theta)
+      va += fx(theta_of(rho, rho * rt), kFxTheta);
     } else {
       const float rtf = rho * theta_of(rho, rt);
       va += fx(rho, kFxRho);
@@ -622,7 +624,7 @@ __global__ void __launch_bounds__(256) k_level_sums(const LevelSumArgs a) {
     long long ta = 0, tb = 0;
     for (int w = 0; w < 8; ++w) { ta += s[w][0]; tb += s[w][1]; }
     acc_add(a.acc_a + k, ta);
-    if (a.mode != 0) acc_add(a.acc_b + k, tb);
+    if (a.mode == 1) acc_add(a.acc_b + k, tb);
   }
 }
 

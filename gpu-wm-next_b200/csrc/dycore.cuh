@@ -81,7 +81,8 @@ constexpr int kTmaOwnBox[2] = {32, 16};
 constexpr int kTmaYFaceBox[2] = {40, 19};
 
 // Level sums of a stored state.  mode 0: theta = rt/max(rho,1e-6) (the host loop of
-// dry_core.cu:462-476); mode 1: rho and p(rho, rho*theta) (K6 of dry_fast_modes.cu:42-57).
+// dry_core.cu:462-476); mode 1: rho and p(rho, rho*theta) (K6 of dry_fast_modes.cu:42-57);
+// mode 2: theta of a stage input stored as (rho, theta): theta_of(rho, rho*theta).
 struct LevelSumArgs {
   Geom g;
   const float *rho, *rt;

@@ -1,5 +1,6 @@
 // halo.cu — owned<->padded packing, the reference's virtual-rank halo exchange
 // as device kernels, EOS pressure and deterministic FP64 reductions.
+#include <algorithm>
 #include <cfloat>
 #include <climits>
 #include <mutex>
@@ -36,6 +37,70 @@ __global__ void k_pack(const Geom g, int o, const float* __restrict__ src, float
       v = 0.5f * (src[col] + src[col + (long long)g.ny * fx]);
     }
     store_mirrored(dst, g, o, i, j, k, v);
+  }
+}
+
+// Boundary strips.  Compact index q of a field with owned shape (fx, fy, fz):
+// west/east strips hold (j, k) at q = side*fy*fz + k*fy + j, south/north strips hold
+// (i, k) at q = 2*fy*fz + (side-2)*fx*fz + k*fx + i.
+__device__ __forceinline__ void strip_pos(const Geom& g, int o, long long q, int& side, int& i, int& j,
+                                          int& k) {
+  int fx, fy, fz;
+  owned_shape(g, o, fx, fy, fz);
+  const long long ew = (long long)fy * fz;
+  if (q < 2 * ew) {
+    side = (int)(q / ew);
+    const long long r = q - side * ew;
+    k = (int)(r / fy);
+    j = (int)(r - (long long)k * fy);
+    i = side == 0 ? 0 : fx - 1;
+  } else {
+    const long long ns = (long long)fx * fz;
+    const long long r0 = q - 2 * ew;
+    side = 2 + (int)(r0 / ns);
+    const long long r = r0 - (side - 2) * ns;
+    k = (int)(r / fx);
+    i = (int)(r - (long long)k * fx);
+    j = side == 2 ? 0 : fy - 1;
+  }
+}
+
+__global__ void k_strips(const Geom g, const StripJobs jobs) {
+  const StripJob& jb = jobs.j[blockIdx.y];
+  const int o = jb.orient;
+  int fx, fy, fz;
+  owned_shape(g, o, fx, fy, fz);
+  const long long n = 2LL * fz * (fx + fy);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    int side, i, j, k;
+    strip_pos(g, o, q, side, i, j, k);
+    const bool open = side < 2 ? !g.per_x : !g.per_y;
+    switch (jb.mode) {
+      case 0:
+        if (open) store_mirrored(jb.padded, g, o, i, j, k, jb.compact[q]);
+        break;
+      case 1:
+        jb.compact[q] = jb.padded[gidx(g, i, j, k)];
+        break;
+      case 2: {
+        const long long at = ((long long)k * fy + j) * fx + i;
+        float v = jb.aux[at];
+        if (o == kFaceX && g.per_x && (i == 0 || i == g.nx)) v = 0.5f * (jb.aux[at - i] + jb.aux[at - i + g.nx]);
+        if (o == kFaceY && g.per_y && (j == 0 || j == g.ny)) {
+          const long long col = at - (long long)j * fx;
+          v = 0.5f * (jb.aux[col] + jb.aux[col + (long long)g.ny * fx]);
+        }
+        jb.compact[q] = v;
+        break;
+      }
+      case 3:
+        if (open) store_mirrored(jb.padded, g, o, i, j, k, theta_of(jb.aux[q], jb.compact[q]));
+        break;
+      case 4:
+        if (open) store_mirrored(jb.padded, g, o, i, j, k, 0.0f);
+        break;
+    }
   }
 }
 
@@ -294,6 +359,21 @@ cudaError_t launch_pack(const Geom& g, int orient, const float* src, float* dst,
   const long long n = (long long)(g.nx + (orient == kFaceX)) * (g.ny + (orient == kFaceY)) *
                       (g.nz + (orient == kFaceZ));
   k_pack<<<blocks_for(n, 256), 256, 0, s>>>(g, orient, src, dst);
+  return cudaGetLastError();
+}
+
+long long strip_len(const Geom& g, int orient) {
+  const long long fx = g.nx + (orient == kFaceX), fy = g.ny + (orient == kFaceY), fz = g.nz + (orient == kFaceZ);
+  return 2 * fz * (fx + fy);
+}
+
+cudaError_t launch_strips(const Geom& g, const StripJobs& jobs, cudaStream_t s) {
+  if (jobs.n <= 0) return cudaSuccess;
+  if (jobs.n > kMaxStripJobs) return cudaErrorInvalidValue;
+  long long n = 0;
+  for (int t = 0; t < jobs.n; ++t) n = std::max(n, strip_len(g, jobs.j[t].orient));
+  const int bx = (int)std::min<long long>((n + 255) / 256, 1024);
+  k_strips<<<dim3(bx, jobs.n), 256, 0, s>>>(g, jobs);
   return cudaGetLastError();
 }
 

@@ -28,6 +28,28 @@ struct RankTable {
 // op 1: synchronize_owned_face_interfaces (:217-285).
 cudaError_t launch_rank_halo(const RankTable& t, int op, cudaStream_t s);
 
+// Boundary strips (apply_reference_boundaries, src/dycore/boundary_conditions.cpp:8-208):
+// the outermost owned strips of a field, over the field's own storage extents
+// (fx, fy, fz) = owned shape of its orientation, stored compactly as
+//   [west: fy*fz | east: fy*fz | south: fx*fz | north: fx*fz], k-major within a strip.
+// Job modes: 0 apply compact -> padded (open sides only, periodic mirrors written);
+// 1 save padded -> compact; 2 extract owned global array -> compact (aliased periodic
+// faces averaged, as launch_pack does); 3 apply theta = rt/max(rho, 1e-6) from two
+// compact strips (c1 = rho*theta, c2 = rho); 4 zero the padded strips (open sides).
+struct StripJob {
+  float* padded;        // modes 0, 1, 3, 4
+  float* compact;       // modes 0-3 (read for 0, 3; written for 1, 2)
+  const float* aux;     // mode 2: owned global array; mode 3: rho strips
+  int orient, mode;
+};
+constexpr int kMaxStripJobs = 8;
+struct StripJobs {
+  int n;
+  StripJob j[kMaxStripJobs];
+};
+long long strip_len(const Geom& g, int orient);  // compact floats of one field
+cudaError_t launch_strips(const Geom& g, const StripJobs& jobs, cudaStream_t s);
+
 // EOS over n values (K20 compute_pressure_kernel, dry_pressure_gradient.cu:27-35).
 cudaError_t launch_pressure(const float* rho, const float* rt, float* p, long long n, cudaStream_t s);
 

@@ -149,6 +149,18 @@ int gwm_b200_fast_modes(gwm_b200_ctx* ctx);
  * the five tendency fields are written to host arrays in the field I/O layout
  * (rho_theta_m receives the rho*theta tendency). */
 int gwm_b200_slow_tendencies(gwm_b200_ctx* ctx, int member, gwm_b200_fields* host_out);
+/* Reference boundary state of a member (host arrays in the field I/O layout; tracers
+ * optional, used when the member is moist).  While set, every step applies
+ * apply_reference_boundaries (src/dycore/boundary_conditions.cpp:111-208) on the open
+ * sides at the reference's BoundaryUpdater points: the dry stage starts
+ * (dry_core.cu:568, 591, 620) and the tracer stage inputs (dry_transport.cu:484-517),
+ * leaving the SSPRK3 blend partner q0 as it was before the first application.  The
+ * strips are kept on the device (perimeter x nz floats per field); aliased periodic
+ * faces of the boundary state are averaged as on upload.  NULL removes it (the Null
+ * updaters).  Periodic sides are never touched. */
+int gwm_b200_set_boundary_state(gwm_b200_ctx* ctx, int member, const gwm_b200_fields* boundary);
+/* apply_reference_boundaries once on the current state (dry fields and, when set, tracers). */
+int gwm_b200_apply_reference_boundaries(gwm_b200_ctx* ctx, int member);
 /* FP64 budgets of the current state. */
 int gwm_b200_budgets(gwm_b200_ctx* ctx, int member, gwm_b200_budget* out);
 /* Tile shape of a kernel.  kernel 0 = slow stage: rows 3 = owned 32x16 tiles fed by

@@ -76,6 +76,8 @@ def lib():
         L.gwo_max_threads.restype = C.c_int
         L.gwo_run.argtypes = [C.POINTER(Grid), C.POINTER(Step), C.POINTER(Rain), C.c_int, C.c_int,
                               C.c_int, C.POINTER(Fields)]
+        L.gwo_run_boundary.argtypes = [C.POINTER(Grid), C.POINTER(Step), C.POINTER(Rain), C.c_int,
+                                       C.c_int, C.c_int, C.POINTER(Fields), C.POINTER(Fields)]
         L.gwo_slow_tendencies.argtypes = [C.POINTER(Grid), C.POINTER(Step), C.c_int,
                                           C.POINTER(Fields), C.POINTER(Fields)]
         L.gwo_fast_modes.argtypes = [C.POINTER(Grid), C.POINTER(Step), C.c_int, C.POINTER(Fields)]
@@ -193,14 +195,22 @@ PHASE_DRY, PHASE_TRACERS, PHASE_RAIN, PHASE_RAIN_NOMINAL = 1, 2, 4, 8
 
 
 def run(g: GridSpec, step: StepSpec, state: dict, nsteps: int = 1, phases: int = PHASE_DRY,
-        rain: Optional[RainSpec] = None, precision: int = 64) -> dict:
-    """Advance copies of ``state`` by ``nsteps`` steps; returns the new fields."""
+        rain: Optional[RainSpec] = None, precision: int = 64, boundary: Optional[dict] = None) -> dict:
+    """Advance copies of ``state`` by ``nsteps`` steps; returns the new fields.
+    ``boundary`` (same keys as a state; tracers optional) is a reference boundary state
+    applied by apply_reference_boundaries at every stage start."""
     out = {k: np.array(v, dtype=np.float64, copy=True) for k, v in state.items() if v is not None}
     gc, sc = g.c(), step.c()
     rc = rain.c() if rain is not None else None
     f = _fields(out)
-    _check(lib().gwo_run(C.byref(gc), C.byref(sc), C.byref(rc) if rc is not None else None,
-                         phases, nsteps, precision, C.byref(f)))
+    rcp = C.byref(rc) if rc is not None else None
+    if boundary is None:
+        _check(lib().gwo_run(C.byref(gc), C.byref(sc), rcp, phases, nsteps, precision, C.byref(f)))
+    else:
+        bnd = {k: np.array(v, dtype=np.float64, copy=True) for k, v in boundary.items() if v is not None}
+        fb = _fields(bnd)
+        _check(lib().gwo_run_boundary(C.byref(gc), C.byref(sc), rcp, phases, nsteps, precision,
+                                      C.byref(f), C.byref(fb)))
     return out
 
 

@@ -866,21 +866,63 @@ template <class T> void blend_state(DryState<T>& out, const DryState<T>& a, cons
   blend_field(out.mw, a.mw, b.mw, wa, wb);
 }
 
-// advance_dry_state_ssprk3: dry_core.cu:541-651 (Null boundary updater)
+// ---------------------------------------------------------------------------
+// Reference boundaries: src/dycore/boundary_conditions.cpp:8-99 (strip copies),
+// :95-109 (touches_*), :111-161 (dry state), :163-208 (tracers).  On an open side the
+// outermost owned strip of every field (cells and faces, over the field's own storage
+// extents) is copied from the boundary state.
+inline bool touches_west(const Desc& d) { return !d.px && d.cx == 0; }
+inline bool touches_east(const Desc& d) { return !d.px && d.cx == d.rx - 1; }
+inline bool touches_south(const Desc& d) { return !d.py && d.cy == 0; }
+inline bool touches_north(const Desc& d) { return !d.py && d.cy == d.ry - 1; }
+
+template <class T> void copy_strips(Field<T>& dst, const Field<T>& src, const Desc& d) {
+  if (touches_west(d))
+    for (int k = 0; k < dst.nz; ++k)
+      for (int j = 0; j < dst.ny; ++j) dst(0, j, k) = src(0, j, k);
+  if (touches_east(d))
+    for (int k = 0; k < dst.nz; ++k)
+      for (int j = 0; j < dst.ny; ++j) dst(dst.nx - 1, j, k) = src(dst.nx - 1, j, k);
+  if (touches_south(d))
+    for (int k = 0; k < dst.nz; ++k)
+      for (int i = 0; i < dst.nx; ++i) dst(i, 0, k) = src(i, 0, k);
+  if (touches_north(d))
+    for (int k = 0; k < dst.nz; ++k)
+      for (int i = 0; i < dst.nx; ++i) dst(i, dst.ny - 1, k) = src(i, dst.ny - 1, k);
+}
+
+template <class T>
+void apply_reference_boundaries(std::vector<DryState<T>>& S, const std::vector<DryState<T>>& B,
+                                const std::vector<Desc>& L) {
+  for (size_t r = 0; r < S.size(); ++r) {
+    copy_strips(S[r].rho, B[r].rho, L[r]);
+    copy_strips(S[r].rt, B[r].rt, L[r]);
+    copy_strips(S[r].mu, B[r].mu, L[r]);
+    copy_strips(S[r].mv, B[r].mv, L[r]);
+    copy_strips(S[r].mw, B[r].mw, L[r]);
+  }
+}
+
+// advance_dry_state_ssprk3: dry_core.cu:541-651.  With a boundary state B the
+// updater applies apply_reference_boundaries at the three stage starts (:568, :591,
+// :620); the blend partner q0 is the state before the first application.
 template <class T>
 void advance_dry_ssprk3(States<T>& S, const std::vector<Desc>& L, const Metrics<T>& M,
-                        const StepCfg<T>& cfg) {
+                        const StepCfg<T>& cfg, const States<T>* B = nullptr) {
   const size_t n = S.size();
   States<T> q0 = S, q1 = S, q2 = S, tmp = S, tend;
+  if (B) apply_reference_boundaries(S, *B, L);
   compute_slow_tendencies(S, L, M, cfg, tend);
   for (size_t r = 0; r < n; ++r) update_state(q1[r], S[r], tend[r], cfg.dt);
   if (cfg.fast_modes) fast_modes(q1, L, M, cfg);
+  if (B) apply_reference_boundaries(q1, *B, L);
   compute_slow_tendencies(q1, L, M, cfg, tend);
   for (size_t r = 0; r < n; ++r) {
     update_state(tmp[r], q1[r], tend[r], cfg.dt);
     blend_state(q2[r], q0[r], tmp[r], T(0.75f), T(0.25f));
   }
   if (cfg.fast_modes) fast_modes(q2, L, M, cfg);
+  if (B) apply_reference_boundaries(q2, *B, L);
   compute_slow_tendencies(q2, L, M, cfg, tend);
   for (size_t r = 0; r < n; ++r) {
     update_state(tmp[r], q2[r], tend[r], cfg.dt);
@@ -919,10 +961,13 @@ void tracer_stage(const Field<T>& qin, const Field<T>& rho, const Field<T>& u, c
       }
 }
 
-// tracers[r][t] is tracer t of rank r (registry order).
+// tracers[r][t] is tracer t of rank r (registry order).  With boundary tracers QB the
+// tracer updater applies apply_reference_boundaries to each stage input
+// (dry_transport.cu:254-276, 484-517): a copy of the state, then q1, then q2.
 template <class T>
 void advance_tracers_ssprk3(std::vector<std::vector<Field<T>>>& Q, const States<T>& S,
-                            const std::vector<Desc>& L, const Metrics<T>& M, const StepCfg<T>& cfg) {
+                            const std::vector<Desc>& L, const Metrics<T>& M, const StepCfg<T>& cfg,
+                            const std::vector<std::vector<Field<T>>>* QB = nullptr) {
   const size_t n = S.size();
   if (n == 0 || Q.empty() || Q[0].empty()) return;
   std::vector<Field<T>> R(n), U(n), V(n), W(n);
@@ -936,13 +981,20 @@ void advance_tracers_ssprk3(std::vector<std::vector<Field<T>>>& Q, const States<
   for (size_t t = 0; t < nt; ++t) {
     std::vector<Field<T>> q0(n), q1(n), q2(n), tmp(n), st(n);
     for (size_t r = 0; r < n; ++r) { q0[r] = Q[r][t]; st[r] = Q[r][t]; q1[r] = q2[r] = tmp[r] = Q[r][t]; }
+    auto bnd = [&](std::vector<Field<T>>& F) {
+      if (QB)
+        for (size_t r = 0; r < n; ++r) copy_strips(F[r], (*QB)[r][t], L[r]);
+    };
+    bnd(st);
     exchange_scalar(st, L);
     for (size_t r = 0; r < n; ++r) tracer_stage(st[r], R[r], U[r], V[r], W[r], q1[r], L[r], M, cfg.dt);
+    bnd(q1);
     exchange_scalar(q1, L);
     for (size_t r = 0; r < n; ++r) {
       tracer_stage(q1[r], R[r], U[r], V[r], W[r], tmp[r], L[r], M, cfg.dt);
       blend_field(q2[r], q0[r], tmp[r], T(0.75f), T(0.25f));
     }
+    bnd(q2);
     exchange_scalar(q2, L);
     for (size_t r = 0; r < n; ++r) {
       tracer_stage(q2[r], R[r], U[r], V[r], W[r], tmp[r], L[r], M, cfg.dt);

@@ -162,11 +162,31 @@ template <class T> gwo::RainCfg<T> rain_from(const gwo_rain* r) {
 
 template <class T>
 int run_impl(const gwo_grid* g, const gwo_step* st, const gwo_rain* rn, int phases, int nsteps,
-             gwo_fields* io) {
+             gwo_fields* io, const gwo_fields* bnd) {
   const auto L = layout_from(g);
   const auto M = metrics_from<T>(g);
   auto S = make_states<T>(L);
   states_in(S, io, L, g);
+  // reference boundary state (apply_reference_boundaries at every stage start), or none
+  gwo::States<T> B;
+  std::vector<std::vector<gwo::Field<T>>> QB;
+  if (bnd) {
+    B = make_states<T>(L);
+    states_in(B, bnd, L, g);
+    if (bnd->qv && bnd->qc && bnd->qr) {
+      for (const auto& d : L) {
+        std::vector<gwo::Field<T>> q;
+        for (int t = 0; t < 3; ++t) q.emplace_back(d.nxl(), d.nyl(), d.nz, d.halo);
+        QB.push_back(std::move(q));
+      }
+      double* src[3] = {bnd->qv, bnd->qc, bnd->qr};
+      for (int t = 0; t < 3; ++t) {
+        std::vector<gwo::Field<T>*> f;
+        for (auto& q : QB) f.push_back(&q[t]);
+        scatter(src[t], f, L, g);
+      }
+    }
+  }
   const bool moist = (phases & 6) != 0;
   std::vector<std::vector<gwo::Field<T>>> Q;
   std::vector<std::vector<T>> P;
@@ -193,8 +213,8 @@ int run_impl(const gwo_grid* g, const gwo_step* st, const gwo_rain* rn, int phas
   gwo::RainCfg<T> rc;
   if (rn) rc = rain_from<T>(rn);
   for (int s = 0; s < nsteps; ++s) {  // gwm_prepared_case_driver.cpp:427-463
-    if (phases & 1) gwo::advance_dry_ssprk3(S, L, M, cfg);
-    if (phases & 2) gwo::advance_tracers_ssprk3(Q, S, L, M, cfg);
+    if (phases & 1) gwo::advance_dry_ssprk3(S, L, M, cfg, bnd ? &B : nullptr);
+    if (phases & 2) gwo::advance_tracers_ssprk3(Q, S, L, M, cfg, QB.empty() ? nullptr : &QB);
     if (phases & 4) gwo::apply_warm_rain(S, Q, L, &M, rc, io->precip ? &P : nullptr);
     if (phases & 8) gwo::apply_warm_rain<T>(S, Q, L, nullptr, rc, io->precip ? &P : nullptr);
   }
@@ -388,8 +408,18 @@ int gwo_max_threads(void) {
 int gwo_run(const gwo_grid* g, const gwo_step* st, const gwo_rain* rn, int phases, int nsteps,
             int precision, gwo_fields* io) {
   return guard([&] {
-    return precision == 32 ? run_impl<float>(g, st, rn, phases, nsteps, io)
-                           : run_impl<double>(g, st, rn, phases, nsteps, io);
+    return precision == 32 ? run_impl<float>(g, st, rn, phases, nsteps, io, nullptr)
+                           : run_impl<double>(g, st, rn, phases, nsteps, io, nullptr);
+  });
+}
+
+// gwo_run with a reference boundary state (global owned arrays; tracers optional)
+// applied by apply_reference_boundaries at every stage start.
+int gwo_run_boundary(const gwo_grid* g, const gwo_step* st, const gwo_rain* rn, int phases, int nsteps,
+                     int precision, gwo_fields* io, const gwo_fields* bnd) {
+  return guard([&] {
+    return precision == 32 ? run_impl<float>(g, st, rn, phases, nsteps, io, bnd)
+                           : run_impl<double>(g, st, rn, phases, nsteps, io, bnd);
   });
 }
 

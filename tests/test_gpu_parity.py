@@ -515,3 +515,84 @@ def test_tma_slow_stage_without_fast_modes(gwm, periodic):
             outs[r] = m.download()
     for k in outs[16]:
         assert np.array_equal(outs[3][k], outs[16][k]), k
+
+
+def _boundary_of(state, g, factor=1.01):
+    """A reference boundary state: the state scaled, with aliased periodic faces equal."""
+    b = {k: (np.asarray(v, np.float64) * factor).astype(np.float32) for k, v in state.items() if k != "precip"}
+    if g.periodic_x:
+        b["u"][:, :, -1] = b["u"][:, :, 0]
+    if g.periodic_y:
+        b["v"][:, -1, :] = b["v"][:, 0, :]
+    return b
+
+
+@pytest.mark.parametrize("slow_tile", [16, 3])
+def test_reference_boundaries_dry_vs_oracle(gwm, orc, slow_tile):
+    # apply_reference_boundaries at every stage start (open x, periodic y): the CUDA path
+    # against the oracle's restatement of boundary_conditions.cpp + dry_core.cu:568-620
+    g = gwm.GridSpec(40, 24, 10, dx=1000.0, dy=1000.0, z_top=10000.0, periodic_x=False, periodic_y=True)
+    s = c1_state(gwm, g, u=3.0, v=1.0)
+    s["u"][:, :, -1] = s["u"][:, :, -1]  # open x: face nx is its own
+    s["v"][:, -1, :] = s["v"][:, 0, :]
+    b = _boundary_of(s, g)
+    step = gwm.StepConfig(dt=1.0, fast_substeps=3)
+    with gwm.Model(g, gwm.MemberSpec(step=step)) as m:
+        m.set_tile("slow_stage", slow_tile)
+        m.upload(s)
+        m.set_boundary_state(b)
+        m.advance_dry_state_ssprk3(3)
+        out = m.download()
+    kw = dict(boundary={k: v.astype(np.float64) for k, v in b.items()})
+    ref = orc.run(ogrid(orc, g), ostep(orc, step), to64(s), 3, precision=64, **kw)
+    ref32 = orc.run(ogrid(orc, g), ostep(orc, step), to64(s), 3, precision=32, **kw)
+    plain = orc.run(ogrid(orc, g), ostep(orc, step), to64(s), 3, precision=64)
+    base = to64(s)
+    # the boundary must matter at all (guards against a no-op on both sides)
+    assert np.abs(ref["rho"] - plain["rho"]).max() > 1e-4
+    assert_envelope(out, ref, ref32, ("rho", "rho_theta"), floor=2e-6, factor=3.0, tag="bnd")
+    assert_envelope(out, ref, ref32, ("u", "v", "w"), base=base, floor=2e-4, factor=3.0, tag="bnd")
+
+
+def test_reference_boundaries_moist_vs_oracle(gwm, orc):
+    # moist step with dry and tracer boundary states, open on both axes
+    g = gwm.GridSpec(36, 28, 12, dx=2000.0, dy=2000.0, z_top=8000.0, periodic_x=False, periodic_y=False)
+    p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=4, relative_humidity=1.03)
+    s = gwm.build_case("moist_sounding", g, p, moist=True)
+    b = _boundary_of(s, g, factor=1.005)
+    step = gwm.StepConfig(dt=2.0, fast_substeps=4)
+    rain = gwm.WarmRainConfig(dt=2.0, rain_terminal_velocity=12.0)
+    with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=True)) as m:
+        m.upload(s)
+        m.set_boundary_state(b)
+        m.step(2)
+        out = m.download()
+    kw = dict(phases=orc.PHASE_DRY | orc.PHASE_TRACERS | orc.PHASE_RAIN,
+              rain=orc.RainSpec(dt=2.0, terminal_velocity=12.0),
+              boundary={k: v.astype(np.float64) for k, v in b.items()})
+    ref = orc.run(ogrid(orc, g), ostep(orc, step), to64(s), 2, precision=64, **kw)
+    ref32 = orc.run(ogrid(orc, g), ostep(orc, step), to64(s), 2, precision=32, **kw)
+    base = to64(s)
+    assert_envelope(out, ref, ref32, ("rho", "rho_theta"), floor=2e-6, factor=3.0, tag="bnd-moist")
+    assert_envelope(out, ref, ref32, ("u", "v", "w"), base=base, floor=2e-4, factor=3.0, tag="bnd-moist")
+    for k in ("qv", "qc", "qr"):
+        assert rel_err(out[k], ref[k], floor=1e-9) < 1e-3, k
+
+
+def test_apply_reference_boundaries_strips(gwm):
+    # the stand-alone operator copies exactly the outermost owned strips of open sides
+    g = gwm.GridSpec(20, 14, 6, dx=1000.0, dy=1000.0, z_top=6000.0, periodic_x=False, periodic_y=True)
+    s = c1_state(gwm, g, u=2.0)
+    s["v"][:, -1, :] = s["v"][:, 0, :]
+    b = _boundary_of(s, g, factor=1.5)
+    with gwm.Model(g, gwm.MemberSpec()) as m:
+        m.upload(s)
+        before = m.download()
+        m.set_boundary_state(b)
+        m.apply_reference_boundaries()
+        out = m.download()
+    for k in ("rho", "rho_theta", "u", "v", "w"):
+        exp = before[k].copy()
+        exp[:, :, 0] = b[k][:, :, 0]      # west strip (open x); periodic y untouched
+        exp[:, :, -1] = b[k][:, :, -1]    # east strip
+        assert np.array_equal(out[k], exp), k

@@ -1,0 +1,74 @@
+"""The N>1 path of bench.py on CPU: two gloo ranks (127.0.0.1), no GPU.
+
+Each rank advances an independent replica (no data-path collective), so the only
+cross-rank steps are the timing reduction (max over ranks) and the whole-job
+throughput; the reference arm runs on rank 0 alone.  These tests run those host
+pieces under a real two-process torch.distributed group.
+"""
+import os
+import socket
+import sys
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, q):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        local_ms = 10.0 + 5.0 * rank            # rank 1 is the slow one
+        ms_max = bench.max_over_ranks(local_ms, torch, dist, "cpu")
+        value = bench.job_throughput(1000, 4, world, ms_max)
+        # the reference arm: rank 0 alone works, the other ranks return at once
+        class A:
+            steps, warmup = 1, 0
+        if rank != 0:
+            bench.run_reference(A(), rank, world)
+        dist.barrier()
+        q.put((rank, ms_max, value))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_timing_reduction():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+        assert p.exitcode == 0, f"rank exited with {p.exitcode}"
+    got = sorted(q.get(timeout=5) for _ in range(2))
+    for rank, ms_max, value in got:
+        assert ms_max == pytest.approx(15.0), rank           # max over ranks, on every rank
+        assert value == pytest.approx(1000 * 4 * 2 / 15e-3)  # whole job: both replicas
+
+
+def test_single_rank_helpers_without_group():
+    import torch
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.max_over_ranks(7.5, torch, None, "cpu") == 7.5
+    assert bench.job_throughput(10, 3, 1, 2.0) == pytest.approx(10 * 3 / 2e-3)
