@@ -227,6 +227,7 @@ def main():
     model.set_stream(stream.cuda_stream)
     model.upload(state)
     tiles = None
+    tile_ms = None
     if args.fast_tile is not None:
         args.no_tune = True
         model.set_tile("fast_substep", args.fast_tile)
@@ -237,6 +238,7 @@ def main():
         # pick each stencil kernel's tile by timing it, then restart from the initial state
         with torch.cuda.stream(stream):
             tiles = model.autotune(1)
+        tile_ms = {k: {str(r): round(t, 4) for r, t in v.items()} for k, v in model.tile_times.items()}
         model.upload(state)
     else:
         tiles = {k: model.get_tile(k) for k in ("slow_stage", "fast_substep", "tracer_stage")}
@@ -293,7 +295,7 @@ def main():
                        "dt_s": DT, "fast_substeps": NS, "rain_terminal_velocity": VT,
                        "phases": "dry SSPRK3 + 3-tracer SSPRK3 + warm rain/fallout",
                        "l2": "inputs larger than L2 (each field 282 MB)",
-                       "graph": not args.no_graph, "tile_rows": tiles,
+                       "graph": not args.no_graph, "tile_rows": tiles, "tile_autotune_ms": tile_ms,
                        "parallelism": f"replicas{world}"},
             "gpu_launches": launches,
             "state_finite": finite,
@@ -326,16 +328,27 @@ def substep_roofline(model, g, stream, torch, steps=2):
     achieved = SUBSTEP_ALGO_BYTES_PER_CELL * cells / (fast["avg_ms"] * 1e-3) / 1e9
     total = sum(v["total_ms"] for v in rep.values())
     shares = {k: round(v["total_ms"] / total, 4) for k, v in rep.items()}
-    return {"bound": "hbm", "achieved": achieved, "unit": "GB/s", "traffic": read_traffic(g),
-            "kernel": "k_fast_substep (one acoustic substep)",
+    fast_tile = model.get_tile("fast_substep")
+    kname = {0: "k_fast_flat", 3: "k_fast_tma"}.get(fast_tile, f"k_fast_substep<{fast_tile}>")
+    return {"bound": "hbm", "achieved": achieved, "unit": "GB/s", "traffic": read_traffic(g, fast_tile),
+            "kernel": f"{kname} (one acoustic substep)",
             "algorithmic_bytes_per_launch": SUBSTEP_ALGO_BYTES_PER_CELL * cells,
             "avg_launch_ms": fast["avg_ms"], "kernel_shares": shares,
             "kernel_avg_ms": {k: round(v["avg_ms"], 4) for k, v in rep.items()}}
 
 
-def read_traffic(g):
-    """DRAM bytes per substep launch from the committed ncu summary, scaled by cells."""
-    p = os.path.join(ROOT, "profiles", "k_fast_substep_dram.txt")
+# committed ncu summaries of the acoustic-substep kernels (DRAM bytes per cell of one launch)
+TRAFFIC_PROFILES = {0: "k_fast_flat_768x768x64.txt", 3: "k_fast_tma_768x768x64.txt"}
+
+
+def read_traffic(g, fast_tile):
+    """DRAM bytes per substep launch from the committed ncu summary of the substep kernel
+    in use, captured on a 768 x 768 x 64 case and scaled by cells (traffic per cell does
+    not depend on the horizontal size: inputs exceed L2 in both)."""
+    name = TRAFFIC_PROFILES.get(fast_tile)
+    if name is None:
+        return None
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     vals = {}

@@ -476,8 +476,10 @@ class Model:
         kinds = {"slow_stage": "k_slow_stage", "fast_substep": "k_fast_substep",
                  "tracer_stage": "k_tracer_stage"}
         best = {k: self.get_tile(k) for k in candidates}
+        self.tile_times = {}
         for kernel, rows_list in candidates.items():
             times = {}
+            self.tile_times[kernel] = times
             for rows in rows_list:
                 self.set_tile(kernel, rows)
                 self.profile(True)

@@ -533,7 +533,6 @@ def test_reference_boundaries_dry_vs_oracle(gwm, orc, slow_tile):
     # against the oracle's restatement of boundary_conditions.cpp + dry_core.cu:568-620
     g = gwm.GridSpec(40, 24, 10, dx=1000.0, dy=1000.0, z_top=10000.0, periodic_x=False, periodic_y=True)
     s = c1_state(gwm, g, u=3.0, v=1.0)
-    s["u"][:, :, -1] = s["u"][:, :, -1]  # open x: face nx is its own
     s["v"][:, -1, :] = s["v"][:, 0, :]
     b = _boundary_of(s, g)
     step = gwm.StepConfig(dt=1.0, fast_substeps=3)
