@@ -202,6 +202,8 @@ def main():
                     help="acoustic-substep kernel (0 owned tile, 3 TMA-fed, 8/16 overlapped); implies --no-tune")
     ap.add_argument("--slow-tile", type=int, default=None,
                     help="slow-stage kernel (3 TMA-fed owned tile, 8/16 overlapped); implies --no-tune")
+    ap.add_argument("--tracer-tile", type=int, default=None,
+                    help="tracer-stage kernel (3 TMA-fed owned tile, 8/16 overlapped); implies --no-tune")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -234,6 +236,9 @@ def main():
     if args.slow_tile is not None:
         args.no_tune = True
         model.set_tile("slow_stage", args.slow_tile)
+    if args.tracer_tile is not None:
+        args.no_tune = True
+        model.set_tile("tracer_stage", args.tracer_tile)
     if not args.no_tune:
         # pick each stencil kernel's tile by timing it, then restart from the initial state
         with torch.cuda.stream(stream):

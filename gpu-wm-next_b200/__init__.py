@@ -119,7 +119,8 @@ class _CaseParams(C.Structure):
         "center_x_fraction", "center_y_fraction", "center_z_fraction", "radius_x_fraction",
         "radius_y_fraction", "radius_z_fraction", "theta_perturbation", "rho_surface",
         "theta_ref", "p_surface", "theta_lapse_k_per_m", "relative_humidity", "rh_top_m",
-        "qv_scale_height_m", "qv_floor", "noise_rms_k", "noise_depth_m")] + [("seed", C.c_uint64)]
+        "qv_scale_height_m", "qv_floor", "noise_rms_k", "noise_depth_m", "brunt_vaisala")] + [
+        ("seed", C.c_uint64)]
 
 
 class _TerrainParams(C.Structure):
@@ -162,6 +163,8 @@ def lib():
     L.gwm_b200_set_tile.argtypes = [vp, C.c_int, C.c_int]
     L.gwm_b200_set_boundary_state.argtypes = [vp, C.c_int, C.POINTER(_Fields)]
     L.gwm_b200_apply_reference_boundaries.argtypes = [vp, C.c_int]
+    L.gwm_b200_set_damping.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double)]
     L.gwm_b200_get_tile.argtypes = [vp, C.c_int]
     L.gwm_b200_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double),
                                         C.POINTER(C.c_longlong), C.POINTER(C.c_char_p)]
@@ -190,7 +193,7 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_step", "gwm_b200_advance_dry", "gwm_b200_advance_tracers",
             "gwm_b200_warm_rain", "gwm_b200_fast_modes", "gwm_b200_slow_tendencies",
             "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_get_tile", "gwm_b200_set_boundary_state",
-            "gwm_b200_apply_reference_boundaries", "gwm_b200_layout",
+            "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_layout",
             "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_ranks_to_global",
             "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
 
@@ -375,6 +378,22 @@ class Model:
                 keep.append(a)
                 setattr(f, cname, _fptr(a))
         self._check(lib().gwm_b200_set_boundary_state(self._h, member, C.byref(f)), "set_boundary_state")
+
+    def set_damping(self, z_bottom: float, rate: float, u_ref=None, v_ref=None, member: int = 0):
+        """Rayleigh damping layer above ``z_bottom`` (extension); rate <= 0 removes it."""
+        nz = self.grids[member].nz
+        ptrs = []
+        for ref in (u_ref, v_ref):
+            if ref is None:
+                ptrs.append(None)
+            else:
+                a = np.ascontiguousarray(ref, dtype=np.float64)
+                if a.shape != (nz,):
+                    raise ValueError(f"reference profile shape {a.shape} != ({nz},)")
+                ptrs.append(a)
+        args = [p.ctypes.data_as(C.POINTER(C.c_double)) if p is not None else None for p in ptrs]
+        self._check(lib().gwm_b200_set_damping(self._h, member, float(z_bottom), float(rate), *args),
+                    "set_damping")
 
     def apply_reference_boundaries(self, member: int = 0):
         """apply_reference_boundaries once on the current state."""
@@ -604,6 +623,7 @@ class CaseParams:
     qv_floor: float = 1.0e-5
     noise_rms_k: float = 0.0
     noise_depth_m: float = 1000.0
+    brunt_vaisala: float = 0.01
     seed: int = 0
 
     def c(self) -> _CaseParams:

@@ -72,6 +72,9 @@ struct Member {
   float* bsave = nullptr;
   long long boff[9]{};
   bool has_boundary = false, has_tracer_boundary = false;
+  // Rayleigh damping layer (extension): [tau_c(nz) | tau_f(nz+1) | u_ref(nz) | v_ref(nz)]
+  float* damp = nullptr;
+  bool damping = false;
   // TMA descriptors of the substep's buffers: (buffer, box kind 0 cell / 1 face / 2 own, map)
   std::vector<std::tuple<const float*, int, CUtensorMap>> tmaps;
   const CUtensorMap* tmap(const float* buf, int kind) const {
@@ -287,7 +290,8 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   const size_t extra = ((2 * plane2 * sizeof(double) + 255) / 256) * 256 +
                        3 * kSlot * sizeof(unsigned long long) + owned_max * sizeof(float) +
                        3 * kReduceBlocks * sizeof(double) + 32 * sizeof(ReduceOut) + 4096 +
-                       3 * 4 * (kMaxNz + 1) * sizeof(float) + 3 * kMaxNz * sizeof(double) + 512;
+                       3 * 4 * (kMaxNz + 1) * sizeof(float) + 3 * kMaxNz * sizeof(double) + 512 +
+                       4 * (kMaxNz + 1) * sizeof(float) + 256;
   const size_t total = nfields * fbytes + extra;
   CK(cudaMalloc(&M.block, total));
   CK(cudaMemsetAsync(M.block, 0, total, c->stream));
@@ -311,6 +315,7 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   M.red_part = (double*)take(3 * kReduceBlocks * sizeof(double));
   M.red_out = (ReduceOut*)take(32 * sizeof(ReduceOut));
   M.err = (int*)take(sizeof(int));
+  M.damp = (float*)take(4 * (kMaxNz + 1) * sizeof(float));
   // metrics
   const HostMetrics H = build_metrics(M);
   if (M.terrain_active) {
@@ -574,6 +579,10 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
     a.inv_count = inv_count(M);
     a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf; a.base = M.base;
     a.err = M.err;
+    if (M.damping) {
+      a.damp_c = M.damp; a.damp_f = M.damp + (kMaxNz + 1);
+      a.uref = M.damp + 2 * (kMaxNz + 1); a.vref = M.damp + 3 * (kMaxNz + 1);
+    }
     if (M.has_boundary) {
       float* base[3] = {const_cast<float*>(a.u), const_cast<float*>(a.v), const_cast<float*>(a.w)};
       float* inc[3] = {const_cast<float*>(a.du), const_cast<float*>(a.dv), const_cast<float*>(a.dw)};
@@ -891,6 +900,39 @@ int gwm_b200_set_boundary_state(gwm_b200_ctx* c, int member, const gwm_b200_fiel
   return GWM_B200_OK;
 }
 
+// Rayleigh damping rate tau(z) = rate * sin^2(pi/2 (z - z_d)/(z_top - z_d)) above z_d at a
+// level's terrain-free height eta * z_top (an extension: the reference has no damping layer).
+static double rayleigh_rate(double z, double z_d, double z_top, double rate) {
+  if (rate <= 0.0 || z <= z_d || z_top <= z_d) return 0.0;
+  const double s = std::sin(0.5 * 3.14159265358979323846 * std::min(1.0, (z - z_d) / (z_top - z_d)));
+  return rate * s * s;
+}
+
+int gwm_b200_set_damping(gwm_b200_ctx* c, int member, double z_bottom, double rate, const double* u_ref,
+                         const double* v_ref) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  drop_graph(c);
+  if (rate <= 0.0) { M.damping = false; return GWM_B200_OK; }
+  const int nz = M.g.nz;
+  const double zt = M.gd.z_top;
+  std::vector<float> h(4 * (kMaxNz + 1), 0.0f);
+  for (int k = 0; k < nz; ++k) {
+    const double ec = M.eta.empty() ? ((double)k + 0.5) / nz : 0.5 * (M.eta[k] + M.eta[k + 1]);
+    h[k] = (float)rayleigh_rate(ec * zt, z_bottom, zt, rate);
+    h[2 * (kMaxNz + 1) + k] = u_ref ? (float)u_ref[k] : 0.0f;
+    h[3 * (kMaxNz + 1) + k] = v_ref ? (float)v_ref[k] : 0.0f;
+  }
+  for (int k = 0; k <= nz; ++k) {
+    const double ei = M.eta.empty() ? (double)k / nz : M.eta[k];
+    h[(kMaxNz + 1) + k] = (float)rayleigh_rate(ei * zt, z_bottom, zt, rate);
+  }
+  CK(cudaMemcpy(M.damp, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+  M.damping = true;
+  return GWM_B200_OK;
+}
+
 int gwm_b200_apply_reference_boundaries(gwm_b200_ctx* c, int member) {
   int rc = check_member(c, member);
   if (rc) return rc;
@@ -1135,6 +1177,10 @@ int gwm_b200_slow_tendencies(gwm_b200_ctx* c, int member, gwm_b200_fields* h) {
   a.acc_mode = 0;
   a.inv_count = inv_count(M);
   a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf; a.base = M.base;
+  if (M.damping) {
+    a.damp_c = M.damp; a.damp_f = M.damp + (kMaxNz + 1);
+    a.uref = M.damp + 2 * (kMaxNz + 1); a.vref = M.damp + 3 * (kMaxNz + 1);
+  }
   CK(launch_slow(a, M.terrain_active, c->stream, c->slow_tile_rows == kSlowTma ? 16 : c->slow_tile_rows));
   gwm_b200_fields tmp{};
   tmp.rho_d = h->rho_d; tmp.rho_theta_m = h->rho_theta_m;

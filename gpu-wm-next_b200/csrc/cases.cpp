@@ -194,6 +194,43 @@ int gwm_b200_build_case(const char* kind_c, const gwm_b200_grid_desc* g, const g
           }
     return GWM_B200_OK;
   }
+  if (kind == "stratified_mountain_wave") {
+    // constant N: theta(z) = theta0 exp(N^2 z / g); hydrostatic Exner function
+    // pi(z) = pi_s - g^2 / (cp theta0 N^2) (1 - exp(-N^2 z / g)), p = p0 pi^(1/kappa)
+    const double n2 = (double)c->brunt_vaisala * (double)c->brunt_vaisala;
+    if (n2 <= 0.0) return GWM_B200_ERR_ARG;
+    const double th0 = c->theta_ref, gg = kG, cpd = (double)cp();
+    const double pis = std::pow((double)c->p_surface / kP0, (double)kKappa);
+    fill(out->mom_w, nw, 0.0f);
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          const double z = z_center(*g, i, j, k);
+          const double th = th0 * std::exp(n2 * z / gg);
+          const double pi = std::max(1.0e-4, pis - gg * gg / (cpd * th0 * n2) * (1.0 - std::exp(-n2 * z / gg)));
+          const float p = (float)(kP0 * std::pow(pi, 1.0 / kKappa));
+          const float r = eos_rho(p, (float)th);
+          rho[cidx(*g, i, j, k)] = r;
+          rt[cidx(*g, i, j, k)] = r * (float)th;
+        }
+    auto R = [&](int i, int j, int k) { return rho[cidx(*g, i, j, k)]; };
+    const float ub = c->u_background, vb = c->v_background;
+    if (out->mom_u)  // face-averaged density times the background wind (idealized_cases.cpp:36-103)
+      for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+          for (int i = 0; i <= nx; ++i) {
+            const float fd = (nx == 1 || i <= 0) ? R(0, j, k) : (i >= nx ? R(nx - 1, j, k) : 0.5f * (R(i - 1, j, k) + R(i, j, k)));
+            out->mom_u[((size_t)k * ny + j) * (nx + 1) + i] = fd * ub;
+          }
+    if (out->mom_v)
+      for (int k = 0; k < nz; ++k)
+        for (int j = 0; j <= ny; ++j)
+          for (int i = 0; i < nx; ++i) {
+            const float fd = (ny == 1 || j <= 0) ? R(i, 0, k) : (j >= ny ? R(i, ny - 1, k) : 0.5f * (R(i, j - 1, k) + R(i, j, k)));
+            out->mom_v[((size_t)k * (ny + 1) + j) * nx + i] = fd * vb;
+          }
+    return GWM_B200_OK;
+  }
   if (kind == "moist_sounding") {
     fill(out->mom_u, nu, 0.0f); fill(out->mom_v, nv, 0.0f); fill(out->mom_w, nw, 0.0f);
     const float th0 = c->theta_ref;

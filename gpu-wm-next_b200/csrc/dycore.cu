@@ -236,6 +236,7 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
           } else {
             t_u += -((pr - pl) * idx);
           }
+          if (a.damp_c) t_u += -__ldg(a.damp_c + k) * (qc - __ldg(a.uref + k));
         }
         if (a.tend_only) {
           a.o_u[o] = t_u;
@@ -271,6 +272,7 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
           } else {
             t_v += -((pn - ps) * idy);
           }
+          if (a.damp_c) t_v += -__ldg(a.damp_c + k) * (qc - __ldg(a.vref + k));
         }
         if (a.tend_only) {
           a.o_v[o] = t_v;
@@ -302,6 +304,7 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
           const float rf = 0.5f * (cm.rho + cc.rho);
           const float b = a.gravity * (tf - trf) / fmaxf(trf, 1.0e-6f);
           t_w += rf * b;
+          if (a.damp_c) t_w += -__ldg(a.damp_f + k) * qc;
         }
         if (a.tend_only) {
           a.o_w[o] = t_w;

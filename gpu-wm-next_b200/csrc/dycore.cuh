@@ -35,6 +35,9 @@ struct SlowArgs {
   const float *zc, *idz_c, *idz_f;  // metrics: padded 3-D (terrain) or per level (flat)
   const double* base;               // FP64 base state [rt_ref | 1/rt_ref | p_ref] per level
   int* err;                         // error word: set to 1 when a bounded wait gave up
+  // Rayleigh damping layer (extension; null: off): per-level rates at cell centres and
+  // Z faces, and the momentum profiles u, v relax to
+  const float *damp_c, *damp_f, *uref, *vref;
 };
 
 // TMA descriptors of one slow stage (flat terrain, k_slow_tma): 3-D tiled maps over the

@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         if (!top) flt = upwind(0.5f * (wc[d - 1] + wc[d]), qc, qt);
         t_u = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
         t_u += -((pc - pp[d - 1]) * idx);
+        if (a.damp_c) t_u += -__ldg(a.damp_c + k) * (qc - __ldg(a.uref + k));
       }
       float u1 = fmaxf(-1.0e30f, uf + dt * t_u);
       if (blend) u1 = a.wa * q0.u + a.wb * u1;
@@ -260,6 +261,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         if (!top) flt = upwind(0.5f * (wc[d - DW] + wc[d]), qc, qt);
         t_v = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
         t_v += -((pc - pp[d - DW]) * idy);
+        if (a.damp_c) t_v += -__ldg(a.damp_c + k) * (qc - __ldg(a.vref + k));
       }
       float v1 = fmaxf(-1.0e30f, vf + dt * t_v);
       if (blend) v1 = a.wa * q0.v + a.wb * v1;
@@ -286,6 +288,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         const float rf = 0.5f * (cy.rho + rho);
         const float bu = a.gravity * (tf - trf) / fmaxf(trf, 1.0e-6f);
         t_w += rf * bu;
+        if (a.damp_c) t_w += -__ldg(a.damp_f + k) * qc;
       }
       float w1 = fmaxf(-1.0e30f, wf + dt * t_w);
       if (blend) w1 = a.wa * q0.w + a.wb * w1;

@@ -159,6 +159,13 @@ int gwm_b200_slow_tendencies(gwm_b200_ctx* ctx, int member, gwm_b200_fields* hos
  * faces of the boundary state are averaged as on upload.  NULL removes it (the Null
  * updaters).  Periodic sides are never touched. */
 int gwm_b200_set_boundary_state(gwm_b200_ctx* ctx, int member, const gwm_b200_fields* boundary);
+/* Rayleigh damping layer (an extension: the reference has none).  Above z_bottom the
+ * slow tendencies gain -tau(z) (u - u_ref(k)), -tau(z) (v - v_ref(k)) and -tau(z) w,
+ * with tau(z) = rate * sin^2(pi/2 (z - z_bottom)/(z_top - z_bottom)) at each level's
+ * terrain-free height eta * z_top, on the faces whose tendency the reference computes.
+ * u_ref, v_ref: nz momenta per level (NULL: 0).  rate <= 0 removes the layer. */
+int gwm_b200_set_damping(gwm_b200_ctx* ctx, int member, double z_bottom, double rate,
+                         const double* u_ref, const double* v_ref);
 /* apply_reference_boundaries once on the current state (dry fields and, when set, tracers). */
 int gwm_b200_apply_reference_boundaries(gwm_b200_ctx* ctx, int member);
 /* FP64 budgets of the current state. */

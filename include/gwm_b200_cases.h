@@ -30,6 +30,8 @@ typedef struct {
   float qv_floor;
   float noise_rms_k;          /* Gaussian theta noise below noise_depth_m */
   float noise_depth_m;
+  /* stratified_mountain_wave: Brunt-Vaisala frequency N (1/s) of the background */
+  float brunt_vaisala;
   uint64_t seed;
 } gwm_b200_case_params;
 
@@ -40,7 +42,10 @@ typedef struct {
 } gwm_b200_terrain_params;
 
 /* kind: "constant", "warm_bubble", "density_current", "hydrostatic_rest",
- * "mountain_wave_background", "hydrostatic_warm_bubble", "moist_sounding".
+ * "mountain_wave_background", "hydrostatic_warm_bubble", "moist_sounding",
+ * "stratified_mountain_wave" (an extension: constant-N background
+ * theta = theta_ref exp(N^2 z / g) in hydrostatic balance from p_surface, with the
+ * mountain-wave face momenta of u_background, v_background).
  * Fills host arrays in the field I/O layout of gwm_b200.h (NULL members skipped;
  * rho_d and rho_theta_m required). */
 int gwm_b200_build_case(const char* kind, const gwm_b200_grid_desc* grid,

@@ -37,7 +37,9 @@ class Grid(C.Structure):
 
 class Step(C.Structure):
     _fields_ = [("dt", C.c_double), ("fast_substeps", C.c_int), ("gravity", C.c_double),
-                ("fast_hmom", C.c_int), ("fast_density", C.c_int), ("fast_modes", C.c_int)]
+                ("fast_hmom", C.c_int), ("fast_density", C.c_int), ("fast_modes", C.c_int),
+                ("damp_z_bottom", C.c_double), ("damp_rate", C.c_double),
+                ("damp_u_ref", C.POINTER(C.c_double)), ("damp_v_ref", C.POINTER(C.c_double))]
 
 
 class Rain(C.Structure):
@@ -141,10 +143,22 @@ class StepSpec:
     fast_hmom: bool = True
     fast_density: bool = True
     fast_modes: bool = True
+    damp_z_bottom: float = 0.0        # Rayleigh damping layer (extension): bottom height (m)
+    damp_rate: float = 0.0            # maximum rate (1/s); <= 0: off
+    damp_u_ref: Optional[np.ndarray] = None  # (nz,) momentum profiles the layer relaxes to
+    damp_v_ref: Optional[np.ndarray] = None
 
     def c(self) -> Step:
-        return Step(self.dt, self.fast_substeps, self.gravity, int(self.fast_hmom),
-                    int(self.fast_density), int(self.fast_modes))
+        st = Step(self.dt, self.fast_substeps, self.gravity, int(self.fast_hmom),
+                  int(self.fast_density), int(self.fast_modes), self.damp_z_bottom, self.damp_rate,
+                  None, None)
+        if self.damp_u_ref is not None:
+            self._u = np.ascontiguousarray(self.damp_u_ref, dtype=np.float64)
+            st.damp_u_ref = _ptr(self._u)
+        if self.damp_v_ref is not None:
+            self._v = np.ascontiguousarray(self.damp_v_ref, dtype=np.float64)
+            st.damp_v_ref = _ptr(self._v)
+        return st
 
 
 @dataclass

@@ -449,7 +449,18 @@ template <class T> struct StepCfg {
   bool fast_hmom = true;
   bool fast_density = true;
   bool fast_modes = true;
+  // Rayleigh damping layer (extension; not in the reference): per-level rates at cell
+  // centres and Z faces, and the per-level momentum profiles u, v relax to (empty: off)
+  std::vector<T> damp_c, damp_f, u_ref, v_ref;
 };
+
+// Rayleigh damping rate tau(z) = rate * sin^2(pi/2 (z - z_d)/(z_top - z_d)) above z_d,
+// evaluated at a level's terrain-free height eta * z_top.
+inline double rayleigh_rate(double z, double z_d, double z_top, double rate) {
+  if (rate <= 0.0 || z <= z_d || z_top <= z_d) return 0.0;
+  const double s = std::sin(0.5 * 3.14159265358979323846 * std::min(1.0, (z - z_d) / (z_top - z_d)));
+  return rate * s * s;
+}
 
 template <class T> using States = std::vector<DryState<T>>;
 
@@ -659,6 +670,28 @@ void compute_slow_tendencies(const States<T>& S, const std::vector<Desc>& L,
           const T b = cfg.gravity * (tf - trf) / std::max(trf, T(1.0e-6f));
           o.mw(i, j, kf) += rf * b;
         }
+    // Rayleigh damping layer (extension): relaxation of the momenta on the faces whose
+    // tendency the reference computes (open-boundary faces and Z faces 0, nz excluded)
+    if (!cfg.damp_c.empty()) {
+      const Field<T>& u = S[r].mu;
+      const Field<T>& v = S[r].mv;
+      const Field<T>& w = S[r].mw;
+      for (int k = 0; k < nz; ++k) {
+        for (int j = 0; j < ny; ++j)
+          for (int i = 0; i <= nx; ++i) {
+            if ((i == 0 && ow) || (i == nx && oe)) continue;
+            o.mu(i, j, k) += -cfg.damp_c[k] * (u(i, j, k) - cfg.u_ref[k]);
+          }
+        for (int j = 0; j <= ny; ++j)
+          for (int i = 0; i < nx; ++i) {
+            if ((j == 0 && os) || (j == ny && on)) continue;
+            o.mv(i, j, k) += -cfg.damp_c[k] * (v(i, j, k) - cfg.v_ref[k]);
+          }
+      }
+      for (int kf = 1; kf < nz; ++kf)
+        for (int j = 0; j < ny; ++j)
+          for (int i = 0; i < nx; ++i) o.mw(i, j, kf) += -cfg.damp_f[kf] * w(i, j, kf);
+    }
   }
 }
 

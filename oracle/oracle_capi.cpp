@@ -32,6 +32,9 @@ typedef struct {
   int fast_substeps;
   double gravity;
   int fast_hmom, fast_density, fast_modes;
+  // Rayleigh damping layer (extension): rate <= 0 disables; u_ref/v_ref: nz values or NULL
+  double damp_z_bottom, damp_rate;
+  const double *damp_u_ref, *damp_v_ref;
 } gwo_step;
 
 typedef struct {
@@ -136,7 +139,7 @@ void states_out(gwo::States<T>& S, gwo_fields* io, const std::vector<gwo::Desc>&
   gather(io->u, c, L, g); gather(io->v, d, L, g); gather(io->w, e, L, g);
 }
 
-template <class T> gwo::StepCfg<T> step_from(const gwo_step* s) {
+template <class T> gwo::StepCfg<T> step_from(const gwo_step* s, const gwo::Metrics<T>* M = nullptr) {
   gwo::StepCfg<T> c;
   c.dt = (T)(float)s->dt;
   c.fast_substeps = s->fast_substeps;
@@ -144,6 +147,21 @@ template <class T> gwo::StepCfg<T> step_from(const gwo_step* s) {
   c.fast_hmom = s->fast_hmom != 0;
   c.fast_density = s->fast_density != 0;
   c.fast_modes = s->fast_modes != 0;
+  if (M && s->damp_rate > 0.0) {
+    const int nz = M->nz;
+    c.damp_c.resize(nz);
+    c.damp_f.resize(nz + 1);
+    c.u_ref.assign(nz, T(0));
+    c.v_ref.assign(nz, T(0));
+    for (int k = 0; k < nz; ++k)
+      c.damp_c[k] = (T)(float)gwo::rayleigh_rate(M->eta_c[k] * M->z_top, s->damp_z_bottom, M->z_top, s->damp_rate);
+    for (int k = 0; k <= nz; ++k)
+      c.damp_f[k] = (T)(float)gwo::rayleigh_rate(M->eta_i[k] * M->z_top, s->damp_z_bottom, M->z_top, s->damp_rate);
+    for (int k = 0; k < nz; ++k) {
+      if (s->damp_u_ref) c.u_ref[k] = (T)(float)s->damp_u_ref[k];
+      if (s->damp_v_ref) c.v_ref[k] = (T)(float)s->damp_v_ref[k];
+    }
+  }
   return c;
 }
 
@@ -209,7 +227,7 @@ int run_impl(const gwo_grid* g, const gwo_step* st, const gwo_rain* rn, int phas
           for (int i = 0; i < L[r].nxl(); ++i)
             P[r][(size_t)j * L[r].nxl() + i] = (T)io->precip[(size_t)(L[r].j0 + j) * g->nx + L[r].i0 + i];
   }
-  const auto cfg = step_from<T>(st);
+  const auto cfg = step_from<T>(st, &M);
   gwo::RainCfg<T> rc;
   if (rn) rc = rain_from<T>(rn);
   for (int s = 0; s < nsteps; ++s) {  // gwm_prepared_case_driver.cpp:427-463
@@ -242,7 +260,7 @@ int slow_impl(const gwo_grid* g, const gwo_step* st, const gwo_fields* in, gwo_f
   auto S = make_states<T>(L);
   states_in(S, in, L, g);
   gwo::States<T> tend;
-  gwo::compute_slow_tendencies(S, L, M, step_from<T>(st), tend);
+  gwo::compute_slow_tendencies(S, L, M, step_from<T>(st, &M), tend);
   states_out(tend, out, L, g);
   return 0;
 }
@@ -253,7 +271,7 @@ int fast_impl(const gwo_grid* g, const gwo_step* st, gwo_fields* io) {
   const auto M = metrics_from<T>(g);
   auto S = make_states<T>(L);
   states_in(S, io, L, g);
-  gwo::fast_modes(S, L, M, step_from<T>(st));
+  gwo::fast_modes(S, L, M, step_from<T>(st, &M));
   states_out(S, io, L, g);
   return 0;
 }

@@ -595,3 +595,60 @@ def test_apply_reference_boundaries_strips(gwm):
         exp[:, :, 0] = b[k][:, :, 0]      # west strip (open x); periodic y untouched
         exp[:, :, -1] = b[k][:, :, -1]    # east strip
         assert np.array_equal(out[k], exp), k
+
+
+def _c2_case(gwm, nx=40, ny=28, nz=20, periodic=True):
+    """C2-style case on a small grid: Agnesi hill, stretched hybrid-height levels, constant-N
+    stratified background with a 10 m/s wind (extensions of the reference's cases)."""
+    a = 1.2
+    eta = (np.exp(a * np.arange(nz + 1) / nz) - 1.0) / (np.exp(a) - 1.0)
+    terrain = gwm.build_terrain("agnesi", nx, ny, 1000.0, 1000.0, height=400.0, half_width_x=6000.0,
+                                half_width_y=6000.0)
+    g = gwm.GridSpec(nx, ny, nz, dx=1000.0, dy=1000.0, z_top=20000.0, terrain=terrain,
+                     eta_interfaces=eta, periodic_x=periodic, periodic_y=periodic)
+    p = gwm.CaseParams(theta_ref=288.0, p_surface=100000.0, u_background=10.0, brunt_vaisala=0.01)
+    s = gwm.build_case("stratified_mountain_wave", g, p)
+    if periodic:
+        s["u"][:, :, -1] = s["u"][:, :, 0]
+    return g, s
+
+
+def test_c2_stratified_damped_terrain_vs_oracle(gwm, orc):
+    g, s = _c2_case(gwm)
+    uref = s["u"].astype(np.float64).mean(axis=(1, 2))
+    step = gwm.StepConfig(dt=1.0, fast_substeps=6)   # c dt / dz_min = 0.64 (stable window)
+    with gwm.Model(g, gwm.MemberSpec(step=step)) as m:
+        m.upload(s)
+        m.set_damping(14000.0, 0.05, u_ref=uref)
+        m.advance_dry_state_ssprk3(3)
+        out = m.download()
+    ost = ostep(orc, step)
+    ost.damp_z_bottom, ost.damp_rate, ost.damp_u_ref, ost.damp_v_ref = 14000.0, 0.05, uref, np.zeros(g.nz)
+    ref = orc.run(ogrid(orc, g), ost, to64(s), 3, precision=64)
+    ref32 = orc.run(ogrid(orc, g), ost, to64(s), 3, precision=32)
+    base = to64(s)
+    assert_envelope(out, ref, ref32, ("rho", "rho_theta"), floor=2e-6, factor=3.0, tag="c2")
+    assert_envelope(out, ref, ref32, ("u", "v", "w"), base=base, floor=2e-4, factor=3.0, tag="c2")
+
+
+def test_damping_tma_and_overlapped_slow_agree(gwm):
+    # flat terrain with the damping layer: the TMA slow stage and the overlapped tiles agree
+    nz = 16
+    g = gwm.GridSpec(72, 40, nz, dx=1000.0, dy=1000.0, z_top=16000.0)
+    p = gwm.CaseParams(theta_ref=288.0, u_background=10.0, v_background=-3.0, brunt_vaisala=0.01)
+    s = gwm.build_case("stratified_mountain_wave", g, p)
+    s["u"][:, :, -1] = s["u"][:, :, 0]
+    s["v"][:, -1, :] = s["v"][:, 0, :]
+    s["w"][8:] = 0.3
+    uref = s["u"].astype(np.float64).mean(axis=(1, 2))
+    vref = s["v"].astype(np.float64).mean(axis=(1, 2))
+    outs = {}
+    for r in (3, 16):
+        with gwm.Model(g, gwm.MemberSpec(step=gwm.StepConfig(dt=1.0, fast_substeps=3))) as m:
+            m.set_tile("slow_stage", r)
+            m.upload(s)
+            m.set_damping(10000.0, 0.1, u_ref=uref, v_ref=vref)
+            m.advance_dry_state_ssprk3(2)
+            outs[r] = m.download()
+    for k in outs[16]:
+        assert np.array_equal(outs[3][k], outs[16][k]), k

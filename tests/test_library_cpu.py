@@ -116,3 +116,43 @@ def test_moist_sounding_properties(gwm):
     assert np.array_equal(s["rho_theta"], s2["rho_theta"])
     s3 = gwm.build_case("moist_sounding", g, gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=4), moist=True)
     assert not np.array_equal(s["rho_theta"], s3["rho_theta"])
+
+
+def test_stratified_mountain_wave_background(gwm):
+    # constant-N background (an extension of the reference's constant-theta mountain-wave
+    # case): N^2 = g/theta dtheta/dz recovered from the cell values, hydrostatic residual
+    # small, face momenta = face-mean density x wind
+    nz = 40
+    g = gwm.GridSpec(16, 12, nz, dx=1000.0, dy=1000.0, z_top=20000.0)
+    p = gwm.CaseParams(theta_ref=288.0, p_surface=100000.0, u_background=10.0, brunt_vaisala=0.01)
+    s = gwm.build_case("stratified_mountain_wave", g, p)
+    rho = s["rho"][:, 5, 7].astype(np.float64)
+    th = (s["rho_theta"][:, 5, 7] / s["rho"][:, 5, 7]).astype(np.float64)
+    z = (np.arange(nz) + 0.5) * 20000.0 / nz
+    n2 = 9.81 * np.diff(np.log(th)) / np.diff(z)   # exact for theta0 exp(N^2 z / g)
+    assert np.allclose(n2, 1.0e-4, rtol=2e-3)
+    # hydrostatic: (p_{k+1} - p_k)/dz = -g * mean density, to discretisation accuracy
+    pres = 1.0e5 * (287.05 * rho * th / 1.0e5) ** (1.0 / (1.0 - 0.2854))
+    resid = np.diff(pres) / np.diff(z) + 9.81 * 0.5 * (rho[1:] + rho[:-1])
+    assert np.abs(resid).max() < 2e-3 * 9.81 * rho.max()
+    u = s["u"][:, 5, 7].astype(np.float64)
+    assert np.allclose(u, 10.0 * 0.5 * (s["rho"][:, 5, 6] + s["rho"][:, 5, 7]), rtol=1e-6)
+    assert np.all(s["w"] == 0.0)
+
+
+def test_rayleigh_layer_in_oracle(orc, gwm):
+    # the damping layer (extension) acts only above its bottom and pulls w to zero there
+    g = gwm.GridSpec(16, 12, 20, dx=1000.0, dy=1000.0, z_top=20000.0)
+    p = gwm.CaseParams(theta_ref=288.0, u_background=10.0, brunt_vaisala=0.01)
+    s = gwm.build_case("stratified_mountain_wave", g, p)
+    s["w"][10:, :, :] = 0.5  # an upper-level vertical motion to be damped
+    st = {k: v.astype(np.float64) for k, v in s.items()}
+    og = orc.GridSpec(16, 12, 20, dx=1000.0, dy=1000.0, z_top=20000.0)
+    uref = s["u"].astype(np.float64).mean(axis=(1, 2))
+    free = orc.run(og, orc.StepSpec(dt=1.0, fast_substeps=2), st, 1)
+    damp = orc.run(og, orc.StepSpec(dt=1.0, fast_substeps=2, damp_z_bottom=14000.0, damp_rate=0.2,
+                                    damp_u_ref=uref, damp_v_ref=np.zeros(20)), st, 1)
+    top = slice(16, 20)   # faces above 16 km
+    assert np.abs(damp["w"][top]).mean() < np.abs(free["w"][top]).mean() * 0.95
+    low = slice(1, 10)    # below the layer the two runs agree to rounding at one step
+    assert np.abs(damp["w"][low] - free["w"][low]).max() < 1e-3 * max(np.abs(free["w"][low]).max(), 1e-3)
