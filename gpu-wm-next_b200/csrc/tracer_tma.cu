@@ -116,8 +116,22 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
   float qb0[NTR] = {0.f, 0.f, 0.f}, qb1[NTR] = {0.f, 0.f, 0.f};  // own mixing ratios at k-1
   __syncthreads();
 
+  // blend partner of plane kk at the thread's owned cells (prefetched a plane ahead)
+  auto load_q0 = [&](int gj, bool own, int kk, float* q0v) {
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) q0v[t] = 0.f;
+    if (!own || !blend || kk >= nz) return;
+    const int o = gidx(g, gi, gj, kk);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t)
+      if (t < a.ntracers) q0v[t] = __ldg(a.q0[t] + o);
+  };
+  float q0a[NTR], q0b[NTR];
+  load_q0(gj0, own0, 0, q0a);
+  load_q0(gj1, own1, 0, q0b);
+
   // one owned column of plane k
-  auto column = [&](int k, int r, int gj, bool own, float* qb) {
+  auto column = [&](int k, int r, int gj, bool own, float* qb, const float* q0v) {
     const float* st = ring + (k % NSLOT) * SLOT;
     const float* sn = ring + ((k + 1) % NSLOT) * SLOT;
     const int c = tx + 1;
@@ -126,13 +140,6 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
     const float fs = st[O_V + (r - 1) * FBW + tx], fn = st[O_V + r * FBW + tx];
     const float fb = st[O_W + (r - 1) * OBW + tx], ft = sn[O_W + (r - 1) * OBW + tx];
     const float idz = __ldg(a.idz_c + k);
-    float q0v[NTR] = {0.f, 0.f, 0.f};
-    const int o = gidx(g, gi, gj, k);
-    if (own && blend) {
-#pragma unroll
-      for (int t = 0; t < NTR; ++t)
-        if (t < a.ntracers) q0v[t] = __ldg(a.q0[t] + o);
-    }
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       if (t >= a.ntracers) break;
@@ -159,10 +166,15 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
   for (int k = 0; k < nz; ++k) {
     // mixing ratios of plane k+1 (the own ones are this thread's, the ring published
     // by the barrier below for the next plane)
+    float n0a[NTR], n0b[NTR];
+    load_q0(gj0, own0, k + 1, n0a);
+    load_q0(gj1, own1, k + 1, n0b);
     wait_plane(k + 1, k);
     if (k + 1 < nz) mix(k + 1);
-    column(k, ty + 1, gj0, own0, qb0);
-    column(k, ty + RY + 1, gj1, own1, qb1);
+    column(k, ty + 1, gj0, own0, qb0, q0a);
+    column(k, ty + RY + 1, gj1, own1, qb1, q0b);
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) { q0a[t] = n0a[t]; q0b[t] = n0b[t]; }
     __syncthreads();  // publishes plane k+1's ring; slot k is free
     if (s_abort[k & 1]) { aborted = true; break; }
     if (tid == 0 && k + 3 <= nz) { issue(k + 3); issued = k + 3; }
