@@ -27,8 +27,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _ROOT = os.path.dirname(_HERE)
 _LIB_PATH = os.path.join(_HERE, "_build", "libgwm_b200.so")
 _SOURCES = ["capi.cu", "dycore.cu", "fast_tma.cu", "slow_tma.cu", "tracer_tma.cu", "physics.cu", "halo.cu",
-            "cases.cpp"]
-_HEADERS = ["common.cuh", "dycore.cuh", "physics.cuh", "halo.cuh", "tma.cuh"]
+            "surrogate.cu", "surrogate_rain.cu", "cases.cpp"]
+_HEADERS = ["common.cuh", "dycore.cuh", "physics.cuh", "halo.cuh", "tma.cuh", "rain_cell.cuh", "surrogate.cuh", "surrogate_rain.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -123,6 +123,11 @@ class _CaseParams(C.Structure):
         ("seed", C.c_uint64)]
 
 
+class _MlpTrain(C.Structure):
+    _fields_ = [("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float), ("seed", C.c_ulonglong),
+                ("init", C.c_int)]
+
+
 class _TerrainParams(C.Structure):
     _fields_ = [(k, C.c_double) for k in ("height", "center_x_fraction", "center_y_fraction",
                                           "half_width_x", "half_width_y")]
@@ -165,6 +170,14 @@ def lib():
     L.gwm_b200_apply_reference_boundaries.argtypes = [vp, C.c_int]
     L.gwm_b200_set_damping.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double),
                                        C.POINTER(C.c_double)]
+    L.gwm_b200_rain_record.argtypes = [vp, C.c_int, vp, vp, C.c_longlong, C.c_ulonglong, C.c_float,
+                                       C.c_float, C.POINTER(C.c_longlong)]
+    L.gwm_b200_mlp_train.argtypes = [vp, vp, C.c_longlong, C.POINTER(_MlpTrain), C.POINTER(C.c_float),
+                                     C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_double)]
+    L.gwm_b200_mlp_loss_grad.argtypes = [C.POINTER(C.c_float)] * 4 + [C.c_int, C.POINTER(C.c_float),
+                                                                      C.POINTER(C.c_double)]
+    L.gwm_b200_set_rain_surrogate.argtypes = [vp, C.c_int] + [C.POINTER(C.c_float)] * 3 + [C.c_float, C.c_float]
+    L.gwm_b200_surrogate_fallbacks.argtypes = [vp, C.c_int, C.POINTER(C.c_longlong), C.c_int]
     L.gwm_b200_get_tile.argtypes = [vp, C.c_int]
     L.gwm_b200_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double),
                                         C.POINTER(C.c_longlong), C.POINTER(C.c_char_p)]
@@ -193,7 +206,9 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_step", "gwm_b200_advance_dry", "gwm_b200_advance_tracers",
             "gwm_b200_warm_rain", "gwm_b200_fast_modes", "gwm_b200_slow_tendencies",
             "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_get_tile", "gwm_b200_set_boundary_state",
-            "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_layout",
+            "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_rain_record",
+            "gwm_b200_mlp_train", "gwm_b200_mlp_loss_grad", "gwm_b200_set_rain_surrogate",
+            "gwm_b200_surrogate_fallbacks", "gwm_b200_layout",
             "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_ranks_to_global",
             "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
 
@@ -394,6 +409,38 @@ class Model:
         args = [p.ctypes.data_as(C.POINTER(C.c_double)) if p is not None else None for p in ptrs]
         self._check(lib().gwm_b200_set_damping(self._h, member, float(z_bottom), float(rate), *args),
                     "set_damping")
+
+    def rain_samples(self, x, y, seed: int = 1, p_active: float = 1.0, p_inactive: float = 0.05,
+                     member: int = 0) -> int:
+        """Cell samples of the plain warm-rain scheme at the current state into device
+        buffers ``x`` (capacity, 7) and ``y`` (capacity, 5) (float32 tensors or device
+        pointers); returns the number written."""
+        xp, cap = _dev_ptr(x), _rows(x)
+        yp = _dev_ptr(y)
+        n = C.c_longlong()
+        self._check(lib().gwm_b200_rain_record(self._h, member, xp, yp, cap, seed, p_active, p_inactive,
+                                               C.byref(n)), "rain_samples")
+        return int(n.value)
+
+    def set_rain_surrogate(self, params=None, norm=None, rng=None, tol_water: float = 1e-3,
+                           tol_energy: float = 0.05, member: int = 0):
+        """Warm rain with the trained network (BF16 tensor-core inference, plain-scheme
+        fallback per cell); ``params=None`` restores the plain scheme."""
+        if params is None:
+            self._check(lib().gwm_b200_set_rain_surrogate(self._h, member, None, None, None, 0.0, 0.0),
+                        "set_rain_surrogate")
+            return
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        p, n_, r_ = f(params), f(norm), f(rng)
+        ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        self._check(lib().gwm_b200_set_rain_surrogate(self._h, member, ptr(p), ptr(n_), ptr(r_), tol_water,
+                                                      tol_energy), "set_rain_surrogate")
+
+    def surrogate_fallbacks(self, reset: bool = False, member: int = 0) -> int:
+        n = C.c_longlong()
+        self._check(lib().gwm_b200_surrogate_fallbacks(self._h, member, C.byref(n), int(reset)),
+                    "surrogate_fallbacks")
+        return int(n.value)
 
     def apply_reference_boundaries(self, member: int = 0):
         """apply_reference_boundaries once on the current state."""
@@ -658,3 +705,48 @@ def build_terrain(kind: str, nx: int, ny: int, dx: float, dy: float, height: flo
     if rc != OK:
         raise RuntimeError(f"build_terrain({kind}): status {rc}")
     return out
+
+
+# ---------------------------------------------------------------------------
+# Learned warm-rain microphysics: training side
+MLP_PARAMS = 64 * 7 + 64 + 2 * (64 * 64 + 64) + 5 * 64 + 5
+MLP_NORM = 24
+
+
+def _dev_ptr(t):
+    """Device pointer of a CUDA tensor (or an int pointer)."""
+    return t if isinstance(t, int) else t.data_ptr()
+
+
+def _rows(t):
+    return t.shape[0]
+
+
+def mlp_train(x, y, n: int, epochs: int = 10, batch: int = 65536, lr: float = 1e-3, seed: int = 1,
+              params: Optional[np.ndarray] = None):
+    """Train the 7-64-64-64-5 network on ``n`` device samples with the library's own
+    forward/backward kernels and Adam.  Returns (params, norm, input range, loss per epoch)."""
+    p = np.zeros(MLP_PARAMS, np.float32) if params is None else np.array(params, np.float32)
+    norm = np.zeros(MLP_NORM, np.float32)
+    rng = np.zeros(14, np.float32)
+    loss = np.zeros(epochs, np.float64)
+    cfg = _MlpTrain(epochs, batch, lr, seed, 1 if params is None else 0)
+    f32 = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    rc = lib().gwm_b200_mlp_train(_dev_ptr(x), _dev_ptr(y), n, C.byref(cfg), f32(p), f32(norm), f32(rng),
+                                  loss.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != OK:
+        raise RuntimeError(f"mlp_train: status {rc}")
+    return p, norm, rng, loss
+
+
+def mlp_loss_grad(params, norm, x, y):
+    """Loss and gradient of the network on host samples (the GPU kernels of training)."""
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    p, nm, xx, yy = f32(params), f32(norm), f32(x), f32(y)
+    g = np.zeros(MLP_PARAMS, np.float32)
+    loss = C.c_double()
+    ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    rc = lib().gwm_b200_mlp_loss_grad(ptr(p), ptr(nm), ptr(xx), ptr(yy), xx.shape[0], ptr(g), C.byref(loss))
+    if rc != OK:
+        raise RuntimeError(f"mlp_loss_grad: status {rc}")
+    return loss.value, g

@@ -30,6 +30,8 @@
 #include "dycore.cuh"
 #include "halo.cuh"
 #include "physics.cuh"
+#include "surrogate.cuh"
+#include "surrogate_rain.cuh"
 
 using namespace gwmb;
 
@@ -75,6 +77,10 @@ struct Member {
   // Rayleigh damping layer (extension): [tau_c(nz) | tau_f(nz+1) | u_ref(nz) | v_ref(nz)]
   float* damp = nullptr;
   bool damping = false;
+  // learned warm-rain microphysics: fragments | bias | norm | range | fallback counter
+  char* sur = nullptr;
+  bool use_surrogate = false;
+  float sur_tol_water = 0.0f, sur_tol_energy = 0.0f;
   // TMA descriptors of the substep's buffers: (buffer, box kind 0 cell / 1 face / 2 own, map)
   std::vector<std::tuple<const float*, int, CUtensorMap>> tmaps;
   const CUtensorMap* tmap(const float* buf, int kind) const {
@@ -683,7 +689,19 @@ int enqueue_rain(gwm_b200_ctx* c, Member& M, int fallout) {
   a.idz_c = M.idc; a.terrain = M.terrain_active;
   a.th_acc = M.slot(M.ring);
   a.inv_count = inv_count(M);
-  LAUNCH(launch_warm_rain(a, c->stream), "warm rain");
+  if (M.use_surrogate) {
+    SurrogateArgs sa{};
+    sa.frags = (const uint2*)M.sur;
+    sa.bias = (const float*)(M.sur + kSurFrags * 32 * sizeof(uint2));
+    sa.norm = sa.bias + kSurBias;
+    sa.range = sa.norm + kMlpNorm;
+    sa.fallbacks = (unsigned long long*)(M.sur + 65536);
+    sa.tol_water = M.sur_tol_water;
+    sa.tol_energy = M.sur_tol_energy;
+    LAUNCH(launch_warm_rain_surrogate(a, sa, c->stream), "warm rain");
+  } else {
+    LAUNCH(launch_warm_rain(a, c->stream), "warm rain");
+  }
   return GWM_B200_OK;
 }
 
@@ -778,6 +796,7 @@ void gwm_b200_destroy(gwm_b200_ctx* c) {
   for (auto& M : c->m) {
     if (M.block) cudaFree(M.block);
     if (M.bstrip) cudaFree(M.bstrip);
+    if (M.sur) cudaFree(M.sur);
   }
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -945,6 +964,217 @@ int gwm_b200_apply_reference_boundaries(gwm_b200_ctx* c, int member) {
   CK(launch_strips(M.g, J, c->stream));
   M.theta_valid = false;
   CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Learned warm-rain microphysics: samples, training, gradient.
+namespace {
+RainArgs rain_args(const Member& M, int fallout) {
+  const gwm_b200_warm_rain_config& r = M.md.rain;
+  RainArgs a{};
+  a.g = M.g;
+  a.rho = M.Q[0]; a.rt = M.Q[1];
+  a.qv = M.T0[0]; a.qc = M.T0[1]; a.qr = M.T0[2];
+  a.dt = r.dt; a.relax = r.condensation_relaxation; a.thr = r.cloud_autoconversion_threshold;
+  a.rate = r.cloud_autoconversion_rate; a.evap = r.rain_evaporation_rate;
+  a.vt = r.rain_terminal_velocity; a.layer_depth = r.sedimentation_layer_depth_m;
+  a.latent = r.enable_latent_heating;
+  int mode = 0;
+  if (fallout == 1 && r.rain_terminal_velocity > 0.0f) mode = 1;
+  if (fallout == 2 && r.rain_terminal_velocity > 0.0f && r.sedimentation_layer_depth_m > 0.0f) mode = 2;
+  a.fallout_mode = mode;
+  a.idz_c = M.idc; a.terrain = M.terrain_active;
+  return a;
+}
+
+uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+}  // namespace
+
+int gwm_b200_rain_record(gwm_b200_ctx* c, int member, float* x, float* y, long long capacity,
+                         unsigned long long seed, float p_active, float p_inactive, long long* n_out) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  if (!M.md.moist) return fail(c, GWM_B200_ERR_ARG, "warm-rain samples need a moist member");
+  if (!x || !y || capacity <= 0 || !n_out) return fail(c, GWM_B200_ERR_ARG, "bad sample buffers");
+  RecordArgs a{};
+  a.r = rain_args(M, 1);
+  a.x = x; a.y = y; a.capacity = capacity; a.seed = seed;
+  a.p_active = p_active; a.p_inactive = p_inactive;
+  unsigned long long* count = nullptr;
+  CK(cudaMallocAsync(&count, sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), c->stream));
+  a.count = count;
+  CK(launch_rain_record(a, c->stream));
+  unsigned long long h = 0;
+  CK(cudaMemcpyAsync(&h, count, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaFreeAsync(count, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *n_out = (long long)std::min<unsigned long long>(h, (unsigned long long)capacity);
+  return GWM_B200_OK;
+}
+
+int gwm_b200_mlp_loss_grad(const float* params, const float* norm, const float* x, const float* y, int n,
+                           float* grad, double* loss) {
+  if (!params || !norm || !x || !y || n <= 0 || !grad || !loss) return GWM_B200_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GWM_B200_ERR_NO_DEVICE;
+  cudaStream_t s = nullptr;
+  float *dp = nullptr, *dn = nullptr, *dx = nullptr, *dy = nullptr, *scr = nullptr, *part = nullptr, *dg = nullptr;
+  double* dl = nullptr;
+  auto bad = [&](cudaError_t e) { return e != cudaSuccess; };
+  int rc = GWM_B200_OK;
+  if (bad(cudaMalloc(&dp, kMlpParams * 4)) || bad(cudaMalloc(&dn, kMlpNorm * 4)) ||
+      bad(cudaMalloc(&dx, (size_t)n * kMlpIn * 4)) || bad(cudaMalloc(&dy, (size_t)n * kMlpOut * 4)) ||
+      bad(cudaMalloc(&scr, mlp_scratch_floats(n) * 4)) || bad(cudaMalloc(&part, mlp_partial_floats(n) * 4)) ||
+      bad(cudaMalloc(&dg, kMlpParams * 4)) || bad(cudaMalloc(&dl, sizeof(double)))) {
+    rc = GWM_B200_ERR_CUDA;
+  } else {
+    cudaMemcpy(dp, params, kMlpParams * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dn, norm, kMlpNorm * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dx, x, (size_t)n * kMlpIn * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dy, y, (size_t)n * kMlpOut * 4, cudaMemcpyHostToDevice);
+    MlpBatch b{dp, dn, dx, dy, nullptr, n, scr, part, dg, dl};
+    if (bad(mlp_loss_grad(b, s)) || bad(cudaMemcpy(grad, dg, kMlpParams * 4, cudaMemcpyDeviceToHost)) ||
+        bad(cudaMemcpy(loss, dl, sizeof(double), cudaMemcpyDeviceToHost)))
+      rc = GWM_B200_ERR_CUDA;
+  }
+  for (void* p : {(void*)dp, (void*)dn, (void*)dx, (void*)dy, (void*)scr, (void*)part, (void*)dg, (void*)dl})
+    if (p) cudaFree(p);
+  return rc;
+}
+
+int gwm_b200_mlp_train(const float* x, const float* y, long long n, const gwm_b200_mlp_train_config* cfg,
+                       float* params, float* norm, float* range, double* loss_per_epoch) {
+  if (!x || !y || n <= 0 || !cfg || !params || !norm || cfg->epochs <= 0 || cfg->batch <= 0) return GWM_B200_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GWM_B200_ERR_NO_DEVICE;
+  const int batch = (int)std::min<long long>(cfg->batch, n);
+  cudaStream_t s = nullptr;
+  std::vector<void*> owned;
+  auto alloc = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    owned.push_back(p);
+    return p;
+  };
+  auto cleanup = [&](int rc) {
+    for (void* p : owned) cudaFree(p);
+    return rc;
+  };
+  double* stats = (double*)alloc((2 * kMlpIn + 2 * kMlpIn + 2 * kMlpOut) * sizeof(double));
+  float* dp = (float*)alloc(kMlpParams * 4);
+  float* dn = (float*)alloc(kMlpNorm * 4);
+  float* dg = (float*)alloc(kMlpParams * 4);
+  float* dm = (float*)alloc(kMlpParams * 4);
+  float* dv = (float*)alloc(kMlpParams * 4);
+  float* scr = (float*)alloc(mlp_scratch_floats(batch) * 4);
+  float* part = (float*)alloc(mlp_partial_floats(batch) * 4);
+  double* dl = (double*)alloc(sizeof(double));
+  int* didx = (int*)alloc((size_t)n * sizeof(int));
+  if (!stats || !dp || !dn || !dg || !dm || !dv || !scr || !part || !dl || !didx) return cleanup(GWM_B200_ERR_CUDA);
+  // normalisation: FP64 means and standard deviations of inputs and targets; input range
+  if (mlp_column_stats(x, n, kMlpIn, stats, stats + 2 * kMlpIn, s) != cudaSuccess ||
+      mlp_column_stats(y, n, kMlpOut, stats + 4 * kMlpIn, nullptr, s) != cudaSuccess)
+    return cleanup(GWM_B200_ERR_CUDA);
+  double hs[4 * kMlpIn + 2 * kMlpOut];
+  if (cudaMemcpy(hs, stats, sizeof(hs), cudaMemcpyDeviceToHost) != cudaSuccess) return cleanup(GWM_B200_ERR_CUDA);
+  for (int f = 0; f < kMlpIn; ++f) {
+    norm[f] = (float)hs[f];
+    norm[kMlpIn + f] = hs[kMlpIn + f] > 1e-30 ? (float)hs[kMlpIn + f] : 1.0f;  // constant input (dt)
+    if (range) { range[f] = (float)hs[2 * kMlpIn + f]; range[kMlpIn + f] = (float)hs[3 * kMlpIn + f]; }
+  }
+  for (int o = 0; o < kMlpOut; ++o) {
+    norm[2 * kMlpIn + o] = (float)hs[4 * kMlpIn + o];
+    const double sd = hs[4 * kMlpIn + kMlpOut + o];
+    norm[2 * kMlpIn + kMlpOut + o] = sd > 1e-30 ? (float)sd : 1.0f;
+  }
+  uint64_t rng = cfg->seed ? cfg->seed : 0x5EED5EEDull;
+  if (cfg->init) {  // Xavier-uniform weights, zero biases
+    auto uni = [&]() { return (double)(splitmix(rng) >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0; };
+    auto fill_w = [&](int off, int nout, int nin) {
+      const double lim = std::sqrt(6.0 / (nin + nout));
+      for (int q = 0; q < nout * nin; ++q) params[off + q] = (float)(lim * uni());
+    };
+    std::fill(params, params + kMlpParams, 0.0f);
+    fill_w(kOffW1, kMlpHid, kMlpIn);
+    fill_w(kOffW2, kMlpHid, kMlpHid);
+    fill_w(kOffW3, kMlpHid, kMlpHid);
+    fill_w(kOffW4, kMlpOut, kMlpHid);
+  }
+  cudaMemcpy(dp, params, kMlpParams * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dn, norm, kMlpNorm * 4, cudaMemcpyHostToDevice);
+  cudaMemset(dm, 0, kMlpParams * 4);
+  cudaMemset(dv, 0, kMlpParams * 4);
+  std::vector<int> perm((size_t)n);
+  for (long long q = 0; q < n; ++q) perm[(size_t)q] = (int)q;
+  int t = 0;
+  for (int ep = 0; ep < cfg->epochs; ++ep) {
+    for (long long q = n - 1; q > 0; --q) std::swap(perm[(size_t)q], perm[(size_t)(splitmix(rng) % (uint64_t)(q + 1))]);
+    if (cudaMemcpy(didx, perm.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+      return cleanup(GWM_B200_ERR_CUDA);
+    double ep_loss = 0.0;
+    long long seen = 0;
+    for (long long b0 = 0; b0 + batch <= n; b0 += batch) {
+      MlpBatch b{dp, dn, x, y, didx + b0, batch, scr, part, dg, dl};
+      if (mlp_loss_grad(b, s) != cudaSuccess || mlp_adam(dp, dg, dm, dv, cfg->lr, ++t, s) != cudaSuccess)
+        return cleanup(GWM_B200_ERR_CUDA);
+      double l = 0.0;
+      if (cudaMemcpy(&l, dl, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return cleanup(GWM_B200_ERR_CUDA);
+      ep_loss += l * batch;
+      seen += batch;
+    }
+    if (loss_per_epoch) loss_per_epoch[ep] = seen ? ep_loss / (double)seen : 0.0;
+  }
+  if (cudaMemcpy(params, dp, kMlpParams * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return cleanup(GWM_B200_ERR_CUDA);
+  return cleanup(GWM_B200_OK);
+}
+
+int gwm_b200_set_rain_surrogate(gwm_b200_ctx* c, int member, const float* params, const float* norm,
+                                const float* range, float tol_water, float tol_energy) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  drop_graph(c);
+  if (!params) { M.use_surrogate = false; return GWM_B200_OK; }
+  if (!norm || !range || !M.md.moist) return fail(c, GWM_B200_ERR_ARG, "surrogate needs norm, range and a moist member");
+  if (!M.sur) {
+    CK(cudaMalloc(&M.sur, 65536 + 256));
+    CK(cudaMemset(M.sur + 65536, 0, 256));
+  }
+  static_assert(kSurFrags * 32 * sizeof(uint2) + (kSurBias + kMlpNorm + kMlpRange) * sizeof(float) <= 65536,
+                "surrogate buffer");
+  std::vector<uint2> fr(kSurFrags * 32);
+  std::vector<float> tail(kSurBias + kMlpNorm + kMlpRange);
+  surrogate_fragments(params, fr.data(), tail.data());
+  std::copy(norm, norm + kMlpNorm, tail.begin() + kSurBias);
+  std::copy(range, range + kMlpRange, tail.begin() + kSurBias + kMlpNorm);
+  CK(cudaMemcpy(M.sur, fr.data(), fr.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(M.sur + fr.size() * sizeof(uint2), tail.data(), tail.size() * sizeof(float), cudaMemcpyHostToDevice));
+  M.use_surrogate = true;
+  M.sur_tol_water = tol_water;
+  M.sur_tol_energy = tol_energy;
+  return GWM_B200_OK;
+}
+
+int gwm_b200_surrogate_fallbacks(gwm_b200_ctx* c, int member, long long* count, int reset) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  if (!count) return GWM_B200_ERR_ARG;
+  *count = 0;
+  if (!M.sur) return GWM_B200_OK;
+  unsigned long long h = 0;
+  CK(cudaMemcpyAsync(&h, M.sur + 65536, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  if (reset) CK(cudaMemsetAsync(M.sur + 65536, 0, sizeof(h), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *count = (long long)h;
   return GWM_B200_OK;
 }
 

@@ -2,6 +2,7 @@
 // three-tracer SSPRK3 stage and the warm-rain column kernel.
 #include "dycore.cuh"
 #include "physics.cuh"
+#include "rain_cell.cuh"
 
 namespace gwmb {
 namespace {
@@ -107,17 +108,6 @@ __global__ void __launch_bounds__(BX * TBY) k_tracer_stage(const TracerArgs a) {
   }
 }
 
-__device__ __forceinline__ float sat_vapor_pressure(float tk) {  // moist_thermo.hpp:23-29
-  const float tc = tk - 273.15f;
-  const float es_hpa = 6.112f * expf((17.67f * tc) / fmaxf(tc + 243.5f, 1.0e-6f));
-  return es_hpa * 100.0f;
-}
-__device__ __forceinline__ float qsat(float tk, float p) {  // moist_thermo.hpp:31-36
-  const float eps = kRd / kRv;
-  const float es = sat_vapor_pressure(tk);
-  const float denom = fmaxf(p - (1.0f - eps) * es, 1000.0f);
-  return fminf(fmaxf(eps * es / denom, 0.0f), 0.05f);
-}
 
 constexpr int RB = 128;  // columns per warm-rain block (one row segment)
 
@@ -148,52 +138,10 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
       const int o = gidx(g, gi, gj, k);
       // warm_rain_kernel: warm_rain.cu:36-120
       const float rho_d = c_rho;
-      const float rho = fmaxf(rho_d, 1.0e-6f);
-      const float rt = c_rt;
-      float th = rt / rho;
-      float p = eos_pressure(rho, rt);
-      float temp;
-      {  // dry_temperature_from_conserved: moist_thermo.hpp:55-62
-        const float thc = theta_of(rho, rt);
-        const float pc = eos_pressure(rho, rt);
-        temp = thc * powf(fmaxf(pc / kP0, 1.0e-6f), kKappa);
-      }
-      const float exner = fmaxf(temp / fmaxf(th, 1.0e-6f), 1.0e-6f);
-      float qv = fmaxf(c_qv / rho, 0.0f);
-      float qc = fmaxf(c_qc / rho, 0.0f);
-      float qr = fmaxf(c_qr / rho, 0.0f);
-      const float lh = kLv / (dry_cp() * fmaxf(exner, 1.0e-6f));
-      float qs = qsat(temp, p);
-      if (qv > qs) {
-        const float cond = fminf((qv - qs) * fmaxf(a.relax, 0.0f), qv);
-        qv -= cond;
-        qc += cond;
-        if (a.latent && cond > 0.0f) th += lh * cond;
-      } else if (qv < qs && qc > 0.0f) {
-        const float ev = fminf((qs - qv) * fmaxf(a.relax, 0.0f), qc);
-        qv += ev;
-        qc -= ev;
-        if (a.latent && ev > 0.0f) th -= lh * ev;
-      }
-      const float excess = fmaxf(qc - a.thr, 0.0f);
-      if (excess > 0.0f && a.rate > 0.0f) {
-        const float conv = fminf(excess, a.dt * a.rate * excess);
-        qc -= conv;
-        qr += conv;
-      }
-      p = eos_pressure(rho, rho * th);
-      temp = th * powf(fmaxf(p / kP0, 1.0e-6f), kKappa);
-      qs = qsat(temp, p);
-      if (qr > 0.0f && qv < qs && a.evap > 0.0f) {
-        const float ev = fminf(qr, a.dt * a.evap * fminf(qs - qv, qr));
-        qr -= ev;
-        qv += ev;
-        if (a.latent && ev > 0.0f) th -= lh * ev;
-      }
-      qv = fmaxf(qv, 0.0f);
-      qc = fmaxf(qc, 0.0f);
-      qr = fmaxf(qr, 0.0f);
-      float rqr = rho * qr;
+      MicroCell mc = micro_state(rho_d, c_rt, c_qv, c_qc, c_qr);
+      micro_step(mc, MicroParams{a.dt, a.relax, a.thr, a.rate, a.evap, a.latent});
+      const float rho = mc.rho, th = mc.th, qv = mc.qv, qc = mc.qc;
+      float rqr = rho * mc.qr;
       // fallout of this cell, fed by the cell above
       if (a.fallout_mode == 1) {  // rain_fallout_metric_kernel: warm_rain.cu:156-191
         const float idz = fmaxf(a.terrain ? __ldg(a.idz_c + o) : __ldg(a.idz_c + k), 1.0e-6f);

@@ -1,0 +1,33 @@
+// surrogate_rain.cuh — launch interface of the warm-rain kernel with the learned
+// microphysics (surrogate_rain.cu).
+#pragma once
+
+#include <cstdint>
+
+#include "dycore.cuh"
+#include "surrogate.cuh"
+
+namespace gwmb {
+
+// Weights as mma.sync B fragments, per lane: layer 1 (8), layers 2 and 3 (32 each),
+// output layer (4) fragments of 32 lanes x (b0, b1) BF16 pairs.
+constexpr int kSurFrags = 8 + 32 + 32 + 4;
+// Biases: b1 (64) b2 (64) b3 (64) b4 (5, padded to 8).
+constexpr int kSurBias = 3 * kMlpHid + 8;
+
+struct SurrogateArgs {
+  const uint2* frags;            // kSurFrags * 32
+  const float* bias;             // kSurBias
+  const float* norm;             // kMlpNorm: x mean/std, y mean/std
+  const float* range;            // kMlpRange: x min/max of the training data
+  float tol_water;               // |dqv + dqc + dqr| <= tol_water * (qv + qc + qr)
+  float tol_energy;              // |dtheta + L/(cp pi) dqv| <= tol_energy (K)
+  unsigned long long* fallbacks; // cells that took the plain scheme (accumulated)
+};
+
+cudaError_t launch_warm_rain_surrogate(const RainArgs& a, const SurrogateArgs& s, cudaStream_t st);
+
+// Host: weights (FP32 parameter vector) -> BF16 B fragments and FP32 biases.
+void surrogate_fragments(const float* params, uint2* frags, float* bias);
+
+}  // namespace gwmb

@@ -168,6 +168,39 @@ int gwm_b200_set_damping(gwm_b200_ctx* ctx, int member, double z_bottom, double 
                          const double* u_ref, const double* v_ref);
 /* apply_reference_boundaries once on the current state (dry fields and, when set, tracers). */
 int gwm_b200_apply_reference_boundaries(gwm_b200_ctx* ctx, int member);
+/* ---- learned warm-rain microphysics (training side) ----
+ * Cell samples of the plain scheme at the member's current state (no state change):
+ * x (capacity x 7, device) = (T, p, rho_d, qv, qc, qr, dt), y (capacity x 5, device) =
+ * (dqv, dqc, dqr, dtheta, fallout flux out of the cell over the step, kg m-2).  Cells
+ * with a non-zero tendency are kept with probability p_active, the others with
+ * p_inactive (seeded hash of the cell index); *n_out = samples written. */
+int gwm_b200_rain_record(gwm_b200_ctx* ctx, int member, float* x, float* y, long long capacity,
+                         unsigned long long seed, float p_active, float p_inactive, long long* n_out);
+typedef struct {
+  int epochs, batch;
+  float lr;                 /* Adam learning rate */
+  unsigned long long seed;  /* initialisation and shuffling */
+  int init;                 /* 1: initialise params (Xavier uniform), 0: start from params */
+} gwm_b200_mlp_train_config;
+/* Trains the 7-64-64-64-5 GELU network on n device samples (x, y as above) with the
+ * project's FP32 forward/backward kernels and Adam; params (host, 9157 floats) in/out,
+ * norm (host, 24 floats) out: input mean/std, target mean/std; range (host, 14 floats,
+ * may be NULL) out: input min/max; loss_per_epoch (host, epochs) out: mean squared
+ * error of the normalised targets. */
+int gwm_b200_mlp_train(const float* x, const float* y, long long n, const gwm_b200_mlp_train_config* cfg,
+                       float* params, float* norm, float* range, double* loss_per_epoch);
+/* Warm rain of a member with the trained network (params 9157, norm 24, range 14
+ * floats, host) instead of the plain per-cell microphysics; NULL params restores the
+ * plain scheme.  Cells whose inputs leave the training range or whose outputs break
+ * the water (|dqv+dqc+dqr| > tol_water (qv+qc+qr)) or energy (|dtheta + L/(cp pi) dqv|
+ * > tol_energy K) relations, or would make a mixing ratio negative, take the plain
+ * scheme; gwm_b200_surrogate_fallbacks reports how many (cumulative; reset != 0 clears). */
+int gwm_b200_set_rain_surrogate(gwm_b200_ctx* ctx, int member, const float* params, const float* norm,
+                                const float* range, float tol_water, float tol_energy);
+int gwm_b200_surrogate_fallbacks(gwm_b200_ctx* ctx, int member, long long* count, int reset);
+/* Loss and gradient of the network on n host samples (gradient check). */
+int gwm_b200_mlp_loss_grad(const float* params, const float* norm, const float* x, const float* y, int n,
+                           float* grad, double* loss);
 /* FP64 budgets of the current state. */
 int gwm_b200_budgets(gwm_b200_ctx* ctx, int member, gwm_b200_budget* out);
 /* Tile shape of a kernel.  kernel 0 = slow stage: rows 3 = owned 32x16 tiles fed by

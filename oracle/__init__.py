@@ -80,6 +80,7 @@ def lib():
                               C.c_int, C.POINTER(Fields)]
         L.gwo_run_boundary.argtypes = [C.POINTER(Grid), C.POINTER(Step), C.POINTER(Rain), C.c_int,
                                        C.c_int, C.c_int, C.POINTER(Fields), C.POINTER(Fields)]
+        L.gwo_mlp_loss_grad.argtypes = [DP, DP, DP, DP, C.c_int, DP, DP]
         L.gwo_slow_tendencies.argtypes = [C.POINTER(Grid), C.POINTER(Step), C.c_int,
                                           C.POINTER(Fields), C.POINTER(Fields)]
         L.gwo_fast_modes.argtypes = [C.POINTER(Grid), C.POINTER(Step), C.c_int, C.POINTER(Fields)]
@@ -332,3 +333,18 @@ def set_threads(n: int) -> None:
 
 def max_threads() -> int:
     return int(lib().gwo_max_threads())
+
+
+MLP_PARAMS = 64 * 7 + 64 + 2 * (64 * 64 + 64) + 5 * 64 + 5
+
+
+def mlp_loss_grad(params: np.ndarray, norm: np.ndarray, x: np.ndarray, y: np.ndarray):
+    """FP64 loss and gradient of the warm-rain surrogate MLP (checker of the GPU kernels)."""
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    nm = np.ascontiguousarray(norm, dtype=np.float64)
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    yy = np.ascontiguousarray(y, dtype=np.float64)
+    g = np.zeros(MLP_PARAMS)
+    loss = C.c_double()
+    _check(lib().gwo_mlp_loss_grad(_ptr(p), _ptr(nm), _ptr(xx), _ptr(yy), xx.shape[0], _ptr(g), C.byref(loss)))
+    return loss.value, g

@@ -1,3 +1,4 @@
+#include <algorithm>
 // oracle_capi.cpp — C entry points of the CPU ORACLE (test infrastructure only).
 //
 // Wraps gwm_oracle.hpp for the Python test-suite.  All field I/O goes through
@@ -438,6 +439,80 @@ int gwo_run_boundary(const gwo_grid* g, const gwo_step* st, const gwo_rain* rn, 
   return guard([&] {
     return precision == 32 ? run_impl<float>(g, st, rn, phases, nsteps, io, bnd)
                            : run_impl<double>(g, st, rn, phases, nsteps, io, bnd);
+  });
+}
+
+// MLP of the learned warm-rain surrogate, FP64: loss = mean over samples and the 5
+// outputs of (y_hat - (y - y_mean)/y_std)^2 with inputs (x - x_mean)/x_std, three
+// 64-wide hidden layers with GELU 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))).
+// params: W1 (64x7) b1 W2 (64x64) b2 W3 (64x64) b3 W4 (5x64) b4; grad has the same layout.
+int gwo_mlp_loss_grad(const double* params, const double* norm, const double* x, const double* y, int n,
+                      double* grad, double* loss) {
+  return guard([&] {
+    const int I = 7, H = 64, O = 5;
+    const int oW1 = 0, oB1 = oW1 + H * I, oW2 = oB1 + H, oB2 = oW2 + H * H, oW3 = oB2 + H,
+              oB3 = oW3 + H * H, oW4 = oB3 + H, oB4 = oW4 + O * H, np = oB4 + O;
+    std::fill(grad, grad + np, 0.0);
+    const double c = std::sqrt(2.0 / 3.14159265358979323846);
+    auto gelu = [&](double z, double& dg) {
+      const double u = c * (z + 0.044715 * z * z * z), t = std::tanh(u);
+      dg = 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * c * (1.0 + 3.0 * 0.044715 * z * z);
+      return 0.5 * z * (1.0 + t);
+    };
+    double total = 0.0;
+    std::vector<double> x0(I), z1(H), a1(H), g1(H), z2(H), a2(H), g2(H), z3(H), a3(H), g3(H);
+    std::vector<double> d1(H), d2(H), d3(H), d4(O);
+    for (int b = 0; b < n; ++b) {
+      for (int f = 0; f < I; ++f) x0[f] = (x[b * I + f] - norm[f]) / norm[I + f];
+      auto layer = [&](const double* W, const double* B, const std::vector<double>& in, int nin,
+                       std::vector<double>& z, std::vector<double>& a, std::vector<double>& g) {
+        for (int j = 0; j < H; ++j) {
+          double s = B[j];
+          for (int f = 0; f < nin; ++f) s += W[j * nin + f] * in[f];
+          z[j] = s;
+          a[j] = gelu(s, g[j]);
+        }
+      };
+      layer(params + oW1, params + oB1, x0, I, z1, a1, g1);
+      layer(params + oW2, params + oB2, a1, H, z2, a2, g2);
+      layer(params + oW3, params + oB3, a2, H, z3, a3, g3);
+      for (int o = 0; o < O; ++o) {
+        double s = params[oB4 + o];
+        for (int f = 0; f < H; ++f) s += params[oW4 + o * H + f] * a3[f];
+        const double t = (y[b * O + o] - norm[2 * I + o]) / norm[2 * I + O + o];
+        total += (s - t) * (s - t);
+        d4[o] = 2.0 * (s - t) / ((double)n * O);
+      }
+      for (int o = 0; o < O; ++o) {
+        for (int f = 0; f < H; ++f) grad[oW4 + o * H + f] += d4[o] * a3[f];
+        grad[oB4 + o] += d4[o];
+      }
+      auto back = [&](const double* W, int nout, const std::vector<double>& dout, const std::vector<double>& g,
+                      std::vector<double>& din) {
+        for (int f = 0; f < H; ++f) {
+          double s = 0.0;
+          for (int j = 0; j < nout; ++j) s += W[j * H + f] * dout[j];
+          din[f] = s * g[f];
+        }
+      };
+      back(params + oW4, O, d4, g3, d3);
+      for (int j = 0; j < H; ++j) {
+        for (int f = 0; f < H; ++f) grad[oW3 + j * H + f] += d3[j] * a2[f];
+        grad[oB3 + j] += d3[j];
+      }
+      back(params + oW3, H, d3, g2, d2);
+      for (int j = 0; j < H; ++j) {
+        for (int f = 0; f < H; ++f) grad[oW2 + j * H + f] += d2[j] * a1[f];
+        grad[oB2 + j] += d2[j];
+      }
+      back(params + oW2, H, d2, g1, d1);
+      for (int j = 0; j < H; ++j) {
+        for (int f = 0; f < I; ++f) grad[oW1 + j * I + f] += d1[j] * x0[f];
+        grad[oB1 + j] += d1[j];
+      }
+    }
+    *loss = total / ((double)n * O);
+    return 0;
   });
 }
 

@@ -1,0 +1,150 @@
+"""The learned warm-rain microphysics: gradients, training, inference.
+
+The network's FP32 training kernels are checked against the FP64 CPU oracle of the same
+network (oracle.mlp_loss_grad), which is itself checked against finite differences.
+"""
+import numpy as np
+import pytest
+
+
+def _random_net(seed, scale=0.3):
+    rng = np.random.default_rng(seed)
+    import oracle
+    p = rng.normal(0.0, scale, oracle.MLP_PARAMS)
+    norm = np.concatenate([rng.normal(0, 1, 7), rng.uniform(0.5, 2.0, 7), rng.normal(0, 1, 5),
+                           rng.uniform(0.5, 2.0, 5)])
+    return p, norm
+
+
+def test_oracle_mlp_gradient_finite_differences(orc):
+    p, norm = _random_net(3)
+    rng = np.random.default_rng(4)
+    x = rng.normal(0, 1.5, (40, 7))
+    y = rng.normal(0, 1.5, (40, 5))
+    loss, g = orc.mlp_loss_grad(p, norm, x, y)
+    assert loss > 0.0
+    for idx in rng.choice(orc.MLP_PARAMS, 40, replace=False):
+        h = 1e-6
+        pp, pm = p.copy(), p.copy()
+        pp[idx] += h
+        pm[idx] -= h
+        fd = (orc.mlp_loss_grad(pp, norm, x, y)[0] - orc.mlp_loss_grad(pm, norm, x, y)[0]) / (2 * h)
+        assert abs(fd - g[idx]) <= 1e-6 * max(1.0, abs(g[idx])) + 1e-9, idx
+
+
+@pytest.mark.gpu
+def test_gpu_mlp_gradient_matches_oracle(gwm, orc):
+    p, norm = _random_net(5)
+    rng = np.random.default_rng(6)
+    n = 3000   # three gradient chunks (1024 samples each), the last one partial
+    x = rng.normal(0, 1.5, (n, 7))
+    y = rng.normal(0, 1.5, (n, 5))
+    lg, gg = gwm.mlp_loss_grad(p.astype(np.float32), norm.astype(np.float32), x.astype(np.float32),
+                               y.astype(np.float32))
+    # the oracle sees the same FP32-rounded inputs
+    f = lambda a: a.astype(np.float32).astype(np.float64)
+    lo, go = orc.mlp_loss_grad(f(p), f(norm), f(x), f(y))
+    assert abs(lg - lo) <= 1e-5 * lo
+    assert np.abs(gg - go).max() <= 2e-4 * np.abs(go).max()
+
+
+@pytest.mark.gpu
+def test_rain_samples_and_training(gwm):
+    import torch
+    g = gwm.GridSpec(96, 96, 32, dx=2000.0, dy=2000.0, z_top=8000.0)
+    p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=2, relative_humidity=1.03)
+    s = gwm.build_case("moist_sounding", g, p, moist=True)
+    step = gwm.StepConfig(dt=2.0, fast_substeps=4)
+    rain = gwm.WarmRainConfig(dt=2.0, rain_terminal_velocity=12.0)
+    cap = 200_000
+    x = torch.empty((cap, 7), dtype=torch.float32, device="cuda")
+    y = torch.empty((cap, 5), dtype=torch.float32, device="cuda")
+    with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=True)) as m:
+        m.upload(s)
+        n = 0
+        for it in range(6):
+            m.step(3)
+            n += m.rain_samples(x[n:], y[n:], seed=it + 1, p_active=1.0, p_inactive=0.02)
+    assert n > 10_000
+    xs, ys = x[:n].cpu().numpy(), y[:n].cpu().numpy()
+    assert np.isfinite(xs).all() and np.isfinite(ys).all()
+    assert (ys[:, 0] != 0).mean() > 0.05          # condensation/evaporation present
+    assert np.all(xs[:, 3:6] >= 0)                  # clipped mixing ratios
+    # water is conserved by the microphysics: dqv + dqc + dqr = 0 to rounding
+    assert np.abs(ys[:, 0] + ys[:, 1] + ys[:, 2]).max() < 1e-6
+    params, norm, rng, loss = gwm.mlp_train(x, y, n, epochs=8, batch=8192, lr=2e-3, seed=7)
+    assert np.isfinite(loss).all()
+    assert loss[-1] < 0.5 * loss[0]
+    assert np.allclose(rng[:7], xs.min(axis=0)) and np.allclose(rng[7:], xs.max(axis=0))
+
+
+def _bf16(a):
+    """Round float32 to bfloat16 (nearest even) and back."""
+    u = np.asarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u >> 16) & 1) + 0x7FFF
+    return (((u + r) >> 16) << 16).astype(np.uint32).view(np.float32)
+
+
+def _emulate(params, norm, x):
+    """The network as the inference kernel evaluates it: BF16 inputs and weights, FP32
+    accumulation, GELU (tanh form)."""
+    import oracle
+    o1 = 64 * 7
+    W1, b1 = params[:o1].reshape(64, 7), params[o1:o1 + 64]
+    o2 = o1 + 64
+    W2, b2 = params[o2:o2 + 4096].reshape(64, 64), params[o2 + 4096:o2 + 4160]
+    o3 = o2 + 4160
+    W3, b3 = params[o3:o3 + 4096].reshape(64, 64), params[o3 + 4096:o3 + 4160]
+    o4 = o3 + 4160
+    W4, b4 = params[o4:o4 + 320].reshape(5, 64), params[o4 + 320:o4 + 325]
+    gelu = lambda z: 0.5 * z * (1 + np.tanh(0.7978845608 * (z + 0.044715 * z ** 3)))
+    a = _bf16((x - norm[:7]) / norm[7:14]).astype(np.float64)
+    for W, b in ((W1, b1), (W2, b2), (W3, b3)):
+        a = _bf16(gelu(a @ _bf16(W).T.astype(np.float64) + b)).astype(np.float64)
+    yn = a @ _bf16(W4).T.astype(np.float64) + b4
+    return yn * norm[19:24] + norm[14:19]
+
+
+@pytest.mark.gpu
+def test_surrogate_tensor_core_network_matches_emulation(gwm):
+    # random network with a tiny output scale: every cell takes the network step (closure
+    # tolerances opened, the non-negativity fallback predicted), and the per-cell changes
+    # of qv and qc recovered from the state match the BF16 emulation of the network
+    g = gwm.GridSpec(70, 12, 10, dx=2000.0, dy=2000.0, z_top=6000.0)
+    p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.3, seed=3, relative_humidity=0.8)
+    s = gwm.build_case("moist_sounding", g, p, moist=True)
+    s["qc"] = (s["rho"] * 2e-4).astype(np.float32)      # cloud water everywhere: qc + dqc >= 0
+    rng = np.random.default_rng(11)
+    params = rng.normal(0.0, 0.4, 9157).astype(np.float32)
+    rho = s["rho"].astype(np.float32)
+    th = (s["rho_theta"] / rho).astype(np.float32)
+    pres = (np.float32(1e5) * np.maximum(rho * np.float32(287.05) * th / np.float32(1e5), np.float32(1e-6))
+            ** np.float32(1.0 / (1.0 - 0.2854))).astype(np.float32)
+    temp = (th * np.maximum(pres / np.float32(1e5), np.float32(1e-6)) ** np.float32(0.2854)).astype(np.float32)
+    qv, qc, qr = (np.maximum(s[k] / rho, 0).astype(np.float32) for k in ("qv", "qc", "qr"))
+    x = np.stack([temp, pres, rho, qv, qc, qr, np.full_like(rho, 2.0)], -1).reshape(-1, 7)
+    xmean, xstd = x.mean(0), x.std(0) + 1e-12
+    xstd[6] = 1.0
+    norm = np.concatenate([xmean, xstd, np.zeros(5), np.array([1e-6, 1e-6, 1e-6, 1e-3, 1e-9])]).astype(np.float32)
+    rngv = np.concatenate([x.min(0) - 1.0, x.max(0) + 1.0]).astype(np.float32)
+    rngv[[1, 8]] = [x[:, 1].min() - 100.0, x[:, 1].max() + 100.0]
+    step = gwm.StepConfig(dt=2.0, fast_substeps=2)
+    rain = gwm.WarmRainConfig(dt=2.0, rain_terminal_velocity=0.0)  # no fallout
+    with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=True)) as m:
+        m.upload(s)
+        m.set_rain_surrogate(params, norm, rngv, tol_water=1e9, tol_energy=1e9)
+        m.apply_warm_rain_microphysics("metric")
+        out = m.download()
+        fb = m.surrogate_fallbacks()
+    dq = _emulate(params.astype(np.float64), norm.astype(np.float64), x.astype(np.float64))
+    qr_new = qr.reshape(-1) - dq[:, 0] - dq[:, 1]
+    expect_fb = (qv.reshape(-1) + dq[:, 0] < 0) | (qc.reshape(-1) + dq[:, 1] < 0) | (qr_new < 0)
+    # cells near the non-negativity threshold may land on either side
+    assert abs(fb - expect_fb.sum()) <= max(3, int(0.01 * x.shape[0])), (fb, expect_fb.sum())
+    dqv = (out["qv"] / rho - qv).reshape(-1)
+    dqc = (out["qc"] / rho - qc).reshape(-1)
+    ok = ~expect_fb
+    err_v = np.abs(dqv[ok] - dq[ok, 0])
+    err_c = np.abs(dqc[ok] - dq[ok, 1])
+    assert np.quantile(err_v, 0.99) <= 0.05 * np.abs(dq[ok, 0]).std() + 2e-9
+    assert np.quantile(err_c, 0.99) <= 0.05 * np.abs(dq[ok, 1]).std() + 2e-9
