@@ -148,3 +148,49 @@ def test_surrogate_tensor_core_network_matches_emulation(gwm):
     err_c = np.abs(dqc[ok] - dq[ok, 1])
     assert np.quantile(err_v, 0.99) <= 0.05 * np.abs(dq[ok, 0]).std() + 2e-9
     assert np.quantile(err_c, 0.99) <= 0.05 * np.abs(dq[ok, 1]).std() + 2e-9
+
+
+@pytest.mark.gpu
+def test_trained_surrogate_against_plain_scheme(gwm):
+    # train on two seeds, evaluate on a third: surface precipitation within 5 % of the
+    # plain scheme after the run, total water (vapour + cloud + rain + precipitation)
+    # conserved as well as by the plain scheme, the fallback fraction reported
+    import torch
+    g = gwm.GridSpec(96, 96, 32, dx=2000.0, dy=2000.0, z_top=8000.0)
+    step = gwm.StepConfig(dt=2.0, fast_substeps=4)
+    rain = gwm.WarmRainConfig(dt=2.0, rain_terminal_velocity=12.0)
+    spec = gwm.MemberSpec(step=step, rain=rain, moist=True)
+    cap = 1_500_000
+    x = torch.empty((cap, 7), dtype=torch.float32, device="cuda")
+    y = torch.empty((cap, 5), dtype=torch.float32, device="cuda")
+    n = 0
+    for seed in (1, 2):
+        p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=seed, relative_humidity=1.03)
+        with gwm.Model(g, spec) as m:
+            m.upload(gwm.build_case("moist_sounding", g, p, moist=True))
+            for it in range(40):
+                m.step(1)
+                if it % 2 == 0 and n < cap:
+                    n += m.rain_samples(x[n:], y[n:], seed=100 * seed + it, p_active=0.5, p_inactive=0.01)
+    params, norm, rng, loss = gwm.mlp_train(x, y, n, epochs=20, batch=16384, lr=2e-3, seed=3)
+    p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=9, relative_humidity=1.03)
+    s0 = gwm.build_case("moist_sounding", g, p, moist=True)
+    res = {}
+    for mode in ("plain", "surrogate"):
+        with gwm.Model(g, spec) as m:
+            m.upload(s0)
+            b0 = m.budgets()
+            if mode == "surrogate":
+                m.set_rain_surrogate(params, norm, rng, tol_water=1e-3, tol_energy=0.05)
+            m.step(40)
+            b1 = m.budgets()
+            fb = m.surrogate_fallbacks() if mode == "surrogate" else 0
+        water0 = b0["vapor_water_path_sum_kg_m2"] + b0["cloud_water_path_sum_kg_m2"] + b0["rain_water_path_sum_kg_m2"]
+        water1 = b1["vapor_water_path_sum_kg_m2"] + b1["cloud_water_path_sum_kg_m2"] + b1["rain_water_path_sum_kg_m2"]
+        precip = b1["accumulated_surface_precipitation_sum_mm"]
+        res[mode] = dict(precip=precip, closure=abs(water1 + precip - water0) / water0, fallbacks=fb)
+    cells = 96 * 96 * 32 * 40
+    assert res["plain"]["precip"] > 0
+    assert abs(res["surrogate"]["precip"] - res["plain"]["precip"]) <= 0.05 * res["plain"]["precip"], res
+    assert res["surrogate"]["closure"] <= max(10 * res["plain"]["closure"], 1e-6), res
+    assert res["surrogate"]["fallbacks"] < 0.5 * cells, res
