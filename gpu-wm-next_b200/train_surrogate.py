@@ -1,0 +1,115 @@
+"""Train the learned warm-rain microphysics on cell samples of the plain scheme.
+
+Samples come from moist-sounding runs with the C3 physics (3 km spacing, 64 levels to
+16 km, warm rain with 12 m/s terminal velocity, 0.5 K rms theta noise) on a reduced
+horizontal grid, with seeds 1-8; the network is evaluated on seed 9 against the plain
+scheme (surface precipitation, total-water closure, fallback fraction).  Everything
+runs through the library: the recorder, the FP32 training kernels and the BF16
+tensor-core inference.
+
+Usage:
+    python gpu-wm-next_b200/train_surrogate.py --out gpu-wm-next_b200/surrogate_c3.npz
+"""
+import argparse
+import importlib
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+
+NZ, DX, ZTOP, DT, NS, VT = 64, 3000.0, 16000.0, 1.0, 6, 12.0
+
+
+def model_spec(gwm):
+    step = gwm.StepConfig(dt=DT, fast_substeps=NS)
+    rain = gwm.WarmRainConfig(dt=DT, rain_terminal_velocity=VT)
+    return gwm.MemberSpec(step=step, rain=rain, moist=True)
+
+
+def state(gwm, g, seed):
+    p = gwm.CaseParams(theta_ref=300.0, theta_lapse_k_per_m=0.004, relative_humidity=0.9, rh_top_m=2000.0,
+                       qv_scale_height_m=1500.0, qv_floor=1.0e-5, noise_rms_k=0.5, noise_depth_m=1000.0,
+                       seed=seed)
+    return gwm.build_case("moist_sounding", g, p, moist=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(HERE, "surrogate_c3.npz"))
+    ap.add_argument("--n", type=int, default=256, help="horizontal size of the sampling runs")
+    ap.add_argument("--samples", type=int, default=1 << 24)
+    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--batch", type=int, default=65536)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--spinup", type=int, default=60, help="steps before the first snapshot")
+    ap.add_argument("--snapshots", type=int, default=8)
+    ap.add_argument("--every", type=int, default=15)
+    ap.add_argument("--eval-steps", type=int, default=120)
+    args = ap.parse_args()
+    import torch
+    gwm = importlib.import_module("gpu-wm-next_b200")
+    g = gwm.GridSpec(args.n, args.n, NZ, dx=DX, dy=DX, z_top=ZTOP)
+    spec = model_spec(gwm)
+    cap = args.samples
+    x = torch.empty((cap, 7), dtype=torch.float32, device="cuda")
+    y = torch.empty((cap, 5), dtype=torch.float32, device="cuda")
+    per_snap = cap // (8 * args.snapshots)
+    cells = args.n * args.n * NZ
+    n = 0
+    t0 = time.time()
+    for seed in range(1, 9):
+        with gwm.Model(g, spec) as m:
+            m.upload(state(gwm, g, seed))
+            m.step(args.spinup)
+            for snap in range(args.snapshots):
+                if snap:
+                    m.step(args.every)
+                # keep about per_snap samples per snapshot, active cells preferred
+                got = m.rain_samples(x[n:], y[n:], seed=1000 * seed + snap, p_active=1.0, p_inactive=0.0)
+                pa = min(1.0, per_snap / max(got, 1))
+                n0 = n
+                n += m.rain_samples(x[n0:min(cap, n0 + per_snap)], y[n0:min(cap, n0 + per_snap)],
+                                    seed=1000 * seed + snap, p_active=pa,
+                                    p_inactive=min(1.0, 0.1 * per_snap / cells))
+    t_sample = time.time() - t0
+    t0 = time.time()
+    params, norm, rng, loss = gwm.mlp_train(x, y, n, epochs=args.epochs, batch=args.batch, lr=args.lr, seed=1)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    # evaluation on seed 9: plain scheme against the network
+    s9 = state(gwm, g, 9)
+    res = {}
+    for mode in ("plain", "surrogate"):
+        with gwm.Model(g, spec) as m:
+            m.upload(s9)
+            b0 = m.budgets()
+            if mode == "surrogate":
+                m.set_rain_surrogate(params, norm, rng)
+            m.step(args.eval_steps)
+            b1 = m.budgets()
+            fb = m.surrogate_fallbacks() if mode == "surrogate" else 0
+            out = m.download(keys=["precip"])
+        w0 = sum(b0[k] for k in ("vapor_water_path_sum_kg_m2", "cloud_water_path_sum_kg_m2", "rain_water_path_sum_kg_m2"))
+        w1 = sum(b1[k] for k in ("vapor_water_path_sum_kg_m2", "cloud_water_path_sum_kg_m2", "rain_water_path_sum_kg_m2"))
+        pr = b1["accumulated_surface_precipitation_sum_mm"]
+        res[mode] = {"precip_sum_mm": pr, "water_closure_rel": abs(w1 + pr - w0) / w0,
+                     "fallback_fraction": fb / (cells * args.eval_steps), "precip_field": out["precip"]}
+    rel = abs(res["surrogate"]["precip_sum_mm"] - res["plain"]["precip_sum_mm"]) / max(res["plain"]["precip_sum_mm"], 1e-30)
+    summary = {
+        "samples": n, "epochs": args.epochs, "loss_per_epoch": loss.tolist(),
+        "sampling_s": t_sample, "training_s": t_train, "grid": [args.n, args.n, NZ],
+        "eval_steps": args.eval_steps, "precip_rel_err": rel,
+        "plain": {k: v for k, v in res["plain"].items() if k != "precip_field"},
+        "surrogate": {k: v for k, v in res["surrogate"].items() if k != "precip_field"},
+    }
+    np.savez(args.out, params=params, norm=norm, range=rng, summary=json.dumps(summary))
+    print(json.dumps(summary), flush=True)
+
+
+if __name__ == "__main__":
+    main()

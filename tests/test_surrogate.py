@@ -64,7 +64,8 @@ def test_rain_samples_and_training(gwm):
         n = 0
         for it in range(6):
             m.step(3)
-            n += m.rain_samples(x[n:], y[n:], seed=it + 1, p_active=1.0, p_inactive=0.02)
+            if n < cap:
+                n += m.rain_samples(x[n:], y[n:], seed=it + 1, p_active=0.1, p_inactive=0.02)
     assert n > 10_000
     xs, ys = x[:n].cpu().numpy(), y[:n].cpu().numpy()
     assert np.isfinite(xs).all() and np.isfinite(ys).all()
