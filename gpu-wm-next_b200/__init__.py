@@ -167,6 +167,7 @@ def lib():
     L.gwm_b200_profile.argtypes = [vp, C.c_int]
     L.gwm_b200_set_tile.argtypes = [vp, C.c_int, C.c_int]
     L.gwm_b200_set_boundary_state.argtypes = [vp, C.c_int, C.POINTER(_Fields)]
+    L.gwm_b200_set_concurrent.argtypes = [vp, C.c_int]
     L.gwm_b200_apply_reference_boundaries.argtypes = [vp, C.c_int]
     L.gwm_b200_set_damping.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double),
                                        C.POINTER(C.c_double)]
@@ -205,7 +206,7 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_synchronize", "gwm_b200_use_graph", "gwm_b200_upload", "gwm_b200_download",
             "gwm_b200_step", "gwm_b200_advance_dry", "gwm_b200_advance_tracers",
             "gwm_b200_warm_rain", "gwm_b200_fast_modes", "gwm_b200_slow_tendencies",
-            "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_get_tile", "gwm_b200_set_boundary_state",
+            "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_get_tile", "gwm_b200_set_boundary_state", "gwm_b200_set_concurrent",
             "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_rain_record",
             "gwm_b200_mlp_train", "gwm_b200_mlp_loss_grad", "gwm_b200_set_rain_surrogate",
             "gwm_b200_surrogate_fallbacks", "gwm_b200_layout",
@@ -558,6 +559,10 @@ class Model:
                 best[kernel] = min(times, key=times.get)
             self.set_tile(kernel, best[kernel])
         return best
+
+    def set_concurrent(self, enable: bool = True):
+        """Members advance concurrently on their own streams (one graph branch each)."""
+        self._check(lib().gwm_b200_set_concurrent(self._h, int(enable)), "set_concurrent")
 
     def profile(self, enable: bool = True):
         """Per-kernel CUDA-event timing of subsequent direct (non-graph) launches."""

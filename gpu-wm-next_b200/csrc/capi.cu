@@ -116,6 +116,12 @@ struct gwm_b200_ctx {
   int tracer_tile_rows = 16;  // tracer stage: overlapped tiles of 8 or 16 rows
   long long launches = 0;
   long long cur_launches = 0;
+  // members advance on their own streams, forked from and joined back to `stream`
+  // (one graph with a branch per member when captured)
+  bool concurrent = true;
+  std::vector<cudaStream_t> mstreams;
+  std::vector<cudaEvent_t> mjoin;
+  cudaEvent_t mfork = nullptr;
 };
 
 namespace {
@@ -798,8 +804,18 @@ void gwm_b200_destroy(gwm_b200_ctx* c) {
     if (M.bstrip) cudaFree(M.bstrip);
     if (M.sur) cudaFree(M.sur);
   }
+  for (auto st : c->mstreams) cudaStreamDestroy(st);
+  for (auto ev : c->mjoin) cudaEventDestroy(ev);
+  if (c->mfork) cudaEventDestroy(c->mfork);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
+}
+
+int gwm_b200_set_concurrent(gwm_b200_ctx* c, int enable) {
+  if (!c) return GWM_B200_ERR_ARG;
+  c->concurrent = enable != 0;
+  drop_graph(c);
+  return GWM_B200_OK;
 }
 
 const char* gwm_b200_last_error(const gwm_b200_ctx* c) { return c ? c->err.c_str() : "null context"; }
@@ -1211,6 +1227,42 @@ int gwm_b200_download(gwm_b200_ctx* c, int member, gwm_b200_fields* h) {
   return GWM_B200_OK;
 }
 
+// One pass of `one` over all members: concurrently on per-member streams (fork/join
+// around the context stream) when there are several, else in order on the stream.
+static int enqueue_members(gwm_b200_ctx* c, int (*one)(gwm_b200_ctx*, Member&)) {
+  const size_t n = c->m.size();
+  if (n <= 1 || !c->concurrent || c->profile) {
+    for (auto& M : c->m) {
+      const int rc = one(c, M);
+      if (rc) return rc;
+    }
+    return GWM_B200_OK;
+  }
+  if (c->mstreams.size() != n) {
+    for (size_t i = c->mstreams.size(); i < n; ++i) {
+      cudaStream_t st;
+      cudaEvent_t ev;
+      CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      c->mstreams.push_back(st);
+      c->mjoin.push_back(ev);
+    }
+    if (!c->mfork) CK(cudaEventCreateWithFlags(&c->mfork, cudaEventDisableTiming));
+  }
+  cudaStream_t main = c->stream;
+  CK(cudaEventRecord(c->mfork, main));
+  int rc = GWM_B200_OK;
+  for (size_t i = 0; i < n && !rc; ++i) {
+    CK(cudaStreamWaitEvent(c->mstreams[i], c->mfork, 0));
+    c->stream = c->mstreams[i];
+    rc = one(c, c->m[i]);
+    c->stream = main;
+    CK(cudaEventRecord(c->mjoin[i], c->mstreams[i]));
+    CK(cudaStreamWaitEvent(main, c->mjoin[i], 0));
+  }
+  return rc;
+}
+
 static int run_steps(gwm_b200_ctx* c, int nsteps, int (*one)(gwm_b200_ctx*, Member&)) {
   c->cur_launches = 0;
   for (auto& M : c->m) {
@@ -1227,11 +1279,7 @@ static int run_steps(gwm_b200_ctx* c, int nsteps, int (*one)(gwm_b200_ctx*, Memb
       std::vector<int> rings;
       for (auto& M : c->m) rings.push_back(M.ring);
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      int rc = GWM_B200_OK;
-      for (auto& M : c->m) {
-        rc = one(c, M);
-        if (rc) break;
-      }
+      int rc = enqueue_members(c, one);
       cudaGraph_t graph = nullptr;
       cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
       if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
@@ -1247,11 +1295,10 @@ static int run_steps(gwm_b200_ctx* c, int nsteps, int (*one)(gwm_b200_ctx*, Memb
     for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->graph, c->stream));
     c->cur_launches += c->graph_launches * nsteps;
   } else {
-    for (int s = 0; s < nsteps; ++s)
-      for (auto& M : c->m) {
-        int rc = one(c, M);
-        if (rc) return rc;
-      }
+    for (int s = 0; s < nsteps; ++s) {
+      const int rc = enqueue_members(c, one);
+      if (rc) return rc;
+    }
   }
   c->launches = c->cur_launches;
   if (c->stream == c->own_stream || c->profile) {

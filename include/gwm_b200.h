@@ -214,6 +214,11 @@ int gwm_b200_budgets(gwm_b200_ctx* ctx, int member, gwm_b200_budget* out);
  * computes the same values.  gwm_b200_get_tile returns the current rows (or < 0). */
 int gwm_b200_set_tile(gwm_b200_ctx* ctx, int kernel, int rows);
 int gwm_b200_get_tile(const gwm_b200_ctx* ctx, int kernel);
+/* Members of a context advance concurrently (default 1): each on its own stream,
+ * forked from and joined back to the context stream, so a captured step is one graph
+ * with a branch per member; 0 runs them one after another on the context stream.
+ * Either way every member's result is the same bit for bit. */
+int gwm_b200_set_concurrent(gwm_b200_ctx* ctx, int enable);
 /* Kernel launches issued by the last step call (for accounting). */
 long long gwm_b200_launch_count(const gwm_b200_ctx* ctx);
 /* Per-kernel CUDA-event timing on the context's stream (no graph while enabled).

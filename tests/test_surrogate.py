@@ -51,11 +51,11 @@ def test_gpu_mlp_gradient_matches_oracle(gwm, orc):
 @pytest.mark.gpu
 def test_rain_samples_and_training(gwm):
     import torch
-    g = gwm.GridSpec(96, 96, 32, dx=2000.0, dy=2000.0, z_top=8000.0)
+    g = gwm.GridSpec(96, 96, 32, dx=2000.0, dy=2000.0, z_top=12000.0)  # c dt / dz = 0.9
     p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=2, relative_humidity=1.03)
     s = gwm.build_case("moist_sounding", g, p, moist=True)
-    step = gwm.StepConfig(dt=2.0, fast_substeps=4)
-    rain = gwm.WarmRainConfig(dt=2.0, rain_terminal_velocity=12.0)
+    step = gwm.StepConfig(dt=1.0, fast_substeps=4)
+    rain = gwm.WarmRainConfig(dt=1.0, rain_terminal_velocity=12.0)
     cap = 200_000
     x = torch.empty((cap, 7), dtype=torch.float32, device="cuda")
     y = torch.empty((cap, 5), dtype=torch.float32, device="cuda")
@@ -157,9 +157,9 @@ def test_trained_surrogate_against_plain_scheme(gwm):
     # plain scheme after the run, total water (vapour + cloud + rain + precipitation)
     # conserved as well as by the plain scheme, the fallback fraction reported
     import torch
-    g = gwm.GridSpec(96, 96, 32, dx=2000.0, dy=2000.0, z_top=8000.0)
-    step = gwm.StepConfig(dt=2.0, fast_substeps=4)
-    rain = gwm.WarmRainConfig(dt=2.0, rain_terminal_velocity=12.0)
+    g = gwm.GridSpec(96, 96, 32, dx=2000.0, dy=2000.0, z_top=12000.0)  # c dt / dz = 0.9
+    step = gwm.StepConfig(dt=1.0, fast_substeps=4)
+    rain = gwm.WarmRainConfig(dt=1.0, rain_terminal_velocity=12.0)
     spec = gwm.MemberSpec(step=step, rain=rain, moist=True)
     cap = 1_500_000
     x = torch.empty((cap, 7), dtype=torch.float32, device="cuda")
