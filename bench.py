@@ -202,6 +202,8 @@ def main():
                     help="acoustic-substep kernel (0 owned tile, 3 TMA-fed, 8/16 overlapped); implies --no-tune")
     ap.add_argument("--slow-tile", type=int, default=None,
                     help="slow-stage kernel (3 TMA-fed owned tile, 8/16 overlapped); implies --no-tune")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-member ensemble line")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-microphysics line")
     ap.add_argument("--tracer-tile", type=int, default=None,
                     help="tracer-stage kernel (3 TMA-fed owned tile, 8/16 overlapped); implies --no-tune")
     args = ap.parse_args()
@@ -285,7 +287,14 @@ def main():
     e2e = None
     if not args.no_e2e:
         e2e = end_to_end(gwm, model, g, stream, torch, max(2, min(args.steps, 5)), world, dist)
+    # learned warm-rain microphysics against the plain scheme on the same state
+    surrogate = None
+    if not args.no_surrogate:
+        surrogate = surrogate_line(gwm, model, stream, torch)
     model.close()
+    ensemble = None
+    if not args.no_ensemble:
+        ensemble = ensemble_line(gwm, torch, stream, dist, world)
 
     if rank == 0:
         peak, which = load_peaks()
@@ -312,6 +321,10 @@ def main():
         line["roofline"]["frac"] = roof["achieved"] / peak
         if e2e:
             line["e2e"] = e2e
+        if surrogate:
+            line["surrogate"] = surrogate
+        if ensemble:
+            line["ensemble"] = ensemble
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
@@ -366,6 +379,73 @@ def read_traffic(g, fast_tile):
     except (KeyError, ValueError):
         return None
     return per_cell * g.nx * g.ny * g.nz
+
+
+SURROGATE_WEIGHTS = os.path.join(ROOT, "gpu-wm-next_b200", "surrogate_c3.npz")
+
+
+def surrogate_line(gwm, model, stream, torch, steps=3):
+    """Warm-rain kernel time with the plain scheme and with the trained network (device
+    events around each launch, profiling mode), both continuing from the same state;
+    precipitation and fallbacks of the network run."""
+    if not os.path.exists(SURROGATE_WEIGHTS):
+        return {"unavailable": "no trained weights (gpu-wm-next_b200/train_surrogate.py writes them)"}
+    w = np.load(SURROGATE_WEIGHTS)
+    snap = model.download()
+    out = {}
+    for mode in ("plain", "surrogate"):
+        model.upload(snap)
+        if mode == "surrogate":
+            model.set_rain_surrogate(w["params"], w["norm"], w["range"])
+            model.surrogate_stats(reset=True)
+        with torch.cuda.stream(stream):
+            model.profile(True)
+            model.step(steps)
+            rep = model.profile_report()
+            model.profile(False)
+        b = model.budgets()
+        out[mode] = {"rain_kernel_ms": rep["k_warm_rain"]["avg_ms"],
+                     "precip_sum_mm": b["accumulated_surface_precipitation_sum_mm"]}
+        if mode == "surrogate":
+            st = model.surrogate_stats()
+            cells = model.grids[0].nx * model.grids[0].ny * model.grids[0].nz * steps
+            out[mode]["network_fraction"] = st["network_cells"] / cells
+            out[mode]["fallback_fraction"] = st["fallbacks"] / max(st["network_cells"], 1)
+            model.set_rain_surrogate(None)
+    p0, p1 = out["plain"]["precip_sum_mm"], out["surrogate"]["precip_sum_mm"]
+    return {"plain_rain_ms": out["plain"]["rain_kernel_ms"], "surrogate_rain_ms": out["surrogate"]["rain_kernel_ms"],
+            "speedup": out["plain"]["rain_kernel_ms"] / out["surrogate"]["rain_kernel_ms"],
+            "network_fraction": out["surrogate"]["network_fraction"],
+            "fallback_fraction_of_network_cells": out["surrogate"]["fallback_fraction"],
+            "precip_rel_diff": abs(p1 - p0) / max(abs(p0), 1e-30), "steps": steps,
+            "training": json.loads(str(w["summary"])),
+            "note": "BF16 mma.sync inference in the column sweep with per-cell plain fallback"}
+
+
+def ensemble_line(gwm, torch, stream, dist, world, n=64, steps=3, warmup=3):
+    """C5: 64 uneven members (nx, ny in [64, 512], nz in {40, 64, 80}; warm bubble, cold
+    block, Agnesi mountain wave, moist warm rain) advanced by one captured graph with a
+    branch per member; device-timed throughput in cell updates per second."""
+    ens = importlib.import_module("gpu-wm-next_b200.ensemble")
+    grids, specs, states, damping, kinds = ens.c5_members(n, seed=5)
+    cells = sum(g.nx * g.ny * g.nz for g in grids)
+    with ens.build_model(grids, specs, states, damping, concurrent=True) as m:
+        m.set_stream(stream.cuda_stream)
+        m.use_graph(True)
+        with torch.cuda.stream(stream):
+            m.step(warmup)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        m.step(steps)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(t0.elapsed_time(t1), torch, dist, "cuda")
+        finite = all(np.isfinite(v) for i in range(n) for v in m.budgets(member=i).values())
+    return {"members": n, "cells": cells, "steps": steps, "ms_per_step": ms / steps,
+            "value": job_throughput(cells, steps, world, ms), "unit": "cell-updates/s",
+            "cases": {k: kinds.count(k) for k in set(kinds)}, "state_finite": finite,
+            "note": "one CUDA graph per step with a branch per member; dt 1 s, 4 substeps"}
 
 
 def max_over_ranks(x, torch, dist, device):

@@ -179,6 +179,7 @@ def lib():
                                                                       C.POINTER(C.c_double)]
     L.gwm_b200_set_rain_surrogate.argtypes = [vp, C.c_int] + [C.POINTER(C.c_float)] * 3 + [C.c_float, C.c_float]
     L.gwm_b200_surrogate_fallbacks.argtypes = [vp, C.c_int, C.POINTER(C.c_longlong), C.c_int]
+    L.gwm_b200_surrogate_stats.argtypes = [vp, C.c_int, C.POINTER(C.c_longlong), C.c_int]
     L.gwm_b200_get_tile.argtypes = [vp, C.c_int]
     L.gwm_b200_profile_read.argtypes = [vp, C.c_int, C.POINTER(C.c_double),
                                         C.POINTER(C.c_longlong), C.POINTER(C.c_char_p)]
@@ -209,7 +210,7 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_get_tile", "gwm_b200_set_boundary_state", "gwm_b200_set_concurrent",
             "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_rain_record",
             "gwm_b200_mlp_train", "gwm_b200_mlp_loss_grad", "gwm_b200_set_rain_surrogate",
-            "gwm_b200_surrogate_fallbacks", "gwm_b200_layout",
+            "gwm_b200_surrogate_fallbacks", "gwm_b200_surrogate_stats", "gwm_b200_layout",
             "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_ranks_to_global",
             "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
 
@@ -423,10 +424,13 @@ class Model:
                                                C.byref(n)), "rain_samples")
         return int(n.value)
 
-    def set_rain_surrogate(self, params=None, norm=None, rng=None, tol_water: float = 1e-3,
+    def set_rain_surrogate(self, params=None, norm=None, rng=None, tol_water: float = 1e-2,
                            tol_energy: float = 0.05, member: int = 0):
-        """Warm rain with the trained network (BF16 tensor-core inference, plain-scheme
-        fallback per cell); ``params=None`` restores the plain scheme."""
+        """Warm rain with the trained network (BF16 tensor-core inference, process amounts
+        projected onto the plain scheme's bounds, plain-scheme fallback per cell when the
+        inputs leave the training range or the redundant dqv / dtheta outputs disagree by
+        more than ``tol_water`` x total water / ``tol_energy`` K); ``params=None``
+        restores the plain scheme."""
         if params is None:
             self._check(lib().gwm_b200_set_rain_surrogate(self._h, member, None, None, None, 0.0, 0.0),
                         "set_rain_surrogate")
@@ -442,6 +446,14 @@ class Model:
         self._check(lib().gwm_b200_surrogate_fallbacks(self._h, member, C.byref(n), int(reset)),
                     "surrogate_fallbacks")
         return int(n.value)
+
+    def surrogate_stats(self, reset: bool = False, member: int = 0) -> dict:
+        """Cumulative counters of the network warm rain: cells that fell back, cells the
+        network ran on, and per check the cells that failed it."""
+        st = (C.c_longlong * 6)()
+        self._check(lib().gwm_b200_surrogate_stats(self._h, member, st, int(reset)), "surrogate_stats")
+        keys = ("fallbacks", "network_cells", "out_of_range", "water", "energy", "negative_vapor")
+        return dict(zip(keys, (int(v) for v in st)))
 
     def apply_reference_boundaries(self, member: int = 0):
         """apply_reference_boundaries once on the current state."""

@@ -701,7 +701,7 @@ int enqueue_rain(gwm_b200_ctx* c, Member& M, int fallout) {
     sa.bias = (const float*)(M.sur + kSurFrags * 32 * sizeof(uint2));
     sa.norm = sa.bias + kSurBias;
     sa.range = sa.norm + kMlpNorm;
-    sa.fallbacks = (unsigned long long*)(M.sur + 65536);
+    sa.stats = (unsigned long long*)(M.sur + 65536);
     sa.tol_water = M.sur_tol_water;
     sa.tol_energy = M.sur_tol_energy;
     LAUNCH(launch_warm_rain_surrogate(a, sa, c->stream), "warm rain");
@@ -1109,7 +1109,8 @@ int gwm_b200_mlp_train(const float* x, const float* y, long long n, const gwm_b2
   for (int o = 0; o < kMlpOut; ++o) {
     norm[2 * kMlpIn + o] = (float)hs[4 * kMlpIn + o];
     const double sd = hs[4 * kMlpIn + kMlpOut + o];
-    norm[2 * kMlpIn + kMlpOut + o] = sd > 1e-30 ? (float)sd : 1.0f;
+    // a target that never varies gets scale 0: inference reproduces its mean exactly
+    norm[2 * kMlpIn + kMlpOut + o] = sd > 1e-30 ? (float)sd : 0.0f;
   }
   uint64_t rng = cfg->seed ? cfg->seed : 0x5EED5EEDull;
   if (cfg->init) {  // Xavier-uniform weights, zero biases
@@ -1179,19 +1180,28 @@ int gwm_b200_set_rain_surrogate(gwm_b200_ctx* c, int member, const float* params
   return GWM_B200_OK;
 }
 
-int gwm_b200_surrogate_fallbacks(gwm_b200_ctx* c, int member, long long* count, int reset) {
+int gwm_b200_surrogate_stats(gwm_b200_ctx* c, int member, long long* stats, int reset) {
   int rc = check_member(c, member);
   if (rc) return rc;
   Member& M = c->m[member];
-  if (!count) return GWM_B200_ERR_ARG;
-  *count = 0;
+  if (!stats) return GWM_B200_ERR_ARG;
+  std::fill(stats, stats + GWM_B200_SURROGATE_STATS, 0LL);
   if (!M.sur) return GWM_B200_OK;
-  unsigned long long h = 0;
-  CK(cudaMemcpyAsync(&h, M.sur + 65536, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  static_assert(GWM_B200_SURROGATE_STATS == kSurStats, "surrogate counters");
+  unsigned long long h[kSurStats] = {};
+  CK(cudaMemcpyAsync(h, M.sur + 65536, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   if (reset) CK(cudaMemsetAsync(M.sur + 65536, 0, sizeof(h), c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  *count = (long long)h;
+  for (int q = 0; q < kSurStats; ++q) stats[q] = (long long)h[q];
   return GWM_B200_OK;
+}
+
+int gwm_b200_surrogate_fallbacks(gwm_b200_ctx* c, int member, long long* count, int reset) {
+  if (!count) return GWM_B200_ERR_ARG;
+  long long st[GWM_B200_SURROGATE_STATS];
+  int rc = gwm_b200_surrogate_stats(c, member, st, reset);
+  *count = rc ? 0 : st[0];
+  return rc;
 }
 
 int gwm_b200_download(gwm_b200_ctx* c, int member, gwm_b200_fields* h) {

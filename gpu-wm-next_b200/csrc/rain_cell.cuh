@@ -53,19 +53,29 @@ __device__ __forceinline__ MicroCell micro_state(float rho_d, float rt, float rq
 
 // warm_rain_kernel body: warm_rain.cu:63-120 (saturation adjustment with latent heating,
 // autoconversion, rain evaporation, clip at zero).  Updates c.th, c.qv, c.qc, c.qr.
-__device__ __forceinline__ void micro_step(MicroCell& c, const MicroParams& m) {
+// Process amounts of one micro_step (mixing-ratio units): condensation (vapour -> cloud,
+// negative for cloud evaporation), autoconversion (cloud -> rain), rain evaporation
+// (rain -> vapour).
+struct MicroRates {
+  float cond, autoconv, rain_evap;
+};
+
+__device__ __forceinline__ void micro_step(MicroCell& c, const MicroParams& m, MicroRates* rates = nullptr) {
   float th = c.th, qv = c.qv, qc = c.qc, qr = c.qr;
   const float rho = c.rho, lh = c.lh;
   float qs = qsat(c.temp, c.p);
+  float r_cond = 0.0f, r_auto = 0.0f, r_evap = 0.0f;
   if (qv > qs) {
     const float cond = fminf((qv - qs) * fmaxf(m.relax, 0.0f), qv);
     qv -= cond;
     qc += cond;
+    r_cond = cond;
     if (m.latent && cond > 0.0f) th += lh * cond;
   } else if (qv < qs && qc > 0.0f) {
     const float ev = fminf((qs - qv) * fmaxf(m.relax, 0.0f), qc);
     qv += ev;
     qc -= ev;
+    r_cond = -ev;
     if (m.latent && ev > 0.0f) th -= lh * ev;
   }
   const float excess = fmaxf(qc - m.thr, 0.0f);
@@ -73,6 +83,7 @@ __device__ __forceinline__ void micro_step(MicroCell& c, const MicroParams& m) {
     const float conv = fminf(excess, m.dt * m.rate * excess);
     qc -= conv;
     qr += conv;
+    r_auto = conv;
   }
   const float p = eos_pressure(rho, rho * th);
   const float temp = th * powf(fmaxf(p / kP0, 1.0e-6f), kKappa);
@@ -81,8 +92,10 @@ __device__ __forceinline__ void micro_step(MicroCell& c, const MicroParams& m) {
     const float ev = fminf(qr, m.dt * m.evap * fminf(qs - qv, qr));
     qr -= ev;
     qv += ev;
+    r_evap = ev;
     if (m.latent && ev > 0.0f) th -= lh * ev;
   }
+  if (rates) *rates = MicroRates{r_cond, r_auto, r_evap};
   c.th = th;
   c.qv = fmaxf(qv, 0.0f);
   c.qc = fmaxf(qc, 0.0f);

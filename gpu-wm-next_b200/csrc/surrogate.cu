@@ -41,21 +41,10 @@ __global__ void k_rain_record(const RecordArgs a) {
     const float rho_d = r.rho[o];
     const MicroCell c0 = micro_state(rho_d, r.rt[o], r.qv[o], r.qc[o], r.qr[o]);
     MicroCell c1 = c0;
-    micro_step(c1, mp);
-    // fallout flux of the cell over the step (warm_rain.cu:122-191)
-    float flux = 0.0f;
-    const float old_a_rho = fmaxf(c1.rho * c1.qr, 0.0f);
-    if (r.fallout_mode == 1) {
-      const float idz = fmaxf(r.terrain ? r.idz_c[o] : r.idz_c[k], 1.0e-6f);
-      const float frac = fminf(fmaxf(r.vt * r.dt * idz, 0.0f), 1.0f);
-      flux = frac * (old_a_rho * (1.0f / idz));
-    } else if (r.fallout_mode == 2) {
-      const float dz = fmaxf(r.layer_depth, 1.0e-3f);
-      const float frac = fminf(fmaxf(r.vt * r.dt / dz, 0.0f), 1.0f);
-      flux = frac * (old_a_rho * dz);
-    }
-    const float t[kMlpOut] = {c1.qv - c0.qv, c1.qc - c0.qc, c1.qr - c0.qr, c1.th - c0.th, flux};
-    const bool active = t[0] != 0.0f || t[1] != 0.0f || t[2] != 0.0f || t[3] != 0.0f || flux > 0.0f;
+    MicroRates pr;
+    micro_step(c1, mp, &pr);
+    const float t[kMlpOut] = {pr.cond, pr.autoconv, pr.rain_evap, c1.th - c0.th, c1.qv - c0.qv};
+    const bool active = t[0] != 0.0f || t[1] != 0.0f || t[2] != 0.0f || t[3] != 0.0f || t[4] != 0.0f;
     const double u = (double)(mix64(a.seed ^ mix64((unsigned long long)q)) >> 11) * (1.0 / 9007199254740992.0);
     if (u >= (active ? a.p_active : a.p_inactive)) continue;
     const unsigned long long at = atomicAdd(a.count, 1ull);
@@ -178,7 +167,8 @@ __global__ void __launch_bounds__(kFbThreads) k_mlp_fwd_bwd(const MlpBatch bt, d
       float y = w[kOffB4 + o];
 #pragma unroll
       for (int f = 0; f < kMlpHid; ++f) y += w[kOffW4 + o * kMlpHid + f] * in[f];
-      const float t = (bt.y[src * kMlpOut + o] - nrm[2 * kMlpIn + o]) / nrm[2 * kMlpIn + kMlpOut + o];
+      const float sd = nrm[2 * kMlpIn + kMlpOut + o];  // 0: a constant target, normalised to 0
+      const float t = sd > 0.0f ? (bt.y[src * kMlpOut + o] - nrm[2 * kMlpIn + o]) / sd : 0.0f;
       const float e = y - t;
       l += (double)e * (double)e;
       d4[o] = 2.0f * e / ((float)n * (float)kMlpOut);

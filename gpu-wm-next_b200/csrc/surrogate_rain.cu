@@ -10,13 +10,19 @@
 // layout of one 16-column k-step), so activations never leave the registers.
 // GELU is the tanh form with the hardware tanh approximation.
 //
-// Per cell the network gives (dqv, dqc, dqr, dtheta, flux).  Water and energy closure
-// are enforced: qr' = qr - dqv - dqc, theta' = theta - L_v/(c_p pi) dqv (the plain
-// scheme's exact budget relations).  The cell falls back to the plain scheme when an
-// input lies outside the training range, when the network's dqr or dtheta disagree with
-// those relations by more than the tolerances, or when a mixing ratio would go negative.
-// The fallout flux is clipped to the rain the cell holds, and the column accumulation
-// (what leaves a cell enters the one below, the bottom flux is precipitation) is exact.
+// Per cell the network gives the process amounts (condensation c, negative for cloud
+// evaporation; autoconversion a; rain evaporation e) and, redundantly, dtheta and dqv.
+// The amounts are projected onto the bounds the plain scheme obeys (no condensation in
+// subsaturated air nor past saturation, no cloud evaporation past saturation or the cloud
+// water present, no autoconversion of cloud water below the threshold, no more rain
+// evaporated than there is), then applied: qv -= c - e, qc += c - a, qr += a - e,
+// theta += L_v/(c_p pi) (c - e); water and energy close by construction.  The cell takes
+// the plain scheme instead when an input lies outside the training range or when the
+// network's dqv or dtheta disagree with the projected amounts by more than the
+// tolerances.  Quiet cells (no condensate, not supersaturated), which the plain scheme
+// leaves unchanged, skip the network.  Fallout is the scheme's explicit flux in both
+// paths, and the column accumulation (what leaves a cell enters the one below, the
+// bottom flux is precipitation) is exact.
 #include <cstring>
 
 #include <cuda_bf16.h>
@@ -124,12 +130,12 @@ __global__ void __launch_bounds__(kRB) k_warm_rain_surrogate(const RainArgs a, c
   __shared__ float s_bias[kSurBias];
   __shared__ float s_norm[kMlpNorm + kMlpRange];
   __shared__ long long s_th[kMaxNz][kRB / 32];
-  __shared__ unsigned long long s_fb;
+  __shared__ unsigned long long s_st[kSurStats];
   for (int q = threadIdx.x; q < kSurFrags * 32; q += kRB) s_fr[q] = s.frags[q];
   for (int q = threadIdx.x; q < kSurBias; q += kRB) s_bias[q] = s.bias[q];
   for (int q = threadIdx.x; q < kMlpNorm; q += kRB) s_norm[q] = s.norm[q];
   for (int q = threadIdx.x; q < kMlpRange; q += kRB) s_norm[kMlpNorm + q] = s.range[q];
-  if (threadIdx.x == 0) s_fb = 0ull;
+  if (threadIdx.x < kSurStats) s_st[threadIdx.x] = 0ull;
   __syncthreads();
 
   const Geom& g = a.g;
@@ -147,13 +153,19 @@ __global__ void __launch_bounds__(kRB) k_warm_rain_surrogate(const RainArgs a, c
   const float* xmin = s_norm + kMlpNorm;
   const float* xmax = s_norm + kMlpNorm + kMlpIn;
   float incoming = 0.0f;
-  unsigned fallbacks = 0;
+  unsigned st[kSurStats] = {0u, 0u, 0u, 0u, 0u, 0u};
   for (int k = g.nz - 1; k >= 0; --k) {
     const int o = active ? gidx(g, gi, gj, k) : 0;
     const float rho_d = active ? __ldg(a.rho + o) : 1.0f;
     const float rt = active ? a.rt[o] : 300.0f;
     const float rqv = active ? a.qv[o] : 0.0f, rqc = active ? a.qc[o] : 0.0f, rqr = active ? a.qr[o] : 0.0f;
     MicroCell mc = micro_state(rho_d, rt, rqv, rqc, rqr);
+    // activity gate: with no cloud or rain water and no supersaturation the plain scheme
+    // leaves the cell exactly as it is (micro_step takes none of its branches), so the
+    // network is not consulted; a warp whose cells are all quiet skips the MMAs
+    const float qs = qsat(mc.temp, mc.p);
+    const bool quiet = mc.qc == 0.0f && mc.qr == 0.0f && !(mc.qv > qs);
+    const bool net = active && !quiet;
     float x[kMlpIn];
     rain_features(mc, rho_d, a.dt, x);
     bool in_range = true;
@@ -168,9 +180,11 @@ __global__ void __launch_bounds__(kRB) k_warm_rain_surrogate(const RainArgs a, c
 #pragma unroll
     for (int q = 0; q < 4; ++q) p[q] = pack_bf16(xn[2 * q], xn[2 * q + 1]);
     // the warp's two tiles: lanes 0-15 and 16-31
-    float y0[4], y1[4];
-    mlp_tile(s_fr, s_bias, p, gq, gq + 8, t, y0);
-    mlp_tile(s_fr, s_bias, p, 16 + gq, 24 + gq, t, y1);
+    float y0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, y1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (__any_sync(0xffffffffu, net)) {  // warp-uniform
+      mlp_tile(s_fr, s_bias, p, gq, gq + 8, t, y0);
+      mlp_tile(s_fr, s_bias, p, 16 + gq, 24 + gq, t, y1);
+    }
     // gather this lane's 5 outputs: row r of its tile sits in lanes 4 (r % 8) + o/2
     const int r = lane & 15;
     const int src = 4 * (r & 7);
@@ -188,15 +202,30 @@ __global__ void __launch_bounds__(kRB) k_warm_rain_surrogate(const RainArgs a, c
     float dq[kMlpOut];
 #pragma unroll
     for (int q = 0; q < kMlpOut; ++q) dq[q] = out[q] * ys[q] + ym[q];
-    // closure-checked network step, or the plain scheme (lanes past the domain edge
-    // take part in the warp's MMAs and reductions but store nothing)
-    const float lh = mc.lh;
-    const float qv1 = mc.qv + dq[0], qc1 = mc.qc + dq[1];
-    const float qr1 = mc.qr - dq[0] - dq[1];
+    // projected network step, or the plain scheme (lanes past the domain edge take part
+    // in the warp's MMAs and reductions but store nothing)
+    const float lat = a.latent ? mc.lh : 0.0f;
+    const float relax = fmaxf(a.relax, 0.0f);
+    const float c_hi = mc.qv > qs ? fminf((mc.qv - qs) * relax, mc.qv) : 0.0f;
+    const float c_lo = mc.qv < qs ? -fminf((qs - mc.qv) * relax, mc.qc) : 0.0f;
+    const float c_p = fminf(fmaxf(dq[0], c_lo), c_hi);
+    const float qc_mid = mc.qc + c_p;
+    const float a_p = fminf(fmaxf(dq[1], 0.0f), a.rate > 0.0f ? fmaxf(qc_mid - a.thr, 0.0f) : 0.0f);
+    const float qr_mid = mc.qr + a_p;
+    const float e_p = a.evap > 0.0f ? fminf(fmaxf(dq[2], 0.0f), qr_mid) : 0.0f;
     const float wt = mc.qv + mc.qc + mc.qr;
-    const bool water_ok = fabsf(dq[0] + dq[1] + dq[2]) <= s.tol_water * fmaxf(wt, 1.0e-6f);
-    const bool energy_ok = fabsf(dq[3] + lh * dq[0]) <= s.tol_energy;
-    const bool ok = in_range && water_ok && energy_ok && qv1 >= 0.0f && qc1 >= 0.0f && qr1 >= 0.0f;
+    const bool water_ok = fabsf(dq[4] - (e_p - c_p)) <= s.tol_water * fmaxf(wt, 1.0e-6f);
+    const bool energy_ok = fabsf(dq[3] - lat * (c_p - e_p)) <= s.tol_energy;
+    const float qv1 = mc.qv - c_p + e_p;
+    const bool ok = net && in_range && water_ok && energy_ok && qv1 >= 0.0f;
+    if (net) {
+      st[1] += 1u;
+      st[0] += ok ? 0u : 1u;
+      st[2] += in_range ? 0u : 1u;
+      st[3] += water_ok ? 0u : 1u;
+      st[4] += energy_ok ? 0u : 1u;
+      st[5] += qv1 >= 0.0f ? 0u : 1u;
+    }
     float dz = 1.0f, idz = 1.0f;
     if (a.fallout_mode == 1) {
       idz = fmaxf(a.terrain ? __ldg(a.idz_c + o) : __ldg(a.idz_c + k), 1.0e-6f);
@@ -204,29 +233,27 @@ __global__ void __launch_bounds__(kRB) k_warm_rain_surrogate(const RainArgs a, c
     } else if (a.fallout_mode == 2) {
       dz = fmaxf(a.layer_depth, 1.0e-3f);
     }
-    float th, qv, qc, rqr_new, flux;
+    float th, qv, qc, qr;
     const float rho = mc.rho;
     if (ok) {
-      th = mc.th - lh * dq[0];
+      th = mc.th + lat * (c_p - e_p);
       qv = qv1;
-      qc = qc1;
-      rqr_new = rho * qr1;
-      flux = fminf(fmaxf(dq[4], 0.0f), fmaxf(rqr_new, 0.0f) * dz);
+      qc = fmaxf(qc_mid - a_p, 0.0f);
+      qr = fmaxf(qr_mid - e_p, 0.0f);
     } else {
-      if (active) ++fallbacks;
       micro_step(mc, mp);
       th = mc.th;
       qv = mc.qv;
       qc = mc.qc;
-      rqr_new = rho * mc.qr;
-      flux = 0.0f;
-      if (a.fallout_mode == 1) {
-        const float frac = fminf(fmaxf(a.vt * a.dt * idz, 0.0f), 1.0f);
-        flux = frac * (fmaxf(rqr_new, 0.0f) * dz);
-      } else if (a.fallout_mode == 2) {
-        const float frac = fminf(fmaxf(a.vt * a.dt / dz, 0.0f), 1.0f);
-        flux = frac > 0.0f ? frac * (fmaxf(rqr_new, 0.0f) * dz) : 0.0f;
-      }
+      qr = mc.qr;
+    }
+    float rqr_new = rho * qr, flux = 0.0f;
+    if (a.fallout_mode == 1) {
+      const float frac = fminf(fmaxf(a.vt * a.dt * idz, 0.0f), 1.0f);
+      flux = frac * (fmaxf(rqr_new, 0.0f) * dz);
+    } else if (a.fallout_mode == 2) {
+      const float frac = fminf(fmaxf(a.vt * a.dt / dz, 0.0f), 1.0f);
+      flux = frac > 0.0f ? frac * (fmaxf(rqr_new, 0.0f) * dz) : 0.0f;
     }
     if (a.fallout_mode) {  // column accumulation: warm_rain.cu:122-191
       const float old_a = fmaxf(rqr_new, 0.0f) * dz;
@@ -253,10 +280,13 @@ __global__ void __launch_bounds__(kRB) k_warm_rain_surrogate(const RainArgs a, c
     a.precip_comp[q] += (fabs(sp) >= fabs(xp)) ? (sp - tp) + xp : (xp - tp) + sp;
     a.precip[q] = tp;
   }
-  const unsigned fw = __reduce_add_sync(0xffffffffu, fallbacks);
-  if (lane == 0 && fw) atomicAdd(&s_fb, (unsigned long long)fw);
+#pragma unroll
+  for (int q = 0; q < kSurStats; ++q) {
+    const unsigned w = __reduce_add_sync(0xffffffffu, st[q]);
+    if (lane == 0 && w) atomicAdd(&s_st[q], (unsigned long long)w);
+  }
   __syncthreads();
-  if (threadIdx.x == 0 && s_fb && s.fallbacks) atomicAdd(s.fallbacks, s_fb);
+  if (threadIdx.x < kSurStats && s_st[threadIdx.x] && s.stats) atomicAdd(s.stats + threadIdx.x, s_st[threadIdx.x]);
   if (a.th_acc) {
     for (int k = threadIdx.x; k < g.nz; k += kRB) {
       long long tt = 0;

@@ -22,8 +22,12 @@ struct SurrogateArgs {
   const float* range;            // kMlpRange: x min/max of the training data
   float tol_water;               // |dqv + dqc + dqr| <= tol_water * (qv + qc + qr)
   float tol_energy;              // |dtheta + L/(cp pi) dqv| <= tol_energy (K)
-  unsigned long long* fallbacks; // cells that took the plain scheme (accumulated)
+  // accumulated counters (kSurStats): cells that took the plain scheme after the network
+  // ran, cells the network ran on, and per check the cells that failed it (input range,
+  // water, energy, negative vapour; a cell can fail several)
+  unsigned long long* stats;
 };
+constexpr int kSurStats = 6;
 
 cudaError_t launch_warm_rain_surrogate(const RainArgs& a, const SurrogateArgs& s, cudaStream_t st);
 

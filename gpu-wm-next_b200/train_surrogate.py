@@ -92,13 +92,13 @@ def main():
                 m.set_rain_surrogate(params, norm, rng)
             m.step(args.eval_steps)
             b1 = m.budgets()
-            fb = m.surrogate_fallbacks() if mode == "surrogate" else 0
+            st = m.surrogate_stats() if mode == "surrogate" else {}
             out = m.download(keys=["precip"])
         w0 = sum(b0[k] for k in ("vapor_water_path_sum_kg_m2", "cloud_water_path_sum_kg_m2", "rain_water_path_sum_kg_m2"))
         w1 = sum(b1[k] for k in ("vapor_water_path_sum_kg_m2", "cloud_water_path_sum_kg_m2", "rain_water_path_sum_kg_m2"))
         pr = b1["accumulated_surface_precipitation_sum_mm"]
         res[mode] = {"precip_sum_mm": pr, "water_closure_rel": abs(w1 + pr - w0) / w0,
-                     "fallback_fraction": fb / (cells * args.eval_steps), "precip_field": out["precip"]}
+                     "surrogate_stats": st, "precip_field": out["precip"]}
     rel = abs(res["surrogate"]["precip_sum_mm"] - res["plain"]["precip_sum_mm"]) / max(res["plain"]["precip_sum_mm"], 1e-30)
     summary = {
         "samples": n, "epochs": args.epochs, "loss_per_epoch": loss.tolist(),

@@ -184,19 +184,29 @@ typedef struct {
 } gwm_b200_mlp_train_config;
 /* Trains the 7-64-64-64-5 GELU network on n device samples (x, y as above) with the
  * project's FP32 forward/backward kernels and Adam; params (host, 9157 floats) in/out,
- * norm (host, 24 floats) out: input mean/std, target mean/std; range (host, 14 floats,
+ * norm (host, 24 floats) out: input mean/std (std 1 for a constant input), target
+ * mean/std (std 0 for a constant target: it is reproduced exactly); range (host, 14 floats,
  * may be NULL) out: input min/max; loss_per_epoch (host, epochs) out: mean squared
  * error of the normalised targets. */
 int gwm_b200_mlp_train(const float* x, const float* y, long long n, const gwm_b200_mlp_train_config* cfg,
                        float* params, float* norm, float* range, double* loss_per_epoch);
 /* Warm rain of a member with the trained network (params 9157, norm 24, range 14
  * floats, host) instead of the plain per-cell microphysics; NULL params restores the
- * plain scheme.  Cells whose inputs leave the training range or whose outputs break
- * the water (|dqv+dqc+dqr| > tol_water (qv+qc+qr)) or energy (|dtheta + L/(cp pi) dqv|
- * > tol_energy K) relations, or would make a mixing ratio negative, take the plain
- * scheme; gwm_b200_surrogate_fallbacks reports how many (cumulative; reset != 0 clears). */
+ * plain scheme.  Quiet cells (no cloud or rain water, not supersaturated), which the
+ * plain scheme leaves unchanged, are left unchanged without the network.  The network's
+ * condensate changes are projected so that cloud and rain water stay non-negative with
+ * the water budget kept (qr' = qr - dqv - dqc, theta' = theta - L/(cp pi) dqv).  Cells
+ * whose inputs leave the training range or whose outputs break the water
+ * (|dqv+dqc+dqr| > tol_water (qv+qc+qr)) or energy (|dtheta + L/(cp pi) dqv| >
+ * tol_energy K) relations, or would make the vapour negative, take the plain scheme. */
 int gwm_b200_set_rain_surrogate(gwm_b200_ctx* ctx, int member, const float* params, const float* norm,
                                 const float* range, float tol_water, float tol_energy);
+/* Cumulative surrogate counters (reset != 0 clears them): stats[0] cells that fell back
+ * to the plain scheme, [1] cells the network ran on, [2..5] cells failing the input
+ * range, water, energy and vapour checks (a cell can fail several). */
+#define GWM_B200_SURROGATE_STATS 6
+int gwm_b200_surrogate_stats(gwm_b200_ctx* ctx, int member, long long* stats, int reset);
+/* stats[0] alone. */
 int gwm_b200_surrogate_fallbacks(gwm_b200_ctx* ctx, int member, long long* count, int reset);
 /* Loss and gradient of the network on n host samples (gradient check). */
 int gwm_b200_mlp_loss_grad(const float* params, const float* norm, const float* x, const float* y, int n,

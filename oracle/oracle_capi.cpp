@@ -443,7 +443,7 @@ int gwo_run_boundary(const gwo_grid* g, const gwo_step* st, const gwo_rain* rn, 
 }
 
 // MLP of the learned warm-rain surrogate, FP64: loss = mean over samples and the 5
-// outputs of (y_hat - (y - y_mean)/y_std)^2 with inputs (x - x_mean)/x_std, three
+// outputs of (y_hat - (y - y_mean)/y_std)^2 (0 for y_std = 0) with inputs (x - x_mean)/x_std, three
 // 64-wide hidden layers with GELU 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))).
 // params: W1 (64x7) b1 W2 (64x64) b2 W3 (64x64) b3 W4 (5x64) b4; grad has the same layout.
 int gwo_mlp_loss_grad(const double* params, const double* norm, const double* x, const double* y, int n,
@@ -479,7 +479,8 @@ int gwo_mlp_loss_grad(const double* params, const double* norm, const double* x,
       for (int o = 0; o < O; ++o) {
         double s = params[oB4 + o];
         for (int f = 0; f < H; ++f) s += params[oW4 + o * H + f] * a3[f];
-        const double t = (y[b * O + o] - norm[2 * I + o]) / norm[2 * I + O + o];
+        const double sd = norm[2 * I + O + o];  // 0: a constant target, normalised to 0
+        const double t = sd > 0.0 ? (y[b * O + o] - norm[2 * I + o]) / sd : 0.0;
         total += (s - t) * (s - t);
         d4[o] = 2.0 * (s - t) / ((double)n * O);
       }
