@@ -408,6 +408,7 @@ def surrogate_line(gwm, model, stream, torch, steps=3):
                      "precip_sum_mm": b["accumulated_surface_precipitation_sum_mm"]}
         if mode == "surrogate":
             st = model.surrogate_stats()
+            out[mode]["stats"] = st
             cells = model.grids[0].nx * model.grids[0].ny * model.grids[0].nz * steps
             out[mode]["network_fraction"] = st["network_cells"] / cells
             out[mode]["fallback_fraction"] = st["fallbacks"] / max(st["network_cells"], 1)
@@ -419,7 +420,9 @@ def surrogate_line(gwm, model, stream, torch, steps=3):
             "fallback_fraction_of_network_cells": out["surrogate"]["fallback_fraction"],
             "precip_rel_diff": abs(p1 - p0) / max(abs(p0), 1e-30), "steps": steps,
             "training": json.loads(str(w["summary"])),
-            "note": "BF16 mma.sync inference in the column sweep with per-cell plain fallback"}
+            "stats": out["surrogate"]["stats"],
+            "note": "BF16 mma.sync inference of process fractions in the column sweep, quiet cells gated, "
+                    "per-cell plain fallback"}
 
 
 def ensemble_line(gwm, torch, stream, dist, world, n=64, steps=3, warmup=3):

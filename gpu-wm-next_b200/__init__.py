@@ -424,13 +424,14 @@ class Model:
                                                C.byref(n)), "rain_samples")
         return int(n.value)
 
-    def set_rain_surrogate(self, params=None, norm=None, rng=None, tol_water: float = 1e-2,
-                           tol_energy: float = 0.05, member: int = 0):
-        """Warm rain with the trained network (BF16 tensor-core inference, process amounts
-        projected onto the plain scheme's bounds, plain-scheme fallback per cell when the
-        inputs leave the training range or the redundant dqv / dtheta outputs disagree by
-        more than ``tol_water`` x total water / ``tol_energy`` K); ``params=None``
-        restores the plain scheme."""
+    def set_rain_surrogate(self, params=None, norm=None, rng=None, tol_water: float = 0.1,
+                           tol_energy: float = 0.1, member: int = 0):
+        """Warm rain with the trained network (BF16 tensor-core inference of process
+        fractions, amounts bounded as in the plain scheme, plain-scheme fallback per cell
+        when the inputs leave the training range, a fraction leaves its interval by more
+        than ``tol_water``, or the redundant dqv / dtheta outputs disagree with the amounts
+        by more than ``tol_water`` / ``tol_energy`` of the exchange plus the output's
+        spread); ``params=None`` restores the plain scheme."""
         if params is None:
             self._check(lib().gwm_b200_set_rain_surrogate(self._h, member, None, None, None, 0.0, 0.0),
                         "set_rain_surrogate")
@@ -452,7 +453,7 @@ class Model:
         network ran on, and per check the cells that failed it."""
         st = (C.c_longlong * 6)()
         self._check(lib().gwm_b200_surrogate_stats(self._h, member, st, int(reset)), "surrogate_stats")
-        keys = ("fallbacks", "network_cells", "out_of_range", "water", "energy", "negative_vapor")
+        keys = ("fallbacks", "network_cells", "out_of_range", "fraction", "water", "energy")
         return dict(zip(keys, (int(v) for v in st)))
 
     def apply_reference_boundaries(self, member: int = 0):

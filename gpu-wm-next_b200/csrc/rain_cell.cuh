@@ -102,6 +102,24 @@ __device__ __forceinline__ void micro_step(MicroCell& c, const MicroParams& m, M
   c.qr = fmaxf(qr, 0.0f);
 }
 
+// The process amounts of one micro_step as fractions of what bounds them, the
+// surrogate's first three targets:
+//   f_cond:  |cond| / |qv - qs| (the relaxation efficiency; capped by qv or qc),
+//   f_auto:  autoconv / max(qc + cond - thr, 0),
+//   f_evap:  rain_evap / (qr + autoconv).
+// Where a bound is zero the fraction is the value the scheme's rate gives (relax,
+// min(1, dt rate), 0), so the targets stay smooth.
+__device__ __forceinline__ void rain_fractions(const MicroCell& c0, const MicroRates& r, const MicroParams& m,
+                                               float* f) {
+  const float d = c0.qv - qsat(c0.temp, c0.p);
+  const bool can = d > 0.0f || (d < 0.0f && c0.qc > 0.0f);
+  f[0] = can ? fabsf(r.cond) / fabsf(d) : fmaxf(m.relax, 0.0f);
+  const float excess = fmaxf(c0.qc + r.cond - m.thr, 0.0f);
+  f[1] = excess > 0.0f ? r.autoconv / excess : (m.rate > 0.0f ? fminf(m.dt * m.rate, 1.0f) : 0.0f);
+  const float qr_mid = c0.qr + r.autoconv;
+  f[2] = qr_mid > 0.0f ? r.rain_evap / qr_mid : 0.0f;
+}
+
 // Surrogate inputs of a cell: (T, p, rho_d, qv, qc, qr, dt).
 constexpr int kRainIn = 7, kRainOut = 5;
 __device__ __forceinline__ void rain_features(const MicroCell& c, float rho_d, float dt, float* x) {

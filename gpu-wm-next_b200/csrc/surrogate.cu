@@ -43,8 +43,11 @@ __global__ void k_rain_record(const RecordArgs a) {
     MicroCell c1 = c0;
     MicroRates pr;
     micro_step(c1, mp, &pr);
-    const float t[kMlpOut] = {pr.cond, pr.autoconv, pr.rain_evap, c1.th - c0.th, c1.qv - c0.qv};
-    const bool active = t[0] != 0.0f || t[1] != 0.0f || t[2] != 0.0f || t[3] != 0.0f || t[4] != 0.0f;
+    float t[kMlpOut];
+    rain_fractions(c0, pr, mp, t);
+    t[3] = c1.th - c0.th;
+    t[4] = c1.qv - c0.qv;
+    const bool active = pr.cond != 0.0f || pr.autoconv != 0.0f || pr.rain_evap != 0.0f || t[3] != 0.0f || t[4] != 0.0f;
     const double u = (double)(mix64(a.seed ^ mix64((unsigned long long)q)) >> 11) * (1.0 / 9007199254740992.0);
     if (u >= (active ? a.p_active : a.p_inactive)) continue;
     const unsigned long long at = atomicAdd(a.count, 1ull);

@@ -1,10 +1,12 @@
 // surrogate.cuh — the learned warm-rain microphysics: an MLP (T, p, rho_d, qv, qc, qr, dt)
-// -> (condensation, autoconversion, rain evaporation, dtheta, dqv) with three 64-wide
-// GELU hidden layers, trained on cell samples of the plain scheme by the kernels of
-// surrogate.cu and run with BF16 tensor-core inference inside the warm-rain column sweep.
-// The three process amounts move water between vapour, cloud and rain, so the water
-// budget closes by construction; dtheta and dqv are redundant outputs that the inference
-// checks against the latent heating and the vapour change the process amounts imply.
+// -> (f_cond, f_auto, f_evap, dtheta, dqv) with three 64-wide GELU hidden layers, trained
+// on cell samples of the plain scheme by the kernels of surrogate.cu and run with BF16
+// tensor-core inference inside the warm-rain column sweep.  The first three outputs are
+// the condensation, autoconversion and rain-evaporation amounts as fractions of what
+// bounds them (rain_fractions); the amounts move water between vapour, cloud and rain,
+// so the water budget closes by construction.  dtheta and dqv are redundant outputs
+// that the inference checks against the latent heating and the vapour change the
+// amounts imply.
 #pragma once
 
 #include "physics.cuh"
@@ -26,7 +28,7 @@ constexpr int kMlpNorm = 2 * kMlpIn + 2 * kMlpOut, kMlpRange = 2 * kMlpIn;
 struct RecordArgs {
   RainArgs r;                       // the state and the warm-rain configuration
   float* x;                         // (capacity, 7) features
-  float* y;                         // (capacity, 5) targets: cond, autoconv, rain_evap, dtheta, dqv
+  float* y;                         // (capacity, 5) targets: f_cond, f_auto, f_evap, dtheta, dqv
   unsigned long long* count;
   long long capacity;
   unsigned long long seed;

@@ -10,19 +10,20 @@
 // layout of one 16-column k-step), so activations never leave the registers.
 // GELU is the tanh form with the hardware tanh approximation.
 //
-// Per cell the network gives the process amounts (condensation c, negative for cloud
-// evaporation; autoconversion a; rain evaporation e) and, redundantly, dtheta and dqv.
-// The amounts are projected onto the bounds the plain scheme obeys (no condensation in
-// subsaturated air nor past saturation, no cloud evaporation past saturation or the cloud
-// water present, no autoconversion of cloud water below the threshold, no more rain
-// evaporated than there is), then applied: qv -= c - e, qc += c - a, qr += a - e,
+// Per cell the network gives the condensation, autoconversion and rain-evaporation
+// amounts as fractions of their bounds (the saturation deficit |qv - qs|, the cloud
+// water above the autoconversion threshold, the rain present) and, redundantly, dtheta
+// and dqv.  The fractions are held to their intervals widened by tol_water and turned
+// into amounts c (negative for cloud evaporation), a, e with the caps the plain scheme
+// applies (no more vapour condensed or cloud evaporated than there is), then applied: qv -= c - e, qc += c - a, qr += a - e,
 // theta += L_v/(c_p pi) (c - e); water and energy close by construction.  The cell takes
-// the plain scheme instead when an input lies outside the training range or when the
-// network's dqv or dtheta disagree with the projected amounts by more than the
-// tolerances.  Quiet cells (no condensate, not supersaturated), which the plain scheme
-// leaves unchanged, skip the network.  Fallout is the scheme's explicit flux in both
-// paths, and the column accumulation (what leaves a cell enters the one below, the
-// bottom flux is precipitation) is exact.
+// the plain scheme instead when an input lies outside the training range, when a raw
+// fraction lies outside its interval by more than tol_water, or when the network's dqv
+// or dtheta disagree with the amounts by more than tol_water or tol_energy of the
+// cell's exchange plus the output's training spread.  Quiet cells (no condensate, not
+// supersaturated), which the plain scheme leaves unchanged, skip the network.  Fallout
+// is the scheme's explicit flux in both paths, and the column accumulation (what leaves
+// a cell enters the one below, the bottom flux is precipitation) is exact.
 #include <cstring>
 
 #include <cuda_bf16.h>
@@ -202,29 +203,38 @@ __global__ void __launch_bounds__(kRB) k_warm_rain_surrogate(const RainArgs a, c
     float dq[kMlpOut];
 #pragma unroll
     for (int q = 0; q < kMlpOut; ++q) dq[q] = out[q] * ys[q] + ym[q];
-    // projected network step, or the plain scheme (lanes past the domain edge take part
-    // in the warp's MMAs and reductions but store nothing)
+    // network step from the fractions, or the plain scheme (lanes past the domain edge
+    // take part in the warp's MMAs and reductions but store nothing)
     const float lat = a.latent ? mc.lh : 0.0f;
-    const float relax = fmaxf(a.relax, 0.0f);
-    const float c_hi = mc.qv > qs ? fminf((mc.qv - qs) * relax, mc.qv) : 0.0f;
-    const float c_lo = mc.qv < qs ? -fminf((qs - mc.qv) * relax, mc.qc) : 0.0f;
-    const float c_p = fminf(fmaxf(dq[0], c_lo), c_hi);
+    // The fractions are used inside [-tol_water, hi + tol_water], not clipped to
+    // [0, hi]: the plain scheme's efficiency often sits on an end of its interval (full
+    // adjustment, no rain evaporation in saturated air), and clipping the network's
+    // noise there would bias the amounts.  Small reverse amounts stay bounded by the caps
+    // below, which keep every mixing ratio non-negative.
+    const float tw = s.tol_water, te = s.tol_energy;
+    const float fc_hi = fmaxf(fmaxf(a.relax, 0.0f), 1.0f);
+    const float fc = fminf(fmaxf(dq[0], -tw), fc_hi + tw);
+    const float fa = fminf(fmaxf(dq[1], 0.0f), 1.0f);
+    const float fe = fminf(fmaxf(dq[2], -tw), 1.0f);
+    const float d = mc.qv - qs;
+    const float c_p = (d > 0.0f || mc.qc > 0.0f) ? fminf(fmaxf(fc * d, -mc.qc), mc.qv) : 0.0f;
     const float qc_mid = mc.qc + c_p;
-    const float a_p = fminf(fmaxf(dq[1], 0.0f), a.rate > 0.0f ? fmaxf(qc_mid - a.thr, 0.0f) : 0.0f);
+    const float a_p = a.rate > 0.0f ? fa * fmaxf(qc_mid - a.thr, 0.0f) : 0.0f;
     const float qr_mid = mc.qr + a_p;
-    const float e_p = a.evap > 0.0f ? fminf(fmaxf(dq[2], 0.0f), qr_mid) : 0.0f;
-    const float wt = mc.qv + mc.qc + mc.qr;
-    const bool water_ok = fabsf(dq[4] - (e_p - c_p)) <= s.tol_water * fmaxf(wt, 1.0e-6f);
-    const bool energy_ok = fabsf(dq[3] - lat * (c_p - e_p)) <= s.tol_energy;
+    const float e_p = a.evap > 0.0f ? fe * qr_mid : 0.0f;
     const float qv1 = mc.qv - c_p + e_p;
-    const bool ok = net && in_range && water_ok && energy_ok && qv1 >= 0.0f;
+    const bool frac_ok = dq[0] >= -tw && dq[0] <= fc_hi + tw && dq[1] >= -tw && dq[1] <= 1.0f + tw &&
+                         dq[2] >= -tw && dq[2] <= 1.0f + tw && qv1 >= 0.0f;
+    const bool water_ok = fabsf(dq[4] - (e_p - c_p)) <= tw * (fabsf(c_p) + fabsf(e_p) + ys[4]);
+    const bool energy_ok = fabsf(dq[3] - lat * (c_p - e_p)) <= te * (lat * fabsf(c_p - e_p) + ys[3]);
+    const bool ok = net && in_range && frac_ok && water_ok && energy_ok;
     if (net) {
       st[1] += 1u;
       st[0] += ok ? 0u : 1u;
       st[2] += in_range ? 0u : 1u;
-      st[3] += water_ok ? 0u : 1u;
-      st[4] += energy_ok ? 0u : 1u;
-      st[5] += qv1 >= 0.0f ? 0u : 1u;
+      st[3] += frac_ok ? 0u : 1u;
+      st[4] += water_ok ? 0u : 1u;
+      st[5] += energy_ok ? 0u : 1u;
     }
     float dz = 1.0f, idz = 1.0f;
     if (a.fallout_mode == 1) {

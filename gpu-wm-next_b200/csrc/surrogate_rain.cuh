@@ -20,11 +20,11 @@ struct SurrogateArgs {
   const float* bias;             // kSurBias
   const float* norm;             // kMlpNorm: x mean/std, y mean/std
   const float* range;            // kMlpRange: x min/max of the training data
-  float tol_water;               // |dqv + dqc + dqr| <= tol_water * (qv + qc + qr)
-  float tol_energy;              // |dtheta + L/(cp pi) dqv| <= tol_energy (K)
+  float tol_water;               // fraction margin; |dqv_net - (e - c)| <= tol_water (|c| + |e| + dqv spread)
+  float tol_energy;              // |dtheta_net - L/(cp pi)(c - e)| <= tol_energy (L/(cp pi)|c - e| + dtheta spread)
   // accumulated counters (kSurStats): cells that took the plain scheme after the network
   // ran, cells the network ran on, and per check the cells that failed it (input range,
-  // water, energy, negative vapour; a cell can fail several)
+  // fraction range, water, energy; a cell can fail several)
   unsigned long long* stats;
 };
 constexpr int kSurStats = 6;

@@ -1,11 +1,19 @@
 """Train the learned warm-rain microphysics on cell samples of the plain scheme.
 
-Samples come from moist-sounding runs with the C3 physics (3 km spacing, 64 levels to
-16 km, warm rain with 12 m/s terminal velocity, 0.5 K rms theta noise) on a reduced
+Samples come from moist-sounding runs with the moist warm-rain physics (3 km spacing,
+64 levels to 16 km, warm rain with 12 m/s terminal velocity, theta 300 K rising 4 K/km
+above 1 km, 90 % RH below 2 km, 0.5 K rms theta noise in the lowest km) on a reduced
 horizontal grid, with seeds 1-8; the network is evaluated on seed 9 against the plain
 scheme (surface precipitation, total-water closure, fallback fraction).  Everything
 runs through the library: the recorder, the FP32 training kernels and the BF16
 tensor-core inference.
+
+Snapshots are taken every 15 steps (an odd interval: the plain scheme's one-pass
+saturation adjustment alternates between condensing and evaporating steps, and both
+phases must be sampled) over the first 300 s.  Rain reaches the ground within that
+window; later, the inviscid scheme grows a grid-scale surface density mode under
+low-level convergence in this sounding (the FP64 restatement diverges at the same
+step), so samples and evaluation stay before it.
 
 Usage:
     python gpu-wm-next_b200/train_surrogate.py --out gpu-wm-next_b200/surrogate_c3.npz
@@ -43,13 +51,13 @@ def main():
     ap.add_argument("--out", default=os.path.join(HERE, "surrogate_c3.npz"))
     ap.add_argument("--n", type=int, default=256, help="horizontal size of the sampling runs")
     ap.add_argument("--samples", type=int, default=1 << 24)
-    ap.add_argument("--epochs", type=int, default=12)
-    ap.add_argument("--batch", type=int, default=65536)
+    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--batch", type=int, default=16384)
     ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--spinup", type=int, default=60, help="steps before the first snapshot")
-    ap.add_argument("--snapshots", type=int, default=8)
+    ap.add_argument("--spinup", type=int, default=30, help="steps before the first snapshot")
+    ap.add_argument("--snapshots", type=int, default=18)
     ap.add_argument("--every", type=int, default=15)
-    ap.add_argument("--eval-steps", type=int, default=120)
+    ap.add_argument("--eval-steps", type=int, default=300)
     args = ap.parse_args()
     import torch
     gwm = importlib.import_module("gpu-wm-next_b200")

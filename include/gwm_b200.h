@@ -192,18 +192,21 @@ int gwm_b200_mlp_train(const float* x, const float* y, long long n, const gwm_b2
                        float* params, float* norm, float* range, double* loss_per_epoch);
 /* Warm rain of a member with the trained network (params 9157, norm 24, range 14
  * floats, host) instead of the plain per-cell microphysics; NULL params restores the
- * plain scheme.  Quiet cells (no cloud or rain water, not supersaturated), which the
- * plain scheme leaves unchanged, are left unchanged without the network.  The network's
- * condensate changes are projected so that cloud and rain water stay non-negative with
- * the water budget kept (qr' = qr - dqv - dqc, theta' = theta - L/(cp pi) dqv).  Cells
- * whose inputs leave the training range or whose outputs break the water
- * (|dqv+dqc+dqr| > tol_water (qv+qc+qr)) or energy (|dtheta + L/(cp pi) dqv| >
- * tol_energy K) relations, or would make the vapour negative, take the plain scheme. */
+ * plain scheme.  The network gives condensation, autoconversion and rain evaporation as
+ * fractions of their bounds (saturation deficit, cloud water above the threshold, rain
+ * present) plus dtheta and dqv; the amounts move water between vapour, cloud and rain,
+ * so water and energy close by construction (qv -= c - e, qc += c - a, qr += a - e,
+ * theta += L/(cp pi)(c - e)).  Quiet cells (no cloud or rain water, not supersaturated),
+ * which the plain scheme leaves unchanged, are left unchanged without the network.  A
+ * cell takes the plain scheme when its inputs leave the training range, a raw fraction
+ * leaves its interval by more than tol_water, |dqv_net - (e - c)| > tol_water (|c| + |e|
+ * + dqv spread) or |dtheta_net - L/(cp pi)(c - e)| > tol_energy (L/(cp pi)|c - e| +
+ * dtheta spread), the spreads being the training targets' standard deviations. */
 int gwm_b200_set_rain_surrogate(gwm_b200_ctx* ctx, int member, const float* params, const float* norm,
                                 const float* range, float tol_water, float tol_energy);
 /* Cumulative surrogate counters (reset != 0 clears them): stats[0] cells that fell back
  * to the plain scheme, [1] cells the network ran on, [2..5] cells failing the input
- * range, water, energy and vapour checks (a cell can fail several). */
+ * range, fraction range, water and energy checks (a cell can fail several). */
 #define GWM_B200_SURROGATE_STATS 6
 int gwm_b200_surrogate_stats(gwm_b200_ctx* ctx, int member, long long* stats, int reset);
 /* stats[0] alone. */
