@@ -153,7 +153,7 @@ int gwm_b200_slow_tendencies(gwm_b200_ctx* ctx, int member, gwm_b200_fields* hos
  * optional, used when the member is moist).  While set, every step applies
  * apply_reference_boundaries (src/dycore/boundary_conditions.cpp:111-208) on the open
  * sides at the reference's BoundaryUpdater points: the dry stage starts
- * (dry_core.cu:568, 591, 620) and the tracer stage inputs (dry_transport.cu:484-517),
+ * (dry_core.cu:568, 591, 620) and the tracer stage inputs (dry_transport.cu:259-276, called at 489-508),
  * leaving the SSPRK3 blend partner q0 as it was before the first application.  The
  * strips are kept on the device (perimeter x nz floats per field); aliased periodic
  * faces of the boundary state are averaged as on upload.  NULL removes it (the Null
@@ -171,8 +171,11 @@ int gwm_b200_apply_reference_boundaries(gwm_b200_ctx* ctx, int member);
 /* ---- learned warm-rain microphysics (training side) ----
  * Cell samples of the plain scheme at the member's current state (no state change):
  * x (capacity x 7, device) = (T, p, rho_d, qv, qc, qr, dt), y (capacity x 5, device) =
- * (dqv, dqc, dqr, dtheta, fallout flux out of the cell over the step, kg m-2).  Cells
- * with a non-zero tendency are kept with probability p_active, the others with
+ * (f_cond, f_auto, f_evap, dtheta, dqv): condensation as a fraction of the saturation
+ * deficit |qv - qs|, autoconversion as a fraction of the cloud water above the
+ * threshold, rain evaporation as a fraction of the rain present (each the scheme's
+ * nominal value where its bound is zero), and the step's theta and vapour changes.
+ * Cells with a non-zero tendency are kept with probability p_active, the others with
  * p_inactive (seeded hash of the cell index); *n_out = samples written. */
 int gwm_b200_rain_record(gwm_b200_ctx* ctx, int member, float* x, float* y, long long capacity,
                          unsigned long long seed, float p_active, float p_inactive, long long* n_out);
