@@ -384,7 +384,7 @@ def read_traffic(g, fast_tile):
 SURROGATE_WEIGHTS = os.path.join(ROOT, "gpu-wm-next_b200", "surrogate_c3.npz")
 
 
-def surrogate_line(gwm, model, stream, torch, steps=3):
+def surrogate_line(gwm, model, stream, torch, steps=10):
     """Warm-rain kernel time with the plain scheme and with the trained network (device
     events around each launch, profiling mode), both continuing from the same state;
     precipitation and fallbacks of the network run."""
@@ -421,8 +421,8 @@ def surrogate_line(gwm, model, stream, torch, steps=3):
             "precip_rel_diff": abs(p1 - p0) / max(abs(p0), 1e-30), "steps": steps,
             "training": json.loads(str(w["summary"])),
             "stats": out["surrogate"]["stats"],
-            "note": "BF16 mma.sync inference of process fractions in the column sweep, quiet cells gated, "
-                    "per-cell plain fallback"}
+            "note": "two kernels: BF16 mma.sync inference of process fractions on the active cells packed "
+                    "into dense tiles (quiet cells gated), per-cell plain fallback; then the plain fallout sweep"}
 
 
 def ensemble_line(gwm, torch, stream, dist, world, n=64, steps=3, warmup=3):

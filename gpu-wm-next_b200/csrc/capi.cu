@@ -702,6 +702,7 @@ int enqueue_rain(gwm_b200_ctx* c, Member& M, int fallout) {
     sa.norm = sa.bias + kSurBias;
     sa.range = sa.norm + kMlpNorm;
     sa.stats = (unsigned long long*)(M.sur + 65536);
+    sa.work = (int*)(M.sur + 65536 + 128);
     sa.tol_water = M.sur_tol_water;
     sa.tol_energy = M.sur_tol_energy;
     LAUNCH(launch_warm_rain_surrogate(a, sa, c->stream), "warm rain");

@@ -111,6 +111,10 @@ __global__ void __launch_bounds__(BX * TBY) k_tracer_stage(const TracerArgs a) {
 
 constexpr int RB = 128;  // columns per warm-rain block (one row segment)
 
+// MICRO = false: fallout only, on a state whose microphysics was already applied
+// (the surrogate's network kernel); the reference applies each cell's microphysics
+// before the rain from above arrives, so the split is exact.
+template <bool MICRO>
 __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
   const Geom& g = a.g;
   const int gi = blockIdx.x * RB + threadIdx.x;
@@ -123,25 +127,32 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
   float incoming = 0.0f;
   // one-cell-ahead prefetch down the column
   float n_rho = 0.f, n_rt = 0.f, n_qv = 0.f, n_qc = 0.f, n_qr = 0.f;
+  const bool need_rt = MICRO || a.th_acc;
   if (active) {
     const int o = gidx(g, gi, gj, g.nz - 1);
-    n_rho = __ldg(a.rho + o); n_rt = a.rt[o]; n_qv = a.qv[o]; n_qc = a.qc[o]; n_qr = a.qr[o];
+    n_rho = __ldg(a.rho + o); n_qr = a.qr[o];
+    if (need_rt) n_rt = a.rt[o];
+    if (MICRO) { n_qv = a.qv[o]; n_qc = a.qc[o]; }
   }
   for (int k = g.nz - 1; k >= 0; --k) {
     FxAcc th_sum;
     const float c_rho = n_rho, c_rt = n_rt, c_qv = n_qv, c_qc = n_qc, c_qr = n_qr;
     if (active && k > 0) {
       const int o1 = gidx(g, gi, gj, k - 1);
-      n_rho = __ldg(a.rho + o1); n_rt = a.rt[o1]; n_qv = a.qv[o1]; n_qc = a.qc[o1]; n_qr = a.qr[o1];
+      n_rho = __ldg(a.rho + o1); n_qr = a.qr[o1];
+      if (need_rt) n_rt = a.rt[o1];
+      if (MICRO) { n_qv = a.qv[o1]; n_qc = a.qc[o1]; }
     }
     if (active) {
       const int o = gidx(g, gi, gj, k);
-      // warm_rain_kernel: warm_rain.cu:36-120
       const float rho_d = c_rho;
-      MicroCell mc = micro_state(rho_d, c_rt, c_qv, c_qc, c_qr);
-      micro_step(mc, MicroParams{a.dt, a.relax, a.thr, a.rate, a.evap, a.latent});
-      const float rho = mc.rho, th = mc.th, qv = mc.qv, qc = mc.qc;
-      float rqr = rho * mc.qr;
+      float rho = 0.0f, th = 0.0f, qv = 0.0f, qc = 0.0f, rqr = c_qr;
+      if (MICRO) {  // warm_rain_kernel: warm_rain.cu:36-120
+        MicroCell mc = micro_state(rho_d, c_rt, c_qv, c_qc, c_qr);
+        micro_step(mc, MicroParams{a.dt, a.relax, a.thr, a.rate, a.evap, a.latent});
+        rho = mc.rho; th = mc.th; qv = mc.qv; qc = mc.qc;
+        rqr = rho * mc.qr;
+      }
       // fallout of this cell, fed by the cell above
       if (a.fallout_mode == 1) {  // rain_fallout_metric_kernel: warm_rain.cu:156-191
         const float idz = fmaxf(a.terrain ? __ldg(a.idz_c + o) : __ldg(a.idz_c + k), 1.0e-6f);
@@ -161,12 +172,14 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
           incoming = out;
         }
       }
-      const float rt_new = rho * th;
-      store_tile(a.qv, g, kCell, gi, gj, k, rho * qv, edge);
-      store_tile(a.qc, g, kCell, gi, gj, k, rho * qc, edge);
-      store_tile(a.qr, g, kCell, gi, gj, k, rqr, edge);
-      store_tile(a.rt, g, kCell, gi, gj, k, rt_new, edge);
-      th_sum.add(theta_of(rho_d, rt_new), kFxTheta);
+      const float rt_new = MICRO ? rho * th : c_rt;
+      if (MICRO) {
+        store_tile(a.qv, g, kCell, gi, gj, k, rho * qv, edge);
+        store_tile(a.qc, g, kCell, gi, gj, k, rho * qc, edge);
+        store_tile(a.rt, g, kCell, gi, gj, k, rt_new, edge);
+      }
+      if (MICRO || a.fallout_mode) store_tile(a.qr, g, kCell, gi, gj, k, rqr, edge);
+      if (a.th_acc) th_sum.add(theta_of(rho_d, rt_new), kFxTheta);
     }
     if (a.th_acc) {
       const long long t = th_sum.warp_total();
@@ -202,10 +215,11 @@ cudaError_t launch_tracer_stage(const TracerArgs& a, cudaStream_t s, int tile_ro
   return cudaGetLastError();
 }
 
-cudaError_t launch_warm_rain(const RainArgs& a, cudaStream_t s) {
+cudaError_t launch_warm_rain(const RainArgs& a, cudaStream_t s, bool micro) {
   if (a.g.nz > kMaxNz) return cudaErrorInvalidValue;
   const dim3 grid((a.g.nx + RB - 1) / RB, a.g.ny);
-  k_warm_rain<<<grid, RB, 0, s>>>(a);
+  if (micro) k_warm_rain<true><<<grid, RB, 0, s>>>(a);
+  else if (a.fallout_mode || a.th_acc) k_warm_rain<false><<<grid, RB, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -52,6 +52,8 @@ cudaError_t launch_tracer_stage(const TracerArgs& a, cudaStream_t s, int tile_ro
 // Flat-terrain tracer stage on owned 32 x 16 tiles fed by TMA.
 cudaError_t launch_tracer_tma(const TracerArgs& a, const TracerMaps& m, cudaStream_t s);
 cudaError_t init_tracer_tma();
-cudaError_t launch_warm_rain(const RainArgs& a, cudaStream_t s);
+// micro = false: fallout (and theta level sums) only, on a state whose microphysics
+// was already applied.
+cudaError_t launch_warm_rain(const RainArgs& a, cudaStream_t s, bool micro = true);
 
 }  // namespace gwmb

@@ -1,8 +1,8 @@
 // surrogate.cu — training side of the learned warm-rain microphysics.
 //
-//  * k_rain_record: cell samples of the plain scheme (warm_rain.cu:36-191 through
+//  * k_rain_record_*: cell samples of the plain scheme (warm_rain.cu:36-120 through
 //    rain_cell.cuh): features (T, p, rho_d, qv, qc, qr, dt) of a state and the targets
-//    (dqv, dqc, dqr, dtheta, fallout flux out of the cell over the step).
+//    (the three process fractions, dtheta, dqv), written in cell order.
 //  * mlp_loss_grad: mean squared error of the normalised targets and its exact gradient,
 //    deterministic: one thread per sample for the forward and backward sweeps, then the
 //    weight gradients as tiled products over fixed chunks of samples reduced in a
@@ -27,37 +27,106 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {  // 
   return z ^ (z >> 31);
 }
 
-__global__ void k_rain_record(const RecordArgs a) {
+// Samples are written in cell order, whatever the thread schedule: pass 1 counts the
+// kept cells of each block's contiguous cell range, a single thread turns the counts
+// into offsets, and pass 2 writes each block's kept cells at its offset in order (a
+// block-wide scan per 256 cells).  The training data, and so the trained network, are
+// therefore reproducible run to run.
+constexpr int kRecThreads = 256, kRecIters = 16, kRecCells = kRecThreads * kRecIters;
+
+// The sample of cell q (global C order); returns whether it is kept.
+__device__ __forceinline__ bool record_cell(const RecordArgs& a, long long q, float* x, float* t) {
   const RainArgs& r = a.r;
   const Geom& g = r.g;
-  const long long n = (long long)g.nx * g.ny * g.nz;
   const MicroParams mp{r.dt, r.relax, r.thr, r.rate, r.evap, r.latent};
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
-       q += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(q % g.nx);
-    const long long rest = q / g.nx;
-    const int j = (int)(rest % g.ny), k = (int)(rest / g.ny);
-    const int o = gidx(g, i, j, k);
-    const float rho_d = r.rho[o];
-    const MicroCell c0 = micro_state(rho_d, r.rt[o], r.qv[o], r.qc[o], r.qr[o]);
-    MicroCell c1 = c0;
-    MicroRates pr;
-    micro_step(c1, mp, &pr);
-    float t[kMlpOut];
-    rain_fractions(c0, pr, mp, t);
-    t[3] = c1.th - c0.th;
-    t[4] = c1.qv - c0.qv;
-    const bool active = pr.cond != 0.0f || pr.autoconv != 0.0f || pr.rain_evap != 0.0f || t[3] != 0.0f || t[4] != 0.0f;
-    const double u = (double)(mix64(a.seed ^ mix64((unsigned long long)q)) >> 11) * (1.0 / 9007199254740992.0);
-    if (u >= (active ? a.p_active : a.p_inactive)) continue;
-    const unsigned long long at = atomicAdd(a.count, 1ull);
-    if ((long long)at >= a.capacity) continue;
-    float x[kMlpIn];
-    rain_features(c0, rho_d, r.dt, x);
+  const int i = (int)(q % g.nx);
+  const long long rest = q / g.nx;
+  const int j = (int)(rest % g.ny), k = (int)(rest / g.ny);
+  const int o = gidx(g, i, j, k);
+  const float rho_d = r.rho[o];
+  const MicroCell c0 = micro_state(rho_d, r.rt[o], r.qv[o], r.qc[o], r.qr[o]);
+  MicroCell c1 = c0;
+  MicroRates pr;
+  micro_step(c1, mp, &pr);
+  rain_fractions(c0, pr, mp, t);
+  t[3] = c1.th - c0.th;
+  t[4] = c1.qv - c0.qv;
+  const bool active = pr.cond != 0.0f || pr.autoconv != 0.0f || pr.rain_evap != 0.0f || t[3] != 0.0f || t[4] != 0.0f;
+  const double u = (double)(mix64(a.seed ^ mix64((unsigned long long)q)) >> 11) * (1.0 / 9007199254740992.0);
+  rain_features(c0, rho_d, r.dt, x);
+  return u < (active ? a.p_active : a.p_inactive);
+}
+
+__global__ void __launch_bounds__(kRecThreads) k_rain_record_count(const RecordArgs a, long long n,
+                                                                   unsigned* __restrict__ counts) {
+  const long long q0 = (long long)blockIdx.x * kRecCells;
+  unsigned c = 0;
+  for (int it = 0; it < kRecIters; ++it) {
+    const long long q = q0 + (long long)it * kRecThreads + threadIdx.x;
+    float x[kMlpIn], t[kMlpOut];
+    const bool keep = q < n && record_cell(a, q, x, t);
+    c += (unsigned)__syncthreads_count(keep);
+  }
+  if (threadIdx.x == 0) counts[blockIdx.x] = c;
+}
+
+// Exclusive scan of the block counts (one block of 1024 threads, each over a
+// contiguous segment); *total = all kept samples.
+__global__ void __launch_bounds__(1024) k_rain_record_scan(const unsigned* __restrict__ counts, int nb,
+                                                           unsigned long long* __restrict__ offsets,
+                                                           unsigned long long* total) {
+  __shared__ unsigned long long s[1024];
+  const int per = (nb + 1023) / 1024;
+  const int b0 = min(nb, (int)threadIdx.x * per), b1 = min(nb, b0 + per);
+  unsigned long long sum = 0;
+  for (int b = b0; b < b1; ++b) sum += counts[b];
+  s[threadIdx.x] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long run = 0;
+    for (int q = 0; q < 1024; ++q) {
+      const unsigned long long v = s[q];
+      s[q] = run;
+      run += v;
+    }
+    *total = run;
+  }
+  __syncthreads();
+  unsigned long long run = s[threadIdx.x];
+  for (int b = b0; b < b1; ++b) {
+    offsets[b] = run;
+    run += counts[b];
+  }
+}
+
+__global__ void __launch_bounds__(kRecThreads) k_rain_record_write(const RecordArgs a, long long n,
+                                                                   const unsigned long long* __restrict__ offsets) {
+  __shared__ unsigned s_w[kRecThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long q0 = (long long)blockIdx.x * kRecCells;
+  unsigned long long base = offsets[blockIdx.x];
+  for (int it = 0; it < kRecIters; ++it) {
+    const long long q = q0 + (long long)it * kRecThreads + threadIdx.x;
+    float x[kMlpIn], t[kMlpOut];
+    const bool keep = q < n && record_cell(a, q, x, t);
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) s_w[wid] = __popc(m);
+    __syncthreads();
+    unsigned before = __popc(m & ((1u << lane) - 1u)), all = 0;
+    for (int w = 0; w < kRecThreads / 32; ++w) {
+      const unsigned c = s_w[w];
+      before += w < wid ? c : 0u;
+      all += c;
+    }
+    const unsigned long long at = base + before;
+    if (keep && (long long)at < a.capacity) {
 #pragma unroll
-    for (int f = 0; f < kMlpIn; ++f) a.x[at * kMlpIn + f] = x[f];
+      for (int f = 0; f < kMlpIn; ++f) a.x[at * kMlpIn + f] = x[f];
 #pragma unroll
-    for (int f = 0; f < kMlpOut; ++f) a.y[at * kMlpOut + f] = t[f];
+      for (int f = 0; f < kMlpOut; ++f) a.y[at * kMlpOut + f] = t[f];
+    }
+    base += all;
+    __syncthreads();
   }
 }
 
@@ -290,9 +359,21 @@ __global__ void k_mlp_adam(float* params, const float* grad, float* m, float* v,
 
 cudaError_t launch_rain_record(const RecordArgs& a, cudaStream_t s) {
   const long long n = (long long)a.r.g.nx * a.r.g.ny * a.r.g.nz;
-  const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
-  k_rain_record<<<blocks, 256, 0, s>>>(a);
-  return cudaGetLastError();
+  const long long nb = (n + kRecCells - 1) / kRecCells;
+  if (nb > (1LL << 30)) return cudaErrorInvalidValue;
+  unsigned* counts = nullptr;
+  unsigned long long* offsets = nullptr;
+  cudaError_t e = cudaMallocAsync(&counts, (size_t)nb * sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  e = cudaMallocAsync(&offsets, (size_t)nb * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) { cudaFreeAsync(counts, s); return e; }
+  k_rain_record_count<<<(unsigned)nb, kRecThreads, 0, s>>>(a, n, counts);
+  k_rain_record_scan<<<1, 1024, 0, s>>>(counts, (int)nb, offsets, a.count);
+  k_rain_record_write<<<(unsigned)nb, kRecThreads, 0, s>>>(a, n, offsets);
+  e = cudaGetLastError();
+  cudaFreeAsync(offsets, s);
+  cudaFreeAsync(counts, s);
+  return e;
 }
 
 cudaError_t mlp_column_stats(const float* a, long long n, int d, double* out, double* rng, cudaStream_t s) {

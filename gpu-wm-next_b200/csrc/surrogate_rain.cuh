@@ -26,6 +26,7 @@ struct SurrogateArgs {
   // ran, cells the network ran on, and per check the cells that failed it (input range,
   // fraction range, water, energy; a cell can fail several)
   unsigned long long* stats;
+  int* work;                     // row counter of the network kernel (zeroed before each launch)
 };
 constexpr int kSurStats = 6;
 
