@@ -4,6 +4,7 @@
 // Buffer plan of one member (all fields share one padded geometry, see common.cuh):
 //   Q[5]        step state: rho_d, rho_theta_m, mom_u, mom_v, mom_w
 //   R[2]        density during a step (ping-pong between kernels)
+//   P[2]        pressure perturbation p'(R) handed from one acoustic substep to the next
 //   TH[2]       theta frozen for an RK stage (ping-pong between stages)
 //   B[2][3]     stage base momenta written by the slow kernel
 //   D[2][3]     acoustic momentum increments m - m_base (ping-pong between substeps)
@@ -50,6 +51,7 @@ struct Member {
   char* block = nullptr;
   float* Q[5]{};
   float* R[2]{};
+  float* P[2]{};
   float* TH[2]{};
   float* B[2][3]{};
   float* D[2][3]{};
@@ -260,7 +262,7 @@ bool build_substep_maps(Member& M) {
   };
   bool ok = true;
   for (int i = 0; i < 2; ++i) {
-    ok = ok && add(M.R[i], 0) && add(M.TH[i], 0);
+    ok = ok && add(M.R[i], 0) && add(M.TH[i], 0) && add(M.P[i], 0);
     ok = ok && add(M.D[i][0], 1) && add(M.D[i][1], 1) && add(M.D[i][2], 2);
     for (int f = 0; f < 3; ++f) ok = ok && add(M.B[i][f], 2);
   }
@@ -296,7 +298,7 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   M.field_elems = (size_t)g.plane * (g.nz + 1);
   const size_t fbytes = ((M.field_elems * sizeof(float) + 255) / 256) * 256;
   const bool moist = M.md.moist != 0;
-  const int nfields = 5 + 2 + 2 + 6 + 6 + (moist ? 9 : 0) + (M.terrain_active ? 3 : 0);
+  const int nfields = 5 + 2 + 2 + 2 + 6 + 6 + (moist ? 9 : 0) + (M.terrain_active ? 3 : 0);
   const size_t owned_max = (size_t)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
   const size_t plane2 = (size_t)d.nx * d.ny;
   const size_t extra = ((2 * plane2 * sizeof(double) + 255) / 256) * 256 +
@@ -311,6 +313,7 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   auto take = [&](size_t bytes) { char* r = p; p += ((bytes + 255) / 256) * 256; return r; };
   for (auto& q : M.Q) q = (float*)take(fbytes);
   for (auto& q : M.R) q = (float*)take(fbytes);
+  for (auto& q : M.P) q = (float*)take(fbytes);
   for (auto& q : M.TH) q = (float*)take(fbytes);
   for (auto& b : M.B) for (auto& q : b) q = (float*)take(fbytes);
   for (auto& b : M.D) for (auto& q : b) q = (float*)take(fbytes);
@@ -412,10 +415,12 @@ cudaError_t launch_substep(gwm_b200_ctx* c, const Member& M, const FastArgs& f, 
     const CUtensorMap* bu = fin ? M.tmap(f.bu, 2) : nullptr;
     const CUtensorMap* bv = fin ? M.tmap(f.bv, 2) : nullptr;
     const CUtensorMap* bw = fin ? M.tmap(f.bw, 2) : nullptr;
-    if (!rho || !th || (!first && (!du || !dv || !dw)) || (fin && (!bu || !bv || !bw)))
+    const CUtensorMap* pm = first ? nullptr : M.tmap(f.p_in, 0);
+    if (!rho || !th || (!first && (!du || !dv || !dw || !pm)) || (fin && (!bu || !bv || !bw)) ||
+        (f.final_kind == 0 && !f.p_out))
       return cudaErrorInvalidValue;
     m.rho = *rho; m.th = *th;
-    if (!first) { m.du = *du; m.dv = *dv; m.dw = *dw; }
+    if (!first) { m.du = *du; m.dv = *dv; m.dw = *dw; m.p = *pm; }
     if (fin) { m.bu = *bu; m.bv = *bv; m.bw = *bw; }
     return launch_fast_tma(f, m, first, c->stream);
   }
@@ -614,6 +619,7 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
       FastArgs f{};
       f.g = M.g;
       f.rho_in = M.R[rcur]; f.rho_out = M.R[rcur ^ 1];
+      f.p_in = M.P[rcur]; f.p_out = M.P[rcur ^ 1];
       f.th = M.TH[s & 1];
       const int dout = (n == 0) ? 0 : (dcur ^ 1);
       if (n > 0) { f.du_in = M.D[dcur][0]; f.dv_in = M.D[dcur][1]; f.dw_in = M.D[dcur][2]; }
@@ -1417,6 +1423,7 @@ int gwm_b200_fast_modes(gwm_b200_ctx* c) {
       FastArgs f{};
       f.g = M.g;
       f.rho_in = M.R[rcur]; f.rho_out = M.R[rcur ^ 1];
+      f.p_in = M.P[rcur]; f.p_out = M.P[rcur ^ 1];
       f.th = M.TH[0];
       const int dout = (n == 0) ? 0 : (dcur ^ 1);
       if (n > 0) { f.du_in = M.D[dcur][0]; f.dv_in = M.D[dcur][1]; f.dw_in = M.D[dcur][2]; }

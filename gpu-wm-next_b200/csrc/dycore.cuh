@@ -55,6 +55,8 @@ struct FastArgs {
   const float* th;                  // theta frozen for the RK stage
   const float *du_in, *dv_in, *dw_in;   // increments before the substep (null: zero)
   float *du_out, *dv_out, *dw_out;
+  const float* p_in;                // p'(rho_in) from the previous substep (TMA path, not the first)
+  float* p_out;                     // p'(rho_out) for the next substep (TMA path, inner substeps)
   const float *bu, *bv, *bw;        // stage base momenta (final_kind == 2)
   float *f_rho, *f_rt, *f_u, *f_v, *f_w;  // step result (final_kind == 2)
   int final_kind;                   // 0 inner substep, 1 last of a stage, 2 last of the step
@@ -76,6 +78,7 @@ struct FastMaps {
   CUtensorMap du, dv;      // box 36 x 17: owned faces + the tile's east/north face
   CUtensorMap dw;          // box 32 x 16
   CUtensorMap bu, bv, bw;  // box 32 x 16 (last substep of the step)
+  CUtensorMap p;           // box 40 x 18: p'(rho_in) with the halo ring (not the first substep)
 };
 // Box extents (x, y) of the maps above.
 constexpr int kTmaCellBox[2] = {40, 18};

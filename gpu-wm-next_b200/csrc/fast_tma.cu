@@ -11,6 +11,9 @@
 //                           box starts 4 columns left so x stays 16-byte aligned)
 //   du(k), dv(k)            36 x 17 box: owned faces plus the tile's east/north face
 //   dw(k+1)                 32 x 16 box: owned Z faces above the plane
+//   p'(k)                   40 x 18 box like rho: the pressure perturbation the previous
+//                           substep computed for its level sums (every substep but the
+//                           first of a stage), so the EOS runs once per cell per substep
 //   bu(k), bv(k), bw(k+1)   32 x 16 boxes, last substep of the step only (m = B + D)
 // so the kernel issues no per-thread global loads on the main path, holds no load
 // pipeline in registers and needs no halo threads reading global memory.
@@ -28,18 +31,18 @@ constexpr int OBW = 32, OBH = 16;  // owned box
 // slot layout in floats; every sub-buffer starts on a 128-byte boundary
 // (the base-momentum boxes are only present, and the slot only that long, in the last
 // substep of the step: other substeps use the shorter slot and fit three CTAs per SM)
-constexpr int O_RHO = 0, O_TH = 736, O_DU = 1472, O_DV = 2112, O_DW = 2752, O_BU = 3264,
-              O_BV = 3776, O_BW = 4288, SLOT = 4800, SLOT_SHORT = 3264, NSLOT = 3;
+constexpr int O_RHO = 0, O_TH = 736, O_DU = 1472, O_DV = 2112, O_DW = 2752, O_P = 3264, O_BU = 4000,
+              O_BV = 4512, O_BW = 5024, SLOT = 5536, SLOT_SHORT = 4000, NSLOT = 3;
 constexpr unsigned B_CELL = CBW * CBH * 4, B_FACE = FBW * FBH * 4, B_OWN = OBW * OBH * 4;
 constexpr size_t kDynSmem = size_t(SLOT) * NSLOT * sizeof(float) + 128;
 constexpr size_t kDynSmemShort = size_t(SLOT_SHORT) * NSLOT * sizeof(float) + 128;
-static_assert(O_TH % 32 == 0 && O_DU % 32 == 0 && O_DV % 32 == 0 && O_DW % 32 == 0 && O_BU % 32 == 0 &&
-                  O_BV % 32 == 0 && O_BW % 32 == 0 && SLOT % 32 == 0 && SLOT_SHORT % 32 == 0 &&
-                  SLOT_SHORT == O_BU,
+static_assert(O_TH % 32 == 0 && O_DU % 32 == 0 && O_DV % 32 == 0 && O_DW % 32 == 0 && O_P % 32 == 0 &&
+                  O_BU % 32 == 0 && O_BV % 32 == 0 && O_BW % 32 == 0 && SLOT % 32 == 0 &&
+                  SLOT_SHORT % 32 == 0 && SLOT_SHORT == O_BU,
               "128-byte aligned sub-buffers");
 static_assert(O_TH - O_RHO >= CBW * CBH && O_DU - O_TH >= CBW * CBH && O_DV - O_DU >= FBW * FBH &&
-                  O_DW - O_DV >= FBW * FBH && O_BU - O_DW >= OBW * OBH && O_BV - O_BU >= OBW * OBH &&
-                  O_BW - O_BV >= OBW * OBH && SLOT - O_BW >= OBW * OBH,
+                  O_DW - O_DV >= FBW * FBH && O_P - O_DW >= OBW * OBH && O_BU - O_P >= CBW * CBH &&
+                  O_BV - O_BU >= OBW * OBH && O_BW - O_BV >= OBW * OBH && SLOT - O_BW >= OBW * OBH,
               "boxes fit their sub-buffers");
 }  // namespace ft
 
@@ -106,7 +109,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     uint64_t* bar = &s_bar[kk % NSLOT];
     const bool wface = kk + 1 < nz;
     unsigned bytes = 2 * B_CELL;
-    if (!FIRST) bytes += 2 * B_FACE + (wface ? B_OWN : 0u);
+    if (!FIRST) bytes += 2 * B_FACE + (wface ? B_OWN : 0u) + B_CELL;
     if (final_step) bytes += 3 * B_OWN;
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(bar, bytes);
@@ -116,6 +119,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
       tma_load_3d(st + O_DU, &m.du, i0 + kXOff, j0 + 1, kk, bar);
       tma_load_3d(st + O_DV, &m.dv, i0 + kXOff, j0 + 1, kk, bar);
       if (wface) tma_load_3d(st + O_DW, &m.dw, i0 + kXOff, j0 + 1, kk + 1, bar);
+      tma_load_3d(st + O_P, &m.p, i0 + kXOff - 4, j0, kk, bar);
     }
     if (final_step) {
       tma_load_3d(st + O_BU, &m.bu, i0 + kXOff, j0 + 1, kk, bar);
@@ -150,7 +154,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     if (nz > 1) { issue(1); issued = 1; }
   }
   wait_plane(0, 0);
-  plane_p(0);
+  if (FIRST) plane_p(0);
   float dwc0 = 0.f, dwc1 = 0.f;  // increment at face k (face 0 never changes)
   float bwz0 = 0.f, bwz1 = 0.f;  // base momentum at face 0 (last substep of the step)
   if (final_step) {
@@ -167,10 +171,13 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     // ---- pressure perturbation of plane k+1 (its tiles were issued a plane ago)
     if (k + 1 < nz) {
       wait_plane(k + 1, k);
-      plane_p(k + 1);
+      if (FIRST) plane_p(k + 1);
     }
     // ---- faces of plane k: K12/K13 horizontal momenta, K14 vertical momentum at face k+1
-    const float(*sp)[TX + 2] = s_p[pb];
+    // p'(r, c) of plane k (P0) and k+1 (P1) in s_p coordinates (row 0 = j0-1, column
+    // 0 = i0-1): computed above in the first substep, loaded with the tiles otherwise
+    auto P0 = [&](int r, int c) { return FIRST ? s_p[pb][r][c] : st[O_P + r * CBW + c + 3]; };
+    auto P1 = [&](int r, int c) { return FIRST ? s_p[pb ^ 1][r][c] : stn[O_P + r * CBW + c + 3]; };
     float du0 = 0.f, dv0 = 0.f, du1 = 0.f, dv1 = 0.f, dw0 = 0.f, dw1 = 0.f;
     if (!FIRST) {
       du0 = st[O_DU + ty * FBW + tx];
@@ -179,21 +186,21 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
       dv1 = st[O_DV + (ty + RY) * FBW + tx];
       if (k + 1 < nz) { dw0 = st[O_DW + ty * OBW + tx]; dw1 = st[O_DW + (ty + RY) * OBW + tx]; }
     }
-    const float pc0 = sp[ty + 1][tx + 1], pc1 = sp[ty + RY + 1][tx + 1];
+    const float pc0 = P0(ty + 1, tx + 1), pc1 = P0(ty + RY + 1, tx + 1);
     float un0 = du0, vn0 = dv0, un1 = du1, vn1 = dv1;
     if (hm) {
       if (!skip_u) {
-        un0 = du0 + (-dtf * ((pc0 - sp[ty + 1][tx]) * idx));
-        un1 = du1 + (-dtf * ((pc1 - sp[ty + RY + 1][tx]) * idx));
+        un0 = du0 + (-dtf * ((pc0 - P0(ty + 1, tx)) * idx));
+        un1 = du1 + (-dtf * ((pc1 - P0(ty + RY + 1, tx)) * idx));
       }
-      if (!skip_v0) vn0 = dv0 + (-dtf * ((pc0 - sp[ty][tx + 1]) * idy));
-      vn1 = dv1 + (-dtf * ((pc1 - sp[ty + RY][tx + 1]) * idy));
+      if (!skip_v0) vn0 = dv0 + (-dtf * ((pc0 - P0(ty, tx + 1)) * idy));
+      vn1 = dv1 + (-dtf * ((pc1 - P0(ty + RY, tx + 1)) * idy));
     }
     if (own0) { s_du[pb][ty][tx] = un0; s_dv[pb][ty][tx] = vn0; }
     if (own1) { s_du[pb][ty + RY][tx] = un1; s_dv[pb][ty + RY][tx] = vn1; }
     if (role == 1) {  // the tile's east X face
       float d = FIRST ? 0.f : st[O_DU + (hr - 1) * FBW + w];
-      if (hm && !h_skip) d = d + (-dtf * ((sp[hr][hc] - sp[hr][hc - 1]) * idx));
+      if (hm && !h_skip) d = d + (-dtf * ((P0(hr, hc) - P0(hr, hc - 1)) * idx));
       s_du[pb][hr - 1][w] = d;
       // open east boundary: face nx belongs to no tile; its step value is base + increment
       if (final_step && h_skip) {
@@ -202,7 +209,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
       }
     } else if (role == 3) {  // the tile's north Y face
       float d = FIRST ? 0.f : st[O_DV + h * FBW + hc - 1];
-      if (hm && !h_skip) d = d + (-dtf * ((sp[hr][hc] - sp[hr - 1][hc]) * idy));
+      if (hm && !h_skip) d = d + (-dtf * ((P0(hr, hc) - P0(hr - 1, hc)) * idy));
       s_dv[pb][h][hc - 1] = d;
       if (final_step && h_skip) {
         const int o = gidx(g, hi, hj, k);
@@ -214,8 +221,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     if (k + 1 < nz) {
       const float prl = s_pref[k], pru = s_pref[k + 1], rrl = s_rref[k], rru = s_rref[k + 1];
       const float idzf = s_idzf[k + 1];
-      const float(*spn)[TX + 2] = s_p[pb ^ 1];
-      const float pn0 = spn[ty + 1][tx + 1], pn1 = spn[ty + RY + 1][tx + 1];
+      const float pn0 = P1(ty + 1, tx + 1), pn1 = P1(ty + RY + 1, tx + 1);
       const float rn0 = stn[O_RHO + (ty + 1) * CBW + tx + 4], rn1 = stn[O_RHO + (ty + RY + 1) * CBW + tx + 4];
       wn0 = dw0 + dtf * (-((pn0 - pru) - (pc0 - prl)) * idzf - a.gravity * (0.5f * ((rc0 - rrl) + (rn0 - rru))));
       wn1 = dw1 + dtf * (-((pn1 - pru) - (pc1 - prl)) * idzf - a.gravity * (0.5f * ((rc1 - rrl) + (rn1 - rru))));
@@ -254,7 +260,12 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
         store_tile(a.dv_out, g, kFaceY, gi, gj0, k, vn0, edge);
         if (k + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj0, k + 1, wn0, edge);
       }
-      if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime_ref(rn, rt, s_binv[k], s_bpr[k]), kFxP); }
+      if (acc_mode == 1) {
+        const float pv = eos_pprime_ref(rn, rt, s_binv[k], s_bpr[k]);
+        sa.add(rn, kFxRho);
+        sb.add(pv, kFxP);
+        store_tile(a.p_out, g, kCell, gi, gj0, k, pv, edge);
+      }
       else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
     }
     if (own1) {
@@ -278,7 +289,12 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
         store_tile(a.dv_out, g, kFaceY, gi, gj1, k, vn1, edge);
         if (k + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj1, k + 1, wn1, edge);
       }
-      if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime_ref(rn, rt, s_binv[k], s_bpr[k]), kFxP); }
+      if (acc_mode == 1) {
+        const float pv = eos_pprime_ref(rn, rt, s_binv[k], s_bpr[k]);
+        sa.add(rn, kFxRho);
+        sb.add(pv, kFxP);
+        store_tile(a.p_out, g, kCell, gi, gj1, k, pv, edge);
+      }
       else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
     }
     if (acc_mode) {
