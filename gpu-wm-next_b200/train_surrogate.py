@@ -17,6 +17,8 @@ step), so samples and evaluation stay before it.
 
 Usage:
     python gpu-wm-next_b200/train_surrogate.py --out gpu-wm-next_b200/surrogate_c3.npz
+    python gpu-wm-next_b200/train_surrogate.py --rain-calls --n 512   # a profiling case:
+        seed 9 after 20 steps, two plain and two network warm-rain calls (shipped weights)
 """
 import argparse
 import importlib
@@ -58,11 +60,27 @@ def main():
     ap.add_argument("--snapshots", type=int, default=18)
     ap.add_argument("--every", type=int, default=15)
     ap.add_argument("--eval-steps", type=int, default=300)
+    ap.add_argument("--rain-calls", action="store_true",
+                    help="no training: the seed-9 state after 20 steps, two plain and two network "
+                         "warm-rain calls with the shipped weights (a case for the profiler)")
     args = ap.parse_args()
     import torch
     gwm = importlib.import_module("gpu-wm-next_b200")
     g = gwm.GridSpec(args.n, args.n, NZ, dx=DX, dy=DX, z_top=ZTOP)
     spec = model_spec(gwm)
+    if args.rain_calls:
+        w = np.load(os.path.join(HERE, "surrogate_c3.npz"))
+        with gwm.Model(g, spec) as m:
+            m.upload(state(gwm, g, 9))
+            m.step(20)
+            for mode in ("plain", "network"):
+                if mode == "network":
+                    m.set_rain_surrogate(w["params"], w["norm"], w["range"])
+                for _ in range(2):
+                    m.apply_warm_rain_microphysics("metric")
+            m.synchronize()
+            print(json.dumps(m.surrogate_stats()), flush=True)
+        return
     cap = args.samples
     x = torch.empty((cap, 7), dtype=torch.float32, device="cuda")
     y = torch.empty((cap, 5), dtype=torch.float32, device="cuda")
