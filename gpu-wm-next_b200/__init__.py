@@ -26,6 +26,9 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _ROOT = os.path.dirname(_HERE)
 _LIB_PATH = os.path.join(_HERE, "_build", "libgwm_b200.so")
+# the reference's gwm_idealized_driver command line over the C-ABI (C++, links the library)
+DRIVER_PATH = os.path.join(_HERE, "_build", "gwm_b200_idealized_driver")
+_DRIVER_SRC = os.path.join(_HERE, "drivers", "gwm_b200_idealized_driver.cpp")
 _SOURCES = ["capi.cu", "dycore.cu", "fast_tma.cu", "slow_tma.cu", "tracer_tma.cu", "physics.cu", "halo.cu",
             "surrogate.cu", "surrogate_rain.cu", "cases.cpp"]
 _HEADERS = ["common.cuh", "dycore.cuh", "physics.cuh", "halo.cuh", "tma.cuh", "rain_cell.cuh", "surrogate.cuh", "surrogate_rain.cuh"]
@@ -46,16 +49,22 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile the CUDA library in-tree for sm_100a (nvcc cross-compiles without a GPU)."""
-    if not force and not _stale():
-        return _LIB_PATH
-    os.makedirs(os.path.dirname(_LIB_PATH), exist_ok=True)
-    srcs = [os.path.join(_HERE, "csrc", f) for f in _SOURCES]
-    cmd = ["nvcc", *NVCC_FLAGS, "-o", _LIB_PATH + ".tmp", *srcs]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
-    os.replace(_LIB_PATH + ".tmp", _LIB_PATH)
+    """Compile the CUDA library in-tree for sm_100a (nvcc cross-compiles without a GPU),
+    then the idealized-driver executable that links it."""
+    if force or _stale():
+        os.makedirs(os.path.dirname(_LIB_PATH), exist_ok=True)
+        srcs = [os.path.join(_HERE, "csrc", f) for f in _SOURCES]
+        cmd = ["nvcc", *NVCC_FLAGS, "-o", _LIB_PATH + ".tmp", *srcs]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        subprocess.run(cmd, check=True)
+        os.replace(_LIB_PATH + ".tmp", _LIB_PATH)
+    if force or not os.path.exists(DRIVER_PATH) or os.path.getmtime(DRIVER_PATH) < max(
+            os.path.getmtime(_LIB_PATH), os.path.getmtime(_DRIVER_SRC)):
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(_ROOT, "include"), "-o", DRIVER_PATH + ".tmp",
+               _DRIVER_SRC, "-L", os.path.dirname(_LIB_PATH), "-lgwm_b200", "-Wl,-rpath,$ORIGIN"]
+        subprocess.run(cmd, check=True)
+        os.replace(DRIVER_PATH + ".tmp", DRIVER_PATH)
     return _LIB_PATH
 
 
