@@ -30,7 +30,7 @@ _LIB_PATH = os.path.join(_HERE, "_build", "libgwm_b200.so")
 DRIVER_PATH = os.path.join(_HERE, "_build", "gwm_b200_idealized_driver")
 _DRIVER_SRC = os.path.join(_HERE, "drivers", "gwm_b200_idealized_driver.cpp")
 _SOURCES = ["capi.cu", "dycore.cu", "fast_tma.cu", "slow_tma.cu", "tracer_tma.cu", "physics.cu", "halo.cu",
-            "surrogate.cu", "surrogate_rain.cu", "cases.cpp"]
+            "surrogate.cu", "surrogate_rain.cu", "scalar.cu", "cases.cpp"]
 _HEADERS = ["common.cuh", "dycore.cuh", "physics.cuh", "halo.cuh", "tma.cuh", "rain_cell.cuh", "surrogate.cuh", "surrogate_rain.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
@@ -95,6 +95,12 @@ class _Rain(C.Structure):
 class _Member(C.Structure):
     _fields_ = [("moist", C.c_int), ("enable_tracer_transport", C.c_int),
                 ("enable_warm_rain", C.c_int), ("step", _Step), ("rain", _Rain)]
+
+
+class _ScalarDesc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("periodic_x", C.c_int),
+                ("periodic_y", C.c_int), ("u_adv", C.c_float), ("v_adv", C.c_float), ("dt", C.c_float),
+                ("dx", C.c_float), ("dy", C.c_float)]
 
 
 class _Fields(C.Structure):
@@ -199,6 +205,7 @@ def lib():
                                          C.POINTER(C.c_void_p), vp]
     L.gwm_b200_dry_pressure.argtypes = [vp, vp, vp, C.c_longlong, vp]
     L.gwm_b200_field_stats_noalloc.argtypes = [vp, C.c_longlong, vp, vp]
+    L.gwm_b200_scalar_ssprk3.argtypes = [C.POINTER(_ScalarDesc), vp, C.c_int, vp]
     L.gwm_b200_ranks_to_global.argtypes = [C.POINTER(_LayoutDesc), C.c_int,
                                            C.POINTER(C.c_void_p), vp]
     L.gwm_b200_global_to_ranks.argtypes = [C.POINTER(_LayoutDesc), C.c_int, vp,
@@ -220,7 +227,7 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_rain_record",
             "gwm_b200_mlp_train", "gwm_b200_mlp_loss_grad", "gwm_b200_set_rain_surrogate",
             "gwm_b200_surrogate_fallbacks", "gwm_b200_surrogate_stats", "gwm_b200_layout",
-            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_ranks_to_global",
+            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_scalar_ssprk3", "gwm_b200_ranks_to_global",
             "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
 
 
@@ -632,6 +639,27 @@ def dry_pressure(rho_ptr: int, rho_theta_ptr: int, p_ptr: int, n: int, stream: O
     rc = lib().gwm_b200_dry_pressure(rho_ptr, rho_theta_ptr, p_ptr, n, stream)
     if rc != OK:
         raise RuntimeError(f"dry_pressure: status {rc}")
+
+
+def scalar_ssprk3(q, u_adv: float = 20.0, v_adv: float = 0.0, dt: float = 10.0, dx: float = 1000.0,
+                  dy: float = 1000.0, periodic_x: bool = True, periodic_y: bool = True, nsteps: int = 1):
+    """nsteps of advance_scalar_ssprk3 (dry_transport.cu:285-325) on the GPU.
+
+    q: (nz, ny, nx) float32, a contiguous torch CUDA tensor (advanced in place and
+    returned) or an array (copied to the device and back; the result is returned).
+    Defaults are DryTransportConfig's (dry_transport.hpp:11-17)."""
+    import torch
+    on_device = isinstance(q, torch.Tensor)
+    t = q if on_device else torch.from_numpy(np.ascontiguousarray(q, dtype=np.float32)).cuda()
+    if t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous() or t.dim() != 3:
+        raise ValueError("scalar_ssprk3: q must be a contiguous (nz, ny, nx) float32 CUDA tensor")
+    nz, ny, nx = t.shape
+    d = _ScalarDesc(nx, ny, nz, int(periodic_x), int(periodic_y), u_adv, v_adv, dt, dx, dy)
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = lib().gwm_b200_scalar_ssprk3(C.byref(d), t.data_ptr(), nsteps, stream)
+    if rc != OK:
+        raise RuntimeError(f"scalar_ssprk3: status {rc}")
+    return t if on_device else t.cpu().numpy()
 
 
 def field_stats_noalloc(x_ptr: int, n: int, out_ptr: int, stream: Optional[int] = None):

@@ -275,6 +275,21 @@ int gwm_b200_dry_pressure(const float* rho_d, const float* rho_theta_m, float* p
  * threads without ordering) race and must be serialised by the caller. */
 int gwm_b200_field_stats_noalloc(const float* x, long long n, double* out, void* stream);
 
+/* ---- scalar transport -------------------------------------------------------- */
+/* DryTransportConfig (include/gwm/dycore/dry_transport.hpp:11-17) with the grid of the
+ * advected field. */
+typedef struct {
+  int nx, ny, nz;
+  int periodic_x, periodic_y;  /* else zero beyond the open side, as the halo exchange gives */
+  float u_adv, v_adv, dt, dx, dy;
+} gwm_b200_scalar_desc;
+/* nsteps of advance_scalar_ssprk3 (include/gwm/dycore/dry_transport.hpp:19-21,
+ * src/dycore/dry_transport.cu:285-325) on q, a device array (nz, ny, nx) in the global
+ * owned layout, in place; the arithmetic is the reference's, so results match it bit
+ * for bit.  Two scratch copies of q are taken from the stream-ordered allocator for the
+ * call.  stream: cudaStream_t as void* (NULL: the default stream); returns when done. */
+int gwm_b200_scalar_ssprk3(const gwm_b200_scalar_desc* desc, float* q, int nsteps, void* stream);
+
 /* ---- host layout helpers (no device work) --------------------------------- */
 /* Per-rank halo-padded host buffers <-> global owned arrays.  Faces shared by two
  * ranks (and periodic aliases) take the average of both copies on the way in, as the

@@ -88,6 +88,7 @@ def lib():
         L.gwo_case.argtypes = [C.c_int, C.POINTER(Grid), C.POINTER(CaseParams), C.c_int,
                                C.POINTER(Fields)]
         L.gwo_pressure.argtypes = [C.c_long, DP, DP, DP, C.c_int]
+        L.gwo_scalar_ssprk3.argtypes = [C.c_int] * 5 + [C.c_double] * 5 + [C.c_int, C.c_int, DP]
         L.gwo_layout.argtypes = [C.c_int] * 8 + [C.POINTER(C.c_int)]
         L.gwo_halo.argtypes = [C.c_int] * 10 + [C.POINTER(DP)]
         _lib = L
@@ -285,6 +286,17 @@ def case(kind: str, g: GridSpec, params: CaseSpec, precision: int = 32) -> dict:
     gc, pc = g.c(), params.c()
     f = _fields(out)
     _check(lib().gwo_case(CASE_KINDS[kind], C.byref(gc), C.byref(pc), precision, C.byref(f)))
+    return out
+
+
+def scalar_ssprk3(q: np.ndarray, u_adv: float, v_adv: float, dt: float, dx: float = 1000.0, dy: float = 1000.0,
+                  periodic_x: bool = True, periodic_y: bool = True, nsteps: int = 1,
+                  precision: int = 64) -> np.ndarray:
+    """nsteps of advance_scalar_ssprk3 (dry_transport.cu:285-325) on q (nz, ny, nx)."""
+    out = np.array(q, dtype=np.float64, copy=True, order="C")
+    nz, ny, nx = out.shape
+    _check(lib().gwo_scalar_ssprk3(nx, ny, nz, int(periodic_x), int(periodic_y), float(u_adv), float(v_adv),
+                                   float(dt), float(dx), float(dy), nsteps, precision, _ptr(out)))
     return out
 
 

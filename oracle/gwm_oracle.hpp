@@ -1161,4 +1161,47 @@ template <class T> T hydrostatic_rho_at_height(T rho_s, T theta, T z, T g = T(9.
   return rho_from_pressure_theta(p, theta);
 }
 
+// ---------------------------------------------------------------------------
+// Scalar advection: advance_scalar_ssprk3 (src/dycore/dry_transport.cu:285-325) with
+// upwind_stage_kernel (:13-37) and blend_stage_kernel (:39-46) on the global owned array
+// (nz, ny, nx).  Halo values are the periodic image, or zero beyond an open side (the
+// halo exchange's absent neighbour, src/comm/halo_exchange.cpp:563-620), which is what
+// the virtual-rank exchange gives the stencil.
+template <class T>
+void scalar_upwind_stage(const std::vector<T>& in, std::vector<T>& out, int nx, int ny, int nz, bool px, bool py,
+                         T u, T v, T dt, T dx, T dy) {
+  auto at = [&](int i, int j, int k) -> T {
+    if (i < 0 || i >= nx) {
+      if (!px) return T(0);
+      i = (i + nx) % nx;
+    }
+    if (j < 0 || j >= ny) {
+      if (!py) return T(0);
+      j = (j + ny) % ny;
+    }
+    return in[((size_t)k * ny + j) * nx + i];
+  };
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const T q = at(i, j, k);
+        const T dqx = (u >= T(0)) ? (q - at(i - 1, j, k)) / dx : (at(i + 1, j, k) - q) / dx;
+        const T dqy = (v >= T(0)) ? (q - at(i, j - 1, k)) / dy : (at(i, j + 1, k) - q) / dy;
+        // q - dt*(u*dqx + v*dqy) with the reference build's contractions
+        out[((size_t)k * ny + j) * nx + i] = std::fma(-dt, std::fma(u, dqx, v * dqy), q);
+      }
+}
+
+template <class T>
+void scalar_ssprk3(std::vector<T>& q, int nx, int ny, int nz, bool px, bool py, T u, T v, T dt, T dx, T dy) {
+  const std::vector<T> q0 = q;
+  std::vector<T> q1(q.size()), q2(q.size()), tmp(q.size());
+  scalar_upwind_stage(q, q1, nx, ny, nz, px, py, u, v, dt, dx, dy);
+  scalar_upwind_stage(q1, tmp, nx, ny, nz, px, py, u, v, dt, dx, dy);
+  // wa*a + wb*b as fma(wa, a, wb*b), the reference build's contraction
+  for (size_t n = 0; n < q.size(); ++n) q2[n] = std::fma(T(0.75f), q0[n], T(0.25f) * tmp[n]);
+  scalar_upwind_stage(q2, tmp, nx, ny, nz, px, py, u, v, dt, dx, dy);
+  for (size_t n = 0; n < q.size(); ++n) q[n] = std::fma(T(1.0f / 3.0f), q0[n], T(2.0f / 3.0f) * tmp[n]);
+}
+
 }  // namespace gwo

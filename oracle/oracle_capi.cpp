@@ -544,6 +544,27 @@ int gwo_case(int kind, const gwo_grid* g, const gwo_case_params* c, int precisio
   });
 }
 
+// nsteps of advance_scalar_ssprk3 on q (nz, ny, nx) in place.
+int gwo_scalar_ssprk3(int nx, int ny, int nz, int px, int py, double u, double v, double dt, double dx, double dy,
+                      int nsteps, int precision, double* q) {
+  return guard([&] {
+    const size_t n = (size_t)nx * ny * nz;
+    if (precision == 32) {
+      std::vector<float> f(q, q + n);
+      for (int s = 0; s < nsteps; ++s)
+        gwo::scalar_ssprk3<float>(f, nx, ny, nz, px != 0, py != 0, (float)u, (float)v, (float)dt, (float)dx,
+                                  (float)dy);
+      std::copy(f.begin(), f.end(), q);
+    } else {
+      std::vector<double> f(q, q + n);
+      for (int s = 0; s < nsteps; ++s)
+        gwo::scalar_ssprk3<double>(f, nx, ny, nz, px != 0, py != 0, u, v, dt, dx, dy);
+      std::copy(f.begin(), f.end(), q);
+    }
+    return 0;
+  });
+}
+
 int gwo_pressure(long n, const double* rho, const double* rt, double* p, int precision) {
   for (long q = 0; q < n; ++q)
     p[q] = precision == 32 ? (double)gwo::pressure_from_rho_theta<float>((float)rho[q], (float)rt[q])

@@ -11,6 +11,8 @@
 // advance_passive_tracers_ssprk3 (passive_tracer.hpp:44-49) and
 // apply_warm_rain_microphysics (warm_rain.hpp:57-68; metric or nominal overload).
 //
+// A second case kind (ScalarHeader, magic "GWMSCAL1") runs advance_scalar_ssprk3.
+//
 // Case file (little endian): CaseHeader, then float arrays in global C order
 // (k, j, i): terrain (ny, nx), rho (nz, ny, nx), rho_theta (nz, ny, nx),
 // u (nz, ny, nx+1), v (nz, ny+1, nx), w (nz+1, ny, nx) and, when moist, the
@@ -29,6 +31,7 @@
 #include "gwm/comm/virtual_rank_layout.hpp"
 #include "gwm/domain/grid_metrics.hpp"
 #include "gwm/dycore/dry_core.hpp"
+#include "gwm/dycore/dry_transport.hpp"
 #include "gwm/dycore/passive_tracer.hpp"
 #include "gwm/physics/warm_rain.hpp"
 #include "gwm/state/tracer_registry.hpp"
@@ -226,6 +229,51 @@ int run(const char* in_path, const char* out_path) {
   return 0;
 }
 
+// Scalar-advection case (magic "GWMSCAL1"): ScalarHeader, then q (nz, ny, nx) floats.
+// `steps` calls of advance_scalar_ssprk3 (include/gwm/dycore/dry_transport.hpp:19-21)
+// on the virtual-rank fields; output "GWMSCA01" + q.
+struct ScalarHeader {
+  char magic[8];  // "GWMSCAL1"
+  int nx, ny, nz, ranks_x, ranks_y, periodic_x, periodic_y, steps;
+  float u_adv, v_adv, dt, dx, dy, pad;
+};
+
+int run_scalar(const char* in_path, const char* out_path) {
+  std::FILE* in = std::fopen(in_path, "rb");
+  if (!in) throw std::runtime_error(std::string("cannot open ") + in_path);
+  ScalarHeader h{};
+  if (std::fread(&h, sizeof(h), 1, in) != 1 || std::memcmp(h.magic, "GWMSCAL1", 8) != 0)
+    throw std::runtime_error("bad scalar case header");
+  const auto q = read_floats(in, size_t(h.nx) * h.ny * h.nz);
+  std::fclose(in);
+  const auto layout = gwm::comm::VirtualRankLayout::build(h.nx, h.ny, h.nz, 1, h.ranks_x, h.ranks_y,
+                                                          h.periodic_x != 0, h.periodic_y != 0);
+  std::vector<gwm::state::Field3D<gwm::real>> fields;
+  for (const auto& d : layout) {
+    fields.emplace_back(d.nx_local(), d.ny_local(), h.nz, d.halo, "golden_scalar_" + std::to_string(d.rank));
+    fields.back().fill(0.0f);
+  }
+  std::vector<gwm::state::Field3D<gwm::real>*> p;
+  for (auto& f : fields) p.push_back(&f);
+  scatter(q, {0, 0, 0}, h.nx, h.ny, layout, p);
+  gwm::dycore::DryTransportConfig cfg;
+  cfg.u_adv = h.u_adv;
+  cfg.v_adv = h.v_adv;
+  cfg.dt = h.dt;
+  cfg.dx = h.dx;
+  cfg.dy = h.dy;
+  for (int step = 0; step < h.steps; ++step) gwm::dycore::advance_scalar_ssprk3(fields, layout, cfg);
+  if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("device error after the steps");
+  std::vector<const gwm::state::Field3D<gwm::real>*> cp;
+  for (const auto& f : fields) cp.push_back(&f);
+  std::FILE* out = std::fopen(out_path, "wb");
+  if (!out) throw std::runtime_error(std::string("cannot write ") + out_path);
+  std::fwrite("GWMSCA01", 1, 8, out);
+  write_floats(out, gather({0, 0, 0}, h.nx, h.ny, h.nz, layout, cp));
+  std::fclose(out);
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -234,6 +282,12 @@ int main(int argc, char** argv) {
     return 2;
   }
   try {
+    char magic[8] = {};
+    if (std::FILE* f = std::fopen(argv[1], "rb")) {
+      if (std::fread(magic, 1, 8, f) != 8) magic[0] = 0;
+      std::fclose(f);
+    }
+    if (std::memcmp(magic, "GWMSCAL1", 8) == 0) return run_scalar(argv[1], argv[2]);
     return run(argv[1], argv[2]);
   } catch (const std::exception& e) {
     std::fprintf(stderr, "ref_golden error: %s\n", e.what());

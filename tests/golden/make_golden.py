@@ -6,7 +6,8 @@ step operators compiled from its sources by ``make -C oracle ref``; it needs a
 GPU because the reference runs its kernels on managed memory) and stores inputs,
 parameters and outputs in ``ref_<case>.npz``.  The reference's level-mean
 reduction uses float atomics, so its output is reproducible only to rounding;
-the tests compare against it with tolerances, never bitwise.
+the tests compare against it with tolerances, never bitwise.  The scalar-advection
+cases (advance_scalar_ssprk3, no atomics) are exact and compared bit for bit.
 
 Usage (on a machine with a GPU and the built driver):
     python tests/golden/make_golden.py --out tests/golden
@@ -130,10 +131,57 @@ def read_out(path, spec, shapes):
     return out
 
 
+# Scalar advection cases (advance_scalar_ssprk3): name -> grid, ranks, periodicity,
+# DryTransportConfig, steps and the initial field q(i, j, k).  The first three take the
+# configurations of the reference's own tests (test_constant_state.cpp,
+# test_scalar_mass_conservation.cpp, test_virtual_rank_equivalence.cpp); the wave runs
+# the scalar_advection case file's 300 s (60 steps); the last has an open side.
+SCALAR_CASES = {
+    "scalar_constant": dict(nx=24, ny=24, nz=3, rx=2, ry=2, px=True, py=True, u=20.0, v=-10.0, dt=4.0, steps=1,
+                            init="constant"),
+    "scalar_mass": dict(nx=32, ny=20, nz=1, rx=2, ry=2, px=True, py=True, u=12.0, v=7.0, dt=2.0, steps=1,
+                        init="stripes"),
+    "scalar_wave": dict(nx=32, ny=32, nz=2, rx=2, ry=2, px=True, py=True, u=15.0, v=-5.0, dt=5.0, steps=60,
+                        init="wave"),
+    "scalar_open": dict(nx=40, ny=24, nz=3, rx=2, ry=1, px=False, py=True, u=-18.0, v=6.0, dt=3.0, steps=5,
+                        init="random"),
+}
+
+
+def scalar_field(c):
+    nz, ny, nx = c["nz"], c["ny"], c["nx"]
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    if c["init"] == "constant":
+        q = np.full((nz, ny, nx), 7.5)
+    elif c["init"] == "stripes":
+        q = 1.0 + 0.1 * ((i + 2 * j) % 7)
+    elif c["init"] == "wave":
+        q = np.sin(0.2 * i) + np.cos(0.3 * j)
+    else:
+        q = np.random.default_rng(17).uniform(0.5, 2.0, (nz, ny, nx))
+    return np.asarray(q, dtype=np.float32)
+
+
+def write_scalar_case(path, c, q):
+    hdr = struct.pack("<8s8i6f", b"GWMSCAL1", c["nx"], c["ny"], c["nz"], c["rx"], c["ry"], int(c["px"]),
+                      int(c["py"]), c["steps"], c["u"], c["v"], c["dt"], 1000.0, 1000.0, 0.0)
+    with open(path, "wb") as f:
+        f.write(hdr)
+        f.write(np.ascontiguousarray(q, dtype=np.float32).tobytes())
+
+
+def read_scalar_out(path, c):
+    raw = open(path, "rb").read()
+    assert raw[:8] == b"GWMSCA01", "bad scalar output header"
+    n = c["nx"] * c["ny"] * c["nz"]
+    assert len(raw) == 8 + 4 * n, "scalar output size mismatch"
+    return np.frombuffer(raw, dtype=np.float32, offset=8).reshape(c["nz"], c["ny"], c["nx"]).copy()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
-    ap.add_argument("--cases", nargs="*", default=list(CASES))
+    ap.add_argument("--cases", nargs="*", default=list(CASES) + list(SCALAR_CASES))
     args = ap.parse_args()
     if not os.path.exists(DRIVER):
         sys.exit(f"{DRIVER} missing: build it with `make -C oracle ref`")
@@ -142,6 +190,17 @@ def main():
     os.makedirs(args.out, exist_ok=True)
     with tempfile.TemporaryDirectory() as tmp:
         for name in args.cases:
+            if name in SCALAR_CASES:
+                c = SCALAR_CASES[name]
+                q = scalar_field(c)
+                cpath, opath = os.path.join(tmp, name + ".case"), os.path.join(tmp, name + ".out")
+                write_scalar_case(cpath, c, q)
+                subprocess.run([DRIVER, cpath, opath], check=True, timeout=600)
+                out = read_scalar_out(opath, c)
+                np.savez_compressed(os.path.join(args.out, f"ref_{name}.npz"),
+                                    spec=np.frombuffer(json.dumps(c).encode(), dtype=np.uint8), in_q=q, out_q=out)
+                print(f"{name}: wrote ref_{name}.npz (finite={np.isfinite(out).all()})", flush=True)
+                continue
             spec = CASES[name]
             state, terrain = case_state(gwm, spec)
             cpath, opath = os.path.join(tmp, name + ".case"), os.path.join(tmp, name + ".out")

@@ -147,3 +147,45 @@ def test_driver_virtual_rank_totals(gwm, tmp_path):
     shared_u = np.asarray(s1["u"], np.float64)[:, :, CASE["nx"] // 2].sum()
     assert four["final"]["total_horizontal_momentum_x"] == pytest.approx(
         one["final"]["total_horizontal_momentum_x"] + shared_u, rel=5e-6, abs=5e-6)
+
+
+CASES_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpu-wm-next_b200", "cases")
+
+
+def _harness():
+    import importlib.util
+    path = os.path.join(os.path.dirname(CASES_DIR), "run_idealized_case.py")
+    spec = importlib.util.spec_from_file_location("run_idealized_case", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_case_file_maps_to_driver_flags():
+    h = _harness()
+    case = h.load_case(os.path.join(CASES_DIR, "mountain_wave.yaml"))
+    cmd = h.driver_command(case, "drv", "out.json", steps=5, dt=2.0)
+    flags = dict(zip(cmd[1::2], cmd[2::2]))
+    assert cmd[0] == "drv" and flags["--case"] == "mountain_wave_background"
+    assert flags["--nx"] == "96" and flags["--z-top"] == "16000.0"
+    assert flags["--terrain-kind"] == "cosine_mountain" and flags["--terrain-half-width-x"] == "0.12"
+    assert flags["--terrain-height"] == "800.0" and flags["--u-background"] == "10.0"
+    assert flags["--steps"] == "5" and flags["--dt"] == "2.0" and flags["--summary-json"] == "out.json"
+    assert "--fast-substeps" not in flags and "--theta-background" not in flags
+
+
+@pytest.mark.gpu
+def test_case_files_run(gwm, tmp_path):
+    h = _harness()
+    out = tmp_path / "bubble.json"
+    assert h.main([os.path.join(CASES_DIR, "warm_bubble.yaml"), "--steps", "3", "--dt", "1",
+                   "--fast-substeps", "2", "--summary-json", str(out)]) == 0
+    js = json.loads(out.read_text())
+    assert js["case"] == "warm_bubble" and js["steps"] == 3
+    assert js["final"]["theta_m"]["max"] > 300.0 and js["final"]["w_face"]["max"] > 0.0
+    out = tmp_path / "scalar.json"
+    s = h.run_scalar_case(h.load_case(os.path.join(CASES_DIR, "scalar_advection.yaml")), str(out))
+    assert s["steps"] == 50 and json.loads(out.read_text()) == s
+    # upwind SSPRK3 on a periodic grid conserves mass and does not create new extrema
+    assert abs(s["final"]["mass"] - s["initial"]["mass"]) <= 1e-3 * abs(s["initial"]["mass"]) + 1e-3
+    assert s["initial"]["min"] - 1e-6 <= s["final"]["min"] and s["final"]["max"] <= s["initial"]["max"] + 1e-6
