@@ -1573,6 +1573,17 @@ static int layout_rows(const gwm_b200_layout_desc* d, std::vector<int>& rows) {
   return GWM_B200_OK;
 }
 
+int gwm_b200_grid_z_center(const gwm_b200_grid_desc* d, float* out) {
+  if (!d || !out || d->nx <= 0 || d->ny <= 0 || d->nz <= 0 || !(d->z_top > 0)) return GWM_B200_ERR_ARG;
+  Member M;  // host fields only: the metric builder reads the grid, terrain and levels
+  M.gd = *d;
+  if (d->terrain) M.terrain.assign(d->terrain, d->terrain + (size_t)d->nx * d->ny);
+  if (d->eta_interfaces) M.eta.assign(d->eta_interfaces, d->eta_interfaces + d->nz + 1);
+  const HostMetrics H = build_metrics(M);
+  std::copy(H.zc.begin(), H.zc.end(), out);
+  return GWM_B200_OK;
+}
+
 int gwm_b200_layout(const gwm_b200_layout_desc* d, int* out, int capacity) {
   std::vector<int> rows;
   int rc = layout_rows(d, rows);

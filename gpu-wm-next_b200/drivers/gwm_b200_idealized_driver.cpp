@@ -8,11 +8,17 @@
 // host from the state in the reference's own virtual-rank order, so multi-rank layouts
 // count shared faces once per rank exactly as summarize_dry_states does.
 //
-// Differences, each reported as an error rather than run differently:
-//   --halo other than 1 (every stencil of the step reaches one cell; the device layout
-//   has a one-cell halo), and --plan-view-json (plan-view bundles are not produced here).
+// --plan-view-json writes the dry plan-view bundle of the final state
+// (extract_dry_plan_view + plan_view_bundle_to_json, src/io/plan_view_output.cpp:630-713,
+// 950-1003): terrain height, z_center and the diagnosed cell-centre fields at
+// --plan-view-level, computed on the host with the reference's formulas.
+//
+// One difference is reported as an error rather than run differently: --halo other than
+// 1 (every stencil of the step reaches one cell; the device layout has a one-cell halo).
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
+#include <iomanip>
 #include <cstdlib>
 #include <fstream>
 #include <iostream>
@@ -250,6 +256,68 @@ std::string summary_json(const Summary& s, const std::string& ind) {
   return o.str();
 }
 
+std::string json_string(const std::string& v) {
+  std::string o = "\"";
+  for (char ch : v) {
+    if (ch == '"' || ch == '\\') o += '\\';
+    o += ch;
+  }
+  return o + "\"";
+}
+
+// The dry plan-view bundle at level k of the final state (global owned arrays).
+std::string plan_view_json(const Options& o, const State& s, const std::vector<float>& terrain,
+                           const std::vector<float>& zc, int level) {
+  const Domain& D = o.domain;
+  const int nx = D.nx, ny = D.ny, k = std::clamp(level, 0, D.nz - 1);
+  const size_t plane = (size_t)nx * ny;
+  struct Field {
+    const char* name;
+    const char* units;
+    std::vector<double> v;
+  };
+  std::vector<Field> f = {{"terrain_height", "m", {}}, {"z_center", "m", {}}, {"rho_d", "kg m^-3", {}},
+                          {"theta_m", "K", {}}, {"air_pressure", "Pa", {}}, {"air_temperature", "K", {}},
+                          {"u_velocity", "m s^-1", {}}, {"v_velocity", "m s^-1", {}},
+                          {"wind_speed", "m s^-1", {}}, {"w_velocity", "m s^-1", {}}};
+  double zsum = 0.0;
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const size_t c = (size_t)k * plane + (size_t)j * nx + i;
+      const float rho = s.rho[c], rt = s.rt[c], rr = std::max(rho, 1.0e-6f);
+      const float theta = rt / rr;  // dry_theta_from_conserved (dry_thermo.hpp:21-24)
+      const float ratio = std::max(rho * 287.05f * theta / 100000.0f, 1.0e-6f);
+      const float p = 100000.0f * std::pow(ratio, 1.0f / (1.0f - 0.2854f));
+      const float temp = theta * std::pow(std::max(p, 1.0f) / 100000.0f, 0.2854f);
+      const float uc = 0.5f * (s.u[((size_t)k * ny + j) * (nx + 1) + i] + s.u[((size_t)k * ny + j) * (nx + 1) + i + 1]);
+      const float vc = 0.5f * (s.v[((size_t)k * (ny + 1) + j) * nx + i] + s.v[((size_t)k * (ny + 1) + j + 1) * nx + i]);
+      const float wc = 0.5f * (s.w[c] + s.w[c + plane]);
+      const float u = uc / rr, v = vc / rr, w = wc / rr;
+      const float z = zc[c];
+      zsum += (double)z;
+      const double vals[10] = {terrain.empty() ? 0.0 : (double)terrain[(size_t)j * nx + i], z, rho, theta, p, temp,
+                               u, v, std::sqrt(u * u + v * v), w};
+      for (int q = 0; q < 10; ++q) f[q].v.push_back(vals[q]);
+    }
+  std::ostringstream js;
+  js << std::setprecision(10);
+  js << "{\n  \"schema_version\": " << json_string("gwm-next-plan-view/v1") << ",\n";
+  js << "  \"case\": " << json_string(o.case_kind) << ",\n";
+  js << "  \"steps\": " << o.steps << ",\n  \"dt\": " << o.step.dt << ",\n  \"slice_k\": " << k << ",\n";
+  js << "  \"grid\": {\n    \"nx\": " << nx << ",\n    \"ny\": " << ny << ",\n    \"dx\": " << D.dx
+     << ",\n    \"dy\": " << D.dy << ",\n    \"slice_mean_height_m\": " << zsum / (double)(nx * ny) << "\n  },\n";
+  js << "  \"fields\": [\n";
+  for (size_t n = 0; n < f.size(); ++n) {
+    js << "    {\n      \"name\": " << json_string(f[n].name) << ",\n      \"units\": " << json_string(f[n].units)
+       << ",\n      \"location\": \"cell_center\",\n      \"nx\": " << nx << ",\n      \"ny\": " << ny
+       << ",\n      \"storage\": \"row_major_yx\",\n      \"values\": [";
+    for (size_t q = 0; q < f[n].v.size(); ++q) js << (q ? ", " : "") << f[n].v[q];
+    js << "]\n    }" << (n + 1 < f.size() ? "," : "") << "\n";
+  }
+  js << "  ]\n}";
+  return js.str();
+}
+
 void check(int rc, gwm_b200_ctx* ctx, const char* what) {
   if (rc == GWM_B200_OK) return;
   std::string msg = std::string(what) + " failed with status " + std::to_string(rc);
@@ -267,7 +335,6 @@ int main(int argc, char** argv) {
     const Domain& D = o.domain;
     if (D.nx <= 0 || D.ny <= 0 || D.nz <= 0) throw std::runtime_error("--nx, --ny and --nz must be positive");
     if (D.halo != 1) throw std::runtime_error("only --halo 1 is supported (every stencil of the step reaches one cell)");
-    if (!o.plan_view_json_path.empty()) throw std::runtime_error("--plan-view-json is not supported by this driver");
 
     std::vector<float> terrain((size_t)D.nx * D.ny, 0.0f);
     if (D.terrain_kind == "cosine_mountain") {
@@ -314,6 +381,15 @@ int main(int argc, char** argv) {
       std::ofstream out(o.summary_json_path, std::ios::binary);
       if (!out) throw std::runtime_error("Failed to open summary path: " + o.summary_json_path);
       out << js.str() << "\n";
+    }
+    if (!o.plan_view_json_path.empty()) {
+      std::vector<float> zc(cells);
+      check(gwm_b200_grid_z_center(&grid, zc.data()), nullptr, "grid metrics");
+      const std::string pv = plan_view_json(o, s, D.terrain_kind == "flat" ? std::vector<float>() : terrain, zc,
+                                            o.plan_view_level);
+      std::ofstream out(o.plan_view_json_path, std::ios::binary);
+      if (!out) throw std::runtime_error("Failed to open plan-view output path: " + o.plan_view_json_path);
+      out << pv << "\n";
     }
     return EXIT_SUCCESS;
   } catch (const std::exception& ex) {

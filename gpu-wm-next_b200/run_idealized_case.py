@@ -16,7 +16,8 @@ with a summary of the field's mass and range before and after.
 
 Usage:
     python gpu-wm-next_b200/run_idealized_case.py case.yaml [--steps N] [--dt S]
-        [--fast-substeps N] [--summary-json PATH] [--driver PATH] [--print-command]
+        [--fast-substeps N] [--summary-json PATH] [--plan-view-json PATH] [--plan-view-level K]
+        [--driver PATH] [--print-command]
 """
 import argparse
 import importlib
@@ -51,7 +52,8 @@ def load_case(path):
     return data
 
 
-def driver_command(case, driver, summary_json, steps=None, dt=None, fast_substeps=None):
+def driver_command(case, driver, summary_json, steps=None, dt=None, fast_substeps=None, plan_view_json=None,
+                   plan_view_level=None):
     """The gwm_b200_idealized_driver command line of a dry idealized case file."""
     grid, terrain, init = case.get("grid", {}), case.get("terrain", {}), case.get("initialization", {})
     cmd = [driver, "--case", str(init.get("kind", "density_current"))]
@@ -60,7 +62,8 @@ def driver_command(case, driver, summary_json, steps=None, dt=None, fast_substep
         cmd += ["--terrain-kind", str(terrain["kind"])]
         cmd += [x for k, flag in TERRAIN_KEYS.items() if k in terrain for x in (flag, str(terrain[k]))]
     cmd += [x for k in INIT_KEYS if k in init for x in ("--" + k.replace("_", "-"), str(init[k]))]
-    for flag, value in (("--steps", steps), ("--dt", dt), ("--fast-substeps", fast_substeps)):
+    for flag, value in (("--steps", steps), ("--dt", dt), ("--fast-substeps", fast_substeps),
+                        ("--plan-view-json", plan_view_json), ("--plan-view-level", plan_view_level)):
         if value is not None:
             cmd += [flag, str(value)]
     return cmd + ["--summary-json", summary_json]
@@ -96,6 +99,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--dt", type=float, default=None)
     ap.add_argument("--fast-substeps", type=int, default=None)
+    ap.add_argument("--plan-view-json", default=None, help="also write the dry plan-view bundle here")
+    ap.add_argument("--plan-view-level", type=int, default=None)
     ap.add_argument("--print-command", action="store_true", help="print the driver command and stop")
     args = ap.parse_args(argv)
     case = load_case(args.case_file)
@@ -111,7 +116,8 @@ def main(argv=None):
         gwm = importlib.import_module("gpu-wm-next_b200")
         gwm.build()
         driver = gwm.DRIVER_PATH
-    cmd = driver_command(case, driver, summary_json, args.steps, args.dt, args.fast_substeps)
+    cmd = driver_command(case, driver, summary_json, args.steps, args.dt, args.fast_substeps, args.plan_view_json,
+                         args.plan_view_level)
     print(" ".join(cmd), flush=True)
     if args.print_command:
         return 0

@@ -291,6 +291,9 @@ typedef struct {
 int gwm_b200_scalar_ssprk3(const gwm_b200_scalar_desc* desc, float* q, int nsteps, void* stream);
 
 /* ---- host layout helpers (no device work) --------------------------------- */
+/* Cell-centre heights GridMetrics::z_center (include/gwm/domain/grid_metrics.hpp:87-239:
+ * FP64 compute, FP32 result) of a grid into out (nz, ny, nx), host memory. */
+int gwm_b200_grid_z_center(const gwm_b200_grid_desc* grid, float* out);
 /* Per-rank halo-padded host buffers <-> global owned arrays.  Faces shared by two
  * ranks (and periodic aliases) take the average of both copies on the way in, as the
  * reference's first interface sync does. */

@@ -28,7 +28,6 @@ def _driver(gwm):
     (["--nx", "8", "--ny", "8", "--nz", "4", "--terrain-kind", "agnesi"], "Unsupported terrain kind: agnesi"),
     (["--nx", "8", "--ny", "8", "--nz", "4", "--case", "squall_line"], "Unsupported case kind: squall_line"),
     (["--nx", "8", "--ny", "8", "--nz", "4", "--halo", "2"], "only --halo 1"),
-    (["--nx", "8", "--ny", "8", "--nz", "4", "--plan-view-json", "x.json"], "--plan-view-json"),
     (["--nx"], "Missing value for --nx"),
 ])
 def test_driver_argument_errors(gwm, args, message):
@@ -189,3 +188,52 @@ def test_case_files_run(gwm, tmp_path):
     # upwind SSPRK3 on a periodic grid conserves mass and does not create new extrema
     assert abs(s["final"]["mass"] - s["initial"]["mass"]) <= 1e-3 * abs(s["initial"]["mass"]) + 1e-3
     assert s["initial"]["min"] - 1e-6 <= s["final"]["min"] and s["final"]["max"] <= s["initial"]["max"] + 1e-6
+
+
+@pytest.mark.gpu
+def test_driver_plan_view_bundle(gwm, orc, tmp_path):
+    # extract_dry_plan_view + plan_view_bundle_to_json (plan_view_output.cpp:630-713,
+    # 950-1003) of the final state: the schema, the field list, and every value against
+    # the library's own state diagnosed with the reference's formulas
+    nx, ny, nz, level = 32, 16, 12, 3
+    args = ["--case", "mountain_wave_background", "--nx", str(nx), "--ny", str(ny), "--nz", str(nz),
+            "--z-top", "12000", "--terrain-kind", "cosine_mountain", "--terrain-height", "600",
+            "--terrain-half-width-x", "0.2", "--terrain-half-width-y", "0.4", "--u-background", "8",
+            "--dt", "1", "--fast-substeps", "2", "--steps", "2", "--plan-view-level", str(level)]
+    path = tmp_path / "pv.json"
+    r = subprocess.run([_driver(gwm), *args, "--plan-view-json", str(path)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    pv = json.loads(path.read_text())
+    assert pv["schema_version"] == "gwm-next-plan-view/v1" and pv["case"] == "mountain_wave_background"
+    assert pv["steps"] == 2 and pv["slice_k"] == level and pv["grid"]["nx"] == nx and pv["grid"]["ny"] == ny
+    names = [f["name"] for f in pv["fields"]]
+    assert names == ["terrain_height", "z_center", "rho_d", "theta_m", "air_pressure", "air_temperature",
+                     "u_velocity", "v_velocity", "wind_speed", "w_velocity"]
+    f = {x["name"]: np.asarray(x["values"]).reshape(ny, nx) for x in pv["fields"]}
+    assert all(x["storage"] == "row_major_yx" and x["location"] == "cell_center" for x in pv["fields"])
+    terrain = gwm.build_terrain("cosine_mountain", nx, ny, 1000.0, 1000.0, height=600.0, half_width_x=0.2,
+                                half_width_y=0.4)
+    g = gwm.GridSpec(nx, ny, nz, dx=1000.0, dy=1000.0, z_top=12000.0, terrain=terrain)
+    s0 = gwm.build_case("mountain_wave_background", g, gwm.CaseParams(rho_surface=1.18, theta_ref=300.0,
+                                                                      u_background=8.0))
+    with gwm.Model(g, gwm.MemberSpec(step=gwm.StepConfig(dt=1.0, fast_substeps=2))) as m:
+        m.upload(s0)
+        m.advance_dry_state_ssprk3(2)
+        s = m.download()
+    zc = orc.metrics(orc.GridSpec(nx, ny, nz, dx=1000.0, dy=1000.0, z_top=12000.0,
+                                  terrain=terrain))["z_centers"]
+    rho = s["rho"][level].astype(np.float64)
+    rr = np.maximum(rho, 1e-6)
+    th = s["rho_theta"][level] / rr
+    p = 1e5 * np.maximum(rho * 287.05 * th / 1e5, 1e-6) ** (1.0 / (1.0 - 0.2854))
+    u = 0.5 * (s["u"][level, :, :-1] + s["u"][level, :, 1:]) / rr
+    v = 0.5 * (s["v"][level, :-1, :] + s["v"][level, 1:, :]) / rr
+    w = 0.5 * (s["w"][level] + s["w"][level + 1]) / rr
+    want = {"terrain_height": terrain, "z_center": zc[level], "rho_d": rho, "theta_m": th, "air_pressure": p,
+            "air_temperature": th * (np.maximum(p, 1.0) / 1e5) ** 0.2854, "u_velocity": u, "v_velocity": v,
+            "wind_speed": np.sqrt(u * u + v * v), "w_velocity": w}
+    for k, v_ in want.items():
+        scale = max(np.abs(v_).max(), 1e-3)
+        assert np.abs(f[k] - v_).max() <= 2e-6 * scale, k
+    assert pv["grid"]["slice_mean_height_m"] == pytest.approx(zc[level].mean(), rel=1e-6)
