@@ -703,12 +703,13 @@ int enqueue_rain(gwm_b200_ctx* c, Member& M, int fallout) {
   a.inv_count = inv_count(M);
   if (M.use_surrogate) {
     SurrogateArgs sa{};
-    sa.frags = (const uint2*)M.sur;
-    sa.bias = (const float*)(M.sur + kSurFrags * 32 * sizeof(uint2));
+    sa.weights = (const unsigned char*)M.sur;
+    sa.bias = (const float*)(M.sur + kSurWeightBytes);
     sa.norm = sa.bias + kSurBias;
     sa.range = sa.norm + kMlpNorm;
     sa.stats = (unsigned long long*)(M.sur + 65536);
     sa.work = (int*)(M.sur + 65536 + 128);
+    sa.err = M.err;
     sa.tol_water = M.sur_tol_water;
     sa.tol_energy = M.sur_tol_energy;
     LAUNCH(launch_warm_rain_surrogate(a, sa, c->stream), "warm rain");
@@ -1172,15 +1173,14 @@ int gwm_b200_set_rain_surrogate(gwm_b200_ctx* c, int member, const float* params
     CK(cudaMalloc(&M.sur, 65536 + 256));
     CK(cudaMemset(M.sur + 65536, 0, 256));
   }
-  static_assert(kSurFrags * 32 * sizeof(uint2) + (kSurBias + kMlpNorm + kMlpRange) * sizeof(float) <= 65536,
-                "surrogate buffer");
-  std::vector<uint2> fr(kSurFrags * 32);
+  static_assert(kSurWeightBytes + (kSurBias + kMlpNorm + kMlpRange) * sizeof(float) <= 65536, "surrogate buffer");
+  std::vector<unsigned char> fr(kSurWeightBytes);
   std::vector<float> tail(kSurBias + kMlpNorm + kMlpRange);
-  surrogate_fragments(params, fr.data(), tail.data());
+  surrogate_operands(params, fr.data(), tail.data());
   std::copy(norm, norm + kMlpNorm, tail.begin() + kSurBias);
   std::copy(range, range + kMlpRange, tail.begin() + kSurBias + kMlpNorm);
-  CK(cudaMemcpy(M.sur, fr.data(), fr.size() * sizeof(uint2), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(M.sur + fr.size() * sizeof(uint2), tail.data(), tail.size() * sizeof(float), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(M.sur, fr.data(), fr.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(M.sur + fr.size(), tail.data(), tail.size() * sizeof(float), cudaMemcpyHostToDevice));
   M.use_surrogate = true;
   M.sur_tol_water = tol_water;
   M.sur_tol_energy = tol_energy;

@@ -1,29 +1,44 @@
 // surrogate_rain.cu — warm rain with the learned microphysics (inference).
 //
-// The column sweep of k_warm_rain (warm_rain.cu:36-191 with metric or nominal fallout),
-// with the per-cell microphysics replaced by the trained network on the tensor cores.
-// A warp owns 32 columns and marches down k; at each level its 32 cells are two 16-row
-// tiles of mma.sync.m16n8k16 (BF16 inputs, FP32 accumulation): 7 (padded to 16) -> 64
-// -> 64 -> 64 -> 5 (padded to 8), 76 MMAs per tile.  The weights sit in shared memory
-// as per-lane B fragments; each layer's accumulator fragments become the next layer's
-// A fragments in registers (the C layout of two adjacent 8-column tiles is the A
-// layout of one 16-column k-step), so activations never leave the registers.
-// GELU is the tanh form with the hardware tanh approximation.
+// Two kernels.  The reference applies each cell's microphysics before the rain from
+// above arrives (warm_rain.cu:36-191: the incoming flux is added after micro_step), so
+// all the microphysics can run first and the fallout sweep after it:
+//   1. k_rain_net: the microphysics of every cell, with the network on the 5th-generation
+//      tensor cores (tcgen05), no dependence between levels;
+//   2. k_warm_rain<false> (physics.cu): the plain column sweep with the microphysics
+//      switched off (fallout, FP64 precipitation, theta level sums).
+//
+// k_rain_net.  A CTA of 128 threads takes units of 128 consecutive cells of one (j, k)
+// row from a counter; each thread builds its cell's state and features and applies the
+// activity gate (quiet cells, which the plain scheme leaves exactly unchanged, are not
+// touched).  The active cells are appended to a 256-row ring of layer-1 inputs in shared
+// memory; whenever 128 are waiting, the CTA runs them as one M = 128 tile:
+//   layer 1  [128 x 16] x [16 x 64]   one tcgen05.mma (K = 16: 7 inputs + padding)
+//   layers 2, 3  [128 x 64] x [64 x 64]   four tcgen05.mma each (K = 16 per MMA)
+//   layer 4  [128 x 64] x [64 x 16]   four tcgen05.mma (5 outputs, N padded to 16)
+// with BF16 operands read by the tensor core from shared memory (canonical K-major
+// layout without swizzle: 8 x 16-byte core matrices) and FP32 accumulators in tensor
+// memory (TMEM, 128 columns per CTA).  One thread issues the MMAs and commits them to an
+// mbarrier; after each layer every thread loads its own row from TMEM (tcgen05.ld,
+// thread t = TMEM lane t), adds the bias, applies GELU (tanh form, hardware tanh
+// approximation), and writes the row back as the next layer's BF16 operand.  Each
+// thread then applies the result of its row's cell.
 //
 // Per cell the network gives the condensation, autoconversion and rain-evaporation
 // amounts as fractions of their bounds (the saturation deficit |qv - qs|, the cloud
 // water above the autoconversion threshold, the rain present) and, redundantly, dtheta
 // and dqv.  The fractions are held to their intervals widened by tol_water and turned
 // into amounts c (negative for cloud evaporation), a, e with the caps the plain scheme
-// applies (no more vapour condensed or cloud evaporated than there is), then applied: qv -= c - e, qc += c - a, qr += a - e,
-// theta += L_v/(c_p pi) (c - e); water and energy close by construction.  The cell takes
-// the plain scheme instead when an input lies outside the training range, when a raw
-// fraction lies outside its interval by more than tol_water, or when the network's dqv
-// or dtheta disagree with the amounts by more than tol_water or tol_energy of the
-// cell's exchange plus the output's training spread.  Quiet cells (no condensate, not
-// supersaturated), which the plain scheme leaves unchanged, skip the network.  Fallout
-// is the scheme's explicit flux in both paths, and the column accumulation (what leaves
-// a cell enters the one below, the bottom flux is precipitation) is exact.
+// applies (no more vapour condensed or cloud evaporated than there is), then applied:
+// qv -= c - e, qc += c - a, qr += a - e, theta += L_v/(c_p pi) (c - e); water and
+// energy close by construction.  The cell takes the plain scheme instead when an input
+// lies outside the training range, when a raw fraction lies outside its interval by
+// more than tol_water, or when the network's dqv or dtheta disagree with the amounts by
+// more than tol_water or tol_energy of the cell's exchange plus the output's training
+// spread.
+//
+// Every wait is bounded: if an MMA group does not complete, the kernel records the
+// error word, stops, frees its TMEM and returns.
 #include <algorithm>
 #include <cstring>
 
@@ -31,326 +46,483 @@
 
 #include "surrogate.cuh"
 #include "surrogate_rain.cuh"
+#include "tma.cuh"
 
 namespace gwmb {
 namespace {
 
-__device__ __forceinline__ void mma_bf16(float& c0, float& c1, float& c2, float& c3, unsigned a0, unsigned a1,
-                                         unsigned a2, unsigned a3, unsigned b0, unsigned b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};"
-      : "+f"(c0), "+f"(c1), "+f"(c2), "+f"(c3)
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+constexpr int kNT = 128;             // rows of one tile = TMEM lanes = consumer threads
+constexpr int kProducerWarps = 4;    // warps 0-3 gate and append; warps 4-7 consume tiles
+constexpr int kThreads = kNT + 32 * kProducerWarps;
+constexpr int kTiles = 4;            // tiles in the layer-1 input ring
+constexpr int kTmemCols = 128;       // columns 0-63: hidden layers, 64-79: outputs
+constexpr int kCellVars = 7;         // cell state kept per ring row
+// shared-memory operand layout (bytes): K-major, no swizzle; element (row, k) of a
+// [rows x K] BF16 matrix sits at (row / 8) * SBO + (k / 8) * 128 + (row % 8) * 16 +
+// (k % 8) * 2 with SBO = K / 8 * 128 (LBO = 128 between the K halves of an MMA)
+constexpr int kW1 = 0, kW2 = kW1 + 64 * 16 * 2, kW3 = kW2 + 64 * 64 * 2, kW4 = kW3 + 64 * 64 * 2,
+              kWBytes = kW4 + 16 * 64 * 2;  // 20480
+constexpr int kA1Bytes = kTiles * kNT * 16 * 2, kAhBytes = kNT * 64 * 2;
+constexpr int kDynSmem = kWBytes + kA1Bytes + kAhBytes + 128;  // + alignment slack
+
+__host__ __device__ constexpr int op_offset(int row, int k, int K) {
+  return (row >> 3) * (K / 8 * 128) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
+
+// tcgen05 shared-memory matrix descriptor: start address, LBO, SBO (all >> 4),
+// version 1, no swizzle
+__device__ __forceinline__ uint64_t smem_desc(unsigned addr, unsigned lbo, unsigned sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor, kind::f16: FP32 accumulator, BF16 A and B, both K-major
+__host__ __device__ constexpr unsigned instr_desc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma(unsigned tmem_d, uint64_t a, uint64_t b, unsigned idesc, bool accumulate) {
+  const unsigned acc = accumulate ? 1u : 0u, z = 0u;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// 16 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, float* v) {
+  unsigned r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<const unsigned*>(&v);
 }
-
 __device__ __forceinline__ float tanh_approx(float x) {
   float y;
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-__device__ __forceinline__ float gelu_fast(float z) {
-  return 0.5f * z * (1.0f + tanh_approx(0.7978845608028654f * (z + 0.044715f * z * z * z)));
+// GELU (tanh form) of two pre-activations in FP32, packed as the BF16 operand of the
+// next layer.  (Packed BF16 arithmetic halves the tanh count but moved the shipped
+// network's fallback rate from ~0 to 4 % of the active cells and its surface rain by
+// 20 % on the held-out sounding: the activations need FP32 evaluation.)
+__device__ __forceinline__ unsigned gelu2(float z0, float z1) {
+  const float h0 = 0.5f * z0, h1 = 0.5f * z1;
+  const float t0 = tanh_approx(z0 * fmaf(0.0356774081f, z0 * z0, 0.7978845608f));
+  const float t1 = tanh_approx(z1 * fmaf(0.0356774081f, z1 * z1, 0.7978845608f));
+  return pack_bf16(fmaf(h0, t0, h0), fmaf(h1, t1, h1));
 }
 
-// Two 16-cell tiles (the warp's 32 slots) through the network, interleaved: every
-// weight fragment is loaded once for both tiles and the two tiles' MMA chains are
-// independent.  p[q] (q = 0..3) are this lane's own slot features 2q, 2q+1 packed as
-// BF16 pairs; rows g and g+8 of tile 0 are slots g and g+8, of tile 1 slots 16+g and
-// 24+g.  Returns the output fragments (c0..c3) of the last layer for both tiles.
-__device__ __forceinline__ void mlp_tiles(const uint2* __restrict__ fr, const float* __restrict__ bias,
-                                          const unsigned p[4], int gq, int t, float y0[4], float y1[4]) {
-  unsigned a00 = 0, a01 = 0, a10 = 0, a11 = 0;  // layer 1 A fragments (k 8..15 are padding)
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const unsigned v0 = __shfl_sync(0xffffffffu, p[q], gq), v1 = __shfl_sync(0xffffffffu, p[q], gq + 8);
-    const unsigned v2 = __shfl_sync(0xffffffffu, p[q], 16 + gq), v3 = __shfl_sync(0xffffffffu, p[q], 24 + gq);
-    if (q == t) { a00 = v0; a01 = v1; a10 = v2; a11 = v3; }
-  }
-  const int lane = threadIdx.x & 31;
-  const int c2 = 2 * t;
-  float acc[2][8][4];
-#pragma unroll
-  for (int nt = 0; nt < 8; ++nt) {
-    const float b0 = bias[8 * nt + c2], b1 = bias[8 * nt + c2 + 1];
-    const uint2 w = fr[nt * 32 + lane];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      acc[h][nt][0] = b0; acc[h][nt][1] = b1; acc[h][nt][2] = b0; acc[h][nt][3] = b1;
-    }
-    mma_bf16(acc[0][nt][0], acc[0][nt][1], acc[0][nt][2], acc[0][nt][3], a00, a01, 0u, 0u, w.x, w.y);
-    mma_bf16(acc[1][nt][0], acc[1][nt][1], acc[1][nt][2], acc[1][nt][3], a10, a11, 0u, 0u, w.x, w.y);
-  }
-  auto act = [&](unsigned a[2][4][4]) {
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-      for (int kt = 0; kt < 4; ++kt) {
-        a[h][kt][0] = pack_bf16(gelu_fast(acc[h][2 * kt][0]), gelu_fast(acc[h][2 * kt][1]));
-        a[h][kt][1] = pack_bf16(gelu_fast(acc[h][2 * kt][2]), gelu_fast(acc[h][2 * kt][3]));
-        a[h][kt][2] = pack_bf16(gelu_fast(acc[h][2 * kt + 1][0]), gelu_fast(acc[h][2 * kt + 1][1]));
-        a[h][kt][3] = pack_bf16(gelu_fast(acc[h][2 * kt + 1][2]), gelu_fast(acc[h][2 * kt + 1][3]));
-      }
-  };
-#pragma unroll
-  for (int L = 0; L < 2; ++L) {
-    unsigned a[2][4][4];
-    act(a);
-    const uint2* f = fr + (8 + L * 32) * 32;
-    const float* bb = bias + 64 * (L + 1);
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      const float b0 = bb[8 * nt + c2], b1 = bb[8 * nt + c2 + 1];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        acc[h][nt][0] = b0; acc[h][nt][1] = b1; acc[h][nt][2] = b0; acc[h][nt][3] = b1;
-      }
-#pragma unroll
-      for (int kt = 0; kt < 4; ++kt) {
-        const uint2 w = f[(kt * 8 + nt) * 32 + lane];
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-          mma_bf16(acc[h][nt][0], acc[h][nt][1], acc[h][nt][2], acc[h][nt][3], a[h][kt][0], a[h][kt][1],
-                   a[h][kt][2], a[h][kt][3], w.x, w.y);
-      }
-    }
-  }
-  unsigned a[2][4][4];
-  act(a);
-  const float b0 = bias[192 + c2], b1 = bias[192 + c2 + 1];
-  y0[0] = b0; y0[1] = b1; y0[2] = b0; y0[3] = b1;
-  y1[0] = b0; y1[1] = b1; y1[2] = b0; y1[3] = b1;
-  const uint2* f = fr + 72 * 32;
-#pragma unroll
-  for (int kt = 0; kt < 4; ++kt) {
-    const uint2 w = f[kt * 32 + lane];
-    mma_bf16(y0[0], y0[1], y0[2], y0[3], a[0][kt][0], a[0][kt][1], a[0][kt][2], a[0][kt][3], w.x, w.y);
-    mma_bf16(y1[0], y1[1], y1[2], y1[3], a[1][kt][0], a[1][kt][1], a[1][kt][2], a[1][kt][3], w.x, w.y);
-  }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+// barrier of the four consumer warps (id 1; id 0 is __syncthreads)
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
-// Microphysics of every cell with the network (the first of the two kernels of the
-// surrogate warm rain; the fallout sweep is k_warm_rain without microphysics).
-// A warp walks chunks of 32 consecutive cells of one (j, k) row.  Each lane builds its
-// cell's state and features and applies the activity gate; quiet cells are left as
-// they are (no store).  The active cells of successive chunks are packed into the
-// warp's 32 slots (shared memory); whenever the slots fill, the warp runs them through
-// the network as two 16-row MMA tiles and every lane applies the result of its slot.
-// The network therefore runs on active cells only, in dense tiles, and the work has no
-// dependence between levels.
-constexpr int kNW = 4, kNT = 32 * kNW;
-
-__global__ void __launch_bounds__(kNT, 3) k_rain_net(const RainArgs a, const SurrogateArgs s) {
-  __shared__ uint2 s_fr[kSurFrags * 32];
-  __shared__ float s_bias[kSurBias];
+__global__ void __launch_bounds__(kThreads, 3) k_rain_net(const RainArgs a, const SurrogateArgs s) {
+  extern __shared__ unsigned char s_dyn[];
+  __shared__ __align__(16) float s_bias[kSurBias];
   __shared__ float s_norm[kMlpNorm + kMlpRange];
-  __shared__ int s_ij[kNW][32], s_kf[kNW][32];
-  __shared__ unsigned s_pk[kNW][4][32];
+  __shared__ float s_rxs[kMlpIn];  // reciprocals of the input scales
+  __shared__ int s_ij[kTiles * kNT], s_kf[kTiles * kNT];
+  // each ring row's cell state, so that the consumers apply the network without
+  // re-reading or re-deriving it: rho, theta, qv, qc, qr, latent heat, saturation
+  __shared__ float s_cell[kCellVars][kTiles * kNT];
   __shared__ unsigned long long s_st[kSurStats];
-  for (int q = threadIdx.x; q < kSurFrags * 32; q += kNT) s_fr[q] = s.frags[q];
-  for (int q = threadIdx.x; q < kSurBias; q += kNT) s_bias[q] = s.bias[q];
-  for (int q = threadIdx.x; q < kMlpNorm; q += kNT) s_norm[q] = s.norm[q];
-  for (int q = threadIdx.x; q < kMlpRange; q += kNT) s_norm[kMlpNorm + q] = s.range[q];
-  if (threadIdx.x < kSurStats) s_st[threadIdx.x] = 0ull;
+  __shared__ __align__(8) uint64_t s_full[kTiles];  // one arrival per row written into a tile
+  __shared__ __align__(8) uint64_t s_mma;           // tcgen05.commit of one layer
+  __shared__ unsigned s_tmem;
+  __shared__ int s_tail, s_consumed, s_prod_done, s_fail, s_cmd, s_cfail;
+  unsigned char* const base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
+  unsigned char* const sw = base;                       // weights, canonical layout
+  unsigned char* const sa1 = base + kWBytes;            // layer-1 input ring, kTiles tiles
+  unsigned char* const sah = base + kWBytes + kA1Bytes; // hidden-layer operand
+
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  {  // weights (16-byte copies), biases, normalisation
+    const uint4* src = reinterpret_cast<const uint4*>(s.weights);
+    uint4* dst = reinterpret_cast<uint4*>(sw);
+    for (int q = tid; q < kWBytes / 16; q += kThreads) dst[q] = src[q];
+  }
+  for (int q = tid; q < kSurBias; q += kThreads) s_bias[q] = s.bias[q];
+  for (int q = tid; q < kMlpNorm; q += kThreads) s_norm[q] = s.norm[q];
+  for (int q = tid; q < kMlpRange; q += kThreads) s_norm[kMlpNorm + q] = s.range[q];
+  for (int q = tid; q < kMlpIn; q += kThreads) s_rxs[q] = 1.0f / s.norm[kMlpIn + q];
+  if (tid < kSurStats) s_st[tid] = 0ull;
+  if (tid == 0) {
+    for (int t = 0; t < kTiles; ++t) mbar_init(&s_full[t], kNT);
+    mbar_init(&s_mma, 1);
+    mbar_fence_init();
+    s_tail = 0;
+    s_consumed = 0;
+    s_prod_done = 0;
+    s_fail = 0;
+  }
+  if (wid == 0) {  // TMEM for the CTA's accumulators
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_proxy_async_smem();  // the weight copies are read by the tensor core
+  tc_fence_before();
   __syncthreads();
-
+  tc_fence_after();
+  const unsigned tmem = s_tmem;
   const Geom& g = a.g;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, gq = lane >> 2, t = lane & 3;
-  const unsigned lt = (1u << lane) - 1u;
-  const MicroParams mp{a.dt, a.relax, a.thr, a.rate, a.evap, a.latent};
-  const float* xm = s_norm;
-  const float* xs = s_norm + kMlpIn;
-  const float* ym = s_norm + 2 * kMlpIn;
-  const float* ys = s_norm + 2 * kMlpIn + kMlpOut;
-  const float* xmin = s_norm + kMlpNorm;
-  const float* xmax = s_norm + kMlpNorm + kMlpIn;
+  volatile int* const vfail = &s_fail;
 
-  // the slots' cells through the network; lane L applies slot L (L < count)
-  auto run = [&](int count) {
-    __syncwarp();
-    const bool mine = lane < count;
-    unsigned p[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) p[q] = mine ? s_pk[wid][q][lane] : 0u;
-    const int ij = s_ij[wid][lane], kf = s_kf[wid][lane];
-    __syncwarp();
-    // tile 0 holds slots 0-15, tile 1 slots 16-31; row r of a tile sits in lanes
-    // 4 (r % 8) + o/2 of its output fragment, and each lane gathers its own row
-    float y0[4], y1[4];
-    mlp_tiles(s_fr, s_bias, p, gq, t, y0, y1);
-    float out[6];
-    {
-      const int r = lane & 15;
-      const int src = 4 * (r & 7);
-      const bool hi = r >= 8, t1 = lane >= 16;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const float u0 = __shfl_sync(0xffffffffu, y0[0], src + j), u1 = __shfl_sync(0xffffffffu, y0[1], src + j);
-        const float u2 = __shfl_sync(0xffffffffu, y0[2], src + j), u3 = __shfl_sync(0xffffffffu, y0[3], src + j);
-        const float v0 = __shfl_sync(0xffffffffu, y1[0], src + j), v1 = __shfl_sync(0xffffffffu, y1[1], src + j);
-        const float v2 = __shfl_sync(0xffffffffu, y1[2], src + j), v3 = __shfl_sync(0xffffffffu, y1[3], src + j);
-        out[2 * j] = t1 ? (hi ? v2 : v0) : (hi ? u2 : u0);
-        out[2 * j + 1] = t1 ? (hi ? v3 : v1) : (hi ? u3 : u1);
-      }
-    }
-    unsigned fl = 0u;  // this cell's check failures: bit 0 fallback, 2 range, 3 fraction, 4 water, 5 energy
-    if (mine) {
-    const int i = ij & 0xffff, jj = ij >> 16, k = kf & 0xffff;
-    const bool in_range = (kf >> 16) != 0;
-    const int o = gidx(g, i, jj, k);
-    const float rho_d = __ldg(a.rho + o);
-    MicroCell mc = micro_state(rho_d, a.rt[o], a.qv[o], a.qc[o], a.qr[o]);
-    const float qs = qsat(mc.temp, mc.p);
-    float dq[kMlpOut];
-#pragma unroll
-    for (int q = 0; q < kMlpOut; ++q) dq[q] = out[q] * ys[q] + ym[q];
-    // The fractions are used inside [-tol_water, hi + tol_water], not clipped to
-    // [0, hi]: the plain scheme's efficiency often sits on an end of its interval (full
-    // adjustment, no rain evaporation in saturated air), and clipping the network's
-    // noise there would bias the amounts.  Small reverse amounts stay bounded by the caps
-    // below, which keep every mixing ratio non-negative.
-    const float lat = a.latent ? mc.lh : 0.0f;
-    const float tw = s.tol_water, te = s.tol_energy;
-    const float fc_hi = fmaxf(fmaxf(a.relax, 0.0f), 1.0f);
-    const float fc = fminf(fmaxf(dq[0], -tw), fc_hi + tw);
-    const float fa = fminf(fmaxf(dq[1], 0.0f), 1.0f);
-    const float fe = fminf(fmaxf(dq[2], -tw), 1.0f);
-    const float d = mc.qv - qs;
-    const float c_p = (d > 0.0f || mc.qc > 0.0f) ? fminf(fmaxf(fc * d, -mc.qc), mc.qv) : 0.0f;
-    const float qc_mid = mc.qc + c_p;
-    const float a_p = a.rate > 0.0f ? fa * fmaxf(qc_mid - a.thr, 0.0f) : 0.0f;
-    const float qr_mid = mc.qr + a_p;
-    const float e_p = a.evap > 0.0f ? fe * qr_mid : 0.0f;
-    const float qv1 = mc.qv - c_p + e_p;
-    const bool frac_ok = dq[0] >= -tw && dq[0] <= fc_hi + tw && dq[1] >= -tw && dq[1] <= 1.0f + tw &&
-                         dq[2] >= -tw && dq[2] <= 1.0f + tw && qv1 >= 0.0f;
-    const bool water_ok = fabsf(dq[4] - (e_p - c_p)) <= tw * (fabsf(c_p) + fabsf(e_p) + ys[4]);
-    const bool energy_ok = fabsf(dq[3] - lat * (c_p - e_p)) <= te * (lat * fabsf(c_p - e_p) + ys[3]);
-    const bool ok = in_range && frac_ok && water_ok && energy_ok;
-    fl = (ok ? 0u : 1u) | (in_range ? 0u : 4u) | (frac_ok ? 0u : 8u) | (water_ok ? 0u : 16u) |
-         (energy_ok ? 0u : 32u);
-    float th, qv, qc, qr;
-    if (ok) {
-      th = mc.th + lat * (c_p - e_p);
-      qv = qv1;
-      qc = fmaxf(qc_mid - a_p, 0.0f);
-      qr = fmaxf(qr_mid - e_p, 0.0f);
-    } else {
-      micro_step(mc, mp);
-      th = mc.th;
-      qv = mc.qv;
-      qc = mc.qc;
-      qr = mc.qr;
-    }
-    const float rho = mc.rho;
-    const bool edge = (g.per_x && (i <= 1 || i >= g.nx - 2)) || (g.per_y && (jj <= 1 || jj >= g.ny - 2));
-    store_tile(a.qv, g, kCell, i, jj, k, rho * qv, edge);
-    store_tile(a.qc, g, kCell, i, jj, k, rho * qc, edge);
-    store_tile(a.qr, g, kCell, i, jj, k, rho * qr, edge);
-    store_tile(a.rt, g, kCell, i, jj, k, rho * th, edge);
-    }
-    if (lane == 0) atomicAdd(&s_st[1], (unsigned long long)count);
-#pragma unroll
-    for (int q = 0; q < kSurStats; ++q) {
-      if (q == 1) continue;
-      const unsigned b = __ballot_sync(0xffffffffu, (fl >> q) & 1u);
-      if (lane == 0 && b) atomicAdd(&s_st[q], (unsigned long long)__popc(b));
-    }
-  };
-
-  // a warp takes whole (j, k) rows and walks their 32-cell chunks in x, loading the next
-  // chunk's five fields while the current one is processed
-  const int cx = (g.nx + 31) >> 5;
-  const int rows = g.ny * g.nz;
-  int cnt = 0;  // filled slots (warp-uniform)
-  for (;;) {
-    // rows are taken from a shared counter: the active cells cluster in a few levels, and
-    // a static split would leave the warps that drew cloudy rows working alone at the end
-    int row = 0;
-    if (lane == 0) row = atomicAdd(s.work, 1);
-    row = __shfl_sync(0xffffffffu, row, 0);
-    if (row >= rows) break;
-    const int j = row % g.ny, k = row / g.ny;
-    const int obase = gidx(g, 0, j, k);
-    float f_rho = 0.f, f_rt = 0.f, f_qv = 0.f, f_qc = 0.f, f_qr = 0.f;
-    auto fetch = [&](int ci) {
-      const int ii = ci * 32 + lane;
-      if (ci < cx && ii < g.nx) {
-        const int o = obase + ii;
-        f_rho = __ldg(a.rho + o); f_rt = a.rt[o]; f_qv = a.qv[o]; f_qc = a.qc[o]; f_qr = a.qr[o];
-      }
-    };
-    fetch(0);
-    for (int ci = 0; ci < cx; ++ci) {
-      const int i = ci * 32 + lane;
-      const float rho_d = f_rho, rt = f_rt, rqv = f_qv, rqc = f_qc, rqr = f_qr;
-      fetch(ci + 1);
-      bool net = false, in_range = true;
-      unsigned p[4] = {0u, 0u, 0u, 0u};
-      if (i < g.nx) {
-        // activity gate: with no cloud or rain water and no supersaturation the plain
-        // scheme leaves the cell exactly as it is (micro_step takes none of its branches).
-        // A cell without condensate that a fast-math estimate finds clearly subsaturated
-        // (vapour below 0.999 of saturation; the estimate's error is ~1e-6) is quiet
-        // without the exact state; every other cell is decided on the exact state.
-        bool exact = rqc > 0.0f || rqr > 0.0f;
-        if (!exact) {
-          const float rho = fmaxf(rho_d, 1.0e-6f), ir = __fdividef(1.0f, rho);
-          const float ratio = fmaxf(rt * (kRd / kP0), 1.0e-6f);
-          const float p_ = kP0 * __powf(ratio, 1.0f / (1.0f - kKappa));
-          const float temp = rt * ir * __powf(fmaxf(p_ * (1.0f / kP0), 1.0e-6f), kKappa);
-          const float tc = temp - 273.15f;
-          const float es = 611.2f * __expf(__fdividef(17.67f * tc, fmaxf(tc + 243.5f, 1.0e-6f)));
-          const float eps = kRd / kRv;
-          const float qs = fminf(fmaxf(__fdividef(eps * es, fmaxf(p_ - (1.0f - eps) * es, 1000.0f)), 0.0f), 0.05f);
-          exact = !(fmaxf(rqv * ir, 0.0f) < qs * (1.0f - 1.0e-3f));
+  if (wid < kProducerWarps) {
+    // ---------------- producers: gate the cells of whole (j, k) rows, append the active
+    // ones to the ring (rows are taken from a counter: the active cells cluster in a few
+    // levels, and a static split would leave some warps working alone at the end)
+    const float* xm = s_norm;
+    const float* xmin = s_norm + kMlpNorm;
+    const float* xmax = s_norm + kMlpNorm + kMlpIn;
+    const int cx = (g.nx + 31) >> 5, rows = g.ny * g.nz;
+    volatile int* const vconsumed = &s_consumed;
+    bool stop = false;
+    while (!stop) {
+      int row = 0;
+      if (lane == 0) row = *vfail ? rows : atomicAdd(s.work, 1);
+      row = __shfl_sync(0xffffffffu, row, 0);  // warp-uniform
+      if (row >= rows) break;
+      // consecutive rows walk the levels: the active cells cluster in a few levels, and
+      // a CTA that took a level at a time would alternate between gating-bound and
+      // network-bound stretches instead of overlapping the two
+      const int k = row % g.nz, j = row / g.nz;
+      const int obase = gidx(g, 0, j, k);
+      float f_rho = 0.f, f_rt = 0.f, f_qv = 0.f, f_qc = 0.f, f_qr = 0.f;
+      auto fetch = [&](int ci) {  // the next chunk's five fields, loaded ahead
+        const int ii = ci * 32 + lane;
+        if (ci < cx && ii < g.nx) {
+          const int o = obase + ii;
+          f_rho = __ldg(a.rho + o); f_rt = a.rt[o]; f_qv = a.qv[o]; f_qc = a.qc[o]; f_qr = a.qr[o];
         }
-        if (exact) {
-          const MicroCell mc = micro_state(rho_d, rt, rqv, rqc, rqr);
-          net = !(mc.qc == 0.0f && mc.qr == 0.0f && !(mc.qv > qsat(mc.temp, mc.p)));
-          if (net) {
-            float x[kMlpIn];
-            rain_features(mc, rho_d, a.dt, x);
-            float xn[8];
-  #pragma unroll
-            for (int f = 0; f < kMlpIn; ++f) {
-              in_range = in_range && x[f] >= xmin[f] && x[f] <= xmax[f];
-              xn[f] = (x[f] - xm[f]) / xs[f];
+      };
+      fetch(0);
+      for (int ci = 0; ci < cx; ++ci) {
+        const int i = ci * 32 + lane;
+        const float rho_d = f_rho, rt = f_rt, rqv = f_qv, rqc = f_qc, rqr = f_qr;
+        fetch(ci + 1);
+        bool net = false, in_range = true;
+        float xn[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float cv[kCellVars];
+        if (i < g.nx) {
+          // activity gate: with no cloud or rain water and no supersaturation the plain
+          // scheme leaves the cell exactly as it is (micro_step takes none of its
+          // branches).  A cell without condensate that a fast-math estimate finds clearly
+          // subsaturated (vapour below 0.999 of saturation; the estimate's error is
+          // ~1e-6) is quiet without the exact state; every other cell is decided on the
+          // exact state.
+          bool exact = rqc > 0.0f || rqr > 0.0f;
+          if (!exact) {
+            const float rho = fmaxf(rho_d, 1.0e-6f), ir = __fdividef(1.0f, rho);
+            const float ratio = fmaxf(rt * (kRd / kP0), 1.0e-6f);
+            const float p_ = kP0 * __powf(ratio, 1.0f / (1.0f - kKappa));
+            const float temp = rt * ir * __powf(fmaxf(p_ * (1.0f / kP0), 1.0e-6f), kKappa);
+            const float tc = temp - 273.15f;
+            const float es = 611.2f * __expf(__fdividef(17.67f * tc, fmaxf(tc + 243.5f, 1.0e-6f)));
+            const float eps = kRd / kRv;
+            const float qs = fminf(fmaxf(__fdividef(eps * es, fmaxf(p_ - (1.0f - eps) * es, 1000.0f)), 0.0f), 0.05f);
+            exact = !(fmaxf(rqv * ir, 0.0f) < qs * (1.0f - 1.0e-3f));
+          }
+          if (exact) {
+            const MicroCell mc = micro_state(rho_d, rt, rqv, rqc, rqr);
+            const float qs = qsat(mc.temp, mc.p);
+            net = !(mc.qc == 0.0f && mc.qr == 0.0f && !(mc.qv > qs));
+            if (net) {
+              cv[0] = mc.rho; cv[1] = mc.th; cv[2] = mc.qv; cv[3] = mc.qc; cv[4] = mc.qr; cv[5] = mc.lh; cv[6] = qs;
+              float x[kMlpIn];
+              rain_features(mc, rho_d, a.dt, x);
+#pragma unroll
+              for (int f = 0; f < kMlpIn; ++f) {
+                in_range = in_range && x[f] >= xmin[f] && x[f] <= xmax[f];
+                xn[f] = (x[f] - xm[f]) * s_rxs[f];
+              }
             }
-            xn[7] = 0.0f;
-  #pragma unroll
-            for (int q = 0; q < 4; ++q) p[q] = pack_bf16(xn[2 * q], xn[2 * q + 1]);
           }
         }
-      }
-      const unsigned m = __ballot_sync(0xffffffffu, net);
-      if (m == 0u) continue;
-      const int r = __popc(m & lt), n = __popc(m);
-      auto put = [&](int slot) {
-  #pragma unroll
-        for (int q = 0; q < 4; ++q) s_pk[wid][q][slot] = p[q];
-        s_ij[wid][slot] = i | (j << 16);
-        s_kf[wid][slot] = k | (in_range ? 0x10000 : 0);
-      };
-      if (net && cnt + r < 32) put(cnt + r);
-      if (cnt + n >= 32) {
-        run(32);
-        if (net && cnt + r >= 32) put(cnt + r - 32);
-        cnt = cnt + n - 32;
-      } else {
-        cnt += n;
+        const unsigned m = __ballot_sync(0xffffffffu, net);
+        if (m == 0u) continue;
+        const int n = __popc(m);
+        int first = 0, bad = 0;
+        if (lane == 0) {
+          first = atomicAdd(&s_tail, n);
+          // ring space: the last row must lie within kTiles tiles of the oldest unconsumed
+          const int need = (first + n - 1) / kNT - kTiles;
+          unsigned spins = 0;
+          while (*vconsumed <= need && !(bad = *vfail)) {
+            if (++spins > kMaxSpin) {
+              atomicExch(&s_fail, 1);
+              atomicExch(s.err, 1);
+              bad = 1;
+              break;
+            }
+            __nanosleep(64);
+          }
+        }
+        // lane 0's decision for the whole warp: rows are written only into reserved space
+        first = __shfl_sync(0xffffffffu, first, 0);
+        if (__shfl_sync(0xffffffffu, bad, 0)) {
+          stop = true;
+          break;
+        }
+        if (net) {
+          const int slot = first + __popc(m & ((1u << lane) - 1u));
+          const int pos = slot & (kTiles * kNT - 1);
+          uint4 lo;
+          lo.x = pack_bf16(xn[0], xn[1]);
+          lo.y = pack_bf16(xn[2], xn[3]);
+          lo.z = pack_bf16(xn[4], xn[5]);
+          lo.w = pack_bf16(xn[6], 0.0f);
+          *reinterpret_cast<uint4*>(sa1 + op_offset(pos, 0, 16)) = lo;
+          *reinterpret_cast<uint4*>(sa1 + op_offset(pos, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);  // padding
+          s_ij[pos] = i | (j << 16);
+          s_kf[pos] = k | (in_range ? 0x10000 : 0);
+#pragma unroll
+          for (int q = 0; q < kCellVars; ++q) s_cell[q][pos] = cv[q];
+          fence_proxy_async_smem();  // the row is read by the tensor core
+          mbar_arrive(&s_full[(slot / kNT) % kTiles]);
+        }
       }
     }
+    __syncwarp();  // every lane's rows are written before lane 0 reports the warp done
+    if (lane == 0) {
+      __threadfence_block();
+      atomicAdd(&s_prod_done, 1);
+    }
+  } else {
+    // ---------------- consumers: whole tiles through the network, then the cells
+    const int ct = tid - kProducerWarps * 32;               // 0..127: the tile row and TMEM lane
+    const unsigned lane_addr = tmem + ((unsigned)((wid - kProducerWarps) * 32) << 16);
+    const unsigned w_addr = smem_u32(sw), a1_addr = smem_u32(sa1), ah_addr = smem_u32(sah);
+    const unsigned idesc64 = instr_desc(128, 64), idesc16 = instr_desc(128, 16);
+    const MicroParams mp{a.dt, a.relax, a.thr, a.rate, a.evap, a.latent};
+    const float* ym = s_norm + 2 * kMlpIn;
+    const float* ys = s_norm + 2 * kMlpIn + kMlpOut;
+    volatile int* const vdone = &s_prod_done;
+    unsigned phase = 0, failed_phase = 0;
+    bool failed = false;  // consumer-uniform
+    // one committed MMA group: wait (bounded), then order TMEM reads after it
+    auto wait_mma = [&]() {
+      const bool ok = mbar_wait(&s_mma, phase);
+      if (ct == 0) s_cfail = 0;
+      consumer_sync();
+      if (!ok) s_cfail = 1;
+      consumer_sync();
+      if (s_cfail) {
+        if (!failed) failed_phase = phase;
+        if (!failed && ct == 0) {
+          atomicExch(&s_fail, 1);
+          atomicExch(s.err, 1);
+        }
+        failed = true;
+      }
+      phase ^= 1u;
+      tc_fence_after();
+    };
+    // this thread's row of D (64 columns) + bias -> GELU -> BF16 operand row
+    auto hidden_epilogue = [&](const float* bias) {
+      float v[32];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {  // 32 columns per TMEM wait
+        tmem_ld16(lane_addr + 32 * c, v);
+        tmem_ld16(lane_addr + 32 * c + 16, v + 16);
+        tmem_wait_ld();
+        const float4* b4 = reinterpret_cast<const float4*>(bias + 32 * c);
+#pragma unroll
+        for (int q = 0; q < 32; q += 8) {
+          const float4 ba = b4[q / 4], bb = b4[q / 4 + 1];
+          uint4 w;
+          w.x = gelu2(v[q + 0] + ba.x, v[q + 1] + ba.y);
+          w.y = gelu2(v[q + 2] + ba.z, v[q + 3] + ba.w);
+          w.z = gelu2(v[q + 4] + bb.x, v[q + 5] + bb.y);
+          w.w = gelu2(v[q + 6] + bb.z, v[q + 7] + bb.w);
+          *reinterpret_cast<uint4*>(sah + op_offset(ct, 32 * c + q, 64)) = w;
+        }
+      }
+      fence_proxy_async_smem();
+      tc_fence_before();
+      consumer_sync();
+    };
+    for (int t = 0;; ++t) {
+      const int pos = t % kTiles;
+      if (ct == 0) {  // a full tile, or the remainder once every producer has finished
+        int cmd = -1;
+        for (unsigned spins = 0; spins < kMaxSpin; ++spins) {
+          if (*vfail) { cmd = 0; break; }  // a producer gave up: reserved rows may be unwritten
+          if (mbar_try_wait(&s_full[pos], (t / kTiles) & 1)) { cmd = kNT; break; }
+          if (*vdone == kProducerWarps) {
+            __threadfence_block();
+            // a producer that gave up set the flag before it reported itself done
+            const int rem = *vfail ? 0 : *static_cast<volatile int*>(&s_tail) - t * kNT;
+            cmd = rem >= kNT ? kNT : (rem > 0 ? rem : 0);
+            break;
+          }
+          __nanosleep(32);
+        }
+        if (cmd < 0) {
+          atomicExch(&s_fail, 1);
+          atomicExch(s.err, 1);
+          cmd = 0;
+        }
+        s_cmd = cmd;
+      }
+      consumer_sync();
+      const int valid = s_cmd;
+      consumer_sync();  // every consumer has read s_cmd before it is written again
+      if (valid == 0 || failed) break;
+      tc_fence_after();
+      if (ct == 0) {  // layer 1: K = 16, one MMA
+        umma(tmem, smem_desc(a1_addr + pos * (kNT * 32), 128, 256), smem_desc(w_addr + kW1, 128, 256), idesc64,
+             false);
+        umma_commit(&s_mma);
+      }
+      wait_mma();
+      if (!failed) hidden_epilogue(s_bias);
+      for (int L = 0; L < 2 && !failed; ++L) {  // layers 2 and 3
+        if (ct == 0) {
+          tc_fence_after();
+          const unsigned wl = w_addr + (L == 0 ? kW2 : kW3);
+          for (int kt = 0; kt < 4; ++kt)
+            umma(tmem, smem_desc(ah_addr + 256 * kt, 128, 1024), smem_desc(wl + 256 * kt, 128, 1024), idesc64, kt > 0);
+          umma_commit(&s_mma);
+        }
+        wait_mma();
+        if (!failed) hidden_epilogue(s_bias + 64 * (L + 1));
+      }
+      if (!failed) {  // layer 4: N = 16 into columns 64-79
+        if (ct == 0) {
+          tc_fence_after();
+          for (int kt = 0; kt < 4; ++kt)
+            umma(tmem + 64, smem_desc(ah_addr + 256 * kt, 128, 1024), smem_desc(w_addr + kW4 + 256 * kt, 128, 1024),
+                 idesc16, kt > 0);
+          umma_commit(&s_mma);
+        }
+        wait_mma();
+      }
+      float out[16];
+      if (!failed) {
+        tmem_ld16(lane_addr + 64, out);
+        tmem_wait_ld();
+      }
+      tc_fence_before();
+      int i = 0, jj = 0, k = 0, kf = 0;
+      if (ct < valid && !failed) {
+        const int ij = s_ij[pos * kNT + ct];
+        kf = s_kf[pos * kNT + ct];
+        i = ij & 0xffff;
+        jj = (ij >> 16) & 0xffff;
+        k = kf & 0xffff;
+      }
+      // the bounds test is never false for a written row
+      const bool mine = ct < valid && !failed && i < g.nx && jj < g.ny && k < g.nz;
+      unsigned fl = 0u;  // this cell's check failures: bit 0 fallback, 2 range, 3 fraction, 4 water, 5 energy
+      if (mine) {
+        const bool in_range = (kf >> 16) != 0;
+        const int slot = pos * kNT + ct;
+        MicroCell mc;
+        mc.rho = s_cell[0][slot];
+        mc.th = s_cell[1][slot];
+        mc.qv = s_cell[2][slot];
+        mc.qc = s_cell[3][slot];
+        mc.qr = s_cell[4][slot];
+        mc.lh = s_cell[5][slot];
+        const float qs = s_cell[6][slot];
+        float dq[kMlpOut];
+#pragma unroll
+        for (int q = 0; q < kMlpOut; ++q) dq[q] = (out[q] + s_bias[192 + q]) * ys[q] + ym[q];
+        // The fractions are used inside [-tol_water, hi + tol_water], not clipped to
+        // [0, hi]: the plain scheme's efficiency often sits on an end of its interval
+        // (full adjustment, no rain evaporation in saturated air), and clipping the
+        // network's noise there would bias the amounts.  Small reverse amounts stay
+        // bounded by the caps below, which keep every mixing ratio non-negative.
+        const float lat = a.latent ? mc.lh : 0.0f;
+        const float tw = s.tol_water, te = s.tol_energy;
+        const float fc_hi = fmaxf(fmaxf(a.relax, 0.0f), 1.0f);
+        const float fc = fminf(fmaxf(dq[0], -tw), fc_hi + tw);
+        const float fa = fminf(fmaxf(dq[1], 0.0f), 1.0f);
+        const float fe = fminf(fmaxf(dq[2], -tw), 1.0f);
+        const float d = mc.qv - qs;
+        const float c_p = (d > 0.0f || mc.qc > 0.0f) ? fminf(fmaxf(fc * d, -mc.qc), mc.qv) : 0.0f;
+        const float qc_mid = mc.qc + c_p;
+        const float a_p = a.rate > 0.0f ? fa * fmaxf(qc_mid - a.thr, 0.0f) : 0.0f;
+        const float qr_mid = mc.qr + a_p;
+        const float e_p = a.evap > 0.0f ? fe * qr_mid : 0.0f;
+        const float qv1 = mc.qv - c_p + e_p;
+        const bool frac_ok = dq[0] >= -tw && dq[0] <= fc_hi + tw && dq[1] >= -tw && dq[1] <= 1.0f + tw &&
+                             dq[2] >= -tw && dq[2] <= 1.0f + tw && qv1 >= 0.0f;
+        const bool water_ok = fabsf(dq[4] - (e_p - c_p)) <= tw * (fabsf(c_p) + fabsf(e_p) + ys[4]);
+        const bool energy_ok = fabsf(dq[3] - lat * (c_p - e_p)) <= te * (lat * fabsf(c_p - e_p) + ys[3]);
+        const bool ok = in_range && frac_ok && water_ok && energy_ok;
+        fl = (ok ? 0u : 1u) | (in_range ? 0u : 4u) | (frac_ok ? 0u : 8u) | (water_ok ? 0u : 16u) |
+             (energy_ok ? 0u : 32u);
+        float th, qv, qc, qr;
+        if (ok) {
+          th = mc.th + lat * (c_p - e_p);
+          qv = qv1;
+          qc = fmaxf(qc_mid - a_p, 0.0f);
+          qr = fmaxf(qr_mid - e_p, 0.0f);
+        } else {  // the plain scheme from the cell's stored state
+          const int o = gidx(g, i, jj, k);
+          mc = micro_state(__ldg(a.rho + o), a.rt[o], a.qv[o], a.qc[o], a.qr[o]);
+          micro_step(mc, mp);
+          th = mc.th;
+          qv = mc.qv;
+          qc = mc.qc;
+          qr = mc.qr;
+        }
+        const float rho = mc.rho;
+        const bool edge = (g.per_x && (i <= 1 || i >= g.nx - 2)) || (g.per_y && (jj <= 1 || jj >= g.ny - 2));
+        store_tile(a.qv, g, kCell, i, jj, k, rho * qv, edge);
+        store_tile(a.qc, g, kCell, i, jj, k, rho * qc, edge);
+        store_tile(a.qr, g, kCell, i, jj, k, rho * qr, edge);
+        store_tile(a.rt, g, kCell, i, jj, k, rho * th, edge);
+      }
+      const unsigned used = __ballot_sync(0xffffffffu, mine);
+      if (lane == 0 && used) atomicAdd(&s_st[1], (unsigned long long)__popc(used));
+#pragma unroll
+      for (int q = 0; q < kSurStats; ++q) {
+        if (q == 1) continue;
+        const unsigned bq = __ballot_sync(0xffffffffu, (fl >> q) & 1u);
+        if (lane == 0 && bq) atomicAdd(&s_st[q], (unsigned long long)__popc(bq));
+      }
+      consumer_sync();  // every row of the tile is read (and its TMEM columns) before reuse
+      if (ct == 0) {    // the ring position is free for the producers
+        __threadfence_block();
+        atomicExch(&s_consumed, t + 1);
+      }
+      if (valid < kNT) break;  // the remainder was the last tile
+    }
+    // after a wait that gave up, one more bounded wait for that MMA group before the TMEM
+    // it writes is freed
+    if (failed && ct == 0) mbar_wait(&s_mma, failed_phase);
   }
-  if (cnt > 0) run(cnt);
-
+  tc_fence_before();
   __syncthreads();
-  if (threadIdx.x < kSurStats && s_st[threadIdx.x] && s.stats) atomicAdd(s.stats + threadIdx.x, s_st[threadIdx.x]);
+  tc_fence_after();
+  if (wid == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  if (tid < kSurStats && s_st[tid] && s.stats) atomicAdd(s.stats + tid, s_st[tid]);
 }
 
 }  // namespace
@@ -364,26 +536,22 @@ uint16_t bf16_rne(float f) {  // round to nearest even (finite inputs)
 }
 }  // namespace
 
-void surrogate_fragments(const float* params, uint2* frags, float* bias) {
-  // W (nout x nin, row-major) at off -> B fragments of mma.m16n8k16 (B[k][n] = W[n][k]):
-  // lane (g, t): b0 = (B[16kt+2t][8nt+g], B[16kt+2t+1][8nt+g]), b1 = rows 2t+8, 2t+9
-  auto frag = [&](int off, int nout, int nin, int kt, int nt, int lane) {
-    const int gq = lane >> 2, t = lane & 3, n = 8 * nt + gq;
-    auto w = [&](int k) { return (n < nout && k < nin) ? params[off + n * nin + k] : 0.0f; };
-    const int k0 = 16 * kt + 2 * t;
-    uint2 v;
-    v.x = (uint32_t)bf16_rne(w(k0)) | ((uint32_t)bf16_rne(w(k0 + 1)) << 16);
-    v.y = (uint32_t)bf16_rne(w(k0 + 8)) | ((uint32_t)bf16_rne(w(k0 + 9)) << 16);
-    return v;
+void surrogate_operands(const float* params, unsigned char* weights, float* bias) {
+  // W (nout x nin, row-major) = the B operand [N x K] in K-major order; zero padding up
+  // to N = 64 / 16 and K = 16 / 64
+  std::memset(weights, 0, kSurWeightBytes);
+  auto put = [&](int dst, int off, int nout, int nin, int N, int K) {
+    for (int n = 0; n < N; ++n)
+      for (int k = 0; k < K; ++k) {
+        const float w = (n < nout && k < nin) ? params[off + n * nin + k] : 0.0f;
+        const uint16_t b = bf16_rne(w);
+        std::memcpy(weights + dst + op_offset(n, k, K), &b, 2);
+      }
   };
-  for (int lane = 0; lane < 32; ++lane) {
-    for (int nt = 0; nt < 8; ++nt) frags[nt * 32 + lane] = frag(kOffW1, kMlpHid, kMlpIn, 0, nt, lane);
-    for (int L = 0; L < 2; ++L)
-      for (int kt = 0; kt < 4; ++kt)
-        for (int nt = 0; nt < 8; ++nt)
-          frags[(8 + L * 32 + kt * 8 + nt) * 32 + lane] = frag(L == 0 ? kOffW2 : kOffW3, kMlpHid, kMlpHid, kt, nt, lane);
-    for (int kt = 0; kt < 4; ++kt) frags[(72 + kt) * 32 + lane] = frag(kOffW4, kMlpOut, kMlpHid, kt, 0, lane);
-  }
+  put(kW1, kOffW1, kMlpHid, kMlpIn, 64, 16);
+  put(kW2, kOffW2, kMlpHid, kMlpHid, 64, 64);
+  put(kW3, kOffW3, kMlpHid, kMlpHid, 64, 64);
+  put(kW4, kOffW4, kMlpOut, kMlpHid, 16, 64);
   for (int q = 0; q < kMlpHid; ++q) {
     bias[q] = params[kOffB1 + q];
     bias[64 + q] = params[kOffB2 + q];
@@ -393,22 +561,39 @@ void surrogate_fragments(const float* params, uint2* frags, float* bias) {
 }
 
 cudaError_t launch_warm_rain_surrogate(const RainArgs& a, const SurrogateArgs& s, cudaStream_t st) {
-  if (a.g.nz > kMaxNz || a.g.nx > 0xffff || a.g.ny > 0x7fff || a.g.nz > 0xffff) return cudaErrorInvalidValue;
-  static int blocks = 0;  // resident CTAs of the whole device (the work loop is grid-strided)
+  if (a.g.nz > kMaxNz || a.g.nx > 0xffff || a.g.ny > 0x7fff || a.g.nz > 0xffff || !s.work || !s.err ||
+      !s.weights || (reinterpret_cast<uintptr_t>(s.weights) & 15u))
+    return cudaErrorInvalidValue;
+  static_assert(kWBytes == kSurWeightBytes, "weight blob size");
+  static int blocks = 0;  // resident CTAs of the whole device (units are taken from a counter)
   if (blocks == 0) {
-    int dev = 0, sms = 0, per_sm = 0;
+    // CTAs per SM from the kernel's registers and shared memory, counted here: the
+    // runtime's occupancy query reports one CTA per SM for this kernel, where the SM
+    // holds three
+    int dev = 0, sms = 0, regs_sm = 0, smem_sm = 0, smem_rsv = 0;
+    cudaFuncAttributes fa{};
     cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rain_net, cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_rain_net, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rain_net);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rain_net, kNT, 0);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev);
     if (e != cudaSuccess) return e;
-    blocks = sms * (per_sm > 0 ? per_sm : 1);
+    const int warp_regs = (fa.numRegs * 32 + 255) / 256 * 256;  // allocated per warp in 256s
+    const int by_regs = regs_sm / (warp_regs * (kThreads / 32));
+    const int by_smem = smem_sm / ((int)fa.sharedSizeBytes + kDynSmem + smem_rsv);
+    // TMEM holds 512 columns per SM: at most four CTAs of 128 columns run at once
+    blocks = sms * std::max(1, std::min(std::min(by_regs, by_smem), 512 / kTmemCols));
   }
-  if (!s.work) return cudaErrorInvalidValue;
   const long long rows = (long long)a.g.ny * a.g.nz;
-  const int grid = (int)std::min<long long>(blocks, (rows + kNW - 1) / kNW);
+  const int grid = (int)std::min<long long>(blocks, (rows + kProducerWarps - 1) / kProducerWarps);
   cudaError_t e = cudaMemsetAsync(s.work, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
-  k_rain_net<<<grid, kNT, 0, st>>>(a, s);
+  k_rain_net<<<grid, kThreads, kDynSmem, st>>>(a, s);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return launch_warm_rain(a, st, /*micro=*/false);

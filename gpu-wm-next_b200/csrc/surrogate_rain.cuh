@@ -9,14 +9,14 @@
 
 namespace gwmb {
 
-// Weights as mma.sync B fragments, per lane: layer 1 (8), layers 2 and 3 (32 each),
-// output layer (4) fragments of 32 lanes x (b0, b1) BF16 pairs.
-constexpr int kSurFrags = 8 + 32 + 32 + 4;
+// Weights in the tensor cores' shared-memory operand layout (BF16, K-major, no swizzle):
+// W1 [64 x 16], W2 and W3 [64 x 64], W4 [16 x 64] (5 outputs padded), 20480 bytes.
+constexpr int kSurWeightBytes = 20480;
 // Biases: b1 (64) b2 (64) b3 (64) b4 (5, padded to 8).
 constexpr int kSurBias = 3 * kMlpHid + 8;
 
 struct SurrogateArgs {
-  const uint2* frags;            // kSurFrags * 32
+  const unsigned char* weights;  // kSurWeightBytes, 16-byte aligned
   const float* bias;             // kSurBias
   const float* norm;             // kMlpNorm: x mean/std, y mean/std
   const float* range;            // kMlpRange: x min/max of the training data
@@ -26,13 +26,14 @@ struct SurrogateArgs {
   // ran, cells the network ran on, and per check the cells that failed it (input range,
   // fraction range, water, energy; a cell can fail several)
   unsigned long long* stats;
-  int* work;                     // row counter of the network kernel (zeroed before each launch)
+  int* work;                     // unit counter of the network kernel (zeroed before each launch)
+  int* err;                      // error word: set to 1 when a bounded wait gave up
 };
 constexpr int kSurStats = 6;
 
 cudaError_t launch_warm_rain_surrogate(const RainArgs& a, const SurrogateArgs& s, cudaStream_t st);
 
-// Host: weights (FP32 parameter vector) -> BF16 B fragments and FP32 biases.
-void surrogate_fragments(const float* params, uint2* frags, float* bias);
+// Host: weights (FP32 parameter vector) -> the BF16 operand blob and FP32 biases.
+void surrogate_operands(const float* params, unsigned char* weights, float* bias);
 
 }  // namespace gwmb
