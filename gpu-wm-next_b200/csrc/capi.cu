@@ -262,7 +262,7 @@ bool build_substep_maps(Member& M) {
   };
   bool ok = true;
   for (int i = 0; i < 2; ++i) {
-    ok = ok && add(M.R[i], 0) && add(M.TH[i], 0) && add(M.P[i], 0);
+    ok = ok && add(M.R[i], 0) && add(M.TH[i], 0) && add(M.P[i], 0) && add(M.R[i], 2) && add(M.TH[i], 2);
     ok = ok && add(M.D[i][0], 1) && add(M.D[i][1], 1) && add(M.D[i][2], 2);
     for (int f = 0; f < 3; ++f) ok = ok && add(M.B[i][f], 2);
   }
@@ -407,8 +407,10 @@ cudaError_t launch_substep(gwm_b200_ctx* c, const Member& M, const FastArgs& f, 
   if (!terr && c->fast_tile_rows == kFastTma) {
     FastMaps m{};
     const bool fin = f.final_kind == 2;
-    const CUtensorMap* rho = M.tmap(f.rho_in, 0);
-    const CUtensorMap* th = M.tmap(f.th, 0);
+    // rho and theta with the halo ring in the first substep (p' is derived there), owned
+    // boxes otherwise
+    const CUtensorMap* rho = M.tmap(f.rho_in, first ? 0 : 2);
+    const CUtensorMap* th = M.tmap(f.th, first ? 0 : 2);
     const CUtensorMap* du = first ? nullptr : M.tmap(f.du_in, 1);
     const CUtensorMap* dv = first ? nullptr : M.tmap(f.dv_in, 1);
     const CUtensorMap* dw = first ? nullptr : M.tmap(f.dw_in, 2);

@@ -74,7 +74,8 @@ struct FastArgs {
 // TMA descriptors of one acoustic substep (flat terrain, k_fast_tma): 3-D tiled maps
 // over the padded field layout (dims pitch x rows x (nz+1), FP32, no swizzle).
 struct FastMaps {
-  CUtensorMap rho, th;     // box 40 x 18: cells with the halo ring
+  CUtensorMap rho, th;     // first substep of a stage: box 40 x 18, cells with the halo ring;
+                           // other substeps: box 32 x 16, owned cells
   CUtensorMap du, dv;      // box 36 x 17: owned faces + the tile's east/north face
   CUtensorMap dw;          // box 32 x 16
   CUtensorMap bu, bv, bw;  // box 32 x 16 (last substep of the step)

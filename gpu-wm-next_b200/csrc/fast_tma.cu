@@ -3,20 +3,25 @@
 // Same operator as k_fast_flat (LocalSplitExplicitFastMode::apply,
 // dry_fast_modes.cu:400-656, K9-K15 on one substep) and the same per-cell
 // arithmetic, with a different data path: one elected thread per CTA fetches every
-// plane's tiles with cp.async.bulk.tensor.3d into a three-slot shared-memory ring,
-// two planes ahead of the compute, and the 256 threads work from shared memory.
+// plane's tiles with cp.async.bulk.tensor.3d into a four-slot shared-memory ring,
+// three planes ahead of the compute, and the 256 threads work from shared memory.
 // Per plane k the ring slot holds
-//   rho(k), theta(k)        40 x 18 box: columns i0-4 .. i0+35, rows j0-1 .. j0+16
-//                           (the owned 32 x 16 tile and its one-cell halo ring; the
-//                           box starts 4 columns left so x stays 16-byte aligned)
+//   rho(k), theta(k)        first substep of a stage: 40 x 18 boxes, columns i0-4 .. i0+35,
+//                           rows j0-1 .. j0+16 (the owned 32 x 16 tile and its one-cell
+//                           halo ring, from which p' is derived; the box starts 4 columns
+//                           left so x stays 16-byte aligned); other substeps: the owned
+//                           32 x 16 box (p' comes with its halo below)
 //   du(k), dv(k)            36 x 17 box: owned faces plus the tile's east/north face
 //   dw(k+1)                 32 x 16 box: owned Z faces above the plane
-//   p'(k)                   40 x 18 box like rho: the pressure perturbation the previous
-//                           substep computed for its level sums (every substep but the
-//                           first of a stage), so the EOS runs once per cell per substep
+//   p'(k)                   40 x 18 box like the first substep's rho: the pressure
+//                           perturbation the previous substep computed for its level sums
+//                           (every substep but the first of a stage), so the EOS runs once
+//                           per cell per substep
 //   bu(k), bv(k), bw(k+1)   32 x 16 boxes, last substep of the step only (m = B + D)
 // so the kernel issues no per-thread global loads on the main path, holds no load
-// pipeline in registers and needs no halo threads reading global memory.
+// pipeline in registers and needs no halo threads reading global memory.  The level
+// tables (reference means, metric columns, EOS base state) follow the ring in dynamic
+// shared memory, sized by nz.
 #include "dycore.cuh"
 #include "tma.cuh"
 
@@ -28,42 +33,71 @@ constexpr int TX = 32, TY = 16, RY = 8, NT = 256, NW = NT / 32;
 constexpr int CBW = 40, CBH = 18;  // cell box
 constexpr int FBW = 36, FBH = 17;  // face box (owned faces + east/north face)
 constexpr int OBW = 32, OBH = 16;  // owned box
-// slot layout in floats; every sub-buffer starts on a 128-byte boundary
-// (the base-momentum boxes are only present, and the slot only that long, in the last
-// substep of the step: other substeps use the shorter slot and fit three CTAs per SM)
-constexpr int O_RHO = 0, O_TH = 736, O_DU = 1472, O_DV = 2112, O_DW = 2752, O_P = 3264, O_BU = 4000,
-              O_BV = 4512, O_BW = 5024, SLOT = 5536, SLOT_SHORT = 4000, NSLOT = 3;
 constexpr unsigned B_CELL = CBW * CBH * 4, B_FACE = FBW * FBH * 4, B_OWN = OBW * OBH * 4;
-constexpr size_t kDynSmem = size_t(SLOT) * NSLOT * sizeof(float) + 128;
-constexpr size_t kDynSmemShort = size_t(SLOT_SHORT) * NSLOT * sizeof(float) + 128;
-static_assert(O_TH % 32 == 0 && O_DU % 32 == 0 && O_DV % 32 == 0 && O_DW % 32 == 0 && O_P % 32 == 0 &&
-                  O_BU % 32 == 0 && O_BV % 32 == 0 && O_BW % 32 == 0 && SLOT % 32 == 0 &&
-                  SLOT_SHORT % 32 == 0 && SLOT_SHORT == O_BU,
-              "128-byte aligned sub-buffers");
-static_assert(O_TH - O_RHO >= CBW * CBH && O_DU - O_TH >= CBW * CBH && O_DV - O_DU >= FBW * FBH &&
-                  O_DW - O_DV >= FBW * FBH && O_P - O_DW >= OBW * OBH && O_BU - O_P >= CBW * CBH &&
-                  O_BV - O_BU >= OBW * OBH && O_BW - O_BV >= OBW * OBH && SLOT - O_BW >= OBW * OBH,
-              "boxes fit their sub-buffers");
+constexpr int NSLOT = 4, AHEAD = NSLOT - 1;  // ring slots; planes in flight beyond the one computed
+// Slot layouts in floats; every sub-buffer starts on a 128-byte boundary.  The
+// base-momentum boxes are only present, and the slot only that long, in the last
+// substep of the step.  RW, R0, C0: row width of the rho/theta boxes and the box
+// position of owned cell (0, 0).
+template <bool FIRST> struct Slot;
+template <> struct Slot<true> {  // first substep of a stage: rho, theta with the halo ring
+  static constexpr int O_RHO = 0, O_TH = 736, O_DU = 0, O_DV = 0, O_DW = 0, O_P = 0, O_BU = 1472, O_BV = 1984,
+                       O_BW = 2496, LONG = 3008, SHORT = 1472, RW = CBW, R0 = 1, C0 = 4;
+};
+template <> struct Slot<false> {  // inner substeps: owned rho, theta; increments; p' with its ring
+  static constexpr int O_RHO = 0, O_TH = 512, O_DU = 1024, O_DV = 1664, O_DW = 2304, O_P = 2816, O_BU = 3552,
+                       O_BV = 4064, O_BW = 4576, LONG = 5088, SHORT = 3552, RW = OBW, R0 = 0, C0 = 0;
+};
+template <bool FIRST>
+constexpr bool slot_ok() {
+  using L = Slot<FIRST>;
+  constexpr int rb = FIRST ? CBW * CBH : OBW * OBH;
+  return L::O_TH % 32 == 0 && L::O_BU % 32 == 0 && L::O_BV % 32 == 0 && L::O_BW % 32 == 0 &&
+         L::LONG % 32 == 0 && L::SHORT % 32 == 0 && L::SHORT == L::O_BU && L::O_TH - L::O_RHO >= rb &&
+         (FIRST ? L::O_BU - L::O_TH >= rb
+                : (L::O_DU % 32 == 0 && L::O_DV % 32 == 0 && L::O_DW % 32 == 0 && L::O_P % 32 == 0 &&
+                   L::O_DU - L::O_TH >= rb && L::O_DV - L::O_DU >= FBW * FBH && L::O_DW - L::O_DV >= FBW * FBH &&
+                   L::O_P - L::O_DW >= OBW * OBH && L::O_BU - L::O_P >= CBW * CBH)) &&
+         L::O_BV - L::O_BU >= OBW * OBH && L::O_BW - L::O_BV >= OBW * OBH && L::LONG - L::O_BW >= OBW * OBH;
+}
+static_assert(slot_ok<true>() && slot_ok<false>(), "128-byte aligned sub-buffers that fit their boxes");
+// dynamic shared memory: the ring, then the level tables (2 double + 4 float per level)
+constexpr size_t kLevelBytes = 2 * sizeof(double) + 4 * sizeof(float);
+template <bool FIRST>
+constexpr size_t dyn_smem(bool final_step, int nz) {
+  return size_t(final_step ? Slot<FIRST>::LONG : Slot<FIRST>::SHORT) * NSLOT * sizeof(float) + 128 +
+         kLevelBytes * size_t(nz);
+}
 }  // namespace ft
 
 template <bool FIRST>
 __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const __grid_constant__ FastMaps m) {
   using namespace ft;
+  using L = Slot<FIRST>;
+  constexpr int O_RHO = L::O_RHO, O_TH = L::O_TH, O_DU = L::O_DU, O_DV = L::O_DV, O_DW = L::O_DW, O_P = L::O_P,
+                O_BU = L::O_BU, O_BV = L::O_BV, O_BW = L::O_BW, RW = L::RW, R0 = L::R0, C0 = L::C0;
   extern __shared__ unsigned char s_dyn[];
-  __shared__ float s_p[2][TY + 2][TX + 2];  // pressure perturbation, tile + halo ring
+  __shared__ float s_p[2][TY + 2][TX + 2];  // pressure perturbation, tile + halo ring (first substep)
   __shared__ float s_du[2][TY][TX + 1];     // new X-face increments (own + east face)
   __shared__ float s_dv[2][TY + 1][TX];     // new Y-face increments (own + north face)
-  __shared__ float s_pref[kMaxNz], s_rref[kMaxNz], s_idzc[kMaxNz], s_idzf[kMaxNz];
-  __shared__ double s_binv[kMaxNz], s_bpr[kMaxNz];  // EOS base state: 1/rt_ref, p_ref
   __shared__ long long s_red[2][NW][2];
   __shared__ __align__(8) uint64_t s_bar[NSLOT];
   __shared__ int s_abort[2];  // per plane parity: set before barrier k, read after it
+  const int nz = a.g.nz;
+  const bool final_step = a.final_kind == 2;
+  const int slot = final_step ? L::LONG : L::SHORT;
   float* const ring = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
+  double* const s_binv = reinterpret_cast<double*>(ring + slot * NSLOT);  // EOS base state: 1/rt_ref
+  double* const s_bpr = s_binv + nz;                                       // and p_ref
+  float* const s_pref = reinterpret_cast<float*>(s_bpr + nz);               // K6/K7 level means
+  float* const s_rref = s_pref + nz;
+  float* const s_idzc = s_rref + nz;  // metric columns
+  float* const s_idzf = s_idzc + nz;
 
   const Geom& g = a.g;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nx = g.nx, ny = g.ny;
   const int w = min(TX, nx - i0), h = min(TY, ny - j0);
   const bool own0 = tx < w && ty < h, own1 = tx < w && ty + RY < h;
   const int gi = i0 + tx, gj0 = j0 + ty, gj1 = j0 + ty + RY;
@@ -80,10 +114,8 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
   const int hi = i0 + hc - 1, hj = j0 + hr - 1;  // global cell of the halo role
   const bool h_skip = (role == 1 && hi == nx && !g.per_x) || (role == 3 && hj == ny && !g.per_y);
   const float idx = g.inv_dx, idy = g.inv_dy, dtf = a.dtf;
-  const bool final_step = a.final_kind == 2;
   const int acc_mode = a.acc_off ? 0 : (a.final_kind == 0 ? 1 : 2);
   const bool hm = a.hmom != 0, dn = a.dens != 0;
-  const int slot = final_step ? SLOT : SLOT_SHORT;
 
   if (tid == 0) {
     for (int s = 0; s < NSLOT; ++s) mbar_init(&s_bar[s], 1);
@@ -108,13 +140,18 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     float* st = ring + (kk % NSLOT) * slot;
     uint64_t* bar = &s_bar[kk % NSLOT];
     const bool wface = kk + 1 < nz;
-    unsigned bytes = 2 * B_CELL;
+    unsigned bytes = FIRST ? 2 * B_CELL : 2 * B_OWN;
     if (!FIRST) bytes += 2 * B_FACE + (wface ? B_OWN : 0u) + B_CELL;
     if (final_step) bytes += 3 * B_OWN;
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(bar, bytes);
-    tma_load_3d(st + O_RHO, &m.rho, i0 + kXOff - 4, j0, kk, bar);
-    tma_load_3d(st + O_TH, &m.th, i0 + kXOff - 4, j0, kk, bar);
+    if (FIRST) {  // with the halo ring
+      tma_load_3d(st + O_RHO, &m.rho, i0 + kXOff - 4, j0, kk, bar);
+      tma_load_3d(st + O_TH, &m.th, i0 + kXOff - 4, j0, kk, bar);
+    } else {  // owned cells
+      tma_load_3d(st + O_RHO, &m.rho, i0 + kXOff, j0 + 1, kk, bar);
+      tma_load_3d(st + O_TH, &m.th, i0 + kXOff, j0 + 1, kk, bar);
+    }
     if (!FIRST) {
       tma_load_3d(st + O_DU, &m.du, i0 + kXOff, j0 + 1, kk, bar);
       tma_load_3d(st + O_DV, &m.dv, i0 + kXOff, j0 + 1, kk, bar);
@@ -151,7 +188,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
   if (tid == 0) {
     issue(0);
     issued = 0;
-    if (nz > 1) { issue(1); issued = 1; }
+    for (int kk = 1; kk < AHEAD && kk < nz; ++kk) { issue(kk); issued = kk; }
   }
   wait_plane(0, 0);
   if (FIRST) plane_p(0);
@@ -216,17 +253,17 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
         a.f_v[o] = __ldg(a.bv + o) + d;
       }
     }
-    const float rc0 = st[O_RHO + (ty + 1) * CBW + tx + 4], rc1 = st[O_RHO + (ty + RY + 1) * CBW + tx + 4];
+    const float rc0 = st[O_RHO + (ty + R0) * RW + tx + C0], rc1 = st[O_RHO + (ty + RY + R0) * RW + tx + C0];
     float wn0 = dw0, wn1 = dw1;
     if (k + 1 < nz) {
       const float prl = s_pref[k], pru = s_pref[k + 1], rrl = s_rref[k], rru = s_rref[k + 1];
       const float idzf = s_idzf[k + 1];
       const float pn0 = P1(ty + 1, tx + 1), pn1 = P1(ty + RY + 1, tx + 1);
-      const float rn0 = stn[O_RHO + (ty + 1) * CBW + tx + 4], rn1 = stn[O_RHO + (ty + RY + 1) * CBW + tx + 4];
+      const float rn0 = stn[O_RHO + (ty + R0) * RW + tx + C0], rn1 = stn[O_RHO + (ty + RY + R0) * RW + tx + C0];
       wn0 = dw0 + dtf * (-((pn0 - pru) - (pc0 - prl)) * idzf - a.gravity * (0.5f * ((rc0 - rrl) + (rn0 - rru))));
       wn1 = dw1 + dtf * (-((pn1 - pru) - (pc1 - prl)) * idzf - a.gravity * (0.5f * ((rc1 - rrl) + (rn1 - rru))));
     }
-    __syncthreads();  // publishes s_p(k+1), s_du(k), s_dv(k); slot (k-1) is free
+    __syncthreads();  // publishes s_p(k+1), s_du(k), s_dv(k); the slot of plane k-1 is free
     if (s_abort[pb]) { aborted = true; break; }
     if (tid == 0) {
       if (acc_mode && k > 0) {  // level sums of plane k-1 (warp totals published above)
@@ -235,7 +272,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
         acc_add(a.acc_a + k - 1, sa);
         if (acc_mode == 1) acc_add(a.acc_b + k - 1, sb);
       }
-      if (k + 2 < nz) { issue(k + 2); issued = k + 2; }
+      if (k + AHEAD < nz) { issue(k + AHEAD); issued = k + AHEAD; }
     }
     // ---- K15 density of plane k, K10 rho*theta, stores
     const float idzc = s_idzc[k];
@@ -246,7 +283,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
         const float div = (s_du[pb][ty][tx + 1] - un0) * idx + (s_dv[pb][ty + 1][tx] - vn0) * idy + (wn0 - dwc0) * idzc;
         rn = fmaxf(1.0e-6f, rc0 - dtf * div);
       }
-      const float rt = rn * st[O_TH + (ty + 1) * CBW + tx + 4];
+      const float rt = rn * st[O_TH + (ty + R0) * RW + tx + C0];
       if (final_step) {
         store_tile(a.f_rho, g, kCell, gi, gj0, k, rn, edge);
         store_tile(a.f_rt, g, kCell, gi, gj0, k, rt, edge);
@@ -275,7 +312,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
                           (wn1 - dwc1) * idzc;
         rn = fmaxf(1.0e-6f, rc1 - dtf * div);
       }
-      const float rt = rn * st[O_TH + (ty + RY + 1) * CBW + tx + 4];
+      const float rt = rn * st[O_TH + (ty + RY + R0) * RW + tx + C0];
       if (final_step) {
         store_tile(a.f_rho, g, kCell, gi, gj1, k, rn, edge);
         store_tile(a.f_rt, g, kCell, gi, gj1, k, rt, edge);
@@ -326,18 +363,19 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
 
 cudaError_t init_fast_tma() {
   cudaError_t e = cudaFuncSetAttribute(k_fast_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)ft::kDynSmem);
+                                       (int)ft::dyn_smem<true>(true, kMaxNz));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_fast_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ft::kDynSmem);
+  return cudaFuncSetAttribute(k_fast_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)ft::dyn_smem<false>(true, kMaxNz));
 }
 
 cudaError_t launch_fast_tma(const FastArgs& a, const FastMaps& m, bool first, cudaStream_t s) {
-  if (a.g.nz > kMaxNz || !a.err) return cudaErrorInvalidValue;
+  if (a.g.nz > kMaxNz || a.g.nz < 1 || !a.err) return cudaErrorInvalidValue;
   const dim3 block(ft::TX, ft::RY);
   const dim3 grid((a.g.nx + ft::TX - 1) / ft::TX, (a.g.ny + ft::TY - 1) / ft::TY);
-  const size_t smem = a.final_kind == 2 ? ft::kDynSmem : ft::kDynSmemShort;
-  if (first) k_fast_tma<true><<<grid, block, smem, s>>>(a, m);
-  else k_fast_tma<false><<<grid, block, smem, s>>>(a, m);
+  const bool fin = a.final_kind == 2;
+  if (first) k_fast_tma<true><<<grid, block, ft::dyn_smem<true>(fin, a.g.nz), s>>>(a, m);
+  else k_fast_tma<false><<<grid, block, ft::dyn_smem<false>(fin, a.g.nz), s>>>(a, m);
   return cudaGetLastError();
 }
 
