@@ -421,8 +421,9 @@ def surrogate_line(gwm, model, stream, torch, steps=10):
             "precip_rel_diff": abs(p1 - p0) / max(abs(p0), 1e-30), "steps": steps,
             "training": json.loads(str(w["summary"])),
             "stats": out["surrogate"]["stats"],
-            "note": "two kernels: BF16 mma.sync inference of process fractions on the active cells packed "
-                    "into dense tiles (quiet cells gated), per-cell plain fallback; then the plain fallout sweep"}
+            "note": "two kernels: gating warps pack the active cells (quiet cells gated) into 128-row "
+                    "tiles, tcgen05 BF16 inference of process fractions with TMEM accumulators, per-cell "
+                    "plain fallback; then the plain fallout sweep"}
 
 
 def ensemble_line(gwm, torch, stream, dist, world, n=64, steps=3, warmup=3):
