@@ -85,15 +85,19 @@ __device__ __forceinline__ void micro_step(MicroCell& c, const MicroParams& m, M
     qr += conv;
     r_auto = conv;
   }
-  const float p = eos_pressure(rho, rho * th);
-  const float temp = th * powf(fmaxf(p / kP0, 1.0e-6f), kKappa);
-  qs = qsat(temp, p);
-  if (qr > 0.0f && qv < qs && m.evap > 0.0f) {
-    const float ev = fminf(qr, m.dt * m.evap * fminf(qs - qv, qr));
-    qr -= ev;
-    qv += ev;
-    r_evap = ev;
-    if (m.latent && ev > 0.0f) th -= lh * ev;
+  // rain evaporation, from the saturation of the adjusted state: only a cell holding
+  // rain needs it (the state is re-derived only there, with the same result)
+  if (qr > 0.0f && m.evap > 0.0f) {
+    const float p = eos_pressure(rho, rho * th);
+    const float temp = th * powf(fmaxf(p / kP0, 1.0e-6f), kKappa);
+    qs = qsat(temp, p);
+    if (qv < qs) {
+      const float ev = fminf(qr, m.dt * m.evap * fminf(qs - qv, qr));
+      qr -= ev;
+      qv += ev;
+      r_evap = ev;
+      if (m.latent && ev > 0.0f) th -= lh * ev;
+    }
   }
   if (rates) *rates = MicroRates{r_cond, r_auto, r_evap};
   c.th = th;
