@@ -148,8 +148,19 @@ __global__ void __launch_bounds__(RB) k_warm_rain(const RainArgs a) {
       const float rho_d = c_rho;
       float rho = 0.0f, th = 0.0f, qv = 0.0f, qc = 0.0f, rqr = c_qr;
       if (MICRO) {  // warm_rain_kernel: warm_rain.cu:36-120
-        MicroCell mc = micro_state(rho_d, c_rt, c_qv, c_qc, c_qr);
-        micro_step(mc, MicroParams{a.dt, a.relax, a.thr, a.rate, a.evap, a.latent});
+        MicroCell mc;
+        if (a.thr >= 0.0f && surely_quiet(rho_d, c_rt, c_qv, c_qc, c_qr)) {
+          // micro_step leaves the cell as micro_state derives it: only the mixing ratios
+          // and theta are needed, not the temperature, pressure or saturation
+          mc.rho = fmaxf(rho_d, 1.0e-6f);
+          mc.th = c_rt / mc.rho;
+          mc.qv = fmaxf(c_qv / mc.rho, 0.0f);
+          mc.qc = fmaxf(c_qc / mc.rho, 0.0f);
+          mc.qr = fmaxf(c_qr / mc.rho, 0.0f);
+        } else {
+          mc = micro_state(rho_d, c_rt, c_qv, c_qc, c_qr);
+          micro_step(mc, MicroParams{a.dt, a.relax, a.thr, a.rate, a.evap, a.latent});
+        }
         rho = mc.rho; th = mc.th; qv = mc.qv; qc = mc.qc;
         rqr = rho * mc.qr;
       }

@@ -51,6 +51,24 @@ __device__ __forceinline__ MicroCell micro_state(float rho_d, float rt, float rq
   return c;
 }
 
+// A cell the warm-rain step certainly leaves in place: no cloud or rain water, and vapour
+// below 0.999 of saturation by a fast-math estimate of the state (its error is ~1e-6).
+// With a non-negative autoconversion threshold micro_step takes none of its branches
+// for such a cell, so the exact temperature, pressure and saturation are not needed.
+// A false answer decides nothing: the cell is then judged on its exact state.
+__device__ __forceinline__ bool surely_quiet(float rho_d, float rt, float rqv, float rqc, float rqr) {
+  if (rqc > 0.0f || rqr > 0.0f) return false;
+  const float rho = fmaxf(rho_d, 1.0e-6f), ir = __fdividef(1.0f, rho);
+  const float ratio = fmaxf(rt * (kRd / kP0), 1.0e-6f);
+  const float p = kP0 * __powf(ratio, 1.0f / (1.0f - kKappa));
+  const float temp = rt * ir * __powf(fmaxf(p * (1.0f / kP0), 1.0e-6f), kKappa);
+  const float tc = temp - 273.15f;
+  const float es = 611.2f * __expf(__fdividef(17.67f * tc, fmaxf(tc + 243.5f, 1.0e-6f)));
+  const float eps = kRd / kRv;
+  const float qs = fminf(fmaxf(__fdividef(eps * es, fmaxf(p - (1.0f - eps) * es, 1000.0f)), 0.0f), 0.05f);
+  return fmaxf(rqv * ir, 0.0f) < qs * (1.0f - 1.0e-3f);
+}
+
 // warm_rain_kernel body: warm_rain.cu:63-120 (saturation adjustment with latent heating,
 // autoconversion, rain evaporation, clip at zero).  Updates c.th, c.qv, c.qc, c.qr.
 // Process amounts of one micro_step (mixing-ratio units): condensation (vapour -> cloud,

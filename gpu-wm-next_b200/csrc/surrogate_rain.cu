@@ -8,21 +8,24 @@
 //   2. k_warm_rain<false> (physics.cu): the plain column sweep with the microphysics
 //      switched off (fallout, FP64 precipitation, theta level sums).
 //
-// k_rain_net.  A CTA of 128 threads takes units of 128 consecutive cells of one (j, k)
-// row from a counter; each thread builds its cell's state and features and applies the
-// activity gate (quiet cells, which the plain scheme leaves exactly unchanged, are not
-// touched).  The active cells are appended to a 256-row ring of layer-1 inputs in shared
-// memory; whenever 128 are waiting, the CTA runs them as one M = 128 tile:
+// k_rain_net.  A CTA of 256 threads has two roles.  Warps 0-3 (producers) take whole
+// (j, k) rows from a counter, build each cell's state and features and apply the
+// activity gate (quiet cells, which the plain scheme leaves in place, are not touched);
+// the active cells go into a four-tile ring of 128-row layer-1 inputs in shared memory,
+// with their index and state, each written row arriving on its tile's mbarrier.  Warps
+// 4-7 (consumers, one per TMEM lane quarter) run each full tile, or the remainder once
+// every producer is done, as one M = 128 tile:
 //   layer 1  [128 x 16] x [16 x 64]   one tcgen05.mma (K = 16: 7 inputs + padding)
 //   layers 2, 3  [128 x 64] x [64 x 64]   four tcgen05.mma each (K = 16 per MMA)
 //   layer 4  [128 x 64] x [64 x 16]   four tcgen05.mma (5 outputs, N padded to 16)
 // with BF16 operands read by the tensor core from shared memory (canonical K-major
 // layout without swizzle: 8 x 16-byte core matrices) and FP32 accumulators in tensor
-// memory (TMEM, 128 columns per CTA).  One thread issues the MMAs and commits them to an
-// mbarrier; after each layer every thread loads its own row from TMEM (tcgen05.ld,
-// thread t = TMEM lane t), adds the bias, applies GELU (tanh form, hardware tanh
-// approximation), and writes the row back as the next layer's BF16 operand.  Each
-// thread then applies the result of its row's cell.
+// memory (TMEM, 128 columns per CTA).  One consumer thread issues the MMAs and commits
+// them to an mbarrier; after each layer every consumer thread loads its own row from
+// TMEM (tcgen05.ld, thread t = TMEM lane t), adds the bias, applies GELU (tanh form, FP32
+// with the hardware tanh approximation), and writes the row back as the next layer's
+// BF16 operand.  Each consumer thread then applies the result of its row's cell and
+// frees the ring tile for the producers.
 //
 // Per cell the network gives the condensation, autoconversion and rain-evaporation
 // amounts as fractions of their bounds (the saturation deficit |qv - qs|, the cloud
@@ -37,8 +40,8 @@
 // more than tol_water or tol_energy of the cell's exchange plus the output's training
 // spread.
 //
-// Every wait is bounded: if an MMA group does not complete, the kernel records the
-// error word, stops, frees its TMEM and returns.
+// Every wait is bounded (ring space, a full tile, an MMA group): one that gives up records
+// the error word and the CTA drains, frees its TMEM and returns.
 #include <algorithm>
 #include <cstring>
 
@@ -233,18 +236,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_rain_net(const RainArgs a, cons
           // subsaturated (vapour below 0.999 of saturation; the estimate's error is
           // ~1e-6) is quiet without the exact state; every other cell is decided on the
           // exact state.
-          bool exact = rqc > 0.0f || rqr > 0.0f;
-          if (!exact) {
-            const float rho = fmaxf(rho_d, 1.0e-6f), ir = __fdividef(1.0f, rho);
-            const float ratio = fmaxf(rt * (kRd / kP0), 1.0e-6f);
-            const float p_ = kP0 * __powf(ratio, 1.0f / (1.0f - kKappa));
-            const float temp = rt * ir * __powf(fmaxf(p_ * (1.0f / kP0), 1.0e-6f), kKappa);
-            const float tc = temp - 273.15f;
-            const float es = 611.2f * __expf(__fdividef(17.67f * tc, fmaxf(tc + 243.5f, 1.0e-6f)));
-            const float eps = kRd / kRv;
-            const float qs = fminf(fmaxf(__fdividef(eps * es, fmaxf(p_ - (1.0f - eps) * es, 1000.0f)), 0.0f), 0.05f);
-            exact = !(fmaxf(rqv * ir, 0.0f) < qs * (1.0f - 1.0e-3f));
-          }
+          const bool exact = !surely_quiet(rho_d, rt, rqv, rqc, rqr);
           if (exact) {
             const MicroCell mc = micro_state(rho_d, rt, rqv, rqc, rqr);
             const float qs = qsat(mc.temp, mc.p);
