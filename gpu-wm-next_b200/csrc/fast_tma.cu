@@ -35,6 +35,10 @@ constexpr int FBW = 36, FBH = 17;  // face box (owned faces + east/north face)
 constexpr int OBW = 32, OBH = 16;  // owned box
 constexpr unsigned B_CELL = CBW * CBH * 4, B_FACE = FBW * FBH * 4, B_OWN = OBW * OBH * 4;
 constexpr int NSLOT = 4, AHEAD = NSLOT - 1;  // ring slots; planes in flight beyond the one computed
+// the thread that issues the TMA loads and folds the level sums: lane 0 of the last warp,
+// which has no halo role (warps 0-2 carry those), so the per-plane serial work does not
+// land on a warp that is already the slowest
+constexpr int ISSUER = NT - 32;
 // Slot layouts in floats; every sub-buffer starts on a 128-byte boundary.  The
 // base-momentum boxes are only present, and the slot only that long, in the last
 // substep of the step.  RW, R0, C0: row width of the rho/theta boxes and the box
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     if (role >= 0) sp[hr][hc] = cell_p(st, hr, hc, kk);
   };
 
-  if (tid == 0) {
+  if (tid == ISSUER) {
     issue(0);
     issued = 0;
     for (int kk = 1; kk < AHEAD && kk < nz; ++kk) { issue(kk); issued = kk; }
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     }
     __syncthreads();  // publishes s_p(k+1), s_du(k), s_dv(k); the slot of plane k-1 is free
     if (s_abort[pb]) { aborted = true; break; }
-    if (tid == 0) {
+    if (tid == ISSUER) {
       if (acc_mode && k > 0) {  // level sums of plane k-1 (warp totals published above)
         long long sa = 0, sb = 0;
         for (int q = 0; q < NW; ++q) { sa += s_red[pb ^ 1][q][0]; sb += s_red[pb ^ 1][q][1]; }
@@ -343,13 +347,13 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
   }
   if (aborted) {
     // drain the tiles still in flight (bounded) before the CTA's shared memory goes away
-    if (tid == 0)
+    if (tid == ISSUER)
       for (int kk = waited + 1; kk <= issued; ++kk) mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1);
     return;
   }
   if (acc_mode) {  // level sums of the last plane
     __syncthreads();
-    if (tid == 0) {
+    if (tid == ISSUER) {
       const int pb = (nz - 1) & 1;
       long long sa = 0, sb = 0;
       for (int q = 0; q < NW; ++q) { sa += s_red[pb][q][0]; sb += s_red[pb][q][1]; }

@@ -25,6 +25,9 @@ namespace {
 
 namespace sl {
 constexpr int TX = 32, TY = 16, RY = 8, NT = 256, NW = NT / 32;
+// the thread that issues the TMA loads and folds the level sums: lane 0 of the last warp,
+// which has no open-boundary face role (warps 0 and 1 carry those)
+constexpr int ISSUER = NT - 32;
 constexpr int BW = 40, BH = 18, BHV = 19;  // boxes: cells, X and Z faces / Y faces
 constexpr int DW = TX + 2, DH = TY + 2, DN = DW * DH;  // derived plane: 34 x 18
 // raw slot (floats; sub-buffers on 128-byte boundaries)
@@ -151,7 +154,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     return q;
   };
 
-  if (tid == 0) {
+  if (tid == ISSUER) {
     issue(0);
     issue(1);
     issued = 1;
@@ -337,7 +340,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     const SlowBlend n0a = load_q0(gj0, own0, k + 1), n0b = load_q0(gj1, own1, k + 1);
     __syncthreads();  // publishes plane k's derived values; slot (k-1) is free
     if (s_abort[pb]) { aborted = true; break; }
-    if (tid == 0) {
+    if (tid == ISSUER) {
       if (a.acc_mode && k > 0) {
         long long sa = 0, sb = 0;
         for (int q = 0; q < NW; ++q) { sa += s_red[pb ^ 1][q][0]; sb += s_red[pb ^ 1][q][1]; }
@@ -372,13 +375,13 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     q0b = n0b;
   }
   if (aborted) {
-    if (tid == 0)
+    if (tid == ISSUER)
       for (int kk = waited + 1; kk <= issued; ++kk) mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1);
     return;
   }
   if (a.acc_mode) {
     __syncthreads();
-    if (tid == 0) {
+    if (tid == ISSUER) {
       const int pb = (nz - 1) & 1;
       long long sa = 0, sb = 0;
       for (int q = 0; q < NW; ++q) { sa += s_red[pb][q][0]; sb += s_red[pb][q][1]; }

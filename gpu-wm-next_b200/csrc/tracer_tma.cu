@@ -20,6 +20,9 @@ namespace {
 
 namespace tt {
 constexpr int TX = 32, TY = 16, RY = 8, NT = 256, NTR = 3;
+// the thread that issues the TMA loads: lane 0 of the last warp, which has no halo-ring
+// role (warps 0-2 carry those)
+constexpr int ISSUER = NT - 32;
 constexpr int CBW = 40, CBH = 18, FBW = 36, FBH = 17, OBW = 32, OBH = 16;
 constexpr int O_RHO = 0, O_Q = 736, O_U = 2944, O_V = 3584, O_W = 4224, SLOT = 4736, NSLOT = 3;
 constexpr unsigned B_CELL = CBW * CBH * 4, B_FACE = FBW * FBH * 4, B_OWN = OBW * OBH * 4;
@@ -105,7 +108,7 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
     if (hr >= 0) one(hr, hc);
   };
 
-  if (tid == 0) {
+  if (tid == ISSUER) {
     issue(0);
     issue(1);
     issued = 1;
@@ -177,9 +180,9 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
     for (int t = 0; t < NTR; ++t) { q0a[t] = n0a[t]; q0b[t] = n0b[t]; }
     __syncthreads();  // publishes plane k+1's ring; slot k is free
     if (s_abort[k & 1]) { aborted = true; break; }
-    if (tid == 0 && k + 3 <= nz) { issue(k + 3); issued = k + 3; }
+    if (tid == ISSUER && k + 3 <= nz) { issue(k + 3); issued = k + 3; }
   }
-  if (aborted && tid == 0)
+  if (aborted && tid == ISSUER)
     for (int kk = waited + 1; kk <= issued; ++kk) mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1);
 }
 
