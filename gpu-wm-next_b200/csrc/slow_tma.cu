@@ -164,7 +164,22 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
   wait_plane(0, 0);
 
   // one owned column: cell, X face, Y face and Z face of plane k (+ the top face)
-  auto column = [&](int k, int r, int gj, bool own, SlowCarry& cy, const SlowBlend& q0, FxAcc& ra, FxAcc& rb) {
+  // per-plane constants, loaded at the top of the plane so the derive phase covers their latency
+  struct PlaneConst {
+    float idz, idzf, damp_c, damp_f, uref, vref;
+  };
+  auto plane_const = [&](int k) {
+    PlaneConst pc{__ldg(a.idz_c + k), k > 0 ? __ldg(a.idz_f + k) : 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    if (a.damp_c) {
+      pc.damp_c = __ldg(a.damp_c + k);
+      pc.damp_f = __ldg(a.damp_f + k);
+      pc.uref = __ldg(a.uref + k);
+      pc.vref = __ldg(a.vref + k);
+    }
+    return pc;
+  };
+  auto column = [&](int k, int r, int gj, bool own, SlowCarry& cy, const SlowBlend& q0, FxAcc& ra, FxAcc& rb,
+                    const PlaneConst& kc) {
     const float* sr = ring + (k % NSLOT) * slot;
     const float* sn = ring + ((k + 1) % NSLOT) * slot;
     const float* uc = der + D_UC + (k % 3) * DN;
@@ -191,7 +206,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
       tt = theta_of(sn[R_RHO + b], RT(sn, b));
     }
     const float tb = k > 0 ? cy.th : tc;
-    const float idz = __ldg(a.idz_c + k);
+    const float idz = kc.idz;
     // ---- cell: K2 compute_cell_tendencies_kernel (dry_core.cu:62-144)
     {
       const float fw = uf, fe = U(sr, b + 1), fs = vf, fn = V(sr, b + BW);
@@ -241,7 +256,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         if (!top) flt = upwind(0.5f * (wc[d - 1] + wc[d]), qc, qt);
         t_u = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
         t_u += -((pc - pp[d - 1]) * idx);
-        if (a.damp_c) t_u += -__ldg(a.damp_c + k) * (qc - __ldg(a.uref + k));
+        if (a.damp_c) t_u += -kc.damp_c * (qc - kc.uref);
       }
       float u1 = fmaxf(-1.0e30f, uf + dt * t_u);
       if (blend) u1 = a.wa * q0.u + a.wb * u1;
@@ -264,7 +279,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         if (!top) flt = upwind(0.5f * (wc[d - DW] + wc[d]), qc, qt);
         t_v = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
         t_v += -((pc - pp[d - DW]) * idy);
-        if (a.damp_c) t_v += -__ldg(a.damp_c + k) * (qc - __ldg(a.vref + k));
+        if (a.damp_c) t_v += -kc.damp_c * (qc - kc.vref);
       }
       float v1 = fmaxf(-1.0e30f, vf + dt * t_v);
       if (blend) v1 = a.wa * q0.v + a.wb * v1;
@@ -284,14 +299,14 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         if (!(gj + 1 == ny && open_y)) fln = upwind(0.5f * (vcm[d] + vc[d]), qc, qn);
         const float flb = upwind(wcm[d], qb, qc);
         const float flt = upwind(wc[d], qc, qt);
-        const float idzf = __ldg(a.idz_f + k);
+        const float idzf = kc.idzf;
         t_w = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idzf);
         const float tf = 0.5f * (cy.th + tc);
         const float trf = 0.5f * (s_thref[k - 1] + s_thref[k]);
         const float rf = 0.5f * (cy.rho + rho);
         const float bu = a.gravity * (tf - trf) / fmaxf(trf, 1.0e-6f);
         t_w += rf * bu;
-        if (a.damp_c) t_w += -__ldg(a.damp_f + k) * qc;
+        if (a.damp_c) t_w += -kc.damp_f * qc;
       }
       float w1 = fmaxf(-1.0e30f, wf + dt * t_w);
       if (blend) w1 = a.wa * q0.w + a.wb * w1;
@@ -314,6 +329,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
   bool aborted = false;
   for (int k = 0; k < nz; ++k) {
     const int pb = k & 1;
+    const PlaneConst kc = plane_const(k);
     // ---- derive plane k: theta, p', uc, vc, wc at the 34 x 18 positions
     wait_plane(k + 1, k);
     {
@@ -351,8 +367,8 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     }
     // ---- cells and faces of plane k
     FxAcc ra, rb;
-    column(k, ty + 1, gj0, own0, ca, q0a, ra, rb);
-    column(k, ty + RY + 1, gj1, own1, cb, q0b, ra, rb);
+    column(k, ty + 1, gj0, own0, ca, q0a, ra, rb, kc);
+    column(k, ty + RY + 1, gj1, own1, cb, q0b, ra, rb, kc);
     if (xf) {  // open east boundary: X face nx of row j0+tx
       const float* sr = ring + (k % NSLOT) * slot;
       const float uf = U(sr, (tx + 1) * BW + w + 4);

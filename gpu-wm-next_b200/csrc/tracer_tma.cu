@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
   load_q0(gj1, own1, 0, q0b);
 
   // one owned column of plane k
-  auto column = [&](int k, int r, int gj, bool own, float* qb, const float* q0v) {
+  auto column = [&](int k, int r, int gj, bool own, float* qb, const float* q0v, float idz) {
     const float* st = ring + (k % NSLOT) * SLOT;
     const float* sn = ring + ((k + 1) % NSLOT) * SLOT;
     const int c = tx + 1;
@@ -142,7 +142,6 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
     const float fw = st[O_U + (r - 1) * FBW + tx], fe = st[O_U + (r - 1) * FBW + tx + 1];
     const float fs = st[O_V + (r - 1) * FBW + tx], fn = st[O_V + r * FBW + tx];
     const float fb = st[O_W + (r - 1) * OBW + tx], ft = sn[O_W + (r - 1) * OBW + tx];
-    const float idz = __ldg(a.idz_c + k);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) {
       if (t >= a.ntracers) break;
@@ -169,13 +168,14 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
   for (int k = 0; k < nz; ++k) {
     // mixing ratios of plane k+1 (the own ones are this thread's, the ring published
     // by the barrier below for the next plane)
+    const float idz = __ldg(a.idz_c + k);  // loaded ahead of the mixing-ratio work
     float n0a[NTR], n0b[NTR];
     load_q0(gj0, own0, k + 1, n0a);
     load_q0(gj1, own1, k + 1, n0b);
     wait_plane(k + 1, k);
     if (k + 1 < nz) mix(k + 1);
-    column(k, ty + 1, gj0, own0, qb0, q0a);
-    column(k, ty + RY + 1, gj1, own1, qb1, q0b);
+    column(k, ty + 1, gj0, own0, qb0, q0a, idz);
+    column(k, ty + RY + 1, gj1, own1, qb1, q0b, idz);
 #pragma unroll
     for (int t = 0; t < NTR; ++t) { q0a[t] = n0a[t]; q0b[t] = n0b[t]; }
     __syncthreads();  // publishes plane k+1's ring; slot k is free
