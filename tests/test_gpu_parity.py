@@ -498,6 +498,29 @@ def test_tma_substep_bit_exact(gwm, periodic):
         assert np.array_equal(outs[0][k], outs[3][k]), k
 
 
+@pytest.mark.parametrize("nz", [1, 2, 3, 5])
+def test_tma_kernels_on_shallow_columns(gwm, nz):
+    # columns with fewer planes than the TMA rings hold ahead (the substep keeps three
+    # planes in flight, the slow and tracer stages two): every TMA kernel must agree bit
+    # for bit with its per-thread-load counterpart
+    g = gwm.GridSpec(40, 20, nz, dx=2000.0, dy=2000.0, z_top=1500.0 * nz)
+    p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=4, relative_humidity=1.02)
+    s = gwm.build_case("moist_sounding", g, p, moist=True)
+    step = gwm.StepConfig(dt=1.0, fast_substeps=4)
+    rain = gwm.WarmRainConfig(dt=1.0, rain_terminal_velocity=12.0)
+    outs = {}
+    for tiles in ((0, 16, 16), (3, 3, 3)):
+        with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=True)) as m:
+            for kernel, r in zip(("fast_substep", "slow_stage", "tracer_stage"), tiles):
+                m.set_tile(kernel, r)
+            m.upload(s)
+            m.step(2)
+            outs[tiles[0]] = m.download()
+    for k in outs[0]:
+        assert np.isfinite(outs[3][k]).all(), k
+        assert np.array_equal(outs[0][k], outs[3][k]), k
+
+
 @pytest.mark.parametrize("periodic", [True, False])
 def test_tma_slow_stage_without_fast_modes(gwm, periodic):
     # the TMA slow stage on stage inputs without acoustic increments (fast modes off)
