@@ -19,6 +19,9 @@
 // tracer masses rho*qv, rho*qc, rho*qr (nz, ny, nx).
 // Output file: "GWMOUT01", then the same state arrays after `steps` steps and,
 // when moist, the surface precipitation (ny, nx).
+// Each step's wall time (host clock around the step and a device synchronisation) goes
+// to stderr as "step <n> ms <t>", so the reference's own GPU step can be timed too.
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -184,6 +187,8 @@ int run(const char* in_path, const char* out_path) {
   gwm::dycore::FastModeIntegrator& fm = h.fast_modes ? static_cast<gwm::dycore::FastModeIntegrator&>(fast)
                                                      : static_cast<gwm::dycore::FastModeIntegrator&>(no_fast);
   for (int step = 0; step < h.steps; ++step) {
+    if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("device error before a step");
+    const auto t0 = std::chrono::steady_clock::now();
     gwm::dycore::advance_dry_state_ssprk3(states, layout, metrics, cfg, boundary, fm);
     if (h.moist) {
       gwm::dycore::advance_passive_tracers_ssprk3(tracers, states, layout, metrics, cfg, tracer_boundary);
@@ -192,6 +197,9 @@ int run(const char* in_path, const char* out_path) {
       else if (h.rain_mode == 2)
         gwm::physics::apply_warm_rain_microphysics(states, tracers, rc, &accum);
     }
+    if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("device error in a step");
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    std::fprintf(stderr, "step %d ms %.3f\n", step, ms);
   }
   if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("device error after the steps");
 
