@@ -166,19 +166,17 @@ __device__ __forceinline__ double acc_read(const unsigned long long* acc, double
 // Per-thread fixed-point accumulator for at most 4 cells (the warp's sum of lo
 // parts must stay below 2^32), reduced across
 // the warp with two 32-bit integer reductions.  A cell's fixed-point value
-// x = rint(v * scale) (the integer fx() returns) is split as x = hi * 2^24 + lo
-// with 0 <= lo < 2^24; every step is exact in FP32 (x and hi * 2^24 are integers
-// representable in FP32, their difference is below 2^24).  The warp total
-// sum(hi) * 2^24 + sum(lo) therefore equals the int64 sum of fx() over the same
-// cells, bit for bit, at a fraction of the cost of 64-bit shuffles.
+// x = fx(v, scale) is split as x = hi * 2^24 + lo with 0 <= lo < 2^24 (an arithmetic
+// shift and a mask of the int64).  The warp total sum(hi) * 2^24 + sum(lo) therefore
+// equals the int64 sum of fx() over the same cells, bit for bit, at a fraction of the
+// cost of 64-bit shuffles.
 struct FxAcc {
   int hi = 0;
   unsigned lo = 0;
   __device__ __forceinline__ void add(float v, float scale) {
-    const float x = rintf(v * scale);
-    const float h = floorf(x * 5.9604644775390625e-08f);  // 2^-24
-    hi += (int)h;
-    lo += (unsigned)fmaf(-h, 16777216.0f, x);
+    const long long x = fx(v, scale);
+    hi += (int)(x >> 24);
+    lo += (unsigned)(x & 0xffffffLL);
   }
   // warp total (all lanes get it); every lane of the warp must call it
   __device__ __forceinline__ long long warp_total() const {
