@@ -29,3 +29,37 @@ def test_documented_adapter_compiles_against_reference_headers():
     if "reference tree absent" in out:
         pytest.skip("reference tree absent")
     assert r.returncode == 0 and "adapter-ok" in out, out[-2000:]
+
+
+SNIPPET_PARAMS = {
+    "check(gwm_b200_set_boundary_state": (
+        "gwm_b200_ctx* ctx, int member, float* rho_b, float* rt_b, float* u_b, float* v_b, float* w_b, "
+        "float* qv_b, float* qc_b, float* qr_b, const double* u_ref_per_level, const double* v_ref_per_level, "
+        "float* x_dev, float* y_dev, long long capacity, unsigned long long seed, float* params, float* norm, "
+        "float* range, double* loss_per_epoch"),
+    "gwm_b200_scalar_desc d{": "int nx, int ny, int nz, float* q_dev, void* stream",
+}
+
+
+def test_documented_abi_calls_compile_against_the_header():
+    # the C listings of INTEGRATION.md's call reference, each wrapped in a function whose
+    # parameters are the listing's free names, compiled against include/gwm_b200.h
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    text = open(os.path.join(ROOT, "INTEGRATION.md"), encoding="utf-8").read()
+    blocks = re.findall(r"```cpp\n(.*?)```", text, re.S)
+    parts = ['#include "gwm_b200.h"', "static void check(int) {}"]
+    found = 0
+    for n, block in enumerate(blocks):
+        for marker, params in SNIPPET_PARAMS.items():
+            if marker in block:
+                parts.append(f"void listing_{n}({params}) {{\n{block}\n}}")
+                found += 1
+    assert found == len(SNIPPET_PARAMS), "a listing of INTEGRATION.md section 3 is missing"
+    with tempfile.TemporaryDirectory() as tmp:
+        src = os.path.join(tmp, "listings.cpp")
+        with open(src, "w") as f:
+            f.write("\n".join(parts) + "\n")
+        r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-Werror", "-Wno-unused-variable",
+                            "-I", os.path.join(ROOT, "include"), src], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-3000:]
