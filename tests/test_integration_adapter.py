@@ -1,7 +1,10 @@
-"""The C++ adapter that INTEGRATION.md gives gwm-next maintainers compiles against the
-reference's own headers (dry_core.hpp's DryState, SubdomainDescriptor, GridMetrics and
-DryStepperConfig) and this library's C-ABI header.  Runs where the reference tree is
-present; otherwise it is skipped."""
+"""The integration guide's listings compile: the C++ adapter it gives gwm-next
+maintainers against the reference's own headers (dry_core.hpp's DryState,
+SubdomainDescriptor, GridMetrics and DryStepperConfig) and this library's C-ABI header
+(skipped where the reference tree is absent), and its C call listings against the C-ABI
+header alone."""
+
+GUIDE = "INTEGRATION.md"  # the integration guide at the repository root
 import os
 import re
 import shutil
@@ -16,9 +19,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def test_documented_adapter_compiles_against_reference_headers():
     if shutil.which("nvcc") is None:
         pytest.skip("nvcc not available")
-    text = open(os.path.join(ROOT, "INTEGRATION.md"), encoding="utf-8").read()
+    text = open(os.path.join(ROOT, GUIDE), encoding="utf-8").read()
     m = re.search(r"```cpp\n(// gwm_b200_adapter\.cpp.*?)```", text, re.S)
-    assert m, "adapter listing not found in INTEGRATION.md"
+    assert m, "adapter listing not found in the integration guide"
     with tempfile.TemporaryDirectory() as tmp:
         src = os.path.join(tmp, "gwm_b200_adapter.cpp")
         with open(src, "w") as f:
@@ -42,11 +45,11 @@ SNIPPET_PARAMS = {
 
 
 def test_documented_abi_calls_compile_against_the_header():
-    # the C listings of INTEGRATION.md's call reference, each wrapped in a function whose
+    # the guide's C call listings, each wrapped in a function whose
     # parameters are the listing's free names, compiled against include/gwm_b200.h
     if shutil.which("g++") is None:
         pytest.skip("g++ not available")
-    text = open(os.path.join(ROOT, "INTEGRATION.md"), encoding="utf-8").read()
+    text = open(os.path.join(ROOT, GUIDE), encoding="utf-8").read()
     blocks = re.findall(r"```cpp\n(.*?)```", text, re.S)
     parts = ['#include "gwm_b200.h"', "static void check(int) {}"]
     found = 0
@@ -55,7 +58,7 @@ def test_documented_abi_calls_compile_against_the_header():
             if marker in block:
                 parts.append(f"void listing_{n}({params}) {{\n{block}\n}}")
                 found += 1
-    assert found == len(SNIPPET_PARAMS), "a listing of INTEGRATION.md section 3 is missing"
+    assert found == len(SNIPPET_PARAMS), "a C call listing of the integration guide is missing"
     with tempfile.TemporaryDirectory() as tmp:
         src = os.path.join(tmp, "listings.cpp")
         with open(src, "w") as f:
