@@ -4,7 +4,6 @@ SubdomainDescriptor, GridMetrics and DryStepperConfig) and this library's C-ABI 
 (skipped where the reference tree is absent), and its C call listings against the C-ABI
 header alone."""
 
-GUIDE = "INTEGRATION.md"  # the integration guide at the repository root
 import os
 import re
 import shutil
@@ -14,6 +13,7 @@ import tempfile
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GUIDE = "INTEGRATION.md"  # the integration guide at the repository root
 
 
 def test_documented_adapter_compiles_against_reference_headers():
