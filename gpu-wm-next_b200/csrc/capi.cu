@@ -403,28 +403,31 @@ cudaError_t launch_stage(gwm_b200_ctx* c, const Member& M, const SlowArgs& a, bo
 
 // One acoustic substep: the TMA-fed kernel when selected on flat terrain, else the
 // owned-tile or overlapped-tile kernels.
-cudaError_t launch_substep(gwm_b200_ctx* c, const Member& M, const FastArgs& f, bool first, bool terr) {
+// p_ready: the first substep's p' (with its halo) is in f.p_in, written by the slow stage
+cudaError_t launch_substep(gwm_b200_ctx* c, const Member& M, const FastArgs& f, bool first, bool terr,
+                           bool p_ready = false) {
   if (!terr && c->fast_tile_rows == kFastTma) {
     FastMaps m{};
     const bool fin = f.final_kind == 2;
-    // rho and theta with the halo ring in the first substep (p' is derived there), owned
-    // boxes otherwise
-    const CUtensorMap* rho = M.tmap(f.rho_in, first ? 0 : 2);
-    const CUtensorMap* th = M.tmap(f.th, first ? 0 : 2);
+    const bool pin = !first || p_ready;  // p' loaded with its ring, not derived
+    // rho and theta with the halo ring where p' is derived from them, owned boxes otherwise
+    const CUtensorMap* rho = M.tmap(f.rho_in, pin ? 2 : 0);
+    const CUtensorMap* th = M.tmap(f.th, pin ? 2 : 0);
     const CUtensorMap* du = first ? nullptr : M.tmap(f.du_in, 1);
     const CUtensorMap* dv = first ? nullptr : M.tmap(f.dv_in, 1);
     const CUtensorMap* dw = first ? nullptr : M.tmap(f.dw_in, 2);
     const CUtensorMap* bu = fin ? M.tmap(f.bu, 2) : nullptr;
     const CUtensorMap* bv = fin ? M.tmap(f.bv, 2) : nullptr;
     const CUtensorMap* bw = fin ? M.tmap(f.bw, 2) : nullptr;
-    const CUtensorMap* pm = first ? nullptr : M.tmap(f.p_in, 0);
-    if (!rho || !th || (!first && (!du || !dv || !dw || !pm)) || (fin && (!bu || !bv || !bw)) ||
+    const CUtensorMap* pm = pin ? M.tmap(f.p_in, 0) : nullptr;
+    if (!rho || !th || (!first && (!du || !dv || !dw)) || (pin && !pm) || (fin && (!bu || !bv || !bw)) ||
         (f.final_kind == 0 && !f.p_out))
       return cudaErrorInvalidValue;
     m.rho = *rho; m.th = *th;
-    if (!first) { m.du = *du; m.dv = *dv; m.dw = *dw; m.p = *pm; }
+    if (!first) { m.du = *du; m.dv = *dv; m.dw = *dw; }
+    if (pin) m.p = *pm;
     if (fin) { m.bu = *bu; m.bv = *bv; m.bw = *bw; }
-    return launch_fast_tma(f, m, first, c->stream);
+    return launch_fast_tma(f, m, first, p_ready, c->stream);
   }
   return launch_fast(f, first, terr, c->stream, c->fast_tile_rows);
 }
@@ -595,6 +598,11 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
     a.acc_a = M.slot(M.ring + 1); a.acc_b = M.slot(M.ring + 1) + kMaxNz;
     a.clr_a = M.slot(M.ring + 2); a.clr_b = M.slot(M.ring + 2) + kMaxNz;
     a.acc_mode = fast ? (terr ? 0 : 1) : ((s == 2 && rain_theta) ? 0 : 2);
+    // the TMA slow stage stores the p' it evaluates for the level sums, and the first
+    // substep (TMA too) loads it with its ring instead of deriving it again
+    const bool p_handoff = fast && !terr && a.acc_mode == 1 && c->slow_tile_rows == kSlowTma &&
+                           c->fast_tile_rows == kFastTma;
+    if (p_handoff) a.p_out = M.P[rnext];
     a.inv_count = inv_count(M);
     a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf; a.base = M.base;
     a.err = M.err;
@@ -638,7 +646,7 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
       f.clr_a = M.slot(M.ring + 2); f.clr_b = M.slot(M.ring + 2) + kMaxNz;
       f.zc = M.zc; f.idz_c = M.idc; f.idz_f = M.idf; f.base = M.base;
       f.err = M.err;
-      LAUNCH(launch_substep(c, M, f, n == 0, terr), "fast substep");
+      LAUNCH(launch_substep(c, M, f, n == 0, terr, n == 0 && p_handoff), "fast substep");
       M.ring = (M.ring + 1) % 3;
       rcur ^= 1;
       dcur = dout;

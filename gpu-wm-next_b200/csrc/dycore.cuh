@@ -31,6 +31,8 @@ struct SlowArgs {
   unsigned long long *acc_a, *acc_b; // level sums of the output (see acc_mode)
   unsigned long long *clr_a, *clr_b; // ring slot cleared by block (0,0)
   int acc_mode;                     // 0 none, 1 rho & p of output, 2 theta of output
+  float* p_out;                     // acc_mode 1, TMA kernel only: p' of the output (owned cells
+                                    // and periodic halo), for the first substep (may be null)
   double inv_count;                 // 1 / (nx*ny)
   const float *zc, *idz_c, *idz_f;  // metrics: padded 3-D (terrain) or per level (flat)
   const double* base;               // FP64 base state [rt_ref | 1/rt_ref | p_ref] per level
@@ -74,12 +76,13 @@ struct FastArgs {
 // TMA descriptors of one acoustic substep (flat terrain, k_fast_tma): 3-D tiled maps
 // over the padded field layout (dims pitch x rows x (nz+1), FP32, no swizzle).
 struct FastMaps {
-  CUtensorMap rho, th;     // first substep of a stage: box 40 x 18, cells with the halo ring;
-                           // other substeps: box 32 x 16, owned cells
+  CUtensorMap rho, th;     // first substep of a stage deriving p': box 40 x 18, cells with
+                           // the halo ring; otherwise box 32 x 16, owned cells
   CUtensorMap du, dv;      // box 36 x 17: owned faces + the tile's east/north face
   CUtensorMap dw;          // box 32 x 16
   CUtensorMap bu, bv, bw;  // box 32 x 16 (last substep of the step)
-  CUtensorMap p;           // box 40 x 18: p'(rho_in) with the halo ring (not the first substep)
+  CUtensorMap p;           // box 40 x 18: p'(rho_in) with the halo ring (loaded unless the
+                           // first substep derives it)
 };
 // Box extents (x, y) of the maps above.
 constexpr int kTmaCellBox[2] = {40, 18};
@@ -106,7 +109,9 @@ cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_
 cudaError_t launch_slow_tma(const SlowArgs& a, const SlowMaps& m, cudaStream_t s);
 cudaError_t init_slow_tma();
 // Flat-terrain acoustic substep fed by TMA tile loads (owned 32 x 16 tiles).
-cudaError_t launch_fast_tma(const FastArgs& a, const FastMaps& m, bool first, cudaStream_t s);
+// first: the first substep of a stage (no increments in); p_ready: its p' (with the
+// halo ring) is in a.p_in, written by the slow stage, instead of derived from rho, theta
+cudaError_t launch_fast_tma(const FastArgs& a, const FastMaps& m, bool first, bool p_ready, cudaStream_t s);
 // One-time kernel attributes (dynamic shared memory) of the TMA substep.
 cudaError_t init_fast_tma();
 cudaError_t launch_level_sums(const LevelSumArgs& a, cudaStream_t s);

@@ -6,17 +6,17 @@
 // plane's tiles with cp.async.bulk.tensor.3d into a four-slot shared-memory ring,
 // three planes ahead of the compute, and the 256 threads work from shared memory.
 // Per plane k the ring slot holds
-//   rho(k), theta(k)        first substep of a stage: 40 x 18 boxes, columns i0-4 .. i0+35,
-//                           rows j0-1 .. j0+16 (the owned 32 x 16 tile and its one-cell
-//                           halo ring, from which p' is derived; the box starts 4 columns
-//                           left so x stays 16-byte aligned); other substeps: the owned
+//   rho(k), theta(k)        first substep of a stage deriving p': 40 x 18 boxes, columns
+//                           i0-4 .. i0+35, rows j0-1 .. j0+16 (the owned 32 x 16 tile and
+//                           its one-cell halo ring, from which p' is derived; the box starts
+//                           4 columns left so x stays 16-byte aligned); otherwise the owned
 //                           32 x 16 box (p' comes with its halo below)
 //   du(k), dv(k)            36 x 17 box: owned faces plus the tile's east/north face
 //   dw(k+1)                 32 x 16 box: owned Z faces above the plane
 //   p'(k)                   40 x 18 box like the first substep's rho: the pressure
 //                           perturbation the previous substep computed for its level sums
-//                           (every substep but the first of a stage), so the EOS runs once
-//                           per cell per substep
+//                           (the slow stage, for the first substep of a stage, when it ran
+//                           on the TMA path), so the EOS runs once per cell per substep
 //   bu(k), bv(k), bw(k+1)   32 x 16 boxes, last substep of the step only (m = B + D)
 // so the kernel issues no per-thread global loads on the main path, holds no load
 // pipeline in registers and needs no halo threads reading global memory.  The level
@@ -43,41 +43,50 @@ constexpr int ISSUER = NT - 32;
 // base-momentum boxes are only present, and the slot only that long, in the last
 // substep of the step.  RW, R0, C0: row width of the rho/theta boxes and the box
 // position of owned cell (0, 0).
-template <bool FIRST> struct Slot;
-template <> struct Slot<true> {  // first substep of a stage: rho, theta with the halo ring
+template <bool FIRST, bool PIN> struct Slot;  // PIN: p' loaded (with its ring) by TMA
+template <> struct Slot<true, false> {  // first substep deriving p': rho, theta with the halo ring
   static constexpr int O_RHO = 0, O_TH = 736, O_DU = 0, O_DV = 0, O_DW = 0, O_P = 0, O_BU = 1472, O_BV = 1984,
                        O_BW = 2496, LONG = 3008, SHORT = 1472, RW = CBW, R0 = 1, C0 = 4;
 };
-template <> struct Slot<false> {  // inner substeps: owned rho, theta; increments; p' with its ring
+template <> struct Slot<true, true> {  // first substep with p' from the slow stage: owned rho, theta; p'
+  static constexpr int O_RHO = 0, O_TH = 512, O_DU = 0, O_DV = 0, O_DW = 0, O_P = 1024, O_BU = 1760,
+                       O_BV = 2272, O_BW = 2784, LONG = 3296, SHORT = 1760, RW = OBW, R0 = 0, C0 = 0;
+};
+template <> struct Slot<false, true> {  // inner substeps: owned rho, theta; increments; p' with its ring
   static constexpr int O_RHO = 0, O_TH = 512, O_DU = 1024, O_DV = 1664, O_DW = 2304, O_P = 2816, O_BU = 3552,
                        O_BV = 4064, O_BW = 4576, LONG = 5088, SHORT = 3552, RW = OBW, R0 = 0, C0 = 0;
 };
-template <bool FIRST>
+template <bool FIRST, bool PIN>
 constexpr bool slot_ok() {
-  using L = Slot<FIRST>;
-  constexpr int rb = FIRST ? CBW * CBH : OBW * OBH;
+  using L = Slot<FIRST, PIN>;
+  constexpr int rb = (FIRST && !PIN) ? CBW * CBH : OBW * OBH;  // rho, theta boxes
+  constexpr int after_th = !FIRST ? L::O_DU : (PIN ? L::O_P : L::O_BU);
   return L::O_TH % 32 == 0 && L::O_BU % 32 == 0 && L::O_BV % 32 == 0 && L::O_BW % 32 == 0 &&
          L::LONG % 32 == 0 && L::SHORT % 32 == 0 && L::SHORT == L::O_BU && L::O_TH - L::O_RHO >= rb &&
-         (FIRST ? L::O_BU - L::O_TH >= rb
-                : (L::O_DU % 32 == 0 && L::O_DV % 32 == 0 && L::O_DW % 32 == 0 && L::O_P % 32 == 0 &&
-                   L::O_DU - L::O_TH >= rb && L::O_DV - L::O_DU >= FBW * FBH && L::O_DW - L::O_DV >= FBW * FBH &&
-                   L::O_P - L::O_DW >= OBW * OBH && L::O_BU - L::O_P >= CBW * CBH)) &&
+         after_th - L::O_TH >= rb &&
+         (FIRST || (L::O_DU % 32 == 0 && L::O_DV % 32 == 0 && L::O_DW % 32 == 0 &&
+                    L::O_DV - L::O_DU >= FBW * FBH && L::O_DW - L::O_DV >= FBW * FBH &&
+                    L::O_P - L::O_DW >= OBW * OBH)) &&
+         (!PIN || (L::O_P % 32 == 0 && L::O_BU - L::O_P >= CBW * CBH)) &&
          L::O_BV - L::O_BU >= OBW * OBH && L::O_BW - L::O_BV >= OBW * OBH && L::LONG - L::O_BW >= OBW * OBH;
 }
-static_assert(slot_ok<true>() && slot_ok<false>(), "128-byte aligned sub-buffers that fit their boxes");
+static_assert(slot_ok<true, false>() && slot_ok<true, true>() && slot_ok<false, true>(),
+              "128-byte aligned sub-buffers that fit their boxes");
 // dynamic shared memory: the ring, then the level tables (2 double + 4 float per level)
 constexpr size_t kLevelBytes = 2 * sizeof(double) + 4 * sizeof(float);
-template <bool FIRST>
+template <bool FIRST, bool PIN>
 constexpr size_t dyn_smem(bool final_step, int nz) {
-  return size_t(final_step ? Slot<FIRST>::LONG : Slot<FIRST>::SHORT) * NSLOT * sizeof(float) + 128 +
+  return size_t(final_step ? Slot<FIRST, PIN>::LONG : Slot<FIRST, PIN>::SHORT) * NSLOT * sizeof(float) + 128 +
          kLevelBytes * size_t(nz);
 }
 }  // namespace ft
 
-template <bool FIRST>
+// FIRST: the first substep of a stage (no increments in).  PIN: p' of the input (with its
+// ring) is loaded; otherwise (first substep only) it is derived from rho and theta.
+template <bool FIRST, bool PIN>
 __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const __grid_constant__ FastMaps m) {
   using namespace ft;
-  using L = Slot<FIRST>;
+  using L = Slot<FIRST, PIN>;
   constexpr int O_RHO = L::O_RHO, O_TH = L::O_TH, O_DU = L::O_DU, O_DV = L::O_DV, O_DW = L::O_DW, O_P = L::O_P,
                 O_BU = L::O_BU, O_BV = L::O_BV, O_BW = L::O_BW, RW = L::RW, R0 = L::R0, C0 = L::C0;
   extern __shared__ unsigned char s_dyn[];
@@ -144,12 +153,13 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     float* st = ring + (kk % NSLOT) * slot;
     uint64_t* bar = &s_bar[kk % NSLOT];
     const bool wface = kk + 1 < nz;
-    unsigned bytes = FIRST ? 2 * B_CELL : 2 * B_OWN;
-    if (!FIRST) bytes += 2 * B_FACE + (wface ? B_OWN : 0u) + B_CELL;
+    unsigned bytes = (FIRST && !PIN) ? 2 * B_CELL : 2 * B_OWN;
+    if (!FIRST) bytes += 2 * B_FACE + (wface ? B_OWN : 0u);
+    if (PIN) bytes += B_CELL;
     if (final_step) bytes += 3 * B_OWN;
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(bar, bytes);
-    if (FIRST) {  // with the halo ring
+    if (FIRST && !PIN) {  // with the halo ring
       tma_load_3d(st + O_RHO, &m.rho, i0 + kXOff - 4, j0, kk, bar);
       tma_load_3d(st + O_TH, &m.th, i0 + kXOff - 4, j0, kk, bar);
     } else {  // owned cells
@@ -160,8 +170,8 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
       tma_load_3d(st + O_DU, &m.du, i0 + kXOff, j0 + 1, kk, bar);
       tma_load_3d(st + O_DV, &m.dv, i0 + kXOff, j0 + 1, kk, bar);
       if (wface) tma_load_3d(st + O_DW, &m.dw, i0 + kXOff, j0 + 1, kk + 1, bar);
-      tma_load_3d(st + O_P, &m.p, i0 + kXOff - 4, j0, kk, bar);
     }
+    if (PIN) tma_load_3d(st + O_P, &m.p, i0 + kXOff - 4, j0, kk, bar);
     if (final_step) {
       tma_load_3d(st + O_BU, &m.bu, i0 + kXOff, j0 + 1, kk, bar);
       tma_load_3d(st + O_BV, &m.bv, i0 + kXOff, j0 + 1, kk, bar);
@@ -195,7 +205,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     for (int kk = 1; kk < AHEAD && kk < nz; ++kk) { issue(kk); issued = kk; }
   }
   wait_plane(0, 0);
-  if (FIRST) plane_p(0);
+  if (FIRST && !PIN) plane_p(0);
   float dwc0 = 0.f, dwc1 = 0.f;  // increment at face k (face 0 never changes)
   float bwz0 = 0.f, bwz1 = 0.f;  // base momentum at face 0 (last substep of the step)
   if (final_step) {
@@ -212,13 +222,13 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     // ---- pressure perturbation of plane k+1 (its tiles were issued a plane ago)
     if (k + 1 < nz) {
       wait_plane(k + 1, k);
-      if (FIRST) plane_p(k + 1);
+      if (FIRST && !PIN) plane_p(k + 1);
     }
     // ---- faces of plane k: K12/K13 horizontal momenta, K14 vertical momentum at face k+1
     // p'(r, c) of plane k (P0) and k+1 (P1) in s_p coordinates (row 0 = j0-1, column
-    // 0 = i0-1): computed above in the first substep, loaded with the tiles otherwise
-    auto P0 = [&](int r, int c) { return FIRST ? s_p[pb][r][c] : st[O_P + r * CBW + c + 3]; };
-    auto P1 = [&](int r, int c) { return FIRST ? s_p[pb ^ 1][r][c] : stn[O_P + r * CBW + c + 3]; };
+    // 0 = i0-1): loaded with the tiles, or derived above in a first substep
+    auto P0 = [&](int r, int c) { return PIN ? st[O_P + r * CBW + c + 3] : s_p[pb][r][c]; };
+    auto P1 = [&](int r, int c) { return PIN ? stn[O_P + r * CBW + c + 3] : s_p[pb ^ 1][r][c]; };
     float du0 = 0.f, dv0 = 0.f, du1 = 0.f, dv1 = 0.f, dw0 = 0.f, dw1 = 0.f;
     if (!FIRST) {
       du0 = st[O_DU + ty * FBW + tx];
@@ -366,20 +376,24 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
 }  // namespace
 
 cudaError_t init_fast_tma() {
-  cudaError_t e = cudaFuncSetAttribute(k_fast_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)ft::dyn_smem<true>(true, kMaxNz));
+  cudaError_t e = cudaFuncSetAttribute(k_fast_tma<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ft::dyn_smem<true, false>(true, kMaxNz));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_fast_tma<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ft::dyn_smem<true, true>(true, kMaxNz));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_fast_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)ft::dyn_smem<false>(true, kMaxNz));
+  return cudaFuncSetAttribute(k_fast_tma<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)ft::dyn_smem<false, true>(true, kMaxNz));
 }
 
-cudaError_t launch_fast_tma(const FastArgs& a, const FastMaps& m, bool first, cudaStream_t s) {
+cudaError_t launch_fast_tma(const FastArgs& a, const FastMaps& m, bool first, bool p_ready, cudaStream_t s) {
   if (a.g.nz > kMaxNz || a.g.nz < 1 || !a.err) return cudaErrorInvalidValue;
   const dim3 block(ft::TX, ft::RY);
   const dim3 grid((a.g.nx + ft::TX - 1) / ft::TX, (a.g.ny + ft::TY - 1) / ft::TY);
   const bool fin = a.final_kind == 2;
-  if (first) k_fast_tma<true><<<grid, block, ft::dyn_smem<true>(fin, a.g.nz), s>>>(a, m);
-  else k_fast_tma<false><<<grid, block, ft::dyn_smem<false>(fin, a.g.nz), s>>>(a, m);
+  if (first && p_ready) k_fast_tma<true, true><<<grid, block, ft::dyn_smem<true, true>(fin, a.g.nz), s>>>(a, m);
+  else if (first) k_fast_tma<true, false><<<grid, block, ft::dyn_smem<true, false>(fin, a.g.nz), s>>>(a, m);
+  else k_fast_tma<false, true><<<grid, block, ft::dyn_smem<false, true>(fin, a.g.nz), s>>>(a, m);
   return cudaGetLastError();
 }
 

@@ -232,8 +232,11 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         store_tile(a.o_rho, g, kCell, gi, gj, k, r1, edge);
         store_tile(a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1, edge);
         if (a.acc_mode == 1) {
+          // p' of the output: the level sums, and (stored) the first substep's input
+          const float pv = eos_pprime_ref(r1, r1 * th1, s_binv[k], s_bpr[k]);
           ra.add(r1, kFxRho);
-          rb.add(eos_pprime_ref(r1, r1 * th1, s_binv[k], s_bpr[k]), kFxP);
+          rb.add(pv, kFxP);
+          if (a.p_out) store_tile(a.p_out, g, kCell, gi, gj, k, pv, edge);
         } else if (a.acc_mode == 2) {
           ra.add(th1, kFxTheta);
         }
