@@ -206,6 +206,7 @@ def lib():
     L.gwm_b200_dry_pressure.argtypes = [vp, vp, vp, C.c_longlong, vp]
     L.gwm_b200_field_stats_noalloc.argtypes = [vp, C.c_longlong, vp, vp]
     L.gwm_b200_scalar_ssprk3.argtypes = [C.POINTER(_ScalarDesc), vp, C.c_int, vp]
+    L.gwm_b200_grid_z_center.argtypes = [C.POINTER(_Grid), vp]
     L.gwm_b200_ranks_to_global.argtypes = [C.POINTER(_LayoutDesc), C.c_int,
                                            C.POINTER(C.c_void_p), vp]
     L.gwm_b200_global_to_ranks.argtypes = [C.POINTER(_LayoutDesc), C.c_int, vp,
@@ -639,6 +640,17 @@ def dry_pressure(rho_ptr: int, rho_theta_ptr: int, p_ptr: int, n: int, stream: O
     rc = lib().gwm_b200_dry_pressure(rho_ptr, rho_theta_ptr, p_ptr, n, stream)
     if rc != OK:
         raise RuntimeError(f"dry_pressure: status {rc}")
+
+
+def grid_z_center(grid: "GridSpec") -> np.ndarray:
+    """Cell-centre heights of a grid (GridMetrics::z_center, grid_metrics.hpp:87-239: FP64
+    compute, FP32 result), shape (nz, ny, nx); host code, no device needed."""
+    out = np.empty((grid.nz, grid.ny, grid.nx), dtype=np.float32)
+    gc = grid.c()
+    rc = lib().gwm_b200_grid_z_center(C.byref(gc), out.ctypes.data_as(C.c_void_p))
+    if rc != OK:
+        raise RuntimeError(f"grid_z_center: status {rc}")
+    return out
 
 
 def scalar_ssprk3(q, u_adv: float = 20.0, v_adv: float = 0.0, dt: float = 10.0, dx: float = 1000.0,

@@ -156,3 +156,38 @@ def test_rayleigh_layer_in_oracle(orc, gwm):
     assert np.abs(damp["w"][top]).mean() < np.abs(free["w"][top]).mean() * 0.95
     low = slice(1, 10)    # below the layer the two runs agree to rounding at one step
     assert np.abs(damp["w"][low] - free["w"][low]).max() < 1e-3 * max(np.abs(free["w"][low]).max(), 1e-3)
+
+
+@pytest.mark.parametrize("kind", ["flat", "cosine_mountain", "agnesi_stretched"])
+def test_grid_z_center_matches_oracle(gwm, orc, kind):
+    # GridMetrics::z_center through the C-ABI (host code, no device): the FP64 heights of
+    # the oracle's metric builder, rounded once to FP32
+    nx, ny, nz = 24, 18, 12
+    kw, okw = {}, {}
+    if kind != "flat":
+        shape = "cosine_mountain" if kind == "cosine_mountain" else "agnesi"
+        t = gwm.build_terrain(shape, nx, ny, 1000.0, 1000.0, height=700.0)
+        kw["terrain"] = okw["terrain"] = t
+    if kind == "agnesi_stretched":
+        eta = (np.linspace(0.0, 1.0, nz + 1) ** 1.4).astype(np.float64)
+        kw["eta_interfaces"] = okw["eta_interfaces"] = eta
+    g = gwm.GridSpec(nx, ny, nz, dx=1000.0, dy=1000.0, z_top=15000.0, **kw)
+    og = orc.GridSpec(nx, ny, nz, dx=1000.0, dy=1000.0, z_top=15000.0, **okw)
+    zc = gwm.grid_z_center(g)
+    ref = orc.metrics(og)["z_centers"]
+    assert zc.shape == ref.shape
+    assert np.array_equal(zc, ref.astype(np.float32))
+
+
+def test_host_entry_points_reject_bad_arguments(gwm):
+    # argument checks come before any device work, so they answer without a GPU
+    L = gwm.lib()
+    assert L.gwm_b200_grid_z_center(None, None) == gwm.ERR_ARG
+    g = gwm.GridSpec(8, 8, 0, dx=1000.0, dy=1000.0, z_top=1000.0)
+    out = np.empty(8, np.float32)
+    assert L.gwm_b200_grid_z_center(ctypes.byref(g.c()), out.ctypes.data_as(ctypes.c_void_p)) == gwm.ERR_ARG
+    assert L.gwm_b200_scalar_ssprk3(None, None, 1, None) == gwm.ERR_ARG
+    assert L.gwm_b200_field_stats_noalloc(None, 10, None, None) == gwm.ERR_ARG
+    buf, res = np.zeros(4, np.float32), np.zeros(3, np.float64)
+    assert L.gwm_b200_field_stats_noalloc(buf.ctypes.data_as(ctypes.c_void_p), 0,
+                                          res.ctypes.data_as(ctypes.c_void_p), None) == gwm.ERR_ARG
