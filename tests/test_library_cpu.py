@@ -191,3 +191,34 @@ def test_host_entry_points_reject_bad_arguments(gwm):
     buf, res = np.zeros(4, np.float32), np.zeros(3, np.float64)
     assert L.gwm_b200_field_stats_noalloc(buf.ctypes.data_as(ctypes.c_void_p), 0,
                                           res.ctypes.data_as(ctypes.c_void_p), None) == gwm.ERR_ARG
+
+
+D, F, LL, ULL = ctypes.c_double, ctypes.c_float, ctypes.c_longlong, ctypes.c_ulonglong
+NULL_CONTEXT_CALLS = [
+    ("gwm_b200_set_concurrent", (1,)), ("gwm_b200_set_stream", (None,)), ("gwm_b200_synchronize", ()),
+    ("gwm_b200_use_graph", (1,)), ("gwm_b200_set_tile", (1, 3)), ("gwm_b200_upload", (0, None)),
+    ("gwm_b200_set_boundary_state", (0, None)), ("gwm_b200_set_damping", (0, D(1000.0), D(0.1), None, None)),
+    ("gwm_b200_apply_reference_boundaries", (0,)),
+    ("gwm_b200_rain_record", (0, None, None, LL(0), ULL(1), F(1.0), F(0.0), None)),
+    ("gwm_b200_set_rain_surrogate", (0, None, None, None, F(0.1), F(0.1))),
+    ("gwm_b200_download", (0, None)), ("gwm_b200_profile", (1,)), ("gwm_b200_step", (1,)),
+    ("gwm_b200_advance_dry", (1,)), ("gwm_b200_advance_tracers", ()), ("gwm_b200_warm_rain", (1,)),
+    ("gwm_b200_fast_modes", ()), ("gwm_b200_slow_tendencies", (0, None)), ("gwm_b200_budgets", (0, None)),
+]
+
+
+@pytest.mark.parametrize("name,args", NULL_CONTEXT_CALLS, ids=[c[0] for c in NULL_CONTEXT_CALLS])
+def test_null_context_is_an_argument_error(gwm, name, args):
+    # every context call answers a NULL context with the invalid-argument status (the
+    # reference's require() failures become status codes; nothing is dereferenced)
+    assert getattr(gwm.lib(), name)(None, *args) == gwm.ERR_ARG
+
+
+def test_null_context_counters_and_destroy(gwm):
+    L = gwm.lib()
+    count = ctypes.c_longlong(7)
+    stats = (ctypes.c_longlong * 6)()
+    assert L.gwm_b200_surrogate_stats(None, 0, stats, 0) == gwm.ERR_ARG
+    assert L.gwm_b200_surrogate_fallbacks(None, 0, ctypes.byref(count), 0) == gwm.ERR_ARG
+    assert count.value == 0
+    L.gwm_b200_destroy(None)  # a no-op
