@@ -72,3 +72,20 @@ def test_single_rank_helpers_without_group():
     import bench
     assert bench.max_over_ranks(7.5, torch, None, "cpu") == 7.5
     assert bench.job_throughput(10, 3, 1, 2.0) == pytest.approx(10 * 3 / 2e-3)
+
+
+def test_bench_reads_the_committed_traffic_summaries():
+    # the roofline object's `traffic` comes from the committed ncu summaries of the
+    # substep kernels (per-cell DRAM bytes scaled to the bench grid); a summary that
+    # lost its machine-readable line would silently turn it into null
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class G:
+        nx, ny, nz = 1024, 1024, 64
+
+    for tile in bench.TRAFFIC_PROFILES:
+        t = bench.read_traffic(G, tile)
+        assert t is not None, bench.TRAFFIC_PROFILES[tile]
+        per_cell = t / (G.nx * G.ny * G.nz)
+        assert 30.0 < per_cell < 60.0, (tile, per_cell)
