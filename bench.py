@@ -36,6 +36,9 @@ ZTOP = 16000.0
 DT = 1.0
 NS = 6
 VT = 12.0
+# the moist sounding of the workload (both arms build it: the library, or the oracle)
+SOUNDING = dict(theta_ref=300.0, theta_lapse_k_per_m=0.004, relative_humidity=0.9, rh_top_m=2000.0,
+                qv_scale_height_m=1500.0, qv_floor=1e-5, noise_rms_k=0.5, noise_depth_m=1000.0)
 
 
 def grid_spec(gwm, nx=NX, ny=NY, nz=NZ):
@@ -43,9 +46,7 @@ def grid_spec(gwm, nx=NX, ny=NY, nz=NZ):
 
 
 def case_params(gwm, seed=1):
-    return gwm.CaseParams(theta_ref=300.0, theta_lapse_k_per_m=0.004, relative_humidity=0.9,
-                          rh_top_m=2000.0, qv_scale_height_m=1500.0, qv_floor=1e-5,
-                          noise_rms_k=0.5, noise_depth_m=1000.0, seed=seed)
+    return gwm.CaseParams(seed=seed, **SOUNDING)
 
 
 def member_spec(gwm):
@@ -125,61 +126,73 @@ def load_peaks():
 SUBSTEP_ALGO_BYTES_PER_CELL = 12 * 4
 
 
-def cpu_baseline(steps_sample=2, nx=128, ny=128):
+# CPU sample per step: the per-cell cost of the CPU restatement does not depend on the
+# horizontal size (0.84e6, 0.86e6 and 0.80e6 cell-updates/s at 64^2, 128^2 and 256^2 x 64 on
+# 8 threads), so a 256 x 256 x 64 periodic subdomain of the workload stands for it
+CPU_SAMPLE = 256
+
+
+def workload_config(nx=NX, ny=NY, world=1):
+    """The workload both arms report (what is timed per step is stated beside it)."""
+    return {"workload": "moist warm-rain step, 1024x1024x64 C3 grid",
+            "nx": nx, "ny": ny, "nz": NZ, "dx_m": DX, "z_top_m": ZTOP,
+            "dt_s": DT, "fast_substeps": NS, "rain_terminal_velocity": VT,
+            "phases": "dry SSPRK3 + 3-tracer SSPRK3 + warm rain/fallout",
+            "l2": "inputs larger than L2 (each field 282 MB)",
+            "parallelism": f"replicas{world}"}
+
+
+def oracle_sample(n, seed=1):
+    """The CPU restatement and a periodic n x n x 64 subdomain of the workload, built by
+    the oracle itself (no product code is loaded)."""
     import oracle
     oracle.build()
     threads = oracle.max_threads()
     oracle.set_threads(threads)
-    gwm = importlib.import_module("gpu-wm-next_b200")
-    g = grid_spec(gwm, nx, ny, NZ)
-    s = gwm.build_case("moist_sounding", g, case_params(gwm), moist=True)
-    og = oracle.GridSpec(nx, ny, NZ, dx=DX, dy=DX, z_top=ZTOP)
-    st = {k: v.astype(np.float64) for k, v in s.items()}
+    og = oracle.GridSpec(n, n, NZ, dx=DX, dy=DX, z_top=ZTOP)
+    st = oracle.moist_sounding(og, seed=seed, **SOUNDING)
+    kw = dict(phases=oracle.PHASE_DRY | oracle.PHASE_TRACERS | oracle.PHASE_RAIN,
+              rain=oracle.RainSpec(dt=DT, terminal_velocity=VT), precision=32)
+    return oracle, og, st, oracle.StepSpec(dt=DT, fast_substeps=NS), kw, threads
+
+
+def cpu_baseline(steps_sample=2, n=128):
+    oracle, og, st, step, kw, threads = oracle_sample(n)
     t0 = time.perf_counter()
-    oracle.run(og, oracle.StepSpec(dt=DT, fast_substeps=NS), st, steps_sample,
-               phases=oracle.PHASE_DRY | oracle.PHASE_TRACERS | oracle.PHASE_RAIN,
-               rain=oracle.RainSpec(dt=DT, terminal_velocity=VT), precision=32)
+    oracle.run(og, step, st, steps_sample, **kw)
     dt = time.perf_counter() - t0
-    cells = nx * ny * NZ * steps_sample
+    cells = n * n * NZ * steps_sample
     return {"value": cells / dt, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-            "sample": f"{nx}x{ny}x{NZ} subdomain of the workload, {steps_sample} full moist steps, "
+            "sample": f"{n}x{n}x{NZ} periodic subdomain of the workload, {steps_sample} full moist steps, "
                       f"FP32 oracle restatement, OpenMP {threads} threads, {dt:.2f} s"}
 
 
 def run_reference(args, rank, world):
-    """CPU restatement of the reference algorithm (the reference has no CPU step)."""
+    """The reference's algorithm on the host cores.  The reference has no CPU step (its
+    kernels are CUDA and its host code moves halos), so this times its CPU restatement,
+    the oracle, with every host thread; each step advances a 256 x 256 x 64 periodic
+    subdomain of the workload (initial state from the oracle's own builder)."""
     if rank != 0:
         return
-    import oracle
-    oracle.build()
-    threads = oracle.max_threads()
-    oracle.set_threads(threads)
-    gwm = importlib.import_module("gpu-wm-next_b200")
-    nx = ny = 128
-    g = grid_spec(gwm, nx, ny, NZ)
-    s = gwm.build_case("moist_sounding", g, case_params(gwm), moist=True)
-    og = oracle.GridSpec(nx, ny, NZ, dx=DX, dy=DX, z_top=ZTOP)
-    st = {k: v.astype(np.float64) for k, v in s.items()}
-    kw = dict(phases=oracle.PHASE_DRY | oracle.PHASE_TRACERS | oracle.PHASE_RAIN,
-              rain=oracle.RainSpec(dt=DT, terminal_velocity=VT), precision=32)
-    step = oracle.StepSpec(dt=DT, fast_substeps=NS)
+    n = CPU_SAMPLE
+    oracle, og, st, step, kw, threads = oracle_sample(n)
     for _ in range(args.warmup):
         st = oracle.run(og, step, st, 1, **kw)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         st = oracle.run(og, step, st, 1, **kw)
     el = time.perf_counter() - t0
-    cells = nx * ny * NZ
+    cells = n * n * NZ
     val = cells * args.steps / el
-    sample = (f"{nx}x{ny}x{NZ} subdomain of the workload per step, FP32 oracle restatement "
-              f"(OpenMP {threads} threads)")
+    sample = (f"{n}x{n}x{NZ} periodic subdomain of the 1024x1024x64 workload per step (the per-cell "
+              f"cost does not depend on the horizontal size), FP32 oracle restatement, OpenMP {threads} threads")
     print(json.dumps({
         "impl": "reference", "metric": "cell-updates/s", "value": val, "unit": "cell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "moist warm-rain step, 1024x1024x64 C3 grid (sampled)",
-                   "nx": nx, "ny": ny, "nz": NZ, "dt": DT, "fast_substeps": NS},
+        "config": workload_config(world=world),
+        "sampled_grid": {"nx": n, "ny": n, "nz": NZ},
         "cpu_baseline": {"value": val, "unit": "cell-updates/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": val, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -304,13 +317,8 @@ def main():
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "sim_s_per_wall_s": DT * args.steps / (ms_max * 1e-3),
-            "config": {"workload": "moist warm-rain step, 1024x1024x64 C3 grid",
-                       "nx": args.nx, "ny": args.ny, "nz": NZ, "dx_m": DX, "z_top_m": ZTOP,
-                       "dt_s": DT, "fast_substeps": NS, "rain_terminal_velocity": VT,
-                       "phases": "dry SSPRK3 + 3-tracer SSPRK3 + warm rain/fallout",
-                       "l2": "inputs larger than L2 (each field 282 MB)",
-                       "graph": not args.no_graph, "tile_rows": tiles, "tile_autotune_ms": tile_ms,
-                       "parallelism": f"replicas{world}"},
+            "config": dict(workload_config(args.nx, args.ny, world), graph=not args.no_graph,
+                           tile_rows=tiles, tile_autotune_ms=tile_ms),
             "gpu_launches": launches,
             "state_finite": finite,
             "roofline": roof,

@@ -62,6 +62,12 @@ class CaseParams(C.Structure):
         "rho_surface", "theta_ref")]
 
 
+class Sounding(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "p_surface", "theta_ref", "theta_lapse_k_per_m", "relative_humidity", "rh_top_m",
+        "qv_scale_height_m", "qv_floor", "noise_rms_k", "noise_depth_m")] + [("seed", C.c_ulonglong)]
+
+
 def build() -> str:
     """Compile the oracle library (gcc, OpenMP) if it is missing or stale."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
@@ -87,6 +93,7 @@ def lib():
         L.gwo_metrics.argtypes = [C.POINTER(Grid), C.c_int, DP, DP, DP, DP]
         L.gwo_case.argtypes = [C.c_int, C.POINTER(Grid), C.POINTER(CaseParams), C.c_int,
                                C.POINTER(Fields)]
+        L.gwo_moist_sounding.argtypes = [C.POINTER(Grid), C.POINTER(Sounding), C.POINTER(Fields)]
         L.gwo_pressure.argtypes = [C.c_long, DP, DP, DP, C.c_int]
         L.gwo_scalar_ssprk3.argtypes = [C.c_int] * 5 + [C.c_double] * 5 + [C.c_int, C.c_int, DP]
         L.gwo_layout.argtypes = [C.c_int] * 8 + [C.POINTER(C.c_int)]
@@ -286,6 +293,22 @@ def case(kind: str, g: GridSpec, params: CaseSpec, precision: int = 32) -> dict:
     gc, pc = g.c(), params.c()
     f = _fields(out)
     _check(lib().gwo_case(CASE_KINDS[kind], C.byref(gc), C.byref(pc), precision, C.byref(f)))
+    return out
+
+
+def moist_sounding(g: GridSpec, p_surface: float = 100000.0, theta_ref: float = 300.0,
+                   theta_lapse_k_per_m: float = 0.004, relative_humidity: float = 0.9, rh_top_m: float = 2000.0,
+                   qv_scale_height_m: float = 1500.0, qv_floor: float = 1e-5, noise_rms_k: float = 0.5,
+                   noise_depth_m: float = 1000.0, seed: int = 1) -> dict:
+    """The moist warm-rain benchmark's initial state (FP32 values as float64 arrays), built
+    by the oracle itself: the seeded sounding balanced column by column, at rest, with no
+    cloud or rain water (flat grid)."""
+    out = zeros(g, moist=True)
+    gc = g.c()
+    sc = Sounding(p_surface, theta_ref, theta_lapse_k_per_m, relative_humidity, rh_top_m, qv_scale_height_m,
+                  qv_floor, noise_rms_k, noise_depth_m, seed)
+    f = _fields(out)
+    _check(lib().gwo_moist_sounding(C.byref(gc), C.byref(sc), C.byref(f)))
     return out
 
 

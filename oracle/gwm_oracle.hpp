@@ -1161,6 +1161,103 @@ template <class T> T hydrostatic_rho_at_height(T rho_s, T theta, T z, T g = T(9.
   return rho_from_pressure_theta(p, theta);
 }
 
+// rho*theta that reproduces pressure p through the dry EOS: prepared_case_init.cpp:39-53
+// (an isentropic first guess refined by two ratio corrections).
+template <class T> T rho_theta_for_pressure(T p) {
+  T rt = (K<T>::p0 / K<T>::Rd) * std::pow(std::max(p / K<T>::p0, T(1.0e-6f)), T(1) - K<T>::kappa);
+  for (int it = 0; it < 2; ++it) {
+    const T pe = pressure_from_rho_theta(T(1), rt);
+    rt *= std::pow(std::max(p / std::max(pe, T(1)), T(1.0e-6f)), T(1) - K<T>::kappa);
+  }
+  return rt;
+}
+
+// ---------------------------------------------------------------------------
+// Synthetic moist sounding of the moist warm-rain benchmark, built independently of the
+// library (input generator of the CPU baseline and of the parity tests).  Arithmetic in
+// float, as the reference's initialisers.  Per column:
+//   theta(z) = theta_ref for z <= 1 km, theta_ref + lapse (z - 1 km) above, plus a
+//     Gaussian deviate of rms noise_rms below noise_depth: Box-Muller of two uniforms
+//     from a splitmix64 counter hash of (seed, 2q) and (seed, 2q + 1), q = (k ny + j) nx + i;
+//   the first level from p_surface over an isentropic layer (Exner drop g z / (cp theta));
+//   the levels above balanced as prepared_case_init.cpp:357-377 (trapezoidal hydrostatic
+//     step, four density refinements, pressure floored at 1 Pa);
+//   rho*theta from the balanced pressure (prepared_case_init.cpp:39-53);
+//   qv = RH qsat(T, p) below rh_top (and at k = 0), above it exponential decay with
+//     scale height qv_scale from the last level below rh_top, floored at qv_floor.
+struct Sounding {
+  float p_surface = 100000.0f, theta_ref = 300.0f, lapse = 0.004f, rh = 0.9f, rh_top = 2000.0f;
+  float qv_scale = 1500.0f, qv_floor = 1.0e-5f, noise_rms = 0.5f, noise_depth = 1000.0f;
+  uint64_t seed = 1;
+};
+
+inline uint64_t mix64(uint64_t x) {  // splitmix64 finaliser
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Outputs (global owned arrays, float): rho, rt, qv as rho*qv; flat terrain only.
+// Compiled without floating-point contraction, so the values do not depend on the
+// target's FMA support.
+#pragma GCC push_options
+#pragma GCC optimize("fp-contract=off")
+inline void moist_sounding(int nx, int ny, int nz, double z_top, const double* eta_interfaces, const Sounding& s,
+                           std::vector<float>& rho, std::vector<float>& rt, std::vector<float>& qv) {
+  using F = float;
+  const size_t n = (size_t)nx * ny * nz;
+  rho.assign(n, 0.0f); rt.assign(n, 0.0f); qv.assign(n, 0.0f);
+  std::vector<F> zc(nz);
+  for (int k = 0; k < nz; ++k) {
+    const double ec = eta_interfaces ? 0.5 * (eta_interfaces[k] + eta_interfaces[k + 1]) : ((double)k + 0.5) / nz;
+    zc[k] = (F)(ec * z_top);
+  }
+  const F g = 9.81f, cp = dry_cp<F>();
+  const uint64_t key = s.seed * 0x100000001B3ull;
+#pragma omp parallel for schedule(static)
+  for (int col = 0; col < nx * ny; ++col) {
+    std::vector<F> th(nz), p(nz), r(nz);
+    for (int k = 0; k < nz; ++k) {
+      const size_t q = (size_t)k * nx * ny + col;
+      F t = zc[k] <= 1000.0f ? s.theta_ref : s.theta_ref + s.lapse * (zc[k] - 1000.0f);
+      if (zc[k] < s.noise_depth && s.noise_rms > 0.0f) {
+        const double u1 = ((double)(mix64(key ^ (2 * q)) >> 11) + 0.5) / 9007199254740992.0;
+        const double u2 = ((double)(mix64(key ^ (2 * q + 1)) >> 11) + 0.5) / 9007199254740992.0;
+        t += (F)(s.noise_rms * (std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * 3.14159265358979323846 * u2)));
+      }
+      th[k] = t;
+    }
+    const F ex0 = std::max(1.0e-4f, std::pow(s.p_surface / K<F>::p0, K<F>::kappa) - g * zc[0] / (cp * th[0]));
+    p[0] = K<F>::p0 * std::pow(ex0, 1.0f / K<F>::kappa);
+    r[0] = rho_from_pressure_theta(p[0], th[0]);
+    for (int k = 1; k < nz; ++k) {
+      const F dz = zc[k] - zc[k - 1];
+      F pk = std::max(1.0f, p[k - 1] - g * r[k - 1] * dz);
+      for (int it = 0; it < 4; ++it)
+        pk = std::max(p[k - 1] - g * 0.5f * (r[k - 1] + rho_from_pressure_theta(pk, th[k])) * dz, 1.0f);
+      p[k] = pk;
+      r[k] = rho_from_pressure_theta(pk, th[k]);
+    }
+    F q_anchor = -1.0f, z_anchor = 0.0f;
+    for (int k = 0; k < nz; ++k) {
+      const size_t q = (size_t)k * nx * ny + col;
+      F v;
+      if (zc[k] < s.rh_top || k == 0) {
+        const F tk = th[k] * std::pow(std::max(p[k] / K<F>::p0, 1.0e-6f), K<F>::kappa);
+        v = s.rh * qsat(tk, p[k]);
+        if (zc[k] < s.rh_top || q_anchor < 0.0f) { q_anchor = v; z_anchor = zc[k]; }
+      } else {
+        v = std::max(s.qv_floor, q_anchor * std::exp(-(zc[k] - z_anchor) / s.qv_scale));
+      }
+      rho[q] = r[k];
+      rt[q] = rho_theta_for_pressure(p[k]);
+      qv[q] = r[k] * std::max(v, 0.0f);
+    }
+  }
+}
+#pragma GCC pop_options
+
 // ---------------------------------------------------------------------------
 // Scalar advection: advance_scalar_ssprk3 (src/dycore/dry_transport.cu:285-325) with
 // upwind_stage_kernel (:13-37) and blend_stage_kernel (:39-46) on the global owned array

@@ -51,6 +51,12 @@ typedef struct {
 } gwo_fields;
 
 typedef struct {
+  double p_surface, theta_ref, theta_lapse_k_per_m, relative_humidity, rh_top_m;
+  double qv_scale_height_m, qv_floor, noise_rms_k, noise_depth_m;
+  unsigned long long seed;
+} gwo_sounding;
+
+typedef struct {
   double rho_background, theta_background, u_background, v_background, w_background;
   double center_x_fraction, center_y_fraction, center_z_fraction;
   double radius_x_fraction, radius_y_fraction, radius_z_fraction, theta_perturbation;
@@ -541,6 +547,27 @@ int gwo_metrics(const gwo_grid* g, int precision, double* zc, double* zi, double
 int gwo_case(int kind, const gwo_grid* g, const gwo_case_params* c, int precision, gwo_fields* io) {
   return guard([&] {
     return precision == 32 ? case_impl<float>(kind, g, c, io) : case_impl<double>(kind, g, c, io);
+  });
+}
+
+// Synthetic moist sounding (gwo::moist_sounding) on a flat grid: rho, rho_theta and qv
+// (as rho*qv) written; momenta, cloud, rain and precipitation left to the caller (zero).
+int gwo_moist_sounding(const gwo_grid* g, const gwo_sounding* c, gwo_fields* io) {
+  return guard([&] {
+    gwo::require(g->nx > 0 && g->ny > 0 && g->nz > 0 && !g->terrain, "flat grid with positive dimensions");
+    gwo::Sounding s;
+    s.p_surface = (float)c->p_surface; s.theta_ref = (float)c->theta_ref; s.lapse = (float)c->theta_lapse_k_per_m;
+    s.rh = (float)c->relative_humidity; s.rh_top = (float)c->rh_top_m; s.qv_scale = (float)c->qv_scale_height_m;
+    s.qv_floor = (float)c->qv_floor; s.noise_rms = (float)c->noise_rms_k; s.noise_depth = (float)c->noise_depth_m;
+    s.seed = c->seed;
+    std::vector<float> rho, rt, qv;
+    gwo::moist_sounding(g->nx, g->ny, g->nz, g->z_top, g->eta_interfaces, s, rho, rt, qv);
+    for (size_t q = 0; q < rho.size(); ++q) {
+      io->rho[q] = rho[q];
+      io->rho_theta[q] = rt[q];
+      if (io->qv) io->qv[q] = qv[q];
+    }
+    return 0;
   });
 }
 

@@ -222,3 +222,17 @@ def test_null_context_counters_and_destroy(gwm):
     assert L.gwm_b200_surrogate_fallbacks(None, 0, ctypes.byref(count), 0) == gwm.ERR_ARG
     assert count.value == 0
     L.gwm_b200_destroy(None)  # a no-op
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed", [(16, 12, 24, 7), (40, 33, 64, 3)])
+def test_moist_sounding_oracle_builder_matches_library(gwm, orc, nx, ny, nz, seed):
+    # the CPU baseline builds the benchmark's initial state with the oracle's own builder;
+    # it must be the state the library builds, bit for bit
+    sounding = dict(theta_ref=300.0, theta_lapse_k_per_m=0.004, relative_humidity=0.9, rh_top_m=2000.0,
+                    qv_scale_height_m=1500.0, qv_floor=1e-5, noise_rms_k=0.5, noise_depth_m=1000.0)
+    g = gwm.GridSpec(nx, ny, nz, dx=3000.0, dy=3000.0, z_top=16000.0)
+    a = gwm.build_case("moist_sounding", g, gwm.CaseParams(seed=seed, **sounding), moist=True)
+    b = orc.moist_sounding(orc.GridSpec(nx, ny, nz, dx=3000.0, dy=3000.0, z_top=16000.0), seed=seed, **sounding)
+    for k in a:
+        assert np.array_equal(a[k].astype(np.float64), b[k]), k
+    assert b["qv"].max() > 0 and np.ptp(b["rho_theta"][0]) > 0  # moist, with noise

@@ -89,3 +89,23 @@ def test_bench_reads_the_committed_traffic_summaries():
         assert t is not None, bench.TRAFFIC_PROFILES[tile]
         per_cell = t / (G.nx * G.ny * G.nz)
         assert 30.0 < per_cell < 60.0, (tile, per_cell)
+
+
+def test_reference_arm_loads_no_product_code():
+    # the reference arm times the oracle alone: neither the product package nor its
+    # CUDA library may be imported or mapped by that process
+    import subprocess
+    code = ("import sys, json; sys.path.insert(0, %r); import bench\n"
+            "bench.CPU_SAMPLE = 16\n"
+            "class A:\n    steps, warmup = 1, 1\n"
+            "bench.run_reference(A(), 0, 1)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print(json.dumps({'pkg': any('gpu-wm-next_b200' in m for m in sys.modules),\n"
+            "                  'so': 'libgwm_b200' in maps, 'torch': 'torch' in sys.modules}))\n" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, check=True)
+    import json
+    lines = [json.loads(x) for x in out.stdout.splitlines() if x.startswith("{")]
+    ref, flags = lines[0], lines[-1]
+    assert ref["impl"] == "reference" and ref["value"] > 0 and ref["sampled_grid"]["nx"] == 16
+    assert ref["config"]["nx"] == 1024 and ref["cpu_baseline"]["kind"] == "port"
+    assert flags == {"pkg": False, "so": False, "torch": False}, flags
