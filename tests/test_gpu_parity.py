@@ -478,9 +478,11 @@ def test_stage_tilings_bit_exact(gwm, kernel, periodic):
 
 @pytest.mark.parametrize("periodic", [True, False])
 def test_tma_substep_bit_exact(gwm, periodic):
-    # the TMA-fed substep runs the owned-tile kernel's arithmetic on the same values:
-    # a full moist step (every substep kind: first, inner, stage end, step end) must
-    # agree bit for bit; 100 x 70 leaves partial tiles on both axes
+    # the TMA-fed kernels run the per-thread-load kernels' arithmetic on the same values.
+    # All three stencil kernels switch together, so the slow stage hands p' to the first
+    # substep of every stage (the benchmark's path): a full moist step with every substep
+    # kind (first with the handoff, inner, stage end, step end) must agree bit for bit;
+    # 100 x 70 leaves partial tiles on both axes
     g = gwm.GridSpec(100, 70, 12, dx=2000.0, dy=2000.0, z_top=12000.0,
                      periodic_x=periodic, periodic_y=periodic)
     p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=9, relative_humidity=1.02)
@@ -488,13 +490,42 @@ def test_tma_substep_bit_exact(gwm, periodic):
     step = gwm.StepConfig(dt=1.0, fast_substeps=4)
     rain = gwm.WarmRainConfig(dt=1.0, rain_terminal_velocity=12.0)
     outs = {}
-    for r in (0, 3):
+    for tiles in ((0, 16, 16), (3, 3, 3), (3, 16, 16)):
         with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=True)) as m:
-            m.set_tile("fast_substep", r)
+            for kernel, r in zip(("fast_substep", "slow_stage", "tracer_stage"), tiles):
+                m.set_tile(kernel, r)
             m.upload(s)
             m.step(3)
-            outs[r] = m.download()
+            outs[tiles] = m.download()
+    ref = outs[(0, 16, 16)]
+    for tiles in ((3, 3, 3), (3, 16, 16)):
+        for k in ref:
+            assert np.array_equal(ref[k], outs[tiles][k]), (tiles, k)
+
+
+@pytest.mark.parametrize("nz", [12, 40])
+def test_tma_kernels_with_open_boundary_state(gwm, nz):
+    # open x with a reference boundary state (strips written at every stage start), deep
+    # and shallow columns: the TMA-fed kernels with the slow-stage p' handoff against the
+    # per-thread-load kernels, bit for bit
+    g = gwm.GridSpec(72, 40, nz, dx=2000.0, dy=2000.0, z_top=500.0 * nz, periodic_x=False, periodic_y=True)
+    p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=6, relative_humidity=1.02)
+    s = gwm.build_case("moist_sounding", g, p, moist=True)
+    s["u"][:] = np.float32(2.0)
+    b = _boundary_of(s, g, factor=1.004)
+    step = gwm.StepConfig(dt=1.0, fast_substeps=4)
+    rain = gwm.WarmRainConfig(dt=1.0, rain_terminal_velocity=12.0)
+    outs = {}
+    for tiles in ((0, 16, 16), (3, 3, 3)):
+        with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=True)) as m:
+            for kernel, r in zip(("fast_substep", "slow_stage", "tracer_stage"), tiles):
+                m.set_tile(kernel, r)
+            m.upload(s)
+            m.set_boundary_state(b)
+            m.step(2)
+            outs[tiles[0]] = m.download()
     for k in outs[0]:
+        assert np.isfinite(outs[3][k]).all(), k
         assert np.array_equal(outs[0][k], outs[3][k]), k
 
 
