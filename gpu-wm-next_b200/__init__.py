@@ -204,6 +204,7 @@ def lib():
     L.gwm_b200_halo_exchange.argtypes = [C.POINTER(_LayoutDesc), C.c_int, C.c_int,
                                          C.POINTER(C.c_void_p), vp]
     L.gwm_b200_dry_pressure.argtypes = [vp, vp, vp, C.c_longlong, vp]
+    L.gwm_b200_test_stall_tile_load.argtypes = [vp, C.c_int, C.c_int]
     L.gwm_b200_field_stats_noalloc.argtypes = [vp, C.c_longlong, vp, vp]
     L.gwm_b200_scalar_ssprk3.argtypes = [C.POINTER(_ScalarDesc), vp, C.c_int, vp]
     L.gwm_b200_grid_z_center.argtypes = [C.POINTER(_Grid), vp]
@@ -228,7 +229,7 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_rain_record",
             "gwm_b200_mlp_train", "gwm_b200_mlp_loss_grad", "gwm_b200_set_rain_surrogate",
             "gwm_b200_surrogate_fallbacks", "gwm_b200_surrogate_stats", "gwm_b200_layout",
-            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_scalar_ssprk3", "gwm_b200_grid_z_center", "gwm_b200_ranks_to_global",
+            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_test_stall_tile_load", "gwm_b200_scalar_ssprk3", "gwm_b200_grid_z_center", "gwm_b200_ranks_to_global",
             "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
 
 
@@ -472,6 +473,12 @@ class Model:
         self._check(lib().gwm_b200_surrogate_stats(self._h, member, st, int(reset)), "surrogate_stats")
         keys = ("fallbacks", "network_cells", "out_of_range", "fraction", "water", "energy")
         return dict(zip(keys, (int(v) for v in st)))
+
+    def test_stall_tile_load(self, plane: int, member: int = 0):
+        """Failure-path testing: the next TMA-fed stencil launch leaves one CTA's tile
+        loads of ``plane`` unissued, so its bounded wait runs out (the step call then
+        fails with GWM_B200_ERR_TIMEOUT)."""
+        self._check(lib().gwm_b200_test_stall_tile_load(self._h, member, plane), "test_stall_tile_load")
 
     def apply_reference_boundaries(self, member: int = 0):
         """apply_reference_boundaries once on the current state."""

@@ -1213,6 +1213,17 @@ int gwm_b200_surrogate_stats(gwm_b200_ctx* c, int member, long long* stats, int 
   return GWM_B200_OK;
 }
 
+int gwm_b200_test_stall_tile_load(gwm_b200_ctx* c, int member, int plane) {
+  const int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  if (plane < 0 || plane > M.g.nz) return fail(c, GWM_B200_ERR_ARG, "plane out of range");
+  const int word = plane + 1;  // err[1]: 0 = no request
+  CK(cudaMemcpyAsync(M.err + 1, &word, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
 int gwm_b200_surrogate_fallbacks(gwm_b200_ctx* c, int member, long long* count, int reset) {
   if (!count) return GWM_B200_ERR_ARG;
   long long st[GWM_B200_SURROGATE_STATS];

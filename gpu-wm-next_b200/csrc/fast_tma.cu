@@ -149,6 +149,10 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
   __syncthreads();
 
   // producer: all tiles of plane kk into slot kk % NSLOT, completing on its barrier
+  // err[1] > 0 (set only by failure-path tests): the first CTA to see it leaves the loads
+  // of plane err[1] - 1 unissued, so that CTA's bounded wait runs out
+  int stall = -1;
+  if (tid == ISSUER && *(volatile int*)(a.err + 1) > 0) stall = atomicExch(a.err + 1, 0) - 1;
   auto issue = [&](int kk) {
     float* st = ring + (kk % NSLOT) * slot;
     uint64_t* bar = &s_bar[kk % NSLOT];
@@ -159,6 +163,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     if (final_step) bytes += 3 * B_OWN;
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(bar, bytes);
+    if (kk == stall) return;  // failure-path testing: this plane's loads stay unissued
     if (FIRST && !PIN) {  // with the halo ring
       tma_load_3d(st + O_RHO, &m.rho, i0 + kXOff - 4, j0, kk, bar);
       tma_load_3d(st + O_TH, &m.th, i0 + kXOff - 4, j0, kk, bar);
@@ -183,8 +188,9 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
     if (!mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1)) {
       s_abort[epoch & 1] = 1;
       atomicExch(a.err, 1);
+    } else {
+      waited = kk;  // a plane whose wait gave up stays in the drain below
     }
-    waited = kk;
   };
   // K10 + K20: pressure perturbation of plane kk at the owned cells and the halo ring
   auto cell_p = [&](const float* st, int r, int c, int kk) {

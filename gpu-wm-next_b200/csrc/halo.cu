@@ -5,6 +5,8 @@
 #include <climits>
 #include <mutex>
 
+#include <cuda.h>
+
 #include "../../include/gwm_b200.h"
 #include "halo.cuh"
 
@@ -427,30 +429,58 @@ cudaError_t launch_reduce_2d(const double* a, const double* b, long long n, doub
 
 // ---------------------------------------------------------------------------
 // Allocation-free entry point (see include/gwm_b200.h).  The device address of
-// g_noalloc_partials is resolved once per device, with that device current, and
-// cached; every later call on the device reuses it.
+// g_noalloc_partials is resolved with the device current and cached together with the
+// context it belongs to.  A module's globals live in one context: if the device's
+// current context is a different one (after cudaDeviceReset, or a context torn down
+// and created again), the address is resolved again before use.
 using namespace gwmb;
 
 namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
-double* g_noalloc_addr[kMaxDevices] = {};
+struct NoAllocSlot {
+  void* ctx = nullptr;   // CUcontext the address was resolved in
+  double* addr = nullptr;
+};
+NoAllocSlot g_noalloc[kMaxDevices];
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {  // driver entry point: no libcuda link needed
+  static CtxGetCurrentFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(p);
+  });
+  return fn;
+}
 }  // namespace
 
 extern "C" int gwm_b200_field_stats_noalloc(const float* x, long long n, double* out, void* stream) {
   if (!x || !out || n <= 0 || n > (long long)INT_MAX) return GWM_B200_ERR_ARG;
+  // an error left pending by other code is the caller's to see: return without clearing it
+  if (cudaPeekAtLastError() != cudaSuccess) return GWM_B200_ERR_CUDA;
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess) return GWM_B200_ERR_CUDA;
   if (dev < 0 || dev >= kMaxDevices) return GWM_B200_ERR_ARG;
   double* part = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    CUcontext ctx = nullptr;
+    const CtxGetCurrentFn get = ctx_get_current();
+    if (get && get(&ctx) != CUDA_SUCCESS) ctx = nullptr;
+    NoAllocSlot& slot = g_noalloc[dev];
+    if (!slot.addr || slot.ctx != (void*)ctx) {
       void* p = nullptr;
       if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return GWM_B200_ERR_CUDA;
-      g_noalloc_addr[dev] = static_cast<double*>(p);
+      if (!ctx && get) get(&ctx);  // the runtime made the primary context current just now
+      slot.addr = static_cast<double*>(p);
+      slot.ctx = (void*)ctx;
     }
-    part = g_noalloc_addr[dev];
+    part = slot.addr;
   }
   cudaStream_t s = (cudaStream_t)stream;
   long long nb = (n + 256LL * 8 - 1) / (256LL * 8);

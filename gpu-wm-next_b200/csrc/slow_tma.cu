@@ -102,6 +102,10 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
   }
   __syncthreads();
 
+  // err[1] > 0 (set only by failure-path tests): the first CTA to see it leaves the loads
+  // of plane err[1] - 1 unissued, so that CTA's bounded wait runs out
+  int stall = -1;
+  if (tid == ISSUER && *(volatile int*)(a.err + 1) > 0) stall = atomicExch(a.err + 1, 0) - 1;
   auto issue = [&](int kk) {  // plane kk in [0, nz] into slot kk % NSLOT
     float* sr = ring + (kk % NSLOT) * slot;
     uint64_t* bar = &s_bar[kk % NSLOT];
@@ -111,6 +115,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     const int x = i0 + kXOff - 4, y = j0;
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(bar, bytes);
+    if (kk == stall) return;  // failure-path testing: this plane's loads stay unissued
     tma_load_3d(sr + R_W, &m.w, x, y, kk, bar);
     if (INC) tma_load_3d(sr + R_DW, &m.dw, x, y, kk, bar);
     if (cells) {
@@ -129,8 +134,9 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     if (!mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1)) {
       s_abort[epoch & 1] = 1;
       atomicExch(a.err, 1);
+    } else {
+      waited = kk;  // a plane whose wait gave up stays in the drain below
     }
-    waited = kk;
   };
   // raw accessors: box index of derived position (r, c) is r * BW + c + 3
   auto U = [&](const float* sr, int b) { return INC ? sr[R_U + b] + sr[R_DU + b] : sr[R_U + b]; };

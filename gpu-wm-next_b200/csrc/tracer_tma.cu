@@ -69,6 +69,10 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
   }
   __syncthreads();
 
+  // err[1] > 0 (set only by failure-path tests): the first CTA to see it leaves the loads
+  // of plane err[1] - 1 unissued, so that CTA's bounded wait runs out
+  int stall = -1;
+  if (tid == ISSUER && *(volatile int*)(a.err + 1) > 0) stall = atomicExch(a.err + 1, 0) - 1;
   auto issue = [&](int kk) {  // plane kk in [0, nz]; plane nz holds the top faces only
     float* st = ring + (kk % NSLOT) * SLOT;
     uint64_t* bar = &s_bar[kk % NSLOT];
@@ -77,6 +81,7 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
     if (cells) bytes += (1 + a.ntracers) * B_CELL + 2 * B_FACE;
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(bar, bytes);
+    if (kk == stall) return;  // failure-path testing: this plane's loads stay unissued
     tma_load_3d(st + O_W, &m.w, i0 + kXOff, j0 + 1, kk, bar);
     if (cells) {
       tma_load_3d(st + O_RHO, &m.rho, i0 + kXOff - 4, j0, kk, bar);
@@ -90,8 +95,9 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
     if (!mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1)) {
       s_abort[epoch & 1] = 1;
       atomicExch(a.err, 1);
+    } else {
+      waited = kk;  // a plane whose wait gave up stays in the drain below
     }
-    waited = kk;
   };
   // mixing ratios of plane kk (dry_transport.cu:91-94) at the owned cells and the ring
   auto mix = [&](int kk) {

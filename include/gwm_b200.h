@@ -217,6 +217,12 @@ int gwm_b200_surrogate_fallbacks(gwm_b200_ctx* ctx, int member, long long* count
 /* Loss and gradient of the network on n host samples (gradient check). */
 int gwm_b200_mlp_loss_grad(const float* params, const float* norm, const float* x, const float* y, int n,
                            float* grad, double* loss);
+/* Failure-path testing (no counterpart in the reference): the next TMA-fed stencil
+ * launch of the member (slow stage, acoustic substep or tracer stage on flat terrain)
+ * leaves the tile loads of `plane` unissued in one CTA, so that CTA's bounded wait runs
+ * out; the step call then returns GWM_B200_ERR_TIMEOUT and the context stays usable.
+ * The request is kept until a TMA-fed kernel takes it. */
+int gwm_b200_test_stall_tile_load(gwm_b200_ctx* ctx, int member, int plane);
 /* FP64 budgets of the current state. */
 int gwm_b200_budgets(gwm_b200_ctx* ctx, int member, gwm_b200_budget* out);
 /* Tile shape of a kernel.  kernel 0 = slow stage: rows 3 = owned 32x16 tiles fed by
@@ -270,7 +276,10 @@ int gwm_b200_dry_pressure(const float* rho_d, const float* rho_theta_m, float* p
  * and callers without a gwm_b200_ctx.  The scratch is a fixed 24 KiB array inside the
  * library (1024 blocks of partials), held on every device that loads the library until
  * process exit; n must lie in [1, 2^31-1].  The first call on a device resolves that
- * array's device address, so make it before any stream capture on that device.  All
+ * array's device address, so make it before any stream capture on that device; after
+ * the device's context is re-created (cudaDeviceReset), the next call resolves it
+ * again, and the same applies to that call.  A CUDA error already pending from other
+ * code is left in place and the call returns GWM_B200_ERR_CUDA without launching.  All
  * calls share the array: calls that can overlap on the GPU (different streams, or
  * threads without ordering) race and must be serialised by the caller. */
 int gwm_b200_field_stats_noalloc(const float* x, long long n, double* out, void* stream);

@@ -39,3 +39,29 @@ def test_field_stats_noalloc_matches_budgets(gwm):
         assert got_min == mn and got_max == mx
     with pytest.raises(RuntimeError):
         gwm.field_stats_noalloc(x.data_ptr(), 0, out.data_ptr())
+
+
+def test_field_stats_noalloc_large_input_allocates_nothing(gwm):
+    # 3,000,000 values: more than the 1024 blocks x 2048 values one pass covers, so each
+    # thread of the first pass strides over several chunks (the capped branch).  Device
+    # free memory is the same before and after the calls that follow the first one.
+    import torch
+    rng = np.random.default_rng(12)
+    n = 3_000_000
+    host = rng.normal(5.0, 3.0, n).astype(np.float32)
+    host[1234567] = np.float32(-40.0)
+    host[2999999] = np.float32(77.0)
+    x = torch.tensor(host, device="cuda")
+    out = torch.zeros(3, dtype=torch.float64, device="cuda")
+    gwm.field_stats_noalloc(x.data_ptr(), n, out.data_ptr())   # first call on the device
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        out.fill_(np.nan)
+        gwm.field_stats_noalloc(x.data_ptr(), n, out.data_ptr())
+        torch.cuda.synchronize()
+        s, mn, mx = out.cpu().tolist()
+        exact = host.astype(np.float64)
+        assert s == pytest.approx(exact.sum(), rel=1e-12)
+        assert mn == -40.0 and mx == 77.0
+    assert torch.cuda.mem_get_info()[0] == free0
