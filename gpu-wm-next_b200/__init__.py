@@ -205,6 +205,14 @@ def lib():
                                          C.POINTER(C.c_void_p), vp]
     L.gwm_b200_dry_pressure.argtypes = [vp, vp, vp, C.c_longlong, vp]
     L.gwm_b200_test_stall_tile_load.argtypes = [vp, C.c_int, C.c_int]
+    L.gwm_b200_tracer_add.argtypes = [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
+    L.gwm_b200_tracer_find.argtypes = [vp, C.c_int, C.c_char_p]
+    L.gwm_b200_tracer_count.argtypes = [vp, C.c_int]
+    L.gwm_b200_tracer_name.argtypes = [vp, C.c_int, C.c_int]
+    L.gwm_b200_tracer_name.restype = C.c_char_p
+    L.gwm_b200_tracer_upload.argtypes = [vp, C.c_int, C.c_int, vp]
+    L.gwm_b200_tracer_download.argtypes = [vp, C.c_int, C.c_int, vp]
+    L.gwm_b200_tracer_total.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.gwm_b200_field_stats_noalloc.argtypes = [vp, C.c_longlong, vp, vp]
     L.gwm_b200_scalar_ssprk3.argtypes = [C.POINTER(_ScalarDesc), vp, C.c_int, vp]
     L.gwm_b200_grid_z_center.argtypes = [C.POINTER(_Grid), vp]
@@ -229,7 +237,9 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_rain_record",
             "gwm_b200_mlp_train", "gwm_b200_mlp_loss_grad", "gwm_b200_set_rain_surrogate",
             "gwm_b200_surrogate_fallbacks", "gwm_b200_surrogate_stats", "gwm_b200_layout",
-            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_test_stall_tile_load", "gwm_b200_scalar_ssprk3", "gwm_b200_grid_z_center", "gwm_b200_ranks_to_global",
+            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_test_stall_tile_load", "gwm_b200_tracer_add",
+            "gwm_b200_tracer_find", "gwm_b200_tracer_count", "gwm_b200_tracer_name", "gwm_b200_tracer_upload",
+            "gwm_b200_tracer_download", "gwm_b200_tracer_total", "gwm_b200_scalar_ssprk3", "gwm_b200_grid_z_center", "gwm_b200_ranks_to_global",
             "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
 
 
@@ -473,6 +483,55 @@ class Model:
         self._check(lib().gwm_b200_surrogate_stats(self._h, member, st, int(reset)), "surrogate_stats")
         keys = ("fallbacks", "network_cells", "out_of_range", "fraction", "water", "energy")
         return dict(zip(keys, (int(v) for v in st)))
+
+    # -- tracer registry (TracerRegistry / TracerState)
+    def add_tracer(self, name: str, units: str = "kg/kg", positive: bool = True, member: int = 0) -> int:
+        """TracerRegistry::add: registers a passive tracer (mass rho*q, starting at zero)
+        that every step transports; returns its index."""
+        rc = lib().gwm_b200_tracer_add(self._h, member, name.encode(), units.encode(), int(positive))
+        if rc < 0:
+            self._check(rc, "add_tracer")
+        return rc
+
+    def find_tracer(self, name: str, member: int = 0) -> Optional[int]:
+        """TracerRegistry::find: the tracer's index, or None."""
+        rc = lib().gwm_b200_tracer_find(self._h, member, name.encode())
+        return rc if rc >= 0 else None
+
+    def tracer_names(self, member: int = 0) -> list:
+        n = lib().gwm_b200_tracer_count(self._h, member)
+        return [lib().gwm_b200_tracer_name(self._h, member, i).decode() for i in range(max(n, 0))]
+
+    def _tracer_index(self, tracer, member):
+        if isinstance(tracer, str):
+            i = self.find_tracer(tracer, member)
+            if i is None:
+                raise KeyError(f"Tracer not found in TracerState: {tracer}")
+            return i
+        return int(tracer)
+
+    def upload_tracer(self, tracer, mass: np.ndarray, member: int = 0):
+        """TracerState::mass(tracer) from a host array (nz, ny, nx) of rho*q."""
+        g = self.grids[member]
+        a = np.ascontiguousarray(mass, dtype=np.float32)
+        if a.shape != (g.nz, g.ny, g.nx):
+            raise ValueError(f"tracer field shape {a.shape}, expected {(g.nz, g.ny, g.nx)}")
+        self._check(lib().gwm_b200_tracer_upload(self._h, member, self._tracer_index(tracer, member),
+                                                 a.ctypes.data), "upload_tracer")
+
+    def download_tracer(self, tracer, member: int = 0) -> np.ndarray:
+        g = self.grids[member]
+        out = np.empty((g.nz, g.ny, g.nx), dtype=np.float32)
+        self._check(lib().gwm_b200_tracer_download(self._h, member, self._tracer_index(tracer, member),
+                                                   out.ctypes.data), "download_tracer")
+        return out
+
+    def tracer_total(self, tracer, member: int = 0) -> float:
+        """TracerState::total_mass: FP64 sum of rho*q over the owned cells."""
+        t = C.c_double()
+        self._check(lib().gwm_b200_tracer_total(self._h, member, self._tracer_index(tracer, member),
+                                                C.byref(t)), "tracer_total")
+        return t.value
 
     def test_stall_tile_load(self, plane: int, member: int = 0):
         """Failure-path testing: the next TMA-fed stencil launch leaves one CTA's tile

@@ -58,6 +58,18 @@ struct Member {
   float* T0[3]{};
   float* T1[3]{};
   float* T2[3]{};
+  // TracerRegistry + TracerState (include/gwm/state/tracer_registry.hpp:23-49,
+  // tracer_state.hpp:12-119): the tracers in registry order, each with its mass field
+  // rho*q and the two SSPRK3 stage buffers.  A moist member registers the warm-rain triple
+  // first (T0/T1/T2: specific humidity, cloud water, rain water); tracers added later get
+  // their own device block (extra).
+  struct Tracer {
+    std::string name, units;
+    bool positive = true;
+    float* f[3]{};
+  };
+  std::vector<Tracer> reg;
+  std::vector<char*> extra;
   float *zc = nullptr, *idc = nullptr, *idf = nullptr;
   double *precip = nullptr, *pcomp = nullptr;
   unsigned long long* acc = nullptr;
@@ -321,6 +333,16 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
     for (auto& q : M.T0) q = (float*)take(fbytes);
     for (auto& q : M.T1) q = (float*)take(fbytes);
     for (auto& q : M.T2) q = (float*)take(fbytes);
+    // make_warm_rain_registry (tracer_registry.hpp:56-62)
+    const char* names[3] = {"specific_humidity", "cloud_water_mixing_ratio", "rain_water_mixing_ratio"};
+    M.reg.clear();
+    for (int t = 0; t < 3; ++t) {
+      Member::Tracer tr;
+      tr.name = names[t];
+      tr.units = "kg/kg";
+      tr.f[0] = M.T0[t]; tr.f[1] = M.T1[t]; tr.f[2] = M.T2[t];
+      M.reg.push_back(tr);
+    }
   }
   M.precip = (double*)take(plane2 * sizeof(double));
   M.pcomp = (double*)take(plane2 * sizeof(double));
@@ -655,38 +677,46 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
   return GWM_B200_OK;
 }
 
-// advance_passive_tracers_ssprk3 (dry_transport.cu:440-518), three tracers per pass.
+// advance_passive_tracers_ssprk3 (dry_transport.cu:440-518) over every registered tracer,
+// three tracers per kernel pass.  Each tracer is advanced on its own (the reference loops
+// over tracers), so grouping does not change any result.  The reference boundary state
+// covers the warm-rain triple; tracers added later take the Null tracer updater.
 int enqueue_tracers(gwm_b200_ctx* c, Member& M) {
-  float* const* ins[3] = {M.T0, M.T1, M.T2};
-  float* const* outs[3] = {M.T1, M.T2, M.T0};
   const float wa[3] = {0.0f, 0.75f, 1.0f / 3.0f}, wb[3] = {1.0f, 0.25f, 2.0f / 3.0f};
-  for (int s = 0; s < 3; ++s) {
-    TracerArgs a{};
-    a.g = M.g;
-    a.rho = M.Q[0]; a.u = M.Q[2]; a.v = M.Q[3]; a.w = M.Q[4];
-    for (int t = 0; t < 3; ++t) {
-      a.q_in[t] = ins[s][t];
-      a.q0[t] = s == 0 ? nullptr : M.T0[t];
-      a.q_out[t] = outs[s][t];
-    }
-    a.wa = wa[s]; a.wb = wb[s]; a.dt = M.md.step.dt;
-    a.ntracers = 3;
-    a.idz_c = M.idc; a.terrain = M.terrain_active;
-    a.err = M.err;
-    if (M.has_tracer_boundary) {  // TracerBoundaryUpdater::apply on the stage input
-      if (s == 0) {
-        StripJobs J{};
-        for (int t = 0; t < 3; ++t) J.j[J.n++] = strip_job(M.T0[t], M.bsave + M.boff[5 + t], nullptr, kCell, 1);
-        LAUNCH(launch_strips(M.g, J, c->stream), "boundary strips");
+  const int nt = (int)M.reg.size();
+  for (int g0 = 0; g0 < nt; g0 += 3) {
+    const int ng = std::min(3, nt - g0);
+    const bool bnd = M.has_tracer_boundary && M.md.moist && g0 == 0;
+    for (int s = 0; s < 3; ++s) {
+      TracerArgs a{};
+      a.g = M.g;
+      a.rho = M.Q[0]; a.u = M.Q[2]; a.v = M.Q[3]; a.w = M.Q[4];
+      for (int t = 0; t < ng; ++t) {
+        const Member::Tracer& T = M.reg[g0 + t];
+        a.q_in[t] = T.f[s];
+        a.q0[t] = s == 0 ? nullptr : T.f[0];
+        a.q_out[t] = T.f[(s + 1) % 3];
       }
-      StripJobs A{};
-      for (int t = 0; t < 3; ++t) A.j[A.n++] = strip_job(ins[s][t], M.bstrip + M.boff[5 + t], nullptr, kCell, 0);
-      LAUNCH(launch_strips(M.g, A, c->stream), "boundary strips");
-    }
-    LAUNCH(launch_tracers(c, M, a), "tracer stage");
-    if (M.has_tracer_boundary && s == 0) {
-      const int rc = restore_stage1_strips(c, M, 5, 3, M.T0);
-      if (rc) return rc;
+      a.wa = wa[s]; a.wb = wb[s]; a.dt = M.md.step.dt;
+      a.ntracers = ng;
+      a.idz_c = M.idc; a.terrain = M.terrain_active;
+      a.err = M.err;
+      if (bnd) {  // TracerBoundaryUpdater::apply on the stage input
+        if (s == 0) {
+          StripJobs J{};
+          for (int t = 0; t < 3; ++t) J.j[J.n++] = strip_job(M.T0[t], M.bsave + M.boff[5 + t], nullptr, kCell, 1);
+          LAUNCH(launch_strips(M.g, J, c->stream), "boundary strips");
+        }
+        StripJobs A{};
+        for (int t = 0; t < 3; ++t)
+          A.j[A.n++] = strip_job(const_cast<float*>(a.q_in[t]), M.bstrip + M.boff[5 + t], nullptr, kCell, 0);
+        LAUNCH(launch_strips(M.g, A, c->stream), "boundary strips");
+      }
+      LAUNCH(launch_tracers(c, M, a), "tracer stage");
+      if (bnd && s == 0) {
+        const int rc = restore_stage1_strips(c, M, 5, 3, M.T0);
+        if (rc) return rc;
+      }
     }
   }
   return GWM_B200_OK;
@@ -732,7 +762,7 @@ int enqueue_rain(gwm_b200_ctx* c, Member& M, int fallout) {
 int enqueue_full_step(gwm_b200_ctx* c, Member& M) {
   int rc = enqueue_dry(c, M);
   if (rc) return rc;
-  if (M.md.moist && M.md.enable_tracer_transport) {
+  if (M.md.enable_tracer_transport && !M.reg.empty()) {
     rc = enqueue_tracers(c, M);
     if (rc) return rc;
   }
@@ -821,6 +851,7 @@ void gwm_b200_destroy(gwm_b200_ctx* c) {
     if (M.block) cudaFree(M.block);
     if (M.bstrip) cudaFree(M.bstrip);
     if (M.sur) cudaFree(M.sur);
+    for (char* b : M.extra) cudaFree(b);
   }
   for (auto st : c->mstreams) cudaStreamDestroy(st);
   for (auto ev : c->mjoin) cudaEventDestroy(ev);
@@ -1232,6 +1263,102 @@ int gwm_b200_surrogate_fallbacks(gwm_b200_ctx* c, int member, long long* count, 
   return rc;
 }
 
+// ---- tracer registry ----------------------------------------------------------
+int gwm_b200_tracer_add(gwm_b200_ctx* c, int member, const char* name, const char* units, int positive) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  if (!name || !*name) return fail(c, GWM_B200_ERR_ARG, "tracer name must not be empty");
+  Member& M = c->m[member];
+  for (const auto& t : M.reg)
+    if (t.name == name) return fail(c, GWM_B200_ERR_ARG, "Tracer already exists in registry");
+  const size_t fbytes = ((M.field_elems * sizeof(float) + 255) / 256) * 256;
+  char* blk = nullptr;
+  CK(cudaMalloc(&blk, 3 * fbytes));
+  M.extra.push_back(blk);
+  CK(cudaMemsetAsync(blk, 0, 3 * fbytes, c->stream));
+  Member::Tracer tr;
+  tr.name = name;
+  tr.units = units ? units : "";
+  tr.positive = positive != 0;
+  for (int q = 0; q < 3; ++q) tr.f[q] = (float*)(blk + q * fbytes);
+  if (!M.terrain_active && !M.tmaps.empty()) {  // TMA maps of the tracer stage (cells with the ring)
+    for (int q = 0; q < 3; ++q) {
+      CUtensorMap m;
+      if (!encode_field_map(&m, tr.f[q], M.g, kTmaCellBox[0], kTmaCellBox[1]))
+        return fail(c, GWM_B200_ERR_CUDA, "tensor map of an added tracer");
+      M.tmaps.emplace_back(tr.f[q], 0, m);
+    }
+  }
+  M.reg.push_back(tr);
+  drop_graph(c);  // the step now launches more tracer passes
+  CK(cudaStreamSynchronize(c->stream));
+  return (int)M.reg.size() - 1;
+}
+
+int gwm_b200_tracer_find(const gwm_b200_ctx* c, int member, const char* name) {
+  if (!c || member < 0 || member >= (int)c->m.size() || !name) return GWM_B200_ERR_ARG;
+  const auto& reg = c->m[member].reg;
+  for (size_t t = 0; t < reg.size(); ++t)
+    if (reg[t].name == name) return (int)t;
+  return GWM_B200_ERR_ARG;
+}
+
+int gwm_b200_tracer_count(const gwm_b200_ctx* c, int member) {
+  if (!c || member < 0 || member >= (int)c->m.size()) return GWM_B200_ERR_ARG;
+  return (int)c->m[member].reg.size();
+}
+
+const char* gwm_b200_tracer_name(const gwm_b200_ctx* c, int member, int index) {
+  if (!c || member < 0 || member >= (int)c->m.size()) return nullptr;
+  const auto& reg = c->m[member].reg;
+  if (index < 0 || index >= (int)reg.size()) return nullptr;
+  return reg[index].name.c_str();
+}
+
+static int tracer_index(gwm_b200_ctx* c, int member, int index) {
+  const int rc = check_member(c, member);
+  if (rc) return rc;
+  if (index < 0 || index >= (int)c->m[member].reg.size()) return fail(c, GWM_B200_ERR_ARG, "tracer index out of range");
+  return GWM_B200_OK;
+}
+
+int gwm_b200_tracer_upload(gwm_b200_ctx* c, int member, int index, const float* host) {
+  int rc = tracer_index(c, member, index);
+  if (rc) return rc;
+  if (!host) return fail(c, GWM_B200_ERR_ARG, "null tracer field");
+  Member& M = c->m[member];
+  const size_t n = (size_t)M.g.nx * M.g.ny * M.g.nz;
+  CK(cudaMemcpyAsync(M.staging, host, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_pack(M.g, kCell, M.staging, M.reg[index].f[0], c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+int gwm_b200_tracer_download(gwm_b200_ctx* c, int member, int index, float* host) {
+  int rc = tracer_index(c, member, index);
+  if (rc) return rc;
+  if (!host) return fail(c, GWM_B200_ERR_ARG, "null tracer field");
+  Member& M = c->m[member];
+  const size_t n = (size_t)M.g.nx * M.g.ny * M.g.nz;
+  CK(launch_unpack(M.g, kCell, M.reg[index].f[0], M.staging, c->stream));
+  CK(cudaMemcpyAsync(host, M.staging, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+int gwm_b200_tracer_total(gwm_b200_ctx* c, int member, int index, double* total) {
+  int rc = tracer_index(c, member, index);
+  if (rc) return rc;
+  if (!total) return fail(c, GWM_B200_ERR_ARG, "null output");
+  Member& M = c->m[member];
+  CK(launch_reduce(M.g, kCell, 0, M.reg[index].f[0], nullptr, nullptr, 0, M.red_part, M.red_out + 20, c->stream));
+  ReduceOut r;
+  CK(cudaMemcpyAsync(&r, M.red_out + 20, sizeof(ReduceOut), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *total = r.sum;
+  return GWM_B200_OK;
+}
+
 int gwm_b200_download(gwm_b200_ctx* c, int member, gwm_b200_fields* h) {
   int rc = check_member(c, member);
   if (rc) return rc;
@@ -1394,7 +1521,7 @@ int gwm_b200_advance_tracers(gwm_b200_ctx* c) {
   if (!c) return GWM_B200_ERR_ARG;
   c->cur_launches = 0;
   for (auto& M : c->m) {
-    if (!M.md.moist) continue;
+    if (M.reg.empty()) continue;
     int rc = enqueue_tracers(c, M);
     if (rc) return rc;
   }

@@ -168,6 +168,29 @@ int gwm_b200_set_damping(gwm_b200_ctx* ctx, int member, double z_bottom, double 
                          const double* u_ref, const double* v_ref);
 /* apply_reference_boundaries once on the current state (dry fields and, when set, tracers). */
 int gwm_b200_apply_reference_boundaries(gwm_b200_ctx* ctx, int member);
+/* ---- tracer registry ----------------------------------------------------------
+ * TracerRegistry / TracerState of a member (include/gwm/state/tracer_registry.hpp:23-49,
+ * tracer_state.hpp:12-119).  A moist member starts with make_warm_rain_registry
+ * (tracer_registry.hpp:56-62): specific_humidity, cloud_water_mixing_ratio and
+ * rain_water_mixing_ratio at indices 0-2 (the qv, qc, qr of gwm_b200_fields); a dry member
+ * starts empty.  Every registered tracer's mass rho*q is carried by
+ * advance_passive_tracers_ssprk3 in each step (dry_transport.cu:440-518); warm rain acts
+ * on indices 0-2 only, and the reference boundary state (gwm_b200_set_boundary_state)
+ * covers those three.
+ * TracerRegistry::add: a new name (duplicates are rejected, as the reference requires);
+ * returns the tracer's index (>= 0) or a negative status.  Its mass starts at zero. */
+int gwm_b200_tracer_add(gwm_b200_ctx* ctx, int member, const char* name, const char* units, int positive);
+/* TracerRegistry::find: the index of name, or GWM_B200_ERR_ARG when it is not registered. */
+int gwm_b200_tracer_find(const gwm_b200_ctx* ctx, int member, const char* name);
+/* TracerRegistry::size (or a negative status). */
+int gwm_b200_tracer_count(const gwm_b200_ctx* ctx, int member);
+/* TracerRegistry::at(index).name, or NULL for an index out of range. */
+const char* gwm_b200_tracer_name(const gwm_b200_ctx* ctx, int member, int index);
+/* TracerState::mass(index) in and out: host array (nz, ny, nx) of rho*q, float32. */
+int gwm_b200_tracer_upload(gwm_b200_ctx* ctx, int member, int index, const float* host);
+int gwm_b200_tracer_download(gwm_b200_ctx* ctx, int member, int index, float* host);
+/* TracerState::total_mass: FP64 sum of rho*q over the owned cells (Field3D::owned_sum). */
+int gwm_b200_tracer_total(gwm_b200_ctx* ctx, int member, int index, double* total);
 /* ---- learned warm-rain microphysics (training side) ----
  * Cell samples of the plain scheme at the member's current state (no state change):
  * x (capacity x 7, device) = (T, p, rho_d, qv, qc, qr, dt), y (capacity x 5, device) =
