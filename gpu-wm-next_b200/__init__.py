@@ -205,6 +205,9 @@ def lib():
                                          C.POINTER(C.c_void_p), vp]
     L.gwm_b200_dry_pressure.argtypes = [vp, vp, vp, C.c_longlong, vp]
     L.gwm_b200_test_stall_tile_load.argtypes = [vp, C.c_int, C.c_int]
+    L.gwm_b200_set_boundary_cache.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(_Fields)]
+    L.gwm_b200_set_step_start_time.argtypes = [vp, C.c_int, C.c_float]
+    L.gwm_b200_get_step_start_time.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
     L.gwm_b200_tracer_add.argtypes = [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
     L.gwm_b200_tracer_find.argtypes = [vp, C.c_int, C.c_char_p]
     L.gwm_b200_tracer_count.argtypes = [vp, C.c_int]
@@ -237,7 +240,8 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_rain_record",
             "gwm_b200_mlp_train", "gwm_b200_mlp_loss_grad", "gwm_b200_set_rain_surrogate",
             "gwm_b200_surrogate_fallbacks", "gwm_b200_surrogate_stats", "gwm_b200_layout",
-            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_test_stall_tile_load", "gwm_b200_tracer_add",
+            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_test_stall_tile_load", "gwm_b200_set_boundary_cache",
+            "gwm_b200_set_step_start_time", "gwm_b200_get_step_start_time", "gwm_b200_tracer_add",
             "gwm_b200_tracer_find", "gwm_b200_tracer_count", "gwm_b200_tracer_name", "gwm_b200_tracer_upload",
             "gwm_b200_tracer_download", "gwm_b200_tracer_total", "gwm_b200_scalar_ssprk3", "gwm_b200_grid_z_center", "gwm_b200_ranks_to_global",
             "gwm_b200_global_to_ranks", "gwm_b200_build_case", "gwm_b200_build_terrain")
@@ -423,6 +427,40 @@ class Model:
                 keep.append(a)
                 setattr(f, cname, _fptr(a))
         self._check(lib().gwm_b200_set_boundary_state(self._h, member, C.byref(f)), "set_boundary_state")
+
+    def set_boundary_cache(self, offsets, snapshots, member: int = 0):
+        """The prepared-case boundary updater: ``snapshots`` are balanced states (dicts of the
+        state keys; tracers qv, qc, qr as mixing ratios, kg/kg) at forecast ``offsets``
+        (seconds, strictly increasing).  Each updater call applies the strips interpolated at
+        the forecast second of the call; the step start time advances by dt per step.  An
+        empty list removes the cache."""
+        n = len(snapshots)
+        if n != len(offsets):
+            raise ValueError("one offset per snapshot")
+        if n == 0:
+            self._check(lib().gwm_b200_set_boundary_cache(self._h, member, 0, None, None), "set_boundary_cache")
+            return
+        sh = self.grids[member].shapes()
+        arr = (_Fields * n)()
+        keep = []
+        for q, snap in enumerate(snapshots):
+            for k, cname in _C_NAMES.items():
+                if snap.get(k) is not None:
+                    a = np.ascontiguousarray(snap[k], dtype=np.float32)
+                    if a.shape != sh[k]:
+                        raise ValueError(f"{k}: shape {a.shape} != {sh[k]}")
+                    keep.append(a)
+                    setattr(arr[q], cname, _fptr(a))
+        off = (C.c_int * n)(*[int(t) for t in offsets])
+        self._check(lib().gwm_b200_set_boundary_cache(self._h, member, n, off, arr), "set_boundary_cache")
+
+    def set_step_start_time(self, t: float, member: int = 0):
+        self._check(lib().gwm_b200_set_step_start_time(self._h, member, float(t)), "set_step_start_time")
+
+    def step_start_time(self, member: int = 0) -> float:
+        t = C.c_float()
+        self._check(lib().gwm_b200_get_step_start_time(self._h, member, C.byref(t)), "step_start_time")
+        return t.value
 
     def set_damping(self, z_bottom: float, rate: float, u_ref=None, v_ref=None, member: int = 0):
         """Rayleigh damping layer above ``z_bottom`` (extension); rate <= 0 removes it."""

@@ -88,6 +88,13 @@ struct Member {
   float* bsave = nullptr;
   long long boff[9]{};
   bool has_boundary = false, has_tracer_boundary = false;
+  // prepared-case boundary cache: n snapshots of strips laid out like bstrip (tracer strips
+  // hold mixing ratios), their forecast offsets (s) and the device clock
+  char* bcache_block = nullptr;
+  float* bcache = nullptr;
+  int* bcache_off = nullptr;
+  BoundaryClock* bclock = nullptr;
+  int bcache_n = 0;
   // Rayleigh damping layer (extension): [tau_c(nz) | tau_f(nz+1) | u_ref(nz) | v_ref(nz)]
   float* damp = nullptr;
   bool damping = false;
@@ -583,6 +590,16 @@ int restore_stage1_strips(gwm_b200_ctx* c, Member& M, int first, int count, floa
   return GWM_B200_OK;
 }
 
+// Strips of the boundary cache interpolated at RK stage s of the current step (the
+// clock kernel of the step filled the stage's bracket and weight).
+int enqueue_boundary_interp(gwm_b200_ctx* c, Member& M, int s) {
+  const int ntr = M.has_tracer_boundary ? 3 : 0;
+  LAUNCH(launch_boundary_interp(M.bcache, M.boff[8], M.boff[5], M.boff[1] - M.boff[0], ntr, M.bclock, s, M.bstrip,
+                                c->stream),
+         "boundary interpolation");
+  return GWM_B200_OK;
+}
+
 // One advance_dry_state_ssprk3 (dry_core.cu:541-651).
 int enqueue_dry(gwm_b200_ctx* c, Member& M) {
   const gwm_b200_step_config& sc = M.md.step;
@@ -633,6 +650,11 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
       a.uref = M.damp + 2 * (kMaxNz + 1); a.vref = M.damp + 3 * (kMaxNz + 1);
     }
     if (M.has_boundary) {
+      if (M.bcache_n > 0) {  // PreparedCaseBoundaryUpdater::apply at sim_time 0, dt, dt/2
+        if (s == 0) LAUNCH(launch_boundary_clock(M.bclock, M.bcache_off, M.bcache_n, c->stream), "boundary clock");
+        const int rc = enqueue_boundary_interp(c, M, s);
+        if (rc) return rc;
+      }
       float* base[3] = {const_cast<float*>(a.u), const_cast<float*>(a.v), const_cast<float*>(a.w)};
       float* inc[3] = {const_cast<float*>(a.du), const_cast<float*>(a.dv), const_cast<float*>(a.dw)};
       const int rc = enqueue_dry_boundary(c, M, s, a.rho, a.th, base, a.du ? inc : nullptr);
@@ -702,6 +724,10 @@ int enqueue_tracers(gwm_b200_ctx* c, Member& M) {
       a.idz_c = M.idc; a.terrain = M.terrain_active;
       a.err = M.err;
       if (bnd) {  // TracerBoundaryUpdater::apply on the stage input
+        if (M.bcache_n > 0) {  // PreparedCaseTracerBoundaryUpdater at sim_time 0, dt, dt/2
+          const int rc = enqueue_boundary_interp(c, M, s);
+          if (rc) return rc;
+        }
         if (s == 0) {
           StripJobs J{};
           for (int t = 0; t < 3; ++t) J.j[J.n++] = strip_job(M.T0[t], M.bsave + M.boff[5 + t], nullptr, kCell, 1);
@@ -852,6 +878,7 @@ void gwm_b200_destroy(gwm_b200_ctx* c) {
     if (M.bstrip) cudaFree(M.bstrip);
     if (M.sur) cudaFree(M.sur);
     for (char* b : M.extra) cudaFree(b);
+    if (M.bcache_block) cudaFree(M.bcache_block);
   }
   for (auto st : c->mstreams) cudaStreamDestroy(st);
   for (auto ev : c->mjoin) cudaEventDestroy(ev);
@@ -953,6 +980,7 @@ int gwm_b200_set_boundary_state(gwm_b200_ctx* c, int member, const gwm_b200_fiel
   if (rc) return rc;
   Member& M = c->m[member];
   drop_graph(c);
+  M.bcache_n = 0;  // a fixed boundary state replaces a boundary cache
   if (!h) {
     M.has_boundary = M.has_tracer_boundary = false;
     return GWM_B200_OK;
@@ -981,6 +1009,89 @@ int gwm_b200_set_boundary_state(gwm_b200_ctx* c, int member, const gwm_b200_fiel
   CK(cudaStreamSynchronize(c->stream));
   M.has_boundary = true;
   M.has_tracer_boundary = tracers;
+  return GWM_B200_OK;
+}
+
+int gwm_b200_set_boundary_cache(gwm_b200_ctx* c, int member, int n, const int* offsets,
+                                const gwm_b200_fields* snapshots) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  drop_graph(c);
+  if (n <= 0 || !offsets || !snapshots) {
+    M.bcache_n = 0;
+    M.has_boundary = M.has_tracer_boundary = false;
+    return n == 0 ? GWM_B200_OK : fail(c, GWM_B200_ERR_ARG, "boundary cache needs snapshots and offsets");
+  }
+  for (int q = 1; q < n; ++q)  // validate_runtime_boundary_cache (runtime_case.cpp:260-262)
+    if (offsets[q] <= offsets[q - 1]) return fail(c, GWM_B200_ERR_ARG, "Boundary cache offsets must be strictly monotonic");
+  bool tracers = M.md.moist != 0;
+  for (int q = 0; q < n; ++q) {
+    const gwm_b200_fields& h = snapshots[q];
+    if (!h.rho_d || !h.rho_theta_m || !h.mom_u || !h.mom_v || !h.mom_w)
+      return fail(c, GWM_B200_ERR_ARG, "boundary snapshots need rho_d, rho_theta_m and the three momenta");
+    tracers = tracers && h.qv && h.qc && h.qr;
+  }
+  if (!M.bstrip) {
+    long long off = 0;
+    for (int f = 0; f < 8; ++f) { M.boff[f] = off; off += strip_len(M.g, kStripOrient[f]); }
+    M.boff[8] = off;
+    CK(cudaMalloc(&M.bstrip, 2 * off * sizeof(float)));
+    CK(cudaMemsetAsync(M.bstrip, 0, 2 * off * sizeof(float), c->stream));
+    M.bsave = M.bstrip + off;
+  }
+  if (M.bcache_block) { CK(cudaFree(M.bcache_block)); M.bcache_block = nullptr; }
+  const size_t snap_bytes = ((size_t)n * M.boff[8] * sizeof(float) + 255) / 256 * 256;
+  const size_t off_bytes = ((size_t)n * sizeof(int) + 255) / 256 * 256;
+  CK(cudaMalloc(&M.bcache_block, snap_bytes + off_bytes + sizeof(BoundaryClock)));
+  M.bcache = (float*)M.bcache_block;
+  M.bcache_off = (int*)(M.bcache_block + snap_bytes);
+  M.bclock = (BoundaryClock*)(M.bcache_block + snap_bytes + off_bytes);
+  const Geom& g = M.g;
+  for (int q = 0; q < n; ++q) {
+    const gwm_b200_fields& h = snapshots[q];
+    const float* src[8] = {h.rho_d, h.rho_theta_m, h.mom_u, h.mom_v, h.mom_w, h.qv, h.qc, h.qr};
+    for (int f = 0; f < (tracers ? 8 : 5); ++f) {
+      const int o = kStripOrient[f];
+      const size_t cnt = (size_t)(g.nx + (o == kFaceX)) * (g.ny + (o == kFaceY)) * (g.nz + (o == kFaceZ));
+      CK(cudaMemcpyAsync(M.staging, src[f], cnt * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+      StripJobs J{};
+      J.j[J.n++] = strip_job(nullptr, M.bcache + (size_t)q * M.boff[8] + M.boff[f], M.staging, o, 2);
+      CK(launch_strips(g, J, c->stream));
+      CK(cudaStreamSynchronize(c->stream));  // the staging buffer is reused by the next copy
+    }
+  }
+  CK(cudaMemcpyAsync(M.bcache_off, offsets, n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  BoundaryClock clk{};
+  clk.t_start = 0.0f;
+  clk.dt = M.md.step.dt;
+  CK(cudaMemcpyAsync(M.bclock, &clk, sizeof(clk), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  M.bcache_n = n;
+  M.has_boundary = true;
+  M.has_tracer_boundary = tracers;
+  return GWM_B200_OK;
+}
+
+int gwm_b200_set_step_start_time(gwm_b200_ctx* c, int member, float t) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  if (M.bcache_n <= 0) return fail(c, GWM_B200_ERR_ARG, "no boundary cache is set");
+  const float t0 = std::max(t, 0.0f);  // set_step_start_time (prepared_case_init.cpp:1006-1009)
+  CK(cudaMemcpyAsync(&M.bclock->t_start, &t0, sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return GWM_B200_OK;
+}
+
+int gwm_b200_get_step_start_time(gwm_b200_ctx* c, int member, float* t) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  if (!t) return fail(c, GWM_B200_ERR_ARG, "null output");
+  if (M.bcache_n <= 0) return fail(c, GWM_B200_ERR_ARG, "no boundary cache is set");
+  CK(cudaMemcpyAsync(t, &M.bclock->t_start, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return GWM_B200_OK;
 }
 

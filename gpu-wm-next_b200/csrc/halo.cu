@@ -379,6 +379,68 @@ cudaError_t launch_strips(const Geom& g, const StripJobs& jobs, cudaStream_t s) 
   return cudaGetLastError();
 }
 
+// BoundaryCacheIR::bracket (include/gwm/ingest/boundary_cache.hpp:52-76) and the
+// weight of interpolate_boundary_snapshot (src/ingest/runtime_case.cpp:205-221) for the
+// three updater calls of a step, then the next step's start time.
+__global__ void k_boundary_clock(BoundaryClock* c, const int* __restrict__ off, int n) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const float t0 = c->t_start, dt = c->dt;
+  const float sim[3] = {0.0f, dt, 0.5f * dt};  // dry_core.cu:568, 591, 620
+  for (int s = 0; s < 3; ++s) {
+    const int t = (int)lroundf(t0 + sim[s]);  // prepared_case_init.cpp:403-404
+    int lo = -1, hi = -1;
+    for (int q = 0; q < n; ++q) {
+      if (off[q] <= t) lo = q;
+      if (off[q] >= t) { hi = q; break; }
+    }
+    if (lo < 0) lo = 0;
+    if (hi < 0) hi = n - 1;
+    float a = 0.0f;
+    if (lo != hi && off[lo] != off[hi]) a = (float)(t - off[lo]) / (float)(off[hi] - off[lo]);
+    else hi = lo;  // the lower snapshot itself
+    c->lo[s] = lo;
+    c->hi[s] = hi;
+    c->alpha[s] = a;
+  }
+  c->t_start = t0 + dt;
+}
+
+// (1 - alpha) lower + alpha upper as interpolate_bundle writes it (runtime_case.cpp:113),
+// without contraction; tracer strips become rho_d * q (prepared_case_init.cpp:590).
+__global__ void k_boundary_interp(const float* __restrict__ cache, long long per_snap, long long dry_len,
+                                  long long cell_len, int ntr, const BoundaryClock* __restrict__ c, int stage,
+                                  float* __restrict__ out) {
+  const int lo = c->lo[stage], hi = c->hi[stage];
+  const float a = c->alpha[stage], b = 1.0f - a;
+  const float* L = cache + lo * per_snap;
+  const float* H = cache + hi * per_snap;
+  auto lerp = [&](long long e) { return lo == hi ? L[e] : __fadd_rn(__fmul_rn(b, L[e]), __fmul_rn(a, H[e])); };
+  const long long n = dry_len + (long long)ntr * cell_len;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    if (e < dry_len) {
+      out[e] = lerp(e);
+    } else {
+      const long long r = (e - dry_len) % cell_len;  // same position of the density strip
+      out[e] = __fmul_rn(lerp(r), lerp(e));
+    }
+  }
+}
+
+cudaError_t launch_boundary_clock(BoundaryClock* clock, const int* offsets, int n, cudaStream_t s) {
+  if (n <= 0) return cudaErrorInvalidValue;
+  k_boundary_clock<<<1, 32, 0, s>>>(clock, offsets, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_boundary_interp(const float* cache, long long per_snap, long long dry_len, long long cell_len,
+                                   int ntr, const BoundaryClock* clock, int stage, float* out, cudaStream_t s) {
+  if (stage < 0 || stage > 2 || cell_len <= 0) return cudaErrorInvalidValue;
+  const long long n = dry_len + (long long)ntr * cell_len;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 1184);
+  k_boundary_interp<<<blocks, 256, 0, s>>>(cache, per_snap, dry_len, cell_len, ntr, clock, stage, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_unpack(const Geom& g, int orient, const float* src, float* dst, cudaStream_t s) {
   const long long n = (long long)(g.nx + (orient == kFaceX)) * (g.ny + (orient == kFaceY)) *
                       (g.nz + (orient == kFaceZ));

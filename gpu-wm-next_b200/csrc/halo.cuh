@@ -50,6 +50,27 @@ struct StripJobs {
 long long strip_len(const Geom& g, int orient);  // compact floats of one field
 cudaError_t launch_strips(const Geom& g, const StripJobs& jobs, cudaStream_t s);
 
+// Prepared-case boundary updater (src/ingest/prepared_case_init.cpp:396-645,1006-1078)
+// on the device.  A cache of snapshots holds, per snapshot, the compact strips of the
+// balanced dry state (rho, rho*theta, u, v, w) and of the tracer mixing ratios; the
+// strips applied at an updater call are those of the snapshot interpolated at the
+// forecast second lround(step_start + sim_time) (runtime_case.cpp:205-228,
+// boundary_cache.hpp:52-76), tracers as rho_d * q (prepared_case_init.cpp:570-645).
+// The clock holds the step start time and, per RK stage (sim_time 0, dt, dt/2), the
+// bracketing snapshots and the weight; one kernel per step fills the table and
+// advances the start time by dt (float, as the driver's sim_time += dt), so a captured
+// step replays with the forecast time moving on.
+struct BoundaryClock {
+  float t_start, dt;
+  int lo[3], hi[3];
+  float alpha[3];
+};
+cudaError_t launch_boundary_clock(BoundaryClock* clock, const int* offsets, int n, cudaStream_t s);
+// Strips of stage `stage` (per snapshot: dry_len dry floats, then ntr cell strips of
+// cell_len floats) into out, laid out like one snapshot.
+cudaError_t launch_boundary_interp(const float* cache, long long per_snap, long long dry_len, long long cell_len,
+                                   int ntr, const BoundaryClock* clock, int stage, float* out, cudaStream_t s);
+
 // EOS over n values (K20 compute_pressure_kernel, dry_pressure_gradient.cu:27-35).
 cudaError_t launch_pressure(const float* rho, const float* rt, float* p, long long n, cudaStream_t s);
 

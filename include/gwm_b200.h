@@ -159,6 +159,30 @@ int gwm_b200_slow_tendencies(gwm_b200_ctx* ctx, int member, gwm_b200_fields* hos
  * faces of the boundary state are averaged as on upload.  NULL removes it (the Null
  * updaters).  Periodic sides are never touched. */
 int gwm_b200_set_boundary_state(gwm_b200_ctx* ctx, int member, const gwm_b200_fields* boundary);
+/* PreparedCaseBoundaryUpdater + PreparedCaseTracerBoundaryUpdater
+ * (src/ingest/prepared_case_init.cpp:396-645,1006-1078) on the device, for open sides.
+ * snapshots[q] (host arrays, field I/O layout) is the balanced state of boundary-cache
+ * entry q at forecast offset offsets[q] seconds (strictly increasing): rho_d,
+ * rho_theta_m and the three momenta, and for moist members the tracer MIXING RATIOS
+ * (kg/kg) in qv, qc, qr (all three, or none).  Only the outermost strips are kept (per
+ * snapshot: perimeter x nz floats per field).  At every updater call of a step (the dry
+ * stage starts, dry_core.cu:568, 591, 620, and the tracer stage inputs,
+ * dry_transport.cu:488-508, at sim_time 0, dt and dt/2) the strips applied are those of
+ * the cache interpolated at the forecast second lround(step_start + sim_time): the
+ * bracketing entries of BoundaryCacheIR::bracket (include/gwm/ingest/boundary_cache.hpp:
+ * 52-76) weighted as interpolate_boundary_snapshot (src/ingest/runtime_case.cpp:205-228),
+ * tracers as rho_d * q (prepared_case_init.cpp:570-645).  The reference interpolates the
+ * raw analysis fields and rebalances them on the host (hydrostatic columns, SOR face
+ * projection: ingest code); here the caller supplies each entry already balanced and the
+ * device interpolates the balanced strips.  The step start time starts at 0 and every
+ * step advances it by dt on the device (float, as the driver's sim_time += dt), also
+ * inside a replayed CUDA graph.  n = 0 removes the cache (the Null updaters); setting a
+ * fixed boundary state (gwm_b200_set_boundary_state) replaces it. */
+int gwm_b200_set_boundary_cache(gwm_b200_ctx* ctx, int member, int n, const int* offsets,
+                                const gwm_b200_fields* snapshots);
+/* PreparedCaseBoundaryUpdater::set_step_start_time (max(t, 0)) / the current value. */
+int gwm_b200_set_step_start_time(gwm_b200_ctx* ctx, int member, float t);
+int gwm_b200_get_step_start_time(gwm_b200_ctx* ctx, int member, float* t);
 /* Rayleigh damping layer (an extension: the reference has none).  Above z_bottom the
  * slow tendencies gain -tau(z) (u - u_ref(k)), -tau(z) (v - v_ref(k)) and -tau(z) w,
  * with tau(z) = rate * sin^2(pi/2 (z - z_bottom)/(z_top - z_bottom)) at each level's

@@ -86,6 +86,9 @@ def lib():
                               C.c_int, C.POINTER(Fields)]
         L.gwo_run_boundary.argtypes = [C.POINTER(Grid), C.POINTER(Step), C.POINTER(Rain), C.c_int,
                                        C.c_int, C.c_int, C.POINTER(Fields), C.POINTER(Fields)]
+        L.gwo_run_boundary_cache.argtypes = [C.POINTER(Grid), C.POINTER(Step), C.POINTER(Rain), C.c_int,
+                                             C.c_int, C.c_int, C.POINTER(Fields), C.c_int,
+                                             C.POINTER(C.c_int), C.POINTER(Fields), C.c_double]
         L.gwo_mlp_loss_grad.argtypes = [DP, DP, DP, DP, C.c_int, DP, DP]
         L.gwo_slow_tendencies.argtypes = [C.POINTER(Grid), C.POINTER(Step), C.c_int,
                                           C.POINTER(Fields), C.POINTER(Fields)]
@@ -218,16 +221,27 @@ PHASE_DRY, PHASE_TRACERS, PHASE_RAIN, PHASE_RAIN_NOMINAL = 1, 2, 4, 8
 
 
 def run(g: GridSpec, step: StepSpec, state: dict, nsteps: int = 1, phases: int = PHASE_DRY,
-        rain: Optional[RainSpec] = None, precision: int = 64, boundary: Optional[dict] = None) -> dict:
+        rain: Optional[RainSpec] = None, precision: int = 64, boundary: Optional[dict] = None,
+        boundary_cache: Optional[tuple] = None) -> dict:
     """Advance copies of ``state`` by ``nsteps`` steps; returns the new fields.
     ``boundary`` (same keys as a state; tracers optional) is a reference boundary state
-    applied by apply_reference_boundaries at every stage start."""
+    applied by apply_reference_boundaries at every stage start.  ``boundary_cache`` =
+    (offsets, snapshots, t_start) is the prepared-case updater: balanced snapshot states
+    (tracers qv, qc, qr as mixing ratios) at integer forecast offsets, interpolated at
+    lround(step start + stage time); t_start is the first step's start time."""
     out = {k: np.array(v, dtype=np.float64, copy=True) for k, v in state.items() if v is not None}
     gc, sc = g.c(), step.c()
     rc = rain.c() if rain is not None else None
     f = _fields(out)
     rcp = C.byref(rc) if rc is not None else None
-    if boundary is None:
+    if boundary_cache is not None:
+        offsets, snaps, t_start = boundary_cache
+        keep = [{k: np.array(v, dtype=np.float64, copy=True) for k, v in sn.items() if v is not None} for sn in snaps]
+        arr = (Fields * len(keep))(*[_fields(d) for d in keep])
+        off = (C.c_int * len(keep))(*[int(t) for t in offsets])
+        _check(lib().gwo_run_boundary_cache(C.byref(gc), C.byref(sc), rcp, phases, nsteps, precision, C.byref(f),
+                                            len(keep), off, arr, float(t_start)))
+    elif boundary is None:
         _check(lib().gwo_run(C.byref(gc), C.byref(sc), rcp, phases, nsteps, precision, C.byref(f)))
     else:
         bnd = {k: np.array(v, dtype=np.float64, copy=True) for k, v in boundary.items() if v is not None}

@@ -936,18 +936,21 @@ void apply_reference_boundaries(std::vector<DryState<T>>& S, const std::vector<D
   }
 }
 
-// advance_dry_state_ssprk3: dry_core.cu:541-651.  With a boundary state B the
-// updater applies apply_reference_boundaries at the three stage starts (:568, :591,
-// :620); the blend partner q0 is the state before the first application.
+// advance_dry_state_ssprk3: dry_core.cu:541-651.  With boundary states the updater
+// applies apply_reference_boundaries at the three stage starts (:568, :591, :620), with
+// Bs[0], Bs[1], Bs[2] (the boundary at sim_time 0, dt, dt/2); the blend partner q0 is the
+// state before the first application.
 template <class T>
 void advance_dry_ssprk3(States<T>& S, const std::vector<Desc>& L, const Metrics<T>& M,
-                        const StepCfg<T>& cfg, const States<T>* B = nullptr) {
+                        const StepCfg<T>& cfg, const States<T>* const* Bs = nullptr) {
   const size_t n = S.size();
   States<T> q0 = S, q1 = S, q2 = S, tmp = S, tend;
+  const States<T>* B = Bs ? Bs[0] : nullptr;
   if (B) apply_reference_boundaries(S, *B, L);
   compute_slow_tendencies(S, L, M, cfg, tend);
   for (size_t r = 0; r < n; ++r) update_state(q1[r], S[r], tend[r], cfg.dt);
   if (cfg.fast_modes) fast_modes(q1, L, M, cfg);
+  if (Bs) B = Bs[1];
   if (B) apply_reference_boundaries(q1, *B, L);
   compute_slow_tendencies(q1, L, M, cfg, tend);
   for (size_t r = 0; r < n; ++r) {
@@ -955,6 +958,7 @@ void advance_dry_ssprk3(States<T>& S, const std::vector<Desc>& L, const Metrics<
     blend_state(q2[r], q0[r], tmp[r], T(0.75f), T(0.25f));
   }
   if (cfg.fast_modes) fast_modes(q2, L, M, cfg);
+  if (Bs) B = Bs[2];
   if (B) apply_reference_boundaries(q2, *B, L);
   compute_slow_tendencies(q2, L, M, cfg, tend);
   for (size_t r = 0; r < n; ++r) {
@@ -994,13 +998,14 @@ void tracer_stage(const Field<T>& qin, const Field<T>& rho, const Field<T>& u, c
       }
 }
 
-// tracers[r][t] is tracer t of rank r (registry order).  With boundary tracers QB the
+// tracers[r][t] is tracer t of rank r (registry order).  With boundary tracers QBs the
 // tracer updater applies apply_reference_boundaries to each stage input
-// (dry_transport.cu:254-276, 484-517): a copy of the state, then q1, then q2.
+// (dry_transport.cu:254-276, 484-517): a copy of the state (QBs[0], sim_time 0), then q1
+// (QBs[1], dt), then q2 (QBs[2], dt/2).
 template <class T>
 void advance_tracers_ssprk3(std::vector<std::vector<Field<T>>>& Q, const States<T>& S,
                             const std::vector<Desc>& L, const Metrics<T>& M, const StepCfg<T>& cfg,
-                            const std::vector<std::vector<Field<T>>>* QB = nullptr) {
+                            const std::vector<std::vector<Field<T>>>* const* QBs = nullptr) {
   const size_t n = S.size();
   if (n == 0 || Q.empty() || Q[0].empty()) return;
   std::vector<Field<T>> R(n), U(n), V(n), W(n);
@@ -1014,20 +1019,20 @@ void advance_tracers_ssprk3(std::vector<std::vector<Field<T>>>& Q, const States<
   for (size_t t = 0; t < nt; ++t) {
     std::vector<Field<T>> q0(n), q1(n), q2(n), tmp(n), st(n);
     for (size_t r = 0; r < n; ++r) { q0[r] = Q[r][t]; st[r] = Q[r][t]; q1[r] = q2[r] = tmp[r] = Q[r][t]; }
-    auto bnd = [&](std::vector<Field<T>>& F) {
-      if (QB)
-        for (size_t r = 0; r < n; ++r) copy_strips(F[r], (*QB)[r][t], L[r]);
+    auto bnd = [&](std::vector<Field<T>>& F, int stage) {
+      if (QBs && QBs[stage])
+        for (size_t r = 0; r < n; ++r) copy_strips(F[r], (*QBs[stage])[r][t], L[r]);
     };
-    bnd(st);
+    bnd(st, 0);
     exchange_scalar(st, L);
     for (size_t r = 0; r < n; ++r) tracer_stage(st[r], R[r], U[r], V[r], W[r], q1[r], L[r], M, cfg.dt);
-    bnd(q1);
+    bnd(q1, 1);
     exchange_scalar(q1, L);
     for (size_t r = 0; r < n; ++r) {
       tracer_stage(q1[r], R[r], U[r], V[r], W[r], tmp[r], L[r], M, cfg.dt);
       blend_field(q2[r], q0[r], tmp[r], T(0.75f), T(0.25f));
     }
-    bnd(q2);
+    bnd(q2, 2);
     exchange_scalar(q2, L);
     for (size_t r = 0; r < n; ++r) {
       tracer_stage(q2[r], R[r], U[r], V[r], W[r], tmp[r], L[r], M, cfg.dt);

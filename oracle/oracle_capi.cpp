@@ -185,9 +185,20 @@ template <class T> gwo::RainCfg<T> rain_from(const gwo_rain* r) {
   return c;
 }
 
+// Prepared-case boundary cache (test restatement of prepared_case_init.cpp:396-645,
+// 1006-1078, runtime_case.cpp:205-228, boundary_cache.hpp:52-76): snapshots of balanced
+// states (tracers as mixing ratios) at integer forecast offsets; the boundary of an
+// updater call is the snapshot interpolated at lround(step_start + sim_time).
+struct BoundaryCacheIn {
+  int n = 0;
+  const int* offsets = nullptr;
+  const gwo_fields* snapshots = nullptr;
+  float t_start = 0.0f;
+};
+
 template <class T>
 int run_impl(const gwo_grid* g, const gwo_step* st, const gwo_rain* rn, int phases, int nsteps,
-             gwo_fields* io, const gwo_fields* bnd) {
+             gwo_fields* io, const gwo_fields* bnd, const BoundaryCacheIn* cache = nullptr) {
   const auto L = layout_from(g);
   const auto M = metrics_from<T>(g);
   auto S = make_states<T>(L);
@@ -237,9 +248,88 @@ int run_impl(const gwo_grid* g, const gwo_step* st, const gwo_rain* rn, int phas
   const auto cfg = step_from<T>(st, &M);
   gwo::RainCfg<T> rc;
   if (rn) rc = rain_from<T>(rn);
+  // boundary cache: the snapshots on the rank layout, and per stage the interpolated state
+  std::vector<gwo::States<T>> CS;
+  std::vector<std::vector<std::vector<gwo::Field<T>>>> CQ;  // [snapshot][rank][tracer] mixing ratios
+  gwo::States<T> BS[3];
+  std::vector<std::vector<gwo::Field<T>>> QS[3];
+  bool cache_tracers = false;
+  if (cache && cache->n > 0) {
+    cache_tracers = moist;
+    for (int q = 0; q < cache->n; ++q) {
+      const gwo_fields& f = cache->snapshots[q];
+      CS.push_back(make_states<T>(L));
+      states_in(CS.back(), &f, L, g);
+      cache_tracers = cache_tracers && f.qv && f.qc && f.qr;
+    }
+    if (cache_tracers)
+      for (int q = 0; q < cache->n; ++q) {
+        std::vector<std::vector<gwo::Field<T>>> per_rank;
+        for (const auto& d : L) {
+          std::vector<gwo::Field<T>> tq;
+          for (int t = 0; t < 3; ++t) tq.emplace_back(d.nxl(), d.nyl(), d.nz, d.halo);
+          per_rank.push_back(std::move(tq));
+        }
+        double* src[3] = {cache->snapshots[q].qv, cache->snapshots[q].qc, cache->snapshots[q].qr};
+        for (int t = 0; t < 3; ++t) {
+          std::vector<gwo::Field<T>*> fp;
+          for (auto& rq : per_rank) fp.push_back(&rq[t]);
+          scatter(src[t], fp, L, g);
+        }
+        CQ.push_back(std::move(per_rank));
+      }
+  }
+  float t_start = cache ? std::max(cache->t_start, 0.0f) : 0.0f;
   for (int s = 0; s < nsteps; ++s) {  // gwm_prepared_case_driver.cpp:427-463
-    if (phases & 1) gwo::advance_dry_ssprk3(S, L, M, cfg, bnd ? &B : nullptr);
-    if (phases & 2) gwo::advance_tracers_ssprk3(Q, S, L, M, cfg, QB.empty() ? nullptr : &QB);
+    const gwo::States<T>* Bs[3] = {&B, &B, &B};
+    const std::vector<std::vector<gwo::Field<T>>>* QBs[3] = {&QB, &QB, &QB};
+    if (!CS.empty()) {
+      const float dtf = (float)st->dt;
+      const float sim[3] = {0.0f, dtf, 0.5f * dtf};
+      for (int k = 0; k < 3; ++k) {
+        const int t = (int)std::lround(t_start + sim[k]);
+        int lo = -1, hi = -1;
+        for (int q = 0; q < cache->n; ++q) {
+          if (cache->offsets[q] <= t) lo = q;
+          if (cache->offsets[q] >= t) { hi = q; break; }
+        }
+        if (lo < 0) lo = 0;
+        if (hi < 0) hi = cache->n - 1;
+        const bool one = lo == hi || cache->offsets[lo] == cache->offsets[hi];
+        const float alpha = one ? 0.0f : (float)(t - cache->offsets[lo]) / (float)(cache->offsets[hi] - cache->offsets[lo]);
+        const T a = (T)alpha, b = T(1) - (T)alpha;
+        auto lerp = [&](const gwo::Field<T>& x, const gwo::Field<T>& y, gwo::Field<T>& out) {
+          out = x;
+          if (!one)
+            for (size_t e = 0; e < out.d.size(); ++e) out.d[e] = b * x.d[e] + a * y.d[e];
+        };
+        BS[k] = CS[lo];
+        for (size_t r = 0; r < L.size(); ++r) {
+          lerp(CS[lo][r].rho, CS[hi][r].rho, BS[k][r].rho);
+          lerp(CS[lo][r].rt, CS[hi][r].rt, BS[k][r].rt);
+          lerp(CS[lo][r].mu, CS[hi][r].mu, BS[k][r].mu);
+          lerp(CS[lo][r].mv, CS[hi][r].mv, BS[k][r].mv);
+          lerp(CS[lo][r].mw, CS[hi][r].mw, BS[k][r].mw);
+        }
+        QS[k].clear();
+        if (cache_tracers)
+          for (size_t r = 0; r < L.size(); ++r) {
+            std::vector<gwo::Field<T>> tq(3);
+            for (int t2 = 0; t2 < 3; ++t2) {
+              lerp(CQ[lo][r][t2], CQ[hi][r][t2], tq[t2]);
+              for (size_t e = 0; e < tq[t2].d.size(); ++e) tq[t2].d[e] *= BS[k][r].rho.d[e];  // rho_d * q
+            }
+            QS[k].push_back(std::move(tq));
+          }
+        Bs[k] = &BS[k];
+        QBs[k] = cache_tracers ? &QS[k] : nullptr;
+      }
+      t_start = t_start + dtf;  // the driver's sim_time += dt (float)
+    }
+    const bool dry_bnd = bnd || !CS.empty();
+    const bool tr_bnd = !CS.empty() ? cache_tracers : !QB.empty();
+    if (phases & 1) gwo::advance_dry_ssprk3(S, L, M, cfg, dry_bnd ? Bs : nullptr);
+    if (phases & 2) gwo::advance_tracers_ssprk3(Q, S, L, M, cfg, tr_bnd ? QBs : nullptr);
     if (phases & 4) gwo::apply_warm_rain(S, Q, L, &M, rc, io->precip ? &P : nullptr);
     if (phases & 8) gwo::apply_warm_rain<T>(S, Q, L, nullptr, rc, io->precip ? &P : nullptr);
   }
@@ -445,6 +535,20 @@ int gwo_run_boundary(const gwo_grid* g, const gwo_step* st, const gwo_rain* rn, 
   return guard([&] {
     return precision == 32 ? run_impl<float>(g, st, rn, phases, nsteps, io, bnd)
                            : run_impl<double>(g, st, rn, phases, nsteps, io, bnd);
+  });
+}
+
+// gwo_run with a prepared-case boundary cache: n snapshots (balanced states; tracers as
+// mixing ratios, optional) at strictly increasing forecast offsets (s); t_start is the
+// first step's start time.
+int gwo_run_boundary_cache(const gwo_grid* g, const gwo_step* st, const gwo_rain* rn, int phases, int nsteps,
+                           int precision, gwo_fields* io, int n, const int* offsets, const gwo_fields* snapshots,
+                           double t_start) {
+  return guard([&] {
+    BoundaryCacheIn c;
+    c.n = n; c.offsets = offsets; c.snapshots = snapshots; c.t_start = (float)t_start;
+    return precision == 32 ? run_impl<float>(g, st, rn, phases, nsteps, io, nullptr, &c)
+                           : run_impl<double>(g, st, rn, phases, nsteps, io, nullptr, &c);
   });
 }
 

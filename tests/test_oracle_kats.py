@@ -260,3 +260,23 @@ def test_virtual_rank_equivalence(orc, precision):
     for k in ("rho", "rho_theta", "u", "v", "w"):
         a, b = outs[0][k], outs[1][k]
         assert np.max(np.abs(a - b)) <= tol * max(1.0, np.max(np.abs(a))), k
+
+
+def test_boundary_cache_single_entry_is_the_fixed_boundary(orc):
+    # the prepared-case updater with one cache entry (or past its last entry) applies that
+    # entry's strips at every call: the same step as apply_reference_boundaries with it
+    g = orc.GridSpec(14, 10, 6, dx=1000.0, dy=1000.0, z_top=6000.0, periodic_x=False, periodic_y=False)
+    s = orc.case("density_current", g, orc.CaseSpec(theta_perturbation=3.0, center_z_fraction=0.4,
+                                                     radius_x_fraction=0.3, radius_y_fraction=0.3,
+                                                     radius_z_fraction=0.3, u_background=2.0))
+    b0 = {k: v * 1.01 for k, v in s.items()}
+    b1 = {k: v * 0.98 for k, v in s.items()}
+    st = orc.StepSpec(dt=1.0, fast_substeps=2)
+    fixed = orc.run(g, st, s, 3, precision=64, boundary=b1)
+    one = orc.run(g, st, s, 3, precision=64, boundary_cache=([0], [b1], 0.0))
+    past = orc.run(g, st, s, 3, precision=64, boundary_cache=([0, 10], [b0, b1], 100.0))
+    for k in ("rho", "rho_theta", "u", "v", "w"):
+        assert np.array_equal(fixed[k], one[k]), k
+        assert np.array_equal(fixed[k], past[k]), k
+    mid = orc.run(g, st, s, 3, precision=64, boundary_cache=([0, 10], [b0, b1], 4.0))
+    assert not np.array_equal(mid["rho"], fixed["rho"])
