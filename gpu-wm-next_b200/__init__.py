@@ -206,6 +206,8 @@ def lib():
     L.gwm_b200_dry_pressure.argtypes = [vp, vp, vp, C.c_longlong, vp]
     L.gwm_b200_test_stall_tile_load.argtypes = [vp, C.c_int, C.c_int]
     L.gwm_b200_set_boundary_cache.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(_Fields)]
+    L.gwm_b200_runtime_summary_json.argtypes = [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_longlong,
+                                                 C.POINTER(C.c_longlong)]
     L.gwm_b200_set_step_start_time.argtypes = [vp, C.c_int, C.c_float]
     L.gwm_b200_get_step_start_time.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
     L.gwm_b200_tracer_add.argtypes = [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
@@ -240,7 +242,7 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_rain_record",
             "gwm_b200_mlp_train", "gwm_b200_mlp_loss_grad", "gwm_b200_set_rain_surrogate",
             "gwm_b200_surrogate_fallbacks", "gwm_b200_surrogate_stats", "gwm_b200_layout",
-            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_test_stall_tile_load", "gwm_b200_set_boundary_cache",
+            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_test_stall_tile_load", "gwm_b200_set_boundary_cache", "gwm_b200_runtime_summary_json",
             "gwm_b200_set_step_start_time", "gwm_b200_get_step_start_time", "gwm_b200_tracer_add",
             "gwm_b200_tracer_find", "gwm_b200_tracer_count", "gwm_b200_tracer_name", "gwm_b200_tracer_upload",
             "gwm_b200_tracer_download", "gwm_b200_tracer_total", "gwm_b200_scalar_ssprk3", "gwm_b200_grid_z_center", "gwm_b200_ranks_to_global",
@@ -427,6 +429,22 @@ class Model:
                 keep.append(a)
                 setattr(f, cname, _fptr(a))
         self._check(lib().gwm_b200_set_boundary_state(self._h, member, C.byref(f)), "set_boundary_state")
+
+    def runtime_summary(self, member: int = 0, indent: str = "  ") -> dict:
+        """summarize_runtime_state as the reference's JSON (runtime_state_summary_to_json),
+        reduced on the device; returned parsed, with the text under "_json"."""
+        import json
+        need = C.c_longlong()
+        lib().gwm_b200_runtime_summary_json(self._h, member, indent.encode(), None, 0, C.byref(need))
+        buf = C.create_string_buffer(int(need.value))
+        rc = lib().gwm_b200_runtime_summary_json(self._h, member, indent.encode(), buf, len(buf), None)
+        text = buf.value.decode()
+        if rc not in (OK, ERR_STATE):
+            self._check(rc, "runtime_summary")
+        out = json.loads(text.replace("nan", "NaN").replace("inf", "Infinity"))
+        out["_json"] = text
+        out["_status"] = rc
+        return out
 
     def set_boundary_cache(self, offsets, snapshots, member: int = 0):
         """The prepared-case boundary updater: ``snapshots`` are balanced states (dicts of the

@@ -20,6 +20,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <iomanip>
+#include <sstream>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -1796,6 +1798,107 @@ int gwm_b200_budgets(gwm_b200_ctx* c, int member, gwm_b200_budget* out) {
   if (!std::isfinite(b.total_dry_mass) || !std::isfinite(b.total_rho_theta_m) || !(b.rho_min > 0.0))
     return fail(c, GWM_B200_ERR_STATE, "non-finite or non-positive density in the state");
   return GWM_B200_OK;
+}
+
+// summarize_runtime_state + runtime_state_summary_to_json (src/core/runtime_summary.cpp:
+// 27-178, 180-247) from FP64 device reductions over the member's global fields.
+int gwm_b200_runtime_summary_json(gwm_b200_ctx* c, int member, const char* indent, char* buf, long long cap,
+                                  long long* len) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  gwm_b200_budget b{};
+  const int state_rc = gwm_b200_budgets(c, member, &b);
+  if (state_rc != GWM_B200_OK && state_rc != GWM_B200_ERR_STATE) return state_rc;
+  const Geom& g = M.g;
+  cudaStream_t s = c->stream;
+  const int nt = (int)M.reg.size();
+  std::vector<ReduceOut> col(nt), mix(nt);
+  for (int t = 0; t < nt; ++t) {
+    CK(launch_reduce(g, kCell, 2, M.reg[t].f[0], nullptr, M.idc, M.terrain_active, M.red_part, M.red_out + 20, s));
+    CK(launch_reduce(g, kCell, 1, M.reg[t].f[0], M.Q[0], nullptr, 0, M.red_part, M.red_out + 21, s));
+    ReduceOut r[2];
+    CK(cudaMemcpyAsync(r, M.red_out + 20, sizeof(r), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    col[t] = r[0];
+    mix[t] = r[1];
+  }
+  // moisture budget: water paths from the warm-rain tracers, surface precipitation from
+  // the accumulation (moist members)
+  auto path = [&](const char* name) {
+    for (int t = 0; t < nt; ++t)
+      if (M.reg[t].name == name) return col[t].sum;
+    return 0.0;
+  };
+  const double vap = path("specific_humidity"), cld = path("cloud_water_mixing_ratio"),
+               rain = path("rain_water_mixing_ratio");
+  double psum = 0.0, pmean = 0.0, pmax = 0.0, pfrac = 0.0, pmean_wet = 0.0;
+  long long ncell = 0, nwet = 0;
+  if (M.md.moist) {
+    const long long n2 = (long long)g.nx * g.ny;
+    CK(launch_reduce_2d(M.precip, M.pcomp, n2, M.red_part, M.red_out + 20, s, 0));
+    CK(launch_reduce_2d(M.precip, M.pcomp, n2, M.red_part, M.red_out + 21, s, 1));
+    ReduceOut r[2];
+    CK(cudaMemcpyAsync(r, M.red_out + 20, sizeof(r), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    psum = r[0].sum;
+    pmean = r[0].sum / (double)n2;
+    pmax = r[0].mx;
+    ncell = n2;
+    nwet = (long long)r[1].sum;
+    pfrac = (double)nwet / (double)n2;
+    // every accumulated value is >= 0, so the precipitating cells hold the whole sum
+    if (nwet > 0) pmean_wet = r[0].sum / (double)nwet;
+  }
+  const std::string in = indent ? indent : "  ";
+  std::ostringstream o;
+  o << std::setprecision(17);
+  o << "{\n";
+  o << in << "\"total_dry_mass\": " << b.total_dry_mass << ",\n";
+  o << in << "\"total_rho_theta_m\": " << b.total_rho_theta_m << ",\n";
+  o << in << "\"total_horizontal_momentum_x\": " << b.total_horizontal_momentum_x << ",\n";
+  o << in << "\"total_horizontal_momentum_y\": " << b.total_horizontal_momentum_y << ",\n";
+  o << in << "\"total_vertical_momentum\": " << b.total_vertical_momentum << ",\n";
+  o << in << "\"rho_d\": {\"min\": " << b.rho_min << ", \"max\": " << b.rho_max << "},\n";
+  o << in << "\"theta_m\": {\"min\": " << b.theta_min << ", \"max\": " << b.theta_max << "},\n";
+  o << in << "\"u_face\": {\"min\": " << b.u_min << ", \"max\": " << b.u_max << "},\n";
+  o << in << "\"v_face\": {\"min\": " << b.v_min << ", \"max\": " << b.v_max << "},\n";
+  o << in << "\"w_face\": {\"min\": " << b.w_min << ", \"max\": " << b.w_max << "},\n";
+  o << in << "\"moisture\": {\n";
+  o << in << "  \"vapor_water_path_sum_kg_m2\": " << vap << ",\n";
+  o << in << "  \"cloud_water_path_sum_kg_m2\": " << cld << ",\n";
+  o << in << "  \"rain_water_path_sum_kg_m2\": " << rain << ",\n";
+  o << in << "  \"condensed_water_path_sum_kg_m2\": " << cld + rain << ",\n";
+  o << in << "  \"total_water_path_sum_kg_m2\": " << vap + (cld + rain) << ",\n";
+  o << in << "  \"accumulated_surface_precipitation_sum_mm\": " << psum << ",\n";
+  o << in << "  \"mean_surface_precipitation_mm\": " << pmean << ",\n";
+  o << in << "  \"max_surface_precipitation_mm\": " << pmax << ",\n";
+  o << in << "  \"total_surface_cell_count\": " << ncell << ",\n";
+  o << in << "  \"precipitating_surface_cell_count\": " << nwet << ",\n";
+  o << in << "  \"precipitating_surface_fraction\": " << pfrac << ",\n";
+  o << in << "  \"mean_precipitating_surface_precipitation_mm\": " << pmean_wet << "\n";
+  o << in << "},\n";
+  o << in << "\"tracers\": {\n";
+  for (int t = 0; t < nt; ++t) {
+    const auto& T = M.reg[t];
+    o << in << "  \"" << T.name << "\": {\n";
+    o << in << "    \"units\": \"" << T.units << "\",\n";
+    o << in << "    \"positive\": " << (T.positive ? "true" : "false") << ",\n";
+    o << in << "    \"column_integrated_sum_kg_m2\": " << col[t].sum << ",\n";
+    o << in << "    \"mixing_ratio\": {\"min\": " << mix[t].mn << ", \"max\": " << mix[t].mx << "}\n";
+    o << in << "  }" << (t + 1 != nt ? "," : "") << "\n";
+  }
+  o << in << "}\n";
+  o << "}";
+  const std::string js = o.str();
+  if (len) *len = (long long)js.size() + 1;
+  if (buf && cap > 0) {
+    const size_t n = std::min<size_t>(js.size(), (size_t)cap - 1);
+    std::memcpy(buf, js.data(), n);
+    buf[n] = 0;
+    if ((long long)js.size() + 1 > cap) return fail(c, GWM_B200_ERR_ARG, "summary buffer too small");
+  }
+  return state_rc;
 }
 
 // ---------------------------------------------------------------------------

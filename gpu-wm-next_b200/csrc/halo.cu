@@ -297,11 +297,13 @@ __global__ void __launch_bounds__(256) k_reduce_pass1(const Geom g, int o, int m
   }
 }
 
-__global__ void k_reduce_2d_pass1(const double* a, const double* b, long long n, double* part) {
+// mode 0: the value a + b; 1: 1 where a + b > 0, else 0 (a count of positive cells)
+__global__ void k_reduce_2d_pass1(const double* a, const double* b, long long n, double* part, int mode) {
   double s = 0.0, mn = DBL_MAX, mx = -DBL_MAX;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
        q += (long long)gridDim.x * blockDim.x) {
-    const double v = a[q] + (b ? b[q] : 0.0);
+    double v = a[q] + (b ? b[q] : 0.0);
+    if (mode == 1) v = v > 0.0 ? 1.0 : 0.0;
     s += v;
     mn = fmin(mn, v);
     mx = fmax(mx, v);
@@ -479,8 +481,8 @@ cudaError_t launch_reduce(const Geom& g, int orient, int mode, const float* f, c
 }
 
 cudaError_t launch_reduce_2d(const double* a, const double* b, long long n, double* partials,
-                             ReduceOut* out, cudaStream_t s) {
-  k_reduce_2d_pass1<<<kReduceBlocks, 256, 0, s>>>(a, b, n, partials);
+                             ReduceOut* out, cudaStream_t s, int mode) {
+  k_reduce_2d_pass1<<<kReduceBlocks, 256, 0, s>>>(a, b, n, partials, mode);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_reduce_pass2<<<1, 256, 0, s>>>(partials, kReduceBlocks, out);

@@ -86,6 +86,6 @@ cudaError_t launch_reduce(const Geom& g, int orient, int mode, const float* f, c
                           const float* idz, int idz_terrain, double* partials, ReduceOut* out,
                           cudaStream_t s);
 cudaError_t launch_reduce_2d(const double* a, const double* b, long long n, double* partials,
-                             ReduceOut* out, cudaStream_t s);
+                             ReduceOut* out, cudaStream_t s, int mode = 0);
 
 }  // namespace gwmb

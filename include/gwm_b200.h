@@ -272,6 +272,17 @@ int gwm_b200_mlp_loss_grad(const float* params, const float* norm, const float* 
 int gwm_b200_test_stall_tile_load(gwm_b200_ctx* ctx, int member, int plane);
 /* FP64 budgets of the current state. */
 int gwm_b200_budgets(gwm_b200_ctx* ctx, int member, gwm_b200_budget* out);
+/* summarize_runtime_state + runtime_state_summary_to_json (src/core/runtime_summary.cpp:
+ * 27-247): the dry summary, every registered tracer's column integral sum(rho q dz) and
+ * mixing-ratio range (rho q / max(rho, 1e-12)), and the moisture budget (water paths of the
+ * warm-rain tracers, surface precipitation sum, mean, maximum and precipitating cells),
+ * reduced in FP64 on the device over the member's global fields (the reference's
+ * per-rank sums for a one-rank layout), written as the reference's JSON (17 digits) with
+ * `indent` (NULL: two spaces) into buf (cap bytes, NUL-terminated).  *len (may be NULL)
+ * receives the bytes needed.  A state with a non-finite or non-positive density is
+ * written and reported as GWM_B200_ERR_STATE. */
+int gwm_b200_runtime_summary_json(gwm_b200_ctx* ctx, int member, const char* indent, char* buf, long long cap,
+                                  long long* len);
 /* Tile shape of a kernel.  kernel 0 = slow stage: rows 3 = owned 32x16 tiles fed by
  * TMA tile loads (flat terrain; terrain falls back to 16), 8 or 16 = overlapped 32-wide
  * tiles (default 16).  kernel 2 = tracer stage: rows 3 = owned 32x16 tiles fed by TMA
