@@ -261,9 +261,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_rain_net(const RainArgs a, cons
           first = atomicAdd(&s_tail, n);
           // ring space: the last row must lie within kTiles tiles of the oldest unconsumed
           const int need = (first + n - 1) / kNT - kTiles;
-          unsigned spins = 0;
+          WaitDeadline dl;
           while (*vconsumed <= need && !(bad = *vfail)) {
-            if (++spins > kMaxSpin) {
+            if (dl.expired()) {
               atomicExch(&s_fail, 1);
               atomicExch(s.err, 1);
               bad = 1;
@@ -360,7 +360,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_rain_net(const RainArgs a, cons
       const int pos = t % kTiles;
       if (ct == 0) {  // a full tile, or the remainder once every producer has finished
         int cmd = -1;
-        for (unsigned spins = 0; spins < kMaxSpin; ++spins) {
+        WaitDeadline dl;
+        while (!dl.expired()) {
           if (*vfail) { cmd = 0; break; }  // a producer gave up: reserved rows may be unwritten
           if (mbar_try_wait(&s_full[pos], (t / kTiles) & 1)) { cmd = kNT; break; }
           if (*vdone == kProducerWarps) {

@@ -3,9 +3,11 @@
 //
 // A field plane tile (with its halo) is fetched by one elected thread with
 // cp.async.bulk.tensor.3d into shared memory; completion is tracked by an mbarrier
-// transaction count.  Every wait is bounded: after kMaxSpin polls the waiting thread
-// records an error in the kernel's error word and the kernel unwinds cleanly (the
-// caller checks the word after the launch).  Tiles are never multicast.
+// transaction count.  Every wait is bounded in device time: after kWaitNs (%globaltimer)
+// the waiting thread records an error in the kernel's error word and the kernel unwinds
+// cleanly (the caller checks the word after the launch).  The limit is a time, not a
+// poll count, because mbarrier.try_wait may suspend the thread for a hardware-defined
+// interval on every call.  Tiles are never multicast.
 //
 // Alignment rules honoured by every caller: the innermost box coordinate x is a
 // multiple of 4 floats (16 bytes), boxes are a multiple of 16 bytes wide, and the
@@ -18,7 +20,27 @@
 
 namespace gwmb {
 
-constexpr unsigned kMaxSpin = 1u << 24;  // ~ tens of ms of polling before giving up
+constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s of device time before giving up
+
+__device__ __forceinline__ unsigned long long device_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Deadline of one bounded wait: expired() turns true once kWaitNs have passed since its
+// first call (the clock is read on the first call and then every 32nd).
+struct WaitDeadline {
+  unsigned long long t0 = 0;
+  unsigned n = 0;
+  __device__ __forceinline__ bool expired() {
+    if (n++ == 0) {
+      t0 = device_ns();
+      return false;
+    }
+    return (n & 31u) == 0 && device_ns() - t0 > kWaitNs;
+  }
+};
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -58,9 +80,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
 
 // Bounded wait for phase `parity` of an mbarrier.  Returns false on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  for (unsigned n = 0; n < kMaxSpin; ++n)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
+  WaitDeadline d;
+  while (!mbar_try_wait(bar, parity))
+    if (d.expired()) return false;
+  return true;
 }
 
 // 3-D tiled TMA load of box (x, y, z) of `map` into shared memory `dst`,
