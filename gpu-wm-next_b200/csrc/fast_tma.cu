@@ -22,6 +22,8 @@
 // pipeline in registers and needs no halo threads reading global memory.  The level
 // tables (reference means, metric columns, EOS base state) follow the ring in dynamic
 // shared memory, sized by nz.
+#include <type_traits>
+
 #include "dycore.cuh"
 #include "tma.cuh"
 
@@ -220,147 +222,162 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
   }
   __syncthreads();
 
-  bool aborted = false;
-  for (int k = 0; k < nz; ++k) {
-    const int pb = k & 1;
-    const float* st = ring + (k % NSLOT) * slot;
-    const float* stn = ring + ((k + 1) % NSLOT) * slot;
-    // ---- pressure perturbation of plane k+1 (its tiles were issued a plane ago)
-    if (k + 1 < nz) {
-      wait_plane(k + 1, k);
-      if (FIRST && !PIN) plane_p(k + 1);
+  // Interior tiles (full, away from every periodic edge ring and open side) run a copy
+  // of the plane loop compiled without the edge logic: plain stores instead of the
+  // periodic mirror stores, and none of the open-boundary face tests.  Both copies do
+  // the same arithmetic on the same values.
+  const bool interior = !edge && (g.per_x || (i0 > 0 && i0 + TX < nx)) && (g.per_y || (j0 > 0 && j0 + TY < ny));
+  auto plane_loop = [&](auto tile_class) -> bool {  // true when a bounded wait gave up
+    constexpr bool IN = decltype(tile_class)::value;
+    const bool o0 = IN || own0, o1 = IN || own1;
+    const bool su = !IN && skip_u, sv = !IN && skip_v0, hs = !IN && h_skip;
+    auto put = [&](float* f, const Geom& gg, int o, int i, int j, int kk, float v) {
+      if (IN) f[gidx(gg, i, j, kk)] = v;
+      else store_tile(f, gg, o, i, j, kk, v, edge);
+    };
+    for (int k = 0; k < nz; ++k) {
+      const int pb = k & 1;
+      const float* st = ring + (k % NSLOT) * slot;
+      const float* stn = ring + ((k + 1) % NSLOT) * slot;
+      // ---- pressure perturbation of plane k+1 (its tiles were issued a plane ago)
+      if (k + 1 < nz) {
+        wait_plane(k + 1, k);
+        if (FIRST && !PIN) plane_p(k + 1);
+      }
+      // ---- faces of plane k: K12/K13 horizontal momenta, K14 vertical momentum at face k+1
+      // p'(r, c) of plane k (P0) and k+1 (P1) in s_p coordinates (row 0 = j0-1, column
+      // 0 = i0-1): loaded with the tiles, or derived above in a first substep
+      auto P0 = [&](int r, int c) { return PIN ? st[O_P + r * CBW + c + 3] : s_p[pb][r][c]; };
+      auto P1 = [&](int r, int c) { return PIN ? stn[O_P + r * CBW + c + 3] : s_p[pb ^ 1][r][c]; };
+      float du0 = 0.f, dv0 = 0.f, du1 = 0.f, dv1 = 0.f, dw0 = 0.f, dw1 = 0.f;
+      if (!FIRST) {
+        du0 = st[O_DU + ty * FBW + tx];
+        dv0 = st[O_DV + ty * FBW + tx];
+        du1 = st[O_DU + (ty + RY) * FBW + tx];
+        dv1 = st[O_DV + (ty + RY) * FBW + tx];
+        if (k + 1 < nz) { dw0 = st[O_DW + ty * OBW + tx]; dw1 = st[O_DW + (ty + RY) * OBW + tx]; }
+      }
+      const float pc0 = P0(ty + 1, tx + 1), pc1 = P0(ty + RY + 1, tx + 1);
+      float un0 = du0, vn0 = dv0, un1 = du1, vn1 = dv1;
+      if (hm) {
+        if (!su) {
+          un0 = du0 + (-dtf * ((pc0 - P0(ty + 1, tx)) * idx));
+          un1 = du1 + (-dtf * ((pc1 - P0(ty + RY + 1, tx)) * idx));
+        }
+        if (!sv) vn0 = dv0 + (-dtf * ((pc0 - P0(ty, tx + 1)) * idy));
+        vn1 = dv1 + (-dtf * ((pc1 - P0(ty + RY, tx + 1)) * idy));
+      }
+      if (o0) { s_du[pb][ty][tx] = un0; s_dv[pb][ty][tx] = vn0; }
+      if (o1) { s_du[pb][ty + RY][tx] = un1; s_dv[pb][ty + RY][tx] = vn1; }
+      if (role == 1) {  // the tile's east X face
+        float d = FIRST ? 0.f : st[O_DU + (hr - 1) * FBW + w];
+        if (hm && !hs) d = d + (-dtf * ((P0(hr, hc) - P0(hr, hc - 1)) * idx));
+        s_du[pb][hr - 1][w] = d;
+        // open east boundary: face nx belongs to no tile; its step value is base + increment
+        if (final_step && hs) {
+          const int o = gidx(g, hi, hj, k);
+          a.f_u[o] = __ldg(a.bu + o) + d;
+        }
+      } else if (role == 3) {  // the tile's north Y face
+        float d = FIRST ? 0.f : st[O_DV + h * FBW + hc - 1];
+        if (hm && !hs) d = d + (-dtf * ((P0(hr, hc) - P0(hr - 1, hc)) * idy));
+        s_dv[pb][h][hc - 1] = d;
+        if (final_step && hs) {
+          const int o = gidx(g, hi, hj, k);
+          a.f_v[o] = __ldg(a.bv + o) + d;
+        }
+      }
+      const float rc0 = st[O_RHO + (ty + R0) * RW + tx + C0], rc1 = st[O_RHO + (ty + RY + R0) * RW + tx + C0];
+      float wn0 = dw0, wn1 = dw1;
+      if (k + 1 < nz) {
+        const float prl = s_pref[k], pru = s_pref[k + 1], rrl = s_rref[k], rru = s_rref[k + 1];
+        const float idzf = s_idzf[k + 1];
+        const float pn0 = P1(ty + 1, tx + 1), pn1 = P1(ty + RY + 1, tx + 1);
+        const float rn0 = stn[O_RHO + (ty + R0) * RW + tx + C0], rn1 = stn[O_RHO + (ty + RY + R0) * RW + tx + C0];
+        wn0 = dw0 + dtf * (-((pn0 - pru) - (pc0 - prl)) * idzf - a.gravity * (0.5f * ((rc0 - rrl) + (rn0 - rru))));
+        wn1 = dw1 + dtf * (-((pn1 - pru) - (pc1 - prl)) * idzf - a.gravity * (0.5f * ((rc1 - rrl) + (rn1 - rru))));
+      }
+      __syncthreads();  // publishes s_p(k+1), s_du(k), s_dv(k); the slot of plane k-1 is free
+      if (s_abort[pb]) return true;
+      if (tid == ISSUER) {
+        if (acc_mode && k > 0) {  // level sums of plane k-1 (warp totals published above)
+          long long sa = 0, sb = 0;
+          for (int q = 0; q < NW; ++q) { sa += s_red[pb ^ 1][q][0]; sb += s_red[pb ^ 1][q][1]; }
+          acc_add(a.acc_a + k - 1, sa);
+          if (acc_mode == 1) acc_add(a.acc_b + k - 1, sb);
+        }
+        if (k + AHEAD < nz) { issue(k + AHEAD); issued = k + AHEAD; }
+      }
+      // ---- K15 density of plane k, K10 rho*theta, stores
+      const float idzc = s_idzc[k];
+      FxAcc sa, sb;
+      if (o0) {
+        float rn = rc0;
+        if (dn) {
+          const float div = (s_du[pb][ty][tx + 1] - un0) * idx + (s_dv[pb][ty + 1][tx] - vn0) * idy + (wn0 - dwc0) * idzc;
+          rn = fmaxf(1.0e-6f, rc0 - dtf * div);
+        }
+        const float rt = rn * st[O_TH + (ty + R0) * RW + tx + C0];
+        if (final_step) {
+          put(a.f_rho, g, kCell, gi, gj0, k, rn);
+          put(a.f_rt, g, kCell, gi, gj0, k, rt);
+          put(a.f_u, g, kFaceX, gi, gj0, k, st[O_BU + ty * OBW + tx] + un0);
+          put(a.f_v, g, kFaceY, gi, gj0, k, st[O_BV + ty * OBW + tx] + vn0);
+          if (k == 0) put(a.f_w, g, kFaceZ, gi, gj0, 0, bwz0);
+          put(a.f_w, g, kFaceZ, gi, gj0, k + 1, st[O_BW + ty * OBW + tx] + wn0);
+        } else {
+          put(a.rho_out, g, kCell, gi, gj0, k, rn);
+          put(a.du_out, g, kFaceX, gi, gj0, k, un0);
+          put(a.dv_out, g, kFaceY, gi, gj0, k, vn0);
+          if (k + 1 < nz) put(a.dw_out, g, kFaceZ, gi, gj0, k + 1, wn0);
+        }
+        if (acc_mode == 1) {
+          const float pv = eos_pprime_ref(rn, rt, s_binv[k], s_bpr[k]);
+          sa.add(rn, kFxRho);
+          sb.add(pv, kFxP);
+          put(a.p_out, g, kCell, gi, gj0, k, pv);
+        }
+        else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
+      }
+      if (o1) {
+        float rn = rc1;
+        if (dn) {
+          const float div = (s_du[pb][ty + RY][tx + 1] - un1) * idx + (s_dv[pb][ty + RY + 1][tx] - vn1) * idy +
+                            (wn1 - dwc1) * idzc;
+          rn = fmaxf(1.0e-6f, rc1 - dtf * div);
+        }
+        const float rt = rn * st[O_TH + (ty + RY + R0) * RW + tx + C0];
+        if (final_step) {
+          put(a.f_rho, g, kCell, gi, gj1, k, rn);
+          put(a.f_rt, g, kCell, gi, gj1, k, rt);
+          put(a.f_u, g, kFaceX, gi, gj1, k, st[O_BU + (ty + RY) * OBW + tx] + un1);
+          put(a.f_v, g, kFaceY, gi, gj1, k, st[O_BV + (ty + RY) * OBW + tx] + vn1);
+          if (k == 0) put(a.f_w, g, kFaceZ, gi, gj1, 0, bwz1);
+          put(a.f_w, g, kFaceZ, gi, gj1, k + 1, st[O_BW + (ty + RY) * OBW + tx] + wn1);
+        } else {
+          put(a.rho_out, g, kCell, gi, gj1, k, rn);
+          put(a.du_out, g, kFaceX, gi, gj1, k, un1);
+          put(a.dv_out, g, kFaceY, gi, gj1, k, vn1);
+          if (k + 1 < nz) put(a.dw_out, g, kFaceZ, gi, gj1, k + 1, wn1);
+        }
+        if (acc_mode == 1) {
+          const float pv = eos_pprime_ref(rn, rt, s_binv[k], s_bpr[k]);
+          sa.add(rn, kFxRho);
+          sb.add(pv, kFxP);
+          put(a.p_out, g, kCell, gi, gj1, k, pv);
+        }
+        else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
+      }
+      if (acc_mode) {
+        const long long ta = sa.warp_total(), tb = sb.warp_total();
+        if (tx == 0) { s_red[pb][ty][0] = ta; s_red[pb][ty][1] = tb; }
+      }
+      dwc0 = wn0;
+      dwc1 = wn1;
     }
-    // ---- faces of plane k: K12/K13 horizontal momenta, K14 vertical momentum at face k+1
-    // p'(r, c) of plane k (P0) and k+1 (P1) in s_p coordinates (row 0 = j0-1, column
-    // 0 = i0-1): loaded with the tiles, or derived above in a first substep
-    auto P0 = [&](int r, int c) { return PIN ? st[O_P + r * CBW + c + 3] : s_p[pb][r][c]; };
-    auto P1 = [&](int r, int c) { return PIN ? stn[O_P + r * CBW + c + 3] : s_p[pb ^ 1][r][c]; };
-    float du0 = 0.f, dv0 = 0.f, du1 = 0.f, dv1 = 0.f, dw0 = 0.f, dw1 = 0.f;
-    if (!FIRST) {
-      du0 = st[O_DU + ty * FBW + tx];
-      dv0 = st[O_DV + ty * FBW + tx];
-      du1 = st[O_DU + (ty + RY) * FBW + tx];
-      dv1 = st[O_DV + (ty + RY) * FBW + tx];
-      if (k + 1 < nz) { dw0 = st[O_DW + ty * OBW + tx]; dw1 = st[O_DW + (ty + RY) * OBW + tx]; }
-    }
-    const float pc0 = P0(ty + 1, tx + 1), pc1 = P0(ty + RY + 1, tx + 1);
-    float un0 = du0, vn0 = dv0, un1 = du1, vn1 = dv1;
-    if (hm) {
-      if (!skip_u) {
-        un0 = du0 + (-dtf * ((pc0 - P0(ty + 1, tx)) * idx));
-        un1 = du1 + (-dtf * ((pc1 - P0(ty + RY + 1, tx)) * idx));
-      }
-      if (!skip_v0) vn0 = dv0 + (-dtf * ((pc0 - P0(ty, tx + 1)) * idy));
-      vn1 = dv1 + (-dtf * ((pc1 - P0(ty + RY, tx + 1)) * idy));
-    }
-    if (own0) { s_du[pb][ty][tx] = un0; s_dv[pb][ty][tx] = vn0; }
-    if (own1) { s_du[pb][ty + RY][tx] = un1; s_dv[pb][ty + RY][tx] = vn1; }
-    if (role == 1) {  // the tile's east X face
-      float d = FIRST ? 0.f : st[O_DU + (hr - 1) * FBW + w];
-      if (hm && !h_skip) d = d + (-dtf * ((P0(hr, hc) - P0(hr, hc - 1)) * idx));
-      s_du[pb][hr - 1][w] = d;
-      // open east boundary: face nx belongs to no tile; its step value is base + increment
-      if (final_step && h_skip) {
-        const int o = gidx(g, hi, hj, k);
-        a.f_u[o] = __ldg(a.bu + o) + d;
-      }
-    } else if (role == 3) {  // the tile's north Y face
-      float d = FIRST ? 0.f : st[O_DV + h * FBW + hc - 1];
-      if (hm && !h_skip) d = d + (-dtf * ((P0(hr, hc) - P0(hr - 1, hc)) * idy));
-      s_dv[pb][h][hc - 1] = d;
-      if (final_step && h_skip) {
-        const int o = gidx(g, hi, hj, k);
-        a.f_v[o] = __ldg(a.bv + o) + d;
-      }
-    }
-    const float rc0 = st[O_RHO + (ty + R0) * RW + tx + C0], rc1 = st[O_RHO + (ty + RY + R0) * RW + tx + C0];
-    float wn0 = dw0, wn1 = dw1;
-    if (k + 1 < nz) {
-      const float prl = s_pref[k], pru = s_pref[k + 1], rrl = s_rref[k], rru = s_rref[k + 1];
-      const float idzf = s_idzf[k + 1];
-      const float pn0 = P1(ty + 1, tx + 1), pn1 = P1(ty + RY + 1, tx + 1);
-      const float rn0 = stn[O_RHO + (ty + R0) * RW + tx + C0], rn1 = stn[O_RHO + (ty + RY + R0) * RW + tx + C0];
-      wn0 = dw0 + dtf * (-((pn0 - pru) - (pc0 - prl)) * idzf - a.gravity * (0.5f * ((rc0 - rrl) + (rn0 - rru))));
-      wn1 = dw1 + dtf * (-((pn1 - pru) - (pc1 - prl)) * idzf - a.gravity * (0.5f * ((rc1 - rrl) + (rn1 - rru))));
-    }
-    __syncthreads();  // publishes s_p(k+1), s_du(k), s_dv(k); the slot of plane k-1 is free
-    if (s_abort[pb]) { aborted = true; break; }
-    if (tid == ISSUER) {
-      if (acc_mode && k > 0) {  // level sums of plane k-1 (warp totals published above)
-        long long sa = 0, sb = 0;
-        for (int q = 0; q < NW; ++q) { sa += s_red[pb ^ 1][q][0]; sb += s_red[pb ^ 1][q][1]; }
-        acc_add(a.acc_a + k - 1, sa);
-        if (acc_mode == 1) acc_add(a.acc_b + k - 1, sb);
-      }
-      if (k + AHEAD < nz) { issue(k + AHEAD); issued = k + AHEAD; }
-    }
-    // ---- K15 density of plane k, K10 rho*theta, stores
-    const float idzc = s_idzc[k];
-    FxAcc sa, sb;
-    if (own0) {
-      float rn = rc0;
-      if (dn) {
-        const float div = (s_du[pb][ty][tx + 1] - un0) * idx + (s_dv[pb][ty + 1][tx] - vn0) * idy + (wn0 - dwc0) * idzc;
-        rn = fmaxf(1.0e-6f, rc0 - dtf * div);
-      }
-      const float rt = rn * st[O_TH + (ty + R0) * RW + tx + C0];
-      if (final_step) {
-        store_tile(a.f_rho, g, kCell, gi, gj0, k, rn, edge);
-        store_tile(a.f_rt, g, kCell, gi, gj0, k, rt, edge);
-        store_tile(a.f_u, g, kFaceX, gi, gj0, k, st[O_BU + ty * OBW + tx] + un0, edge);
-        store_tile(a.f_v, g, kFaceY, gi, gj0, k, st[O_BV + ty * OBW + tx] + vn0, edge);
-        if (k == 0) store_tile(a.f_w, g, kFaceZ, gi, gj0, 0, bwz0, edge);
-        store_tile(a.f_w, g, kFaceZ, gi, gj0, k + 1, st[O_BW + ty * OBW + tx] + wn0, edge);
-      } else {
-        store_tile(a.rho_out, g, kCell, gi, gj0, k, rn, edge);
-        store_tile(a.du_out, g, kFaceX, gi, gj0, k, un0, edge);
-        store_tile(a.dv_out, g, kFaceY, gi, gj0, k, vn0, edge);
-        if (k + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj0, k + 1, wn0, edge);
-      }
-      if (acc_mode == 1) {
-        const float pv = eos_pprime_ref(rn, rt, s_binv[k], s_bpr[k]);
-        sa.add(rn, kFxRho);
-        sb.add(pv, kFxP);
-        store_tile(a.p_out, g, kCell, gi, gj0, k, pv, edge);
-      }
-      else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
-    }
-    if (own1) {
-      float rn = rc1;
-      if (dn) {
-        const float div = (s_du[pb][ty + RY][tx + 1] - un1) * idx + (s_dv[pb][ty + RY + 1][tx] - vn1) * idy +
-                          (wn1 - dwc1) * idzc;
-        rn = fmaxf(1.0e-6f, rc1 - dtf * div);
-      }
-      const float rt = rn * st[O_TH + (ty + RY + R0) * RW + tx + C0];
-      if (final_step) {
-        store_tile(a.f_rho, g, kCell, gi, gj1, k, rn, edge);
-        store_tile(a.f_rt, g, kCell, gi, gj1, k, rt, edge);
-        store_tile(a.f_u, g, kFaceX, gi, gj1, k, st[O_BU + (ty + RY) * OBW + tx] + un1, edge);
-        store_tile(a.f_v, g, kFaceY, gi, gj1, k, st[O_BV + (ty + RY) * OBW + tx] + vn1, edge);
-        if (k == 0) store_tile(a.f_w, g, kFaceZ, gi, gj1, 0, bwz1, edge);
-        store_tile(a.f_w, g, kFaceZ, gi, gj1, k + 1, st[O_BW + (ty + RY) * OBW + tx] + wn1, edge);
-      } else {
-        store_tile(a.rho_out, g, kCell, gi, gj1, k, rn, edge);
-        store_tile(a.du_out, g, kFaceX, gi, gj1, k, un1, edge);
-        store_tile(a.dv_out, g, kFaceY, gi, gj1, k, vn1, edge);
-        if (k + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj1, k + 1, wn1, edge);
-      }
-      if (acc_mode == 1) {
-        const float pv = eos_pprime_ref(rn, rt, s_binv[k], s_bpr[k]);
-        sa.add(rn, kFxRho);
-        sb.add(pv, kFxP);
-        store_tile(a.p_out, g, kCell, gi, gj1, k, pv, edge);
-      }
-      else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
-    }
-    if (acc_mode) {
-      const long long ta = sa.warp_total(), tb = sb.warp_total();
-      if (tx == 0) { s_red[pb][ty][0] = ta; s_red[pb][ty][1] = tb; }
-    }
-    dwc0 = wn0;
-    dwc1 = wn1;
-  }
+    return false;
+  };
+  const bool aborted = interior ? plane_loop(std::true_type{}) : plane_loop(std::false_type{});
   if (aborted) {
     // drain the tiles still in flight (bounded) before the CTA's shared memory goes away
     if (tid == ISSUER)

@@ -17,6 +17,8 @@
 // wc are triple-buffered (a face at plane k reads planes k-1 and k while the next
 // plane is derived), theta and p double-buffered, so one barrier per plane suffices.
 // The blend partner q0 is read per thread (owned positions only, coalesced).
+#include <type_traits>
+
 #include "dycore.cuh"
 #include "tma.cuh"
 
@@ -184,8 +186,16 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     }
     return pc;
   };
-  auto column = [&](int k, int r, int gj, bool own, SlowCarry& cy, const SlowBlend& q0, FxAcc& ra, FxAcc& rb,
+  // store of an owned value: a plain store in interior tiles, else with the periodic mirrors
+  auto put = [&](bool in, float* f, const Geom& gg, int o, int i, int j, int kk, float v) {
+    if (in) f[gidx(gg, i, j, kk)] = v;
+    else store_tile(f, gg, o, i, j, kk, v, edge);
+  };
+  auto column = [&](auto tile_class, int k, int r, int gj, bool own_rt, SlowCarry& cy, const SlowBlend& q0,
+                    FxAcc& ra, FxAcc& rb,
                     const PlaneConst& kc) {
+    constexpr bool IN = decltype(tile_class)::value;  // an interior tile
+    const bool own = IN || own_rt;
     const float* sr = ring + (k % NSLOT) * slot;
     const float* sn = ring + ((k + 1) % NSLOT) * slot;
     const float* uc = der + D_UC + (k % 3) * DN;
@@ -235,14 +245,14 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
       }
       const float th1 = q1 / fmaxf(r1, 1.0e-6f);
       if (own) {
-        store_tile(a.o_rho, g, kCell, gi, gj, k, r1, edge);
-        store_tile(a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1, edge);
+        put(IN, a.o_rho, g, kCell, gi, gj, k, r1);
+        put(IN, a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1);
         if (a.acc_mode == 1) {
           // p' of the output: the level sums, and (stored) the first substep's input
           const float pv = eos_pprime_ref(r1, r1 * th1, s_binv[k], s_bpr[k]);
           ra.add(r1, kFxRho);
           rb.add(pv, kFxP);
-          if (a.p_out) store_tile(a.p_out, g, kCell, gi, gj, k, pv, edge);
+          if (a.p_out) put(IN, a.p_out, g, kCell, gi, gj, k, pv);
         } else if (a.acc_mode == 2) {
           ra.add(th1, kFxTheta);
         }
@@ -251,7 +261,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     // ---- X face: K17 (dry_momentum_flux.cu:79-156) + K21 (dry_pressure_gradient.cu:75-123)
     {
       float t_u = 0.0f;
-      if (!(gi == 0 && open_x)) {
+      if ((IN || !(gi == 0 && open_x))) {
         const float qw = U(sr, b - 1), qc = uf, qe = U(sr, b + 1);
         const float qs = U(sr, b - BW), qn = U(sr, b + BW);
         const float qb = k > 0 ? cy.uf : qc;
@@ -259,8 +269,8 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         const float flw = upwind(uc[d - 1], qw, qc);
         const float fle = upwind(uc[d], qc, qe);
         float fls = 0.0f, fln = 0.0f, flb = 0.0f, flt = 0.0f;
-        if (!(gj == 0 && open_y)) fls = upwind(0.5f * (vc[d - DW - 1] + vc[d - DW]), qs, qc);
-        if (!(gj + 1 == ny && open_y)) fln = upwind(0.5f * (vc[d - 1] + vc[d]), qc, qn);
+        if ((IN || !(gj == 0 && open_y))) fls = upwind(0.5f * (vc[d - DW - 1] + vc[d - DW]), qs, qc);
+        if ((IN || !(gj + 1 == ny && open_y))) fln = upwind(0.5f * (vc[d - 1] + vc[d]), qc, qn);
         if (k > 0) flb = upwind(0.5f * (wcm[d - 1] + wcm[d]), qb, qc);
         if (!top) flt = upwind(0.5f * (wc[d - 1] + wc[d]), qc, qt);
         t_u = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
@@ -269,19 +279,19 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
       }
       float u1 = fmaxf(-1.0e30f, uf + dt * t_u);
       if (blend) u1 = a.wa * q0.u + a.wb * u1;
-      if (own) store_tile(a.o_u, g, kFaceX, gi, gj, k, u1, edge);
+      if (own) put(IN, a.o_u, g, kFaceX, gi, gj, k, u1);
     }
     // ---- Y face: K18 (dry_momentum_flux.cu:158-235) + K22 (dry_pressure_gradient.cu:125-173)
     {
       float t_v = 0.0f;
-      if (!(gj == 0 && open_y)) {
+      if ((IN || !(gj == 0 && open_y))) {
         const float qw = V(sr, b - 1), qc = vf, qe = V(sr, b + 1);
         const float qs = V(sr, b - BW), qn = V(sr, b + BW);
         const float qb = k > 0 ? cy.vf : qc;
         const float qt = top ? qc : vft;
         float flw = 0.0f, fle = 0.0f, flb = 0.0f, flt = 0.0f;
-        if (!(gi == 0 && open_x)) flw = upwind(0.5f * (uc[d - DW - 1] + uc[d - 1]), qw, qc);
-        if (!(gi + 1 == nx && open_x)) fle = upwind(0.5f * (uc[d - DW] + uc[d]), qc, qe);
+        if ((IN || !(gi == 0 && open_x))) flw = upwind(0.5f * (uc[d - DW - 1] + uc[d - 1]), qw, qc);
+        if ((IN || !(gi + 1 == nx && open_x))) fle = upwind(0.5f * (uc[d - DW] + uc[d]), qc, qe);
         const float fls = upwind(vc[d - DW], qs, qc);
         const float fln = upwind(vc[d], qc, qn);
         if (k > 0) flb = upwind(0.5f * (wcm[d - DW] + wcm[d]), qb, qc);
@@ -292,7 +302,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
       }
       float v1 = fmaxf(-1.0e30f, vf + dt * t_v);
       if (blend) v1 = a.wa * q0.v + a.wb * v1;
-      if (own) store_tile(a.o_v, g, kFaceY, gi, gj, k, v1, edge);
+      if (own) put(IN, a.o_v, g, kFaceY, gi, gj, k, v1);
     }
     // ---- Z face k: K19 (dry_momentum_flux.cu:237-312) + K3 buoyancy (dry_core.cu:146-187)
     {
@@ -302,10 +312,10 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         const float qs = W(sr, b - BW), qn = W(sr, b + BW);
         const float qb = cy.wf, qt = wft;
         float flw = 0.0f, fle = 0.0f, fls = 0.0f, fln = 0.0f;
-        if (!(gi == 0 && open_x)) flw = upwind(0.5f * (ucm[d - 1] + uc[d - 1]), qw, qc);
-        if (!(gi + 1 == nx && open_x)) fle = upwind(0.5f * (ucm[d] + uc[d]), qc, qe);
-        if (!(gj == 0 && open_y)) fls = upwind(0.5f * (vcm[d - DW] + vc[d - DW]), qs, qc);
-        if (!(gj + 1 == ny && open_y)) fln = upwind(0.5f * (vcm[d] + vc[d]), qc, qn);
+        if ((IN || !(gi == 0 && open_x))) flw = upwind(0.5f * (ucm[d - 1] + uc[d - 1]), qw, qc);
+        if ((IN || !(gi + 1 == nx && open_x))) fle = upwind(0.5f * (ucm[d] + uc[d]), qc, qe);
+        if ((IN || !(gj == 0 && open_y))) fls = upwind(0.5f * (vcm[d - DW] + vc[d - DW]), qs, qc);
+        if ((IN || !(gj + 1 == ny && open_y))) fln = upwind(0.5f * (vcm[d] + vc[d]), qc, qn);
         const float flb = upwind(wcm[d], qb, qc);
         const float flt = upwind(wc[d], qc, qt);
         const float idzf = kc.idzf;
@@ -320,11 +330,11 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
       float w1 = fmaxf(-1.0e30f, wf + dt * t_w);
       if (blend) w1 = a.wa * q0.w + a.wb * w1;
       if (own) {
-        store_tile(a.o_w, g, kFaceZ, gi, gj, k, w1, edge);
+        put(IN, a.o_w, g, kFaceZ, gi, gj, k, w1);
         if (top) {  // top face: zero tendency
           float wt = fmaxf(-1.0e30f, wft);
           if (blend) wt = a.wa * __ldg(a.w0 + gidx(g, gi, gj, nz)) + a.wb * wt;
-          store_tile(a.o_w, g, kFaceZ, gi, gj, nz, wt, edge);
+          put(IN, a.o_w, g, kFaceZ, gi, gj, nz, wt);
         }
       }
     }
@@ -335,70 +345,78 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     cy.wf = wf;
   };
 
-  bool aborted = false;
-  for (int k = 0; k < nz; ++k) {
-    const int pb = k & 1;
-    const PlaneConst kc = plane_const(k);
-    // ---- derive plane k: theta, p', uc, vc, wc at the 34 x 18 positions
-    wait_plane(k + 1, k);
-    {
-      const float* sr = ring + (k % NSLOT) * slot;
-      const float* sn = ring + ((k + 1) % NSLOT) * slot;
-      float* uc = der + D_UC + (k % 3) * DN;
-      float* vc = der + D_VC + (k % 3) * DN;
-      float* wc = der + D_WC + (k % 3) * DN;
-      float* th = der + D_TH + pb * DN;
-      float* pp = der + D_P + pb * DN;
-      for (int q = tid; q < DN; q += NT) {
-        const int r = q / DW, c = q - r * DW;
-        const int b = r * BW + c + 3;
-        const float rho = sr[R_RHO + b], rt = RT(sr, b);
-        th[q] = theta_of(rho, rt);
-        pp[q] = eos_pprime_ref(rho, rt, s_binv[k], s_bpr[k]);
-        // cell-centred velocities: dry_momentum_flux.cu:36-73
-        const float rr = fmaxf(rho, 1.0e-6f);
-        uc[q] = 0.5f * (U(sr, b) + U(sr, b + 1)) / rr;
-        vc[q] = 0.5f * (V(sr, b) + V(sr, b + BW)) / rr;
-        wc[q] = 0.5f * (W(sr, b) + W(sn, b)) / rr;
+  // Interior tiles (full, away from every periodic edge ring and open side) run a copy
+  // of the plane loop compiled without the edge logic: plain stores, none of the
+  // open-boundary flux tests.  Both copies do the same arithmetic on the same values.
+  const bool interior = !edge && (g.per_x || (i0 > 0 && i0 + TX < nx)) && (g.per_y || (j0 > 0 && j0 + TY < ny));
+  auto plane_loop = [&](auto tile_class) -> bool {  // true when a bounded wait gave up
+    constexpr bool IN = decltype(tile_class)::value;
+    for (int k = 0; k < nz; ++k) {
+      const int pb = k & 1;
+      const PlaneConst kc = plane_const(k);
+      // ---- derive plane k: theta, p', uc, vc, wc at the 34 x 18 positions
+      wait_plane(k + 1, k);
+      {
+        const float* sr = ring + (k % NSLOT) * slot;
+        const float* sn = ring + ((k + 1) % NSLOT) * slot;
+        float* uc = der + D_UC + (k % 3) * DN;
+        float* vc = der + D_VC + (k % 3) * DN;
+        float* wc = der + D_WC + (k % 3) * DN;
+        float* th = der + D_TH + pb * DN;
+        float* pp = der + D_P + pb * DN;
+        for (int q = tid; q < DN; q += NT) {
+          const int r = q / DW, c = q - r * DW;
+          const int b = r * BW + c + 3;
+          const float rho = sr[R_RHO + b], rt = RT(sr, b);
+          th[q] = theta_of(rho, rt);
+          pp[q] = eos_pprime_ref(rho, rt, s_binv[k], s_bpr[k]);
+          // cell-centred velocities: dry_momentum_flux.cu:36-73
+          const float rr = fmaxf(rho, 1.0e-6f);
+          uc[q] = 0.5f * (U(sr, b) + U(sr, b + 1)) / rr;
+          vc[q] = 0.5f * (V(sr, b) + V(sr, b + BW)) / rr;
+          wc[q] = 0.5f * (W(sr, b) + W(sn, b)) / rr;
+        }
       }
-    }
-    const SlowBlend n0a = load_q0(gj0, own0, k + 1), n0b = load_q0(gj1, own1, k + 1);
-    __syncthreads();  // publishes plane k's derived values; slot (k-1) is free
-    if (s_abort[pb]) { aborted = true; break; }
-    if (tid == ISSUER) {
-      if (a.acc_mode && k > 0) {
-        long long sa = 0, sb = 0;
-        for (int q = 0; q < NW; ++q) { sa += s_red[pb ^ 1][q][0]; sb += s_red[pb ^ 1][q][1]; }
-        acc_add(a.acc_a + k - 1, sa);
-        if (a.acc_mode == 1) acc_add(a.acc_b + k - 1, sb);
+      const SlowBlend n0a = load_q0(gj0, own0, k + 1), n0b = load_q0(gj1, own1, k + 1);
+      __syncthreads();  // publishes plane k's derived values; slot (k-1) is free
+      if (s_abort[pb]) return true;
+      if (tid == ISSUER) {
+        if (a.acc_mode && k > 0) {
+          long long sa = 0, sb = 0;
+          for (int q = 0; q < NW; ++q) { sa += s_red[pb ^ 1][q][0]; sb += s_red[pb ^ 1][q][1]; }
+          acc_add(a.acc_a + k - 1, sa);
+          if (a.acc_mode == 1) acc_add(a.acc_b + k - 1, sb);
+        }
+        if (k + 2 <= nz) { issue(k + 2); issued = k + 2; }
       }
-      if (k + 2 <= nz) { issue(k + 2); issued = k + 2; }
+      // ---- cells and faces of plane k
+      FxAcc ra, rb;
+      column(tile_class, k, ty + 1, gj0, own0, ca, q0a, ra, rb, kc);
+      column(tile_class, k, ty + RY + 1, gj1, own1, cb, q0b, ra, rb, kc);
+      if (!IN && xf) {  // open east boundary: X face nx of row j0+tx
+        const float* sr = ring + (k % NSLOT) * slot;
+        const float uf = U(sr, (tx + 1) * BW + w + 4);
+        float u1 = fmaxf(-1.0e30f, uf + dt * 0.0f);
+        if (blend) u1 = a.wa * __ldg(a.u0 + gidx(g, nx, j0 + tx, k)) + a.wb * u1;
+        put(false, a.o_u, g, kFaceX, nx, j0 + tx, k, u1);
+      }
+      if (!IN && yf) {  // open north boundary: Y face ny of column i0+tx
+        const float* sr = ring + (k % NSLOT) * slot;
+        const float vf = V(sr, (h + 1) * BW + tx + 4);
+        float v1 = fmaxf(-1.0e30f, vf + dt * 0.0f);
+        if (blend) v1 = a.wa * __ldg(a.v0 + gidx(g, i0 + tx, ny, k)) + a.wb * v1;
+        put(false, a.o_v, g, kFaceY, i0 + tx, ny, k, v1);
+      }
+      if (a.acc_mode) {
+        const long long ta = ra.warp_total(), tb = rb.warp_total();
+        if (tx == 0) { s_red[pb][ty][0] = ta; s_red[pb][ty][1] = tb; }
+      }
+      q0a = n0a;
+      q0b = n0b;
     }
-    // ---- cells and faces of plane k
-    FxAcc ra, rb;
-    column(k, ty + 1, gj0, own0, ca, q0a, ra, rb, kc);
-    column(k, ty + RY + 1, gj1, own1, cb, q0b, ra, rb, kc);
-    if (xf) {  // open east boundary: X face nx of row j0+tx
-      const float* sr = ring + (k % NSLOT) * slot;
-      const float uf = U(sr, (tx + 1) * BW + w + 4);
-      float u1 = fmaxf(-1.0e30f, uf + dt * 0.0f);
-      if (blend) u1 = a.wa * __ldg(a.u0 + gidx(g, nx, j0 + tx, k)) + a.wb * u1;
-      store_tile(a.o_u, g, kFaceX, nx, j0 + tx, k, u1, edge);
-    }
-    if (yf) {  // open north boundary: Y face ny of column i0+tx
-      const float* sr = ring + (k % NSLOT) * slot;
-      const float vf = V(sr, (h + 1) * BW + tx + 4);
-      float v1 = fmaxf(-1.0e30f, vf + dt * 0.0f);
-      if (blend) v1 = a.wa * __ldg(a.v0 + gidx(g, i0 + tx, ny, k)) + a.wb * v1;
-      store_tile(a.o_v, g, kFaceY, i0 + tx, ny, k, v1, edge);
-    }
-    if (a.acc_mode) {
-      const long long ta = ra.warp_total(), tb = rb.warp_total();
-      if (tx == 0) { s_red[pb][ty][0] = ta; s_red[pb][ty][1] = tb; }
-    }
-    q0a = n0a;
-    q0b = n0b;
-  }
+    return false;
+  };
+  const bool aborted = interior ? plane_loop(std::true_type{}) : plane_loop(std::false_type{});
   if (aborted) {
     if (tid == ISSUER)
       for (int kk = waited + 1; kk <= issued; ++kk) mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1);

@@ -12,6 +12,8 @@
 //   w                            32 x 16 box: owned Z faces (plane nz: w only)
 // Per plane the mixing ratios of the tile and its ring (no corners) go to shared
 // memory; one barrier per plane publishes them.
+#include <type_traits>
+
 #include "physics.cuh"
 #include "tma.cuh"
 
@@ -140,7 +142,9 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
   load_q0(gj1, own1, 0, q0b);
 
   // one owned column of plane k
-  auto column = [&](int k, int r, int gj, bool own, float* qb, const float* q0v, float idz) {
+  auto column = [&](auto tile_class, int k, int r, int gj, bool own_rt, float* qb, const float* q0v, float idz) {
+    constexpr bool IN = decltype(tile_class)::value;  // interior tile: plain stores
+    const bool own = IN || own_rt;
     const float* st = ring + (k % NSLOT) * SLOT;
     const float* sn = ring + ((k + 1) % NSLOT) * SLOT;
     const int c = tx + 1;
@@ -165,29 +169,38 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
       const float div = (ge - gw) * idx + (gn - gs) * idy + (gt - gb) * idz;
       float out = fmaxf(0.0f, st[O_Q + t * 736 + r * CBW + c + 3] - a.dt * div);
       if (blend) out = a.wa * q0v[t] + a.wb * out;
-      if (own) store_tile(a.q_out[t], g, kCell, gi, gj, k, out, edge);
+      if (own) {
+        if (IN) a.q_out[t][gidx(g, gi, gj, k)] = out;
+        else store_tile(a.q_out[t], g, kCell, gi, gj, k, out, edge);
+      }
       qb[t] = qc;
     }
   };
 
-  bool aborted = false;
-  for (int k = 0; k < nz; ++k) {
-    // mixing ratios of plane k+1 (the own ones are this thread's, the ring published
-    // by the barrier below for the next plane)
-    const float idz = __ldg(a.idz_c + k);  // loaded ahead of the mixing-ratio work
-    float n0a[NTR], n0b[NTR];
-    load_q0(gj0, own0, k + 1, n0a);
-    load_q0(gj1, own1, k + 1, n0b);
-    wait_plane(k + 1, k);
-    if (k + 1 < nz) mix(k + 1);
-    column(k, ty + 1, gj0, own0, qb0, q0a, idz);
-    column(k, ty + RY + 1, gj1, own1, qb1, q0b, idz);
-#pragma unroll
-    for (int t = 0; t < NTR; ++t) { q0a[t] = n0a[t]; q0b[t] = n0b[t]; }
-    __syncthreads();  // publishes plane k+1's ring; slot k is free
-    if (s_abort[k & 1]) { aborted = true; break; }
-    if (tid == ISSUER && k + 3 <= nz) { issue(k + 3); issued = k + 3; }
-  }
+  // Interior tiles (full, away from every periodic edge ring) run a copy of the plane
+  // loop with plain stores instead of the periodic mirror stores; the arithmetic is the same.
+  const bool interior = !edge && i0 + TX <= nx && j0 + TY <= ny;
+  auto plane_loop = [&](auto tile_class) -> bool {  // true when a bounded wait gave up
+    for (int k = 0; k < nz; ++k) {
+      // mixing ratios of plane k+1 (the own ones are this thread's, the ring published
+      // by the barrier below for the next plane)
+      const float idz = __ldg(a.idz_c + k);  // loaded ahead of the mixing-ratio work
+      float n0a[NTR], n0b[NTR];
+      load_q0(gj0, own0, k + 1, n0a);
+      load_q0(gj1, own1, k + 1, n0b);
+      wait_plane(k + 1, k);
+      if (k + 1 < nz) mix(k + 1);
+      column(tile_class, k, ty + 1, gj0, own0, qb0, q0a, idz);
+      column(tile_class, k, ty + RY + 1, gj1, own1, qb1, q0b, idz);
+  #pragma unroll
+      for (int t = 0; t < NTR; ++t) { q0a[t] = n0a[t]; q0b[t] = n0b[t]; }
+      __syncthreads();  // publishes plane k+1's ring; slot k is free
+      if (s_abort[k & 1]) return true;
+      if (tid == ISSUER && k + 3 <= nz) { issue(k + 3); issued = k + 3; }
+    }
+    return false;
+  };
+  const bool aborted = interior ? plane_loop(std::true_type{}) : plane_loop(std::false_type{});
   if (aborted && tid == ISSUER)
     for (int kk = waited + 1; kk <= issued; ++kk) mbar_wait(&s_bar[kk % NSLOT], (kk / NSLOT) & 1);
 }

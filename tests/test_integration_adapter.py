@@ -1,8 +1,7 @@
-"""The integration guide's listings compile: the C++ adapter it gives gwm-next
-maintainers against the reference's own headers (dry_core.hpp's DryState,
-SubdomainDescriptor, GridMetrics and DryStepperConfig) and this library's C-ABI header
-(skipped where the reference tree is absent), and its C call listings against the C-ABI
-header alone."""
+"""The drop-in adapter and the integration guide's listings compile: the adapter source
+(gpu-wm-next_b200/adapter/gwm_b200_adapter.cpp) against the reference's own headers and
+this library's C-ABI header (skipped where the reference tree is absent), and the guide's
+C call listings against the C-ABI header alone."""
 
 import os
 import re
@@ -13,25 +12,24 @@ import tempfile
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-GUIDE = "INTEGRATION.md"  # the integration guide at the repository root
+GUIDE = os.path.join(ROOT, "INTEGRATION.md")
+ADAPTER = os.path.join(ROOT, "gpu-wm-next_b200", "adapter", "gwm_b200_adapter.cpp")
 
 
-def test_documented_adapter_compiles_against_reference_headers():
+def test_adapter_compiles_against_reference_headers():
     if shutil.which("nvcc") is None:
         pytest.skip("nvcc not available")
-    text = open(os.path.join(ROOT, GUIDE), encoding="utf-8").read()
-    m = re.search(r"```cpp\n(// gwm_b200_adapter\.cpp.*?)```", text, re.S)
-    assert m, "adapter listing not found in the integration guide"
-    with tempfile.TemporaryDirectory() as tmp:
-        src = os.path.join(tmp, "gwm_b200_adapter.cpp")
-        with open(src, "w") as f:
-            f.write(m.group(1))
-        r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "adapter-check", f"SRC={src}"],
-                           capture_output=True, text=True, timeout=600)
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "adapter-check", f"SRC={ADAPTER}"],
+                       capture_output=True, text=True, timeout=600)
     out = r.stdout + r.stderr
     if "reference tree absent" in out:
         pytest.skip("reference tree absent")
     assert r.returncode == 0 and "adapter-ok" in out, out[-2000:]
+
+
+def test_guide_names_the_adapter_source():
+    text = open(GUIDE, encoding="utf-8").read()
+    assert "gpu-wm-next_b200/adapter/gwm_b200_adapter.cpp" in text
 
 
 SNIPPET_PARAMS = {
@@ -49,7 +47,7 @@ def test_documented_abi_calls_compile_against_the_header():
     # parameters are the listing's free names, compiled against include/gwm_b200.h
     if shutil.which("g++") is None:
         pytest.skip("g++ not available")
-    text = open(os.path.join(ROOT, GUIDE), encoding="utf-8").read()
+    text = open(GUIDE, encoding="utf-8").read()
     blocks = re.findall(r"```cpp\n(.*?)```", text, re.S)
     parts = ['#include "gwm_b200.h"', "static void check(int) {}"]
     found = 0
@@ -58,7 +56,7 @@ def test_documented_abi_calls_compile_against_the_header():
             if marker in block:
                 parts.append(f"void listing_{n}({params}) {{\n{block}\n}}")
                 found += 1
-    assert found == len(SNIPPET_PARAMS), "a C call listing of the integration guide is missing"
+    assert found == len(SNIPPET_PARAMS), "a C call listing of the guide is missing"
     with tempfile.TemporaryDirectory() as tmp:
         src = os.path.join(tmp, "listings.cpp")
         with open(src, "w") as f:
