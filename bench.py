@@ -217,6 +217,7 @@ def main():
                     help="slow-stage kernel (3 TMA-fed owned tile, 8/16 overlapped); implies --no-tune")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-member ensemble line")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-microphysics line")
+    ap.add_argument("--no-c2", action="store_true", help="skip the mountain-wave (512x512x80 terrain) line")
     ap.add_argument("--tracer-tile", type=int, default=None,
                     help="tracer-stage kernel (3 TMA-fed owned tile, 8/16 overlapped); implies --no-tune")
     args = ap.parse_args()
@@ -308,6 +309,9 @@ def main():
     ensemble = None
     if not args.no_ensemble:
         ensemble = ensemble_line(gwm, torch, stream, dist, world)
+    c2 = None
+    if not args.no_c2:
+        c2 = c2_line(gwm, torch, stream, dist, world)
 
     if rank == 0:
         peak, which = load_peaks()
@@ -333,6 +337,8 @@ def main():
             line["surrogate"] = surrogate
         if ensemble:
             line["ensemble"] = ensemble
+        if c2:
+            line["c2"] = c2
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
@@ -432,6 +438,70 @@ def surrogate_line(gwm, model, stream, torch, steps=10):
             "note": "two kernels: gating warps pack the active cells (quiet cells gated) into 128-row "
                     "tiles, tcgen05 BF16 inference of process fractions with TMEM accumulators, per-cell "
                     "plain fallback; then the plain fallout sweep"}
+
+
+# The mountain-wave configuration at full size: 512 x 512 x 80, dx = dy = 1 km, levels
+# stretched to 20 km, Agnesi hill, constant N = 0.01 1/s from 288 K, 10 m/s, Rayleigh layer
+# above 14 km, 6 acoustic substeps.  dt = 0.5 s: the configured 6 s exceeds the acoustic
+# CFL bound of the reference's slow step on these levels (c dt / dz = 0.95 at 0.5 s on the
+# 183 m bottom level).  Byte model: 322 FP32 accesses per cell and step (1288 B: the slow
+# stages 40 + 9 metric, 18 substeps of 15, 3 stage exits).
+C2_BYTES_PER_CELL = 1288
+
+
+def c2_grid_and_state(gwm, nx=512, ny=512, nz=80, stretch=0.6):
+    """Agnesi hill (400 m, 10 km half width), levels eta_k = (exp(a k / nz) - 1) / (exp(a) - 1)
+    to 20 km (183 m at the ground, 331 m at the top for a = 0.6 and 80 levels), constant-N
+    atmosphere from 288 K with a 10 m/s wind."""
+    eta = (np.exp(stretch * np.arange(nz + 1) / nz) - 1.0) / (np.exp(stretch) - 1.0)
+    terrain = gwm.build_terrain("agnesi", nx, ny, 1000.0, 1000.0, height=400.0, half_width_x=10000.0,
+                                half_width_y=10000.0)
+    g = gwm.GridSpec(nx, ny, nz, dx=1000.0, dy=1000.0, z_top=20000.0, terrain=terrain, eta_interfaces=eta)
+    p = gwm.CaseParams(theta_ref=288.0, p_surface=100000.0, u_background=10.0, brunt_vaisala=0.01)
+    s = gwm.build_case("stratified_mountain_wave", g, p)
+    s["u"][:, :, -1] = s["u"][:, :, 0]
+    return g, s
+
+
+def c2_line(gwm, torch, stream, dist, world, steps=10, warmup=3):
+    """The mountain-wave configuration: device-timed throughput and its roofline on the
+    1288 B/cell model (terrain kernels on overlapped tiles, tiles chosen by timing)."""
+    g, s = c2_grid_and_state(gwm)
+    uref = s["u"].astype(np.float64).mean(axis=(1, 2))
+    spec = gwm.MemberSpec(step=gwm.StepConfig(dt=0.5, fast_substeps=6))
+    cells = g.nx * g.ny * g.nz
+    with gwm.Model(g, spec) as m:
+        m.set_stream(stream.cuda_stream)
+        m.upload(s)
+        m.set_damping(14000.0, 0.05, u_ref=uref)
+        with torch.cuda.stream(stream):
+            tiles = m.autotune(1)
+        m.upload(s)
+        m.use_graph(True)
+        with torch.cuda.stream(stream):
+            m.step(warmup)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        m.step(steps)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(t0.elapsed_time(t1), torch, dist, "cuda")
+        finite = all(np.isfinite(v) for v in m.budgets().values())
+        with torch.cuda.stream(stream):
+            m.profile(True)
+            m.step(1)
+            rep = m.profile_report()
+            m.profile(False)
+    peak, which = load_peaks()
+    achieved = C2_BYTES_PER_CELL * cells * steps / (ms * 1e-3) / 1e9
+    return {"workload": "dry mountain wave, 512x512x80 Agnesi hill, stretched levels to 20 km, N = 0.01, "
+                        "Rayleigh layer above 14 km", "dt_s": 0.5, "fast_substeps": 6, "steps": steps,
+            "ms_per_step": ms / steps, "value": job_throughput(cells, steps, world, ms), "unit": "cell-updates/s",
+            "tile_rows": tiles, "state_finite": finite,
+            "kernel_avg_ms": {k: round(v["avg_ms"], 4) for k, v in rep.items()},
+            "roofline": {"bound": "hbm", "bytes_per_cell_step": C2_BYTES_PER_CELL, "achieved": achieved,
+                         "unit": "GB/s", "peak": peak, "peak_source": which, "frac": achieved / peak}}
 
 
 def ensemble_line(gwm, torch, stream, dist, world, n=64, steps=3, warmup=3):

@@ -31,7 +31,7 @@ DRIVER_PATH = os.path.join(_HERE, "_build", "gwm_b200_idealized_driver")
 _DRIVER_SRC = os.path.join(_HERE, "drivers", "gwm_b200_idealized_driver.cpp")
 _SOURCES = ["capi.cu", "dycore.cu", "fast_tma.cu", "slow_tma.cu", "tracer_tma.cu", "physics.cu", "halo.cu",
             "surrogate.cu", "surrogate_rain.cu", "scalar.cu", "cases.cpp"]
-_HEADERS = ["common.cuh", "dycore.cuh", "physics.cuh", "halo.cuh", "tma.cuh", "rain_cell.cuh", "surrogate.cuh", "surrogate_rain.cuh"]
+_HEADERS = ["common.cuh", "stencil.cuh", "dycore.cuh", "physics.cuh", "halo.cuh", "tma.cuh", "rain_cell.cuh", "surrogate.cuh", "surrogate_rain.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 

@@ -11,6 +11,7 @@
 // that the reference's halo exchange would copy into halo slots are written
 // there by the same store (store_mirrored), so no separate halo pass runs.
 #include "dycore.cuh"
+#include "stencil.cuh"
 
 namespace gwmb {
 namespace {
@@ -60,13 +61,13 @@ __device__ __forceinline__ SlowCol slow_derive(const SlowArgs& a, const SlowRaw&
   if (!valid) return c;
   if (kk < a.g.nz) {
     c.rho = r.rho;
-    c.rt = a.th_is_rt ? r.t : c.rho * r.t;
-    c.th = theta_of(c.rho, c.rt);
+    c.rt = a.th_is_rt ? r.t : fp::mul(c.rho, r.t);
+    c.th = fp::theta(c.rho, c.rt);
     c.p = TERRAIN ? eos_pressure(c.rho, c.rt) : eos_pprime(c.rho, c.rt, a.base, kk, a.g.nz);
-    c.uf = r.u + r.du;
-    c.vf = r.v + r.dv;
+    c.uf = fp::add(r.u, r.du);
+    c.vf = fp::add(r.v, r.dv);
   }
-  c.wf = r.w + r.dw;
+  c.wf = fp::add(r.w, r.dw);
   return c;
 }
 
@@ -160,9 +161,9 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
     // cell-centred velocities of plane k, halo included: dry_momentum_flux.cu:36-73
     {
       const float rr = fmaxf(cc.rho, 1.0e-6f);
-      s_uc[pb][ty][tx] = (tx + 1 < BX) ? 0.5f * (cc.uf + s_u[pb][ty][tx + 1]) / rr : 0.0f;
-      s_vc[pb][ty][tx] = (ty + 1 < SBY) ? 0.5f * (cc.vf + s_v[pb][ty + 1][tx]) / rr : 0.0f;
-      s_wc[pb][ty][tx] = 0.5f * (cc.wf + cn.wf) / rr;
+      s_uc[pb][ty][tx] = (tx + 1 < BX) ? fp::centred(cc.uf, s_u[pb][ty][tx + 1], rr) : 0.0f;
+      s_vc[pb][ty][tx] = (ty + 1 < SBY) ? fp::centred(cc.vf, s_v[pb][ty + 1][tx], rr) : 0.0f;
+      s_wc[pb][ty][tx] = fp::centred(cc.wf, cn.wf, rr);
     }
     __syncthreads();
 
@@ -174,37 +175,33 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
         const float fw = cc.uf, fe = s_u[pb][ty][tx + 1], fs = cc.vf, fn = s_v[pb][ty + 1][tx];
         const float fb = cc.wf, ft = cn.wf;
         const float idz = TERRAIN ? met3(a.idz_c, g, gi, gj, k) : __ldg(a.idz_c + k);
-        const float div = (fe - fw) * idx + (fn - fs) * idy + (ft - fb) * idz;
-        const float t_rho = -div;
+        const float t_rho = -fp::divergence(fe, fw, fn, fs, ft, fb, idx, idy, idz);
         const float tc = cc.th;
         const float tw = s_th[pb][ty][tx - 1], te = s_th[pb][ty][tx + 1];
         const float ts = s_th[pb][ty - 1][tx], tn = s_th[pb][ty + 1][tx];
         const float tb = (k > 0) ? cm.th : tc;
         const float tt = (k + 1 < nz) ? cn.th : tc;
-        const float gw = fw * (fw >= 0.0f ? tw : tc);
-        const float ge = fe * (fe >= 0.0f ? tc : te);
-        const float gs = fs * (fs >= 0.0f ? ts : tc);
-        const float gn = fn * (fn >= 0.0f ? tc : tn);
-        const float gb = fb * (fb >= 0.0f ? tb : tc);
-        const float gt = ft * (ft >= 0.0f ? tc : tt);
-        const float t_rt = -((ge - gw) * idx + (gn - gs) * idy + (gt - gb) * idz);
+        const float gw = fp::upwind(fw, tw, tc), ge = fp::upwind(fe, tc, te);
+        const float gs = fp::upwind(fs, ts, tc), gn = fp::upwind(fn, tc, tn);
+        const float gb = fp::upwind(fb, tb, tc), gt = fp::upwind(ft, tc, tt);
+        const float t_rt = -fp::divergence(ge, gw, gn, gs, gt, gb, idx, idy, idz);
         if (a.tend_only) {
           a.o_rho[o] = t_rho;
           a.o_th[o] = t_rt;
         } else {
           // K4 update (floor 1e-6) and K5 blend
-          float r1 = fmaxf(1.0e-6f, cc.rho + a.dt * t_rho);
-          float q1 = fmaxf(1.0e-6f, cc.rt + a.dt * t_rt);
+          float r1 = fp::update(cc.rho, a.dt, t_rho, 1.0e-6f);
+          float q1 = fp::update(cc.rt, a.dt, t_rt, 1.0e-6f);
           if (blend) {
-            r1 = a.wa * q0c.rho + a.wb * r1;
-            q1 = a.wa * q0c.rt + a.wb * q1;
+            r1 = fp::blend(a.wa, q0c.rho, a.wb, r1);
+            q1 = fp::blend(a.wa, q0c.rt, a.wb, q1);
           }
-          const float th1 = q1 / fmaxf(r1, 1.0e-6f);
+          const float th1 = fp::theta(r1, q1);
           store_tile(a.o_rho, g, kCell, gi, gj, k, r1, edge);
           store_tile(a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1, edge);
           if (a.acc_mode == 1) {
             red_a.add(r1, kFxRho);
-            red_b.add(eos_pprime(r1, r1 * th1, a.base, k, nz), kFxP);
+            red_b.add(eos_pprime(r1, fp::mul(r1, th1), a.base, k, nz), kFxP);
           } else if (a.acc_mode == 2) {
             red_a.add(th1, kFxTheta);
           }
@@ -218,31 +215,29 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
           const float qs = s_u[pb][ty - 1][tx], qn = s_u[pb][ty + 1][tx];
           const float qb = (k > 0) ? cm.uf : qc;
           const float qt = (k + 1 < nz) ? cn.uf : qc;
-          const float flw = upwind(s_uc[pb][ty][tx - 1], qw, qc);
-          const float fle = upwind(s_uc[pb][ty][tx], qc, qe);
+          const float flw = fp::upwind(s_uc[pb][ty][tx - 1], qw, qc);
+          const float fle = fp::upwind(s_uc[pb][ty][tx], qc, qe);
           float fls = 0.0f, fln = 0.0f, flb = 0.0f, flt = 0.0f;
-          if (!(gj == 0 && open_y)) fls = upwind(0.5f * (s_vc[pb][ty - 1][tx - 1] + s_vc[pb][ty - 1][tx]), qs, qc);
-          if (!(gj + 1 == ny && open_y)) fln = upwind(0.5f * (s_vc[pb][ty][tx - 1] + s_vc[pb][ty][tx]), qc, qn);
-          if (k > 0) flb = upwind(0.5f * (s_wc[pb ^ 1][ty][tx - 1] + s_wc[pb ^ 1][ty][tx]), qb, qc);
-          if (k + 1 < nz) flt = upwind(0.5f * (s_wc[pb][ty][tx - 1] + s_wc[pb][ty][tx]), qc, qt);
-          const float idz = TERRAIN ? 0.5f * (met3(a.idz_c, g, gi - 1, gj, k) + met3(a.idz_c, g, gi, gj, k))
+          if (!(gj == 0 && open_y)) fls = fp::upwind(fp::avg(s_vc[pb][ty - 1][tx - 1], s_vc[pb][ty - 1][tx]), qs, qc);
+          if (!(gj + 1 == ny && open_y)) fln = fp::upwind(fp::avg(s_vc[pb][ty][tx - 1], s_vc[pb][ty][tx]), qc, qn);
+          if (k > 0) flb = fp::upwind(fp::avg(s_wc[pb ^ 1][ty][tx - 1], s_wc[pb ^ 1][ty][tx]), qb, qc);
+          if (k + 1 < nz) flt = fp::upwind(fp::avg(s_wc[pb][ty][tx - 1], s_wc[pb][ty][tx]), qc, qt);
+          const float idz = TERRAIN ? fp::avg(met3(a.idz_c, g, gi - 1, gj, k), met3(a.idz_c, g, gi, gj, k))
                                     : __ldg(a.idz_c + k);
-          t_u = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
+          t_u = -fp::divergence(fle, flw, fln, fls, flt, flb, idx, idy, idz);
           const float pl = s_p[pb][ty][tx - 1], pr = cc.p;
-          if (TERRAIN) {
-            const float dzdx = (s_zc[pb][ty][tx] - s_zc[pb][ty][tx - 1]) * idx;
-            const float dpdz = 0.5f * (s_dz[pb][ty][tx - 1] + s_dz[pb][ty][tx]);
-            t_u += -((pr - pl) * idx - dzdx * dpdz);
-          } else {
-            t_u += -((pr - pl) * idx);
-          }
-          if (a.damp_c) t_u += -__ldg(a.damp_c + k) * (qc - __ldg(a.uref + k));
+          if (TERRAIN)
+            t_u = fp::add_pgf_terrain(t_u, pr, pl, s_zc[pb][ty][tx], s_zc[pb][ty][tx - 1], s_dz[pb][ty][tx - 1],
+                                      s_dz[pb][ty][tx], idx);
+          else
+            t_u = fp::add_pgf(t_u, pr, pl, idx);
+          if (a.damp_c) t_u = fp::add_damping(t_u, __ldg(a.damp_c + k), qc, __ldg(a.uref + k));
         }
         if (a.tend_only) {
           a.o_u[o] = t_u;
         } else {
-          float u1 = fmaxf(-1.0e30f, cc.uf + a.dt * t_u);
-          if (blend) u1 = a.wa * q0c.u + a.wb * u1;
+          float u1 = fp::update(cc.uf, a.dt, t_u, -1.0e30f);
+          if (blend) u1 = fp::blend(a.wa, q0c.u, a.wb, u1);
           store_tile(a.o_u, g, kFaceX, gi, gj, k, u1, edge);
         }
       }
@@ -255,30 +250,28 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
           const float qb = (k > 0) ? cm.vf : qc;
           const float qt = (k + 1 < nz) ? cn.vf : qc;
           float flw = 0.0f, fle = 0.0f, flb = 0.0f, flt = 0.0f;
-          if (!(gi == 0 && open_x)) flw = upwind(0.5f * (s_uc[pb][ty - 1][tx - 1] + s_uc[pb][ty][tx - 1]), qw, qc);
-          if (!(gi + 1 == nx && open_x)) fle = upwind(0.5f * (s_uc[pb][ty - 1][tx] + s_uc[pb][ty][tx]), qc, qe);
-          const float fls = upwind(s_vc[pb][ty - 1][tx], qs, qc);
-          const float fln = upwind(s_vc[pb][ty][tx], qc, qn);
-          if (k > 0) flb = upwind(0.5f * (s_wc[pb ^ 1][ty - 1][tx] + s_wc[pb ^ 1][ty][tx]), qb, qc);
-          if (k + 1 < nz) flt = upwind(0.5f * (s_wc[pb][ty - 1][tx] + s_wc[pb][ty][tx]), qc, qt);
-          const float idz = TERRAIN ? 0.5f * (met3(a.idz_c, g, gi, gj - 1, k) + met3(a.idz_c, g, gi, gj, k))
+          if (!(gi == 0 && open_x)) flw = fp::upwind(fp::avg(s_uc[pb][ty - 1][tx - 1], s_uc[pb][ty][tx - 1]), qw, qc);
+          if (!(gi + 1 == nx && open_x)) fle = fp::upwind(fp::avg(s_uc[pb][ty - 1][tx], s_uc[pb][ty][tx]), qc, qe);
+          const float fls = fp::upwind(s_vc[pb][ty - 1][tx], qs, qc);
+          const float fln = fp::upwind(s_vc[pb][ty][tx], qc, qn);
+          if (k > 0) flb = fp::upwind(fp::avg(s_wc[pb ^ 1][ty - 1][tx], s_wc[pb ^ 1][ty][tx]), qb, qc);
+          if (k + 1 < nz) flt = fp::upwind(fp::avg(s_wc[pb][ty - 1][tx], s_wc[pb][ty][tx]), qc, qt);
+          const float idz = TERRAIN ? fp::avg(met3(a.idz_c, g, gi, gj - 1, k), met3(a.idz_c, g, gi, gj, k))
                                     : __ldg(a.idz_c + k);
-          t_v = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
+          t_v = -fp::divergence(fle, flw, fln, fls, flt, flb, idx, idy, idz);
           const float ps = s_p[pb][ty - 1][tx], pn = cc.p;
-          if (TERRAIN) {
-            const float dzdy = (s_zc[pb][ty][tx] - s_zc[pb][ty - 1][tx]) * idy;
-            const float dpdz = 0.5f * (s_dz[pb][ty - 1][tx] + s_dz[pb][ty][tx]);
-            t_v += -((pn - ps) * idy - dzdy * dpdz);
-          } else {
-            t_v += -((pn - ps) * idy);
-          }
-          if (a.damp_c) t_v += -__ldg(a.damp_c + k) * (qc - __ldg(a.vref + k));
+          if (TERRAIN)
+            t_v = fp::add_pgf_terrain(t_v, pn, ps, s_zc[pb][ty][tx], s_zc[pb][ty - 1][tx], s_dz[pb][ty - 1][tx],
+                                      s_dz[pb][ty][tx], idy);
+          else
+            t_v = fp::add_pgf(t_v, pn, ps, idy);
+          if (a.damp_c) t_v = fp::add_damping(t_v, __ldg(a.damp_c + k), qc, __ldg(a.vref + k));
         }
         if (a.tend_only) {
           a.o_v[o] = t_v;
         } else {
-          float v1 = fmaxf(-1.0e30f, cc.vf + a.dt * t_v);
-          if (blend) v1 = a.wa * q0c.v + a.wb * v1;
+          float v1 = fp::update(cc.vf, a.dt, t_v, -1.0e30f);
+          if (blend) v1 = fp::blend(a.wa, q0c.v, a.wb, v1);
           store_tile(a.o_v, g, kFaceY, gi, gj, k, v1, edge);
         }
       }
@@ -290,32 +283,27 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
           const float qs = s_w[pb][ty - 1][tx], qn = s_w[pb][ty + 1][tx];
           const float qb = cm.wf, qt = cn.wf;
           float flw = 0.0f, fle = 0.0f, fls = 0.0f, fln = 0.0f;
-          if (!(gi == 0 && open_x)) flw = upwind(0.5f * (s_uc[pb ^ 1][ty][tx - 1] + s_uc[pb][ty][tx - 1]), qw, qc);
-          if (!(gi + 1 == nx && open_x)) fle = upwind(0.5f * (s_uc[pb ^ 1][ty][tx] + s_uc[pb][ty][tx]), qc, qe);
-          if (!(gj == 0 && open_y)) fls = upwind(0.5f * (s_vc[pb ^ 1][ty - 1][tx] + s_vc[pb][ty - 1][tx]), qs, qc);
-          if (!(gj + 1 == ny && open_y)) fln = upwind(0.5f * (s_vc[pb ^ 1][ty][tx] + s_vc[pb][ty][tx]), qc, qn);
-          const float flb = upwind(s_wc[pb ^ 1][ty][tx], qb, qc);
-          const float flt = upwind(s_wc[pb][ty][tx], qc, qt);
+          if (!(gi == 0 && open_x)) flw = fp::upwind(fp::avg(s_uc[pb ^ 1][ty][tx - 1], s_uc[pb][ty][tx - 1]), qw, qc);
+          if (!(gi + 1 == nx && open_x)) fle = fp::upwind(fp::avg(s_uc[pb ^ 1][ty][tx], s_uc[pb][ty][tx]), qc, qe);
+          if (!(gj == 0 && open_y)) fls = fp::upwind(fp::avg(s_vc[pb ^ 1][ty - 1][tx], s_vc[pb][ty - 1][tx]), qs, qc);
+          if (!(gj + 1 == ny && open_y)) fln = fp::upwind(fp::avg(s_vc[pb ^ 1][ty][tx], s_vc[pb][ty][tx]), qc, qn);
+          const float flb = fp::upwind(s_wc[pb ^ 1][ty][tx], qb, qc);
+          const float flt = fp::upwind(s_wc[pb][ty][tx], qc, qt);
           const float idz = TERRAIN ? met3(a.idz_f, g, gi, gj, k) : __ldg(a.idz_f + k);
-          t_w = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
-          const float tl = cm.th, tu = cc.th;
-          const float tf = 0.5f * (tl + tu);
-          const float trf = 0.5f * (s_thref[k - 1] + s_thref[k]);
-          const float rf = 0.5f * (cm.rho + cc.rho);
-          const float b = a.gravity * (tf - trf) / fmaxf(trf, 1.0e-6f);
-          t_w += rf * b;
-          if (a.damp_c) t_w += -__ldg(a.damp_f + k) * qc;
+          t_w = -fp::divergence(fle, flw, fln, fls, flt, flb, idx, idy, idz);
+          t_w = fp::add_buoyancy(t_w, cm.th, cc.th, s_thref[k - 1], s_thref[k], cm.rho, cc.rho, a.gravity);
+          if (a.damp_c) t_w = fp::add_damping(t_w, __ldg(a.damp_f + k), qc, 0.0f);
         }
         if (a.tend_only) {
           a.o_w[o] = t_w;
           if (k + 1 == nz) a.o_w[o + g.plane] = 0.0f;
         } else {
-          float w1 = fmaxf(-1.0e30f, cc.wf + a.dt * t_w);
-          if (blend) w1 = a.wa * q0c.w + a.wb * w1;
+          float w1 = fp::update(cc.wf, a.dt, t_w, -1.0e30f);
+          if (blend) w1 = fp::blend(a.wa, q0c.w, a.wb, w1);
           store_tile(a.o_w, g, kFaceZ, gi, gj, k, w1, edge);
           if (k + 1 == nz) {  // top face: zero tendency
             float wt = fmaxf(-1.0e30f, cn.wf);
-            if (blend) wt = a.wa * q0c.wtop + a.wb * wt;
+            if (blend) wt = fp::blend(a.wa, q0c.wtop, a.wb, wt);
             store_tile(a.o_w, g, kFaceZ, gi, gj, k + 1, wt, edge);
           }
         }
@@ -379,8 +367,8 @@ __device__ __forceinline__ FastCol fast_derive(const FastArgs& a, const FastRaw&
   if (!valid || kk >= a.g.nz) return c;
   c.rho = r.rho;
   c.th = r.th;
-  const float rt = c.rho * c.th;  // K10 rebuild_rho_theta_from_theta_kernel
-  c.thp = theta_of(c.rho, rt);
+  const float rt = fp::mul(c.rho, c.th);  // K10 rebuild_rho_theta_from_theta_kernel
+  c.thp = fp::theta(c.rho, rt);
   // K20: full pressure for the terrain column reference, perturbation otherwise
   c.p = TERRAIN ? eos_pressure(c.rho, rt) : eos_pprime(c.rho, rt, a.base, kk, a.g.nz);
   if (TERRAIN) {  // K11 build_column_hydrostatic_reference_kernel (dry_fast_modes.cu:108-158)
@@ -388,10 +376,10 @@ __device__ __forceinline__ FastCol fast_derive(const FastArgs& a, const FastRaw&
       c.pref = c.p;
       c.rref = eos_rho(c.pref, c.thp);
     } else {
-      float pn = fmaxf(1.0f, below.pref - a.gravity * below.rref * dzk);
+      float pn = fmaxf(1.0f, fp::fma(-fp::mul(a.gravity, below.rref), dzk, below.pref));
       for (int it = 0; it < 4; ++it) {
         const float rn = eos_rho(pn, c.thp);
-        pn = below.pref - a.gravity * 0.5f * (below.rref + rn) * dzk;
+        pn = fp::fma(-fp::mul(fp::mul(a.gravity, 0.5f), fp::add(below.rref, rn)), dzk, below.pref);
         pn = fmaxf(pn, 1.0f);
       }
       c.pref = pn;
@@ -497,30 +485,18 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
     float du_new = d0.du;
     if (do_u && a.hmom && !skip_u) {
       const float pl = s_p[pb][ty][tx - 1], pr = cc.p;
-      float x;
-      if (TERRAIN) {
-        const float dzdx = (s_zc[pb][ty][tx] - s_zc[pb][ty][tx - 1]) * idx;
-        const float dpdz = 0.5f * (s_dz[pb][ty][tx - 1] + s_dz[pb][ty][tx]);
-        x = (pr - pl) * idx - dzdx * dpdz;
-      } else {
-        x = (pr - pl) * idx;
-      }
-      du_new = d0.du + (-dtf * x);
+      du_new = TERRAIN ? fp::hmom_terrain(d0.du, pr, pl, s_zc[pb][ty][tx], s_zc[pb][ty][tx - 1], s_dz[pb][ty][tx - 1],
+                                          s_dz[pb][ty][tx], idx, dtf)
+                       : fp::hmom(d0.du, pr, pl, idx, dtf);
     }
     s_du[pb][ty][tx] = du_new;
     // K13: Y-face momentum (dry_fast_modes.cu:231-301)
     float dv_new = d0.dv;
     if (do_v && a.hmom && !skip_v) {
       const float ps = s_p[pb][ty - 1][tx], pn = cc.p;
-      float x;
-      if (TERRAIN) {
-        const float dzdy = (s_zc[pb][ty][tx] - s_zc[pb][ty - 1][tx]) * idy;
-        const float dpdz = 0.5f * (s_dz[pb][ty - 1][tx] + s_dz[pb][ty][tx]);
-        x = (pn - ps) * idy - dzdy * dpdz;
-      } else {
-        x = (pn - ps) * idy;
-      }
-      dv_new = d0.dv + (-dtf * x);
+      dv_new = TERRAIN ? fp::hmom_terrain(d0.dv, pn, ps, s_zc[pb][ty][tx], s_zc[pb][ty - 1][tx], s_dz[pb][ty - 1][tx],
+                                          s_dz[pb][ty][tx], idy, dtf)
+                       : fp::hmom(d0.dv, pn, ps, idy, dtf);
     }
     s_dv[pb][ty][tx] = dv_new;
     // K14: Z face k+1 (dry_fast_modes.cu:303-348), perturbations about the reference
@@ -528,10 +504,7 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
     if (own_c && k + 1 < nz) {
       const float prl = TERRAIN ? cc.pref : s_pref[k], pru = TERRAIN ? cn.pref : s_pref[k + 1];
       const float rrl = TERRAIN ? cc.rref : s_rref[k], rru = TERRAIN ? cn.rref : s_rref[k + 1];
-      const float ppl = cc.p - prl, ppu = cn.p - pru;
-      const float rpf = 0.5f * ((cc.rho - rrl) + (cn.rho - rru));
-      const float tend = -(ppu - ppl) * idzf - a.gravity * rpf;
-      dw_n = d0.dw1 + dtf * tend;
+      dw_n = fp::wmom(d0.dw1, cn.p, pru, cc.p, prl, cc.rho, rrl, cn.rho, rru, idzf, a.gravity, dtf);
     }
     __syncthreads();
 
@@ -540,16 +513,15 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
       // K15: density from the perturbation mass-flux divergence (dry_fast_modes.cu:350-394)
       float rho_new = cc.rho;
       if (a.dens) {
-        const float div = (s_du[pb][ty][tx + 1] - s_du[pb][ty][tx]) * idx +
-                          (s_dv[pb][ty + 1][tx] - s_dv[pb][ty][tx]) * idy + (dw_n - dw_c) * idzc;
-        rho_new = fmaxf(1.0e-6f, cc.rho - dtf * div);
+        rho_new = fp::density(cc.rho, s_du[pb][ty][tx + 1], s_du[pb][ty][tx], s_dv[pb][ty + 1][tx], s_dv[pb][ty][tx],
+                              dw_n, dw_c, idx, idy, idzc, dtf);
       }
-      const float rt_new = rho_new * cc.th;  // K10 on the state
+      const float rt_new = fp::mul(rho_new, cc.th);  // K10 on the state
       if (final_step) {
         store_mirrored(a.f_rho, g, kCell, gi, gj, k, rho_new);
         store_mirrored(a.f_rt, g, kCell, gi, gj, k, rt_new);
         if (k == 0) store_mirrored(a.f_w, g, kFaceZ, gi, gj, 0, bw0);
-        store_mirrored(a.f_w, g, kFaceZ, gi, gj, k + 1, bw1 + dw_n);
+        store_mirrored(a.f_w, g, kFaceZ, gi, gj, k + 1, fp::add(bw1, dw_n));
       } else {
         store_mirrored(a.rho_out, g, kCell, gi, gj, k, rho_new);
         if (k + 1 < nz) store_mirrored(a.dw_out, g, kFaceZ, gi, gj, k + 1, dw_n);
@@ -558,15 +530,15 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
         red_a.add(rho_new, kFxRho);
         red_b.add(eos_pprime(rho_new, rt_new, a.base, k, nz), kFxP);
       } else if (acc_mode == 2) {
-        red_a.add(theta_of(rho_new, rt_new), kFxTheta);
+        red_a.add(fp::theta(rho_new, rt_new), kFxTheta);
       }
     }
     if (own_u) {
-      if (final_step) store_mirrored(a.f_u, g, kFaceX, gi, gj, k, bu0 + du_new);
+      if (final_step) store_mirrored(a.f_u, g, kFaceX, gi, gj, k, fp::add(bu0, du_new));
       else store_mirrored(a.du_out, g, kFaceX, gi, gj, k, du_new);
     }
     if (own_v) {
-      if (final_step) store_mirrored(a.f_v, g, kFaceY, gi, gj, k, bv0 + dv_new);
+      if (final_step) store_mirrored(a.f_v, g, kFaceY, gi, gj, k, fp::add(bv0, dv_new));
       else store_mirrored(a.dv_out, g, kFaceY, gi, gj, k, dv_new);
     }
     if (acc_mode) {
@@ -651,7 +623,7 @@ __device__ __forceinline__ Cell derive(const FastArgs& a, float rho, float th, i
   Cell c;
   c.rho = rho;
   c.th = th;
-  c.p = eos_pprime(rho, rho * th, a.base, k, a.g.nz);  // K10 + K20
+  c.p = eos_pprime(rho, fp::mul(rho, th), a.base, k, a.g.nz);  // K10 + K20
   return c;
 }
 }  // namespace flat
@@ -728,7 +700,7 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
   // halo: p' of plane k and the edge-face increment of plane k
   float hp = 0.f, hd = 0.f;
   if (role >= 0) {
-    hp = eos_pprime(__ldg(a.rho_in + hb), __ldg(a.rho_in + hb) * __ldg(a.th + hb), a.base, 0, nz);
+    hp = eos_pprime(__ldg(a.rho_in + hb), fp::mul(__ldg(a.rho_in + hb), __ldg(a.th + hb)), a.base, 0, nz);
     if (!FIRST && role == 1) hd = __ldg(a.du_in + hb);
     if (!FIRST && role == 3) hd = __ldg(a.dv_in + hb);
   }
@@ -746,18 +718,17 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
     if (own0) {
       float rn = prho0;
       if (dn) {
-        const float div = (s_du[pbk][ty][tx + 1] - pun0) * idx + (s_dv[pbk][ty + 1][tx] - pvn0) * idy +
-                          (pwn0 - pwc0) * pidzc;
-        rn = fmaxf(1.0e-6f, prho0 - dtf * div);
+        rn = fp::density(prho0, s_du[pbk][ty][tx + 1], pun0, s_dv[pbk][ty + 1][tx], pvn0, pwn0, pwc0, idx, idy,
+                         pidzc, dtf);
       }
-      const float rt = rn * pth0;
+      const float rt = fp::mul(rn, pth0);
       if (final_step) {
         store_tile(a.f_rho, g, kCell, gi, gj0, kk, rn, edge);
         store_tile(a.f_rt, g, kCell, gi, gj0, kk, rt, edge);
-        store_tile(a.f_u, g, kFaceX, gi, gj0, kk, pbu0 + pun0, edge);
-        store_tile(a.f_v, g, kFaceY, gi, gj0, kk, pbv0 + pvn0, edge);
+        store_tile(a.f_u, g, kFaceX, gi, gj0, kk, fp::add(pbu0, pun0), edge);
+        store_tile(a.f_v, g, kFaceY, gi, gj0, kk, fp::add(pbv0, pvn0), edge);
         if (kk == 0) store_tile(a.f_w, g, kFaceZ, gi, gj0, 0, pbwz0, edge);
-        store_tile(a.f_w, g, kFaceZ, gi, gj0, kk + 1, pbw0 + pwn0, edge);
+        store_tile(a.f_w, g, kFaceZ, gi, gj0, kk + 1, fp::add(pbw0, pwn0), edge);
       } else {
         store_tile(a.rho_out, g, kCell, gi, gj0, kk, rn, edge);
         store_tile(a.du_out, g, kFaceX, gi, gj0, kk, pun0, edge);
@@ -765,23 +736,22 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
         if (kk + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj0, kk + 1, pwn0, edge);
       }
       if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime(rn, rt, a.base, kk, nz), kFxP); }
-      else if (acc_mode == 2) { sa.add(theta_of(rn, rt), kFxTheta); }
+      else if (acc_mode == 2) { sa.add(fp::theta(rn, rt), kFxTheta); }
     }
     if (own1) {
       float rn = prho1;
       if (dn) {
-        const float div = (s_du[pbk][ty + RY][tx + 1] - pun1) * idx + (s_dv[pbk][ty + RY + 1][tx] - pvn1) * idy +
-                          (pwn1 - pwc1) * pidzc;
-        rn = fmaxf(1.0e-6f, prho1 - dtf * div);
+        rn = fp::density(prho1, s_du[pbk][ty + RY][tx + 1], pun1, s_dv[pbk][ty + RY + 1][tx], pvn1, pwn1, pwc1, idx,
+                         idy, pidzc, dtf);
       }
-      const float rt = rn * pth1;
+      const float rt = fp::mul(rn, pth1);
       if (final_step) {
         store_tile(a.f_rho, g, kCell, gi, gj1, kk, rn, edge);
         store_tile(a.f_rt, g, kCell, gi, gj1, kk, rt, edge);
-        store_tile(a.f_u, g, kFaceX, gi, gj1, kk, pbu1 + pun1, edge);
-        store_tile(a.f_v, g, kFaceY, gi, gj1, kk, pbv1 + pvn1, edge);
+        store_tile(a.f_u, g, kFaceX, gi, gj1, kk, fp::add(pbu1, pun1), edge);
+        store_tile(a.f_v, g, kFaceY, gi, gj1, kk, fp::add(pbv1, pvn1), edge);
         if (kk == 0) store_tile(a.f_w, g, kFaceZ, gi, gj1, 0, pbwz1, edge);
-        store_tile(a.f_w, g, kFaceZ, gi, gj1, kk + 1, pbw1 + pwn1, edge);
+        store_tile(a.f_w, g, kFaceZ, gi, gj1, kk + 1, fp::add(pbw1, pwn1), edge);
       } else {
         store_tile(a.rho_out, g, kCell, gi, gj1, kk, rn, edge);
         store_tile(a.du_out, g, kFaceX, gi, gj1, kk, pun1, edge);
@@ -789,7 +759,7 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
         if (kk + 1 < nz) store_tile(a.dw_out, g, kFaceZ, gi, gj1, kk + 1, pwn1, edge);
       }
       if (acc_mode == 1) { sa.add(rn, kFxRho); sb.add(eos_pprime(rn, rt, a.base, kk, nz), kFxP); }
-      else if (acc_mode == 2) { sa.add(theta_of(rn, rt), kFxTheta); }
+      else if (acc_mode == 2) { sa.add(fp::theta(rn, rt), kFxTheta); }
     }
   };
 
@@ -852,31 +822,31 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
     float un0 = du0, vn0 = dv0, un1 = du1, vn1 = dv1;
     if (hm) {
       if (!skip_u) {
-        un0 = du0 + (-dtf * ((c0.p - s_p[pb][ty + 1][tx]) * idx));
-        un1 = du1 + (-dtf * ((c1.p - s_p[pb][ty + RY + 1][tx]) * idx));
+        un0 = fp::hmom(du0, c0.p, s_p[pb][ty + 1][tx], idx, dtf);
+        un1 = fp::hmom(du1, c1.p, s_p[pb][ty + RY + 1][tx], idx, dtf);
       }
-      if (!skip_v0) vn0 = dv0 + (-dtf * ((c0.p - s_p[pb][ty][tx + 1]) * idy));
-      vn1 = dv1 + (-dtf * ((c1.p - s_p[pb][ty + RY][tx + 1]) * idy));
+      if (!skip_v0) vn0 = fp::hmom(dv0, c0.p, s_p[pb][ty][tx + 1], idy, dtf);
+      vn1 = fp::hmom(dv1, c1.p, s_p[pb][ty + RY][tx + 1], idy, dtf);
     }
     if (own0) { s_du[pb][ty][tx] = un0; s_dv[pb][ty][tx] = vn0; }
     if (own1) { s_du[pb][ty + RY][tx] = un1; s_dv[pb][ty + RY][tx] = vn1; }
     if (role == 1) {  // tile's east X face
       float d = hd;
-      if (hm && !h_skip) d = hd + (-dtf * ((hp - s_p[pb][hr][hc - 1]) * idx));
+      if (hm && !h_skip) d = fp::hmom(hd, hp, s_p[pb][hr][hc - 1], idx, dtf);
       s_du[pb][hr - 1][hc - 1] = d;
       // open east boundary: face nx belongs to no tile; its step value is base + 0
-      if (final_step && h_skip) a.f_u[hb + k * P] = __ldg(a.bu + hb + k * P) + d;
+      if (final_step && h_skip) a.f_u[hb + k * P] = fp::add(__ldg(a.bu + hb + k * P), d);
     } else if (role == 3) {  // tile's north Y face
       float d = hd;
-      if (hm && !h_skip) d = hd + (-dtf * ((hp - s_p[pb][hr - 1][hc]) * idy));
+      if (hm && !h_skip) d = fp::hmom(hd, hp, s_p[pb][hr - 1][hc], idy, dtf);
       s_dv[pb][hr - 1][hc - 1] = d;
-      if (final_step && h_skip) a.f_v[hb + k * P] = __ldg(a.bv + hb + k * P) + d;
+      if (final_step && h_skip) a.f_v[hb + k * P] = fp::add(__ldg(a.bv + hb + k * P), d);
     }
     float wn0 = dw0, wn1 = dw1;
     if (k + 1 < nz) {
       const float prl = s_pref[k], pru = s_pref[k + 1], rrl = s_rref[k], rru = s_rref[k + 1];
-      wn0 = dw0 + dtf * (-((n0.p - pru) - (c0.p - prl)) * idzf - a.gravity * (0.5f * ((c0.rho - rrl) + (n0.rho - rru))));
-      wn1 = dw1 + dtf * (-((n1.p - pru) - (c1.p - prl)) * idzf - a.gravity * (0.5f * ((c1.rho - rrl) + (n1.rho - rru))));
+      wn0 = fp::wmom(dw0, n0.p, pru, c0.p, prl, c0.rho, rrl, n0.rho, rru, idzf, a.gravity, dtf);
+      wn1 = fp::wmom(dw1, n1.p, pru, c1.p, prl, c1.rho, rrl, n1.rho, rru, idzf, a.gravity, dtf);
     }
     // ---- hand plane k to the next iteration's density update, advance the pipeline
     pun0 = un0; pvn0 = vn0; pwn0 = wn0; pwc0 = dwc0; prho0 = c0.rho; pth0 = c0.th;
@@ -890,7 +860,7 @@ __global__ void __launch_bounds__(flat::NT, 2) k_fast_flat(const FastArgs a) {
     ra0 = nr0; ta0 = nt0; ra1 = nr1; ta1 = nt1;
     du0 = ndu0; dv0 = ndv0; dw0 = ndw0; du1 = ndu1; dv1 = ndv1; dw1 = ndw1;
     if (role >= 0 && k + 1 < nz) {
-      hp = eos_pprime(hrho, hrho * hth, a.base, k + 1, nz);
+      hp = eos_pprime(hrho, fp::mul(hrho, hth), a.base, k + 1, nz);
       hd = hdn;
     }
   }

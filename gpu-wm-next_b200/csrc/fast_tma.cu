@@ -25,6 +25,7 @@
 #include <type_traits>
 
 #include "dycore.cuh"
+#include "stencil.cuh"
 #include "tma.cuh"
 
 namespace gwmb {
@@ -197,7 +198,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
   // K10 + K20: pressure perturbation of plane kk at the owned cells and the halo ring
   auto cell_p = [&](const float* st, int r, int c, int kk) {
     const float rho = st[O_RHO + r * CBW + c + 3], th = st[O_TH + r * CBW + c + 3];
-    return eos_pprime_ref(rho, rho * th, s_binv[kk], s_bpr[kk]);
+    return eos_pprime_ref(rho, fp::mul(rho, th), s_binv[kk], s_bpr[kk]);
   };
   auto plane_p = [&](int kk) {
     const float* st = ring + (kk % NSLOT) * slot;
@@ -261,30 +262,30 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
       float un0 = du0, vn0 = dv0, un1 = du1, vn1 = dv1;
       if (hm) {
         if (!su) {
-          un0 = du0 + (-dtf * ((pc0 - P0(ty + 1, tx)) * idx));
-          un1 = du1 + (-dtf * ((pc1 - P0(ty + RY + 1, tx)) * idx));
+          un0 = fp::hmom(du0, pc0, P0(ty + 1, tx), idx, dtf);
+          un1 = fp::hmom(du1, pc1, P0(ty + RY + 1, tx), idx, dtf);
         }
-        if (!sv) vn0 = dv0 + (-dtf * ((pc0 - P0(ty, tx + 1)) * idy));
-        vn1 = dv1 + (-dtf * ((pc1 - P0(ty + RY, tx + 1)) * idy));
+        if (!sv) vn0 = fp::hmom(dv0, pc0, P0(ty, tx + 1), idy, dtf);
+        vn1 = fp::hmom(dv1, pc1, P0(ty + RY, tx + 1), idy, dtf);
       }
       if (o0) { s_du[pb][ty][tx] = un0; s_dv[pb][ty][tx] = vn0; }
       if (o1) { s_du[pb][ty + RY][tx] = un1; s_dv[pb][ty + RY][tx] = vn1; }
       if (role == 1) {  // the tile's east X face
         float d = FIRST ? 0.f : st[O_DU + (hr - 1) * FBW + w];
-        if (hm && !hs) d = d + (-dtf * ((P0(hr, hc) - P0(hr, hc - 1)) * idx));
+        if (hm && !hs) d = fp::hmom(d, P0(hr, hc), P0(hr, hc - 1), idx, dtf);
         s_du[pb][hr - 1][w] = d;
         // open east boundary: face nx belongs to no tile; its step value is base + increment
         if (final_step && hs) {
           const int o = gidx(g, hi, hj, k);
-          a.f_u[o] = __ldg(a.bu + o) + d;
+          a.f_u[o] = fp::add(__ldg(a.bu + o), d);
         }
       } else if (role == 3) {  // the tile's north Y face
         float d = FIRST ? 0.f : st[O_DV + h * FBW + hc - 1];
-        if (hm && !hs) d = d + (-dtf * ((P0(hr, hc) - P0(hr - 1, hc)) * idy));
+        if (hm && !hs) d = fp::hmom(d, P0(hr, hc), P0(hr - 1, hc), idy, dtf);
         s_dv[pb][h][hc - 1] = d;
         if (final_step && hs) {
           const int o = gidx(g, hi, hj, k);
-          a.f_v[o] = __ldg(a.bv + o) + d;
+          a.f_v[o] = fp::add(__ldg(a.bv + o), d);
         }
       }
       const float rc0 = st[O_RHO + (ty + R0) * RW + tx + C0], rc1 = st[O_RHO + (ty + RY + R0) * RW + tx + C0];
@@ -294,8 +295,8 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
         const float idzf = s_idzf[k + 1];
         const float pn0 = P1(ty + 1, tx + 1), pn1 = P1(ty + RY + 1, tx + 1);
         const float rn0 = stn[O_RHO + (ty + R0) * RW + tx + C0], rn1 = stn[O_RHO + (ty + RY + R0) * RW + tx + C0];
-        wn0 = dw0 + dtf * (-((pn0 - pru) - (pc0 - prl)) * idzf - a.gravity * (0.5f * ((rc0 - rrl) + (rn0 - rru))));
-        wn1 = dw1 + dtf * (-((pn1 - pru) - (pc1 - prl)) * idzf - a.gravity * (0.5f * ((rc1 - rrl) + (rn1 - rru))));
+        wn0 = fp::wmom(dw0, pn0, pru, pc0, prl, rc0, rrl, rn0, rru, idzf, a.gravity, dtf);
+        wn1 = fp::wmom(dw1, pn1, pru, pc1, prl, rc1, rrl, rn1, rru, idzf, a.gravity, dtf);
       }
       __syncthreads();  // publishes s_p(k+1), s_du(k), s_dv(k); the slot of plane k-1 is free
       if (s_abort[pb]) return true;
@@ -314,17 +315,16 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
       if (o0) {
         float rn = rc0;
         if (dn) {
-          const float div = (s_du[pb][ty][tx + 1] - un0) * idx + (s_dv[pb][ty + 1][tx] - vn0) * idy + (wn0 - dwc0) * idzc;
-          rn = fmaxf(1.0e-6f, rc0 - dtf * div);
+          rn = fp::density(rc0, s_du[pb][ty][tx + 1], un0, s_dv[pb][ty + 1][tx], vn0, wn0, dwc0, idx, idy, idzc, dtf);
         }
-        const float rt = rn * st[O_TH + (ty + R0) * RW + tx + C0];
+        const float rt = fp::mul(rn, st[O_TH + (ty + R0) * RW + tx + C0]);
         if (final_step) {
           put(a.f_rho, g, kCell, gi, gj0, k, rn);
           put(a.f_rt, g, kCell, gi, gj0, k, rt);
-          put(a.f_u, g, kFaceX, gi, gj0, k, st[O_BU + ty * OBW + tx] + un0);
-          put(a.f_v, g, kFaceY, gi, gj0, k, st[O_BV + ty * OBW + tx] + vn0);
+          put(a.f_u, g, kFaceX, gi, gj0, k, fp::add(st[O_BU + ty * OBW + tx], un0));
+          put(a.f_v, g, kFaceY, gi, gj0, k, fp::add(st[O_BV + ty * OBW + tx], vn0));
           if (k == 0) put(a.f_w, g, kFaceZ, gi, gj0, 0, bwz0);
-          put(a.f_w, g, kFaceZ, gi, gj0, k + 1, st[O_BW + ty * OBW + tx] + wn0);
+          put(a.f_w, g, kFaceZ, gi, gj0, k + 1, fp::add(st[O_BW + ty * OBW + tx], wn0));
         } else {
           put(a.rho_out, g, kCell, gi, gj0, k, rn);
           put(a.du_out, g, kFaceX, gi, gj0, k, un0);
@@ -337,23 +337,22 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
           sb.add(pv, kFxP);
           put(a.p_out, g, kCell, gi, gj0, k, pv);
         }
-        else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
+        else if (acc_mode == 2) sa.add(fp::theta(rn, rt), kFxTheta);
       }
       if (o1) {
         float rn = rc1;
         if (dn) {
-          const float div = (s_du[pb][ty + RY][tx + 1] - un1) * idx + (s_dv[pb][ty + RY + 1][tx] - vn1) * idy +
-                            (wn1 - dwc1) * idzc;
-          rn = fmaxf(1.0e-6f, rc1 - dtf * div);
+          rn = fp::density(rc1, s_du[pb][ty + RY][tx + 1], un1, s_dv[pb][ty + RY + 1][tx], vn1, wn1, dwc1, idx, idy,
+                           idzc, dtf);
         }
-        const float rt = rn * st[O_TH + (ty + RY + R0) * RW + tx + C0];
+        const float rt = fp::mul(rn, st[O_TH + (ty + RY + R0) * RW + tx + C0]);
         if (final_step) {
           put(a.f_rho, g, kCell, gi, gj1, k, rn);
           put(a.f_rt, g, kCell, gi, gj1, k, rt);
-          put(a.f_u, g, kFaceX, gi, gj1, k, st[O_BU + (ty + RY) * OBW + tx] + un1);
-          put(a.f_v, g, kFaceY, gi, gj1, k, st[O_BV + (ty + RY) * OBW + tx] + vn1);
+          put(a.f_u, g, kFaceX, gi, gj1, k, fp::add(st[O_BU + (ty + RY) * OBW + tx], un1));
+          put(a.f_v, g, kFaceY, gi, gj1, k, fp::add(st[O_BV + (ty + RY) * OBW + tx], vn1));
           if (k == 0) put(a.f_w, g, kFaceZ, gi, gj1, 0, bwz1);
-          put(a.f_w, g, kFaceZ, gi, gj1, k + 1, st[O_BW + (ty + RY) * OBW + tx] + wn1);
+          put(a.f_w, g, kFaceZ, gi, gj1, k + 1, fp::add(st[O_BW + (ty + RY) * OBW + tx], wn1));
         } else {
           put(a.rho_out, g, kCell, gi, gj1, k, rn);
           put(a.du_out, g, kFaceX, gi, gj1, k, un1);
@@ -366,7 +365,7 @@ __global__ void __launch_bounds__(ft::NT, 3) k_fast_tma(const FastArgs a, const 
           sb.add(pv, kFxP);
           put(a.p_out, g, kCell, gi, gj1, k, pv);
         }
-        else if (acc_mode == 2) sa.add(theta_of(rn, rt), kFxTheta);
+        else if (acc_mode == 2) sa.add(fp::theta(rn, rt), kFxTheta);
       }
       if (acc_mode) {
         const long long ta = sa.warp_total(), tb = sb.warp_total();

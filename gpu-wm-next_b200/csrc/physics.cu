@@ -2,6 +2,7 @@
 // three-tracer SSPRK3 stage and the warm-rain column kernel.
 #include "dycore.cuh"
 #include "physics.cuh"
+#include "stencil.cuh"
 #include "rain_cell.cuh"
 
 namespace gwmb {
@@ -88,15 +89,12 @@ __global__ void __launch_bounds__(BX * TBY) k_tracer_stage(const TracerArgs a) {
         const float qs = s_q[t][pb][ty - 1][tx], qn = s_q[t][pb][ty + 1][tx];
         const float qb = (k > 0) ? cm.q[t] : qc;
         const float qt = (k + 1 < nz) ? cn.q[t] : qc;
-        const float gw = fw * (fw >= 0.0f ? qw : qc);
-        const float ge = fe * (fe >= 0.0f ? qc : qe);
-        const float gs = fs * (fs >= 0.0f ? qs : qc);
-        const float gn = fn * (fn >= 0.0f ? qc : qn);
-        const float gb = fb * (fb >= 0.0f ? qb : qc);
-        const float gt = ft * (ft >= 0.0f ? qc : qt);
-        const float div = (ge - gw) * idx + (gn - gs) * idy + (gt - gb) * idz;
-        float out = fmaxf(0.0f, cc.rq[t] - a.dt * div);
-        if (blend) out = a.wa * q0v[t] + a.wb * out;
+        const float gw = fp::upwind(fw, qw, qc), ge = fp::upwind(fe, qc, qe);
+        const float gs = fp::upwind(fs, qs, qc), gn = fp::upwind(fn, qc, qn);
+        const float gb = fp::upwind(fb, qb, qc), gt = fp::upwind(ft, qc, qt);
+        const float div = fp::divergence(ge, gw, gn, gs, gt, gb, idx, idy, idz);
+        float out = fp::update(cc.rq[t], -a.dt, div, 0.0f);
+        if (blend) out = fp::blend(a.wa, q0v[t], a.wb, out);
         store_tile(a.q_out[t], g, kCell, gi, gj, k, out, edge);
       }
     }

@@ -20,6 +20,7 @@
 #include <type_traits>
 
 #include "dycore.cuh"
+#include "stencil.cuh"
 #include "tma.cuh"
 
 namespace gwmb {
@@ -141,12 +142,12 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     }
   };
   // raw accessors: box index of derived position (r, c) is r * BW + c + 3
-  auto U = [&](const float* sr, int b) { return INC ? sr[R_U + b] + sr[R_DU + b] : sr[R_U + b]; };
-  auto V = [&](const float* sr, int b) { return INC ? sr[R_V + b] + sr[R_DV + b] : sr[R_V + b]; };
-  auto W = [&](const float* sr, int b) { return INC ? sr[R_W + b] + sr[R_DW + b] : sr[R_W + b]; };
+  auto U = [&](const float* sr, int b) { return INC ? fp::add(sr[R_U + b], sr[R_DU + b]) : sr[R_U + b]; };
+  auto V = [&](const float* sr, int b) { return INC ? fp::add(sr[R_V + b], sr[R_DV + b]) : sr[R_V + b]; };
+  auto W = [&](const float* sr, int b) { return INC ? fp::add(sr[R_W + b], sr[R_DW + b]) : sr[R_W + b]; };
   auto RT = [&](const float* sr, int b) {
     const float t = sr[R_TH + b];
-    return a.th_is_rt ? t : sr[R_RHO + b] * t;
+    return a.th_is_rt ? t : fp::mul(sr[R_RHO + b], t);
   };
 
   // blend partner of plane kk at the thread's owned positions
@@ -219,7 +220,7 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     if (!top) {
       uft = U(sn, b);
       vft = V(sn, b);
-      tt = theta_of(sn[R_RHO + b], RT(sn, b));
+      tt = fp::theta(sn[R_RHO + b], RT(sn, b));
     }
     const float tb = k > 0 ? cy.th : tc;
     const float idz = kc.idz;
@@ -227,29 +228,25 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
     {
       const float fw = uf, fe = U(sr, b + 1), fs = vf, fn = V(sr, b + BW);
       const float fb = wf, ft = wft;
-      const float div = (fe - fw) * idx + (fn - fs) * idy + (ft - fb) * idz;
-      const float t_rho = -div;
+      const float t_rho = -fp::divergence(fe, fw, fn, fs, ft, fb, idx, idy, idz);
       const float tw = th[d - 1], te = th[d + 1], ts = th[d - DW], tn = th[d + DW];
-      const float gw = fw * (fw >= 0.0f ? tw : tc);
-      const float ge = fe * (fe >= 0.0f ? tc : te);
-      const float gs = fs * (fs >= 0.0f ? ts : tc);
-      const float gn = fn * (fn >= 0.0f ? tc : tn);
-      const float gb = fb * (fb >= 0.0f ? tb : tc);
-      const float gt = ft * (ft >= 0.0f ? tc : tt);
-      const float t_rt = -((ge - gw) * idx + (gn - gs) * idy + (gt - gb) * idz);
-      float r1 = fmaxf(1.0e-6f, rho + dt * t_rho);
-      float q1 = fmaxf(1.0e-6f, rt + dt * t_rt);
+      const float gw = fp::upwind(fw, tw, tc), ge = fp::upwind(fe, tc, te);
+      const float gs = fp::upwind(fs, ts, tc), gn = fp::upwind(fn, tc, tn);
+      const float gb = fp::upwind(fb, tb, tc), gt = fp::upwind(ft, tc, tt);
+      const float t_rt = -fp::divergence(ge, gw, gn, gs, gt, gb, idx, idy, idz);
+      float r1 = fp::update(rho, dt, t_rho, 1.0e-6f);
+      float q1 = fp::update(rt, dt, t_rt, 1.0e-6f);
       if (blend) {
-        r1 = a.wa * q0.rho + a.wb * r1;
-        q1 = a.wa * q0.rt + a.wb * q1;
+        r1 = fp::blend(a.wa, q0.rho, a.wb, r1);
+        q1 = fp::blend(a.wa, q0.rt, a.wb, q1);
       }
-      const float th1 = q1 / fmaxf(r1, 1.0e-6f);
+      const float th1 = fp::theta(r1, q1);
       if (own) {
         put(IN, a.o_rho, g, kCell, gi, gj, k, r1);
         put(IN, a.o_th, g, kCell, gi, gj, k, a.out_rt ? q1 : th1);
         if (a.acc_mode == 1) {
           // p' of the output: the level sums, and (stored) the first substep's input
-          const float pv = eos_pprime_ref(r1, r1 * th1, s_binv[k], s_bpr[k]);
+          const float pv = eos_pprime_ref(r1, fp::mul(r1, th1), s_binv[k], s_bpr[k]);
           ra.add(r1, kFxRho);
           rb.add(pv, kFxP);
           if (a.p_out) put(IN, a.p_out, g, kCell, gi, gj, k, pv);
@@ -266,19 +263,19 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         const float qs = U(sr, b - BW), qn = U(sr, b + BW);
         const float qb = k > 0 ? cy.uf : qc;
         const float qt = top ? qc : uft;
-        const float flw = upwind(uc[d - 1], qw, qc);
-        const float fle = upwind(uc[d], qc, qe);
+        const float flw = fp::upwind(uc[d - 1], qw, qc);
+        const float fle = fp::upwind(uc[d], qc, qe);
         float fls = 0.0f, fln = 0.0f, flb = 0.0f, flt = 0.0f;
-        if ((IN || !(gj == 0 && open_y))) fls = upwind(0.5f * (vc[d - DW - 1] + vc[d - DW]), qs, qc);
-        if ((IN || !(gj + 1 == ny && open_y))) fln = upwind(0.5f * (vc[d - 1] + vc[d]), qc, qn);
-        if (k > 0) flb = upwind(0.5f * (wcm[d - 1] + wcm[d]), qb, qc);
-        if (!top) flt = upwind(0.5f * (wc[d - 1] + wc[d]), qc, qt);
-        t_u = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
-        t_u += -((pc - pp[d - 1]) * idx);
-        if (a.damp_c) t_u += -kc.damp_c * (qc - kc.uref);
+        if ((IN || !(gj == 0 && open_y))) fls = fp::upwind(fp::avg(vc[d - DW - 1], vc[d - DW]), qs, qc);
+        if ((IN || !(gj + 1 == ny && open_y))) fln = fp::upwind(fp::avg(vc[d - 1], vc[d]), qc, qn);
+        if (k > 0) flb = fp::upwind(fp::avg(wcm[d - 1], wcm[d]), qb, qc);
+        if (!top) flt = fp::upwind(fp::avg(wc[d - 1], wc[d]), qc, qt);
+        t_u = -fp::divergence(fle, flw, fln, fls, flt, flb, idx, idy, idz);
+        t_u = fp::add_pgf(t_u, pc, pp[d - 1], idx);
+        if (a.damp_c) t_u = fp::add_damping(t_u, kc.damp_c, qc, kc.uref);
       }
-      float u1 = fmaxf(-1.0e30f, uf + dt * t_u);
-      if (blend) u1 = a.wa * q0.u + a.wb * u1;
+      float u1 = fp::update(uf, dt, t_u, -1.0e30f);
+      if (blend) u1 = fp::blend(a.wa, q0.u, a.wb, u1);
       if (own) put(IN, a.o_u, g, kFaceX, gi, gj, k, u1);
     }
     // ---- Y face: K18 (dry_momentum_flux.cu:158-235) + K22 (dry_pressure_gradient.cu:125-173)
@@ -290,18 +287,18 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         const float qb = k > 0 ? cy.vf : qc;
         const float qt = top ? qc : vft;
         float flw = 0.0f, fle = 0.0f, flb = 0.0f, flt = 0.0f;
-        if ((IN || !(gi == 0 && open_x))) flw = upwind(0.5f * (uc[d - DW - 1] + uc[d - 1]), qw, qc);
-        if ((IN || !(gi + 1 == nx && open_x))) fle = upwind(0.5f * (uc[d - DW] + uc[d]), qc, qe);
-        const float fls = upwind(vc[d - DW], qs, qc);
-        const float fln = upwind(vc[d], qc, qn);
-        if (k > 0) flb = upwind(0.5f * (wcm[d - DW] + wcm[d]), qb, qc);
-        if (!top) flt = upwind(0.5f * (wc[d - DW] + wc[d]), qc, qt);
-        t_v = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idz);
-        t_v += -((pc - pp[d - DW]) * idy);
-        if (a.damp_c) t_v += -kc.damp_c * (qc - kc.vref);
+        if ((IN || !(gi == 0 && open_x))) flw = fp::upwind(fp::avg(uc[d - DW - 1], uc[d - 1]), qw, qc);
+        if ((IN || !(gi + 1 == nx && open_x))) fle = fp::upwind(fp::avg(uc[d - DW], uc[d]), qc, qe);
+        const float fls = fp::upwind(vc[d - DW], qs, qc);
+        const float fln = fp::upwind(vc[d], qc, qn);
+        if (k > 0) flb = fp::upwind(fp::avg(wcm[d - DW], wcm[d]), qb, qc);
+        if (!top) flt = fp::upwind(fp::avg(wc[d - DW], wc[d]), qc, qt);
+        t_v = -fp::divergence(fle, flw, fln, fls, flt, flb, idx, idy, idz);
+        t_v = fp::add_pgf(t_v, pc, pp[d - DW], idy);
+        if (a.damp_c) t_v = fp::add_damping(t_v, kc.damp_c, qc, kc.vref);
       }
-      float v1 = fmaxf(-1.0e30f, vf + dt * t_v);
-      if (blend) v1 = a.wa * q0.v + a.wb * v1;
+      float v1 = fp::update(vf, dt, t_v, -1.0e30f);
+      if (blend) v1 = fp::blend(a.wa, q0.v, a.wb, v1);
       if (own) put(IN, a.o_v, g, kFaceY, gi, gj, k, v1);
     }
     // ---- Z face k: K19 (dry_momentum_flux.cu:237-312) + K3 buoyancy (dry_core.cu:146-187)
@@ -312,28 +309,23 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
         const float qs = W(sr, b - BW), qn = W(sr, b + BW);
         const float qb = cy.wf, qt = wft;
         float flw = 0.0f, fle = 0.0f, fls = 0.0f, fln = 0.0f;
-        if ((IN || !(gi == 0 && open_x))) flw = upwind(0.5f * (ucm[d - 1] + uc[d - 1]), qw, qc);
-        if ((IN || !(gi + 1 == nx && open_x))) fle = upwind(0.5f * (ucm[d] + uc[d]), qc, qe);
-        if ((IN || !(gj == 0 && open_y))) fls = upwind(0.5f * (vcm[d - DW] + vc[d - DW]), qs, qc);
-        if ((IN || !(gj + 1 == ny && open_y))) fln = upwind(0.5f * (vcm[d] + vc[d]), qc, qn);
-        const float flb = upwind(wcm[d], qb, qc);
-        const float flt = upwind(wc[d], qc, qt);
-        const float idzf = kc.idzf;
-        t_w = -((fle - flw) * idx + (fln - fls) * idy + (flt - flb) * idzf);
-        const float tf = 0.5f * (cy.th + tc);
-        const float trf = 0.5f * (s_thref[k - 1] + s_thref[k]);
-        const float rf = 0.5f * (cy.rho + rho);
-        const float bu = a.gravity * (tf - trf) / fmaxf(trf, 1.0e-6f);
-        t_w += rf * bu;
-        if (a.damp_c) t_w += -kc.damp_f * qc;
+        if ((IN || !(gi == 0 && open_x))) flw = fp::upwind(fp::avg(ucm[d - 1], uc[d - 1]), qw, qc);
+        if ((IN || !(gi + 1 == nx && open_x))) fle = fp::upwind(fp::avg(ucm[d], uc[d]), qc, qe);
+        if ((IN || !(gj == 0 && open_y))) fls = fp::upwind(fp::avg(vcm[d - DW], vc[d - DW]), qs, qc);
+        if ((IN || !(gj + 1 == ny && open_y))) fln = fp::upwind(fp::avg(vcm[d], vc[d]), qc, qn);
+        const float flb = fp::upwind(wcm[d], qb, qc);
+        const float flt = fp::upwind(wc[d], qc, qt);
+        t_w = -fp::divergence(fle, flw, fln, fls, flt, flb, idx, idy, kc.idzf);
+        t_w = fp::add_buoyancy(t_w, cy.th, tc, s_thref[k - 1], s_thref[k], cy.rho, rho, a.gravity);
+        if (a.damp_c) t_w = fp::add_damping(t_w, kc.damp_f, qc, 0.0f);
       }
-      float w1 = fmaxf(-1.0e30f, wf + dt * t_w);
-      if (blend) w1 = a.wa * q0.w + a.wb * w1;
+      float w1 = fp::update(wf, dt, t_w, -1.0e30f);
+      if (blend) w1 = fp::blend(a.wa, q0.w, a.wb, w1);
       if (own) {
         put(IN, a.o_w, g, kFaceZ, gi, gj, k, w1);
         if (top) {  // top face: zero tendency
           float wt = fmaxf(-1.0e30f, wft);
-          if (blend) wt = a.wa * __ldg(a.w0 + gidx(g, gi, gj, nz)) + a.wb * wt;
+          if (blend) wt = fp::blend(a.wa, __ldg(a.w0 + gidx(g, gi, gj, nz)), a.wb, wt);
           put(IN, a.o_w, g, kFaceZ, gi, gj, nz, wt);
         }
       }
@@ -368,13 +360,13 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
           const int r = q / DW, c = q - r * DW;
           const int b = r * BW + c + 3;
           const float rho = sr[R_RHO + b], rt = RT(sr, b);
-          th[q] = theta_of(rho, rt);
+          th[q] = fp::theta(rho, rt);
           pp[q] = eos_pprime_ref(rho, rt, s_binv[k], s_bpr[k]);
           // cell-centred velocities: dry_momentum_flux.cu:36-73
           const float rr = fmaxf(rho, 1.0e-6f);
-          uc[q] = 0.5f * (U(sr, b) + U(sr, b + 1)) / rr;
-          vc[q] = 0.5f * (V(sr, b) + V(sr, b + BW)) / rr;
-          wc[q] = 0.5f * (W(sr, b) + W(sn, b)) / rr;
+          uc[q] = fp::centred(U(sr, b), U(sr, b + 1), rr);
+          vc[q] = fp::centred(V(sr, b), V(sr, b + BW), rr);
+          wc[q] = fp::centred(W(sr, b), W(sn, b), rr);
         }
       }
       const SlowBlend n0a = load_q0(gj0, own0, k + 1), n0b = load_q0(gj1, own1, k + 1);
@@ -396,15 +388,15 @@ __global__ void __launch_bounds__(sl::NT, 2) k_slow_tma(const SlowArgs a, const 
       if (!IN && xf) {  // open east boundary: X face nx of row j0+tx
         const float* sr = ring + (k % NSLOT) * slot;
         const float uf = U(sr, (tx + 1) * BW + w + 4);
-        float u1 = fmaxf(-1.0e30f, uf + dt * 0.0f);
-        if (blend) u1 = a.wa * __ldg(a.u0 + gidx(g, nx, j0 + tx, k)) + a.wb * u1;
+        float u1 = fp::update(uf, dt, 0.0f, -1.0e30f);
+        if (blend) u1 = fp::blend(a.wa, __ldg(a.u0 + gidx(g, nx, j0 + tx, k)), a.wb, u1);
         put(false, a.o_u, g, kFaceX, nx, j0 + tx, k, u1);
       }
       if (!IN && yf) {  // open north boundary: Y face ny of column i0+tx
         const float* sr = ring + (k % NSLOT) * slot;
         const float vf = V(sr, (h + 1) * BW + tx + 4);
-        float v1 = fmaxf(-1.0e30f, vf + dt * 0.0f);
-        if (blend) v1 = a.wa * __ldg(a.v0 + gidx(g, i0 + tx, ny, k)) + a.wb * v1;
+        float v1 = fp::update(vf, dt, 0.0f, -1.0e30f);
+        if (blend) v1 = fp::blend(a.wa, __ldg(a.v0 + gidx(g, i0 + tx, ny, k)), a.wb, v1);
         put(false, a.o_v, g, kFaceY, i0 + tx, ny, k, v1);
       }
       if (a.acc_mode) {

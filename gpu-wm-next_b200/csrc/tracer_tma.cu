@@ -15,6 +15,7 @@
 #include <type_traits>
 
 #include "physics.cuh"
+#include "stencil.cuh"
 #include "tma.cuh"
 
 namespace gwmb {
@@ -160,15 +161,12 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
       const float qs = s_q[t][pb][r - 1][c], qn = s_q[t][pb][r + 1][c];
       const float qbt = (k > 0) ? qb[t] : qc;
       const float qt = (k + 1 < nz) ? s_q[t][pb ^ 1][r][c] : qc;
-      const float gw = fw * (fw >= 0.0f ? qw : qc);
-      const float ge = fe * (fe >= 0.0f ? qc : qe);
-      const float gs = fs * (fs >= 0.0f ? qs : qc);
-      const float gn = fn * (fn >= 0.0f ? qc : qn);
-      const float gb = fb * (fb >= 0.0f ? qbt : qc);
-      const float gt = ft * (ft >= 0.0f ? qc : qt);
-      const float div = (ge - gw) * idx + (gn - gs) * idy + (gt - gb) * idz;
-      float out = fmaxf(0.0f, st[O_Q + t * 736 + r * CBW + c + 3] - a.dt * div);
-      if (blend) out = a.wa * q0v[t] + a.wb * out;
+      const float gw = fp::upwind(fw, qw, qc), ge = fp::upwind(fe, qc, qe);
+      const float gs = fp::upwind(fs, qs, qc), gn = fp::upwind(fn, qc, qn);
+      const float gb = fp::upwind(fb, qbt, qc), gt = fp::upwind(ft, qc, qt);
+      const float div = fp::divergence(ge, gw, gn, gs, gt, gb, idx, idy, idz);
+      float out = fp::update(st[O_Q + t * 736 + r * CBW + c + 3], -a.dt, div, 0.0f);
+      if (blend) out = fp::blend(a.wa, q0v[t], a.wb, out);
       if (own) {
         if (IN) a.q_out[t][gidx(g, gi, gj, k)] = out;
         else store_tile(a.q_out[t], g, kCell, gi, gj, k, out, edge);

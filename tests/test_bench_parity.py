@@ -91,25 +91,12 @@ def test_c3_bench_member_vs_oracles(gwm, orc):
     assert _rel(out["precip"], ref["precip"], floor=1e-12) < 1e-3
 
 
-def c2_grid_and_state(gwm, nx=512, ny=512, nz=80, stretch=0.6):
-    """The mountain-wave configuration: Agnesi hill (400 m, 10 km half width), levels
-    stretched as eta_k = (exp(a k / nz) - 1) / (exp(a) - 1) to 20 km (183 m at the ground,
-    331 m at the top for a = 0.6, 80 levels), constant N = 0.01 1/s from 288 K, 10 m/s."""
-    eta = (np.exp(stretch * np.arange(nz + 1) / nz) - 1.0) / (np.exp(stretch) - 1.0)
-    terrain = gwm.build_terrain("agnesi", nx, ny, 1000.0, 1000.0, height=400.0, half_width_x=10000.0,
-                                half_width_y=10000.0)
-    g = gwm.GridSpec(nx, ny, nz, dx=1000.0, dy=1000.0, z_top=20000.0, terrain=terrain, eta_interfaces=eta)
-    p = gwm.CaseParams(theta_ref=288.0, p_surface=100000.0, u_background=10.0, brunt_vaisala=0.01)
-    s = gwm.build_case("stratified_mountain_wave", g, p)
-    s["u"][:, :, -1] = s["u"][:, :, 0]
-    return g, s
-
-
 def test_c2_full_size_vs_oracles(gwm, orc):
     if _host_gb() < 24:
         pytest.skip(f"the FP64 oracle at 512x512x80 needs ~12 GB of host memory ({_host_gb():.0f} GB free)")
     _oracle(orc)
-    g, s = c2_grid_and_state(gwm)
+    import bench
+    g, s = bench.c2_grid_and_state(gwm)
     uref = s["u"].astype(np.float64).mean(axis=(1, 2))
     # dt 0.5 s: c dt / dz = 0.95 on the 183 m bottom levels (the slow step is bounded by
     # the acoustic CFL of the reference discretisation, about 1.4)

@@ -17,7 +17,7 @@ MOISTURE = ["vapor_water_path_sum_kg_m2", "cloud_water_path_sum_kg_m2", "rain_wa
             "precipitating_surface_fraction", "mean_precipitating_surface_precipitation_mm"]
 
 
-def test_runtime_summary_matches_host_sums(gwm):
+def test_runtime_summary_matches_host_sums(gwm, orc):
     g = gwm.GridSpec(40, 32, 16, dx=2000.0, dy=2000.0, z_top=6000.0)
     p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=2, relative_humidity=1.04)
     s = gwm.build_case("moist_sounding", g, p, moist=True)
@@ -40,7 +40,9 @@ def test_runtime_summary_matches_host_sums(gwm):
     d = {k: v.astype(np.float64) for k, v in out.items()}
     assert summ["total_dry_mass"] == pytest.approx(d["rho"].sum(), rel=1e-13)
     assert summ["rho_d"] == {"min": d["rho"].min(), "max": d["rho"].max()}
-    dz = g.z_top / g.nz
+    # dz = 1 / inv_dz_cell with the metric in FP32, as runtime_summary.cpp:72-81 takes it
+    idz = orc.metrics(orc.GridSpec(g.nx, g.ny, g.nz, dx=g.dx, dy=g.dy, z_top=g.z_top), precision=32)["inv_dz_cell"]
+    dz = 1.0 / np.asarray(idz, np.float64).reshape(g.nz, g.ny, g.nx)
     rho = np.maximum(d["rho"], 1e-12)
     for name, key in (("specific_humidity", "qv"), ("cloud_water_mixing_ratio", "qc"),
                       ("rain_water_mixing_ratio", "qr")):
