@@ -30,8 +30,8 @@ _LIB_PATH = os.path.join(_HERE, "_build", "libgwm_b200.so")
 DRIVER_PATH = os.path.join(_HERE, "_build", "gwm_b200_idealized_driver")
 _DRIVER_SRC = os.path.join(_HERE, "drivers", "gwm_b200_idealized_driver.cpp")
 _SOURCES = ["capi.cu", "dycore.cu", "fast_tma.cu", "slow_tma.cu", "tracer_tma.cu", "physics.cu", "halo.cu",
-            "surrogate.cu", "surrogate_rain.cu", "scalar.cu", "cases.cpp"]
-_HEADERS = ["common.cuh", "stencil.cuh", "dycore.cuh", "physics.cuh", "halo.cuh", "tma.cuh", "rain_cell.cuh", "surrogate.cuh", "surrogate_rain.cuh"]
+            "plan_view.cu", "surrogate.cu", "surrogate_rain.cu", "scalar.cu", "cases.cpp"]
+_HEADERS = ["common.cuh", "stencil.cuh", "dycore.cuh", "physics.cuh", "halo.cuh", "tma.cuh", "plan_view.cuh", "rain_cell.cuh", "surrogate.cuh", "surrogate_rain.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -101,6 +101,15 @@ class _ScalarDesc(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("periodic_x", C.c_int),
                 ("periodic_y", C.c_int), ("u_adv", C.c_float), ("v_adv", C.c_float), ("dt", C.c_float),
                 ("dx", C.c_float), ("dy", C.c_float)]
+
+
+class _PreparedMeta(C.Structure):
+    _fields_ = [("source", C.c_char_p), ("cycle_time_utc", C.c_char_p), ("analysis_valid_time_utc", C.c_char_p),
+                ("enable_boundaries", C.c_int), ("surface_ntile", C.c_int), ("surface_nsoil", C.c_int)] + [
+                (n, C.c_double) for n in ("max_rel_eos", "max_rel_hydrostatic", "max_rel_fast_vertical",
+                                          "max_abs_mass_divergence", "max_rel_mass_divergence",
+                                          "max_abs_mom_w_bottom", "max_abs_mom_w_top", "max_abs_tracer_closure")] + [
+                ("has_max_abs_z_src_minus_metric", C.c_int), ("max_abs_z_src_minus_metric", C.c_double)]
 
 
 class _Fields(C.Structure):
@@ -208,6 +217,18 @@ def lib():
     L.gwm_b200_set_boundary_cache.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(_Fields)]
     L.gwm_b200_runtime_summary_json.argtypes = [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_longlong,
                                                  C.POINTER(C.c_longlong)]
+    L.gwm_b200_phase_summary_json.argtypes = [vp, C.c_int, C.c_int, C.c_float, C.c_char_p, C.c_char_p,
+                                              C.c_longlong, C.POINTER(C.c_longlong)]
+    L.gwm_b200_prepared_steps.argtypes = [vp, C.c_int, C.POINTER(C.c_float), C.c_char_p, C.c_int, C.c_int,
+                                          C.c_int]
+    L.gwm_b200_prepared_summary_json.argtypes = [vp, C.c_int, C.POINTER(_PreparedMeta), C.c_int, C.c_char_p,
+                                                 C.c_char_p, C.c_longlong, C.POINTER(C.c_longlong)]
+    L.gwm_b200_plan_view.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_longlong,
+                                     C.POINTER(C.c_int)]
+    L.gwm_b200_plan_view_field.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p)]
+    L.gwm_b200_plan_view_json.argtypes = [vp, C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_double, C.c_char_p,
+                                          C.c_longlong, C.POINTER(C.c_longlong)]
+    L.gwm_b200_mlp_infer.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float), vp, vp, C.c_longlong, vp]
     L.gwm_b200_set_step_start_time.argtypes = [vp, C.c_int, C.c_float]
     L.gwm_b200_get_step_start_time.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
     L.gwm_b200_tracer_add.argtypes = [vp, C.c_int, C.c_char_p, C.c_char_p, C.c_int]
@@ -242,7 +263,9 @@ EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b
             "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_rain_record",
             "gwm_b200_mlp_train", "gwm_b200_mlp_loss_grad", "gwm_b200_set_rain_surrogate",
             "gwm_b200_surrogate_fallbacks", "gwm_b200_surrogate_stats", "gwm_b200_layout",
-            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_test_stall_tile_load", "gwm_b200_set_boundary_cache", "gwm_b200_runtime_summary_json",
+            "gwm_b200_halo_exchange", "gwm_b200_dry_pressure", "gwm_b200_field_stats_noalloc", "gwm_b200_test_stall_tile_load", "gwm_b200_set_boundary_cache", "gwm_b200_runtime_summary_json", "gwm_b200_mlp_infer",
+            "gwm_b200_plan_view", "gwm_b200_plan_view_field", "gwm_b200_plan_view_json",
+            "gwm_b200_phase_summary_json", "gwm_b200_prepared_steps", "gwm_b200_prepared_summary_json",
             "gwm_b200_set_step_start_time", "gwm_b200_get_step_start_time", "gwm_b200_tracer_add",
             "gwm_b200_tracer_find", "gwm_b200_tracer_count", "gwm_b200_tracer_name", "gwm_b200_tracer_upload",
             "gwm_b200_tracer_download", "gwm_b200_tracer_total", "gwm_b200_scalar_ssprk3", "gwm_b200_grid_z_center", "gwm_b200_ranks_to_global",
@@ -445,6 +468,87 @@ class Model:
         out["_json"] = text
         out["_status"] = rc
         return out
+
+    def _text(self, fn, what, *args):
+        need = C.c_longlong()
+        rc = fn(self._h, *args, None, 0, C.byref(need))
+        if rc not in (OK, ERR_STATE):
+            self._check(rc, what)
+        buf = C.create_string_buffer(int(need.value))
+        rc = fn(self._h, *args, buf, len(buf), None)
+        if rc not in (OK, ERR_STATE):
+            self._check(rc, what)
+        return buf.value.decode()
+
+    def phase_summary(self, step: int, step_start_seconds: float, phase: str, member: int = 0) -> str:
+        """maybe_write_phase_summary's JSON document for the current state."""
+        return self._text(lib().gwm_b200_phase_summary_json, "phase_summary", member, step, step_start_seconds,
+                          phase.encode())
+
+    def prepared_steps(self, nsteps: int, sim_time: float = 0.0, phase_summary_dir: Optional[str] = None,
+                       step: Optional[int] = None, step_min: Optional[int] = None,
+                       step_max: Optional[int] = None) -> float:
+        """The prepared-case driver's step loop with its phase summaries; unset arguments
+        take GWM_PHASE_SUMMARY_DIR / _STEP / _STEP_MIN / _STEP_MAX from the environment,
+        as the driver does.  Returns the start time after the last step."""
+        env = os.environ
+
+        def opt(v, name):
+            if v is not None:
+                return int(v)
+            e = env.get(name, "")
+            return int(e) if e else -1
+        d = phase_summary_dir if phase_summary_dir is not None else env.get("GWM_PHASE_SUMMARY_DIR", "")
+        if d:
+            os.makedirs(d, exist_ok=True)
+        t = C.c_float(sim_time)
+        self._check(lib().gwm_b200_prepared_steps(self._h, nsteps, C.byref(t), d.encode() if d else None,
+                                                  opt(step, "GWM_PHASE_SUMMARY_STEP"),
+                                                  opt(step_min, "GWM_PHASE_SUMMARY_STEP_MIN"),
+                                                  opt(step_max, "GWM_PHASE_SUMMARY_STEP_MAX")), "prepared_steps")
+        return t.value
+
+    def prepared_summary(self, steps: int, initial_json: str, member: int = 0, **meta) -> str:
+        """prepared_summary_json: keyword arguments fill gwm_b200_prepared_meta (strings for
+        source / cycle_time_utc / analysis_valid_time_utc, the startup-balance numbers;
+        max_abs_z_src_minus_metric given sets its presence flag)."""
+        m = _PreparedMeta()
+        for k, v in meta.items():
+            if k == "max_abs_z_src_minus_metric":
+                m.has_max_abs_z_src_minus_metric = 1
+            setattr(m, k, v.encode() if isinstance(v, str) else v)
+        return self._text(lib().gwm_b200_prepared_summary_json, "prepared_summary", member, C.byref(m), steps,
+                          initial_json.encode())
+
+    def plan_view(self, level: int, steps: int = 0, dt: float = 0.0, member: int = 0) -> dict:
+        """extract_runtime_plan_view of the current state at ``level``, computed on the
+        device: {field name: (ny, nx) float64 array} in the bundle's order, with the units
+        under "_units"."""
+        nf = C.c_int()
+        self._check(lib().gwm_b200_plan_view(self._h, member, level, steps, dt, None, 0, C.byref(nf)), "plan_view")
+        g = self.grids[member]
+        out = np.empty((nf.value, g.ny, g.nx), np.float64)
+        self._check(lib().gwm_b200_plan_view(self._h, member, level, steps, dt, out.ctypes.data_as(C.c_void_p),
+                                             out.size, C.byref(nf)),
+                    "plan_view")
+        res, units = {}, {}
+        for q in range(nf.value):
+            name, unit = C.c_char_p(), C.c_char_p()
+            lib().gwm_b200_plan_view_field(q, C.byref(name), C.byref(unit))
+            res[name.value.decode()] = out[q]
+            units[name.value.decode()] = unit.value.decode()
+        res["_units"] = units
+        return res
+
+    def plan_view_json(self, level: int, case_kind: str, steps: int, dt: float, member: int = 0) -> str:
+        """The runtime plan-view bundle as plan_view_bundle_to_json writes it."""
+        need = C.c_longlong()
+        self._check(lib().gwm_b200_plan_view_json(self._h, member, level, case_kind.encode(), steps, dt, None, 0,
+                                                  C.byref(need)), "plan_view_json")
+        buf = C.create_string_buffer(int(need.value))
+        self._check(lib().gwm_b200_plan_view_json(self._h, member, level, case_kind.encode(), steps, dt, buf,
+                                                  len(buf), None), "plan_view_json")
+        return buf.value.decode()
 
     def set_boundary_cache(self, offsets, snapshots, member: int = 0):
         """The prepared-case boundary updater: ``snapshots`` are balanced states (dicts of the
@@ -675,7 +779,8 @@ class Model:
     def set_tile(self, kernel: str, rows: int):
         """CTA tile rows of a kernel: "slow_stage" 3 (owned flat tiles fed by TMA), 8 or 16;
         "tracer_stage" 3 (owned flat tiles fed by TMA), 8 or 16; "fast_substep" 0 (owned
-        flat tiles), 3 (owned flat tiles fed by TMA), 8 or 16."""
+        flat tiles), 3 (owned flat tiles fed by TMA), 4 (the same, all substeps of an RK
+        stage in one persistent launch), 8 or 16."""
         self._check(lib().gwm_b200_set_tile(self._h, self._TILE_KERNELS[kernel], rows), "set_tile")
 
     def get_tile(self, kernel: str) -> int:
@@ -926,6 +1031,17 @@ def mlp_train(x, y, n: int, epochs: int = 10, batch: int = 65536, lr: float = 1e
     if rc != OK:
         raise RuntimeError(f"mlp_train: status {rc}")
     return p, norm, rng, loss
+
+
+def mlp_infer(params, norm, x_ptr: int, y_ptr: int, n: int, stream: Optional[int] = None):
+    """The network through the warm-rain surrogate's tensor-core inference on n device
+    feature rows (x: n x 7 float32 at x_ptr) into y (n x 5 float32 at y_ptr), outputs
+    de-normalised; params and norm are host arrays."""
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    p, nm = f32(params), f32(norm)
+    rc = lib().gwm_b200_mlp_infer(_fptr(p), _fptr(nm), x_ptr, y_ptr, int(n), stream)
+    if rc != OK:
+        raise RuntimeError(f"mlp_infer: status {rc}")
 
 
 def mlp_loss_grad(params, norm, x, y):

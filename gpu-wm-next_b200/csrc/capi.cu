@@ -33,6 +33,7 @@
 #include "dycore.cuh"
 #include "halo.cuh"
 #include "physics.cuh"
+#include "plan_view.cuh"
 #include "surrogate.cuh"
 #include "surrogate_rain.cuh"
 
@@ -83,6 +84,7 @@ struct Member {
   int ring = 0;
   bool theta_valid = false;
   int* err = nullptr;                // device error word (bounded waits that gave up)
+  unsigned* gbar = nullptr;          // grid-barrier words of the persistent acoustic launch
   // reference boundary state (apply_reference_boundaries at every stage start): compact
   // strips of rho, rho*theta, u, v, w and the three tracers; bsave holds the stage-1
   // input's own strips, which the blends of stages 2 and 3 need unchanged
@@ -326,7 +328,7 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
                        3 * kSlot * sizeof(unsigned long long) + owned_max * sizeof(float) +
                        3 * kReduceBlocks * sizeof(double) + 32 * sizeof(ReduceOut) + 4096 +
                        3 * 4 * (kMaxNz + 1) * sizeof(float) + 3 * kMaxNz * sizeof(double) + 512 +
-                       4 * (kMaxNz + 1) * sizeof(float) + 256;
+                       4 * (kMaxNz + 1) * sizeof(float) + 256 + 256;
   const size_t total = nfields * fbytes + extra;
   CK(cudaMalloc(&M.block, total));
   CK(cudaMemsetAsync(M.block, 0, total, c->stream));
@@ -361,6 +363,7 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   M.red_part = (double*)take(3 * kReduceBlocks * sizeof(double));
   M.red_out = (ReduceOut*)take(32 * sizeof(ReduceOut));
   M.err = (int*)take(sizeof(int));
+  M.gbar = (unsigned*)take(2 * sizeof(unsigned));
   M.damp = (float*)take(4 * (kMaxNz + 1) * sizeof(float));
   // metrics
   const HostMetrics H = build_metrics(M);
@@ -392,6 +395,9 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
 }
 
 constexpr int kFastTma = 3;  // fast_tile_rows value selecting the TMA-fed substep
+// fast_tile_rows value selecting the TMA-fed substeps of a stage in one persistent launch
+constexpr int kFastStage = 4;
+bool fast_tma_path(const gwm_b200_ctx* c) { return c->fast_tile_rows == kFastTma || c->fast_tile_rows == kFastStage; }
 constexpr int kSlowTma = 3;  // slow_tile_rows value selecting the TMA-fed slow stage
 constexpr int kTracerTma = 3;  // tracer_tile_rows value selecting the TMA-fed tracer stage
 
@@ -435,32 +441,53 @@ cudaError_t launch_stage(gwm_b200_ctx* c, const Member& M, const SlowArgs& a, bo
 // One acoustic substep: the TMA-fed kernel when selected on flat terrain, else the
 // owned-tile or overlapped-tile kernels.
 // p_ready: the first substep's p' (with its halo) is in f.p_in, written by the slow stage
+// TMA descriptors of one substep's inputs (k_fast_tma); false when one is missing
+bool fast_maps(const Member& M, const FastArgs& f, bool first, bool p_ready, FastMaps& m) {
+  const bool fin = f.final_kind == 2;
+  const bool pin = !first || p_ready;  // p' loaded with its ring, not derived
+  // rho and theta with the halo ring where p' is derived from them, owned boxes otherwise
+  const CUtensorMap* rho = M.tmap(f.rho_in, pin ? 2 : 0);
+  const CUtensorMap* th = M.tmap(f.th, pin ? 2 : 0);
+  const CUtensorMap* du = first ? nullptr : M.tmap(f.du_in, 1);
+  const CUtensorMap* dv = first ? nullptr : M.tmap(f.dv_in, 1);
+  const CUtensorMap* dw = first ? nullptr : M.tmap(f.dw_in, 2);
+  const CUtensorMap* bu = fin ? M.tmap(f.bu, 2) : nullptr;
+  const CUtensorMap* bv = fin ? M.tmap(f.bv, 2) : nullptr;
+  const CUtensorMap* bw = fin ? M.tmap(f.bw, 2) : nullptr;
+  const CUtensorMap* pm = pin ? M.tmap(f.p_in, 0) : nullptr;
+  if (!rho || !th || (!first && (!du || !dv || !dw)) || (pin && !pm) || (fin && (!bu || !bv || !bw)) ||
+      (f.final_kind == 0 && !f.p_out))
+    return false;
+  m.rho = *rho; m.th = *th;
+  if (!first) { m.du = *du; m.dv = *dv; m.dw = *dw; }
+  if (pin) m.p = *pm;
+  if (fin) { m.bu = *bu; m.bv = *bv; m.bw = *bw; }
+  return true;
+}
+
 cudaError_t launch_substep(gwm_b200_ctx* c, const Member& M, const FastArgs& f, bool first, bool terr,
                            bool p_ready = false) {
-  if (!terr && c->fast_tile_rows == kFastTma) {
+  if (!terr && fast_tma_path(c)) {
     FastMaps m{};
-    const bool fin = f.final_kind == 2;
-    const bool pin = !first || p_ready;  // p' loaded with its ring, not derived
-    // rho and theta with the halo ring where p' is derived from them, owned boxes otherwise
-    const CUtensorMap* rho = M.tmap(f.rho_in, pin ? 2 : 0);
-    const CUtensorMap* th = M.tmap(f.th, pin ? 2 : 0);
-    const CUtensorMap* du = first ? nullptr : M.tmap(f.du_in, 1);
-    const CUtensorMap* dv = first ? nullptr : M.tmap(f.dv_in, 1);
-    const CUtensorMap* dw = first ? nullptr : M.tmap(f.dw_in, 2);
-    const CUtensorMap* bu = fin ? M.tmap(f.bu, 2) : nullptr;
-    const CUtensorMap* bv = fin ? M.tmap(f.bv, 2) : nullptr;
-    const CUtensorMap* bw = fin ? M.tmap(f.bw, 2) : nullptr;
-    const CUtensorMap* pm = pin ? M.tmap(f.p_in, 0) : nullptr;
-    if (!rho || !th || (!first && (!du || !dv || !dw)) || (pin && !pm) || (fin && (!bu || !bv || !bw)) ||
-        (f.final_kind == 0 && !f.p_out))
-      return cudaErrorInvalidValue;
-    m.rho = *rho; m.th = *th;
-    if (!first) { m.du = *du; m.dv = *dv; m.dw = *dw; }
-    if (pin) m.p = *pm;
-    if (fin) { m.bu = *bu; m.bv = *bv; m.bw = *bw; }
+    if (!fast_maps(M, f, first, p_ready, m)) return cudaErrorInvalidValue;
     return launch_fast_tma(f, m, first, p_ready, c->stream);
   }
   return launch_fast(f, first, terr, c->stream, c->fast_tile_rows);
+}
+
+// Substeps first .. first + n - 1 of a stage (flat terrain) in one persistent launch.
+cudaError_t launch_substeps_persistent(gwm_b200_ctx* c, const Member& M, const FastArgs* f, int n, bool stage_first,
+                                       bool p_ready) {
+  FastStage st{};
+  st.n = n;
+  st.count = M.gbar;
+  st.gen = M.gbar + 1;
+  for (int q = 0; q < n; ++q) {
+    st.a[q] = f[q];
+    if (!fast_maps(M, f[q], stage_first && q == 0, p_ready, st.m[q])) return cudaErrorInvalidValue;
+  }
+  if (!stage_first) return cudaErrorInvalidValue;  // the launch starts with the stage's first substep
+  return launch_fast_stage_tma(st, p_ready, c->stream);
 }
 
 constexpr int kStripOrient[8] = {kCell, kCell, kFaceX, kFaceY, kFaceZ, kCell, kCell, kCell};
@@ -641,8 +668,7 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
     a.acc_mode = fast ? (terr ? 0 : 1) : ((s == 2 && rain_theta) ? 0 : 2);
     // the TMA slow stage stores the p' it evaluates for the level sums, and the first
     // substep (TMA too) loads it with its ring instead of deriving it again
-    const bool p_handoff = fast && !terr && a.acc_mode == 1 && c->slow_tile_rows == kSlowTma &&
-                           c->fast_tile_rows == kFastTma;
+    const bool p_handoff = fast && !terr && a.acc_mode == 1 && c->slow_tile_rows == kSlowTma && fast_tma_path(c);
     if (p_handoff) a.p_out = M.P[rnext];
     a.inv_count = inv_count(M);
     a.zc = M.zc; a.idz_c = M.idc; a.idz_f = M.idf; a.base = M.base;
@@ -671,6 +697,11 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
     rcur = rnext;
     if (!fast) continue;
     dcur = -1;
+    // persistent mode: the stage's substeps are collected and launched together (the
+    // step's very last substep, with its longer ring, keeps its own launch)
+    const bool persistent = !terr && c->fast_tile_rows == kFastStage && ns <= kFastStageMax + 1;
+    FastArgs pend[kFastStageMax];
+    int npend = 0;
     for (int n = 0; n < ns; ++n) {
       FastArgs f{};
       f.g = M.g;
@@ -692,11 +723,20 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
       f.clr_a = M.slot(M.ring + 2); f.clr_b = M.slot(M.ring + 2) + kMaxNz;
       f.zc = M.zc; f.idz_c = M.idc; f.idz_f = M.idf; f.base = M.base;
       f.err = M.err;
-      LAUNCH(launch_substep(c, M, f, n == 0, terr, n == 0 && p_handoff), "fast substep");
+      if (persistent && f.final_kind != 2 && npend < kFastStageMax) {
+        pend[npend++] = f;
+      } else {
+        if (npend > 0) {
+          LAUNCH(launch_substeps_persistent(c, M, pend, npend, true, p_handoff), "fast substep");
+          npend = 0;
+        }
+        LAUNCH(launch_substep(c, M, f, n == 0, terr, n == 0 && p_handoff), "fast substep");
+      }
       M.ring = (M.ring + 1) % 3;
       rcur ^= 1;
       dcur = dout;
     }
+    if (npend > 0) LAUNCH(launch_substeps_persistent(c, M, pend, npend, true, p_handoff), "fast substep");
   }
   return GWM_B200_OK;
 }
@@ -922,11 +962,12 @@ long long gwm_b200_launch_count(const gwm_b200_ctx* c) { return c ? c->launches 
 
 int gwm_b200_set_tile(gwm_b200_ctx* c, int kernel, int rows) {
   if (!c) return GWM_B200_ERR_ARG;
-  const bool ok = kernel == 1   ? (rows == 0 || rows == kFastTma || rows == 8 || rows == 16)
+  const bool ok = kernel == 1   ? (rows == 0 || rows == kFastTma || rows == kFastStage || rows == 8 || rows == 16)
                   : kernel == 0 ? (rows == kSlowTma || rows == 8 || rows == 16)
                                 : kernel == 2 && (rows == kTracerTma || rows == 8 || rows == 16);
   if (!ok) return GWM_B200_ERR_ARG;
-  if ((kernel == 1 && rows == kFastTma) || (kernel == 0 && rows == kSlowTma) || (kernel == 2 && rows == kTracerTma))
+  if ((kernel == 1 && (rows == kFastTma || rows == kFastStage)) || (kernel == 0 && rows == kSlowTma) ||
+      (kernel == 2 && rows == kTracerTma))
     for (const auto& M : c->m)
       if (!M.terrain_active && M.tmaps.empty())
         return fail(c, GWM_B200_ERR_ARG, "TMA substep unavailable (tensor-map encoder not found)");
@@ -1313,6 +1354,41 @@ int gwm_b200_mlp_train(const float* x, const float* y, long long n, const gwm_b2
   }
   if (cudaMemcpy(params, dp, kMlpParams * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return cleanup(GWM_B200_ERR_CUDA);
   return cleanup(GWM_B200_OK);
+}
+
+int gwm_b200_mlp_infer(const float* params, const float* norm, const float* x, float* y, long long n, void* stream) {
+  if (!params || !norm || !x || !y || n <= 0 || n > 0x7fffff00LL) return GWM_B200_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return GWM_B200_ERR_NO_DEVICE;
+  std::vector<unsigned char> fr(kSurWeightBytes);
+  std::vector<float> tail(kSurBias + kMlpNorm + kMlpRange, 0.0f);
+  surrogate_operands(params, fr.data(), tail.data());
+  std::copy(norm, norm + kMlpNorm, tail.begin() + kSurBias);
+  char* buf = nullptr;
+  if (cudaMalloc(&buf, 65536 + 256) != cudaSuccess) return GWM_B200_ERR_CUDA;
+  cudaStream_t s = (cudaStream_t)stream;
+  bool ok = cudaMemsetAsync(buf + 65536, 0, 256, s) == cudaSuccess &&
+            cudaMemcpyAsync(buf, fr.data(), fr.size(), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemcpyAsync(buf + fr.size(), tail.data(), tail.size() * sizeof(float), cudaMemcpyHostToDevice, s) ==
+                cudaSuccess;
+  SurrogateArgs sa{};
+  sa.weights = (const unsigned char*)buf;
+  sa.bias = (const float*)(buf + kSurWeightBytes);
+  sa.norm = sa.bias + kSurBias;
+  sa.range = sa.norm + kMlpNorm;
+  sa.stats = nullptr;
+  sa.work = (int*)(buf + 65536 + 128);
+  sa.err = (int*)(buf + 65536 + 192);
+  sa.eval_x = x;
+  sa.eval_y = y;
+  sa.eval_n = n;
+  int err = 0;
+  ok = ok && launch_rain_net_eval(sa, s) == cudaSuccess &&
+       cudaMemcpyAsync(&err, sa.err, sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+       cudaStreamSynchronize(s) == cudaSuccess;
+  cudaFree(buf);
+  if (!ok) return GWM_B200_ERR_CUDA;
+  return err ? GWM_B200_ERR_TIMEOUT : GWM_B200_OK;
 }
 
 int gwm_b200_set_rain_surrogate(gwm_b200_ctx* c, int member, const float* params, const float* norm,
@@ -1802,10 +1878,11 @@ int gwm_b200_budgets(gwm_b200_ctx* c, int member, gwm_b200_budget* out) {
 
 // summarize_runtime_state + runtime_state_summary_to_json (src/core/runtime_summary.cpp:
 // 27-178, 180-247) from FP64 device reductions over the member's global fields.
-int gwm_b200_runtime_summary_json(gwm_b200_ctx* c, int member, const char* indent, char* buf, long long cap,
-                                  long long* len) {
-  int rc = check_member(c, member);
-  if (rc) return rc;
+namespace {
+// runtime_state_summary_to_json (runtime_summary.cpp:180-251) of a member's state; the
+// return value is the budget's state status (GWM_B200_ERR_STATE for a non-finite or
+// non-positive density) or an error of the reductions.
+int runtime_summary_text(gwm_b200_ctx* c, int member, const char* indent, std::string& js) {
   Member& M = c->m[member];
   gwm_b200_budget b{};
   const int state_rc = gwm_b200_budgets(c, member, &b);
@@ -1890,15 +1967,337 @@ int gwm_b200_runtime_summary_json(gwm_b200_ctx* c, int member, const char* inden
   }
   o << in << "}\n";
   o << "}";
+  js = o.str();
+  return state_rc;
+}
+
+// text into the caller's buffer (cap bytes, NUL-terminated); *len receives the bytes needed
+int put_text(gwm_b200_ctx* c, const std::string& js, char* buf, long long cap, long long* len) {
+  if (len) *len = (long long)js.size() + 1;
+  if (buf && cap > 0) {
+    const size_t n = std::min<size_t>(js.size(), (size_t)cap - 1);
+    std::memcpy(buf, js.data(), n);
+    buf[n] = 0;
+    if ((long long)js.size() + 1 > cap) return fail(c, GWM_B200_ERR_ARG, "output buffer too small");
+  }
+  return GWM_B200_OK;
+}
+
+// one phase of enqueue_full_step (the same enqueues in the same order)
+int enqueue_phase_tracers(gwm_b200_ctx* c, Member& M) {
+  return (M.md.enable_tracer_transport && !M.reg.empty()) ? enqueue_tracers(c, M) : GWM_B200_OK;
+}
+int enqueue_phase_rain(gwm_b200_ctx* c, Member& M) {
+  return (M.md.moist && M.md.enable_warm_rain) ? enqueue_rain(c, M, 1) : GWM_B200_OK;
+}
+
+// maybe_write_phase_summary's document (gwm_prepared_case_driver.cpp:97-131)
+int phase_summary_text(gwm_b200_ctx* c, int member, int step, float t, const char* phase, std::string& js) {
+  std::string summary;
+  const int rc = runtime_summary_text(c, member, "    ", summary);
+  if (rc != GWM_B200_OK && rc != GWM_B200_ERR_STATE) return rc;
+  std::ostringstream o;
+  o << "{\n  \"step\": " << step << ",\n  \"step_start_seconds\": " << t << ",\n  \"phase\": \""
+    << (phase ? phase : "") << "\",\n  \"summary\": " << summary << "\n}\n";
+  js = o.str();
+  return rc;
+}
+}  // namespace
+
+int gwm_b200_runtime_summary_json(gwm_b200_ctx* c, int member, const char* indent, char* buf, long long cap,
+                                  long long* len) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  std::string js;
+  const int state_rc = runtime_summary_text(c, member, indent, js);
+  if (state_rc != GWM_B200_OK && state_rc != GWM_B200_ERR_STATE) return state_rc;
+  rc = put_text(c, js, buf, cap, len);
+  return rc ? rc : state_rc;
+}
+
+int gwm_b200_phase_summary_json(gwm_b200_ctx* c, int member, int step, float step_start_seconds,
+                                const char* phase, char* buf, long long cap, long long* len) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  std::string js;
+  const int state_rc = phase_summary_text(c, member, step, step_start_seconds, phase, js);
+  if (state_rc != GWM_B200_OK && state_rc != GWM_B200_ERR_STATE) return state_rc;
+  rc = put_text(c, js, buf, cap, len);
+  return rc ? rc : state_rc;
+}
+
+int gwm_b200_prepared_steps(gwm_b200_ctx* c, int nsteps, float* sim_time, const char* phase_summary_dir,
+                            int only_step, int step_min, int step_max) {
+  if (!c || nsteps < 0 || c->m.empty()) return GWM_B200_ERR_ARG;
+  float t = sim_time ? *sim_time : 0.0f;
+  const float dt = c->m[0].md.step.dt;
+  const bool phases = phase_summary_dir && *phase_summary_dir;
+  auto selected = [&](int step) {  // phase_summary_step_selected (:71-88)
+    if (only_step >= 0) return step == only_step;
+    return !(step_min >= 0 && step < step_min) && !(step_max >= 0 && step > step_max);
+  };
+  auto write = [&](int step, const char* phase) {
+    for (int m = 0; m < (int)c->m.size(); ++m) {
+      std::string js;
+      const int rc = phase_summary_text(c, m, step, t, phase, js);
+      if (rc != GWM_B200_OK && rc != GWM_B200_ERR_STATE) return rc;
+      std::string path = std::string(phase_summary_dir) + "/step_" + std::to_string(step) + "_" + phase;
+      if (m > 0) path += "_member" + std::to_string(m);
+      path += ".json";
+      std::FILE* f = std::fopen(path.c_str(), "wb");
+      if (!f) return fail(c, GWM_B200_ERR_ARG, "Failed to open phase summary path: " + path);
+      const bool ok = std::fwrite(js.data(), 1, js.size(), f) == js.size();
+      std::fclose(f);
+      if (!ok) return fail(c, GWM_B200_ERR_ARG, "Failed to write phase summary: " + path);
+    }
+    return GWM_B200_OK;
+  };
+  for (int step = 0; step < nsteps; ++step) {
+    int rc;
+    if (!phases || !selected(step)) {
+      rc = run_steps(c, 1, enqueue_full_step);
+    } else {
+      bool tracers = false, rain = false;
+      for (const auto& M : c->m) {
+        tracers |= M.md.enable_tracer_transport && !M.reg.empty();
+        rain |= M.md.moist && M.md.enable_warm_rain;
+      }
+      rc = run_steps(c, 1, enqueue_dry);
+      if (!rc) rc = write(step, "dry");
+      if (!rc && tracers) rc = run_steps(c, 1, enqueue_phase_tracers);
+      if (!rc && tracers) rc = write(step, "tracers");
+      if (!rc && rain) rc = run_steps(c, 1, enqueue_phase_rain);
+      if (!rc && rain) rc = write(step, "warm_rain");
+    }
+    if (rc) return rc;
+    t += dt;
+  }
+  if (sim_time) *sim_time = t;
+  CK(cudaStreamSynchronize(c->stream));
+  return check_device_errors(c);
+}
+
+int gwm_b200_prepared_summary_json(gwm_b200_ctx* c, int member, const gwm_b200_prepared_meta* meta, int steps,
+                                   const char* initial_json, char* buf, long long cap, long long* len) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  if (!meta || !initial_json || steps < 0) return fail(c, GWM_B200_ERR_ARG, "prepared summary: missing input");
+  const Member& M = c->m[member];
+  std::string final_js;
+  const int state_rc = runtime_summary_text(c, member, "    ", final_js);
+  if (state_rc != GWM_B200_OK && state_rc != GWM_B200_ERR_STATE) return state_rc;
+  // prepared_summary_json (gwm_prepared_case_driver.cpp:252-350)
+  const float dt = M.md.step.dt;
+  const gwm_b200_warm_rain_config& w = M.md.rain;
+  auto b = [](int v) { return v ? "true" : "false"; };
+  const double elapsed = (double)steps * (double)dt;
+  std::ostringstream o;
+  o << std::setprecision(17);
+  o << "{\n";
+  o << "  \"case\": \"prepared_case\",\n";
+  o << "  \"source\": \"" << (meta->source ? meta->source : "") << "\",\n";
+  o << "  \"cycle_time_utc\": \"" << (meta->cycle_time_utc ? meta->cycle_time_utc : "") << "\",\n";
+  o << "  \"analysis_valid_time_utc\": \""
+    << (meta->analysis_valid_time_utc ? meta->analysis_valid_time_utc : "") << "\",\n";
+  o << "  \"steps\": " << steps << ",\n";
+  o << "  \"dt\": " << dt << ",\n";
+  o << "  \"fast_substeps\": " << M.md.step.fast_substeps << ",\n";
+  o << "  \"enable_boundaries\": " << b(meta->enable_boundaries) << ",\n";
+  o << "  \"enable_fast_modes\": " << b(M.md.step.enable_fast_modes) << ",\n";
+  o << "  \"enable_tracer_transport\": " << b(M.md.enable_tracer_transport) << ",\n";
+  o << "  \"enable_warm_rain\": " << b(M.md.enable_warm_rain) << ",\n";
+  o << "  \"fast_update_horizontal_momentum\": " << b(M.md.step.fast_update_horizontal_momentum) << ",\n";
+  o << "  \"fast_update_density\": " << b(M.md.step.fast_update_density) << ",\n";
+  o << "  \"warm_rain\": {\n";
+  o << "    \"condensation_relaxation\": " << w.condensation_relaxation << ",\n";
+  o << "    \"cloud_autoconversion_threshold\": " << w.cloud_autoconversion_threshold << ",\n";
+  o << "    \"cloud_autoconversion_rate\": " << w.cloud_autoconversion_rate << ",\n";
+  o << "    \"rain_evaporation_rate\": " << w.rain_evaporation_rate << ",\n";
+  o << "    \"rain_terminal_velocity\": " << w.rain_terminal_velocity << ",\n";
+  o << "    \"sedimentation_layer_depth_m\": " << w.sedimentation_layer_depth_m << ",\n";
+  o << "    \"enable_latent_heating\": " << b(w.enable_latent_heating) << "\n";
+  o << "  },\n";
+  o << "  \"elapsed_seconds\": " << elapsed << ",\n";
+  o << "  \"elapsed_hours\": " << elapsed / 3600.0 << ",\n";
+  o << "  \"grid\": {\n";
+  o << "    \"nx\": " << M.gd.nx << ",\n    \"ny\": " << M.gd.ny << ",\n    \"nz\": " << M.gd.nz << ",\n";
+  o << "    \"dx\": " << M.gd.dx << ",\n    \"dy\": " << M.gd.dy << ",\n    \"z_top\": " << M.gd.z_top << "\n";
+  o << "  },\n";
+  o << "  \"surface_runtime\": {\n";
+  o << "    \"ntile\": " << meta->surface_ntile << ",\n    \"nsoil\": " << meta->surface_nsoil << "\n";
+  o << "  },\n";
+  o << "  \"startup_balance\": {\n";
+  o << "    \"max_rel_eos\": " << meta->max_rel_eos << ",\n";
+  o << "    \"max_rel_hydrostatic\": " << meta->max_rel_hydrostatic << ",\n";
+  o << "    \"max_rel_fast_vertical\": " << meta->max_rel_fast_vertical << ",\n";
+  o << "    \"max_abs_mass_divergence\": " << meta->max_abs_mass_divergence << ",\n";
+  o << "    \"max_rel_mass_divergence\": " << meta->max_rel_mass_divergence << ",\n";
+  o << "    \"max_abs_mom_w_bottom\": " << meta->max_abs_mom_w_bottom << ",\n";
+  o << "    \"max_abs_mom_w_top\": " << meta->max_abs_mom_w_top << ",\n";
+  o << "    \"max_abs_tracer_closure\": " << meta->max_abs_tracer_closure;
+  if (meta->has_max_abs_z_src_minus_metric)
+    o << ",\n    \"max_abs_z_src_minus_metric\": " << meta->max_abs_z_src_minus_metric << "\n";
+  else
+    o << "\n";
+  o << "  },\n";
+  o << "  \"initial\": " << initial_json << ",\n";
+  o << "  \"final\": " << final_js << "\n";
+  o << "}";
+  rc = put_text(c, o.str(), buf, cap, len);
+  return rc ? rc : state_rc;
+}
+
+// ---------------------------------------------------------------------------
+// Runtime plan view (extract_runtime_plan_view, src/io/plan_view_output.cpp:715-834).
+namespace {
+struct PlanViewName {
+  const char* name;
+  const char* units;
+};
+const PlanViewName kPlanViewNames[kPvAll] = {
+    {"terrain_height", "m"}, {"z_center", "m"}, {"rho_d", "kg m^-3"}, {"theta_m", "K"},
+    {"air_pressure", "Pa"}, {"air_temperature", "K"}, {"u_velocity", "m s^-1"}, {"v_velocity", "m s^-1"},
+    {"wind_speed", "m s^-1"}, {"w_velocity", "m s^-1"}, {"specific_humidity", "kg kg^-1"},
+    {"relative_humidity", "%"}, {"dewpoint", "K"}, {"cloud_water_mixing_ratio", "kg kg^-1"},
+    {"rain_water_mixing_ratio", "kg kg^-1"}, {"total_condensate", "kg kg^-1"}, {"column_cloud_water", "kg m^-2"},
+    {"column_rain_water", "kg m^-2"}, {"column_total_condensate", "kg m^-2"}, {"column_rain_fraction", "1"},
+    {"synthetic_reflectivity", "dBZ"}, {"accumulated_surface_precipitation", "mm"},
+    {"mean_surface_precipitation_rate", "mm h^-1"}};
+
+const Member::Tracer* find_tracer(const Member& M, const char* name) {
+  for (const auto& t : M.reg)
+    if (t.name == name) return &t;
+  return nullptr;
+}
+
+// The bundle's fields for the member's state at level k into a host vector; the
+// field count follows the member's tracers as extract_runtime_plan_view's branches do.
+int plan_view_fields(gwm_b200_ctx* c, Member& M, int k, int steps, double dt, std::vector<double>& host,
+                     int* nfields) {
+  const Geom& g = M.g;
+  PlanViewArgs a{};
+  a.g = g;
+  a.k = k;
+  a.rho = M.Q[0]; a.rt = M.Q[1]; a.u = M.Q[2]; a.v = M.Q[3]; a.w = M.Q[4];
+  a.zc = M.zc; a.idc = M.idc; a.metric_3d = M.terrain_active ? 1 : 0;
+  a.nfields = kPvDry;
+  if (!M.reg.empty()) {  // a runtime tracer state: specific humidity is required
+    const auto* qv = find_tracer(M, "specific_humidity");
+    if (!qv) return fail(c, GWM_B200_ERR_ARG, "specific_humidity tracer missing from runtime tracer state");
+    a.qv = qv->f[0];
+    a.nfields = kPvVapour;
+    const auto *qc = find_tracer(M, "cloud_water_mixing_ratio"), *qr = find_tracer(M, "rain_water_mixing_ratio");
+    if (qc && qr) {
+      a.qc = qc->f[0];
+      a.qr = qr->f[0];
+      a.nfields = kPvWarmRain;
+      if (M.md.moist) {  // the warm-rain surface accumulation
+        a.precip = M.precip;
+        a.precip_comp = M.pcomp;
+        a.inv_hours = 1.0 / std::max((double)steps * (double)(float)dt / 3600.0, 1.0e-9);
+        a.nfields = kPvAll;
+      }
+    }
+  }
+  const size_t plane = (size_t)g.nx * g.ny;
+  double* dev = nullptr;
+  CK(cudaMalloc(&dev, (size_t)a.nfields * plane * sizeof(double)));
+  a.out = dev;
+  host.assign((size_t)a.nfields * plane, 0.0);
+  cudaError_t e = launch_plan_view(a, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(host.data() + plane, dev + plane, (size_t)(a.nfields - 1) * plane * sizeof(double),
+                        cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(dev);
+  CK(e);
+  if (!M.terrain.empty())  // terrain height (the metric's input; zero on flat grids)
+    for (size_t q = 0; q < plane; ++q) host[q] = (double)M.terrain[q];
+  *nfields = a.nfields;
+  return GWM_B200_OK;
+}
+}  // namespace
+
+int gwm_b200_plan_view_field(int field, const char** name, const char** units) {
+  if (field < 0 || field >= kPvAll) return GWM_B200_ERR_ARG;
+  if (name) *name = kPlanViewNames[field].name;
+  if (units) *units = kPlanViewNames[field].units;
+  return GWM_B200_OK;
+}
+
+int gwm_b200_plan_view(gwm_b200_ctx* c, int member, int level, int steps, double dt, double* out, long long cap,
+                       int* nfields) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  const int k = std::clamp(level, 0, M.g.nz - 1);
+  std::vector<double> host;
+  int nf = 0;
+  rc = plan_view_fields(c, M, k, steps, dt, host, &nf);
+  if (rc) return rc;
+  if (nfields) *nfields = nf;
+  if (out) {
+    if (cap < (long long)host.size()) return fail(c, GWM_B200_ERR_ARG, "plan-view buffer too small");
+    std::copy(host.begin(), host.end(), out);
+  }
+  return GWM_B200_OK;
+}
+
+int gwm_b200_plan_view_json(gwm_b200_ctx* c, int member, int level, const char* case_kind, int steps, double dt,
+                            char* buf, long long cap, long long* len) {
+  int rc = check_member(c, member);
+  if (rc) return rc;
+  Member& M = c->m[member];
+  const Geom& g = M.g;
+  const int k = std::clamp(level, 0, g.nz - 1);
+  std::vector<double> f;
+  int nf = 0;
+  rc = plan_view_fields(c, M, k, steps, dt, f, &nf);
+  if (rc) return rc;
+  // plan_view_bundle_to_json (plan_view_output.cpp:950-1003); dt is the bundle's FP32 real,
+  // the mean height the FP64 mean of the level's z_center in row order
+  const size_t plane = (size_t)g.nx * g.ny;
+  const HostMetrics H = build_metrics(M);
+  double zsum = 0.0;
+  for (size_t q = 0; q < plane; ++q) zsum += (double)H.zc[(size_t)k * plane + q];
+  auto jstr = [](const std::string& v) {
+    std::string o = "\"";
+    for (char ch : v) {
+      if (ch == '"' || ch == '\\') o += '\\';
+      o += ch;
+    }
+    return o + "\"";
+  };
+  std::ostringstream o;
+  o << std::setprecision(10);
+  o << "{\n  \"schema_version\": " << jstr("gwm-next-plan-view/v1") << ",\n";
+  o << "  \"case\": " << jstr(case_kind ? case_kind : "") << ",\n";
+  o << "  \"steps\": " << steps << ",\n  \"dt\": " << (float)dt << ",\n  \"slice_k\": " << k << ",\n";
+  o << "  \"grid\": {\n    \"nx\": " << g.nx << ",\n    \"ny\": " << g.ny << ",\n    \"dx\": " << M.gd.dx
+    << ",\n    \"dy\": " << M.gd.dy << ",\n    \"slice_mean_height_m\": " << zsum / (double)(g.nx * g.ny)
+    << "\n  },\n";
+  o << "  \"fields\": [\n";
+  for (int n = 0; n < nf; ++n) {
+    o << "    {\n      \"name\": " << jstr(kPlanViewNames[n].name) << ",\n      \"units\": "
+      << jstr(kPlanViewNames[n].units) << ",\n      \"location\": \"cell_center\",\n      \"nx\": " << g.nx
+      << ",\n      \"ny\": " << g.ny << ",\n      \"storage\": \"row_major_yx\",\n      \"values\": [";
+    const double* v = f.data() + (size_t)n * plane;
+    for (size_t q = 0; q < plane; ++q) {
+      if (q) o << ", ";
+      o << v[q];
+    }
+    o << "]\n    }" << (n + 1 < nf ? "," : "") << "\n";
+  }
+  o << "  ]\n}";
   const std::string js = o.str();
   if (len) *len = (long long)js.size() + 1;
   if (buf && cap > 0) {
     const size_t n = std::min<size_t>(js.size(), (size_t)cap - 1);
     std::memcpy(buf, js.data(), n);
     buf[n] = 0;
-    if ((long long)js.size() + 1 > cap) return fail(c, GWM_B200_ERR_ARG, "summary buffer too small");
+    if ((long long)js.size() + 1 > cap) return fail(c, GWM_B200_ERR_ARG, "plan-view buffer too small");
   }
-  return state_rc;
+  return GWM_B200_OK;
 }
 
 // ---------------------------------------------------------------------------

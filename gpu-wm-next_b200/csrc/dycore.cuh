@@ -112,6 +112,19 @@ cudaError_t init_slow_tma();
 // first: the first substep of a stage (no increments in); p_ready: its p' (with the
 // halo ring) is in a.p_in, written by the slow stage, instead of derived from rho, theta
 cudaError_t launch_fast_tma(const FastArgs& a, const FastMaps& m, bool first, bool p_ready, cudaStream_t s);
+// Consecutive acoustic substeps of one RK stage (flat terrain, TMA path) in one
+// cooperative launch: a[q], m[q] as launch_fast_tma takes them for substep q (q = 0 the
+// stage's first); count/gen: two device words of the grid barrier (count is zeroed on the
+// stream before the launch).  Results equal one launch per substep bit for bit.
+constexpr int kFastStageMax = 8;
+struct FastStage {
+  FastMaps m[kFastStageMax];
+  FastArgs a[kFastStageMax];
+  unsigned *count, *gen;
+  int n;
+  int slot_floats;  // set by the launch: the longest ring slot of the substeps
+};
+cudaError_t launch_fast_stage_tma(FastStage& st, bool p_ready, cudaStream_t s);
 // One-time kernel attributes (dynamic shared memory) of the TMA substep.
 cudaError_t init_fast_tma();
 cudaError_t launch_level_sums(const LevelSumArgs& a, cudaStream_t s);

@@ -140,6 +140,9 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 // barrier of the four consumer warps (id 1; id 0 is __syncthreads)
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
+// EVAL: the network on given feature rows (s.eval_x -> s.eval_y) instead of the cells of a
+// state: every row is active, the consumers write the outputs and apply nothing.
+template <bool EVAL>
 __global__ void __launch_bounds__(kThreads, 3) k_rain_net(const RainArgs a, const SurrogateArgs s) {
   extern __shared__ unsigned char s_dyn[];
   __shared__ __align__(16) float s_bias[kSurBias];
@@ -200,7 +203,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_rain_net(const RainArgs a, cons
     const float* xm = s_norm;
     const float* xmin = s_norm + kMlpNorm;
     const float* xmax = s_norm + kMlpNorm + kMlpIn;
-    const int cx = (g.nx + 31) >> 5, rows = g.ny * g.nz;
+    const int cx = EVAL ? 1 : (g.nx + 31) >> 5;
+    const int rows = EVAL ? (int)((s.eval_n + 31) >> 5) : g.ny * g.nz;
     volatile int* const vconsumed = &s_consumed;
     bool stop = false;
     while (!stop) {
@@ -211,12 +215,12 @@ __global__ void __launch_bounds__(kThreads, 3) k_rain_net(const RainArgs a, cons
       // consecutive rows walk the levels: the active cells cluster in a few levels, and
       // a CTA that took a level at a time would alternate between gating-bound and
       // network-bound stretches instead of overlapping the two
-      const int k = row % g.nz, j = row / g.nz;
-      const int obase = gidx(g, 0, j, k);
+      const int k = EVAL ? 0 : row % g.nz, j = EVAL ? row : row / g.nz;
+      const int obase = EVAL ? 0 : gidx(g, 0, j, k);
       float f_rho = 0.f, f_rt = 0.f, f_qv = 0.f, f_qc = 0.f, f_qr = 0.f;
       auto fetch = [&](int ci) {  // the next chunk's five fields, loaded ahead
         const int ii = ci * 32 + lane;
-        if (ci < cx && ii < g.nx) {
+        if (!EVAL && ci < cx && ii < g.nx) {
           const int o = obase + ii;
           f_rho = __ldg(a.rho + o); f_rt = a.rt[o]; f_qv = a.qv[o]; f_qc = a.qc[o]; f_qr = a.qr[o];
         }
@@ -228,8 +232,15 @@ __global__ void __launch_bounds__(kThreads, 3) k_rain_net(const RainArgs a, cons
         fetch(ci + 1);
         bool net = false, in_range = true;
         float xn[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        float cv[kCellVars];
-        if (i < g.nx) {
+        float cv[kCellVars] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        const long long erow = (long long)row * 32 + lane;  // EVAL: this lane's feature row
+        if (EVAL) {
+          if (erow < s.eval_n) {
+            net = true;
+#pragma unroll
+            for (int f = 0; f < kMlpIn; ++f) xn[f] = (s.eval_x[erow * kMlpIn + f] - xm[f]) * s_rxs[f];
+          }
+        } else if (i < g.nx) {
           // activity gate: with no cloud or rain water and no supersaturation the plain
           // scheme leaves the cell exactly as it is (micro_step takes none of its
           // branches).  A cell without condensate that a fast-math estimate finds clearly
@@ -288,7 +299,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_rain_net(const RainArgs a, cons
           lo.w = pack_bf16(xn[6], 0.0f);
           *reinterpret_cast<uint4*>(sa1 + op_offset(pos, 0, 16)) = lo;
           *reinterpret_cast<uint4*>(sa1 + op_offset(pos, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);  // padding
-          s_ij[pos] = i | (j << 16);
+          s_ij[pos] = EVAL ? (int)erow : (i | (j << 16));
           s_kf[pos] = k | (in_range ? 0x10000 : 0);
 #pragma unroll
           for (int q = 0; q < kCellVars; ++q) s_cell[q][pos] = cv[q];
@@ -419,6 +430,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_rain_net(const RainArgs a, cons
         tmem_wait_ld();
       }
       tc_fence_before();
+      if (EVAL) {
+        if (ct < valid && !failed) {
+          const long long row = s_ij[pos * kNT + ct];
+#pragma unroll
+          for (int q = 0; q < kMlpOut; ++q) s.eval_y[row * kMlpOut + q] = (out[q] + s_bias[192 + q]) * ys[q] + ym[q];
+        }
+        consumer_sync();
+        if (ct == 0) {
+          __threadfence_block();
+          atomicExch(&s_consumed, t + 1);
+        }
+        if (valid < kNT) break;
+        continue;
+      }
       int i = 0, jj = 0, k = 0, kf = 0;
       if (ct < valid && !failed) {
         const int ij = s_ij[pos * kNT + ct];
@@ -566,11 +591,11 @@ cudaError_t launch_warm_rain_surrogate(const RainArgs& a, const SurrogateArgs& s
     int dev = 0, sms = 0, regs_sm = 0, smem_sm = 0, smem_rsv = 0;
     cudaFuncAttributes fa{};
     cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rain_net, cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rain_net<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmem);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_rain_net, cudaFuncAttributePreferredSharedMemoryCarveout,
+      e = cudaFuncSetAttribute(k_rain_net<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                cudaSharedmemCarveoutMaxShared);
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rain_net);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rain_net<false>);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
@@ -586,10 +611,29 @@ cudaError_t launch_warm_rain_surrogate(const RainArgs& a, const SurrogateArgs& s
   const int grid = (int)std::min<long long>(blocks, (rows + kProducerWarps - 1) / kProducerWarps);
   cudaError_t e = cudaMemsetAsync(s.work, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
-  k_rain_net<<<grid, kThreads, kDynSmem, st>>>(a, s);
+  k_rain_net<false><<<grid, kThreads, kDynSmem, st>>>(a, s);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return launch_warm_rain(a, st, /*micro=*/false);
+}
+
+cudaError_t launch_rain_net_eval(const SurrogateArgs& s, cudaStream_t st) {
+  if (!s.work || !s.err || !s.weights || (reinterpret_cast<uintptr_t>(s.weights) & 15u) || !s.eval_x || !s.eval_y ||
+      s.eval_n <= 0 || s.eval_n > 0x7fffff00LL)  // row indices are kept as int
+    return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_rain_net<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  RainArgs a{};  // no cells: the geometry is unused
+  const long long chunks = (s.eval_n + 31) / 32;
+  const int grid = (int)std::min<long long>(sms, (chunks + kProducerWarps - 1) / kProducerWarps);
+  e = cudaMemsetAsync(s.work, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  k_rain_net<true><<<grid, kThreads, kDynSmem, st>>>(a, s);
+  return cudaGetLastError();
 }
 
 }  // namespace gwmb

@@ -28,10 +28,18 @@ struct SurrogateArgs {
   unsigned long long* stats;
   int* work;                     // unit counter of the network kernel (zeroed before each launch)
   int* err;                      // error word: set to 1 when a bounded wait gave up
+  // feature evaluation (launch_rain_net_eval): n rows of kMlpIn features in, the network's
+  // kMlpOut outputs in physical units out (device arrays); unused by the warm-rain launch
+  const float* eval_x;
+  float* eval_y;
+  long long eval_n;
 };
 constexpr int kSurStats = 6;
 
 cudaError_t launch_warm_rain_surrogate(const RainArgs& a, const SurrogateArgs& s, cudaStream_t st);
+// The same tensor-core network on s.eval_n feature rows (no gate, no checks, no cells):
+// s.eval_y[row * kMlpOut + q] = output q of row, de-normalised.
+cudaError_t launch_rain_net_eval(const SurrogateArgs& s, cudaStream_t st);
 
 // Host: weights (FP32 parameter vector) -> the BF16 operand blob and FP32 biases.
 void surrogate_operands(const float* params, unsigned char* weights, float* bias);

@@ -240,6 +240,13 @@ typedef struct {
  * error of the normalised targets. */
 int gwm_b200_mlp_train(const float* x, const float* y, long long n, const gwm_b200_mlp_train_config* cfg,
                        float* params, float* norm, float* range, double* loss_per_epoch);
+/* The trained network evaluated by the warm-rain surrogate's tensor-core inference (BF16
+ * operands, FP32 accumulation in tensor memory, GELU in FP32) on n feature rows: x (n x 7,
+ * device) -> y (n x 5, device), de-normalised outputs (f_cond, f_auto, f_evap, dtheta,
+ * dqv) before any check.  params (9157) and norm (24) are host arrays as for
+ * gwm_b200_set_rain_surrogate.  For validating the inference (no counterpart in the
+ * reference, which has no learned part).  Returns when done. */
+int gwm_b200_mlp_infer(const float* params, const float* norm, const float* x, float* y, long long n, void* stream);
 /* Warm rain of a member with the trained network (params 9157, norm 24, range 14
  * floats, host) instead of the plain per-cell microphysics; NULL params restores the
  * plain scheme.  The network gives condensation, autoconversion and rain evaporation as
@@ -283,13 +290,74 @@ int gwm_b200_budgets(gwm_b200_ctx* ctx, int member, gwm_b200_budget* out);
  * written and reported as GWM_B200_ERR_STATE. */
 int gwm_b200_runtime_summary_json(gwm_b200_ctx* ctx, int member, const char* indent, char* buf, long long cap,
                                   long long* len);
+/* The phase summary of maybe_write_phase_summary (src/core/gwm_prepared_case_driver.cpp:
+ * 97-131): step, step start time, phase name and the runtime summary (indent "    ") of
+ * the member's current state; buf/cap/len as gwm_b200_runtime_summary_json. */
+int gwm_b200_phase_summary_json(gwm_b200_ctx* ctx, int member, int step, float step_start_seconds,
+                                const char* phase, char* buf, long long cap, long long* len);
+/* nsteps of the prepared-case driver's step loop (gwm_prepared_case_driver.cpp:427-463)
+ * over every member, with its phase summaries.  A step whose summaries are not wanted is
+ * gwm_b200_step (one CUDA graph when graphs are on).  When phase_summary_dir is non-empty
+ * and the step is selected (step == only_step when only_step >= 0, else step_min <= step
+ * <= step_max, a negative bound being absent: the GWM_PHASE_SUMMARY_STEP/_MIN/_MAX rules
+ * of :71-88), the step runs as its three phases (dry step; tracer transport; warm rain,
+ * the same kernels in the same order, so the state is the same bit for bit) and after
+ * each phase step_<n>_<phase>.json is written into the directory (which must exist) for
+ * member 0, step_<n>_<phase>_member<m>.json for member m > 0.  *sim_time (may be NULL:
+ * 0) is the first step's start time and receives the time after the last step; it
+ * advances by member 0's dt in FP32, as the driver's sim_time does. */
+int gwm_b200_prepared_steps(gwm_b200_ctx* ctx, int nsteps, float* sim_time, const char* phase_summary_dir,
+                            int only_step, int step_min, int step_max);
+/* What the prepared-case summary reports beyond the member's own configuration: the
+ * analysis' identity, the boundary switch, the surface runtime's extents and the startup
+ * balance diagnostics (ingest and the surface layer stay with the caller). */
+typedef struct {
+  const char* source;                   /* to_string(analysis.source), e.g. "HRRR" */
+  const char* cycle_time_utc;
+  const char* analysis_valid_time_utc;
+  int enable_boundaries;
+  int surface_ntile, surface_nsoil;
+  double max_rel_eos, max_rel_hydrostatic, max_rel_fast_vertical, max_abs_mass_divergence,
+      max_rel_mass_divergence, max_abs_mom_w_bottom, max_abs_mom_w_top, max_abs_tracer_closure;
+  int has_max_abs_z_src_minus_metric;
+  double max_abs_z_src_minus_metric;
+} gwm_b200_prepared_meta;
+/* prepared_summary_json (gwm_prepared_case_driver.cpp:252-350) after `steps` steps: the
+ * member's step and warm-rain configuration and grid, meta, the caller's initial runtime
+ * summary (initial_json, as gwm_b200_runtime_summary_json wrote it with indent "    ")
+ * and the final summary of the member's current state. */
+int gwm_b200_prepared_summary_json(gwm_b200_ctx* ctx, int member, const gwm_b200_prepared_meta* meta, int steps,
+                                   const char* initial_json, char* buf, long long cap, long long* len);
+/* Runtime plan view of a member's current state at level `level` (clamped to [0, nz-1]),
+ * computed on the device: extract_runtime_plan_view (src/io/plan_view_output.cpp:715-834)
+ * over extract_dry_plan_view (:630-713), with the reference's FP32 diagnostics and FP64
+ * column integrals.  The field list follows the member's tracers as the reference's
+ * branches do: without tracers the dry bundle's 10 fields; with a specific_humidity
+ * tracer + specific humidity, relative humidity and dewpoint (13; any other tracer state
+ * without it is GWM_B200_ERR_ARG, as the reference's require is); with the cloud and rain
+ * water tracers too + their mixing ratios, total condensate, the column cloud, rain and
+ * total condensate, the column rain fraction and the synthetic reflectivity (21); for a
+ * moist member + the accumulated surface precipitation and its mean rate over steps * dt
+ * (23).  out (host, may be NULL): *nfields x ny x nx doubles, row-major (y, x); cap is the
+ * number of doubles out holds.  gwm_b200_plan_view_field names field n (0-based, the
+ * bundle's order) and gives its units. */
+int gwm_b200_plan_view(gwm_b200_ctx* ctx, int member, int level, int steps, double dt, double* out, long long cap,
+                       int* nfields);
+int gwm_b200_plan_view_field(int field, const char** name, const char** units);
+/* The same bundle as plan_view_bundle_to_json writes it (plan_view_output.cpp:950-1003),
+ * with case_kind, steps and dt as the bundle's metadata; buf/cap/len as
+ * gwm_b200_runtime_summary_json. */
+int gwm_b200_plan_view_json(gwm_b200_ctx* ctx, int member, int level, const char* case_kind, int steps, double dt,
+                            char* buf, long long cap, long long* len);
 /* Tile shape of a kernel.  kernel 0 = slow stage: rows 3 = owned 32x16 tiles fed by
  * TMA tile loads (flat terrain; terrain falls back to 16), 8 or 16 = overlapped 32-wide
  * tiles (default 16).  kernel 2 = tracer stage: rows 3 = owned 32x16 tiles fed by TMA
  * (flat terrain; terrain falls back to 16), 8 or 16 (overlapped, default 16).  kernel 1 = acoustic substep: rows 0 = owned
  * 32x16 tiles (flat terrain; terrain falls back to 8), 3 = owned 32x16 tiles fed by TMA
- * tile loads (flat terrain; terrain falls back to 8), 8 or 16 = overlapped 32-wide
- * tiles of that many rows.  The environment variable GWM_B200_FAST_TILE_ROWS sets the
+ * tile loads (flat terrain; terrain falls back to 8), 4 = the same tiles with all the
+ * substeps of an RK stage in one persistent cooperative launch (a bounded grid barrier
+ * between substeps; the step's last substep keeps its own launch), 8 or 16 = overlapped
+ * 32-wide tiles of that many rows.  The environment variable GWM_B200_FAST_TILE_ROWS sets the
  * acoustic default at context creation.  The choice changes speed only: every tiling
  * computes the same values.  gwm_b200_get_tile returns the current rows (or < 0). */
 int gwm_b200_set_tile(gwm_b200_ctx* ctx, int kernel, int rows);

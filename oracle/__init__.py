@@ -98,6 +98,7 @@ def lib():
                                C.POINTER(Fields)]
         L.gwo_moist_sounding.argtypes = [C.POINTER(Grid), C.POINTER(Sounding), C.POINTER(Fields)]
         L.gwo_pressure.argtypes = [C.c_long, DP, DP, DP, C.c_int]
+        L.gwo_plan_view.argtypes = [C.POINTER(Grid), C.c_int, C.c_int, C.c_int, C.c_double] + [DP] * 10
         L.gwo_scalar_ssprk3.argtypes = [C.c_int] * 5 + [C.c_double] * 5 + [C.c_int, C.c_int, DP]
         L.gwo_layout.argtypes = [C.c_int] * 8 + [C.POINTER(C.c_int)]
         L.gwo_halo.argtypes = [C.c_int] * 10 + [C.POINTER(DP)]
@@ -343,6 +344,30 @@ def pressure(rho: np.ndarray, rho_theta: np.ndarray, precision: int = 64) -> np.
     p = np.zeros_like(r)
     _check(lib().gwo_pressure(r.size, _ptr(r), _ptr(t), _ptr(p), precision))
     return p
+
+
+# Fields of the runtime plan-view bundle, in its order (plan_view_output.cpp:630-834).
+PLAN_VIEW_FIELDS = ("terrain_height", "z_center", "rho_d", "theta_m", "air_pressure", "air_temperature",
+                    "u_velocity", "v_velocity", "wind_speed", "w_velocity", "specific_humidity",
+                    "relative_humidity", "dewpoint", "cloud_water_mixing_ratio", "rain_water_mixing_ratio",
+                    "total_condensate", "column_cloud_water", "column_rain_water", "column_total_condensate",
+                    "column_rain_fraction", "synthetic_reflectivity", "accumulated_surface_precipitation",
+                    "mean_surface_precipitation_rate")
+
+
+def plan_view(g: GridSpec, state: dict, level: int, steps: int = 0, dt: float = 0.0,
+              nfields: Optional[int] = None) -> dict:
+    """extract_runtime_plan_view of a state (global arrays; the warm-rain tracers as
+    masses rho*q, "precip" the surface accumulation) at ``level``: {field: (ny, nx)}.
+    nfields defaults to what the state holds (10 dry, 21 with qv/qc/qr, 23 with precip)."""
+    if nfields is None:
+        nfields = 10 if "qv" not in state else (21 if "precip" not in state else 23)
+    arr = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in state.items()}
+    out = np.zeros((nfields, g.ny, g.nx), np.float64)
+    gc = g.c()
+    _check(lib().gwo_plan_view(C.byref(gc), level, nfields, steps, dt, *[_ptr(arr.get(k)) for k in (
+        "rho", "rho_theta", "u", "v", "w", "qv", "qc", "qr", "precip")], _ptr(out)))
+    return {PLAN_VIEW_FIELDS[q]: out[q] for q in range(nfields)}
 
 
 def layout(nx, ny, nz, halo, rx, ry, px=True, py=True) -> np.ndarray:

@@ -1264,6 +1264,108 @@ inline void moist_sounding(int nx, int ny, int nz, double z_top, const double* e
 #pragma GCC pop_options
 
 // ---------------------------------------------------------------------------
+// Runtime plan view: extract_runtime_plan_view (src/io/plan_view_output.cpp:715-834)
+// over extract_dry_plan_view (:630-713) on global owned arrays (float, the state's
+// storage type), with the FP32 formulas of dry_thermo.hpp:21-33 and
+// moist_thermo.hpp:23-74 and the FP64 column integrals of :282-416.  nfields is 10
+// (dry), 13 (+ specific humidity), 21 (+ cloud and rain) or 23 (+ the surface
+// precipitation and its mean rate); out holds nfields x ny x nx doubles in the
+// bundle's field order.  Field 0 (terrain height) and 1 (z_center) come from the
+// caller's metric arrays (terrain (ny, nx), zc and idc (nz, ny, nx), FP32).
+#pragma GCC push_options
+#pragma GCC optimize("fp-contract=off")
+struct PlanViewIn {
+  int nx, ny, nz, k, nfields, steps;
+  float dt;
+  const float *terrain, *zc, *idc;
+  const float *rho, *rt, *u, *v, *w;   // cells, X faces (nz, ny, nx+1), Y faces (nz, ny+1, nx), Z faces
+  const float *qv, *qc, *qr;           // tracer masses rho*q
+  const float* precip;                 // liquid_precipitation_kg_m2 (ny, nx)
+};
+
+inline float pv_pressure(float rho, float rt) {  // dry_pressure_from_rho_theta_m
+  const float theta = rt / std::max(rho, 1.0e-6f);
+  const float ratio = std::max(rho * 287.05f * theta / 100000.0f, 1.0e-6f);
+  return 100000.0f * std::pow(ratio, 1.0f / (1.0f - 0.2854f));
+}
+inline float pv_qsat(float t, float p) {  // saturation_specific_humidity
+  const float eps = 287.05f / 461.5f;
+  const float tc = t - 273.15f;
+  const float es = 6.112f * std::exp((17.67f * tc) / std::max(tc + 243.5f, 1.0e-6f)) * 100.0f;
+  const float denom = std::max(p - (1.0f - eps) * es, 1000.0f);
+  return std::min(std::max(eps * es / denom, 0.0f), 0.05f);
+}
+inline float pv_rh(float q, float t, float p) {  // relative_humidity_from_specific_humidity
+  const float qs = pv_qsat(t, p);
+  return std::min(std::max((qs > 0.0f) ? (100.0f * q / qs) : 0.0f, 0.0f), 100.0f);
+}
+inline float pv_dewpoint(float q_in, float p) {  // dewpoint_from_specific_humidity
+  const float eps = 287.05f / 461.5f;
+  const float q = std::min(std::max(q_in, 0.0f), 1.0f);
+  const float e = p * q / std::max(eps + (1.0f - eps) * q, 1.0e-6f);
+  const float e_hpa = std::max(e * 0.01f, 1.0e-6f);
+  const float l = std::log(e_hpa / 6.112f);
+  return (243.5f * l) / (17.67f - l) + 273.15f;
+}
+inline float pv_dbz(float rho, float qr_in) {  // synthetic_reflectivity_dbz_from_rain
+  const float qr = std::max(qr_in, 0.0f);
+  if (qr <= 1.0e-8f || rho <= 1.0e-8f) return -20.0f;
+  const float z = 3.63e9f * std::pow(rho * qr, 1.75f);
+  return 10.0f * std::log10(std::max(z, 1.0e-6f));
+}
+
+inline void plan_view(const PlanViewIn& a, double* out) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz, k = a.k;
+  const size_t plane = (size_t)nx * ny;
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const size_t o = (size_t)j * nx + i, c = (size_t)k * plane + o;
+      auto put = [&](int f, double v) { out[(size_t)f * plane + o] = v; };
+      const float rho = a.rho[c], rr = std::max(rho, 1.0e-6f);
+      const float theta = a.rt[c] / rr;
+      const float p = pv_pressure(rho, a.rt[c]);
+      const float t = theta * std::pow(std::max(p, 1.0f) / 100000.0f, 0.2854f);
+      const size_t cu = ((size_t)k * ny + j) * (nx + 1) + i, cv = ((size_t)k * (ny + 1) + j) * nx + i;
+      const float uc = 0.5f * (a.u[cu] + a.u[cu + 1]) / rr;
+      const float vc = 0.5f * (a.v[cv] + a.v[cv + nx]) / rr;
+      const float wc = 0.5f * (a.w[c] + a.w[c + plane]) / rr;
+      const double vals[10] = {a.terrain ? (double)a.terrain[o] : 0.0, (double)a.zc[c], rho, theta, p, t, uc, vc,
+                               std::sqrt(uc * uc + vc * vc), wc};
+      for (int f = 0; f < 10; ++f) put(f, vals[f]);
+      if (a.nfields <= 10) continue;
+      const float q = a.qv[c] / rr;
+      put(10, q);
+      put(11, pv_rh(q, t, p));
+      put(12, pv_dewpoint(q, p));
+      if (a.nfields <= 13) continue;
+      const float qcm = a.qc[c] / rr, qrm = a.qr[c] / rr;
+      put(13, qcm);
+      put(14, qrm);
+      put(15, qcm + qrm);
+      double col_c = 0.0, col_r = 0.0;
+      float dbz = -20.0f;
+      for (int kk = 0; kk < nz; ++kk) {
+        const size_t ck = (size_t)kk * plane + o;
+        const double dz = (double)(1.0f / a.idc[ck]);
+        col_c += (double)a.qc[ck] * dz;
+        col_r += (double)a.qr[ck] * dz;
+        dbz = std::max(dbz, pv_dbz(a.rho[ck], a.qr[ck] / std::max(a.rho[ck], 1.0e-6f)));
+      }
+      const double total = col_c + col_r, tpos = std::max(total, 0.0);
+      put(16, col_c);
+      put(17, col_r);
+      put(18, total);
+      put(19, tpos <= 0.0 ? 0.0 : std::clamp(col_r / tpos, 0.0, 1.0));
+      put(20, dbz);
+      if (a.nfields <= 21) continue;
+      const double hours = std::max((double)a.steps * (double)a.dt / 3600.0, 1.0e-9);
+      put(21, (double)a.precip[o]);
+      put(22, (double)a.precip[o] / hours);
+    }
+}
+#pragma GCC pop_options
+
+// ---------------------------------------------------------------------------
 // Scalar advection: advance_scalar_ssprk3 (src/dycore/dry_transport.cu:285-325) with
 // upwind_stage_kernel (:13-37) and blend_stage_kernel (:39-46) on the global owned array
 // (nz, ny, nx).  Halo values are the periodic image, or zero beyond an open side (the

@@ -696,6 +696,42 @@ int gwo_scalar_ssprk3(int nx, int ny, int nz, int px, int py, double u, double v
   });
 }
 
+// Runtime plan view (gwo::plan_view) of a state given as global float64 arrays (the
+// values are FP32 state values; they are rounded to float first).  Metrics from the grid
+// in FP32.  qv/qc/qr/precip may be NULL as nfields allows.
+int gwo_plan_view(const gwo_grid* g, int level, int nfields, int steps, double dt, const double* rho,
+                  const double* rt, const double* u, const double* v, const double* w, const double* qv,
+                  const double* qc, const double* qr, const double* precip, double* out) {
+  return guard([&] {
+    gwo::require(nfields == 10 || nfields == 13 || nfields == 21 || nfields == 23, "plan-view field count");
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const size_t nc = (size_t)nx * ny * nz;
+    auto f32 = [](const double* p, size_t n) {
+      std::vector<float> v(p ? n : 0);
+      for (size_t q = 0; p && q < n; ++q) v[q] = (float)p[q];
+      return v;
+    };
+    const auto M = metrics_from<float>(g);
+    const auto r = f32(rho, nc), t = f32(rt, nc), fu = f32(u, (size_t)(nx + 1) * ny * nz),
+               fv = f32(v, (size_t)nx * (ny + 1) * nz), fw = f32(w, nc + (size_t)nx * ny), fqv = f32(qv, nc),
+               fqc = f32(qc, nc), fqr = f32(qr, nc), fp = f32(precip, (size_t)nx * ny),
+               ter = f32(g->terrain, (size_t)nx * ny);
+    std::vector<float> zc(M.zc.begin(), M.zc.end()), idc(M.inv_dz_cell.begin(), M.inv_dz_cell.end());
+    gwo::PlanViewIn a{};
+    a.nx = nx; a.ny = ny; a.nz = nz; a.k = std::clamp(level, 0, nz - 1); a.nfields = nfields;
+    a.steps = steps; a.dt = (float)dt;
+    a.terrain = g->terrain ? ter.data() : nullptr; a.zc = zc.data(); a.idc = idc.data();
+    a.rho = r.data(); a.rt = t.data(); a.u = fu.data(); a.v = fv.data(); a.w = fw.data();
+    a.qv = qv ? fqv.data() : nullptr; a.qc = qc ? fqc.data() : nullptr; a.qr = qr ? fqr.data() : nullptr;
+    a.precip = precip ? fp.data() : nullptr;
+    gwo::require(nfields <= 10 || a.qv, "specific humidity required");
+    gwo::require(nfields <= 13 || (a.qc && a.qr), "cloud and rain water required");
+    gwo::require(nfields <= 21 || a.precip, "precipitation required");
+    gwo::plan_view(a, out);
+    return 0;
+  });
+}
+
 int gwo_pressure(long n, const double* rho, const double* rt, double* p, int precision) {
   for (long q = 0; q < n; ++q)
     p[q] = precision == 32 ? (double)gwo::pressure_from_rho_theta<float>((float)rho[q], (float)rt[q])

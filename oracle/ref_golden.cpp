@@ -21,6 +21,9 @@
 // when moist, the surface precipitation (ny, nx).
 // Each step's wall time (host clock around the step and a device synchronisation) goes
 // to stderr as "step <n> ms <t>", so the reference's own GPU step can be timed too.
+// With a third and fourth argument (path, level) the reference's runtime plan view of the
+// final state (extract_runtime_plan_view, src/io/plan_view_output.cpp:715-834, with the
+// warm-rain accumulation of a moist case) is written there by plan_view_bundle_to_json.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -36,6 +39,7 @@
 #include "gwm/dycore/dry_core.hpp"
 #include "gwm/dycore/dry_transport.hpp"
 #include "gwm/dycore/passive_tracer.hpp"
+#include "gwm/io/plan_view_output.hpp"
 #include "gwm/physics/warm_rain.hpp"
 #include "gwm/state/tracer_registry.hpp"
 
@@ -107,7 +111,7 @@ std::vector<float> gather(const Ext& e, int gnx, int gny, int gnz,
   return g;
 }
 
-int run(const char* in_path, const char* out_path) {
+int run(const char* in_path, const char* out_path, const char* plan_view_path, int plan_view_level) {
   std::FILE* in = std::fopen(in_path, "rb");
   if (!in) throw std::runtime_error(std::string("cannot open ") + in_path);
   CaseHeader h{};
@@ -234,6 +238,15 @@ int run(const char* in_path, const char* out_path) {
     write_floats(out, pr);
   }
   std::fclose(out);
+  if (plan_view_path) {
+    const auto bundle = gwm::io::extract_runtime_plan_view(states, tracers, layout, metrics, "golden", h.steps,
+                                                           cfg.dt, plan_view_level, h.moist ? &accum : nullptr);
+    std::FILE* pv = std::fopen(plan_view_path, "wb");
+    if (!pv) throw std::runtime_error(std::string("cannot write ") + plan_view_path);
+    const std::string js = gwm::io::plan_view_bundle_to_json(bundle);
+    std::fwrite(js.data(), 1, js.size(), pv);
+    std::fclose(pv);
+  }
   return 0;
 }
 
@@ -285,8 +298,8 @@ int run_scalar(const char* in_path, const char* out_path) {
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc != 3) {
-    std::fprintf(stderr, "usage: %s <case.bin> <out.bin>\n", argv[0]);
+  if (argc != 3 && argc != 5) {
+    std::fprintf(stderr, "usage: %s <case.bin> <out.bin> [<plan_view.json> <level>]\n", argv[0]);
     return 2;
   }
   try {
@@ -296,7 +309,7 @@ int main(int argc, char** argv) {
       std::fclose(f);
     }
     if (std::memcmp(magic, "GWMSCAL1", 8) == 0) return run_scalar(argv[1], argv[2]);
-    return run(argv[1], argv[2]);
+    return run(argv[1], argv[2], argc == 5 ? argv[3] : nullptr, argc == 5 ? std::atoi(argv[4]) : 0);
   } catch (const std::exception& e) {
     std::fprintf(stderr, "ref_golden error: %s\n", e.what());
     return 1;

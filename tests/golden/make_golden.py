@@ -8,6 +8,9 @@ parameters and outputs in ``ref_<case>.npz``.  The reference's level-mean
 reduction uses float atomics, so its output is reproducible only to rounding;
 the tests compare against it with tolerances, never bitwise.  The scalar-advection
 cases (advance_scalar_ssprk3, no atomics) are exact and compared bit for bit.
+The plan-view cases (``ref_pv_<case>.npz``) also keep the reference's runtime plan view
+of its final state (extract_runtime_plan_view + plan_view_bundle_to_json, as JSON text)
+beside that state, so the diagnostics are compared on exactly the state they describe.
 
 Usage (on a machine with a GPU and the built driver):
     python tests/golden/make_golden.py --out tests/golden
@@ -68,6 +71,20 @@ CASES = {
         rain=dict(mode=2, terminal_velocity=5.0, layer_depth=500.0), steps=2),
 }
 
+# Plan-view cases: a step case whose final state's runtime plan view (at `level`) is
+# kept.  The moist case starts with a seeded cloud and rain bump reaching the ground, so
+# every moist field, the column maps and the surface precipitation are non-trivial.
+PLAN_VIEW_CASES = {
+    "pv_moist_rain": dict(
+        grid=dict(nx=20, ny=16, nz=12, dx=2000.0, dy=2000.0, z_top=8000.0, ranks_x=2),
+        kind="moist_sounding",
+        params=dict(theta_ref=300.0, relative_humidity=1.02, noise_rms_k=0.5, seed=5),
+        step=dict(dt=2.0, fast_substeps=3), moist=True,
+        rain=dict(mode=1, terminal_velocity=12.0), steps=3,
+        bump=dict(qc=1.5e-3, qr=8.0e-4, sigma=3.0, depth=6), level=2),
+    "pv_dry_terrain": dict(CASES["terrain_cosine"], level=3),
+}
+
 RAIN_DEFAULTS = dict(mode=1, relax=1.0, autoconv_threshold=1.0e-4, autoconv_rate=1.0e-3,
                      evap_rate=5.0e-3, terminal_velocity=0.0, layer_depth=0.0, latent=True)
 STEP_DEFAULTS = dict(dt=2.0, fast_substeps=1, gravity=9.81, fast_hmom=True, fast_density=True,
@@ -93,6 +110,14 @@ def case_state(gwm, spec):
         rv = np.concatenate([r[:, :1, :], 0.5 * (r[:, 1:, :] + r[:, :-1, :]), r[:, -1:, :]], axis=1)
         s["u"] = (ru * ub).astype(np.float32)
         s["v"] = (rv * vb).astype(np.float32)
+    if "bump" in spec:  # cloud and rain mass in a Gaussian column over the lowest levels
+        b = spec["bump"]
+        nz, ny, nx = s["rho"].shape
+        j, i = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+        f = np.exp(-((i - 0.5 * nx) ** 2 + (j - 0.5 * ny) ** 2) / (2.0 * b["sigma"] ** 2))
+        col = (np.arange(nz) < b["depth"]).astype(np.float64)[:, None, None] * f[None]
+        s["qc"] = (s["qc"] + s["rho"] * b["qc"] * col).astype(np.float32)
+        s["qr"] = (s["qr"] + s["rho"] * b["qr"] * col).astype(np.float32)
     return s, terrain
 
 
@@ -181,7 +206,7 @@ def read_scalar_out(path, c):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
-    ap.add_argument("--cases", nargs="*", default=list(CASES) + list(SCALAR_CASES))
+    ap.add_argument("--cases", nargs="*", default=list(CASES) + list(SCALAR_CASES) + list(PLAN_VIEW_CASES))
     args = ap.parse_args()
     if not os.path.exists(DRIVER):
         sys.exit(f"{DRIVER} missing: build it with `make -C oracle ref`")
@@ -201,16 +226,22 @@ def main():
                                     spec=np.frombuffer(json.dumps(c).encode(), dtype=np.uint8), in_q=q, out_q=out)
                 print(f"{name}: wrote ref_{name}.npz (finite={np.isfinite(out).all()})", flush=True)
                 continue
-            spec = CASES[name]
+            spec = CASES[name] if name in CASES else PLAN_VIEW_CASES[name]
             state, terrain = case_state(gwm, spec)
             cpath, opath = os.path.join(tmp, name + ".case"), os.path.join(tmp, name + ".out")
             write_case(cpath, spec, state, terrain)
-            subprocess.run([DRIVER, cpath, opath], check=True, timeout=600)
+            cmd = [DRIVER, cpath, opath]
+            pv_path = os.path.join(tmp, name + ".pv.json")
+            if name in PLAN_VIEW_CASES:
+                cmd += [pv_path, str(spec["level"])]
+            subprocess.run(cmd, check=True, timeout=600)
             shapes = gwm.GridSpec(**{k: v for k, v in spec["grid"].items()}).shapes()
             out = read_out(opath, spec, shapes)
             arrays = {"in_" + k: np.asarray(v, dtype=np.float32) for k, v in state.items() if k != "precip"}
             arrays.update({"out_" + k: v for k, v in out.items()})
             arrays["terrain"] = terrain
+            if name in PLAN_VIEW_CASES:
+                arrays["plan_view_json"] = np.frombuffer(open(pv_path, "rb").read(), dtype=np.uint8)
             np.savez_compressed(os.path.join(args.out, f"ref_{name}.npz"),
                                 spec=np.frombuffer(json.dumps(spec).encode(), dtype=np.uint8), **arrays)
             fin = all(np.isfinite(v).all() for v in out.values())

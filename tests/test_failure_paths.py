@@ -7,7 +7,9 @@
   gwm_b200_test_stall_tile_load: the wait is on a barrier nothing completes) makes the
   kernel's bounded wait run out: the step call returns GWM_B200_ERR_TIMEOUT (-5), the
   CTA drains the loads it did issue and exits, and the context stays usable: the next
-  step from the same state matches a fresh context bit for bit.
+  step from the same state matches a fresh context bit for bit.  In the persistent
+  acoustic launch (all substeps of a stage in one cooperative kernel) the other CTAs
+  find out at the grid barrier, whose wait is bounded the same way.
 """
 import numpy as np
 import pytest
@@ -38,7 +40,10 @@ def test_bad_uploaded_state_is_a_state_error(gwm, field, value):
         assert b["rho_min"] > 0 and np.isfinite(b["total_rho_theta_m"])
 
 
-TILES = {"slow_stage": (0, 3, 16), "fast_substep": (3, 16, 16), "tracer_stage": (0, 16, 3)}
+# (acoustic, slow, tracer) tiles per stalled kernel; "fast_stage": the substeps of a stage
+# in one persistent launch, whose other CTAs then give up at the grid barrier
+TILES = {"slow_stage": (0, 3, 16), "fast_substep": (3, 16, 16), "tracer_stage": (0, 16, 3),
+         "fast_stage": (4, 3, 16)}
 
 
 @pytest.mark.parametrize("graph", [False, True])

@@ -503,6 +503,31 @@ def test_tma_substep_bit_exact(gwm, periodic):
             assert np.array_equal(ref[k], outs[tiles][k]), (tiles, k)
 
 
+@pytest.mark.parametrize("periodic,slow,ns", [(True, 3, 4), (False, 3, 6), (True, 16, 9), (False, 16, 4)])
+def test_persistent_stage_substeps_bit_exact(gwm, periodic, slow, ns):
+    # all substeps of an RK stage in one cooperative launch with a grid barrier between
+    # them (acoustic tiles 4) against one launch per substep (tiles 3), graph replay on:
+    # with and without the slow stage's p' handoff, partial tiles on both axes, and more
+    # substeps than one launch takes (9: eight in the launch, then one on its own)
+    g = gwm.GridSpec(100, 70, 12, dx=2000.0, dy=2000.0, z_top=12000.0,
+                     periodic_x=periodic, periodic_y=periodic)
+    p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=13, relative_humidity=1.02)
+    s = gwm.build_case("moist_sounding", g, p, moist=True)
+    step = gwm.StepConfig(dt=1.0, fast_substeps=ns)
+    rain = gwm.WarmRainConfig(dt=1.0, rain_terminal_velocity=12.0)
+    outs = {}
+    for fast in (3, 4):
+        with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=True)) as m:
+            m.set_tile("fast_substep", fast)
+            m.set_tile("slow_stage", slow)
+            m.use_graph(True)
+            m.upload(s)
+            m.step(3)
+            outs[fast] = m.download()
+    for k in outs[3]:
+        assert np.array_equal(outs[3][k], outs[4][k]), k
+
+
 @pytest.mark.parametrize("nz", [12, 40])
 def test_tma_kernels_with_open_boundary_state(gwm, nz):
     # open x with a reference boundary state (strips written at every stage start), deep

@@ -39,6 +39,10 @@ SNIPPET_PARAMS = {
         "float* x_dev, float* y_dev, long long capacity, unsigned long long seed, float* params, float* norm, "
         "float* range, double* loss_per_epoch"),
     "gwm_b200_scalar_desc d{": "int nx, int ny, int nz, float* q_dev, void* stream",
+    "int smoke = gwm_b200_tracer_add": (
+        "gwm_b200_ctx* ctx, int member, const float* rho_q_host, int n_snapshots, const int* offsets_s, "
+        "const gwm_b200_fields* snapshots, int steps, char* buf, long long cap, const char* initial_summary, "
+        "double dt"),
 }
 
 

@@ -64,3 +64,93 @@ def test_runtime_summary_matches_host_sums(gwm, orc):
     assert mo["total_surface_cell_count"] == g.nx * g.ny
     assert mo["precipitating_surface_cell_count"] == int((pr > 0).sum())
     assert mo["mean_precipitating_surface_precipitation_mm"] == pytest.approx(pr[pr > 0].mean(), rel=1e-12)
+
+
+PREPARED_KEYS = ["case", "source", "cycle_time_utc", "analysis_valid_time_utc", "steps", "dt", "fast_substeps",
+                 "enable_boundaries", "enable_fast_modes", "enable_tracer_transport", "enable_warm_rain",
+                 "fast_update_horizontal_momentum", "fast_update_density", "warm_rain", "elapsed_seconds",
+                 "elapsed_hours", "grid", "surface_runtime", "startup_balance", "initial", "final"]
+
+
+def _moist_member(gwm, seed=4):
+    g = gwm.GridSpec(32, 24, 14, dx=2000.0, dy=2000.0, z_top=7000.0)
+    s = gwm.build_case("moist_sounding", g, gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=seed,
+                                                           relative_humidity=1.04), moist=True)
+    spec = gwm.MemberSpec(step=gwm.StepConfig(dt=1.5, fast_substeps=3),
+                          rain=gwm.WarmRainConfig(dt=1.5, rain_terminal_velocity=20.0), moist=True)
+    return g, s, spec
+
+
+def test_prepared_steps_phase_summaries(gwm, tmp_path):
+    """gwm_prepared_case_driver.cpp:427-463 with maybe_write_phase_summary (:97-131): the
+    selected steps run phase by phase and leave step_<n>_<phase>.json; the state equals
+    the graph-replayed step bit for bit."""
+    g, s, spec = _moist_member(gwm)
+    with gwm.Model(g, spec) as m:
+        m.use_graph(True)
+        m.upload(s)
+        m.step(6)
+        want = m.download()
+    with gwm.Model(g, spec) as m:
+        m.use_graph(True)
+        m.upload(s)
+        t = m.prepared_steps(6, phase_summary_dir=str(tmp_path), step_min=2, step_max=3)
+        got = m.download()
+        final = m.runtime_summary(indent="    ")
+    for k in want:
+        assert np.array_equal(got[k], want[k]), k
+    assert t == np.float32(np.float32(1.5) * 6)
+    names = sorted(p.name for p in tmp_path.iterdir())
+    assert names == sorted(f"step_{n}_{ph}.json" for n in (2, 3) for ph in ("dry", "tracers", "warm_rain"))
+    for n in (2, 3):
+        for ph in ("dry", "tracers", "warm_rain"):
+            text = (tmp_path / f"step_{n}_{ph}.json").read_text()
+            doc = json.loads(text)
+            assert list(doc) == ["step", "step_start_seconds", "phase", "summary"]
+            assert doc["step"] == n and doc["phase"] == ph
+            assert doc["step_start_seconds"] == pytest.approx(1.5 * n)
+            assert list(doc["summary"]) == KEYS
+            assert text.startswith('{\n  "step": ') and text.endswith("\n}\n")
+    # the phase summary after the last selected step's rain is the state's summary then;
+    # a run to step 4 reproduces it
+    with gwm.Model(g, spec) as m:
+        m.upload(s)
+        m.prepared_steps(4)
+        at4 = m.runtime_summary(indent="    ")
+    doc = json.loads((tmp_path / "step_3_warm_rain.json").read_text())
+    assert doc["summary"] == json.loads(at4["_json"])
+    assert final["_status"] == 0
+
+
+def test_prepared_steps_single_step_selection(gwm, tmp_path):
+    g, s, spec = _moist_member(gwm, seed=6)
+    with gwm.Model(g, spec) as m:
+        m.upload(s)
+        m.prepared_steps(3, phase_summary_dir=str(tmp_path), step=1)
+    assert sorted(p.name for p in tmp_path.iterdir()) == ["step_1_dry.json", "step_1_tracers.json",
+                                                         "step_1_warm_rain.json"]
+
+
+def test_prepared_summary_layout(gwm):
+    g, s, spec = _moist_member(gwm, seed=8)
+    with gwm.Model(g, spec) as m:
+        m.upload(s)
+        initial = m.runtime_summary(indent="    ")["_json"]
+        m.prepared_steps(5)
+        text = m.prepared_summary(5, initial, source="HRRR", cycle_time_utc="2026-04-04T00:00:00Z",
+                                  analysis_valid_time_utc="2026-04-04T01:00:00Z", enable_boundaries=1,
+                                  surface_ntile=3, surface_nsoil=4, max_rel_eos=1.5e-7,
+                                  max_abs_tracer_closure=2.0e-9)
+        final = m.runtime_summary(indent="    ")["_json"]
+    doc = json.loads(text)
+    assert list(doc) == PREPARED_KEYS
+    assert doc["case"] == "prepared_case" and doc["source"] == "HRRR" and doc["steps"] == 5
+    assert doc["dt"] == 1.5 and doc["fast_substeps"] == 3 and doc["enable_boundaries"] is True
+    assert doc["enable_warm_rain"] is True and doc["warm_rain"]["rain_terminal_velocity"] == 20.0
+    assert doc["elapsed_seconds"] == 7.5 and doc["elapsed_hours"] == pytest.approx(7.5 / 3600.0, rel=1e-15)
+    assert doc["grid"] == {"nx": 32, "ny": 24, "nz": 14, "dx": 2000.0, "dy": 2000.0, "z_top": 7000.0}
+    assert doc["surface_runtime"] == {"ntile": 3, "nsoil": 4}
+    assert "max_abs_z_src_minus_metric" not in doc["startup_balance"]
+    assert doc["startup_balance"]["max_rel_eos"] == 1.5e-7
+    assert doc["initial"] == json.loads(initial) and doc["final"] == json.loads(final)
+    assert doc["initial"] != doc["final"]

@@ -3,6 +3,8 @@
 The network's FP32 training kernels are checked against the FP64 CPU oracle of the same
 network (oracle.mlp_loss_grad), which is itself checked against finite differences.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -267,3 +269,33 @@ def test_shipped_surrogate_on_held_out_seed(gwm):
     assert abs(res["surrogate"]["precip"] - res["plain"]["precip"]) <= 0.02 * res["plain"]["precip"], res
     assert res["surrogate"]["closure"] <= max(2 * res["plain"]["closure"], 1e-6), res
     assert 0 < res["surrogate"]["fallbacks"] <= 0.1 * res["surrogate"]["network_cells"], res
+
+
+@pytest.mark.gpu
+def test_tensor_core_network_outputs_match_bf16_emulation(gwm):
+    # the raw network outputs of the tcgen05 inference path (BF16 operands, FP32
+    # accumulation in tensor memory) against a numpy evaluation with the same BF16
+    # roundings; the GPU uses the hardware tanh approximation inside GELU, so single
+    # activations can round to the neighbouring BF16 value: the bound is on normalised
+    # outputs, mean and maximum over 100k rows
+    import torch
+    w = np.load(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpu-wm-next_b200",
+                             "surrogate_c3.npz"))
+    params, norm, rng = w["params"].astype(np.float64), w["norm"].astype(np.float64), w["range"].astype(np.float64)
+    r = np.random.default_rng(21)
+    n = 100_003  # a partial last tile
+    lo, hi = rng[:7], rng[7:]
+    x = (lo + (hi - lo) * r.uniform(0, 1, (n, 7))).astype(np.float32)
+    xd = torch.tensor(x, device="cuda")
+    yd = torch.full((n, 5), float("nan"), dtype=torch.float32, device="cuda")
+    gwm.mlp_infer(params.astype(np.float32), norm.astype(np.float32), xd.data_ptr(), yd.data_ptr(), n)
+    torch.cuda.synchronize()
+    y = yd.cpu().numpy().astype(np.float64)
+    assert np.isfinite(y).all()
+    ye = _emulate(params.astype(np.float32).astype(np.float64), norm.astype(np.float32).astype(np.float64),
+                  x.astype(np.float64))
+    ys = norm[19:24]
+    scale = np.where(ys > 0, ys, 1.0)
+    dn = np.abs(y - ye) / scale   # error in normalised output units
+    assert dn.mean(axis=0).max() < 1e-3, dn.mean(axis=0)
+    assert dn.max() < 2e-2, dn.max(axis=0)
