@@ -218,6 +218,8 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-member ensemble line")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-microphysics line")
     ap.add_argument("--no-c2", action="store_true", help="skip the mountain-wave (512x512x80 terrain) line")
+    ap.add_argument("--only-c2", type=int, default=None, metavar="N",
+                    help="run only the mountain-wave object on an N x N x 80 grid (profiling); prints it alone")
     ap.add_argument("--no-persistent", action="store_true",
                     help="skip timing the acoustic substeps of a stage as one persistent launch")
     ap.add_argument("--tracer-tile", type=int, default=None,
@@ -240,6 +242,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     gwm = importlib.import_module("gpu-wm-next_b200")
+    if args.only_c2:
+        stream = torch.cuda.Stream()
+        c2 = c2_line(gwm, torch, stream, dist, world, steps=args.steps, warmup=args.warmup, n=args.only_c2)
+        if rank == 0:
+            print(json.dumps({"c2": c2}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
     g = grid_spec(gwm, args.nx, args.ny, NZ)
     state = gwm.build_case("moist_sounding", g, case_params(gwm, seed=1 + rank), moist=True)
     model = gwm.Model(g, member_spec(gwm))
@@ -527,10 +537,10 @@ def c2_grid_and_state(gwm, nx=512, ny=512, nz=80, stretch=0.6):
     return g, s
 
 
-def c2_line(gwm, torch, stream, dist, world, steps=10, warmup=3):
+def c2_line(gwm, torch, stream, dist, world, steps=10, warmup=3, n=512):
     """The mountain-wave configuration: device-timed throughput and its roofline on the
     1288 B/cell model (terrain kernels on overlapped tiles, tiles chosen by timing)."""
-    g, s = c2_grid_and_state(gwm)
+    g, s = c2_grid_and_state(gwm, n, n)
     uref = s["u"].astype(np.float64).mean(axis=(1, 2))
     spec = gwm.MemberSpec(step=gwm.StepConfig(dt=0.5, fast_substeps=6))
     cells = g.nx * g.ny * g.nz
@@ -559,7 +569,7 @@ def c2_line(gwm, torch, stream, dist, world, steps=10, warmup=3):
             m.profile(False)
     peak, which = load_peaks()
     achieved = C2_BYTES_PER_CELL * cells * steps / (ms * 1e-3) / 1e9
-    return {"workload": "dry mountain wave, 512x512x80 Agnesi hill, stretched levels to 20 km, N = 0.01, "
+    return {"workload": f"dry mountain wave, {n}x{n}x80 Agnesi hill, stretched levels to 20 km, N = 0.01, "
                         "Rayleigh layer above 14 km", "dt_s": 0.5, "fast_substeps": 6, "steps": steps,
             "ms_per_step": ms / steps, "value": job_throughput(cells, steps, world, ms), "unit": "cell-updates/s",
             "tile_rows": tiles, "state_finite": finite,

@@ -18,7 +18,6 @@ A rank that is its own neighbour (one rank along a periodic axis) copies locally
 """
 from __future__ import annotations
 
-from typing import Optional
 
 import numpy as np
 
@@ -179,6 +178,3 @@ def mpi_interface_sync_reference(rank_arrays, rows, halo: int, orientation: int)
                                                                    rank_arrays[north][:, h, h:h + nxl])
     return out
 
-
-def make(nx, ny, nz, halo, ranks_x, ranks_y, periodic_x, periodic_y, group: Optional[object] = None) -> HaloComm:
-    return HaloComm(nx, ny, nz, halo, ranks_x, ranks_y, periodic_x, periodic_y, group)

@@ -9,11 +9,11 @@
 // the FMAs are placed where a multiply feeds an add, the contraction a CUDA build of the
 // reference makes of the same expressions.
 //
-// Every formula takes V = float (one cell) or V = float2 (two cells of a thread at once).
-// The float2 forms issue the packed FP32 instructions of sm_100 (__fadd2_rn, __fmul2_rn,
-// __ffma2_rn: two results per instruction); each lane rounds exactly as the float
-// operation does, so a thread computing two cells in pairs gets the same bits as threads
-// computing them one at a time.
+// Scalar FP32 on purpose: a variant of the TMA slow stage that ran a thread's two cells
+// through the packed FP32 instructions (two results per instruction) was 6.6 % faster but
+// differed from the one-cell kernels by one ulp in rare cells (one ρθ value in 84,000
+// cells per stage on a moist 100 x 70 x 12 case), which breaks the bit-for-bit agreement
+// of the tilings.  The formulas stay templates on the value type V.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -31,18 +31,6 @@ __device__ __forceinline__ float neg(float a) { return -a; }
 __device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ float select_ge0(float a, float x, float y) { return a >= 0.0f ? x : y; }
 __device__ __forceinline__ float splat(float s, float) { return s; }
-
-__device__ __forceinline__ float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 neg(float2 a) { return make_float2(-a.x, -a.y); }
-__device__ __forceinline__ float2 sub(float2 a, float2 b) { return __fadd2_rn(a, neg(b)); }
-__device__ __forceinline__ float2 mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 div(float2 a, float2 b) { return make_float2(__fdiv_rn(a.x, b.x), __fdiv_rn(a.y, b.y)); }
-__device__ __forceinline__ float2 vmax(float2 a, float2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
-__device__ __forceinline__ float2 select_ge0(float2 a, float2 x, float2 y) {
-  return make_float2(a.x >= 0.0f ? x.x : y.x, a.y >= 0.0f ? x.y : y.y);
-}
-__device__ __forceinline__ float2 splat(float s, float2) { return make_float2(s, s); }
 
 // scalar operand broadcast to V
 template <class V> __device__ __forceinline__ V sc(float s) { return splat(s, V{}); }
