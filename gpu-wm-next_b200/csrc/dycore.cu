@@ -360,9 +360,11 @@ __device__ __forceinline__ FastRaw fast_raw(const FastArgs& a, bool valid, int b
   return r;
 }
 
+// col_ref: the column hydrostatic reference (K11) is built only for owned columns, the
+// only ones whose vertical-momentum update reads it.
 template <bool TERRAIN>
 __device__ __forceinline__ FastCol fast_derive(const FastArgs& a, const FastRaw& r, bool valid, int kk,
-                                               const FastCol& below, float dzk) {
+                                               const FastCol& below, float dzk, bool col_ref) {
   FastCol c{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (!valid || kk >= a.g.nz) return c;
   c.rho = r.rho;
@@ -371,7 +373,7 @@ __device__ __forceinline__ FastCol fast_derive(const FastArgs& a, const FastRaw&
   c.thp = fp::theta(c.rho, rt);
   // K20: full pressure for the terrain column reference, perturbation otherwise
   c.p = TERRAIN ? eos_pressure(c.rho, rt) : eos_pprime(c.rho, rt, a.base, kk, a.g.nz);
-  if (TERRAIN) {  // K11 build_column_hydrostatic_reference_kernel (dry_fast_modes.cu:108-158)
+  if (TERRAIN && col_ref) {  // K11 build_column_hydrostatic_reference_kernel (dry_fast_modes.cu:108-158)
     if (kk == 0) {
       c.pref = c.p;
       c.rref = eos_rho(c.pref, c.thp);
@@ -448,8 +450,8 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
 
   float zm = 0.f, zcc = r0.z, zn = r1.z;
   FastCol none{};
-  FastCol cm{}, cc = fast_derive<TERRAIN>(a, r0, valid, 0, none, 0.f);
-  FastCol cn = fast_derive<TERRAIN>(a, r1, valid, 1, cc, zn - zcc);
+  FastCol cm{}, cc = fast_derive<TERRAIN>(a, r0, valid, 0, none, 0.f, own_c);
+  FastCol cn = fast_derive<TERRAIN>(a, r1, valid, 1, cc, zn - zcc, own_c);
   float dw_c = 0.0f;  // increment at face k (face 0 never changes)
 
   for (int k = 0; k < nz; ++k) {
@@ -553,7 +555,7 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
     zm = zcc;
     zcc = zn;
     zn = r2.z;
-    cn = fast_derive<TERRAIN>(a, r2, valid, k + 2, cc, zn - zcc);
+    cn = fast_derive<TERRAIN>(a, r2, valid, k + 2, cc, zn - zcc, own_c);
     r2 = r3;
   }
   if (acc_mode) {

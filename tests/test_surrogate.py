@@ -296,6 +296,15 @@ def test_tensor_core_network_outputs_match_bf16_emulation(gwm):
                   x.astype(np.float64))
     ys = norm[19:24]
     scale = np.where(ys > 0, ys, 1.0)
-    dn = np.abs(y - ye) / scale   # error in normalised output units
+    # the kernel de-normalises in FP32: (out + b) ys + ym.  Where ys is below the FP32
+    # spacing of ym (the autoconversion output: ys 5e-11 about ym 1e-3, spacing 1.2e-10)
+    # the result cannot resolve the network's variation, so differences within two FP32
+    # spacings of the value are not network errors
+    res = 2.0 * np.spacing(np.abs(ye).astype(np.float32)).astype(np.float64)
+    dn = np.maximum(np.abs(y - ye) - res, 0.0) / scale   # error in normalised output units
     assert dn.mean(axis=0).max() < 1e-3, dn.mean(axis=0)
     assert dn.max() < 2e-2, dn.max(axis=0)
+    # the resolvable outputs also hold the bound without the allowance
+    big = ys > 1e3 * np.spacing(np.abs(norm[14:19]).astype(np.float32))
+    dn_raw = (np.abs(y - ye) / scale)[:, big]
+    assert big.sum() >= 4 and dn_raw.mean(axis=0).max() < 1e-3, dn_raw.mean(axis=0)
