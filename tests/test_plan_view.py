@@ -84,11 +84,18 @@ def _kat_precip():
     return pr
 
 
+# the reference (and the oracle restating it) holds the surface accumulation in FP32;
+# this path keeps it in FP64 with a compensation term
+PRECIP = {"accumulated_surface_precipitation", "mean_surface_precipitation_rate"}
+
+
 def _compare(got, want, tag=""):
     for name, w in want.items():
         g = np.asarray(got[name], np.float64)
         w = np.asarray(w, np.float64)
-        if name in TRANSCENDENTAL:
+        if name in PRECIP:
+            assert np.allclose(g, w, rtol=6e-8, atol=0.0), f"{tag} {name}: max |diff| {np.abs(g - w).max():.3e}"
+        elif name in TRANSCENDENTAL:
             scale = np.maximum(np.abs(w), 1e-30)
             err = float((np.abs(g - w) / scale).max())
             assert err <= 4e-6, f"{tag} {name}: relative {err:.3e}"
