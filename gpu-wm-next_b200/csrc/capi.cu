@@ -74,6 +74,7 @@ struct Member {
   std::vector<Tracer> reg;
   std::vector<char*> extra;
   float *zc = nullptr, *idc = nullptr, *idf = nullptr;
+  float* colref[2]{};                // terrain: the substep input's column reference (K11)
   double *precip = nullptr, *pcomp = nullptr;
   unsigned long long* acc = nullptr;
   double* base = nullptr;            // FP64 base state of the perturbation EOS
@@ -120,16 +121,16 @@ struct Member {
 }  // namespace
 
 // Per-kernel CUDA-event timing (profiling mode, direct launches only).
-enum KernelKind { kKSlow = 0, kKFast, kKTracer, kKRain, kKOther, kKinds };
+enum KernelKind { kKSlow = 0, kKFast, kKTracer, kKRain, kKColumn, kKOther, kKinds };
 const char* const kKindNames[kKinds] = {"k_slow_stage", "k_fast_substep", "k_tracer_stage",
-                                        "k_warm_rain", "other"};
+                                        "k_warm_rain", "k_column_reference", "other"};
 
 struct gwm_b200_ctx {
   std::vector<Member> m;
   bool profile = false;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_events;
-  double prof_ms[kKinds] = {0, 0, 0, 0, 0};
-  long long prof_n[kKinds] = {0, 0, 0, 0, 0};
+  double prof_ms[kKinds] = {};
+  long long prof_n[kKinds] = {};
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   std::string err;
@@ -321,7 +322,7 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   M.field_elems = (size_t)g.plane * (g.nz + 1);
   const size_t fbytes = ((M.field_elems * sizeof(float) + 255) / 256) * 256;
   const bool moist = M.md.moist != 0;
-  const int nfields = 5 + 2 + 2 + 2 + 6 + 6 + (moist ? 9 : 0) + (M.terrain_active ? 3 : 0);
+  const int nfields = 5 + 2 + 2 + 2 + 6 + 6 + (moist ? 9 : 0) + (M.terrain_active ? 5 : 0);
   const size_t owned_max = (size_t)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
   const size_t plane2 = (size_t)d.nx * d.ny;
   const size_t extra = ((2 * plane2 * sizeof(double) + 255) / 256) * 256 +
@@ -368,6 +369,8 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
   // metrics
   const HostMetrics H = build_metrics(M);
   if (M.terrain_active) {
+    M.colref[0] = (float*)take(fbytes);  // column hydrostatic reference: pressure, density
+    M.colref[1] = (float*)take(fbytes);
     M.zc = (float*)take(fbytes);
     M.idc = (float*)take(fbytes);
     M.idf = (float*)take(fbytes);
@@ -528,6 +531,7 @@ int kind_of(const char* name) {
   if (n == "fast substep") return kKFast;
   if (n == "tracer stage") return kKTracer;
   if (n == "warm rain") return kKRain;
+  if (n == "column reference") return kKColumn;
   return kKOther;
 }
 
@@ -729,6 +733,10 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
         if (npend > 0) {
           LAUNCH(launch_substeps_persistent(c, M, pend, npend, true, p_handoff), "fast substep");
           npend = 0;
+        }
+        if (terr) {  // the substep input's column reference, then the substep
+          f.col_pref = M.colref[0]; f.col_rref = M.colref[1];
+          LAUNCH(launch_column_reference(f, c->stream), "column reference");
         }
         LAUNCH(launch_substep(c, M, f, n == 0, terr, n == 0 && p_handoff), "fast substep");
       }
@@ -1776,6 +1784,10 @@ int gwm_b200_fast_modes(gwm_b200_ctx* c) {
       f.clr_a = M.slot(M.ring + 2); f.clr_b = M.slot(M.ring + 2) + kMaxNz;
       f.zc = M.zc; f.idz_c = M.idc; f.idz_f = M.idf; f.base = M.base;
       f.err = M.err;
+      if (terr) {
+        f.col_pref = M.colref[0]; f.col_rref = M.colref[1];
+        LAUNCH(launch_column_reference(f, c->stream), "column reference");
+      }
       LAUNCH(launch_substep(c, M, f, n == 0, terr), "fast substep");
       M.ring = (M.ring + 1) % 3;
       rcur ^= 1;

@@ -339,7 +339,6 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
 // Acoustic substep.
 struct FastCol {
   float rho, th, thp, p;   // thp: theta recovered from (rho, rho*theta) as the reference does
-  float pref, rref;        // column hydrostatic reference (terrain)
 };
 struct FastRaw {
   float rho, th, z;        // plane values loaded ahead of use
@@ -360,12 +359,9 @@ __device__ __forceinline__ FastRaw fast_raw(const FastArgs& a, bool valid, int b
   return r;
 }
 
-// col_ref: the column hydrostatic reference (K11) is built only for owned columns, the
-// only ones whose vertical-momentum update reads it.
 template <bool TERRAIN>
-__device__ __forceinline__ FastCol fast_derive(const FastArgs& a, const FastRaw& r, bool valid, int kk,
-                                               const FastCol& below, float dzk, bool col_ref) {
-  FastCol c{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+__device__ __forceinline__ FastCol fast_derive(const FastArgs& a, const FastRaw& r, bool valid, int kk) {
+  FastCol c{0.f, 0.f, 0.f, 0.f};
   if (!valid || kk >= a.g.nz) return c;
   c.rho = r.rho;
   c.th = r.th;
@@ -373,22 +369,43 @@ __device__ __forceinline__ FastCol fast_derive(const FastArgs& a, const FastRaw&
   c.thp = fp::theta(c.rho, rt);
   // K20: full pressure for the terrain column reference, perturbation otherwise
   c.p = TERRAIN ? eos_pressure(c.rho, rt) : eos_pprime(c.rho, rt, a.base, kk, a.g.nz);
-  if (TERRAIN && col_ref) {  // K11 build_column_hydrostatic_reference_kernel (dry_fast_modes.cu:108-158)
-    if (kk == 0) {
-      c.pref = c.p;
-      c.rref = eos_rho(c.pref, c.thp);
+  return c;
+}
+
+// K11 build_column_hydrostatic_reference_kernel (dry_fast_modes.cu:108-158): per column,
+// bottom to top, the reference pressure and density the terrain substep takes its
+// perturbations about.  A column is a chain of dependent powf evaluations (four
+// fixed-point iterations per level), so it runs apart from the substep with every
+// column in flight at once; the values are the ones the substep used to build inline.
+__global__ void __launch_bounds__(128) k_column_reference(const FastArgs a) {
+  const Geom& g = a.g;
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y;
+  if (i >= g.nx || j >= g.ny) return;
+  const int base = gidx(g, i, j, 0);
+  float pref = 0.f, rref = 0.f, zb = 0.f;
+  for (int k = 0; k < g.nz; ++k) {
+    const int o = base + k * g.plane;
+    const float rho = __ldg(a.rho_in + o), th = __ldg(a.th + o), z = __ldg(a.zc + o);
+    const float rt = fp::mul(rho, th);
+    const float thp = fp::theta(rho, rt);
+    if (k == 0) {
+      pref = eos_pressure(rho, rt);
+      rref = eos_rho(pref, thp);
     } else {
-      float pn = fmaxf(1.0f, fp::fma(-fp::mul(a.gravity, below.rref), dzk, below.pref));
+      const float dzk = z - zb;
+      float pn = fmaxf(1.0f, fp::fma(-fp::mul(a.gravity, rref), dzk, pref));
       for (int it = 0; it < 4; ++it) {
-        const float rn = eos_rho(pn, c.thp);
-        pn = fp::fma(-fp::mul(fp::mul(a.gravity, 0.5f), fp::add(below.rref, rn)), dzk, below.pref);
+        const float rn = eos_rho(pn, thp);
+        pn = fp::fma(-fp::mul(fp::mul(a.gravity, 0.5f), fp::add(rref, rn)), dzk, pref);
         pn = fmaxf(pn, 1.0f);
       }
-      c.pref = pn;
-      c.rref = eos_rho(pn, c.thp);
+      pref = pn;
+      rref = eos_rho(pn, thp);
     }
+    a.col_pref[o] = pref;
+    a.col_rref[o] = rref;
+    zb = z;
   }
-  return c;
 }
 
 template <bool FIRST>
@@ -449,10 +466,12 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
   const int acc_mode = a.acc_off ? 0 : (a.final_kind == 0 ? (TERRAIN ? 0 : 1) : 2);
 
   float zm = 0.f, zcc = r0.z, zn = r1.z;
-  FastCol none{};
-  FastCol cm{}, cc = fast_derive<TERRAIN>(a, r0, valid, 0, none, 0.f, own_c);
-  FastCol cn = fast_derive<TERRAIN>(a, r1, valid, 1, cc, zn - zcc, own_c);
+  FastCol cm{}, cc = fast_derive<TERRAIN>(a, r0, valid, 0);
+  FastCol cn = fast_derive<TERRAIN>(a, r1, valid, 1);
   float dw_c = 0.0f;  // increment at face k (face 0 never changes)
+  // terrain: the column reference of the owned column at levels k and k+1
+  float pref_c = 0.f, rref_c = 0.f;
+  if (TERRAIN && own_c) { pref_c = __ldg(a.col_pref + base); rref_c = __ldg(a.col_rref + base); }
 
   for (int k = 0; k < nz; ++k) {
     const int pb = k & 1;
@@ -465,6 +484,11 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
       if (own_u) bu0 = __ldg(a.bu + o);
       if (own_v) bv0 = __ldg(a.bv + o);
       if (own_c) { bw1 = __ldg(a.bw + o + g.plane); if (k == 0) bw0 = __ldg(a.bw + o); }
+    }
+    float pref_n = 0.f, rref_n = 0.f;
+    if (TERRAIN && own_c && k + 1 < nz) {
+      pref_n = __ldg(a.col_pref + o + g.plane);
+      rref_n = __ldg(a.col_rref + o + g.plane);
     }
     float idzf = 0.f, idzc = 0.f;
     if (own_c) {
@@ -504,8 +528,8 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
     // K14: Z face k+1 (dry_fast_modes.cu:303-348), perturbations about the reference
     float dw_n = d0.dw1;
     if (own_c && k + 1 < nz) {
-      const float prl = TERRAIN ? cc.pref : s_pref[k], pru = TERRAIN ? cn.pref : s_pref[k + 1];
-      const float rrl = TERRAIN ? cc.rref : s_rref[k], rru = TERRAIN ? cn.rref : s_rref[k + 1];
+      const float prl = TERRAIN ? pref_c : s_pref[k], pru = TERRAIN ? pref_n : s_pref[k + 1];
+      const float rrl = TERRAIN ? rref_c : s_rref[k], rru = TERRAIN ? rref_n : s_rref[k + 1];
       dw_n = fp::wmom(d0.dw1, cn.p, pru, cc.p, prl, cc.rho, rrl, cn.rho, rru, idzf, a.gravity, dtf);
     }
     __syncthreads();
@@ -549,13 +573,15 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
     }
     dw_c = dw_n;
     d0 = d1;
+    pref_c = pref_n;
+    rref_c = rref_n;
     // advance the column window
     cm = cc;
     cc = cn;
     zm = zcc;
     zcc = zn;
     zn = r2.z;
-    cn = fast_derive<TERRAIN>(a, r2, valid, k + 2, cc, zn - zcc, own_c);
+    cn = fast_derive<TERRAIN>(a, r2, valid, k + 2);
     r2 = r3;
   }
   if (acc_mode) {
@@ -957,6 +983,13 @@ cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_
   }
   if (tile_rows == 16) return launch_fast_tile<16>(a, first, terrain, s);
   return launch_fast_tile<8>(a, first, terrain, s);
+}
+
+cudaError_t launch_column_reference(const FastArgs& a, cudaStream_t s) {
+  if (!a.col_pref || !a.col_rref || !a.zc || a.g.nx <= 0 || a.g.ny <= 0) return cudaErrorInvalidValue;
+  const dim3 block(32, 4), grid((a.g.nx + 31) / 32, (a.g.ny + 3) / 4);
+  k_column_reference<<<grid, block, 0, s>>>(a);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_level_sums(const LevelSumArgs& a, cudaStream_t s) {

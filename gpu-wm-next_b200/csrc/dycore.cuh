@@ -71,6 +71,9 @@ struct FastArgs {
   const float *zc, *idz_c, *idz_f;
   const double* base;
   int* err;                         // error word: set to 1 when a bounded wait gave up
+  // terrain: the column hydrostatic reference (K11) of rho_in, pressure and density per
+  // cell, written by launch_column_reference before the substep and read by it
+  float *col_pref, *col_rref;
 };
 
 // TMA descriptors of one acoustic substep (flat terrain, k_fast_tma): 3-D tiled maps
@@ -112,6 +115,9 @@ cudaError_t init_slow_tma();
 // first: the first substep of a stage (no increments in); p_ready: its p' (with the
 // halo ring) is in a.p_in, written by the slow stage, instead of derived from rho, theta
 cudaError_t launch_fast_tma(const FastArgs& a, const FastMaps& m, bool first, bool p_ready, cudaStream_t s);
+// K11 build_column_hydrostatic_reference_kernel (dry_fast_modes.cu:108-158) of a.rho_in
+// and a.th into a.col_pref / a.col_rref: one thread per owned column, bottom to top.
+cudaError_t launch_column_reference(const FastArgs& a, cudaStream_t s);
 // Consecutive acoustic substeps of one RK stage (flat terrain, TMA path) in one
 // cooperative launch: a[q], m[q] as launch_fast_tma takes them for substep q (q = 0 the
 // stage's first); count/gen: two device words of the grid barrier (count is zeroed on the
