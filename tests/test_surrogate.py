@@ -301,7 +301,11 @@ def test_tensor_core_network_outputs_match_bf16_emulation(gwm):
     # the result cannot resolve the network's variation, so differences within two FP32
     # spacings of the value are not network errors
     res = 2.0 * np.spacing(np.abs(ye).astype(np.float32)).astype(np.float64)
-    dn = np.maximum(np.abs(y - ye) - res, 0.0) / scale   # error in normalised output units
+    # error in normalised output units, relative to the output where it exceeds 1: the
+    # random rows span the whole input box, far outside the training distribution, and
+    # drive normalised outputs up to ~140, where BF16 activations carry ~1e-3 of the value
+    yen = np.abs(ye - norm[14:19]) / scale
+    dn = np.maximum(np.abs(y - ye) - res, 0.0) / scale / np.maximum(1.0, yen)
     assert dn.mean(axis=0).max() < 1e-3, dn.mean(axis=0)
     assert dn.max() < 2e-2, dn.max(axis=0)
     # the resolvable outputs also hold the bound without the allowance
