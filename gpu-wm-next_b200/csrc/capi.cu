@@ -478,18 +478,17 @@ cudaError_t launch_substep(gwm_b200_ctx* c, const Member& M, const FastArgs& f, 
   return launch_fast(f, first, terr, c->stream, c->fast_tile_rows);
 }
 
-// Substeps first .. first + n - 1 of a stage (flat terrain) in one persistent launch.
-cudaError_t launch_substeps_persistent(gwm_b200_ctx* c, const Member& M, const FastArgs* f, int n, bool stage_first,
-                                       bool p_ready) {
+// The first n substeps of a stage (flat terrain) in one persistent launch; f[0] is the
+// stage's first substep.
+cudaError_t launch_substeps_persistent(gwm_b200_ctx* c, const Member& M, const FastArgs* f, int n, bool p_ready) {
   FastStage st{};
   st.n = n;
   st.count = M.gbar;
   st.gen = M.gbar + 1;
   for (int q = 0; q < n; ++q) {
     st.a[q] = f[q];
-    if (!fast_maps(M, f[q], stage_first && q == 0, p_ready, st.m[q])) return cudaErrorInvalidValue;
+    if (!fast_maps(M, f[q], q == 0, p_ready, st.m[q])) return cudaErrorInvalidValue;
   }
-  if (!stage_first) return cudaErrorInvalidValue;  // the launch starts with the stage's first substep
   return launch_fast_stage_tma(st, p_ready, c->stream);
 }
 
@@ -731,7 +730,7 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
         pend[npend++] = f;
       } else {
         if (npend > 0) {
-          LAUNCH(launch_substeps_persistent(c, M, pend, npend, true, p_handoff), "fast substep");
+          LAUNCH(launch_substeps_persistent(c, M, pend, npend, p_handoff), "fast substep");
           npend = 0;
         }
         if (terr) {  // the substep input's column reference, then the substep
@@ -744,7 +743,7 @@ int enqueue_dry(gwm_b200_ctx* c, Member& M) {
       rcur ^= 1;
       dcur = dout;
     }
-    if (npend > 0) LAUNCH(launch_substeps_persistent(c, M, pend, npend, true, p_handoff), "fast substep");
+    if (npend > 0) LAUNCH(launch_substeps_persistent(c, M, pend, npend, p_handoff), "fast substep");
   }
   return GWM_B200_OK;
 }
