@@ -5,7 +5,7 @@
 
 * warm bubble: +2 K cos^2 bubble on a 300 K hydrostatic base (dry);
 * density current: a -15 K cold block (a box at the surface, not the reference's cos^2
-  shape) on the same base (dry);
+  shape) on the same base, in pressure balance (rho*theta kept, the cold air denser; dry);
 * mountain wave: Witch-of-Agnesi hill (400 m, 10 km half width) under a 10 m/s wind in a
   constant-N (0.01 1/s) atmosphere, Rayleigh layer over the top 30 % (dry, terrain);
 * moist warm rain: the moist sounding with warm rain and 12 m/s fallout.
@@ -63,13 +63,17 @@ def c5_members(n: int = 64, seed: int = 5, dt: float = 1.0, substeps: int = 4, s
                                radius_y_fraction=2000.0 / (ny * 1000.0), radius_z_fraction=2000.0 / z_top)
             s = gwm.build_case("hydrostatic_warm_bubble", g, p)
             if kind == "cold_block":
-                rho = s["rho"]
-                th = np.full_like(rho, 300.0)
+                # -15 K in a surface box, in pressure balance: the EOS depends on rho*theta
+                # alone, so rho*theta (and p) keep their hydrostatic values and the cold air
+                # is denser, rho = rho*theta / theta
+                rt = (s["rho"].astype(np.float64) * 300.0)
+                th = np.full(rt.shape, 300.0)
                 zc = (np.arange(nz) + 0.5) * z_top / nz
-                box = np.zeros_like(rho, dtype=bool)
+                box = np.zeros(rt.shape, dtype=bool)
                 box[zc < 2500.0, int(0.4 * ny):int(0.6 * ny), int(0.4 * nx):int(0.6 * nx)] = True
                 th[box] -= 15.0
-                s["rho_theta"] = (rho * th).astype(np.float32)
+                s["rho_theta"] = rt.astype(np.float32)
+                s["rho"] = (rt / th).astype(np.float32)
             spec = gwm.MemberSpec(step=step)
         grids.append(g)
         specs.append(spec)
