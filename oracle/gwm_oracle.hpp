@@ -3,8 +3,9 @@
 // This header is a plain C++ restatement of the reference's time-step hot path
 // (FahrenheitResearch/gpu-wm-next), templated on the arithmetic type T so the
 // same code runs as an FP32 replay of the reference arithmetic and as the FP64
-// judge.  It is NEVER linked into the product: only tests/, the smoke() check
-// and bench.py's CPU-baseline leg load it, always as the checker.
+// standard that both are measured against.  It is NEVER linked into the product:
+// only tests/, the smoke() check and bench.py's CPU-baseline leg load it, always
+// as the checker.
 //
 // Every function cites the reference file:line it restates.  The data layout
 // is the reference's own: one halo-padded array per virtual rank, x fastest,
