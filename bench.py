@@ -622,9 +622,7 @@ def ensemble_line(gwm, torch, stream, dist, world, n=64, steps=20, warmup=3):
             "value": job_throughput(cells, steps, world, ms), "unit": "cell-updates/s",
             "tile_rows": tiles, "cases": {k: kinds.count(k) for k in set(kinds)}, "state_finite": finite,
             "note": "one CUDA graph per step with a branch per member; dt 1 s, 4 substeps (4 s is beyond "
-                    "the acoustic limit of the reference discretisation on these 250 m levels); the -15 K "
-                    "cold-block members leave the scheme's stable range within the timed steps, as the "
-                    "reference's own density-current regression does"}
+                    "the acoustic limit of the reference discretisation on these 250 m levels)"}
 
 
 def max_over_ranks(x, torch, dist, device):
