@@ -144,3 +144,102 @@ def test_layout_mismatch_is_refused(gwm):
         assert torch.count_nonzero(g[:, 0, :]) == 0 and torch.count_nonzero(g[:, 7, :]) == 0  # open in y
     finally:
         dist.destroy_process_group()
+
+
+# ---- the reference's own MPI unit tests (tests/unit/test_mpi_scalar_halo_exchange.cpp,
+# test_mpi_face_halo_exchange.cpp, test_mpi_face_interface_sync.cpp,
+# test_mpi_halo_mismatch_rejects.cpp): a 2 x 2 periodic layout of 8 x 8 x 2, every owned
+# storage value 1000 k + 100 gj + gi of its global index, the MPI operators against the
+# virtual-rank operators on the same fields
+KAT = (8, 8, 2, 1, 2, 2, True, True)
+
+
+def _kat_field(row, nz, h, o):
+    nxl, nyl = int(row[4] - row[3]), int(row[6] - row[5])
+    a = np.zeros((nz + (o == 3), nyl + (o == 2) + 2 * h, nxl + (o == 1) + 2 * h), np.float32)
+    k, j, i = np.meshgrid(np.arange(a.shape[0]), np.arange(nyl + (o == 2)), np.arange(nxl + (o == 1)),
+                          indexing="ij")
+    a[:, h:h + nyl + (o == 2), h:h + nxl + (o == 1)] = 1000 * k + 100 * (row[5] + j) + (row[3] + i)
+    return a
+
+
+def _rank_kat(rank, world, port, q):
+    import datetime
+    import importlib
+
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        comm = importlib.import_module("gpu-wm-next_b200.comm")
+        nx, ny, nz, h, rx, ry, px, py = KAT
+        hc = comm.HaloComm(nx, ny, nz, h, rx, ry, px, py)
+        out = {}
+        for o in (0, 1, 2, 3):
+            t = torch.from_numpy(_kat_field(hc.rows[rank], nz, h, o))
+            out[("exchange", o)] = hc.exchange(t.clone(), o).numpy()
+            if o in (1, 2):
+                out[("sync", o)] = hc.synchronize_owned_face_interfaces(t.clone(), o).numpy()
+        # test_mpi_halo_mismatch_rejects: a layout whose rank count is not the group's
+        try:
+            comm.HaloComm(nx, ny, nz, h, 1, 1, px, py)
+            out["mismatch"] = False
+        except ValueError:
+            out["mismatch"] = True
+        q.put((rank, out))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_reference_mpi_unit_tests(gwm, orc):
+    import torch.multiprocessing as mp
+    comm = __import__("importlib").import_module("gpu-wm-next_b200.comm")
+    nx, ny, nz, h, rx, ry, px, py = KAT
+    world = rx * ry
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_kat, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=180) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    rows = gwm.layout(nx, ny, nz, h, rx, ry, px, py)
+    names = {0: "cell", 1: "x", 2: "y", 3: "z"}
+    for o in (0, 1, 2, 3):
+        fields = [_kat_field(r, nz, h, o) for r in rows]
+        virt = orc.halo([f.astype(np.float64) for f in fields], nx, ny, nz, h, rx, ry, px, py, names[o], "exchange")
+        for r in range(world):  # test_mpi_scalar_halo_exchange / test_mpi_face_halo_exchange
+            np.testing.assert_array_equal(res[r][("exchange", o)], virt[r].astype(np.float32))
+        if o in (1, 2):
+            # test_mpi_face_interface_sync expects the virtual-rank result.  The two agree on
+            # every interface between distinct subdomains; on the periodic wrap interface the
+            # MPI code (halo_exchange.cpp:463-561) averages the two copies, 1000 k + 100 gj + nx
+            # and 1000 k + 100 gj + 0 here, where the virtual-rank sync leaves them, so the
+            # backend follows the MPI code there
+            virt = orc.halo([f.astype(np.float64) for f in fields], nx, ny, nz, h, rx, ry, px, py, names[o], "sync")
+            mpi = comm.mpi_interface_sync_reference(fields, rows, h, o)
+            for r in range(world):
+                got = res[r][("sync", o)]
+                np.testing.assert_array_equal(got, mpi[r])
+                row = rows[r]
+                nxl, nyl = int(row[4] - row[3]), int(row[6] - row[5])
+                interior = np.ones(got.shape, bool)  # drop the wrap interfaces
+                if o == 1:
+                    if row[3] == 0:
+                        interior[:, :, h] = False
+                    if row[4] == nx:
+                        interior[:, :, h + nxl] = False
+                else:
+                    if row[5] == 0:
+                        interior[:, h, :] = False
+                    if row[6] == ny:
+                        interior[:, h + nyl, :] = False
+                np.testing.assert_array_equal(got[interior], virt[r].astype(np.float32)[interior])
+    assert all(res[r]["mismatch"] for r in range(world))
