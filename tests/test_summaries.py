@@ -154,3 +154,37 @@ def test_prepared_summary_layout(gwm):
     assert doc["startup_balance"]["max_rel_eos"] == 1.5e-7
     assert doc["initial"] == json.loads(initial) and doc["final"] == json.loads(final)
     assert doc["initial"] != doc["final"]
+
+
+def test_runtime_summary_reference_kats(gwm):
+    """tests/unit/test_runtime_summary.cpp: a 2 x 1 x 1 column pair (1 km deep), rho 1,
+    theta 300, qv masses 0.010 / 0.012, qc 0.001 in the first column, qr 0.002 in the
+    second, 0.75 mm accumulated over the second."""
+    g = gwm.GridSpec(2, 1, 1, dx=1000.0, dy=1000.0, z_top=1000.0)
+    s = gwm.build_case("constant", g, gwm.CaseParams(rho_background=1.0, theta_background=300.0), moist=True)
+    s["qv"][0, 0, :] = np.float32([0.010, 0.012])
+    s["qc"][0, 0, :] = np.float32([0.001, 0.0])
+    s["qr"][0, 0, :] = np.float32([0.0, 0.002])
+    s["precip"] = np.array([[0.0, np.float32(0.75)]])
+    with gwm.Model(g, gwm.MemberSpec(step=gwm.StepConfig(dt=1.0, fast_substeps=1), moist=True)) as m:
+        m.upload(s)
+        summ = m.runtime_summary()
+    mo = summ["moisture"]
+    assert mo["vapor_water_path_sum_kg_m2"] == pytest.approx(0.010 * 1000 + 0.012 * 1000, abs=1e-5)
+    assert mo["cloud_water_path_sum_kg_m2"] == pytest.approx(1.0, abs=1e-5)
+    assert mo["rain_water_path_sum_kg_m2"] == pytest.approx(2.0, abs=1e-5)
+    assert mo["condensed_water_path_sum_kg_m2"] == pytest.approx(3.0, abs=1e-5)
+    assert mo["total_water_path_sum_kg_m2"] == pytest.approx(25.0, abs=1e-5)
+    assert mo["accumulated_surface_precipitation_sum_mm"] == pytest.approx(0.75, abs=1e-6)
+    assert mo["mean_surface_precipitation_mm"] == pytest.approx(0.375, abs=1e-6)
+    assert mo["max_surface_precipitation_mm"] == pytest.approx(0.75, abs=1e-6)
+    tr = summ["tracers"]
+    assert len(tr) == 3
+    for name, lo, hi in (("specific_humidity", 0.010, 0.012), ("cloud_water_mixing_ratio", 0.0, 0.001),
+                         ("rain_water_mixing_ratio", 0.0, 0.002)):
+        assert tr[name]["mixing_ratio"]["min"] == pytest.approx(lo, abs=1e-6)
+        assert tr[name]["mixing_ratio"]["max"] == pytest.approx(hi, abs=1e-6)
+        assert tr[name]["positive"] is True
+    for key in ('"specific_humidity"', '"total_water_path_sum_kg_m2"', '"accumulated_surface_precipitation_sum_mm"',
+                '"mixing_ratio"'):
+        assert key in summ["_json"]
