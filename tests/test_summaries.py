@@ -188,3 +188,22 @@ def test_runtime_summary_reference_kats(gwm):
     for key in ('"specific_humidity"', '"total_water_path_sum_kg_m2"', '"accumulated_surface_precipitation_sum_mm"',
                 '"mixing_ratio"'):
         assert key in summ["_json"]
+
+
+def test_dry_summary_reference_kats(gwm):
+    """tests/unit/test_dry_diagnostics.cpp: summarize_dry_states of a constant 4 x 3 x 2
+    state (rho 1.5, theta 300, velocities 2, -1, 0.25), face totals over every storage face
+    (5 X faces per row, 4 Y faces per column, 3 Z faces per column)."""
+    g = gwm.GridSpec(4, 3, 2, dx=1000.0, dy=1000.0, z_top=2000.0)
+    s = gwm.build_case("constant", g, gwm.CaseParams(rho_background=1.5, theta_background=300.0, u_background=2.0,
+                                                     v_background=-1.0, w_background=0.25))
+    with gwm.Model(g, gwm.MemberSpec(step=gwm.StepConfig(dt=1.0, fast_substeps=1))) as m:
+        m.upload(s)
+        b = m.budgets()
+    assert b["total_dry_mass"] == pytest.approx(4 * 3 * 2 * 1.5, abs=1e-6)
+    assert b["total_rho_theta_m"] == pytest.approx(4 * 3 * 2 * 1.5 * 300.0, abs=1e-6)
+    assert b["total_horizontal_momentum_x"] == pytest.approx(5 * 3 * 2 * 1.5 * 2.0, abs=1e-6)
+    assert b["total_horizontal_momentum_y"] == pytest.approx(4 * 4 * 2 * 1.5 * -1.0, abs=1e-6)
+    assert b["total_vertical_momentum"] == pytest.approx(4 * 3 * 3 * 1.5 * 0.25, abs=1e-6)
+    for key, val in (("rho", 1.5), ("theta", 300.0), ("u", 3.0), ("v", -1.5), ("w", 0.375)):
+        assert b[f"{key}_min"] == pytest.approx(val, abs=1e-6) and b[f"{key}_max"] == pytest.approx(val, abs=1e-6)
