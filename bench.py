@@ -55,16 +55,60 @@ def member_spec(gwm):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region.
 
-    def __init__(self, index=0):
+    Reads NVML in a polling thread (10 ms period; read-only queries) on the NVML device
+    whose PCI bus id matches the CUDA device, so that a sub-second timed region still
+    gets tens of samples; falls back to an `nvidia-smi -lms 100` pipe when NVML is
+    unavailable."""
+
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
+
+    def __init__(self, index=0, period_s=0.01):
         self.index = index
-        self.samples = []
+        self.period_s = period_s
+        self.samples = []          # (sm_mhz, sm_max_mhz, {reason names})
         self._stop = threading.Event()
         self._proc = None
+        self._thread = None
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            p = torch.cuda.get_device_properties(self.index)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+        try:
+            nv, h = self._nvml_handle()
+            smmax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        except Exception:
+            self._start_smi()
+            return
+        self.source = "nvml"
+
+        def poll():
+            while not self._stop.is_set():
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                except Exception:
+                    break
+                self.samples.append((float(sm), float(smmax), {n for n, b in self.REASONS if bits & b}))
+                self._stop.wait(self.period_s)
+
+        self._thread = threading.Thread(target=poll, daemon=True)
+        self._thread.start()
+
+    def _start_smi(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
         try:
@@ -74,41 +118,45 @@ class ClockSampler:
         except OSError:
             self._proc = None
             return
-        threading.Thread(target=self._read, daemon=True).start()
+        self.source = "nvidia-smi"
 
-    def _read(self):
-        for line in self._proc.stdout:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 7:
-                self.samples.append(parts)
+        def read():
+            for line in self._proc.stdout:
+                s = [x.strip() for x in line.split(",")]
+                if len(s) >= 6 and s[0].replace(".", "").isdigit() and s[1].replace(".", "").isdigit():
+                    self.samples.append((float(s[0]), float(s[1]),
+                                         {n for (n, _), v in zip(self.REASONS, s[2:6]) if v == "Active"}))
+
+        self._thread = threading.Thread(target=read, daemon=True)
+        self._thread.start()
 
     def wait_first(self, timeout):
         t = time.time()
-        while self._proc and not self.samples and time.time() - t < timeout:
-            time.sleep(0.05)
+        while self.source and not self.samples and time.time() - t < timeout:
+            time.sleep(0.01)
 
     def mark(self):
         """Only samples taken after this point describe the timed region."""
         self._start = len(self.samples)
 
     def stop(self):
+        self._stop.set()
         if self._proc:
             self._proc.terminate()
             try:
                 self._proc.wait(timeout=5)
             except Exception:
                 self._proc.kill()
+        if self._thread:
+            self._thread.join(timeout=5)
 
     def summary(self):
-        self.samples = self.samples[getattr(self, "_start", 0):]
-        if not self.samples:
+        s = self.samples[getattr(self, "_start", 0):]
+        if not s:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i] == "Active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        return {"sm_mhz": float(np.median([x[0] for x in s])), "sm_max_mhz": max(x[1] for x in s),
+                "reasons": sorted(set().union(*(x[2] for x in s))), "samples": len(s),
+                "source": self.source}
 
 
 def load_peaks():

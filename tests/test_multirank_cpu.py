@@ -109,3 +109,41 @@ def test_reference_arm_loads_no_product_code():
     assert ref["impl"] == "reference" and ref["value"] > 0 and ref["sampled_grid"]["nx"] == 16
     assert ref["config"]["nx"] == 1024 and ref["cpu_baseline"]["kind"] == "port"
     assert flags == {"pkg": False, "so": False, "torch": False}, flags
+
+
+def test_clock_sampler_decodes_nvml_reasons(monkeypatch):
+    # The clock record reads NVML only; a fake NVML module stands in for the device.
+    import types
+    import time
+
+    sys.path.insert(0, ROOT)
+    import bench
+    seq = iter([(1965, 0x0), (1965, 0x4), (1800, 0x4 | 0x8)] + [(1965, 0x1)] * 10000)
+    fake = types.SimpleNamespace(
+        NVML_CLOCK_SM=1, nvmlInit=lambda: None,
+        nvmlDeviceGetHandleByIndex=lambda i: ("dev", i),
+        nvmlDeviceGetHandleByPciBusId=lambda b: ("dev", b),
+        nvmlDeviceGetMaxClockInfo=lambda h, k: 1965)
+    cur = {}
+
+    def clock(h, k):
+        cur["s"] = next(seq)
+        return cur["s"][0]
+
+    fake.nvmlDeviceGetClockInfo = clock
+    fake.nvmlDeviceGetCurrentClocksEventReasons = lambda h: cur["s"][1]
+    monkeypatch.setitem(sys.modules, "pynvml", fake)
+    c = bench.ClockSampler(0, period_s=0.001)
+    c.start()
+    c.wait_first(2.0)
+    time.sleep(0.05)
+    c.stop()
+    s = c.summary()
+    assert c.source == "nvml" and s["samples"] >= 4
+    assert s["sm_max_mhz"] == 1965 and s["sm_mhz"] == 1965
+    assert s["reasons"] == ["hw_slowdown", "sw_power_cap"]
+    # samples before mark() do not describe the timed region
+    c2 = bench.ClockSampler(0)
+    c2.samples = [(1200.0, 1965.0, {"hw_slowdown"}), (1965.0, 1965.0, set())]
+    c2._start = 1
+    assert c2.summary()["reasons"] == [] and c2.summary()["sm_mhz"] == 1965.0
