@@ -306,6 +306,25 @@ bool build_substep_maps(Member& M) {
   return ok;
 }
 
+// Maps of every buffer the terrain TMA substep may read (false if unavailable).
+bool build_terrain_substep_maps(Member& M) {
+  M.tmaps.clear();
+  const int* boxes[3] = {kTmaCellBox, kTmaFaceBox, kTmaOwnBox};
+  auto add = [&](const float* buf, int kind) {
+    CUtensorMap m;
+    if (!encode_field_map(&m, buf, M.g, boxes[kind][0], boxes[kind][1])) return false;
+    M.tmaps.emplace_back(buf, kind, m);
+    return true;
+  };
+  bool ok = add(M.zc, 0);
+  for (int i = 0; i < 2; ++i) {
+    ok = ok && add(M.R[i], 0) && add(M.TH[i], 0) && add(M.P[i], 0) && add(M.R[i], 2) && add(M.TH[i], 2);
+    ok = ok && add(M.D[i][0], 1) && add(M.D[i][1], 1) && add(M.D[i][2], 2);
+  }
+  if (!ok) M.tmaps.clear();
+  return ok;
+}
+
 int alloc_member(gwm_b200_ctx* c, Member& M) {
   const gwm_b200_grid_desc& d = M.gd;
   Geom& g = M.g;
@@ -392,7 +411,9 @@ int alloc_member(gwm_b200_ctx* c, Member& M) {
     CK(cudaMemcpy(M.idf, idf.data(), idf.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
   if ((size_t)(p - M.block) > total) return fail(c, GWM_B200_ERR_ARG, "internal: buffer plan overflow");
-  if (!M.terrain_active) build_substep_maps(M);  // empty when TMA descriptors are unavailable
+  // empty when TMA descriptors are unavailable
+  if (M.terrain_active) build_terrain_substep_maps(M);
+  else build_substep_maps(M);
   CK(cudaStreamSynchronize(c->stream));
   return GWM_B200_OK;
 }
@@ -441,8 +462,8 @@ cudaError_t launch_stage(gwm_b200_ctx* c, const Member& M, const SlowArgs& a, bo
   return launch_slow(a, terr, c->stream, c->slow_tile_rows == kSlowTma ? 16 : c->slow_tile_rows);
 }
 
-// One acoustic substep: the TMA-fed kernel when selected on flat terrain, else the
-// owned-tile or overlapped-tile kernels.
+// One acoustic substep: the TMA-fed kernels when selected (flat terrain or terrain),
+// else the owned-tile or overlapped-tile kernels.
 // p_ready: the first substep's p' (with its halo) is in f.p_in, written by the slow stage
 // TMA descriptors of one substep's inputs (k_fast_tma); false when one is missing
 bool fast_maps(const Member& M, const FastArgs& f, bool first, bool p_ready, FastMaps& m) {
@@ -468,8 +489,28 @@ bool fast_maps(const Member& M, const FastArgs& f, bool first, bool p_ready, Fas
   return true;
 }
 
+// TMA descriptors of one terrain substep's inputs (k_fast_terrain_tma); false when one is missing
+bool fast_terrain_maps(const Member& M, const FastArgs& f, bool first, FastTerrainMaps& m) {
+  const CUtensorMap* rho = M.tmap(f.rho_in, first ? 0 : 2);
+  const CUtensorMap* th = M.tmap(f.th, first ? 0 : 2);
+  const CUtensorMap* z = M.tmap(f.zc, 0);
+  const CUtensorMap* pm = first ? nullptr : M.tmap(f.p_in, 0);
+  const CUtensorMap* du = first ? nullptr : M.tmap(f.du_in, 1);
+  const CUtensorMap* dv = first ? nullptr : M.tmap(f.dv_in, 1);
+  const CUtensorMap* dw = first ? nullptr : M.tmap(f.dw_in, 2);
+  if (!rho || !th || !z || (!first && (!pm || !du || !dv || !dw))) return false;
+  m.rho = *rho; m.th = *th; m.z = *z;
+  if (!first) { m.p = *pm; m.du = *du; m.dv = *dv; m.dw = *dw; }
+  return true;
+}
+
 cudaError_t launch_substep(gwm_b200_ctx* c, const Member& M, const FastArgs& f, bool first, bool terr,
                            bool p_ready = false) {
+  if (terr && fast_tma_path(c)) {
+    FastTerrainMaps m{};
+    if (!fast_terrain_maps(M, f, first, m)) return cudaErrorInvalidValue;
+    return launch_fast_terrain_tma(f, m, first, c->stream);
+  }
   if (!terr && fast_tma_path(c)) {
     FastMaps m{};
     if (!fast_maps(M, f, first, p_ready, m)) return cudaErrorInvalidValue;
@@ -875,7 +916,8 @@ int gwm_b200_create(const gwm_b200_grid_desc* grids, const gwm_b200_member_desc*
   cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { delete c; return GWM_B200_ERR_CUDA; }
   c->stream = c->own_stream;
-  if (init_fast_tma() != cudaSuccess || init_slow_tma() != cudaSuccess || init_tracer_tma() != cudaSuccess) {
+  if (init_fast_tma() != cudaSuccess || init_fast_terrain_tma() != cudaSuccess || init_slow_tma() != cudaSuccess ||
+      init_tracer_tma() != cudaSuccess) {
     cudaStreamDestroy(c->own_stream);
     delete c;
     return GWM_B200_ERR_CUDA;
@@ -976,7 +1018,7 @@ int gwm_b200_set_tile(gwm_b200_ctx* c, int kernel, int rows) {
   if ((kernel == 1 && (rows == kFastTma || rows == kFastStage)) || (kernel == 0 && rows == kSlowTma) ||
       (kernel == 2 && rows == kTracerTma))
     for (const auto& M : c->m)
-      if (!M.terrain_active && M.tmaps.empty())
+      if (M.tmaps.empty())
         return fail(c, GWM_B200_ERR_ARG, "TMA substep unavailable (tensor-map encoder not found)");
   drop_graph(c);
   (kernel == 0 ? c->slow_tile_rows : kernel == 1 ? c->fast_tile_rows : c->tracer_tile_rows) = rows;

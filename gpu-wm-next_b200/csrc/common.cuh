@@ -56,6 +56,15 @@ __device__ __forceinline__ float eos_rho(float p, float th) {
   return p / fmaxf(kRd * th * ex, 1.0e-6f);
 }
 __device__ __forceinline__ float dry_cp() { return kRd / kKappa; }
+// One-sided / centred dp/dz of a column (terrain pressure gradient):
+// dry_pressure_gradient.cu:37-73.
+__device__ __forceinline__ float column_dpdz(int k, int nz, float pm, float pc, float pn, float zm,
+                                             float zcc, float zn) {
+  if (nz == 1) return 0.0f;
+  if (k == 0) return (pn - pc) / fmaxf(zn - zcc, 1.0e-6f);
+  if (k + 1 == nz) return (pc - pm) / fmaxf(zcc - zm, 1.0e-6f);
+  return (pn - pm) / fmaxf(zn - zm, 1.0e-6f);
+}
 
 // ---------------------------------------------------------------------------
 // Pressure perturbation about an FP64 base state.  The reference EOS

@@ -87,15 +87,6 @@ __device__ __forceinline__ SlowQ0 slow_q0(const SlowArgs& a, int base, int kk, b
   return q;
 }
 
-// One-sided / centred dp/dz of a column: dry_pressure_gradient.cu:37-73.
-__device__ __forceinline__ float column_dpdz(int k, int nz, float pm, float pc, float pn, float zm,
-                                             float zcc, float zn) {
-  if (nz == 1) return 0.0f;
-  if (k == 0) return (pn - pc) / fmaxf(zn - zcc, 1.0e-6f);
-  if (k + 1 == nz) return (pc - pm) / fmaxf(zcc - zm, 1.0e-6f);
-  return (pn - pm) / fmaxf(zn - zm, 1.0e-6f);
-}
-
 template <bool TERRAIN, int SBY>
 __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
   constexpr int SNT = BX * SBY, SNW = SNT / 32;
@@ -238,7 +229,9 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
         } else {
           float u1 = fp::update(cc.uf, a.dt, t_u, -1.0e30f);
           if (blend) u1 = fp::blend(a.wa, q0c.u, a.wb, u1);
-          store_tile(a.o_u, g, kFaceX, gi, gj, k, u1, edge);
+          // periodic face nx is written by face 0's mirror store, never read here (the
+          // output may be the blend partner's buffer)
+          if (!(g.per_x && gi == nx)) store_tile(a.o_u, g, kFaceX, gi, gj, k, u1, edge);
         }
       }
       // ---- Y face: K18 (dry_momentum_flux.cu:158-235) + K22 (dry_pressure_gradient.cu:125-173)
@@ -272,7 +265,7 @@ __global__ void __launch_bounds__(BX * SBY) k_slow_stage(const SlowArgs a) {
         } else {
           float v1 = fp::update(cc.vf, a.dt, t_v, -1.0e30f);
           if (blend) v1 = fp::blend(a.wa, q0c.v, a.wb, v1);
-          store_tile(a.o_v, g, kFaceY, gi, gj, k, v1, edge);
+          if (!(g.per_y && gj == ny)) store_tile(a.o_v, g, kFaceY, gi, gj, k, v1, edge);
         }
       }
       // ---- Z face k: K19 (dry_momentum_flux.cu:237-312) + K3 buoyancy (dry_core.cu:146-187)
@@ -394,13 +387,25 @@ __global__ void __launch_bounds__(128) k_column_reference(const FastArgs a) {
     } else {
       const float dzk = z - zb;
       float pn = fmaxf(1.0f, fp::fma(-fp::mul(a.gravity, rref), dzk, pref));
+      // Four fixed-point iterations, then the density of the result.  An iteration that
+      // returns its own input is a fixed point: every later iteration repeats it, and the
+      // final density is the one just evaluated, so the loop stops there with the same
+      // result (the iterations contract by about g dz / (2 c^2) ~ 1e-2 and reach the
+      // FP32 fixed point after two or three of the four).
+      float rn = 0.0f;
+      bool fixed = false;
       for (int it = 0; it < 4; ++it) {
-        const float rn = eos_rho(pn, thp);
-        pn = fp::fma(-fp::mul(fp::mul(a.gravity, 0.5f), fp::add(rref, rn)), dzk, pref);
-        pn = fmaxf(pn, 1.0f);
+        rn = eos_rho(pn, thp);
+        const float pq =
+            fmaxf(fp::fma(-fp::mul(fp::mul(a.gravity, 0.5f), fp::add(rref, rn)), dzk, pref), 1.0f);
+        if (pq == pn) {
+          fixed = true;
+          break;
+        }
+        pn = pq;
       }
       pref = pn;
-      rref = eos_rho(pn, thp);
+      rref = fixed ? rn : eos_rho(pn, thp);
     }
     a.col_pref[o] = pref;
     a.col_rref[o] = rref;
@@ -435,8 +440,11 @@ __global__ void __launch_bounds__(BX * FBY) k_fast_substep(const FastArgs a) {
   // faces computed by this thread (owned or the tile's far-edge duplicate)
   const bool do_u = tx >= 1 && ty >= 1 && ty <= FBY - 2 && gi >= 0 && gi <= nx && gj >= 0 && gj < ny;
   const bool do_v = ty >= 1 && tx >= 1 && tx <= BX - 2 && gi >= 0 && gi < nx && gj >= 0 && gj <= ny;
-  const bool own_u = do_u && tx <= BX - 2;
-  const bool own_v = do_v && ty <= FBY - 2;
+  // stored faces: owned ones, except periodic faces nx / ny, which face 0's mirror store
+  // writes (in the stand-alone fast modes the step result overwrites the base momenta the
+  // substep reads, so face nx must not be read after that store and written again)
+  const bool own_u = do_u && tx <= BX - 2 && !(g.per_x && gi == nx);
+  const bool own_v = do_v && ty <= FBY - 2 && !(g.per_y && gj == ny);
   const bool skip_u = (gi == 0 || gi == nx) && !g.per_x;
   const bool skip_v = (gj == 0 || gj == ny) && !g.per_y;
   const int base = valid ? gidx(g, gi, gj, 0) : 0;

@@ -87,6 +87,15 @@ struct FastMaps {
   CUtensorMap p;           // box 40 x 18: p'(rho_in) with the halo ring (loaded unless the
                            // first substep derives it)
 };
+// TMA descriptors of one acoustic substep on terrain (k_fast_terrain_tma), same layout.
+struct FastTerrainMaps {
+  CUtensorMap rho, th;  // first substep of a stage: box 40 x 18 (cells with the halo
+                        // ring); otherwise box 32 x 16 (owned cells)
+  CUtensorMap z;        // box 40 x 18: cell-centre heights
+  CUtensorMap p;        // box 40 x 18: full pressure of rho_in (not the first substep)
+  CUtensorMap du, dv;   // box 36 x 17 (not the first substep)
+  CUtensorMap dw;       // box 32 x 16 (not the first substep)
+};
 // Box extents (x, y) of the maps above.
 constexpr int kTmaCellBox[2] = {40, 18};
 constexpr int kTmaFaceBox[2] = {36, 17};
@@ -115,6 +124,12 @@ cudaError_t init_slow_tma();
 // first: the first substep of a stage (no increments in); p_ready: its p' (with the
 // halo ring) is in a.p_in, written by the slow stage, instead of derived from rho, theta
 cudaError_t launch_fast_tma(const FastArgs& a, const FastMaps& m, bool first, bool p_ready, cudaStream_t s);
+// Acoustic substep on terrain fed by TMA tile loads (owned 32 x 16 tiles): the
+// arithmetic of the overlapped-tile terrain kernel.  Needs a.col_pref / a.col_rref
+// (launch_column_reference of a.rho_in first); inner substeps (final_kind 0) store the
+// full pressure of their result in a.p_out, which the next substep loads as a.p_in.
+cudaError_t launch_fast_terrain_tma(const FastArgs& a, const FastTerrainMaps& m, bool first, cudaStream_t s);
+cudaError_t init_fast_terrain_tma();
 // K11 build_column_hydrostatic_reference_kernel (dry_fast_modes.cu:108-158) of a.rho_in
 // and a.th into a.col_pref / a.col_rref: one thread per owned column, bottom to top.
 cudaError_t launch_column_reference(const FastArgs& a, cudaStream_t s);
