@@ -186,6 +186,7 @@ def lib():
     L.gwm_b200_set_stream.argtypes = [vp, vp]
     L.gwm_b200_upload.argtypes = [vp, C.c_int, C.POINTER(_Fields)]
     L.gwm_b200_download.argtypes = [vp, C.c_int, C.POINTER(_Fields)]
+    L.gwm_b200_step_host.argtypes = [vp, C.POINTER(_Fields), C.POINTER(_Fields)]
     L.gwm_b200_slow_tendencies.argtypes = [vp, C.c_int, C.POINTER(_Fields)]
     L.gwm_b200_budgets.argtypes = [vp, C.c_int, C.POINTER(_Budget)]
     L.gwm_b200_profile.argtypes = [vp, C.c_int]
@@ -257,7 +258,7 @@ def lib():
 # C-ABI symbols the header declares (checked by the CPU test-suite).
 EXPORTED = ("gwm_b200_create", "gwm_b200_destroy", "gwm_b200_last_error", "gwm_b200_set_stream",
             "gwm_b200_synchronize", "gwm_b200_use_graph", "gwm_b200_upload", "gwm_b200_download",
-            "gwm_b200_step", "gwm_b200_advance_dry", "gwm_b200_advance_tracers",
+            "gwm_b200_step", "gwm_b200_step_host", "gwm_b200_advance_dry", "gwm_b200_advance_tracers",
             "gwm_b200_warm_rain", "gwm_b200_fast_modes", "gwm_b200_slow_tendencies",
             "gwm_b200_budgets", "gwm_b200_launch_count", "gwm_b200_profile", "gwm_b200_profile_read", "gwm_b200_set_tile", "gwm_b200_get_tile", "gwm_b200_set_boundary_state", "gwm_b200_set_concurrent",
             "gwm_b200_apply_reference_boundaries", "gwm_b200_set_damping", "gwm_b200_rain_record",
@@ -731,6 +732,40 @@ class Model:
     def step(self, nsteps: int = 1):
         """The prepared-case driver loop (gwm_prepared_case_driver.cpp:427-463)."""
         self._check(lib().gwm_b200_step(self._h, nsteps), "step")
+
+    def step_host(self, state: Dict[str, np.ndarray], out: Optional[Dict[str, np.ndarray]] = None
+                  ) -> Dict[str, np.ndarray]:
+        """One step from host arrays to host arrays (single-member models): the full state
+        in, one ``step``, the full state out, with the copies overlapping the step's phases.
+        ``out`` may be ``state`` itself; pinned (page-locked) arrays copy at full PCIe rate."""
+        if len(self.grids) != 1:
+            raise ValueError("step_host takes a single-member model")
+        g = self.grids[0]
+        sh = g.shapes()
+        keys = STATE_KEYS + ((TRACER_KEYS + ("precip",)) if self.members[0].moist else ())
+        out = {} if out is None else out
+        fin, fout, keep = _Fields(), _Fields(), []
+        for k in keys:
+            dtype = np.float64 if k == "precip" else np.float32
+            if k not in state:
+                raise ValueError(f"step_host needs {k}")
+            a = np.ascontiguousarray(state[k], dtype=dtype)
+            if a.shape != sh[k]:
+                raise ValueError(f"{k}: shape {a.shape} != {sh[k]}")
+            keep.append(a)
+            if k not in out:
+                out[k] = np.empty(sh[k], dtype=dtype)
+            o = out[k]
+            if o.shape != sh[k] or o.dtype != dtype or not o.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"step_host target {k} must be a C-contiguous {dtype} array of {sh[k]}")
+            if k == "precip":
+                fin.precip = a.ctypes.data_as(C.POINTER(C.c_double))
+                fout.precip = o.ctypes.data_as(C.POINTER(C.c_double))
+            else:
+                setattr(fin, _C_NAMES[k], _fptr(a))
+                setattr(fout, _C_NAMES[k], _fptr(o))
+        self._check(lib().gwm_b200_step_host(self._h, C.byref(fin), C.byref(fout)), "step_host")
+        return out
 
     def advance_dry_state_ssprk3(self, nsteps: int = 1):
         self._check(lib().gwm_b200_advance_dry(self._h, nsteps), "advance_dry_state_ssprk3")

@@ -80,6 +80,7 @@ struct Member {
   double* base = nullptr;            // FP64 base state of the perturbation EOS
   bool base_valid = false;
   float* staging = nullptr;
+  float* io_stage = nullptr;         // host-to-host stepping: one staging buffer per field
   double* red_part = nullptr;
   ReduceOut* red_out = nullptr;
   int ring = 0;
@@ -148,6 +149,10 @@ struct gwm_b200_ctx {
   std::vector<cudaStream_t> mstreams;
   std::vector<cudaEvent_t> mjoin;
   cudaEvent_t mfork = nullptr;
+  // host-to-host stepping: copy-in and copy-out streams, and their events (the fields in,
+  // the end of the dry step, the end of the step)
+  cudaStream_t cin = nullptr, cout = nullptr;
+  std::vector<cudaEvent_t> io_ev;
 };
 
 namespace {
@@ -970,7 +975,11 @@ void gwm_b200_destroy(gwm_b200_ctx* c) {
     if (M.sur) cudaFree(M.sur);
     for (char* b : M.extra) cudaFree(b);
     if (M.bcache_block) cudaFree(M.bcache_block);
+    if (M.io_stage) cudaFree(M.io_stage);
   }
+  if (c->cin) cudaStreamDestroy(c->cin);
+  if (c->cout) cudaStreamDestroy(c->cout);
+  for (auto ev : c->io_ev) cudaEventDestroy(ev);
   for (auto st : c->mstreams) cudaStreamDestroy(st);
   for (auto ev : c->mjoin) cudaEventDestroy(ev);
   if (c->mfork) cudaEventDestroy(c->mfork);
@@ -1743,6 +1752,112 @@ int gwm_b200_profile_read(const gwm_b200_ctx* c, int kind, double* total_ms, lon
 int gwm_b200_step(gwm_b200_ctx* c, int nsteps) {
   if (!c || nsteps < 0) return GWM_B200_ERR_ARG;
   return run_steps(c, nsteps, enqueue_full_step);
+}
+
+// One full step of a single-member context from host buffers to host buffers: the state
+// is copied in from `in`, advanced as gwm_b200_step does, and copied out to `out` (the
+// same buffers may be given for both).  The copies overlap the step's phases on two copy
+// streams.  The moisture fields and the precipitation go up while the dry step runs (it
+// does not read them), and rho and the momenta, which neither the tracers nor the warm
+// rain change, come down while those run.  Results equal upload + step + download.
+int gwm_b200_step_host(gwm_b200_ctx* c, const gwm_b200_fields* in, gwm_b200_fields* out) {
+  if (!c || !in || !out) return GWM_B200_ERR_ARG;
+  if (c->m.size() != 1) return fail(c, GWM_B200_ERR_ARG, "host-to-host stepping takes a single-member context");
+  Member& M = c->m[0];
+  const Geom& g = M.g;
+  const bool moist = M.md.moist != 0;
+  const float* src[8] = {in->rho_d, in->rho_theta_m, in->mom_u, in->mom_v, in->mom_w, in->qv, in->qc, in->qr};
+  float* dst[8] = {out->rho_d, out->rho_theta_m, out->mom_u, out->mom_v, out->mom_w, out->qv, out->qc, out->qr};
+  float* dev[8] = {M.Q[0], M.Q[1], M.Q[2], M.Q[3], M.Q[4], M.T0[0], M.T0[1], M.T0[2]};
+  constexpr int orient[8] = {kCell, kCell, kFaceX, kFaceY, kFaceZ, kCell, kCell, kCell};
+  const int nf = moist ? 8 : 5;
+  for (int f = 0; f < nf; ++f)
+    if (!src[f] || !dst[f]) return fail(c, GWM_B200_ERR_ARG, "host-to-host stepping needs every field of the state");
+  if (moist && (!in->precip || !out->precip))
+    return fail(c, GWM_B200_ERR_ARG, "host-to-host stepping of a moist member needs the precipitation");
+  if (!moist && (in->qv || in->qc || in->qr || in->precip))
+    return fail(c, GWM_B200_ERR_ARG, "tracer fields given to a dry member");
+  const size_t owned_max = (size_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+  if (!c->cin) {
+    CK(cudaStreamCreateWithFlags(&c->cin, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->cout, cudaStreamNonBlocking));
+    c->io_ev.assign(11, nullptr);
+    for (auto& ev : c->io_ev) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  }
+  if (!M.io_stage) CK(cudaMalloc(&M.io_stage, 8 * owned_max * sizeof(float)));
+  auto stage = [&](int f) { return M.io_stage + (size_t)f * owned_max; };
+  auto count = [&](int f) {
+    const int o = orient[f];
+    return (size_t)(g.nx + (o == kFaceX)) * (g.ny + (o == kFaceY)) * (g.nz + (o == kFaceZ));
+  };
+  cudaEvent_t* ev_in = c->io_ev.data();  // [0..8]: field f (8: precipitation) is on the device
+  cudaEvent_t ev_dry = c->io_ev[9], ev_end = c->io_ev[10];
+  const size_t n2 = (size_t)g.nx * g.ny;
+  c->cur_launches = 0;
+  // the dry fields up, each packed as soon as it lands
+  for (int f = 0; f < 5; ++f) {
+    CK(cudaMemcpyAsync(stage(f), src[f], count(f) * sizeof(float), cudaMemcpyHostToDevice, c->cin));
+    CK(cudaEventRecord(ev_in[f], c->cin));
+    CK(cudaStreamWaitEvent(c->stream, ev_in[f], 0));
+    CK(launch_pack(g, orient[f], stage(f), dev[f], c->stream));
+  }
+  // the moisture fields up behind them, during the dry step
+  if (moist) {
+    for (int f = 5; f < 8; ++f) {
+      CK(cudaMemcpyAsync(stage(f), src[f], count(f) * sizeof(float), cudaMemcpyHostToDevice, c->cin));
+      CK(cudaEventRecord(ev_in[f], c->cin));
+    }
+    CK(cudaMemcpyAsync(M.precip, in->precip, n2 * sizeof(double), cudaMemcpyHostToDevice, c->cin));
+    CK(cudaMemsetAsync(M.pcomp, 0, n2 * sizeof(double), c->cin));
+    CK(cudaEventRecord(ev_in[8], c->cin));
+  }
+  M.theta_valid = false;
+  M.base_valid = false;
+  int rc = ensure_base(c, M);
+  if (rc) return rc;
+  rc = enqueue_theta(c, M);
+  if (rc) return rc;
+  rc = enqueue_dry(c, M);
+  if (rc) return rc;
+  CK(cudaEventRecord(ev_dry, c->stream));
+  // rho and the momenta down while the tracers and the warm rain run
+  CK(cudaStreamWaitEvent(c->cout, ev_dry, 0));
+  for (int f : {0, 2, 3, 4}) {
+    CK(launch_unpack(g, orient[f], dev[f], stage(f), c->cout));
+    CK(cudaMemcpyAsync(dst[f], stage(f), count(f) * sizeof(float), cudaMemcpyDeviceToHost, c->cout));
+  }
+  if (moist) {
+    for (int f = 5; f < 9; ++f) CK(cudaStreamWaitEvent(c->stream, ev_in[f], 0));
+    for (int f = 5; f < 8; ++f) CK(launch_pack(g, orient[f], stage(f), dev[f], c->stream));
+  }
+  if (M.md.enable_tracer_transport && !M.reg.empty()) {
+    rc = enqueue_tracers(c, M);
+    if (rc) return rc;
+  }
+  if (moist && M.md.enable_warm_rain) {
+    rc = enqueue_rain(c, M, 1);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(ev_end, c->stream));
+  // the rest down after the step
+  CK(cudaStreamWaitEvent(c->cout, ev_end, 0));
+  std::vector<double> comp;
+  for (int f = 1; f < nf; f += (f == 1 ? 4 : 1)) {  // rho*theta, then the tracers
+    CK(launch_unpack(g, orient[f], dev[f], stage(f), c->cout));
+    CK(cudaMemcpyAsync(dst[f], stage(f), count(f) * sizeof(float), cudaMemcpyDeviceToHost, c->cout));
+  }
+  if (moist) {
+    comp.resize(n2);
+    CK(cudaMemcpyAsync(out->precip, M.precip, n2 * sizeof(double), cudaMemcpyDeviceToHost, c->cout));
+    CK(cudaMemcpyAsync(comp.data(), M.pcomp, n2 * sizeof(double), cudaMemcpyDeviceToHost, c->cout));
+  }
+  CK(cudaStreamSynchronize(c->cout));
+  CK(cudaStreamSynchronize(c->stream));
+  c->launches = c->cur_launches;
+  rc = check_device_errors(c);
+  if (rc) return rc;
+  for (size_t q = 0; q < comp.size(); ++q) out->precip[q] += comp[q];
+  return GWM_B200_OK;
 }
 
 int gwm_b200_advance_dry(gwm_b200_ctx* c, int nsteps) {

@@ -133,6 +133,14 @@ int gwm_b200_download(gwm_b200_ctx* ctx, int member, gwm_b200_fields* host);
 /* nsteps of the prepared-case driver loop (gwm_prepared_case_driver.cpp:427-463):
  * dry SSPRK3 step, then (moist members) tracer transport and warm rain. */
 int gwm_b200_step(gwm_b200_ctx* ctx, int nsteps);
+/* One step of a single-member context from host buffers to host buffers: every field of
+ * the state (and the precipitation of a moist member) copied in from `in`, one
+ * gwm_b200_step, every field copied out to `out` (`in` and `out` may be the same
+ * buffers).  The copies overlap the step on two copy streams: the moisture fields go up
+ * during the dry step, rho and the momenta come down during the tracers and warm rain.
+ * The result equals gwm_b200_upload + gwm_b200_step(1) + gwm_b200_download.  Pinned host
+ * memory gives full PCIe bandwidth.  Returns after the outputs are in `out`. */
+int gwm_b200_step_host(gwm_b200_ctx* ctx, const gwm_b200_fields* in, gwm_b200_fields* out);
 /* advance_dry_state_ssprk3 with NullBoundaryUpdater and LocalSplitExplicitFastMode
  * (include/gwm/dycore/dry_core.hpp:106-110, src/dycore/dry_core.cu:541-651). */
 int gwm_b200_advance_dry(gwm_b200_ctx* ctx, int nsteps);
