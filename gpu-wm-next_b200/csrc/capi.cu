@@ -1794,12 +1794,21 @@ int gwm_b200_step_host(gwm_b200_ctx* c, const gwm_b200_fields* in, gwm_b200_fiel
   cudaEvent_t ev_dry = c->io_ev[9], ev_end = c->io_ev[10];
   const size_t n2 = (size_t)g.nx * g.ny;
   c->cur_launches = 0;
-  // the dry fields up, each packed as soon as it lands
+  // the dry fields up, each packed as soon as it lands; rho and rho*theta first, so the
+  // EOS base state and the theta level sums of the new state run while the momenta land
+  M.theta_valid = false;
+  M.base_valid = false;
   for (int f = 0; f < 5; ++f) {
     CK(cudaMemcpyAsync(stage(f), src[f], count(f) * sizeof(float), cudaMemcpyHostToDevice, c->cin));
     CK(cudaEventRecord(ev_in[f], c->cin));
     CK(cudaStreamWaitEvent(c->stream, ev_in[f], 0));
     CK(launch_pack(g, orient[f], stage(f), dev[f], c->stream));
+    if (f == 1) {
+      int rb = ensure_base(c, M);
+      if (rb) return rb;
+      rb = enqueue_theta(c, M);
+      if (rb) return rb;
+    }
   }
   // the moisture fields up behind them, during the dry step
   if (moist) {
@@ -1811,13 +1820,7 @@ int gwm_b200_step_host(gwm_b200_ctx* c, const gwm_b200_fields* in, gwm_b200_fiel
     CK(cudaMemsetAsync(M.pcomp, 0, n2 * sizeof(double), c->cin));
     CK(cudaEventRecord(ev_in[8], c->cin));
   }
-  M.theta_valid = false;
-  M.base_valid = false;
-  int rc = ensure_base(c, M);
-  if (rc) return rc;
-  rc = enqueue_theta(c, M);
-  if (rc) return rc;
-  rc = enqueue_dry(c, M);
+  int rc = enqueue_dry(c, M);
   if (rc) return rc;
   CK(cudaEventRecord(ev_dry, c->stream));
   // rho and the momenta down while the tracers and the warm rain run
