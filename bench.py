@@ -587,7 +587,8 @@ def c2_grid_and_state(gwm, nx=512, ny=512, nz=80, stretch=0.6):
 
 def c2_line(gwm, torch, stream, dist, world, steps=10, warmup=3, n=512):
     """The mountain-wave configuration: device-timed throughput and its roofline on the
-    1288 B/cell model (terrain kernels on overlapped tiles, tiles chosen by timing)."""
+    1288 B/cell model (tiles chosen by timing; the acoustic substep's candidates are
+    charged their column reference, see Model.autotune)."""
     g, s = c2_grid_and_state(gwm, n, n)
     uref = s["u"].astype(np.float64).mean(axis=(1, 2))
     spec = gwm.MemberSpec(step=gwm.StepConfig(dt=0.5, fast_substeps=6))
@@ -620,8 +621,11 @@ def c2_line(gwm, torch, stream, dist, world, steps=10, warmup=3, n=512):
     return {"workload": f"dry mountain wave, {n}x{n}x80 Agnesi hill, stretched levels to 20 km, N = 0.01, "
                         "Rayleigh layer above 14 km", "dt_s": 0.5, "fast_substeps": 6, "steps": steps,
             "ms_per_step": ms / steps, "value": job_throughput(cells, steps, world, ms), "unit": "cell-updates/s",
-            "tile_rows": tiles, "state_finite": finite,
+            "tile_rows": tiles, "tile_autotune_ms": {k: {str(r): round(t, 4) for r, t in v.items()}
+                                                     for k, v in m.tile_times.items()},
+            "state_finite": finite,
             "kernel_avg_ms": {k: round(v["avg_ms"], 4) for k, v in rep.items()},
+            "kernel_launches_per_step": {k: v["launches"] for k, v in rep.items()},
             "roofline": {"bound": "hbm", "bytes_per_cell_step": C2_BYTES_PER_CELL, "achieved": achieved,
                          "unit": "GB/s", "peak": peak, "peak_source": which, "frac": achieved / peak}}
 

@@ -369,7 +369,8 @@ __device__ __forceinline__ FastCol fast_derive(const FastArgs& a, const FastRaw&
 // bottom to top, the reference pressure and density the terrain substep takes its
 // perturbations about.  A column is a chain of dependent powf evaluations (four
 // fixed-point iterations per level), so it runs apart from the substep with every
-// column in flight at once; the values are the ones the substep used to build inline.
+// column in flight at once; the values are the ones the substep used to build inline
+// (one level per call of fp::column_reference_level).
 __global__ void __launch_bounds__(128) k_column_reference(const FastArgs a) {
   const Geom& g = a.g;
   const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y;
@@ -379,37 +380,9 @@ __global__ void __launch_bounds__(128) k_column_reference(const FastArgs a) {
   for (int k = 0; k < g.nz; ++k) {
     const int o = base + k * g.plane;
     const float rho = __ldg(a.rho_in + o), th = __ldg(a.th + o), z = __ldg(a.zc + o);
-    const float rt = fp::mul(rho, th);
-    const float thp = fp::theta(rho, rt);
-    if (k == 0) {
-      pref = eos_pressure(rho, rt);
-      rref = eos_rho(pref, thp);
-    } else {
-      const float dzk = z - zb;
-      float pn = fmaxf(1.0f, fp::fma(-fp::mul(a.gravity, rref), dzk, pref));
-      // Four fixed-point iterations, then the density of the result.  An iteration that
-      // returns its own input is a fixed point: every later iteration repeats it, and the
-      // final density is the one just evaluated, so the loop stops there with the same
-      // result (the iterations contract by about g dz / (2 c^2) ~ 1e-2 and reach the
-      // FP32 fixed point after two or three of the four).
-      float rn = 0.0f;
-      bool fixed = false;
-      for (int it = 0; it < 4; ++it) {
-        rn = eos_rho(pn, thp);
-        const float pq =
-            fmaxf(fp::fma(-fp::mul(fp::mul(a.gravity, 0.5f), fp::add(rref, rn)), dzk, pref), 1.0f);
-        if (pq == pn) {
-          fixed = true;
-          break;
-        }
-        pn = pq;
-      }
-      pref = pn;
-      rref = fixed ? rn : eos_rho(pn, thp);
-    }
+    fp::column_reference_level(k, rho, fp::mul(rho, th), z, a.gravity, pref, rref, zb);
     a.col_pref[o] = pref;
     a.col_rref[o] = rref;
-    zb = z;
   }
 }
 

@@ -57,8 +57,10 @@ struct FastArgs {
   const float* th;                  // theta frozen for the RK stage
   const float *du_in, *dv_in, *dw_in;   // increments before the substep (null: zero)
   float *du_out, *dv_out, *dw_out;
-  const float* p_in;                // p'(rho_in) from the previous substep (TMA path, not the first)
-  float* p_out;                     // p'(rho_out) for the next substep (TMA path, inner substeps)
+  // pressure of rho_in from the previous substep, and of rho_out for the next one (TMA
+  // paths, inner substeps): the perturbation p' on flat terrain, the full pressure on terrain
+  const float* p_in;
+  float* p_out;
   const float *bu, *bv, *bw;        // stage base momenta (final_kind == 2)
   float *f_rho, *f_rt, *f_u, *f_v, *f_w;  // step result (final_kind == 2)
   int final_kind;                   // 0 inner substep, 1 last of a stage, 2 last of the step

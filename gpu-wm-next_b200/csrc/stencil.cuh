@@ -18,6 +18,8 @@
 
 #include <cuda_runtime.h>
 
+#include "common.cuh"
+
 namespace gwmb {
 namespace fp {
 
@@ -120,6 +122,39 @@ __device__ __forceinline__ V add_buoyancy(V t, V th_l, V th_u, float tref_l, flo
   const V tf = avg(th_l, th_u);
   const V b = div(mul(sc<V>(gravity), sub(tf, sc<V>(trf))), sc<V>(fmaxf(trf, 1.0e-6f)));
   return fma(avg(rho_l, rho_u), b, t);
+}
+
+// K11 build_column_hydrostatic_reference_kernel (dry_fast_modes.cu:108-158), one level of
+// a column, bottom to top: the reference pressure and density at level k from the cell's
+// rho, rho*theta and height z, given those of the level below (pref, rref at height zb);
+// updates pref, rref and zb.  Four fixed-point iterations, then the density of the result.
+// An iteration that returns its own input is a fixed point that every later iteration
+// repeats, and the final density is then the one just evaluated, so the loop stops there
+// with the same result (the iterations contract by about g dz / (2 c^2) ~ 1e-2).
+__device__ __forceinline__ void column_reference_level(int k, float rho, float rt, float z, float gravity,
+                                                       float& pref, float& rref, float& zb) {
+  const float thp = theta(rho, rt);
+  if (k == 0) {
+    pref = eos_pressure(rho, rt);
+    rref = eos_rho(pref, thp);
+  } else {
+    const float dzk = z - zb;
+    float pn = fmaxf(1.0f, fma(-mul(gravity, rref), dzk, pref));
+    float rn = 0.0f;
+    bool fixed = false;
+    for (int it = 0; it < 4; ++it) {
+      rn = eos_rho(pn, thp);
+      const float pq = fmaxf(fma(-mul(mul(gravity, 0.5f), add(rref, rn)), dzk, pref), 1.0f);
+      if (pq == pn) {
+        fixed = true;
+        break;
+      }
+      pn = pq;
+    }
+    pref = pn;
+    rref = fixed ? rn : eos_rho(pn, thp);
+  }
+  zb = z;
 }
 
 }  // namespace fp
