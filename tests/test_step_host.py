@@ -17,9 +17,16 @@ def _pinned_copy(state):
     return out
 
 
-@pytest.mark.parametrize("moist,periodic", [(True, True), (True, False), (False, True)])
-def test_step_host_equals_upload_step_download(gwm, moist, periodic):
-    g = gwm.GridSpec(100, 70, 12, dx=2000.0, dy=2000.0, z_top=12000.0, periodic_x=periodic, periodic_y=periodic)
+@pytest.mark.parametrize("moist,periodic,terrain", [(True, True, False), (True, False, False), (False, True, False),
+                                                   (False, False, True)])
+def test_step_host_equals_upload_step_download(gwm, moist, periodic, terrain):
+    kw = {}
+    if terrain:  # Agnesi hill on stretched levels (the terrain TMA substep and its column reference)
+        eta = (np.exp(1.2 * np.arange(13) / 12) - 1.0) / (np.exp(1.2) - 1.0)
+        kw = dict(terrain=gwm.build_terrain("agnesi", 100, 70, 2000.0, 2000.0, height=400.0,
+                                            half_width_x=12000.0, half_width_y=12000.0), eta_interfaces=eta)
+    g = gwm.GridSpec(100, 70, 12, dx=2000.0, dy=2000.0, z_top=12000.0, periodic_x=periodic, periodic_y=periodic,
+                     **kw)
     p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=21, relative_humidity=1.02, u_background=5.0)
     s = gwm.build_case("moist_sounding" if moist else "warm_bubble", g, p, moist=moist)
     if moist:
