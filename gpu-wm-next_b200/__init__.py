@@ -29,7 +29,8 @@ _LIB_PATH = os.path.join(_HERE, "_build", "libgwm_b200.so")
 # the reference's gwm_idealized_driver command line over the C-ABI (C++, links the library)
 DRIVER_PATH = os.path.join(_HERE, "_build", "gwm_b200_idealized_driver")
 _DRIVER_SRC = os.path.join(_HERE, "drivers", "gwm_b200_idealized_driver.cpp")
-_SOURCES = ["capi.cu", "dycore.cu", "fast_tma.cu", "fast_terrain_tma.cu", "slow_tma.cu", "tracer_tma.cu",
+_SOURCES = ["capi.cu", "dycore.cu", "fast_tma.cu", "fast_terrain_tma.cu", "slow_tma.cu", "slow_terrain_tma.cu",
+            "tracer_tma.cu",
             "physics.cu", "halo.cu", "plan_view.cu", "surrogate.cu", "surrogate_rain.cu", "scalar.cu", "cases.cpp"]
 _HEADERS = ["common.cuh", "stencil.cuh", "dycore.cuh", "physics.cuh", "halo.cuh", "tma.cuh", "plan_view.cuh", "rain_cell.cuh", "surrogate.cuh", "surrogate_rain.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",

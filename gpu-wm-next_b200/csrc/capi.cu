@@ -314,7 +314,7 @@ bool build_substep_maps(Member& M) {
 // Maps of every buffer the terrain TMA substep may read (false if unavailable).
 bool build_terrain_substep_maps(Member& M) {
   M.tmaps.clear();
-  const int* boxes[3] = {kTmaCellBox, kTmaFaceBox, kTmaOwnBox};
+  const int* boxes[4] = {kTmaCellBox, kTmaFaceBox, kTmaOwnBox, kTmaYFaceBox};
   auto add = [&](const float* buf, int kind) {
     CUtensorMap m;
     if (!encode_field_map(&m, buf, M.g, boxes[kind][0], boxes[kind][1])) return false;
@@ -325,6 +325,13 @@ bool build_terrain_substep_maps(Member& M) {
   for (int i = 0; i < 2; ++i) {
     ok = ok && add(M.R[i], 0) && add(M.TH[i], 0) && add(M.P[i], 0) && add(M.R[i], 2) && add(M.TH[i], 2);
     ok = ok && add(M.D[i][0], 1) && add(M.D[i][1], 1) && add(M.D[i][2], 2);
+  }
+  // slow stage: inputs with 40 x 18 boxes (kind 0) and Y faces with 40 x 19 (kind 3)
+  for (int f : {0, 1, 2, 4}) ok = ok && add(M.Q[f], 0);
+  ok = ok && add(M.Q[3], 3);
+  for (int i = 0; i < 2; ++i) {
+    ok = ok && add(M.B[i][0], 0) && add(M.B[i][2], 0) && add(M.B[i][1], 3);
+    ok = ok && add(M.D[i][0], 0) && add(M.D[i][2], 0) && add(M.D[i][1], 3);
   }
   if (!ok) M.tmaps.clear();
   return ok;
@@ -450,9 +457,10 @@ cudaError_t launch_tracers(gwm_b200_ctx* c, const Member& M, const TracerArgs& a
   return launch_tracer_stage(a, c->stream, c->tracer_tile_rows == kTracerTma ? 16 : c->tracer_tile_rows);
 }
 
-// One slow stage: the TMA-fed kernel when selected on flat terrain, else overlapped tiles.
+// One slow stage: the TMA-fed kernels when selected (flat terrain, or terrain without the
+// p' level sums), else overlapped tiles.
 cudaError_t launch_stage(gwm_b200_ctx* c, const Member& M, const SlowArgs& a, bool terr) {
-  if (!terr && !a.tend_only && c->slow_tile_rows == kSlowTma) {
+  if (!a.tend_only && c->slow_tile_rows == kSlowTma && (!terr || a.acc_mode != 1)) {
     SlowMaps m{};
     const CUtensorMap* p[8] = {M.tmap(a.rho, 0), M.tmap(a.th, 0), M.tmap(a.u, 0), M.tmap(a.v, 3),
                                M.tmap(a.w, 0), a.du ? M.tmap(a.du, 0) : nullptr,
@@ -462,6 +470,12 @@ cudaError_t launch_stage(gwm_b200_ctx* c, const Member& M, const SlowArgs& a, bo
     if (a.du && (!p[5] || !p[6] || !p[7] || !a.dv || !a.dw)) return cudaErrorInvalidValue;
     m.rho = *p[0]; m.th = *p[1]; m.u = *p[2]; m.v = *p[3]; m.w = *p[4];
     if (a.du) { m.du = *p[5]; m.dv = *p[6]; m.dw = *p[7]; }
+    if (terr) {
+      const CUtensorMap* z = M.tmap(a.zc, 0);
+      if (!z) return cudaErrorInvalidValue;
+      m.z = *z;
+      return launch_slow_terrain_tma(a, m, c->stream);
+    }
     return launch_slow_tma(a, m, c->stream);
   }
   return launch_slow(a, terr, c->stream, c->slow_tile_rows == kSlowTma ? 16 : c->slow_tile_rows);
@@ -922,7 +936,7 @@ int gwm_b200_create(const gwm_b200_grid_desc* grids, const gwm_b200_member_desc*
   if (e != cudaSuccess) { delete c; return GWM_B200_ERR_CUDA; }
   c->stream = c->own_stream;
   if (init_fast_tma() != cudaSuccess || init_fast_terrain_tma() != cudaSuccess || init_slow_tma() != cudaSuccess ||
-      init_tracer_tma() != cudaSuccess) {
+      init_slow_terrain_tma() != cudaSuccess || init_tracer_tma() != cudaSuccess) {
     cudaStreamDestroy(c->own_stream);
     delete c;
     return GWM_B200_ERR_CUDA;

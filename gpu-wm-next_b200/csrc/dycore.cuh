@@ -46,6 +46,7 @@ struct SlowArgs {
 // padded layout with 40 x 18 boxes (cells, X and Z faces) and 40 x 19 (Y faces).
 struct SlowMaps {
   CUtensorMap rho, th, u, v, w, du, dv, dw;
+  CUtensorMap z;  // cell-centre heights (terrain form only)
 };
 
 // Arguments of one acoustic substep: src/dycore/dry_fast_modes.cu:495-652
@@ -122,6 +123,10 @@ cudaError_t launch_fast(const FastArgs& a, bool first, bool terrain, cudaStream_
 // Flat-terrain slow stage on owned 32 x 16 tiles fed by TMA (not for tend_only).
 cudaError_t launch_slow_tma(const SlowArgs& a, const SlowMaps& m, cudaStream_t s);
 cudaError_t init_slow_tma();
+// Terrain slow stage on owned 32 x 16 tiles fed by TMA (not for tend_only, no p' level
+// sums): the arithmetic of the overlapped-tile terrain kernel; m.z maps the heights.
+cudaError_t launch_slow_terrain_tma(const SlowArgs& a, const SlowMaps& m, cudaStream_t s);
+cudaError_t init_slow_terrain_tma();
 // Flat-terrain acoustic substep fed by TMA tile loads (owned 32 x 16 tiles).
 // first: the first substep of a stage (no increments in); p_ready: its p' (with the
 // halo ring) is in a.p_in, written by the slow stage, instead of derived from rho, theta

@@ -503,39 +503,48 @@ def test_tma_substep_bit_exact(gwm, periodic):
             assert np.array_equal(ref[k], outs[tiles][k]), (tiles, k)
 
 
-@pytest.mark.parametrize("periodic,moist,bnd,ns", [(True, False, False, 4), (False, False, False, 6),
-                                                   (True, True, False, 3), (False, True, True, 4),
-                                                   (False, False, True, 1)])
-def test_terrain_tma_substep_bit_exact(gwm, periodic, moist, bnd, ns):
-    # on terrain, acoustic tiles 3 select the TMA-fed substep (full pressure handed from
-    # substep to substep, dp/dz derived a plane ahead); it runs the overlapped-tile
-    # kernel's arithmetic on the same values: full steps with every substep kind (first,
-    # inner, stage end, step end; one substep that is first and last at once), the
-    # stand-alone fast modes, periodic and open sides with the reference boundary strips,
-    # moist members (theta level sums left to the rain), and 100 x 70 leaves partial tiles
+@pytest.mark.parametrize("periodic,moist,bnd,ns,fast_modes", [(True, False, False, 4, True), (False, False, False, 6, True),
+                                                              (True, True, False, 3, True), (False, True, True, 4, True),
+                                                              (False, False, True, 1, True), (True, False, False, 2, False),
+                                                              (False, True, True, 2, False)])
+def test_terrain_tma_substep_bit_exact(gwm, periodic, moist, bnd, ns, fast_modes):
+    # on terrain, tiles 3 select the TMA-fed acoustic substep (full pressure handed from
+    # substep to substep, dp/dz derived a plane ahead) and the TMA-fed slow stage; they
+    # run the overlapped-tile kernels' arithmetic on the same values: full steps with every
+    # substep kind (first, inner, stage end, step end; one substep that is first and last
+    # at once), stage inputs with and without acoustic increments, fast modes off (theta
+    # level sums from the slow stage), the stand-alone fast modes, periodic and open sides
+    # with the reference boundary strips, moist members (theta level sums left to the
+    # rain), and 100 x 70 leaves partial tiles
     g, s = _c2_case(gwm, nx=100, ny=70, nz=12, periodic=periodic)
     if moist:
         p = gwm.CaseParams(theta_ref=300.0, noise_rms_k=0.5, seed=5, relative_humidity=1.02)
         s = gwm.build_case("moist_sounding", g, p, moist=True)
     b = _boundary_of(s, g, factor=1.002) if bnd else None
-    step = gwm.StepConfig(dt=1.0, fast_substeps=ns)
-    rain = gwm.WarmRainConfig(dt=1.0, rain_terminal_velocity=12.0)
+    step = gwm.StepConfig(dt=1.0 if fast_modes else 0.25, fast_substeps=ns, enable_fast_modes=fast_modes)
+    rain = gwm.WarmRainConfig(dt=step.dt, rain_terminal_velocity=12.0)
     outs, fm = {}, {}
-    for fast in (8, 3):
+    tilings = ((8, 16), (8, 3), (3, 3))   # (acoustic substep, slow stage)
+    for fast, slow in tilings:
         with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=moist)) as m:
             m.set_tile("fast_substep", fast)
+            m.set_tile("slow_stage", slow)
             m.upload(s)
             if b is not None:
                 m.set_boundary_state(b)
             m.step(3)
-            outs[fast] = m.download()
-            m.upload(s)
-            m.fast_modes()
-            fm[fast] = m.download()
-    for k in outs[8]:
-        assert np.array_equal(outs[8][k], outs[3][k]), ("step", k)
-        assert np.array_equal(fm[8][k], fm[3][k]), ("fast_modes", k)
-    assert all(np.isfinite(v).all() for v in outs[3].values())
+            outs[fast, slow] = m.download()
+            if fast_modes:
+                m.upload(s)
+                m.fast_modes()
+                fm[fast, slow] = m.download()
+    ref = tilings[0]
+    for t in tilings[1:]:
+        for k in outs[ref]:
+            assert np.array_equal(outs[ref][k], outs[t][k]), ("step", t, k)
+            if fast_modes:
+                assert np.array_equal(fm[ref][k], fm[t][k]), ("fast_modes", t, k)
+    assert all(np.isfinite(v).all() for v in outs[3, 3].values())
 
 
 @pytest.mark.parametrize("periodic,slow,ns", [(True, 3, 4), (False, 3, 6), (True, 16, 9), (False, 16, 4)])
