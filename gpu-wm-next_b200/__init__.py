@@ -825,24 +825,41 @@ class Model:
             raise ValueError(kernel)
         return r
 
-    def autotune(self, steps: int = 1) -> Dict[str, int]:
+    def autotune(self, steps: int = 1, whole_step: bool = False) -> Dict[str, int]:
         """Pick the fastest tile of each stencil kernel by timing real steps.
 
         Every tiling computes the same values, so the tuning steps are ordinary
         model steps: the state advances by ``steps`` per candidate (10 candidates
-        per pass).  Re-upload the initial state afterwards to start from it.
-        Returns the chosen rows per kernel.  An acoustic substep on terrain is charged the
-        column reference kernel that precedes it, so the time compared is per substep launch."""
+        per pass; one more step each with ``whole_step``).  Re-upload the initial state
+        afterwards to start from it.  Returns the chosen rows per kernel.
+
+        By default each candidate is timed per kernel launch with the profiling events,
+        which run the members one after another; an acoustic substep on terrain is
+        charged the column reference kernel that precedes it.  ``whole_step`` times
+        whole steps instead, replayed from the captured graph with the members running
+        side by side as they do in a timed run (the right measure for an ensemble of small
+        members, whose kernels share the GPU); it leaves graph replay on."""
+        import time
         candidates = {"slow_stage": (3, 8, 16), "fast_substep": (0, 3, 8, 16), "tracer_stage": (3, 8, 16)}
         kinds = {"slow_stage": ("k_slow_stage",), "fast_substep": ("k_fast_substep", "k_column_reference"),
                  "tracer_stage": ("k_tracer_stage",)}
         best = {k: self.get_tile(k) for k in candidates}
         self.tile_times = {}
+        if whole_step:
+            self.use_graph(True)
         for kernel, rows_list in candidates.items():
             times = {}
             self.tile_times[kernel] = times
             for rows in rows_list:
                 self.set_tile(kernel, rows)
+                if whole_step:
+                    self.step(1)            # captures the step graph of this tiling
+                    self.synchronize()
+                    t0 = time.perf_counter()
+                    self.step(steps)
+                    self.synchronize()
+                    times[rows] = (time.perf_counter() - t0) * 1e3 / steps
+                    continue
                 self.profile(True)
                 self.step(steps)
                 rep = self.profile_report()
