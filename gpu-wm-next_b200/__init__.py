@@ -813,10 +813,11 @@ class Model:
     _TILE_KERNELS = {"slow_stage": 0, "fast_substep": 1, "tracer_stage": 2}
 
     def set_tile(self, kernel: str, rows: int):
-        """CTA tile rows of a kernel: "slow_stage" 3 (owned flat tiles fed by TMA), 8 or 16;
-        "tracer_stage" 3 (owned flat tiles fed by TMA), 8 or 16; "fast_substep" 0 (owned
-        flat tiles), 3 (owned flat tiles fed by TMA), 4 (the same, all substeps of an RK
-        stage in one persistent launch), 8 or 16."""
+        """CTA tile rows of a kernel: "slow_stage" 3 (owned tiles fed by TMA, flat terrain
+        and terrain), 8 or 16; "tracer_stage" 3 (owned flat tiles fed by TMA), 8 or 16;
+        "fast_substep" 0 (owned flat tiles), 3 (owned tiles fed by TMA, flat terrain and
+        terrain), 4 (the same, all substeps of a flat RK stage in one persistent launch),
+        8 or 16 (overlapped tiles)."""
         self._check(lib().gwm_b200_set_tile(self._h, self._TILE_KERNELS[kernel], rows), "set_tile")
 
     def get_tile(self, kernel: str) -> int:

@@ -358,14 +358,15 @@ int gwm_b200_plan_view_field(int field, const char** name, const char** units);
 int gwm_b200_plan_view_json(gwm_b200_ctx* ctx, int member, int level, const char* case_kind, int steps, double dt,
                             char* buf, long long cap, long long* len);
 /* Tile shape of a kernel.  kernel 0 = slow stage: rows 3 = owned 32x16 tiles fed by
- * TMA tile loads (flat terrain; terrain falls back to 16), 8 or 16 = overlapped 32-wide
- * tiles (default 16).  kernel 2 = tracer stage: rows 3 = owned 32x16 tiles fed by TMA
- * (flat terrain; terrain falls back to 16), 8 or 16 (overlapped, default 16).  kernel 1 = acoustic substep: rows 0 = owned
- * 32x16 tiles (flat terrain; terrain falls back to 8), 3 = owned 32x16 tiles fed by TMA
- * tile loads (flat terrain; terrain falls back to 8), 4 = the same tiles with all the
- * substeps of an RK stage in one persistent cooperative launch (a bounded grid barrier
- * between substeps; the step's last substep keeps its own launch), 8 or 16 = overlapped
- * 32-wide tiles of that many rows.  The environment variable GWM_B200_FAST_TILE_ROWS sets the
+ * TMA tile loads (flat terrain and terrain; the stand-alone slow tendencies use 16),
+ * 8 or 16 = overlapped 32-wide tiles (default 16).  kernel 2 = tracer stage: rows 3 =
+ * owned 32x16 tiles fed by TMA (flat terrain; terrain falls back to 16), 8 or 16
+ * (overlapped, default 16).  kernel 1 = acoustic substep: rows 0 = owned 32x16 tiles
+ * (flat terrain; terrain falls back to 8), 3 = owned 32x16 tiles fed by TMA tile loads
+ * (flat terrain and terrain), 4 = the same tiles with all the substeps of an RK stage in
+ * one persistent cooperative launch (a bounded grid barrier between substeps; the
+ * step's last substep keeps its own launch; terrain runs one launch per substep), 8 or
+ * 16 = overlapped 32-wide tiles of that many rows.  The environment variable GWM_B200_FAST_TILE_ROWS sets the
  * acoustic default at context creation.  The choice changes speed only: every tiling
  * computes the same values.  gwm_b200_get_tile returns the current rows (or < 0). */
 int gwm_b200_set_tile(gwm_b200_ctx* ctx, int kernel, int rows);
