@@ -814,7 +814,8 @@ class Model:
 
     def set_tile(self, kernel: str, rows: int):
         """CTA tile rows of a kernel: "slow_stage" 3 (owned tiles fed by TMA, flat terrain
-        and terrain), 8 or 16; "tracer_stage" 3 (owned flat tiles fed by TMA), 8 or 16;
+        and terrain), 8 or 16; "tracer_stage" 3 (owned tiles fed by TMA, flat terrain and
+        terrain), 8 or 16;
         "fast_substep" 0 (owned flat tiles), 3 (owned tiles fed by TMA, flat terrain and
         terrain), 4 (the same, all substeps of a flat RK stage in one persistent launch),
         8 or 16 (overlapped tiles)."""

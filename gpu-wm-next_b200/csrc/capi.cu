@@ -333,6 +333,10 @@ bool build_terrain_substep_maps(Member& M) {
     ok = ok && add(M.B[i][0], 0) && add(M.B[i][2], 0) && add(M.B[i][1], 3);
     ok = ok && add(M.D[i][0], 0) && add(M.D[i][2], 0) && add(M.D[i][1], 3);
   }
+  // tracer stage: the three tracer generations (cells), the frozen X/Y fluxes and Z faces
+  if (M.md.moist)
+    for (int t = 0; t < 3; ++t) ok = ok && add(M.T0[t], 0) && add(M.T1[t], 0) && add(M.T2[t], 0);
+  ok = ok && add(M.Q[2], 1) && add(M.Q[3], 1) && add(M.Q[4], 2);
   if (!ok) M.tmaps.clear();
   return ok;
 }
@@ -437,9 +441,9 @@ bool fast_tma_path(const gwm_b200_ctx* c) { return c->fast_tile_rows == kFastTma
 constexpr int kSlowTma = 3;  // slow_tile_rows value selecting the TMA-fed slow stage
 constexpr int kTracerTma = 3;  // tracer_tile_rows value selecting the TMA-fed tracer stage
 
-// One tracer stage: the TMA-fed kernel when selected on flat terrain, else overlapped tiles.
+// One tracer stage: the TMA-fed kernel when selected, else overlapped tiles.
 cudaError_t launch_tracers(gwm_b200_ctx* c, const Member& M, const TracerArgs& a) {
-  if (!a.terrain && c->tracer_tile_rows == kTracerTma) {
+  if (c->tracer_tile_rows == kTracerTma) {
     TracerMaps m{};
     const CUtensorMap* rho = M.tmap(a.rho, 0);
     const CUtensorMap* u = M.tmap(a.u, 1);
@@ -1542,7 +1546,7 @@ int gwm_b200_tracer_add(gwm_b200_ctx* c, int member, const char* name, const cha
   tr.units = units ? units : "";
   tr.positive = positive != 0;
   for (int q = 0; q < 3; ++q) tr.f[q] = (float*)(blk + q * fbytes);
-  if (!M.terrain_active && !M.tmaps.empty()) {  // TMA maps of the tracer stage (cells with the ring)
+  if (!M.tmaps.empty()) {  // TMA maps of the tracer stage (cells with the ring)
     for (int q = 0; q < 3; ++q) {
       CUtensorMap m;
       if (!encode_field_map(&m, tr.f[q], M.g, kTmaCellBox[0], kTmaCellBox[1]))

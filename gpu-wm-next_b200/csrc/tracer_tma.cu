@@ -1,5 +1,5 @@
-// tracer_tma.cu — one SSPRK3 stage of the three passive tracers (flat terrain) on
-// owned tiles fed by TMA.
+// tracer_tma.cu — one SSPRK3 stage of up to three passive tracers on owned tiles fed by
+// TMA (flat terrain, and terrain with the per-cell inverse layer depth).
 //
 // Same operator and per-cell arithmetic as k_tracer_stage: the upwind mixing-ratio
 // flux divergence with frozen end-of-step dry mass fluxes
@@ -38,6 +38,7 @@ static_assert(O_Q - O_RHO >= CBW * CBH && O_U - O_Q >= NTR * 736 && O_V - O_U >=
               "boxes fit their sub-buffers");
 }  // namespace tt
 
+template <bool TERRAIN>
 __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, const __grid_constant__ TracerMaps m) {
   using namespace tt;
   extern __shared__ unsigned char s_dyn[];
@@ -179,17 +180,26 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
   // loop with plain stores instead of the periodic mirror stores; the arithmetic is the same.
   const bool interior = !edge && i0 + TX <= nx && j0 + TY <= ny;
   auto plane_loop = [&](auto tile_class) -> bool {  // true when a bounded wait gave up
+    [[maybe_unused]] constexpr bool IN = decltype(tile_class)::value;
     for (int k = 0; k < nz; ++k) {
       // mixing ratios of plane k+1 (the own ones are this thread's, the ring published
       // by the barrier below for the next plane)
-      const float idz = __ldg(a.idz_c + k);  // loaded ahead of the mixing-ratio work
+      // inverse layer depth (per level on flat terrain, per cell on terrain), loaded ahead
+      // of the mixing-ratio work
+      float idz0, idz1;
+      if constexpr (TERRAIN) {
+        idz0 = (IN || own0) ? __ldg(a.idz_c + gidx(g, gi, gj0, k)) : 0.f;
+        idz1 = (IN || own1) ? __ldg(a.idz_c + gidx(g, gi, gj1, k)) : 0.f;
+      } else {
+        idz0 = idz1 = __ldg(a.idz_c + k);
+      }
       float n0a[NTR], n0b[NTR];
       load_q0(gj0, own0, k + 1, n0a);
       load_q0(gj1, own1, k + 1, n0b);
       wait_plane(k + 1, k);
       if (k + 1 < nz) mix(k + 1);
-      column(tile_class, k, ty + 1, gj0, own0, qb0, q0a, idz);
-      column(tile_class, k, ty + RY + 1, gj1, own1, qb1, q0b, idz);
+      column(tile_class, k, ty + 1, gj0, own0, qb0, q0a, idz0);
+      column(tile_class, k, ty + RY + 1, gj1, own1, qb1, q0b, idz1);
   #pragma unroll
       for (int t = 0; t < NTR; ++t) { q0a[t] = n0a[t]; q0b[t] = n0b[t]; }
       __syncthreads();  // publishes plane k+1's ring; slot k is free
@@ -206,14 +216,18 @@ __global__ void __launch_bounds__(tt::NT, 3) k_tracer_tma(const TracerArgs a, co
 }  // namespace
 
 cudaError_t init_tracer_tma() {
-  return cudaFuncSetAttribute(k_tracer_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tt::kDynSmem);
+  const cudaError_t e =
+      cudaFuncSetAttribute(k_tracer_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tt::kDynSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_tracer_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tt::kDynSmem);
 }
 
 cudaError_t launch_tracer_tma(const TracerArgs& a, const TracerMaps& m, cudaStream_t s) {
-  if (a.g.nz < 1 || !a.err || a.terrain || a.ntracers < 1 || a.ntracers > tt::NTR) return cudaErrorInvalidValue;
+  if (a.g.nz < 1 || !a.err || a.ntracers < 1 || a.ntracers > tt::NTR) return cudaErrorInvalidValue;
   const dim3 block(tt::TX, tt::RY);
   const dim3 grid((a.g.nx + tt::TX - 1) / tt::TX, (a.g.ny + tt::TY - 1) / tt::TY);
-  k_tracer_tma<<<grid, block, tt::kDynSmem, s>>>(a, m);
+  if (a.terrain) k_tracer_tma<true><<<grid, block, tt::kDynSmem, s>>>(a, m);
+  else k_tracer_tma<false><<<grid, block, tt::kDynSmem, s>>>(a, m);
   return cudaGetLastError();
 }
 

@@ -360,8 +360,8 @@ int gwm_b200_plan_view_json(gwm_b200_ctx* ctx, int member, int level, const char
 /* Tile shape of a kernel.  kernel 0 = slow stage: rows 3 = owned 32x16 tiles fed by
  * TMA tile loads (flat terrain and terrain; the stand-alone slow tendencies use 16),
  * 8 or 16 = overlapped 32-wide tiles (default 16).  kernel 2 = tracer stage: rows 3 =
- * owned 32x16 tiles fed by TMA (flat terrain; terrain falls back to 16), 8 or 16
- * (overlapped, default 16).  kernel 1 = acoustic substep: rows 0 = owned 32x16 tiles
+ * owned 32x16 tiles fed by TMA (flat terrain and terrain), 8 or 16 (overlapped,
+ * default 16).  kernel 1 = acoustic substep: rows 0 = owned 32x16 tiles
  * (flat terrain; terrain falls back to 8), 3 = owned 32x16 tiles fed by TMA tile loads
  * (flat terrain and terrain), 4 = the same tiles with all the substeps of an RK stage in
  * one persistent cooperative launch (a bounded grid barrier between substeps; the

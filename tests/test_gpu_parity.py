@@ -509,7 +509,7 @@ def test_tma_substep_bit_exact(gwm, periodic):
                                                               (False, True, True, 2, False)])
 def test_terrain_tma_substep_bit_exact(gwm, periodic, moist, bnd, ns, fast_modes):
     # on terrain, tiles 3 select the TMA-fed acoustic substep (full pressure handed from
-    # substep to substep, dp/dz derived a plane ahead) and the TMA-fed slow stage; they
+    # substep to substep, dp/dz derived a plane ahead), slow stage and tracer stage; they
     # run the overlapped-tile kernels' arithmetic on the same values: full steps with every
     # substep kind (first, inner, stage end, step end; one substep that is first and last
     # at once), stage inputs with and without acoustic increments, fast modes off (theta
@@ -524,27 +524,27 @@ def test_terrain_tma_substep_bit_exact(gwm, periodic, moist, bnd, ns, fast_modes
     step = gwm.StepConfig(dt=1.0 if fast_modes else 0.25, fast_substeps=ns, enable_fast_modes=fast_modes)
     rain = gwm.WarmRainConfig(dt=step.dt, rain_terminal_velocity=12.0)
     outs, fm = {}, {}
-    tilings = ((8, 16), (8, 3), (3, 3))   # (acoustic substep, slow stage)
-    for fast, slow in tilings:
+    tilings = ((8, 16, 16), (8, 3, 16), (3, 3, 3))   # (acoustic substep, slow stage, tracer stage)
+    for t in tilings:
         with gwm.Model(g, gwm.MemberSpec(step=step, rain=rain, moist=moist)) as m:
-            m.set_tile("fast_substep", fast)
-            m.set_tile("slow_stage", slow)
+            for kernel, rows in zip(("fast_substep", "slow_stage", "tracer_stage"), t):
+                m.set_tile(kernel, rows)
             m.upload(s)
             if b is not None:
                 m.set_boundary_state(b)
             m.step(3)
-            outs[fast, slow] = m.download()
+            outs[t] = m.download()
             if fast_modes:
                 m.upload(s)
                 m.fast_modes()
-                fm[fast, slow] = m.download()
+                fm[t] = m.download()
     ref = tilings[0]
     for t in tilings[1:]:
         for k in outs[ref]:
             assert np.array_equal(outs[ref][k], outs[t][k]), ("step", t, k)
             if fast_modes:
                 assert np.array_equal(fm[ref][k], fm[t][k]), ("fast_modes", t, k)
-    assert all(np.isfinite(v).all() for v in outs[3, 3].values())
+    assert all(np.isfinite(v).all() for v in outs[3, 3, 3].values())
 
 
 @pytest.mark.parametrize("periodic,slow,ns", [(True, 3, 4), (False, 3, 6), (True, 16, 9), (False, 16, 4)])
