@@ -417,7 +417,7 @@ def main():
             line["c2"] = c2
         if persistent:
             line["persistent_substeps"] = persistent
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:  # the host cores' baseline: rank 0 at N=1 only
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
     if dist:
