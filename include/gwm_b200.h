@@ -139,7 +139,9 @@ int gwm_b200_step(gwm_b200_ctx* ctx, int nsteps);
  * buffers).  The copies overlap the step on two copy streams: the moisture fields go up
  * during the dry step, rho and the momenta come down during the tracers and warm rain.
  * The result equals gwm_b200_upload + gwm_b200_step(1) + gwm_b200_download.  Pinned host
- * memory gives full PCIe bandwidth.  Returns after the outputs are in `out`. */
+ * memory gives full PCIe bandwidth.  Returns after the outputs are in `out`.  The first call
+ * allocates one device staging buffer per field (together about the state's owned size,
+ * 2.2 GB at 1024 x 1024 x 64) and two copy streams, kept until gwm_b200_destroy. */
 int gwm_b200_step_host(gwm_b200_ctx* ctx, const gwm_b200_fields* in, gwm_b200_fields* out);
 /* advance_dry_state_ssprk3 with NullBoundaryUpdater and LocalSplitExplicitFastMode
  * (include/gwm/dycore/dry_core.hpp:106-110, src/dycore/dry_core.cu:541-651). */
