@@ -267,7 +267,8 @@ def main():
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-microphysics line")
     ap.add_argument("--no-c2", action="store_true", help="skip the mountain-wave (512x512x80 terrain) line")
     ap.add_argument("--only-c2", type=int, default=None, metavar="N",
-                    help="run only the mountain-wave object on an N x N x 80 grid (profiling); prints it alone")
+                    help="run only the mountain-wave object on an N x N x 80 grid (profiling); prints it alone; "
+                         "--fast-tile/--slow-tile/--tracer-tile fix its tiles instead of tuning them")
     ap.add_argument("--only-ensemble", action="store_true",
                     help="run only the 64-member ensemble object (profiling); prints it alone")
     ap.add_argument("--no-persistent", action="store_true",
@@ -294,7 +295,10 @@ def main():
     gwm = importlib.import_module("gpu-wm-next_b200")
     if args.only_c2:
         stream = torch.cuda.Stream()
-        c2 = c2_line(gwm, torch, stream, dist, world, steps=args.steps, warmup=args.warmup, n=args.only_c2)
+        fixed = {k: r for k, r in (("fast_substep", args.fast_tile), ("slow_stage", args.slow_tile),
+                                   ("tracer_stage", args.tracer_tile)) if r is not None}
+        c2 = c2_line(gwm, torch, stream, dist, world, steps=args.steps, warmup=args.warmup, n=args.only_c2,
+                     tiles=fixed or None)
         if rank == 0:
             print(json.dumps({"c2": c2}), flush=True)
         if dist:
@@ -595,10 +599,10 @@ def c2_grid_and_state(gwm, nx=512, ny=512, nz=80, stretch=0.6):
     return g, s
 
 
-def c2_line(gwm, torch, stream, dist, world, steps=10, warmup=3, n=512):
+def c2_line(gwm, torch, stream, dist, world, steps=10, warmup=3, n=512, tiles=None):
     """The mountain-wave configuration: device-timed throughput and its roofline on the
-    1288 B/cell model (tiles chosen by timing; the acoustic substep's candidates are
-    charged their column reference, see Model.autotune)."""
+    1288 B/cell model (tiles chosen by timing, the acoustic substep's candidates charged
+    their column reference, see Model.autotune; or fixed by ``tiles``, kernel -> rows)."""
     g, s = c2_grid_and_state(gwm, n, n)
     uref = s["u"].astype(np.float64).mean(axis=(1, 2))
     spec = gwm.MemberSpec(step=gwm.StepConfig(dt=0.5, fast_substeps=6))
@@ -607,8 +611,14 @@ def c2_line(gwm, torch, stream, dist, world, steps=10, warmup=3, n=512):
         m.set_stream(stream.cuda_stream)
         m.upload(s)
         m.set_damping(14000.0, 0.05, u_ref=uref)
-        with torch.cuda.stream(stream):
-            tiles = m.autotune(1)
+        if tiles:
+            for kernel, rows in tiles.items():
+                m.set_tile(kernel, rows)
+            m.tile_times = {}
+            tiles = {k: m.get_tile(k) for k in ("slow_stage", "fast_substep", "tracer_stage")}
+        else:
+            with torch.cuda.stream(stream):
+                tiles = m.autotune(1)
         m.upload(s)
         m.use_graph(True)
         with torch.cuda.stream(stream):
